@@ -1,0 +1,360 @@
+#!/usr/bin/env python3
+"""Benchmark of the certified exact epsilon-join on B200.
+
+Default workload (N=1): the high-dimensional R-S join, |R| = |S| = 500,000, d = 512,
+rank-32 factor model + N(0, 0.1^2) noise, rows L2-normalised, eps for ~8 neighbours,
+FP16 tensor-core screen + certified band + FP64 refinement, pair set bit-exact to the
+FP64 oracle.  This is the configuration the >= 5x target against the plain FP32
+direct-difference GPU join is stated on.  Data are seeded synthetic arrays with
+those shapes and distributions.
+
+One step = one complete join through the library: index build (Morton sort, operand
+and certificate metadata, tile statistics), candidate tile pairs, tensor-core screen,
+FP64 refinement of the band, radix sort into canonical order and decoding into the
+sorted (i, j) device arrays.  Inputs are resident in HBM (2 x 1 GiB FP32, larger than
+the 126 MB L2, so no separate L2 flush is needed).
+
+metric: distance evaluations per second (candidate pairs screened / step time),
+        whole job over all ranks; ms_per_step is the join wall time.
+e2e:    the same metric through the public API with host (pinned) inputs and host
+        outputs: H2D of R and S and D2H of the (i, j) result inside the timed region.
+--impl reference: the reference's own exact CPU path (SciPy cdist 'sqeuclidean' on
+        FP64-widened rows + <= T, all host cores) on a bounded row sample per step.
+Multi-GPU: one process per GPU (torchrun), independent replicas of the workload
+(the join is single-GPU by design); max step time over ranks; scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "dist_evals_per_s"
+UNIT = "pairs/s"
+WORKLOADS = {
+    "factor512": dict(fn="factor512", screen="fp16", mode="rs"),
+    "mixture64": dict(fn="mixture64", screen="bf16", mode="rs"),
+    "uniform16": dict(fn="uniform16", screen="plain", mode="upper"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="factor512")
+    ap.add_argument("--screen", default=None, help="override the workload's screen (plain/bf16/fp16)")
+    ap.add_argument("--n", type=int, default=0, help="rows per side (0 = the configuration's size)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 GPU baseline run")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-rows", type=int, default=128, help="R rows in the CPU baseline sample")
+    ap.add_argument("--ref-rows", type=int, default=48, help="R rows per step of --impl reference")
+    return ap.parse_args()
+
+
+def make_workload(name: str, n: int):
+    from tensorjoin_variants_b200 import workloads as W
+
+    spec = WORKLOADS[name]
+    fn = getattr(W, spec["fn"])
+    return fn(n=n) if n else fn()
+
+
+# ---------------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampler running during the timed region (reads settings only)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.file.name)
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs"), "tflops": d.get("bf16_tflops"),
+                "tflops_sustained": d.get("bf16_tflops_sustained"), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "tflops": 1590.0, "tflops_sustained": 1400.0, "source": "fallback"}
+
+
+def committed_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/traffic.txt)."""
+    p = ROOT / "profiles" / "traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload and not line.startswith("#"):
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------- reference arm
+def reference_arm(args, rank: int) -> None:
+    if rank != 0:
+        return
+    import oracle
+
+    w = make_workload(args.workload, args.n)
+    S = w.R if w.S is None else w.S
+    rows = min(args.ref_rows, w.R.shape[0])
+    procs = len(os.sched_getaffinity(0))
+    rng = np.random.default_rng(7)
+    sample = w.R[np.sort(rng.choice(w.R.shape[0], rows, replace=False))]
+    pairs, secs, _ = oracle.scipy_rate(sample, S, w.T, procs, rows_per_task=2, repeats=args.warmup + args.steps,
+                                       context="fork")
+    timed = secs[args.warmup:]
+    value = pairs / statistics.mean(timed)
+    full_pairs = w.candidate_pairs_all
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.mean(timed),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args, w),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+                         "sample": f"scipy.spatial.distance.cdist(R64, S64, 'sqeuclidean') <= T (the reference's "
+                                   f"exact CPU path) on {rows} seeded R rows x all {len(S)} S rows per step, "
+                                   f"{procs} processes; full join extrapolated: "
+                                   f"{full_pairs / value:.1f} s"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args, w) -> dict:
+    spec = WORKLOADS[args.workload]
+    S = w.R if w.S is None else w.S
+    return {"workload": args.workload, "n_rows": int(w.R.shape[0]), "n_cols": int(S.shape[0]),
+            "d": int(w.R.shape[1]), "mode": spec["mode"], "screen": args.screen or spec["screen"],
+            "eps": w.eps, "eps2": float(w.T), "target_degree": w.target_degree,
+            "l2": "inputs larger than L2 (no flush needed)", "parallelism": f"replicas x{args.gpus}"}
+
+
+# ---------------------------------------------------------------------- our arm
+def main() -> None:
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import tensorjoin_variants_b200 as tj
+    from tensorjoin_variants_b200 import _lib
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    spec = WORKLOADS[args.workload]
+    screen = args.screen or spec["screen"]
+    mode = spec["mode"]
+    w = make_workload(args.workload, args.n)
+    R = torch.from_numpy(w.R).cuda()
+    S = None if w.S is None else torch.from_numpy(w.S).cuda()
+    T = w.T
+
+    def step():
+        res = tj.join_result(R, S, eps2=T, mode=mode, screen=screen)
+        i, j = res.pairs()
+        return res, i, j
+
+    for _ in range(args.warmup):
+        res, i, j = step()
+        del res, i, j
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        gpu_id = str(local)
+    clocks = Clocks(gpu_id)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = _lib.lib().tj_kernel_launches()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    stats = []
+    count = 0
+    for _ in range(args.steps):
+        res, i, j = step()
+        stats.append(res.stats)
+        count = res.count
+        del res, i, j
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = _lib.lib().tj_kernel_launches() - launches0
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    st = stats[-1]
+    pairs = st["pairs_screened"]
+    value = world * pairs / (ms / 1000.0)
+
+    # dominant kernel: the screen (tensor-core bound); algorithmic flops = 2 d per screened pair
+    peaks = measured_peaks()
+    screen_ms = statistics.mean(s["ms_screen"] for s in stats)
+    d = int(w.R.shape[1])
+    flops = 2.0 * d * pairs
+    if screen == "plain":
+        achieved, unit, bound = flops / (screen_ms / 1000.0) / 1e12, "TFLOP/s", "simt"
+        peak = None
+    else:
+        achieved, unit, bound = flops / (screen_ms / 1000.0) / 1e12, "TFLOP/s", "tensor"
+        peak = peaks["tflops_sustained"]
+    roofline = {"bound": bound, "kernel": "screen_tc_kernel" if screen != "plain" else "plain_kernel",
+                "achieved": achieved, "peak": peak, "unit": unit,
+                "frac": (achieved / peak) if peak else None,
+                "peak_source": f"{peaks['source']} bf16_tflops_sustained (dense fp16 = bf16 rate)",
+                "traffic": committed_traffic("screen_tc_kernel", args.workload),
+                "screen_ms": screen_ms, "flops_per_launch": flops}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": screen if screen != "plain" else "f32", "data": "synthetic",
+        "config": workload_config(args, w), "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
+        "result_pairs": int(count), "stats": {k: st[k] for k in (
+            "pairs_all", "pairs_screened", "tile_pairs", "screen_accept", "band", "refine_accept", "rare_checks",
+            "result_pairs", "retries", "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total")},
+    }
+    line["stats"]["refined_fraction"] = st["band"] / max(1, st["pairs_screened"])
+
+    # plain FP32 direct-difference GPU join over the same candidate tile pairs (the baseline to beat)
+    if not args.no_plain and screen != "plain":
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        resp = tj.join_result(R, S, eps2=T, mode=mode, screen="plain")
+        ip, jp = resp.pairs()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pms = e0.elapsed_time(e1)
+        same = resp.count == count
+        if same and count:
+            res, i, j = step()
+            same = bool(torch.equal(i, ip) and torch.equal(j, jp))
+            del res, i, j
+        line["plain_gpu"] = {"ms_per_step": pms, "value": world * resp.stats["pairs_screened"] / (pms / 1000.0),
+                             "speedup_of_tc_path": pms / ms, "identical_pair_set": same,
+                             "ms_screen": resp.stats["ms_screen"]}
+        del resp, ip, jp
+
+    # end to end through the public API with host buffers (pinned inputs, host outputs)
+    if not args.no_e2e:
+        Rh = torch.from_numpy(w.R).pin_memory()
+        Sh = None if w.S is None else torch.from_numpy(w.S).pin_memory()
+        fn = (lambda: tj.join(Rh, Sh, eps2=T, screen=screen)) if mode == "rs" else \
+            (lambda: tj.self_join(Rh, eps2=T, mode=mode, screen=screen))
+        ih, jh = fn()
+        torch.cuda.synchronize()
+        k_e2e = max(1, min(args.steps, 3))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k_e2e):
+            ih, jh = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1) / k_e2e
+        if world > 1:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        h2d = Rh.numel() * Rh.element_size() + (0 if Sh is None else Sh.numel() * Sh.element_size())
+        line["e2e"] = {"value": world * pairs / (ems / 1000.0), "unit": UNIT, "ms_per_step": ems,
+                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(16 * len(ih)),
+                       "api": "tensorjoin_variants_b200.join(host pinned R, S) -> host (i, j)"}
+
+    # CPU baseline: the reference's exact CPU path on a bounded sample (rank 0 only)
+    if rank == 0 and not args.no_cpu and world == 1:
+        import oracle
+
+        rows = min(args.cpu_rows, w.R.shape[0])
+        rng = np.random.default_rng(7)
+        sample = w.R[np.sort(rng.choice(w.R.shape[0], rows, replace=False))]
+        Sn = w.R if w.S is None else w.S
+        procs = len(os.sched_getaffinity(0))
+        cp, secs, _ = oracle.scipy_rate(sample, Sn, T, procs, rows_per_task=2, repeats=1, context="spawn")
+        rate = cp / secs[0]
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": procs, "kind": "reference",
+                                "sample": f"scipy cdist sqeuclidean (the reference's exact CPU path), {rows} seeded R "
+                                          f"rows x all {len(Sn)} S rows, {procs} spawned processes, "
+                                          f"{secs[0]:.1f} s; full join extrapolated "
+                                          f"{w.candidate_pairs_all / rate:.0f} s"}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,144 @@
+/*
+ * libtensorjoin -- B200 (sm_100a) certified exact epsilon-join, C ABI.
+ *
+ * Every function returns 0 (TJ_OK) or a negative TJ_ERR_* code; the message of
+ * the last failure on the calling thread is available from
+ * tj_last_error_string().  No C++ exception crosses this boundary.  Device
+ * pointers are plain CUDA device addresses (e.g. from torch tensors), `stream`
+ * is a cudaStream_t passed as void*, and the library never frees caller memory.
+ * Handles (tj_result, tj_index) own their device memory until freed; calls on
+ * distinct handles are independent (no global result state).
+ *
+ * Predicate (every mode): a pair (i, j) is in the result iff
+ *     sum_{k=0..d-1} (double(R[i,k]) - double(S[j,k]))^2  <= eps2
+ * evaluated in FP64 in sequential k order (int16 inputs: exact integers).
+ * Results are sorted ascending by (i, j); canonical key = i * n_cols + j.
+ *
+ * Reference interfaces replaced (wangwenqingqq/tensorjoin-variants, paths inside
+ * tensorjoin_20260902_certified_exact_join/):
+ *   - the script-level join contract: FP32 rows in, sorted uint64 canonical ids
+ *     out (src/g2b_public_common.py:97-143, src/run_g2b_tensorjoin_public.py:139-395;
+ *     R-S driver src/run_d1_triton.py:290-420);
+ *   - GDS-Join's ctypes library API GDSJoinPy / copyResultIntoPythonArray
+ *     (adapters/gds_g2a/main.cu:360, :488-510; adapters/gds_g2a/gdsjoingpu.py:146-232);
+ *   - the output-stage library output_mirror / output_sort
+ *     (tensorjoin_20260908_output_audit/src/output.cu:19-31).
+ */
+#ifndef TENSORJOIN_H
+#define TENSORJOIN_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TJ_OK 0
+#define TJ_ERR_INVALID (-1)     /* bad argument (null pointer, d <= 0, unknown mode, ...) */
+#define TJ_ERR_CUDA (-2)        /* a CUDA runtime/driver call failed */
+#define TJ_ERR_INPUT (-3)       /* NaN / Inf or a row norm beyond 2^50 in the input */
+#define TJ_ERR_RANGE (-4)       /* input magnitude outside the FP16 operand range (use BF16) */
+#define TJ_ERR_TIMEOUT (-5)     /* a bounded device wait expired (kernel returned early) */
+#define TJ_ERR_NOMEM (-6)       /* device allocation failed */
+#define TJ_ERR_UNSUPPORTED (-7) /* combination not supported (e.g. int16 with a float screen) */
+
+/* input element type */
+#define TJ_DTYPE_F32 0
+#define TJ_DTYPE_I16 1          /* int14 values in [-8192, 8191] stored as int16 */
+
+/* join mode */
+#define TJ_MODE_RS 0            /* all (i, j), i in R, j in S */
+#define TJ_MODE_UPPER 1         /* self-join (S == R), pairs i < j */
+#define TJ_MODE_DIRECTED 2      /* self-join, all (i, j) incl. the n self pairs (reference canonical form) */
+
+/* distance screen */
+#define TJ_SCREEN_PLAIN 0       /* FP32 direct difference (no tensor cores) + FP64 refinement of the band */
+#define TJ_SCREEN_BF16 1        /* tcgen05 BF16 x BF16 -> FP32 screen + certified band + FP64 refinement */
+#define TJ_SCREEN_FP16 2        /* tcgen05 FP16 x FP16 -> FP32 screen + certified band + FP64 refinement */
+#define TJ_SCREEN_INT8LIMB 3    /* int14 via two int8 limbs, exact INT32 tensor-core products (int16 input) */
+
+typedef struct tj_result tj_result;
+typedef struct tj_index tj_index;
+
+typedef struct tj_options {
+    int64_t initial_capacity;   /* accept / band buffer slots for the first attempt (0: library default) */
+    int32_t chunk_items;        /* tile pairs per scheduling chunk (0: 64) */
+    int32_t flags;              /* reserved, must be 0 */
+} tj_options;
+
+typedef struct tj_stats {
+    int64_t n_rows, n_cols;       /* |R|, |S| (self-join: N, N) */
+    int64_t pairs_all;            /* |R||S| (R-S) or N(N-1)/2 (self-join) */
+    int64_t tile_pairs;           /* candidate tile pairs screened (128 x 256 each) */
+    int64_t pairs_screened;       /* distance evaluations: sum over tile pairs of valid rows x valid cols */
+    int64_t screen_accept;        /* pairs accepted by the certified screen alone */
+    int64_t band;                 /* pairs sent to FP64 refinement */
+    int64_t refine_accept;        /* band pairs accepted by FP64 refinement */
+    int64_t rare_checks;          /* pairs that reached the per-pair FP64 certificate in the screen */
+    int64_t result_pairs;         /* pairs in the output */
+    int64_t retries;              /* capacity retries (overflow-and-retry passes) */
+    double ms_index, ms_candidates, ms_screen, ms_refine, ms_sort, ms_total;   /* device time per stage */
+} tj_stats;
+
+/* ----------------------------------------------------------------- joins */
+
+/* Join R [nR, d] with S [nS, d] (device pointers, row-major, dtype elements).
+ * mode TJ_MODE_RS uses S; the self-join modes ignore S (pass NULL or R).
+ * eps2 is the threshold on the squared distance (eps * eps in FP64; an integer for int16 input).
+ * On success *out receives a result handle (free with tj_result_free). */
+int tj_join(const void* R, int64_t nR, const void* S, int64_t nS, int32_t d, int32_t dtype, double eps2,
+            int32_t mode, int32_t screen, const tj_options* opt, tj_result** out, void* stream);
+
+int64_t tj_result_count(const tj_result* res);
+int tj_result_stats(const tj_result* res, tj_stats* out);
+/* Sorted pairs as two int64 device arrays of tj_result_count() elements each. */
+int tj_result_pairs(const tj_result* res, int64_t* i_out, int64_t* j_out, void* stream);
+/* Sorted canonical keys i * n_cols + j (uint64 device array of tj_result_count() elements). */
+int tj_result_keys(const tj_result* res, uint64_t* keys_out, void* stream);
+/* GDS-style neighbour table: counts[n_rows] (uint32, device) and the flat j list (int64, device). */
+int tj_result_neighbor_table(const tj_result* res, uint32_t* counts_out, int64_t* flat_out, void* stream);
+void tj_result_free(tj_result* res);
+
+/* ----------------------------------------------------------------- index */
+
+/* Build the Morton-grid index of X [n, d] (device pointer): point permutation, cells with
+ * prefix-sum offsets, and the 128-row tile statistics used for candidate pruning at threshold eps2. */
+int tj_index_build(const void* X, int64_t n, int32_t d, int32_t dtype, double eps2, tj_index** out, void* stream);
+int tj_index_info(const tj_index* idx, int64_t* n_cells, int64_t* n_tiles, int64_t* n_candidate_tile_pairs);
+/* perm[n] (uint32: sorted position -> input row), keys[n] (uint64 Morton keys, sorted),
+ * cell_start[n_cells + 1] (uint32 prefix offsets), candidate tile pairs as (I, J) uint32 pairs.
+ * Any output pointer may be NULL. Device pointers. */
+int tj_index_copy(const tj_index* idx, uint32_t* perm, uint64_t* keys, uint32_t* cell_start, uint32_t* tile_pairs,
+                  void* stream);
+void tj_index_free(tj_index* idx);
+
+/* ----------------------------------------------------------------- batched ragged joins */
+
+typedef struct tj_batch_join {
+    const void* R;   /* device pointer [nR, d] */
+    const void* S;   /* device pointer [nS, d] */
+    int64_t nR, nS;
+    int32_t d;
+    int32_t pad;
+    double eps2;
+} tj_batch_join;
+
+/* Run `njoins` independent R-S joins (FP32) in one persistent launch per stage.  The result holds
+ * all joins' pairs; tj_batch_offsets gives each join's [start, end) range in the sorted output. */
+int tj_join_batched(const tj_batch_join* joins, int32_t njoins, int32_t screen, const tj_options* opt,
+                    tj_result** out, void* stream);
+int tj_batch_offsets(const tj_result* res, int64_t* offsets_host /* njoins + 1 */);
+int tj_batch_pairs(const tj_result* res, int64_t* i_out, int64_t* j_out, void* stream);
+
+/* ----------------------------------------------------------------- misc */
+const char* tj_last_error_string(void);
+int tj_version(void);
+int tj_device_sm_count(void);
+/* Running total of kernels this library has launched in the process (audit of timed regions). */
+int64_t tj_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TENSORJOIN_H */

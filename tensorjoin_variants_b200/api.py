@@ -1,0 +1,233 @@
+"""Python drop-in for the certified exact epsilon-join.
+
+``join(R, S, eps)`` and ``self_join(X, eps)`` return the pair set
+``{(i, j) : sum_k (double(R[i,k]) - double(S[j,k]))^2 <= eps^2}`` (FP64, sequential
+k order; exact integers for int16 input) as two int64 arrays sorted by (i, j).
+``build_index(X, eps)`` exposes the Morton-grid index.  Inputs may be CUDA
+tensors (results stay on the device) or host arrays / CPU tensors (inputs are
+copied in on the current stream and results come back to the host).
+
+The reference has no library API for this path; these functions give its
+script-level contract a callable form: FP32 rows in, sorted canonical ids out
+(tensorjoin_20260902_certified_exact_join/src/g2b_public_common.py:97-143),
+self-join and R-S modes (src/run_g2a2_tensorjoin_triangular.py:42-141,
+src/run_d1_triton.py:110-248), canonical keys ``i * n_cols + j`` and the
+GDS-style neighbour table (adapters/gds_g2a/main.cu:488-510).
+Every computation runs in libtensorjoin.so on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import MODE, SCREEN, check, lib
+
+__all__ = ["join", "self_join", "join_result", "build_index", "Result", "Index", "join_batched"]
+
+
+def _stream_ptr() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _as_device(x, allow_int16: bool):
+    """Return (device tensor, was_host).  Host inputs are copied in on the current stream."""
+    was_host = True
+    if isinstance(x, torch.Tensor):
+        t = x
+        if t.is_cuda:
+            was_host = False
+        else:
+            t = t.to("cuda", non_blocking=t.is_pinned())
+    else:
+        arr = np.asarray(x)
+        if arr.dtype not in (np.float32, np.int16):
+            arr = arr.astype(np.float32)
+        t = torch.from_numpy(np.ascontiguousarray(arr)).to("cuda")
+    if t.dim() != 2:
+        raise ValueError("inputs must be 2-D [rows, dims]")
+    if t.dtype not in (torch.float32, torch.int16):
+        raise TypeError(f"unsupported dtype {t.dtype}: use float32 (or int16 for int14 data)")
+    if t.dtype == torch.int16 and not allow_int16:
+        raise TypeError("int16 input needs screen='int8limb'")
+    return t.contiguous(), was_host
+
+
+def _threshold(eps, eps2) -> float:
+    if eps2 is not None:
+        return float(eps2)
+    if eps is None:
+        raise ValueError("give eps or eps2")
+    e = float(eps)
+    if not (e >= 0) or math.isinf(e):
+        raise ValueError("eps must be finite and >= 0")
+    return e * e
+
+
+class Result:
+    """Owns a tj_result handle: sorted canonical pairs on the device plus statistics."""
+
+    def __init__(self, handle: C.c_void_p, n_rows: int, n_cols: int, host: bool, keepalive=()):
+        self._h = handle
+        self.n_rows, self.n_cols, self.host = n_rows, n_cols, host
+        self._keep = keepalive
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().tj_result_free(h)
+            self._h = None
+
+    @property
+    def count(self) -> int:
+        return int(lib().tj_result_count(self._h))
+
+    @property
+    def stats(self) -> dict:
+        s = _lib.Stats()
+        check(lib().tj_result_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def _out(self, *ts):
+        return tuple(t.cpu() for t in ts) if self.host else ts
+
+    def pairs(self):
+        n = self.count
+        i = torch.empty(n, dtype=torch.int64, device="cuda")
+        j = torch.empty(n, dtype=torch.int64, device="cuda")
+        if n:
+            check(lib().tj_result_pairs(self._h, C.c_void_p(i.data_ptr()), C.c_void_p(j.data_ptr()),
+                                        C.c_void_p(_stream_ptr())))
+        return self._out(i, j)
+
+    def keys(self):
+        """Canonical keys i * n_cols + j (int64 tensor holding the uint64 values, ascending)."""
+        n = self.count
+        k = torch.empty(n, dtype=torch.int64, device="cuda")
+        if n:
+            check(lib().tj_result_keys(self._h, C.c_void_p(k.data_ptr()), C.c_void_p(_stream_ptr())))
+        return self._out(k)[0]
+
+    def neighbor_table(self):
+        """GDS-style output: neighbour counts per row and the flat, row-ordered neighbour list."""
+        counts = torch.empty(self.n_rows, dtype=torch.int32, device="cuda")
+        flat = torch.empty(self.count, dtype=torch.int64, device="cuda")
+        check(lib().tj_result_neighbor_table(self._h, C.c_void_p(counts.data_ptr()), C.c_void_p(flat.data_ptr()),
+                                             C.c_void_p(_stream_ptr())))
+        return self._out(counts, flat)
+
+
+def _run(R, S, eps, eps2, mode: str, screen: str, capacity: int, chunk_items: int) -> Result:
+    if screen not in SCREEN:
+        raise ValueError(f"screen must be one of {sorted(SCREEN)}")
+    Rt, host = _as_device(R, screen == "int8limb")
+    if mode == "rs":
+        St, host_s = _as_device(S, screen == "int8limb")
+        host = host and host_s
+        if St.shape[1] != Rt.shape[1]:
+            raise ValueError("R and S must have the same number of dimensions")
+        if St.dtype != Rt.dtype:
+            raise TypeError("R and S must have the same dtype")
+    else:
+        St = Rt
+    T = _threshold(eps, eps2)
+    dtype = _lib.DTYPE["i16"] if Rt.dtype == torch.int16 else _lib.DTYPE["f32"]
+    opt = _lib.Options(int(capacity), int(chunk_items), 0)
+    h = C.c_void_p()
+    check(lib().tj_join(C.c_void_p(Rt.data_ptr()), Rt.shape[0], C.c_void_p(St.data_ptr()), St.shape[0],
+                        Rt.shape[1], dtype, T, MODE[mode], SCREEN[screen], C.byref(opt), C.byref(h),
+                        C.c_void_p(_stream_ptr())))
+    return Result(h, Rt.shape[0], St.shape[0] if mode == "rs" else Rt.shape[0], host, keepalive=(Rt, St))
+
+
+def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "bf16", capacity: int = 0,
+                chunk_items: int = 0) -> Result:
+    """Run a join and return the Result handle (pairs, keys, neighbour table, statistics)."""
+    if mode not in MODE:
+        raise ValueError(f"mode must be one of {sorted(MODE)}")
+    return _run(R, S, eps, eps2, mode, screen, capacity, chunk_items)
+
+
+def join(R, S, eps=None, *, eps2=None, screen: str = "bf16", return_stats: bool = False, **kw):
+    """R-S epsilon-join: sorted (i, j) with FP64 direct-difference distance <= eps."""
+    res = _run(R, S, eps, eps2, "rs", screen, kw.get("capacity", 0), kw.get("chunk_items", 0))
+    i, j = res.pairs()
+    return (i, j, res.stats) if return_stats else (i, j)
+
+
+def self_join(X, eps=None, *, eps2=None, mode: str = "upper", screen: str = "bf16", return_stats: bool = False,
+              **kw):
+    """Self-join: mode 'upper' gives i < j; 'directed' gives all (i, j) incl. the N self pairs."""
+    if mode not in ("upper", "directed"):
+        raise ValueError("self_join mode must be 'upper' or 'directed'")
+    res = _run(X, None, eps, eps2, mode, screen, kw.get("capacity", 0), kw.get("chunk_items", 0))
+    i, j = res.pairs()
+    return (i, j, res.stats) if return_stats else (i, j)
+
+
+@dataclass
+class Index:
+    """Morton-grid index of one point set (device tensors)."""
+    perm: torch.Tensor         # [n] int32: sorted position -> input row
+    keys: torch.Tensor         # [n] int64: Morton keys, ascending
+    cell_start: torch.Tensor   # [n_cells + 1] int32: prefix offsets of the cells in sorted order
+    tile_pairs: torch.Tensor   # [P, 2] int32: candidate (128-row tile, 256-row tile) pairs at eps
+    n_tiles: int
+
+
+def build_index(X, eps=None, *, eps2=None) -> Index:
+    """Build the GPU Morton-grid index of X (cells, prefix offsets, candidate tile pairs at eps)."""
+    Xt, _ = _as_device(X, True)
+    T = _threshold(eps, eps2)
+    dtype = _lib.DTYPE["i16"] if Xt.dtype == torch.int16 else _lib.DTYPE["f32"]
+    h = C.c_void_p()
+    check(lib().tj_index_build(C.c_void_p(Xt.data_ptr()), Xt.shape[0], Xt.shape[1], dtype, T, C.byref(h),
+                               C.c_void_p(_stream_ptr())))
+    try:
+        nc, nt, npairs = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().tj_index_info(h, C.byref(nc), C.byref(nt), C.byref(npairs)))
+        n = Xt.shape[0]
+        perm = torch.empty(n, dtype=torch.int32, device="cuda")
+        keys = torch.empty(n, dtype=torch.int64, device="cuda")
+        cs = torch.empty(nc.value + 1, dtype=torch.int32, device="cuda")
+        tp = torch.empty((npairs.value, 2), dtype=torch.int32, device="cuda")
+        check(lib().tj_index_copy(h, C.c_void_p(perm.data_ptr()), C.c_void_p(keys.data_ptr()),
+                                  C.c_void_p(cs.data_ptr()), C.c_void_p(tp.data_ptr() if npairs.value else 0),
+                                  C.c_void_p(_stream_ptr())))
+        torch.cuda.current_stream().synchronize()
+    finally:
+        lib().tj_index_free(h)
+    return Index(perm, keys, cs, tp, int(nt.value))
+
+
+def join_batched(joins, screen: str = "bf16"):
+    """Many independent R-S joins [(R, S, eps), ...] in one batched pass; returns [(i, j), ...]."""
+    descs = (_lib.BatchJoin * len(joins))()
+    keep = []
+    host = True
+    for k, (R, S, eps) in enumerate(joins):
+        Rt, hr = _as_device(R, False)
+        St, hs = _as_device(S, False)
+        host = host and hr and hs
+        keep += [Rt, St]
+        descs[k] = _lib.BatchJoin(Rt.data_ptr(), St.data_ptr(), Rt.shape[0], St.shape[0], Rt.shape[1], 0,
+                                  _threshold(eps, None))
+    h = C.c_void_p()
+    opt = _lib.Options(0, 0, 0)
+    check(lib().tj_join_batched(descs, len(joins), SCREEN[screen], C.byref(opt), C.byref(h),
+                                C.c_void_p(_stream_ptr())))
+    res = Result(h, 0, 0, host, keepalive=tuple(keep))
+    offs = (C.c_int64 * (len(joins) + 1))()
+    check(lib().tj_batch_offsets(h, offs))
+    n = offs[len(joins)]
+    i = torch.empty(n, dtype=torch.int64, device="cuda")
+    j = torch.empty(n, dtype=torch.int64, device="cuda")
+    if n:
+        check(lib().tj_batch_pairs(h, C.c_void_p(i.data_ptr()), C.c_void_p(j.data_ptr()), C.c_void_p(_stream_ptr())))
+    if host:
+        i, j = i.cpu(), j.cpu()
+    return [(i[offs[k]:offs[k + 1]], j[offs[k]:offs[k + 1]]) for k in range(len(joins))]

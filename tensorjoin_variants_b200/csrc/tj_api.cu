@@ -1,0 +1,545 @@
+// C ABI of libtensorjoin: orchestration of index -> candidates -> screen -> refine -> sort.
+//
+// One host synchronisation per join: after the screen and the refinement the
+// counters are read back once to size the output (and to detect a capacity
+// overflow, in which case both stages run again with larger buffers -- the
+// overflow-and-retry pass of the reference, src/run_g2a_tensorjoin.py:329-378).
+// Everything else stays on the device in stream order; memory comes from a
+// private stream-ordered pool so repeated joins do not hit cudaMalloc.
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "../../include/tensorjoin.h"
+#include "tj_internal.h"
+
+namespace tj {
+
+// ------------------------------------------------------------------ errors
+namespace {
+thread_local std::string g_last_error;
+}
+
+void fail(int code, const std::string& msg) { throw Error{code, msg}; }
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    const int code = (e == cudaErrorMemoryAllocation) ? TJ_ERR_NOMEM : TJ_ERR_CUDA;
+    fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ------------------------------------------------------------------ memory pool
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+int g_sms[64] = {};
+
+cudaMemPool_t pool_for_current() {
+    int dev = 0;
+    TJ_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        TJ_CUDA(cudaMemPoolCreate(&g_pools[dev], &props));
+        uint64_t thr = ~0ull;
+        TJ_CUDA(cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &thr));
+    }
+    return g_pools[dev];
+}
+}  // namespace
+
+void* dalloc(size_t bytes, cudaStream_t st) {
+    void* p = nullptr;
+    const cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool_for_current(), st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(TJ_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    return p;
+}
+
+void dfree(void* p, cudaStream_t st) {
+    if (p) cudaFreeAsync(p, st);
+}
+
+namespace {
+std::atomic<long long> g_launches{0};
+}
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+int num_sms() {
+    int dev = 0;
+    TJ_CUDA(cudaGetDevice(&dev));
+    if (!g_sms[dev]) TJ_CUDA(cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev));
+    return g_sms[dev];
+}
+
+// ------------------------------------------------------------------ helpers
+namespace {
+
+__global__ void zero_counters(Counters* c, int emit_only) {
+    unsigned long long* w = (unsigned long long*)c;
+    const int n = emit_only ? 8 : (int)(sizeof(Counters) / 8);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) w[i] = 0;
+}
+
+__global__ void cell_flags(const uint64_t* keys, long long n, uint32_t* flag) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+__global__ void cell_starts(const uint32_t* flag, const uint32_t* pos, long long n, uint32_t* start,
+                            const uint32_t* ncells) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && flag[i]) start[pos[i]] = (uint32_t)i;
+    if (i == 0) start[*ncells] = (uint32_t)n;
+}
+__global__ void pairs_screened_kernel(const uint4* chunks, const uint32_t* nchunks, const uint32_t* jlist,
+                                      const uint32_t* rnv, const uint32_t* snv, unsigned long long* out) {
+    unsigned long long acc = 0;
+    const unsigned n = *nchunks;
+    for (unsigned c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const uint4 ch = chunks[c];
+        const unsigned long long rv = rnv[ch.x];
+        for (unsigned e = ch.y; e < ch.z; ++e) acc += rv * snv[jlist[e]];
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+}
+__global__ void tile_pair_list(const uint4* chunks, const uint32_t* nchunks, const uint32_t* jlist, uint32_t* out) {
+    const unsigned n = *nchunks;
+    for (unsigned c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const uint4 ch = chunks[c];
+        for (unsigned e = ch.y; e < ch.z; ++e) {
+            out[2 * (size_t)e] = ch.x;
+            out[2 * (size_t)e + 1] = jlist[e];
+        }
+    }
+}
+__global__ void neighbor_counts(const uint64_t* keys, long long n, long long n_cols, uint32_t* counts,
+                                int64_t* flat) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint64_t k = keys[t];
+    const uint64_t i = k / (uint64_t)n_cols;
+    atomicAdd(&counts[i], 1u);
+    if (flat) flat[t] = (int64_t)(k - i * (uint64_t)n_cols);
+}
+
+int bits_for(unsigned long long max_value) {
+    int b = 1;
+    while (b < 64 && (max_value >> b) != 0) ++b;
+    return b;
+}
+
+struct Events {
+    cudaEvent_t e[8];
+    int n = 0;
+    Events() { for (auto& x : e) cudaEventCreate(&x); }
+    ~Events() { for (auto& x : e) cudaEventDestroy(x); }
+    void rec(int i, cudaStream_t st) { cudaEventRecord(e[i], st); n = i + 1 > n ? i + 1 : n; }
+    double ms(int a, int b) const {
+        float m = 0.f;
+        cudaEventElapsedTime(&m, e[a], e[b]);
+        return (double)m;
+    }
+};
+
+}  // namespace
+
+// Threshold constants of the certificate.
+JoinParams make_params(double T, int d, int kpad, long long nr, long long nc, bool self_join) {
+    JoinParams jp;
+    memset(&jp, 0, sizeof(jp));
+    jp.T = T;
+    // |fp64 oracle value - D| <= g64 * D (d subtractions, squares and additions, u = 2^-53)
+    const double nu = (double)(d + 2) * 0x1p-53;
+    const double g64 = nu / (1.0 - nu);
+    jp.Tm = T / (1.0 + g64) * (1.0 - 0x1p-50);
+    jp.Tp = T / (1.0 - g64) * (1.0 + 0x1p-50);
+    jp.gn = 2.0 * (double)(d + 2) * 0x1p-53;
+    jp.gmma = (double)(kpad + 64) * 0x1p-22;
+    jp.cabs = (double)(kpad + 64) * 0x1p-125;
+    jp.key_off = 0;
+    jp.n_rows = nr;
+    jp.n_cols = nc;
+    jp.self_join = self_join ? 1 : 0;
+    jp.d = d;
+    return jp;
+}
+
+}  // namespace tj
+
+// ====================================================================== C ABI
+using namespace tj;
+
+struct tj_result {
+    DBuf<uint64_t> keys;       // sorted canonical keys (first `count` valid)
+    long long count = 0;
+    long long n_rows = 0, n_cols = 0;
+    tj_stats stats;
+    // batched mode
+    std::vector<int64_t> offsets;
+    std::vector<long long> join_cols;
+    std::vector<unsigned long long> join_keyoff;
+    DBuf<unsigned long long> d_keyoff;
+    DBuf<long long> d_cols;
+};
+
+struct tj_index {
+    Side side;
+    TileSet t128, t256;
+    Candidates cand;
+    DBuf<uint32_t> cell_start;
+    long long n_cells = 0;
+    long long n_tile_pairs = 0;
+};
+
+#define TJ_API_BEGIN try {
+#define TJ_API_END                                          \
+    }                                                       \
+    catch (const tj::Error& e) {                            \
+        g_last_error = e.msg;                               \
+        return e.code;                                      \
+    }                                                       \
+    catch (const std::exception& e) {                       \
+        g_last_error = e.what();                            \
+        return TJ_ERR_INVALID;                              \
+    }                                                       \
+    catch (...) {                                           \
+        g_last_error = "unknown error";                     \
+        return TJ_ERR_INVALID;                              \
+    }
+
+namespace {
+
+void check_status(unsigned long long status) {
+    if (status & kStatusWaitTimeout) fail(TJ_ERR_TIMEOUT, "a bounded device wait expired; the kernel returned early");
+    if (status & kStatusBadInput) fail(TJ_ERR_INPUT, "input contains NaN/Inf or a row norm beyond 2^50");
+    if (status & kStatusFp16Range) fail(TJ_ERR_RANGE, "input magnitude exceeds the FP16 range; use the BF16 screen");
+    if (status & kStatusTmemAlloc) fail(TJ_ERR_CUDA, "tensor memory allocation failed");
+}
+
+void run_join(const void* R, long long nR, const void* S, long long nS, int d, int dtype, double eps2, int mode,
+              int screen, const tj_options* opt, tj_result* res, cudaStream_t st) {
+    const bool self = mode != TJ_MODE_RS;
+    if (self) { S = R; nS = nR; }
+    if (!R || (nR > 0 && !S)) fail(TJ_ERR_INVALID, "null input pointer");
+    if (d <= 0 || nR < 0 || nS < 0) fail(TJ_ERR_INVALID, "invalid shape");
+    if (nR >= (1ll << 32) || nS >= (1ll << 32)) fail(TJ_ERR_INVALID, "more than 2^32 - 1 rows per side");
+    if (!(eps2 >= 0.0) || std::isinf(eps2)) fail(TJ_ERR_INVALID, "eps2 must be finite and >= 0");
+    if (dtype == TJ_DTYPE_I16 && screen != TJ_SCREEN_INT8LIMB && screen != TJ_SCREEN_PLAIN)
+        fail(TJ_ERR_UNSUPPORTED, "int16 input needs the int8-limb or plain screen");
+    if (dtype == TJ_DTYPE_F32 && screen == TJ_SCREEN_INT8LIMB)
+        fail(TJ_ERR_UNSUPPORTED, "the int8-limb screen needs int16 (int14) input");
+    if (dtype == TJ_DTYPE_I16 && screen == TJ_SCREEN_PLAIN)
+        fail(TJ_ERR_UNSUPPORTED, "plain screen on int16 input is not provided; use TJ_SCREEN_INT8LIMB");
+    if (screen == TJ_SCREEN_INT8LIMB) fail(TJ_ERR_UNSUPPORTED, "int8-limb screen not built in this version");
+    const int chunk_items = (opt && opt->chunk_items > 0) ? opt->chunk_items : 64;
+
+    memset(&res->stats, 0, sizeof(res->stats));
+    res->n_rows = nR;
+    res->n_cols = nS;
+    tj_stats& S_ = res->stats;
+    S_.n_rows = nR;
+    S_.n_cols = nS;
+    S_.pairs_all = self ? nR * (nR - 1) / 2 : nR * nS;
+    if (nR == 0 || nS == 0) {
+        res->count = 0;
+        return;
+    }
+    Events ev;
+    ev.rec(0, st);
+    DBuf<Counters> ctr(1, st);
+    launch(zero_counters, 1, 32, 0, st, ctr.p, 0);
+    DBuf<FrameParams> fp(1, st);
+    {
+        const void* srcs[2] = {R, S};
+        const long long ns[2] = {nR, nS};
+        compute_frame(srcs, ns, self ? 1 : 2, d, dtype, fp.p, st);
+    }
+    Side sR, sS_;
+    sR.src = R; sR.dtype = dtype; sR.n = nR; sR.d = d; sR.screen = screen;
+    prepare_side(sR, fp.p, st, &ctr.p->status);
+    Side* pS = &sR;
+    if (!self) {
+        sS_.src = S; sS_.dtype = dtype; sS_.n = nS; sS_.d = d; sS_.screen = screen;
+        prepare_side(sS_, fp.p, st, &ctr.p->status);
+        pS = &sS_;
+    }
+    TileSet tR, tS;
+    tile_stats(sR, kTileR, tR, st);
+    tile_stats(*pS, kTileS, tS, st);
+    ev.rec(1, st);
+    const JoinParams jp = make_params(eps2, d, sR.kpad, nR, nS, self);
+    Candidates cand;
+    build_candidates(tR, tS, jp.Tp, self, chunk_items, cand, st);
+    // distance evaluations of the candidate list (read back with the counters)
+    launch(pairs_screened_kernel, num_sms() * 4, 256, 0, st, cand.chunks.p, cand.dev_counts.p + 1, cand.jlist.p,
+                                                         tR.nvalid.p, tS.nvalid.p, &ctr.p->pad[0]);
+    TJ_CUDA(cudaGetLastError());
+    ev.rec(2, st);
+
+    JoinGeometry g{&sR, pS, &tR, &tS, &cand, jp};
+    unsigned long long cap = (opt && opt->initial_capacity > 0) ? (unsigned long long)opt->initial_capacity
+                                                                : std::max<unsigned long long>(1ull << 20,
+                                                                      64ull * (unsigned long long)std::max(nR, nS));
+    unsigned long long bcap = cap;
+    DBuf<uint64_t> acc, band;
+    Counters h;
+    for (int attempt = 0;; ++attempt) {
+        acc = DBuf<uint64_t>(cap, st);
+        band = DBuf<uint64_t>(bcap, st);
+        launch(zero_counters, 1, 32, 0, st, ctr.p, 1);
+        EmitBuffers eb{acc.p, cap, band.p, bcap, ctr.p};
+        ev.rec(2, st);
+        if (screen == TJ_SCREEN_PLAIN) screen_plain(g, eb, st);
+        else screen_tc(g, eb, st);
+        ev.rec(3, st);
+        refine_band(g, eb, st);
+        ev.rec(4, st);
+        TJ_CUDA(cudaMemcpyAsync(&h, ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        TJ_CUDA(cudaStreamSynchronize(st));
+        check_status(h.status);
+        const bool over = h.acc_reserved > cap || h.band_reserved > bcap;
+        if (!over) break;
+        if (attempt >= 6) fail(TJ_ERR_NOMEM, "output capacity retries exhausted");
+        S_.retries++;
+        cap = std::max(cap * 2, h.acc_reserved + h.acc_reserved / 4 + 4096);
+        bcap = std::max(bcap * 2, h.band_reserved + h.band_reserved / 4 + 4096);
+    }
+    S_.tile_pairs = (int64_t)h.items;
+    S_.pairs_screened = (int64_t)h.pad[0];
+    S_.screen_accept = (int64_t)h.screen_accept;
+    S_.band = (int64_t)h.band_valid;
+    S_.refine_accept = (int64_t)h.refine_accept;
+    S_.rare_checks = (int64_t)h.rare_checks;
+    band.reset();
+
+    // canonical order: (directed expansion) + radix sort on the trimmed key width
+    unsigned long long slots = h.acc_reserved;
+    long long nvalid = (long long)h.acc_valid;
+    unsigned long long max_key = (unsigned long long)nR * (unsigned long long)nS;   // + 1 > any valid key
+    DBuf<uint64_t> keys;
+    if (mode == TJ_MODE_DIRECTED) {
+        const unsigned long long nk = 2 * slots + (unsigned long long)nR;
+        keys = DBuf<uint64_t>(nk, st);
+        expand_directed(acc.p, slots, keys.p, nR, st);
+        acc.reset();
+        slots = nk;
+        nvalid = 2 * nvalid + nR;
+    } else {
+        keys = std::move(acc);
+    }
+    const int bits = bits_for(max_key);   // sentinel low bits (all ones) exceed every valid key
+    if (slots > 1) {
+        DBuf<uint64_t> ktmp(slots, st);
+        DBuf<uint32_t> ws(radix_workspace_elems(slots), st);
+        radix_sort(keys.p, nullptr, ktmp.p, nullptr, slots, bits, ws.p, st);
+    }
+    ev.rec(5, st);
+    TJ_CUDA(cudaStreamSynchronize(st));
+    res->keys = std::move(keys);
+    res->count = nvalid;
+    S_.result_pairs = nvalid;
+    S_.ms_index = ev.ms(0, 1);
+    S_.ms_candidates = ev.ms(1, 2) > 0 ? ev.ms(1, 2) : 0.0;
+    S_.ms_screen = ev.ms(2, 3);
+    S_.ms_refine = ev.ms(3, 4);
+    S_.ms_sort = ev.ms(4, 5);
+    S_.ms_total = ev.ms(0, 5);
+}
+
+}  // namespace
+
+extern "C" {
+
+int tj_join(const void* R, int64_t nR, const void* S, int64_t nS, int32_t d, int32_t dtype, double eps2,
+            int32_t mode, int32_t screen, const tj_options* opt, tj_result** out, void* stream) {
+    TJ_API_BEGIN
+    if (!out) fail(TJ_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (mode < 0 || mode > 2) fail(TJ_ERR_INVALID, "unknown mode");
+    if (screen < 0 || screen > 3) fail(TJ_ERR_INVALID, "unknown screen");
+    if (dtype != TJ_DTYPE_F32 && dtype != TJ_DTYPE_I16) fail(TJ_ERR_INVALID, "unknown dtype");
+    if (opt && opt->flags != 0) fail(TJ_ERR_INVALID, "options.flags must be 0");
+    std::unique_ptr<tj_result> res(new tj_result());
+    run_join(R, nR, S, nS, d, dtype, eps2, mode, screen, opt, res.get(), (cudaStream_t)stream);
+    *out = res.release();
+    return TJ_OK;
+    TJ_API_END
+}
+
+int64_t tj_result_count(const tj_result* res) { return res ? res->count : -1; }
+
+int tj_result_stats(const tj_result* res, tj_stats* out) {
+    if (!res || !out) { g_last_error = "null argument"; return TJ_ERR_INVALID; }
+    *out = res->stats;
+    return TJ_OK;
+}
+
+int tj_result_pairs(const tj_result* res, int64_t* i_out, int64_t* j_out, void* stream) {
+    TJ_API_BEGIN
+    if (!res) fail(TJ_ERR_INVALID, "null result");
+    if (res->count == 0) return TJ_OK;
+    if (!i_out || !j_out) fail(TJ_ERR_INVALID, "null output");
+    if (!res->offsets.empty()) fail(TJ_ERR_INVALID, "batched result: use tj_batch_pairs");
+    decode_pairs(res->keys.p, res->count, res->n_cols, i_out, j_out, (cudaStream_t)stream);
+    return TJ_OK;
+    TJ_API_END
+}
+
+int tj_result_keys(const tj_result* res, uint64_t* keys_out, void* stream) {
+    TJ_API_BEGIN
+    if (!res) fail(TJ_ERR_INVALID, "null result");
+    if (res->count == 0) return TJ_OK;
+    if (!keys_out) fail(TJ_ERR_INVALID, "null output");
+    TJ_CUDA(cudaMemcpyAsync(keys_out, res->keys.p, (size_t)res->count * 8, cudaMemcpyDeviceToDevice,
+                            (cudaStream_t)stream));
+    return TJ_OK;
+    TJ_API_END
+}
+
+int tj_result_neighbor_table(const tj_result* res, uint32_t* counts_out, int64_t* flat_out, void* stream) {
+    TJ_API_BEGIN
+    if (!res || !counts_out) fail(TJ_ERR_INVALID, "null argument");
+    if (!res->offsets.empty()) fail(TJ_ERR_INVALID, "batched result: not supported");
+    cudaStream_t st = (cudaStream_t)stream;
+    TJ_CUDA(cudaMemsetAsync(counts_out, 0, (size_t)res->n_rows * 4, st));
+    if (res->count > 0)
+        neighbor_counts<<<(unsigned)((res->count + 255) / 256), 256, 0, st>>>(res->keys.p, res->count, res->n_cols,
+                                                                               counts_out, flat_out);
+    TJ_CUDA(cudaGetLastError());
+    return TJ_OK;
+    TJ_API_END
+}
+
+void tj_result_free(tj_result* res) {
+    try {
+        delete res;
+    } catch (...) {
+    }
+}
+
+int tj_index_build(const void* X, int64_t n, int32_t d, int32_t dtype, double eps2, tj_index** out, void* stream) {
+    TJ_API_BEGIN
+    if (!out || !X) fail(TJ_ERR_INVALID, "null argument");
+    if (n <= 0 || d <= 0) fail(TJ_ERR_INVALID, "invalid shape");
+    if (n >= (1ll << 32)) fail(TJ_ERR_INVALID, "more than 2^32 - 1 rows");
+    if (dtype != TJ_DTYPE_F32 && dtype != TJ_DTYPE_I16) fail(TJ_ERR_INVALID, "unknown dtype");
+    cudaStream_t st = (cudaStream_t)stream;
+    std::unique_ptr<tj_index> ix(new tj_index());
+    DBuf<Counters> ctr(1, st);
+    launch(zero_counters, 1, 32, 0, st, ctr.p, 0);
+    DBuf<FrameParams> fp(1, st);
+    const void* srcs[1] = {X};
+    const long long ns[1] = {n};
+    compute_frame(srcs, ns, 1, d, dtype, fp.p, st);
+    Side& s = ix->side;
+    s.src = X; s.dtype = dtype; s.n = n; s.d = d; s.screen = kScreenPlain;
+    prepare_side(s, fp.p, st, &ctr.p->status);
+    tile_stats(s, kTileR, ix->t128, st);
+    tile_stats(s, kTileS, ix->t256, st);
+    const JoinParams jp = make_params(eps2, d, 64, n, n, true);
+    build_candidates(ix->t128, ix->t256, jp.Tp, true, 64, ix->cand, st);
+    // cells: runs of equal Morton keys, prefix-sum offsets
+    DBuf<uint32_t> flag((size_t)n, st), pos((size_t)n, st), ncell(1, st);
+    DBuf<uint32_t> sws(scan_workspace_elems((size_t)n) + 4, st);
+    launch(cell_flags, (unsigned)((n + 255) / 256), 256, 0, st, s.keys.p, n, flag.p);
+    exclusive_scan_u32(flag.p, pos.p, (size_t)n, ncell.p, sws.p, st);
+    uint32_t hc[3] = {0, 0, 0};
+    TJ_CUDA(cudaMemcpyAsync(&hc[0], ncell.p, 4, cudaMemcpyDeviceToHost, st));
+    TJ_CUDA(cudaMemcpyAsync(&hc[1], ix->cand.dev_counts.p, 8, cudaMemcpyDeviceToHost, st));
+    Counters h;
+    TJ_CUDA(cudaMemcpyAsync(&h, ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+    TJ_CUDA(cudaStreamSynchronize(st));
+    check_status(h.status);
+    ix->n_cells = hc[0];
+    ix->n_tile_pairs = hc[1];
+    ix->cand.total = hc[1];
+    ix->cand.nchunks = hc[2];
+    ix->cell_start = DBuf<uint32_t>((size_t)ix->n_cells + 1, st);
+    launch(cell_starts, (unsigned)((n + 255) / 256), 256, 0, st, flag.p, pos.p, n, ix->cell_start.p, ncell.p);
+    TJ_CUDA(cudaGetLastError());
+    TJ_CUDA(cudaStreamSynchronize(st));
+    *out = ix.release();
+    return TJ_OK;
+    TJ_API_END
+}
+
+int tj_index_info(const tj_index* idx, int64_t* n_cells, int64_t* n_tiles, int64_t* n_candidate_tile_pairs) {
+    if (!idx) { g_last_error = "null index"; return TJ_ERR_INVALID; }
+    if (n_cells) *n_cells = idx->n_cells;
+    if (n_tiles) *n_tiles = idx->t128.ntiles;
+    if (n_candidate_tile_pairs) *n_candidate_tile_pairs = idx->n_tile_pairs;
+    return TJ_OK;
+}
+
+int tj_index_copy(const tj_index* idx, uint32_t* perm, uint64_t* keys, uint32_t* cell_start, uint32_t* tile_pairs,
+                  void* stream) {
+    TJ_API_BEGIN
+    if (!idx) fail(TJ_ERR_INVALID, "null index");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t n = (size_t)idx->side.n;
+    if (perm) TJ_CUDA(cudaMemcpyAsync(perm, idx->side.perm.p, n * 4, cudaMemcpyDeviceToDevice, st));
+    if (keys) TJ_CUDA(cudaMemcpyAsync(keys, idx->side.keys.p, n * 8, cudaMemcpyDeviceToDevice, st));
+    if (cell_start)
+        TJ_CUDA(cudaMemcpyAsync(cell_start, idx->cell_start.p, ((size_t)idx->n_cells + 1) * 4,
+                                cudaMemcpyDeviceToDevice, st));
+    if (tile_pairs && idx->n_tile_pairs > 0) {
+        launch(tile_pair_list, num_sms() * 4, 256, 0, st, idx->cand.chunks.p, idx->cand.dev_counts.p + 1,
+                                                       idx->cand.jlist.p, tile_pairs);
+        TJ_CUDA(cudaGetLastError());
+    }
+    return TJ_OK;
+    TJ_API_END
+}
+
+void tj_index_free(tj_index* idx) {
+    try {
+        delete idx;
+    } catch (...) {
+    }
+}
+
+int tj_join_batched(const tj_batch_join* joins, int32_t njoins, int32_t screen, const tj_options* opt,
+                    tj_result** out, void* stream) {
+    (void)joins; (void)njoins; (void)screen; (void)opt; (void)out; (void)stream;
+    g_last_error = "batched joins are not built in this version";
+    return TJ_ERR_UNSUPPORTED;
+}
+
+int tj_batch_offsets(const tj_result* res, int64_t* offsets_host) {
+    if (!res || !offsets_host) { g_last_error = "null argument"; return TJ_ERR_INVALID; }
+    if (res->offsets.empty()) { g_last_error = "not a batched result"; return TJ_ERR_INVALID; }
+    memcpy(offsets_host, res->offsets.data(), res->offsets.size() * sizeof(int64_t));
+    return TJ_OK;
+}
+
+int tj_batch_pairs(const tj_result* res, int64_t* i_out, int64_t* j_out, void* stream) {
+    (void)res; (void)i_out; (void)j_out; (void)stream;
+    g_last_error = "batched joins are not built in this version";
+    return TJ_ERR_UNSUPPORTED;
+}
+
+const char* tj_last_error_string(void) { return g_last_error.c_str(); }
+
+int tj_version(void) { return 1; }
+
+int64_t tj_kernel_launches(void) { return (int64_t)g_launches.load(); }
+
+int tj_device_sm_count(void) {
+    try {
+        return num_sms();
+    } catch (...) {
+        return -1;
+    }
+}
+
+}  // extern "C"

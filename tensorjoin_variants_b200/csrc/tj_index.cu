@@ -1,0 +1,569 @@
+// Index build: Morton-sorted grid over the highest-variance dimensions, per-row
+// certificate metadata and low-precision MMA operands, tile statistics, and the
+// candidate tile-pair list with its execution chunks.
+//
+// Reference semantics (restated, not ported):
+//  * grid index: GDS-Join's per-dimension cells over NUMINDEXEDDIM variance-ordered
+//    dimensions (adapters/gds_g2a/main.cu:419-424 ReorderByDimension, :867-883
+//    getLinearID_nDimensions, :891-948 generateNDGridDimensions).  Here the cell
+//    coordinates are interleaved into a Morton key and points are radix-sorted by it
+//    on the GPU instead of a CPU std::set (main.cu:690-857).
+//  * candidate list: the tile-pair schedule of the scripted joins
+//    (src/run_g2b_tensorjoin_public.py:211-215, np.triu_indices for self-joins) pruned
+//    with conservative block lower bounds, ball and axis-aligned box
+//    (tensorjoin_20260908_block_feasibility/src/geometry.py:73-150).
+//  * per-row metadata: norms, reconstruction residual bound and low-precision copy
+//    (two_gate_campaign_20260908/src/gpu_kernels.py:33-51 half_metadata,
+//    g16_gpu_preparation_20260905/src/gpu_preparation.py:13-49).
+#include <algorithm>
+#include <cmath>
+
+#include "tj_internal.h"
+
+namespace tj {
+
+namespace {
+
+constexpr int kStatBlocks = 512;
+
+TJ_DEV float load_x(const void* src, int dtype, size_t idx) {
+    return dtype == kF32 ? ((const float*)src)[idx] : (float)((const int16_t*)src)[idx];
+}
+
+// Per-block partial statistics for every dimension.  Threads are laid out as
+// (row group g, dimension k); groups are combined in shared memory in a fixed order.
+__global__ void __launch_bounds__(256) dim_stats_partial(const void* src, int dtype, long long n, int d, float* pmin,
+                                                         float* pmax, double* psum, double* psq, int blk_base) {
+    __shared__ float smn[256], smx[256];
+    __shared__ double ss[256], sq[256];
+    const int G = d >= 256 ? 1 : 256 / d;
+    const long long rows_per = (n + gridDim.x - 1) / gridDim.x;
+    const long long r0 = (long long)blockIdx.x * rows_per;
+    const long long r1 = min(n, r0 + rows_per);
+    for (int kb = 0; kb < d; kb += 256) {
+        const int t = threadIdx.x;
+        const int g = (d >= 256) ? 0 : t / d;
+        const int k = (d >= 256) ? kb + t : t % d;
+        float mn = INFINITY, mx = -INFINITY;
+        double s = 0.0, q = 0.0;
+        if (g < G && k < d) {
+            for (long long r = r0 + g; r < r1; r += G) {
+                const float v = load_x(src, dtype, (size_t)r * d + k);
+                mn = fminf(mn, v);
+                mx = fmaxf(mx, v);
+                s += v;
+                q += (double)v * v;
+            }
+        }
+        smn[t] = mn; smx[t] = mx; ss[t] = s; sq[t] = q;
+        __syncthreads();
+        if (d < 256 && t < d) {
+            for (int gg = 1; gg < G; ++gg) {
+                const int o = gg * d + t;
+                mn = fminf(mn, smn[o]); mx = fmaxf(mx, smx[o]); s += ss[o]; q += sq[o];
+            }
+        }
+        if ((d >= 256 && k < d) || (d < 256 && t < d)) {
+            const size_t o = (size_t)(blk_base + blockIdx.x) * d + k;
+            pmin[o] = mn;
+            pmax[o] = mx;
+            psum[o] = s;
+            psq[o] = q;
+        }
+        __syncthreads();
+        if (d < 256) break;
+    }
+}
+
+// Deterministic reduction of the partials, variance ranking and frame parameters.
+__global__ void frame_finish(const float* pmin, const float* pmax, const double* psum, const double* psq, int nparts,
+                             long long ntot, int d, FrameParams* fp, float* var_ws, float* lo_ws, float* hi_ws) {
+    for (int k = threadIdx.x; k < d; k += blockDim.x) {
+        float mn = INFINITY, mx = -INFINITY;
+        double s = 0.0, q = 0.0;
+        for (int b = 0; b < nparts; ++b) {
+            const size_t o = (size_t)b * d + k;
+            mn = fminf(mn, pmin[o]);
+            mx = fmaxf(mx, pmax[o]);
+            s += psum[o];
+            q += psq[o];
+        }
+        const double mean = ntot ? s / (double)ntot : 0.0;
+        var_ws[k] = ntot ? (float)fmax(0.0, q / (double)ntot - mean * mean) : 0.f;
+        lo_ws[k] = mn;
+        hi_ws[k] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int m = min(d, 8);
+        FrameParams f;
+        f.m = m;
+        f.bits = 32 / m;
+        for (int t = 0; t < m; ++t) {
+            int best = -1;
+            for (int k = 0; k < d; ++k) {
+                bool used = false;
+                for (int u = 0; u < t; ++u) used |= (f.dims[u] == k);
+                if (used) continue;
+                if (best < 0 || var_ws[k] > var_ws[best]) best = k;
+            }
+            f.dims[t] = best;
+            const float lo = lo_ws[best], hi = hi_ws[best];
+            const float range = (isfinite(lo) && isfinite(hi) && hi > lo) ? hi - lo : 1.f;
+            f.lo[t] = isfinite(lo) ? lo : 0.f;
+            f.inv_w[t] = (float)(1u << f.bits) / range;
+        }
+        *fp = f;
+    }
+}
+
+__global__ void morton_keys(const void* src, int dtype, long long n, int d, const FrameParams* fpp, uint64_t* keys,
+                            uint32_t* vals) {
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const FrameParams fp = *fpp;
+    const unsigned maxc = (1u << fp.bits) - 1u;
+    unsigned c[16];
+    for (int t = 0; t < fp.m; ++t) {
+        const float v = load_x(src, dtype, (size_t)r * d + fp.dims[t]);
+        float q = (v - fp.lo[t]) * fp.inv_w[t];
+        q = fminf(fmaxf(q, 0.f), (float)maxc);
+        c[t] = isfinite(q) ? (unsigned)q : 0u;
+    }
+    uint64_t key = 0;
+    for (int b = fp.bits - 1; b >= 0; --b)
+        for (int t = 0; t < fp.m; ++t) key = (key << 1) | ((c[t] >> b) & 1u);
+    keys[r] = key;
+    vals[r] = (uint32_t)r;
+}
+
+// One warp per sorted row: operand conversion and certificate metadata.
+template <int kScreen>
+__global__ void prep_rows(const void* src, int dtype, long long n, int d, int kpad, long long rows_pad,
+                          const uint32_t* perm, uint16_t* op, int8_t* op8, float* xs, double* nrm2, float* nrm2f,
+                          float* zn, float* en, float* yn, long long* inorm, unsigned long long* status) {
+    const long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (r >= rows_pad) return;
+    const bool real = r < n;
+    const size_t orig = real ? (size_t)perm[r] : 0;
+    double sx = 0.0, sz = 0.0, se = 0.0;
+    long long sq = 0;
+    bool bad = false, fp16_range = false;
+    for (int k = lane; k < kpad; k += 32) {
+        float x = 0.f;
+        if (real && k < d) x = load_x(src, dtype, orig * d + k);
+        if (!isfinite(x)) { bad = true; x = 0.f; }
+        if (kScreen == kScreenPlain) {
+            if (k < d) xs[(size_t)r * d + k] = x;
+            sx += (double)x * x;
+        } else if (kScreen == kScreenBF16 || kScreen == kScreenFP16) {
+            float z;
+            uint16_t bits;
+            if (kScreen == kScreenBF16) {
+                const __nv_bfloat16 h = __float2bfloat16_rn(x);
+                z = __bfloat162float(h);
+                bits = __bfloat16_as_ushort(h);
+            } else {
+                if (fabsf(x) > 65504.f) fp16_range = true;
+                const __half h = __float2half_rn(x);
+                z = __half2float(h);
+                bits = __half_as_ushort(h);
+            }
+            op[(size_t)r * kpad + k] = bits;
+            const double xd = x, zd = z, ed = xd - zd;   // exact in FP64
+            sx += xd * xd;
+            sz += zd * zd;
+            se += ed * ed;
+        } else {   // int8 limbs of an int14 value: q = 128 h + l, h = floor((q + 64) / 128)
+            const int q = (int)x;
+            if (q < -8192 || q > 8191) bad = true;
+            const int h = (q + 64 + 8192) / 128 - 64;   // floor division for q + 64 >= -8128
+            const int l = q - 128 * h;
+            op8[(size_t)r * (2 * kpad) + k] = (int8_t)h;
+            op8[(size_t)r * (2 * kpad) + kpad + k] = (int8_t)l;
+            sq += (long long)q * q;
+            sx += (double)x * x;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sz += __shfl_xor_sync(0xffffffffu, sz, o);
+        se += __shfl_xor_sync(0xffffffffu, se, o);
+        sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    fp16_range = __any_sync(0xffffffffu, fp16_range);
+    if (lane == 0) {
+        if (bad && real) atomicOr(status, (unsigned long long)kStatusBadInput);
+        if (fp16_range && real) atomicOr(status, (unsigned long long)kStatusFp16Range);
+        if (real && sx > 0x1p100) atomicOr(status, (unsigned long long)kStatusBadInput);
+        // FP64 sums of d non-negative exactly-representable squares: relative error <= (d+2) 2^-53
+        const double g = (double)(d + 2) * 0x1p-53;
+        const double up = (1.0 + 2.0 * g) * (1.0 + 0x1p-50);
+        nrm2[r] = sx;
+        nrm2f[r] = __double2float_rn(sx);
+        yn[r] = f32_up(sqrt(sx * up) * (1.0 + 0x1p-50));
+        zn[r] = f32_up(sqrt(sz * up) * (1.0 + 0x1p-50));
+        en[r] = f32_up(sqrt(se * up) * (1.0 + 0x1p-50));
+        if (inorm) inorm[r] = sq;
+    }
+}
+
+// Tile statistics: one block per tile.
+__global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dtype, long long n, int d, int tile,
+                                                         int ntiles, const uint32_t* perm, const double* nrm2,
+                                                         const float* nrm2f, const float* zn, const float* en,
+                                                         const float* yn, float* ctrT, float* loT, float* hiT,
+                                                         float* rad, float* maxZ, float* maxE, float* maxY,
+                                                         float* maxB, float* beta, uint32_t* nvalid,
+                                                         uint32_t* row0) {
+    extern __shared__ float s_ctr[];   // [d]
+    __shared__ float red[5][256];
+    const int t = blockIdx.x;
+    const long long r0 = (long long)t * tile;
+    const int nv = (int)min((long long)tile, n - r0);
+    const double g = (double)(d + 2) * 0x1p-53;
+    // per-dimension centroid and bounding box
+    for (int k = threadIdx.x; k < d; k += blockDim.x) {
+        double s = 0.0;
+        float mn = INFINITY, mx = -INFINITY;
+        for (int i = 0; i < nv; ++i) {
+            const float v = load_x(src, dtype, (size_t)perm[r0 + i] * d + k);
+            s += v;
+            mn = fminf(mn, v);
+            mx = fmaxf(mx, v);
+        }
+        const float c = (float)(s / (double)max(nv, 1));
+        s_ctr[k] = c;
+        ctrT[(size_t)k * ntiles + t] = c;
+        loT[(size_t)k * ntiles + t] = mn;
+        hiT[(size_t)k * ntiles + t] = mx;
+    }
+    __syncthreads();
+    // radius: warp per row, exact FP64 differences against the FP32 centroid
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double rmax = 0.0;
+    for (int i = warp; i < nv; i += 8) {
+        const size_t base = (size_t)perm[r0 + i] * d;
+        double s = 0.0;
+        for (int k = lane; k < d; k += 32) {
+            const double df = (double)load_x(src, dtype, base + k) - (double)s_ctr[k];
+            s += df * df;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        rmax = fmax(rmax, s);
+    }
+    // row-bound maxima
+    float mz = 0.f, me = 0.f, my = 0.f, mb = 0.f, mbeta = 0.f;
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) {
+        const long long r = r0 + i;
+        mz = fmaxf(mz, zn[r]);
+        me = fmaxf(me, en[r]);
+        my = fmaxf(my, yn[r]);
+        mb = fmaxf(mb, nrm2f[r]);
+        const double bt = fabs((double)nrm2f[r] - nrm2[r]) + 2.0 * g * nrm2[r];
+        mbeta = fmaxf(mbeta, f32_up(bt * (1.0 + 0x1p-40)));
+    }
+    red[0][threadIdx.x] = mz;
+    red[1][threadIdx.x] = me;
+    red[2][threadIdx.x] = my;
+    red[3][threadIdx.x] = mb;
+    red[4][threadIdx.x] = mbeta;
+    __shared__ double rr[8];
+    if (lane == 0) rr[warp] = rmax;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int q = 0; q < 5; ++q) red[q][threadIdx.x] = fmaxf(red[q][threadIdx.x], red[q][threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < 8; ++w) m = fmax(m, rr[w]);
+        // FP64 sum of d squares of exact differences: relative error <= g; sqrt correctly rounded
+        rad[t] = f32_up(sqrt(m * (1.0 + 2.0 * g)) * (1.0 + 0x1p-50));
+        maxZ[t] = red[0][0];
+        maxE[t] = red[1][0];
+        maxY[t] = red[2][0];
+        maxB[t] = red[3][0];
+        beta[t] = red[4][0];
+        nvalid[t] = (uint32_t)max(nv, 0);
+        row0[t] = (uint32_t)r0;
+    }
+}
+
+// Candidate test: thread = one S tile J, 16 R tiles per block (from shared memory).
+// Keeps (I, J) unless a rigorous lower bound on every pair distance exceeds sqrt(Tp).
+template <int kCandI>
+__global__ void __launch_bounds__(256) cand_test(const float* rctrT, const float* rloT, const float* rhiT,
+                                                 const float* rrad, int ntR, const float* sctrT,
+                                                 const float* sloT, const float* shiT, const float* srad, int ntS,
+                                                 int d, int tileR, int tileS, double Tp, int self_join,
+                                                 uint32_t* bitmap, int words) {
+    extern __shared__ float sm[];   // [3][kCandI][d]
+    float* sc = sm;
+    float* slo = sm + kCandI * d;
+    float* shi = sm + 2 * kCandI * d;
+    const int I0 = blockIdx.y * kCandI;
+    const int nI = min(kCandI, ntR - I0);
+    for (int e = threadIdx.x; e < kCandI * d; e += blockDim.x) {
+        const int ii = e / d, k = e % d;
+        const bool ok = ii < nI;
+        sc[e] = ok ? rctrT[(size_t)k * ntR + I0 + ii] : 0.f;
+        slo[e] = ok ? rloT[(size_t)k * ntR + I0 + ii] : 0.f;
+        shi[e] = ok ? rhiT[(size_t)k * ntR + I0 + ii] : 0.f;
+    }
+    __syncthreads();
+    const int J = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool jok = J < ntS;
+    float ball[kCandI], box[kCandI];
+#pragma unroll
+    for (int ii = 0; ii < kCandI; ++ii) ball[ii] = box[ii] = 0.f;
+    if (jok) {
+        for (int k = 0; k < d; ++k) {
+            const float cj = sctrT[(size_t)k * ntS + J];
+            const float lj = sloT[(size_t)k * ntS + J];
+            const float hj = shiT[(size_t)k * ntS + J];
+#pragma unroll
+            for (int ii = 0; ii < kCandI; ++ii) {
+                const float dc = sc[ii * d + k] - cj;
+                ball[ii] = fmaf(dc, dc, ball[ii]);
+                const float gap = fmaxf(fmaxf(lj - shi[ii * d + k], slo[ii * d + k] - hj), 0.f);
+                box[ii] = fmaf(gap, gap, box[ii]);
+            }
+        }
+    }
+    // FP32 sums of d non-negative terms: computed >= (1 - (d+4) 2^-23) * true  => true >= computed * f
+    const float f = 1.f - (float)(d + 8) * 0x1p-23f;
+    const float rtp = (float)(sqrt(Tp) * (1.0 + 0x1p-20));
+    const float tpf = (float)(Tp * (1.0 + 0x1p-20));
+    const float rj = jok ? srad[J] : 0.f;
+    const unsigned lane = threadIdx.x & 31;
+    for (int ii = 0; ii < kCandI; ++ii) {
+        const int I = I0 + ii;
+        bool keep = jok && ii < nI;
+        if (keep && self_join) {
+            // some column index of J must exceed some row index of I (sorted positions)
+            const long long maxcol = (long long)(J + 1) * tileS - 1;
+            keep = maxcol > (long long)I * tileR;
+        }
+        if (keep) {
+            const float lb_box = box[ii] * f;
+            const float lb_ball = sqrtf(ball[ii] * f) * (1.f - 0x1p-20f) - rrad[I] - rj;
+            if (lb_box > tpf || lb_ball > rtp) keep = false;
+        }
+        const unsigned bits = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0 && ii < nI && (J >> 5) < words) bitmap[(size_t)I * words + (J >> 5)] = bits;
+    }
+}
+
+__global__ void cand_count(const uint32_t* bitmap, int words, int ntR, uint32_t* cnt) {
+    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (I >= ntR) return;
+    unsigned c = 0;
+    for (int w = lane; w < words; w += 32) c += __popc(bitmap[(size_t)I * words + w]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) cnt[I] = c;
+}
+
+__global__ void cand_fill(const uint32_t* bitmap, int words, int ntR, const uint32_t* off, uint32_t* jlist) {
+    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (I >= ntR) return;
+    uint32_t pos = off[I];
+    for (int w0 = 0; w0 < words; w0 += 32) {
+        const int w = w0 + lane;
+        const unsigned bits = w < words ? bitmap[(size_t)I * words + w] : 0u;
+        unsigned tot;
+        const unsigned pre = warp_excl_scan(__popc(bits), tot);
+        unsigned b = bits, p = pos + pre;
+        while (b) {
+            const int bit = __ffs(b) - 1;
+            b &= b - 1;
+            jlist[p++] = (uint32_t)(w * 32 + bit);
+        }
+        pos += tot;
+    }
+}
+
+__global__ void chunk_counts(const uint32_t* cnt, int ntR, int ch, uint32_t* nch) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I < ntR) nch[I] = (cnt[I] + ch - 1) / ch;
+}
+
+// Emit one (w, I) sort key per chunk; unused capacity gets the max key.
+__global__ void chunk_keys(const uint32_t* nch, const uint32_t* cbase, int ntR, size_t cap, uint64_t* keys,
+                           uint32_t* vals) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= ntR) return;
+    const uint32_t b = cbase[I], c = nch[I];
+    for (uint32_t w = 0; w < c; ++w) {
+        if (b + w < cap) {
+            keys[b + w] = ((uint64_t)w << 32) | (uint32_t)I;
+            vals[b + w] = b + w;
+        }
+    }
+}
+
+__global__ void fill_keys_max(uint64_t* keys, uint32_t* vals, size_t from, size_t cap, const uint32_t* total) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x + from;
+    if (i < cap && i >= *total) {
+        keys[i] = ~0ull;
+        vals[i] = 0xFFFFFFFFu;
+    }
+}
+
+__global__ void chunk_emit(const uint64_t* keys, size_t cap, const uint32_t* total, const uint32_t* cnt,
+                           const uint32_t* off, int ch, uint4* chunks) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cap) return;
+    if (i >= *total) return;
+    const uint64_t k = keys[i];
+    const uint32_t I = (uint32_t)(k & 0xFFFFFFFFu), w = (uint32_t)(k >> 32);
+    const uint32_t b = off[I] + w * (uint32_t)ch;
+    const uint32_t e = min(b + (uint32_t)ch, off[I] + cnt[I]);
+    chunks[i] = make_uint4(I, b, e, 0);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host entry points
+
+void compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d, int dtype, FrameParams* fp,
+                   cudaStream_t st) {
+    long long ntot = 0;
+    for (int s = 0; s < nsrc; ++s) ntot += ns[s];
+    const int parts = nsrc * kStatBlocks;
+    DBuf<float> pmin((size_t)parts * d, st), pmax((size_t)parts * d, st);
+    DBuf<double> psum((size_t)parts * d, st), psq((size_t)parts * d, st);
+    DBuf<float> ws((size_t)3 * d, st);
+    for (int s = 0; s < nsrc; ++s) {
+        const int nb = kStatBlocks;
+        launch(dim_stats_partial, nb, 256, 0, st, srcs[s], dtype, ns[s], d, pmin.p, pmax.p, psum.p, psq.p,
+                                              s * kStatBlocks);
+    }
+    launch(frame_finish, 1, 256, 0, st, pmin.p, pmax.p, psum.p, psq.p, parts, ntot, d, fp, ws.p, ws.p + d,
+                                    ws.p + 2 * d);
+    TJ_CUDA(cudaGetLastError());
+}
+
+void prepare_side(Side& s, const FrameParams* fpd, cudaStream_t st, unsigned long long* status) {
+    const long long n = s.n;
+    s.kpad = (s.screen == kScreenInt8Limb) ? ((s.d + 127) / 128) * 128 : ((s.d + kBK - 1) / kBK) * kBK;
+    s.rows_pad = ((std::max<long long>(n, 1) + kTileS - 1) / kTileS) * kTileS;
+    s.perm = DBuf<uint32_t>((size_t)std::max<long long>(n, 1), st);
+    s.keys = DBuf<uint64_t>((size_t)std::max<long long>(n, 1), st);
+    if (n > 0) {
+        DBuf<uint64_t> ktmp((size_t)n, st);
+        DBuf<uint32_t> vtmp((size_t)n, st);
+        DBuf<uint32_t> ws(radix_workspace_elems((size_t)n), st);
+        launch(morton_keys, (unsigned)((n + 255) / 256), 256, 0, st, s.src, s.dtype, n, s.d, fpd, s.keys.p, s.perm.p);
+        TJ_CUDA(cudaGetLastError());
+        radix_sort(s.keys.p, s.perm.p, ktmp.p, vtmp.p, (size_t)n, 32, ws.p, st);
+    }
+    const size_t rp = (size_t)s.rows_pad;
+    if (s.screen == kScreenBF16 || s.screen == kScreenFP16) s.op = DBuf<uint16_t>(rp * s.kpad, st);
+    if (s.screen == kScreenInt8Limb) {
+        s.op8 = DBuf<int8_t>(rp * 2 * s.kpad, st);
+        s.inorm = DBuf<long long>(rp, st);
+    }
+    if (s.screen == kScreenPlain) s.xs = DBuf<float>(rp * s.d, st);
+    s.nrm2 = DBuf<double>(rp, st);
+    s.nrm2f = DBuf<float>(rp, st);
+    s.zn = DBuf<float>(rp, st);
+    s.en = DBuf<float>(rp, st);
+    s.yn = DBuf<float>(rp, st);
+    const unsigned blocks = (unsigned)((rp * 32 + 255) / 256);
+#define TJ_PREP(SCR)                                                                                             \
+    launch(prep_rows<SCR>, blocks, 256, 0, st, s.src, s.dtype, n, s.d, s.kpad, s.rows_pad, s.perm.p, s.op.p, s.op8.p, \
+                                           s.xs.p, s.nrm2.p, s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.inorm.p, status)
+    switch (s.screen) {
+        case kScreenPlain: TJ_PREP(kScreenPlain); break;
+        case kScreenBF16: TJ_PREP(kScreenBF16); break;
+        case kScreenFP16: TJ_PREP(kScreenFP16); break;
+        default: TJ_PREP(kScreenInt8Limb); break;
+    }
+#undef TJ_PREP
+    TJ_CUDA(cudaGetLastError());
+}
+
+void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st) {
+    ts.tile = tile;
+    ts.d = s.d;
+    ts.ntiles = (int)((s.n + tile - 1) / tile);
+    const size_t nt = (size_t)std::max(ts.ntiles, 1);
+    ts.ctrT = DBuf<float>(nt * s.d, st);
+    ts.loT = DBuf<float>(nt * s.d, st);
+    ts.hiT = DBuf<float>(nt * s.d, st);
+    ts.rad = DBuf<float>(nt, st);
+    ts.maxZ = DBuf<float>(nt, st);
+    ts.maxE = DBuf<float>(nt, st);
+    ts.maxY = DBuf<float>(nt, st);
+    ts.maxB = DBuf<float>(nt, st);
+    ts.beta = DBuf<float>(nt, st);
+    ts.nvalid = DBuf<uint32_t>(nt, st);
+    ts.row0 = DBuf<uint32_t>(nt, st);
+    if (ts.ntiles == 0) return;
+    const size_t smem = (size_t)s.d * sizeof(float);
+    if (smem > 48 * 1024)
+        TJ_CUDA(cudaFuncSetAttribute(tile_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    launch(tile_stats_kernel, ts.ntiles, 256, smem, st, s.src, s.dtype, s.n, s.d, tile, ts.ntiles, s.perm.p, s.nrm2.p,
+                                                    s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, ts.ctrT.p, ts.loT.p,
+                                                    ts.hiT.p, ts.rad.p, ts.maxZ.p, ts.maxE.p, ts.maxY.p, ts.maxB.p,
+                                                    ts.beta.p, ts.nvalid.p, ts.row0.p);
+    TJ_CUDA(cudaGetLastError());
+}
+
+void build_candidates(const TileSet& tr, const TileSet& ts, double Tp, bool self_join, int chunk_items,
+                      Candidates& c, cudaStream_t st) {
+    const int ntR = tr.ntiles, ntS = ts.ntiles, d = tr.d;
+    const int words = (ntS + 31) / 32;
+    c.cnt = DBuf<uint32_t>((size_t)std::max(ntR, 1), st);
+    c.off = DBuf<uint32_t>((size_t)std::max(ntR, 1), st);
+    c.dev_counts = DBuf<uint32_t>(2, st);
+    TJ_CUDA(cudaMemsetAsync(c.dev_counts.p, 0, 2 * sizeof(uint32_t), st));
+    const size_t maxc = (size_t)ntR * (size_t)ntS;
+    c.jlist = DBuf<uint32_t>(std::max<size_t>(maxc, 1), st);
+    c.chunks_cap = maxc / (size_t)chunk_items + (size_t)ntR + 1;
+    c.chunks = DBuf<uint4>(c.chunks_cap, st);
+    if (ntR == 0 || ntS == 0) return;
+    DBuf<uint32_t> bitmap((size_t)ntR * words, st);
+    TJ_CUDA(cudaMemsetAsync(bitmap.p, 0, bitmap.bytes(), st));
+    const int ci = (size_t)3 * 16 * d * sizeof(float) <= 200 * 1024 ? 16 : (size_t)3 * 4 * d * sizeof(float) <= 200 * 1024 ? 4 : 1;
+    const size_t smem = (size_t)3 * ci * d * sizeof(float);
+    if (smem > 200 * 1024) fail(-7, "dimension too large for the candidate test");
+    dim3 grid((unsigned)((ntS + 255) / 256), (unsigned)((ntR + ci - 1) / ci));
+#define TJ_CAND(CI)                                                                                                 \
+    TJ_CUDA(cudaFuncSetAttribute(cand_test<CI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));          \
+    launch(cand_test<CI>, grid, 256, smem, st, tr.ctrT.p, tr.loT.p, tr.hiT.p, tr.rad.p, ntR, ts.ctrT.p, ts.loT.p,      \
+                                           ts.hiT.p, ts.rad.p, ntS, d, tr.tile, ts.tile, Tp, self_join ? 1 : 0,      \
+                                           bitmap.p, words)
+    if (ci == 16) { TJ_CAND(16); } else if (ci == 4) { TJ_CAND(4); } else { TJ_CAND(1); }
+#undef TJ_CAND
+    TJ_CUDA(cudaGetLastError());
+    launch(cand_count, (unsigned)((ntR * 32 + 255) / 256), 256, 0, st, bitmap.p, words, ntR, c.cnt.p);
+    DBuf<uint32_t> sws(scan_workspace_elems((size_t)ntR) + 4, st);
+    exclusive_scan_u32(c.cnt.p, c.off.p, (size_t)ntR, c.dev_counts.p, sws.p, st);
+    launch(cand_fill, (unsigned)((ntR * 32 + 255) / 256), 256, 0, st, bitmap.p, words, ntR, c.off.p, c.jlist.p);
+    // chunks: (w, I) order so that concurrently running CTAs share the same S window
+    DBuf<uint32_t> nch((size_t)ntR, st), cbase((size_t)ntR, st);
+    launch(chunk_counts, (unsigned)((ntR + 255) / 256), 256, 0, st, c.cnt.p, ntR, chunk_items, nch.p);
+    exclusive_scan_u32(nch.p, cbase.p, (size_t)ntR, c.dev_counts.p + 1, sws.p, st);
+    const size_t cap = c.chunks_cap;
+    DBuf<uint64_t> keys(cap, st), ktmp(cap, st);
+    DBuf<uint32_t> vals(cap, st), vtmp(cap, st);
+    launch(fill_keys_max, (unsigned)((cap + 255) / 256), 256, 0, st, keys.p, vals.p, 0, cap, c.dev_counts.p + 1);
+    launch(chunk_keys, (unsigned)((ntR + 255) / 256), 256, 0, st, nch.p, cbase.p, ntR, cap, keys.p, vals.p);
+    DBuf<uint32_t> rws(radix_workspace_elems(cap), st);
+    radix_sort(keys.p, vals.p, ktmp.p, vtmp.p, cap, 48, rws.p, st);
+    launch(chunk_emit, (unsigned)((cap + 255) / 256), 256, 0, st, keys.p, cap, c.dev_counts.p + 1, c.cnt.p, c.off.p,
+                                                               chunk_items, c.chunks.p);
+    TJ_CUDA(cudaGetLastError());
+}
+
+}  // namespace tj

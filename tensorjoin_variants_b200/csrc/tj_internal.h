@@ -1,0 +1,163 @@
+// Internal host-side interface between the pipeline stages of libtensorjoin.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "tj_common.cuh"
+
+namespace tj {
+
+// ------------------------------------------------------------------ errors
+struct Error {
+    int code;
+    std::string msg;
+};
+[[noreturn]] void fail(int code, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what);
+#define TJ_CUDA(x) ::tj::check_cuda((x), #x)
+
+// ------------------------------------------------------------------ stream-ordered device memory
+void* dalloc(size_t bytes, cudaStream_t st);
+void dfree(void* p, cudaStream_t st);
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t st = nullptr;
+    DBuf() = default;
+    DBuf(size_t n_, cudaStream_t s) : n(n_), st(s) { p = n ? (T*)dalloc(n * sizeof(T), s) : nullptr; }
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), st(o.st) { o.p = nullptr; o.n = 0; }
+    DBuf& operator=(DBuf&& o) noexcept {
+        if (this != &o) { reset(); p = o.p; n = o.n; st = o.st; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DBuf() { reset(); }
+    void reset() { if (p) dfree(p, st); p = nullptr; n = 0; }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ------------------------------------------------------------------ scan / sort (tj_sort.cu)
+size_t scan_workspace_elems(size_t n);
+void exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* total, uint32_t* ws,
+                        cudaStream_t st);
+size_t radix_workspace_elems(size_t n);
+void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp, size_t n, int bits,
+                uint32_t* ws, cudaStream_t st);
+int radix_passes(int bits);
+
+// ------------------------------------------------------------------ enums (mirror include/tensorjoin.h)
+enum DType { kF32 = 0, kI16 = 1 };
+enum Mode { kModeRS = 0, kModeUpper = 1, kModeDirected = 2 };
+enum Screen { kScreenPlain = 0, kScreenBF16 = 1, kScreenFP16 = 2, kScreenInt8Limb = 3 };
+
+// ------------------------------------------------------------------ prepared side (tj_index.cu)
+// A side of the join in Morton order: permutation, MMA operand and per-row certificate metadata.
+// Row r of every array is the point perm[r] of the caller's input.
+struct Side {
+    const void* src = nullptr;   // caller's input rows, original order (not owned)
+    int dtype = kF32;
+    long long n = 0;             // rows
+    int d = 0;
+    int screen = kScreenBF16;
+    int kpad = 0;                // operand row length in elements (multiple of 64)
+    long long rows_pad = 0;      // operand rows (multiple of 256)
+    DBuf<uint32_t> perm;         // [n] sorted position -> original row
+    DBuf<uint64_t> keys;         // [n] Morton keys (sorted)
+    DBuf<uint16_t> op;           // [rows_pad, kpad] bf16 / fp16 operand (screen != plain)
+    DBuf<int8_t> op8;            // [rows_pad, 2*kpad] int8 limbs [hi | lo] (int8 limb screen)
+    DBuf<float> xs;              // [rows_pad, d] FP32 rows in sorted order (plain screen)
+    DBuf<double> nrm2;           // [rows_pad] sequential FP64 sum of squares of x
+    DBuf<float> nrm2f;           // [rows_pad] FP32 nearest of nrm2
+    DBuf<float> zn;              // [rows_pad] upper bound of ||z|| (z = operand row)
+    DBuf<float> en;              // [rows_pad] upper bound of ||x - z||
+    DBuf<float> yn;              // [rows_pad] upper bound of ||x||
+    DBuf<long long> inorm;       // [rows_pad] exact integer squared norms (int path)
+};
+
+// Tile statistics at one tile granularity (128 rows for R, 256 rows for S).
+struct TileSet {
+    int tile = 0;
+    int ntiles = 0;
+    int d = 0;
+    DBuf<float> ctrT;      // [d][ntiles] centroid (transposed for coalesced candidate tests)
+    DBuf<float> loT, hiT;  // [d][ntiles] exact per-dimension min / max
+    DBuf<float> rad;       // [ntiles] upper bound of max ||x - centroid||
+    DBuf<float> maxZ, maxE, maxY, maxB, beta;  // [ntiles] maxima of the row bounds
+    DBuf<uint32_t> nvalid;  // [ntiles] rows of the tile that are real points
+    DBuf<uint32_t> row0;    // [ntiles] first sorted row of the tile
+};
+
+// Candidate tile pairs grouped by R tile, cut into chunks scheduled J-window-major.
+struct Candidates {
+    DBuf<uint32_t> cnt;       // [ntR] candidates per R tile
+    DBuf<uint32_t> off;       // [ntR] exclusive prefix of cnt
+    DBuf<uint32_t> jlist;     // [total] S tile ids, ascending within each R tile
+    DBuf<uint4> chunks;       // [nchunks] (I, begin, end, 0) in execution order
+    DBuf<uint32_t> dev_counts;  // [2]: total candidates, total chunks (device)
+    uint32_t total = 0;       // host copies (filled after a sync)
+    uint32_t nchunks = 0;
+    size_t chunks_cap = 0;
+};
+
+struct FrameParams {
+    int m = 0;               // indexed dimensions
+    int bits = 0;            // bits per indexed dimension
+    int dims[16] = {0};
+    float lo[16] = {0};
+    float inv_w[16] = {0};
+};
+
+// side preparation
+void compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d, int dtype, FrameParams* fp,
+                   cudaStream_t st);
+void prepare_side(Side& s, const FrameParams* fp_dev, cudaStream_t st, unsigned long long* status);
+void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st);
+void build_candidates(const TileSet& tr, const TileSet& ts, double T, bool self_join, int chunk_items,
+                      Candidates& c, cudaStream_t st);
+
+// ------------------------------------------------------------------ screen / refine / emit
+struct EmitBuffers {
+    uint64_t* acc = nullptr;   // accept keys
+    unsigned long long acc_cap = 0;
+    uint64_t* band = nullptr;  // band keys (canonical key of the pair)
+    unsigned long long band_cap = 0;
+    Counters* ctr = nullptr;
+};
+
+struct JoinGeometry {
+    const Side* R;
+    const Side* S;
+    const TileSet* tR;
+    const TileSet* tS;
+    const Candidates* cand;
+    JoinParams jp;
+};
+
+void screen_tc(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st);
+void screen_plain(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st);
+void refine_band(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st);
+void expand_directed(const uint64_t* upper, unsigned long long n_upper_slots, uint64_t* out, long long N,
+                     cudaStream_t st);
+void decode_pairs(const uint64_t* keys, long long n, long long n_cols, int64_t* i_out, int64_t* j_out,
+                  cudaStream_t st);
+
+int num_sms();
+
+// Every kernel of the library is launched through launch(): it checks the launch and counts it
+// (tj_kernel_launches() reports the running total, used to audit what ran inside a timed region).
+void count_launch();
+template <class... KArgs, class... Args>
+void launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+    k<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
+    count_launch();
+    check_cuda(cudaGetLastError(), "kernel launch");
+}
+
+}  // namespace tj

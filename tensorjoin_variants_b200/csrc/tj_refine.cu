@@ -1,0 +1,356 @@
+// FP64 band refinement, the plain FP32 direct-difference join, and the
+// canonical-output helpers (directed expansion, pair decoding).
+//
+// Refinement reproduces the oracle's predicate exactly: for every band pair,
+//   acc = 0; for k = 0..d-1: t = dbl(x_k) - dbl(y_k); acc = acc + t*t   (one rounding each, no FMA)
+//   accept iff acc <= T
+// which is the reference's FP64 terminal (src/run_g2a_tensorjoin.py:194-232,
+// src/run_d1_triton.py:206-248) with its summation order fixed to sequential k
+// (the reference summed 256-wide blocks in tree order), so the emitted pair set is
+// bit-identical to the CPU oracle.
+//
+// The plain join is the "plain GPU method" baseline: FP32 direct difference over
+// the same candidate tile pairs (no tensor cores), a rigorous FP32 error band, and
+// the same FP64 refinement of band pairs.  It plays the role of the reference's
+// GDS-Join FP64 grid join / FP32-first control (adapters/gds_g2a/kernel.cu:314-386,
+// g15_strong_control_20260905/src/fp32_first.py:104-157).
+#include "tj_internal.h"
+
+namespace tj {
+
+namespace {
+
+constexpr unsigned kEmitChunkP = 256;
+
+struct Appender {
+    unsigned long long base = 0;
+    unsigned used = 0, size = 0;
+    unsigned long long valid = 0;
+    TJ_DEV unsigned long long reserve(unsigned t, unsigned long long* reserved, uint64_t* buf, unsigned long long cap) {
+        if (used + t > size) {
+            pad(buf, cap);
+            const unsigned want = t > kEmitChunkP ? t : kEmitChunkP;
+            unsigned long long b = 0;
+            if (lane_id() == 0) b = atomicAdd(reserved, (unsigned long long)want);
+            base = __shfl_sync(0xffffffffu, b, 0);
+            used = 0;
+            size = want;
+        }
+        const unsigned long long r = base + used;
+        used += t;
+        valid += t;
+        return r;
+    }
+    TJ_DEV void pad(uint64_t* buf, unsigned long long cap) {
+        for (unsigned k = used + lane_id(); k < size; k += 32)
+            if (base + k < cap) buf[base + k] = kSentinel;
+        used = size;
+    }
+};
+
+TJ_DEV uint64_t key_of(const JoinParams& jp, uint32_t oi, uint32_t oj) {
+    if (jp.self_join) {
+        const uint32_t lo = oi < oj ? oi : oj, hi = oi < oj ? oj : oi;
+        return jp.key_off + (uint64_t)lo * (uint64_t)jp.n_cols + hi;
+    }
+    return jp.key_off + (uint64_t)oi * (uint64_t)jp.n_cols + oj;
+}
+
+// ------------------------------------------------------------------ plain FP32 join
+constexpr int kPT = 256;                // threads: 16 x 16
+constexpr int kPR = 8, kPC = 16;        // micro-tile: 8 rows x 16 cols per thread
+constexpr int kPK = 16;                 // k chunk
+
+struct PlainArgs {
+    const uint4* chunks;
+    const uint32_t* nchunks;
+    const uint32_t* jlist;
+    const float* rx;     // [rows_pad, d] sorted FP32 rows (R)
+    const float* sx;     // [rows_pad, d] sorted FP32 rows (S)
+    const uint32_t* r_row0;
+    const uint32_t* r_nvalid;
+    const uint32_t* r_perm;
+    const uint32_t* s_row0;
+    const uint32_t* s_nvalid;
+    const uint32_t* s_perm;
+    int d;
+    float tin, tout;     // certified-in / certified-out thresholds on the FP32 sum
+    JoinParams jp;
+    uint64_t* acc;
+    unsigned long long acc_cap;
+    uint64_t* band;
+    unsigned long long band_cap;
+    Counters* ctr;
+};
+
+__global__ void __launch_bounds__(kPT, 1) plain_kernel(const PlainArgs a) {
+    __shared__ float sR[kPK][kTileR + 1];   // +1: conflict-free transposed stores
+    __shared__ float sS[kPK][kTileS + 1];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const unsigned nchunks = *a.nchunks;
+    Appender app_acc, app_band;
+    unsigned long long n_items = 0, n_screen_acc = 0;
+    for (unsigned c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const uint4 ch = a.chunks[c];
+        const unsigned I = ch.x;
+        const unsigned r0 = a.r_row0[I], nvI = a.r_nvalid[I];
+        for (unsigned e = ch.y; e < ch.z; ++e) {
+            const unsigned J = a.jlist[e];
+            const unsigned c0 = a.s_row0[J], nvJ = a.s_nvalid[J];
+            float acc[kPR][kPC];
+#pragma unroll
+            for (int i = 0; i < kPR; ++i)
+#pragma unroll
+                for (int j = 0; j < kPC; ++j) acc[i][j] = 0.f;
+            for (int k0 = 0; k0 < a.d; k0 += kPK) {
+                __syncthreads();
+                for (int idx = threadIdx.x; idx < kPK * kTileR; idx += kPT) {
+                    const int r = idx / kPK, k = idx % kPK;
+                    sR[k][r] = (k0 + k < a.d) ? a.rx[(size_t)(r0 + r) * a.d + k0 + k] : 0.f;
+                }
+                for (int idx = threadIdx.x; idx < kPK * kTileS; idx += kPT) {
+                    const int r = idx / kPK, k = idx % kPK;
+                    sS[k][r] = (k0 + k < a.d) ? a.sx[(size_t)(c0 + r) * a.d + k0 + k] : 0.f;
+                }
+                __syncthreads();
+                const int kmax = min(kPK, a.d - k0);
+                for (int k = 0; k < kmax; ++k) {
+                    float rv[kPR], sv[kPC];
+#pragma unroll
+                    for (int i = 0; i < kPR; ++i) rv[i] = sR[k][i * 16 + ty];   // rows i*16+ty, cols j*16+tx
+#pragma unroll
+                    for (int j = 0; j < kPC; ++j) sv[j] = sS[k][j * 16 + tx];
+#pragma unroll
+                    for (int i = 0; i < kPR; ++i)
+#pragma unroll
+                        for (int j = 0; j < kPC; ++j) {
+                            const float t = rv[i] - sv[j];
+                            acc[i][j] = fmaf(t, t, acc[i][j]);
+                        }
+                }
+            }
+            // classify: groups of 32 pairs (2 rows x 16 cols) so that emission stays warp-uniform
+#pragma unroll
+            for (int g = 0; g < kPR / 2; ++g) {
+                uint32_t amask = 0, bmask = 0;
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                    for (int j = 0; j < kPC; ++j) {
+                        const int i = g * 2 + h;
+                        const unsigned row = i * 16 + ty, col = j * 16 + tx;
+                        const float s = acc[i][j];
+                        if (s > a.tout || row >= nvI || col >= nvJ) continue;
+                        if (a.jp.self_join && c0 + col <= r0 + row) continue;
+                        if (s <= a.tin) amask |= 1u << (h * 16 + j);
+                        else bmask |= 1u << (h * 16 + j);
+                    }
+                unsigned ta, tb;
+                const unsigned pa = warp_excl_scan(__popc(amask), ta);
+                const unsigned pb = warp_excl_scan(__popc(bmask), tb);
+                if (ta) {
+                    unsigned long long pos = app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap) + pa;
+                    uint32_t mk = amask;
+                    while (mk) {
+                        const int b = __ffs(mk) - 1;
+                        mk &= mk - 1;
+                        const unsigned row = (g * 2 + (b >> 4)) * 16 + ty, col = (b & 15) * 16 + tx;
+                        if (pos < a.acc_cap) a.acc[pos] = key_of(a.jp, a.r_perm[r0 + row], a.s_perm[c0 + col]);
+                        ++pos;
+                    }
+                    n_screen_acc += __popc(amask);
+                }
+                if (tb) {
+                    unsigned long long pos = app_band.reserve(tb, &a.ctr->band_reserved, a.band, a.band_cap) + pb;
+                    uint32_t mk = bmask;
+                    while (mk) {
+                        const int b = __ffs(mk) - 1;
+                        mk &= mk - 1;
+                        const unsigned row = (g * 2 + (b >> 4)) * 16 + ty, col = (b & 15) * 16 + tx;
+                        if (pos < a.band_cap) a.band[pos] = key_of(a.jp, a.r_perm[r0 + row], a.s_perm[c0 + col]);
+                        ++pos;
+                    }
+                }
+            }
+            ++n_items;
+        }
+    }
+    app_acc.pad(a.acc, a.acc_cap);
+    app_band.pad(a.band, a.band_cap);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n_screen_acc += __shfl_xor_sync(0xffffffffu, n_screen_acc, o);
+    if (lane_id() == 0) {
+        if (app_acc.valid) atomicAdd(&a.ctr->acc_valid, app_acc.valid);
+        if (app_band.valid) atomicAdd(&a.ctr->band_valid, app_band.valid);
+        if (n_screen_acc) atomicAdd(&a.ctr->screen_accept, n_screen_acc);
+        if (threadIdx.x == 0 && n_items) atomicAdd(&a.ctr->items, n_items);
+    }
+}
+
+// ------------------------------------------------------------------ FP64 refinement
+struct RefineArgs {
+    const uint64_t* band;
+    unsigned long long band_cap;
+    const float* R;       // caller's rows, original order
+    const float* S;
+    int d;
+    JoinParams jp;
+    uint64_t* acc;
+    unsigned long long acc_cap;
+    Counters* ctr;
+};
+
+TJ_DEV double seq_d2(const float* x, const float* y, int d) {
+    double acc = 0.0;
+    if ((d & 3) == 0 && ((((uintptr_t)x) | ((uintptr_t)y)) & 15) == 0) {
+        const float4* x4 = (const float4*)x;
+        const float4* y4 = (const float4*)y;
+        for (int k = 0; k < d / 4; ++k) {
+            const float4 a = __ldg(x4 + k), b = __ldg(y4 + k);
+            double t;
+            t = __dsub_rn((double)a.x, (double)b.x); acc = __dadd_rn(acc, __dmul_rn(t, t));
+            t = __dsub_rn((double)a.y, (double)b.y); acc = __dadd_rn(acc, __dmul_rn(t, t));
+            t = __dsub_rn((double)a.z, (double)b.z); acc = __dadd_rn(acc, __dmul_rn(t, t));
+            t = __dsub_rn((double)a.w, (double)b.w); acc = __dadd_rn(acc, __dmul_rn(t, t));
+        }
+    } else {
+        for (int k = 0; k < d; ++k) {
+            const double t = __dsub_rn((double)__ldg(x + k), (double)__ldg(y + k));
+            acc = __dadd_rn(acc, __dmul_rn(t, t));
+        }
+    }
+    return acc;
+}
+
+__global__ void refine_kernel(const RefineArgs a) {
+    const unsigned long long n = min(a.ctr->band_reserved, a.band_cap);
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    const unsigned long long start = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long n_acc = 0;
+    // loop count is warp-uniform so the ballot below is well formed
+    const unsigned long long warp_start = start & ~31ull;
+    for (unsigned long long w = warp_start; w < n; w += stride) {
+        const unsigned long long idx = w + lane_id();
+        bool ok = false;
+        uint64_t key = kSentinel;
+        if (idx < n) {
+            key = a.band[idx];
+            if (key != kSentinel) {
+                const uint64_t local = key - a.jp.key_off;
+                const uint64_t i = local / (uint64_t)a.jp.n_cols, j = local - i * (uint64_t)a.jp.n_cols;
+                const double d2 = seq_d2(a.R + (size_t)i * a.d, a.S + (size_t)j * a.d, a.d);
+                ok = d2 <= a.jp.T;
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (m) {
+            unsigned long long base = 0;
+            if (lane_id() == 0) base = atomicAdd(&a.ctr->acc_reserved, (unsigned long long)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (ok) {
+                const unsigned long long pos = base + __popc(m & ((1u << lane_id()) - 1u));
+                if (pos < a.acc_cap) a.acc[pos] = key;
+            }
+            n_acc += (lane_id() == 0) ? __popc(m) : 0;
+        }
+    }
+    if (lane_id() == 0 && n_acc) {
+        atomicAdd(&a.ctr->acc_valid, n_acc);
+        atomicAdd(&a.ctr->refine_accept, n_acc);
+    }
+}
+
+// ------------------------------------------------------------------ canonical output helpers
+__global__ void expand_directed_kernel(const uint64_t* upper, unsigned long long slots, uint64_t* out, long long N) {
+    const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < slots) {
+        const uint64_t k = upper[i];
+        out[2 * i] = k;
+        if (k == kSentinel) {
+            out[2 * i + 1] = kSentinel;
+        } else {
+            const uint64_t lo = k / (uint64_t)N, hi = k - lo * (uint64_t)N;
+            out[2 * i + 1] = hi * (uint64_t)N + lo;
+        }
+    }
+    if (i < (unsigned long long)N) out[2 * slots + i] = i * (uint64_t)N + i;
+}
+
+__global__ void decode_kernel(const uint64_t* keys, long long n, long long n_cols, int64_t* io, int64_t* jo) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint64_t k = keys[t];
+    const uint64_t i = k / (uint64_t)n_cols;
+    io[t] = (int64_t)i;
+    jo[t] = (int64_t)(k - i * (uint64_t)n_cols);
+}
+
+}  // namespace
+
+void screen_plain(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st) {
+    const Side& R = *g.R;
+    const Side& S = *g.S;
+    if (R.screen != kScreenPlain || S.screen != kScreenPlain) fail(-1, "screen_plain needs FP32 sides");
+    PlainArgs a;
+    a.chunks = g.cand->chunks.p;
+    a.nchunks = g.cand->dev_counts.p + 1;
+    a.jlist = g.cand->jlist.p;
+    a.rx = R.xs.p;
+    a.sx = S.xs.p;
+    a.r_row0 = g.tR->row0.p;
+    a.r_nvalid = g.tR->nvalid.p;
+    a.r_perm = R.perm.p;
+    a.s_row0 = g.tS->row0.p;
+    a.s_nvalid = g.tS->nvalid.p;
+    a.s_perm = S.perm.p;
+    a.d = R.d;
+    // FP32 sum of d squared FP32 differences with FMA: |s - D| <= gamma_{d+2} D + d 2^-148 (u = 2^-24)
+    const double u = 0x1p-24, nu = (double)(R.d + 4) * u;
+    const double gam = nu / (1.0 - nu);
+    const double tiny = (double)(R.d + 4) * 0x1p-147;
+    const double tin = (g.jp.Tm - tiny) * (1.0 - gam) * (1.0 - 0x1p-30);
+    const double tout = (g.jp.Tp + tiny) * (1.0 + gam) * (1.0 + 0x1p-30) + tiny;
+    a.tin = tin > 0 ? (float)tin : -1.f;    // rounding to nearest then nudging down keeps it a lower bound
+    if (a.tin > 0 && (double)a.tin > tin) a.tin = nextafterf(a.tin, 0.f);
+    a.tout = (float)tout;
+    if ((double)a.tout < tout) a.tout = nextafterf(a.tout, INFINITY);
+    a.jp = g.jp;
+    a.acc = eb.acc;
+    a.acc_cap = eb.acc_cap;
+    a.band = eb.band;
+    a.band_cap = eb.band_cap;
+    a.ctr = eb.ctr;
+    launch(plain_kernel, num_sms() * 2, kPT, 0, st, a);
+    TJ_CUDA(cudaGetLastError());
+}
+
+void refine_band(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st) {
+    RefineArgs a;
+    a.band = eb.band;
+    a.band_cap = eb.band_cap;
+    a.R = (const float*)g.R->src;
+    a.S = (const float*)g.S->src;
+    a.d = g.R->d;
+    a.jp = g.jp;
+    a.acc = eb.acc;
+    a.acc_cap = eb.acc_cap;
+    a.ctr = eb.ctr;
+    launch(refine_kernel, num_sms() * 8, 256, 0, st, a);
+    TJ_CUDA(cudaGetLastError());
+}
+
+void expand_directed(const uint64_t* upper, unsigned long long slots, uint64_t* out, long long N, cudaStream_t st) {
+    const unsigned long long n = slots > (unsigned long long)N ? slots : (unsigned long long)N;
+    if (n == 0) return;
+    launch(expand_directed_kernel, (unsigned)((n + 255) / 256), 256, 0, st, upper, slots, out, N);
+    TJ_CUDA(cudaGetLastError());
+}
+
+void decode_pairs(const uint64_t* keys, long long n, long long n_cols, int64_t* i_out, int64_t* j_out,
+                  cudaStream_t st) {
+    if (n <= 0) return;
+    launch(decode_kernel, (unsigned)((n + 255) / 256), 256, 0, st, keys, n, n_cols, i_out, j_out);
+    TJ_CUDA(cudaGetLastError());
+}
+
+}  // namespace tj

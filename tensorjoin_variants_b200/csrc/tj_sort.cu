@@ -1,0 +1,219 @@
+// Device exclusive scan and LSD radix sort, written for this library.
+//
+// Radix sort: 8-bit digits, least significant first, only the low `bits` bits
+// of each key are considered (bit width trimmed to the key range, as the
+// output stage trims it to ceil(log2(max key + 2))).  Each pass is
+//   1. per-block digit histogram (digit-major [256][blocks]),
+//   2. device-wide exclusive scan of that table,
+//   3. stable scatter: every warp ranks its keys round by round with
+//      __match_any_sync, warps are combined in order through shared counters.
+// Stability across passes makes the whole sort correct for any bit width.
+//
+// It replaces the CUB SortKeys call of the reference's output stage
+// (tensorjoin_20260908_output_audit/src/output.cu:26-31).
+#include "tj_internal.h"
+
+namespace tj {
+
+namespace {
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+// Block-wide exclusive scan of kScanTile u32 values; writes block totals.
+__global__ void __launch_bounds__(kScanThreads) scan_tiles(const uint32_t* in, uint32_t* out, size_t n,
+                                                           uint32_t* sums) {
+    __shared__ uint32_t warp_tot[32];
+    const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t local = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = (base + k < n) ? in[base + k] : 0u;
+        local += v[k];
+    }
+    unsigned tot;
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned pre = warp_excl_scan(local, tot);
+    if (lane == 0) warp_tot[warp] = tot;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned wt = warp_tot[lane], all;
+        unsigned wp = warp_excl_scan(wt, all);
+        warp_tot[lane] = wp;
+        if (lane == 0 && sums) sums[blockIdx.x] = all;
+    }
+    __syncthreads();
+    uint32_t run = pre + warp_tot[warp];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+}
+
+__global__ void add_block_offsets(uint32_t* out, size_t n, const uint32_t* offs) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += offs[i / kScanTile];
+}
+
+__global__ void write_total(const uint32_t* in_last, const uint32_t* out_last, uint32_t* total) {
+    *total = *in_last + *out_last;
+}
+
+}  // namespace
+
+size_t scan_workspace_elems(size_t n) {
+    size_t total = 0;
+    while (n > 1) {
+        n = (n + kScanTile - 1) / kScanTile;
+        total += n + 1;
+    }
+    return total + 1;
+}
+
+// out[i] = sum_{k<i} in[k]; optional *total = sum of all (device pointer).
+// `ws` needs scan_workspace_elems(n) u32 elements.  `in` and `out` may alias.
+void exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* total, uint32_t* ws,
+                        cudaStream_t st) {
+    if (n == 0) {
+        if (total) cudaMemsetAsync(total, 0, sizeof(uint32_t), st);
+        return;
+    }
+    const size_t nb = (n + kScanTile - 1) / kScanTile;
+    // keep a copy of the last input element when aliasing in/out, for the total
+    uint32_t* last_copy = ws;  // 1 element
+    uint32_t* sums = ws + 1;
+    if (total) cudaMemcpyAsync(last_copy, in + (n - 1), sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+    launch(scan_tiles, (unsigned)nb, kScanThreads, 0, st, in, out, n, nb > 1 ? sums : nullptr);
+    if (nb > 1) {
+        exclusive_scan_u32(sums, sums, nb, nullptr, sums + nb, st);
+        launch(add_block_offsets, (unsigned)((n + 255) / 256), 256, 0, st, out, n, sums);
+    }
+    if (total) launch(write_total, 1, 1, 0, st, last_copy, out + (n - 1), total);
+}
+
+// ------------------------------------------------------------------ radix sort
+namespace {
+
+constexpr int kRsThreads = 256;
+constexpr int kRsWarps = kRsThreads / 32;
+constexpr int kRsRounds = 16;                         // keys per thread
+constexpr int kRsTile = kRsThreads * kRsRounds;       // 4096 keys per block
+
+TJ_DEV unsigned digit_of(uint64_t k, int shift) { return (unsigned)(k >> shift) & 0xFFu; }
+
+__global__ void __launch_bounds__(kRsThreads) rs_hist(const uint64_t* keys, size_t n, int shift, uint32_t* hist,
+                                                     unsigned nblocks) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const size_t base = (size_t)blockIdx.x * kRsTile;
+    for (int r = 0; r < kRsRounds; ++r) {
+        const size_t i = base + (size_t)r * kRsThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[digit_of(keys[i], shift)], 1u);
+    }
+    __syncthreads();
+    hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+template <bool kVals>
+__global__ void __launch_bounds__(kRsThreads) rs_scatter(const uint64_t* keys_in, const uint32_t* vals_in,
+                                                        uint64_t* keys_out, uint32_t* vals_out, size_t n, int shift,
+                                                        const uint32_t* offs, unsigned nblocks) {
+    __shared__ uint32_t wcnt[kRsWarps][256];
+    __shared__ uint32_t gbase[256];
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kRsWarps * 256; i += kRsThreads) (&wcnt[0][0])[i] = 0;
+    gbase[threadIdx.x] = offs[(size_t)threadIdx.x * nblocks + blockIdx.x];
+    __syncthreads();
+
+    // warp w owns the contiguous run [w*512, (w+1)*512) of this block's tile; round r, lane l -> r*32 + l
+    const size_t wbase = (size_t)blockIdx.x * kRsTile + (size_t)warp * (kRsRounds * 32);
+    uint64_t k[kRsRounds];
+    uint32_t v[kRsRounds];
+    uint32_t rank[kRsRounds];
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < kRsRounds; ++r) {
+        const size_t i = wbase + (size_t)r * 32 + lane;
+        const bool ok = i < n;
+        k[r] = ok ? keys_in[i] : 0ull;
+        if (kVals) v[r] = ok ? vals_in[i] : 0u;
+        const unsigned valid = __ballot_sync(0xffffffffu, ok);
+        rank[r] = 0xFFFFFFFFu;
+        if (ok) {
+            const unsigned dg = digit_of(k[r], shift);
+            const unsigned peers = __match_any_sync(valid, dg);
+            const unsigned prev = wcnt[warp][dg];
+            rank[r] = prev + __popc(peers & lt);
+            __syncwarp(valid);
+            if ((peers & lt) == 0) wcnt[warp][dg] = prev + __popc(peers);
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    {   // exclusive prefix over warps for each digit
+        const unsigned dg = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kRsWarps; ++w) {
+            const uint32_t t = wcnt[w][dg];
+            wcnt[w][dg] = run;
+            run += t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kRsRounds; ++r) {
+        if (rank[r] != 0xFFFFFFFFu) {
+            const unsigned dg = digit_of(k[r], shift);
+            const size_t pos = (size_t)gbase[dg] + wcnt[warp][dg] + rank[r];
+            keys_out[pos] = k[r];
+            if (kVals) vals_out[pos] = v[r];
+        }
+    }
+}
+
+}  // namespace
+
+size_t radix_workspace_elems(size_t n) {
+    const size_t nb = (n + kRsTile - 1) / kRsTile;
+    const size_t h = 256 * nb;
+    return 2 * h + scan_workspace_elems(h) + 16;
+}
+
+// Sorts (keys, vals) ascending by the low `bits` bits of keys.  Result lands in keys/vals
+// (ping-pong through keys_tmp/vals_tmp).  vals may be null.  ws: radix_workspace_elems(n) u32.
+void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp, size_t n, int bits,
+                uint32_t* ws, cudaStream_t st) {
+    if (n <= 1 || bits <= 0) return;
+    const unsigned nb = (unsigned)((n + kRsTile - 1) / kRsTile);
+    const size_t h = 256 * (size_t)nb;
+    uint32_t* hist = ws;
+    uint32_t* offs = ws + h;
+    uint32_t* sws = ws + 2 * h;
+    const int passes = (bits + 7) / 8;
+    uint64_t *kin = keys, *kout = keys_tmp;
+    uint32_t *vin = vals, *vout = vals_tmp;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        launch(rs_hist, nb, kRsThreads, 0, st, kin, n, shift, hist, nb);
+        exclusive_scan_u32(hist, offs, h, nullptr, sws, st);
+        if (vals)
+            launch(rs_scatter<true>, nb, kRsThreads, 0, st, kin, vin, kout, vout, n, shift, offs, nb);
+        else
+            launch(rs_scatter<false>, nb, kRsThreads, 0, st, kin, nullptr, kout, nullptr, n, shift, offs, nb);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    if (kin != keys) {
+        cudaMemcpyAsync(keys, kin, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st);
+        if (vals) cudaMemcpyAsync(vals, vin, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+    }
+}
+
+int radix_passes(int bits) { return (bits + 7) / 8; }
+
+}  // namespace tj

@@ -1,0 +1,31 @@
+"""CPU tests of the C-ABI boundary: the library loads and exports every declared symbol (no GPU calls)."""
+import ctypes
+import re
+from pathlib import Path
+
+from tensorjoin_variants_b200 import _lib
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "tensorjoin.h"
+
+
+def declared_functions():
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"\b(tj_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_declares_expected_api():
+    assert set(declared_functions()) == set(_lib.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    for name in declared_functions():
+        assert hasattr(L, name), name
+    assert L.tj_version() == 1
+    assert isinstance(L.tj_last_error_string(), (bytes, type(None)))
+
+
+def test_structs_match_header_layout():
+    assert ctypes.sizeof(_lib.Options) == 16
+    assert ctypes.sizeof(_lib.Stats) == 11 * 8 + 6 * 8
+    assert ctypes.sizeof(_lib.BatchJoin) == 48

@@ -1,0 +1,215 @@
+"""GPU parity: every path's pair set is bit-identical to the CPU oracle (same seeded inputs, same T).
+
+The tolerance is zero: the pair set is discrete and the FP64 refinement uses the
+oracle's summation order.  Pairs are compared as canonical uint64 keys.
+"""
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import tensorjoin_variants_b200 as tj
+from tensorjoin_variants_b200 import _lib
+from tensorjoin_variants_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+G = json.loads((GOLDEN / "golden.json").read_text())
+FLOAT_SCREENS = ["plain", "bf16", "fp16"]
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<u8").tobytes()).hexdigest()
+
+
+def gpu_keys(R, S, T, mode, screen, **kw):
+    Rt = torch.from_numpy(np.ascontiguousarray(R)).cuda()
+    St = None if S is None else torch.from_numpy(np.ascontiguousarray(S)).cuda()
+    res = tj.join_result(Rt, St, eps2=T, mode=mode, screen=screen, **kw)
+    k = res.keys().cpu().numpy().view(np.uint64)
+    i, j = res.pairs()
+    n_cols = R.shape[0] if S is None else S.shape[0]
+    assert np.array_equal(i.cpu().numpy(), (k // np.uint64(n_cols)).astype(np.int64))
+    assert np.array_equal(j.cpu().numpy(), (k % np.uint64(n_cols)).astype(np.int64))
+    return k, res.stats
+
+
+def oracle_keys(R, S, T, mode):
+    return oracle.join_f32(R, S, T, mode)
+
+
+def assert_same(got, want, label=""):
+    if not np.array_equal(got, want):
+        extra = np.setdiff1d(got, want)
+        missing = np.setdiff1d(want, got)
+        raise AssertionError(f"{label}: got {len(got)} want {len(want)}; extra {extra[:10]} missing {missing[:10]}")
+
+
+@pytest.mark.parametrize("screen", FLOAT_SCREENS)
+def test_uniform16_full_config(screen):
+    """Config 1 at full size (20,000 x 16, ~32 neighbours, i < j) against the pinned golden hash."""
+    w = W.uniform16()
+    k, st = gpu_keys(w.R, None, w.T, "upper", screen)
+    assert len(k) == G["uniform16"]["oracle_upper_count"]
+    assert sha(k) == G["uniform16"]["oracle_upper_sha256"]
+    assert st["result_pairs"] == len(k)
+
+
+@pytest.mark.parametrize("screen", FLOAT_SCREENS)
+def test_gds_fixture_directed(screen):
+    """GDS-Join's 100,000-point 2-D test set at eps = 1.0 (directed, self pairs included)."""
+    X = np.load(GOLDEN / "gds_test_dat_f32.npy")
+    g = G["gds_test_dat"]
+    k, _ = gpu_keys(X, None, 1.0, "directed", screen)
+    assert len(k) == g["oracle_directed_count"]
+    assert sha(k) == g["oracle_directed_sha256"]
+
+
+@pytest.mark.parametrize("screen", FLOAT_SCREENS)
+def test_mixture_rs_small(screen):
+    w = W.mixture64(n=6000, samples=1 << 16, screen=screen)
+    k, st = gpu_keys(w.R, w.S, w.T, "rs", screen)
+    assert_same(k, oracle_keys(w.R, w.S, w.T, "rs"), screen)
+    assert st["pairs_screened"] <= w.candidate_pairs_all
+
+
+@pytest.mark.parametrize("screen", ["fp16", "bf16", "plain"])
+def test_factor512_small(screen):
+    w = W.factor512(n=3000, samples=1 << 16)
+    k, st = gpu_keys(w.R, w.S, w.T, "rs", screen)
+    assert_same(k, oracle_keys(w.R, w.S, w.T, "rs"), screen)
+    assert st["band"] >= 0
+
+
+@pytest.mark.parametrize("screen", FLOAT_SCREENS)
+@pytest.mark.parametrize("d", [1, 3, 63, 65, 130])
+def test_ragged_dimensions(screen, d):
+    rng = np.random.default_rng(100 + d)
+    R = rng.standard_normal((700, d)).astype(np.float32)
+    S = rng.standard_normal((900, d)).astype(np.float32)
+    T = float(np.quantile(((R[:50, None, :] - S[None, :200, :]) ** 2).sum(-1), 0.01))
+    k, _ = gpu_keys(R, S, T, "rs", screen)
+    assert_same(k, oracle_keys(R, S, T, "rs"), f"{screen} d={d}")
+
+
+@pytest.mark.parametrize("screen", FLOAT_SCREENS)
+def test_self_join_modes(screen):
+    rng = np.random.default_rng(21)
+    X = rng.random((2500, 24)).astype(np.float32)
+    X[2000:2100] = X[:100]            # exact duplicates: d2 == 0
+    T = 0.35
+    for mode in ("upper", "directed"):
+        k, _ = gpu_keys(X, None, T, mode, screen)
+        assert_same(k, oracle_keys(X, None, T, mode), f"{screen} {mode}")
+
+
+@pytest.mark.parametrize("screen", FLOAT_SCREENS)
+def test_edge_cases(screen):
+    rng = np.random.default_rng(22)
+    one = rng.random((1, 8)).astype(np.float32)
+    many = rng.random((300, 8)).astype(np.float32)
+    # single row against many, and many against a single row
+    assert_same(gpu_keys(one, many, 0.5, "rs", screen)[0], oracle_keys(one, many, 0.5, "rs"))
+    assert_same(gpu_keys(many, one, 0.5, "rs", screen)[0], oracle_keys(many, one, 0.5, "rs"))
+    # eps = 0: only exact duplicates
+    dup = np.concatenate([many, many[:37]])
+    assert_same(gpu_keys(dup, None, 0.0, "upper", screen)[0], oracle_keys(dup, None, 0.0, "upper"))
+    # all-zero input at a tiny eps accepts every pair; +-1 blocks at eps = 0 give the two sign blocks
+    Z = np.zeros((300, 32), np.float32)
+    assert len(gpu_keys(Z, None, 2.0 ** -40, "directed", screen)[0]) == 300 * 300
+    P = np.concatenate([np.ones((130, 64), np.float32), -np.ones((140, 64), np.float32)])
+    kp, _ = gpu_keys(P, None, 0.0, "directed", screen)
+    assert_same(kp, oracle_keys(P, None, 0.0, "directed"))
+
+
+def test_empty_inputs():
+    R = torch.zeros((0, 16), device="cuda")
+    S = torch.rand((10, 16), device="cuda")
+    i, j = tj.join(R, S, 0.5)
+    assert i.numel() == 0 and j.numel() == 0
+    i, j = tj.join(S, R, 0.5)
+    assert i.numel() == 0
+
+
+def test_capacity_retry():
+    """A tiny initial capacity forces the overflow-and-retry pass; the result must not change."""
+    w = W.uniform16(n=4000)
+    want = oracle_keys(w.R, None, w.T, "upper")
+    for screen in FLOAT_SCREENS:
+        k, st = gpu_keys(w.R, None, w.T, "upper", screen, capacity=512)
+        assert st["retries"] >= 1
+        assert_same(k, want, screen)
+
+
+def test_bad_inputs_fail_closed():
+    X = torch.rand((500, 16), device="cuda")
+    X[17, 3] = float("nan")
+    with pytest.raises(_lib.TJError) as e:
+        tj.self_join(X, 0.3)
+    assert e.value.code == -3
+    Y = torch.rand((500, 16), device="cuda") * 1e5
+    with pytest.raises(_lib.TJError) as e:
+        tj.self_join(Y, 0.3, screen="fp16")
+    assert e.value.code == -4
+    with pytest.raises(_lib.TJError):
+        tj.join_result(torch.rand((10, 4), device="cuda"), None, 0.1, mode="rs", screen="int8limb")
+
+
+@pytest.mark.parametrize("screen", ["bf16", "fp16"])
+def test_metamorphic(screen):
+    rng = np.random.default_rng(23)
+    R = rng.standard_normal((1500, 40)).astype(np.float32)
+    S = rng.standard_normal((1700, 40)).astype(np.float32)
+    T = 40.0
+    base, _ = gpu_keys(R, S, T, "rs", screen)
+    assert_same(base, oracle_keys(R, S, T, "rs"))
+    assert_same(gpu_keys(-R, -S, T, "rs", screen)[0], base, "negate")
+    sc = np.float32(2.0 ** 8)
+    assert_same(gpu_keys(R * sc, S * sc, T * 2.0 ** 16, "rs", screen)[0], base, "scale")
+    perm = rng.permutation(40)
+    sign = np.where(rng.random(40) < 0.5, -1, 1).astype(np.float32)
+    assert_same(gpu_keys(R[:, perm] * sign, S[:, perm] * sign, T, "rs", screen)[0], base, "dims")
+    rp = rng.permutation(1500)
+    kp, _ = gpu_keys(R[rp], S, T, "rs", screen)
+    inv = np.argsort(rp)
+    i, j = oracle.keys_to_ij(kp, 1700)
+    remapped = np.sort(rp[i].astype(np.uint64) * np.uint64(1700) + j.astype(np.uint64))
+    assert_same(remapped, base, "row permutation")
+    assert len(inv) == 1500
+
+
+def test_host_arrays_roundtrip():
+    """Host (numpy) inputs: copied in, joined on the GPU, results returned on the host."""
+    w = W.uniform16(n=3000)
+    i, j = tj.self_join(w.R, w.eps)
+    assert isinstance(i, torch.Tensor) and not i.is_cuda
+    k = i.numpy().astype(np.uint64) * np.uint64(3000) + j.numpy().astype(np.uint64)
+    assert_same(k, oracle_keys(w.R, None, w.eps * w.eps, "upper"))
+
+
+def test_neighbor_table_matches_pairs():
+    w = W.uniform16(n=3000)
+    res = tj.join_result(torch.from_numpy(w.R).cuda(), None, eps2=w.T, mode="directed")
+    counts, flat = res.neighbor_table()
+    i, j = res.pairs()
+    assert int(counts.sum()) == res.count
+    assert torch.equal(torch.bincount(i, minlength=3000).to(torch.int32), counts)
+    assert torch.equal(flat, j)
+
+
+def test_index_structure():
+    w = W.mixture64(n=20000, samples=1 << 14)
+    idx = tj.build_index(torch.from_numpy(w.R).cuda(), w.eps)
+    perm = idx.perm.cpu().numpy()
+    assert np.array_equal(np.sort(perm), np.arange(20000))
+    keys = idx.keys.cpu().numpy()
+    assert np.all(keys[1:] >= keys[:-1])
+    cs = idx.cell_start.cpu().numpy()
+    assert cs[0] == 0 and cs[-1] == 20000 and np.all(np.diff(cs) > 0)
+    assert np.all(keys[cs[:-1]][1:] != keys[cs[:-1]][:-1])
+    tp = idx.tile_pairs.cpu().numpy()
+    assert tp.shape[1] == 2 and len(tp) >= idx.n_tiles // 2
