@@ -230,7 +230,7 @@ void run_join(const void* R, long long nR, const void* S, long long nS, int d, i
               int screen, const tj_options* opt, tj_result* res, cudaStream_t st) {
     const bool self = mode != TJ_MODE_RS;
     if (self) { S = R; nS = nR; }
-    if (!R || (nR > 0 && !S)) fail(TJ_ERR_INVALID, "null input pointer");
+    if ((nR > 0 && !R) || (nS > 0 && !S)) fail(TJ_ERR_INVALID, "null input pointer");
     if (d <= 0 || nR < 0 || nS < 0) fail(TJ_ERR_INVALID, "invalid shape");
     if (nR >= (1ll << 32) || nS >= (1ll << 32)) fail(TJ_ERR_INVALID, "more than 2^32 - 1 rows per side");
     if (!(eps2 >= 0.0) || std::isinf(eps2)) fail(TJ_ERR_INVALID, "eps2 must be finite and >= 0");

@@ -155,8 +155,10 @@ def test_bad_inputs_fail_closed():
     with pytest.raises(_lib.TJError) as e:
         tj.self_join(Y, 0.3, screen="fp16")
     assert e.value.code == -4
-    with pytest.raises(_lib.TJError):
-        tj.join_result(torch.rand((10, 4), device="cuda"), None, 0.1, mode="rs", screen="int8limb")
+    F = torch.rand((10, 4), device="cuda")
+    with pytest.raises(_lib.TJError) as e:   # the int8-limb screen takes int14 data only
+        tj.join_result(F, F, 0.1, mode="rs", screen="int8limb")
+    assert e.value.code == -7
 
 
 @pytest.mark.parametrize("screen", ["bf16", "fp16"])
