@@ -130,6 +130,19 @@ int tj_join_batched(const tj_batch_join* joins, int32_t njoins, int32_t screen, 
 int tj_batch_offsets(const tj_result* res, int64_t* offsets_host /* njoins + 1 */);
 int tj_batch_pairs(const tj_result* res, int64_t* i_out, int64_t* j_out, void* stream);
 
+/* ----------------------------------------------------------------- allocation-free sort */
+
+/* Sort n uint64 keys ascending by their low key_bits bits (1..64) into keys_out (device arrays;
+ * keys_out may equal keys_in) without allocating any device memory.  No counterpart in the
+ * reference: it is the canonical-order radix sort of this library, offered for callers that
+ * cannot allocate at the call site (a fixed arena owned by the host engine, HBM reserved by
+ * another allocator, or no allocation latency allowed between launches).  Its scratch is a
+ * file-scope device array of about 9 MiB held by every GPU that loads the library; n is limited
+ * to 1,048,576 keys (larger n returns TJ_ERR_INVALID).  All calls on a device share that array:
+ * calls that overlap on the GPU race and must be serialised by the caller.  The first call on a
+ * device resolves the array's address (cudaGetSymbolAddress); make it before any stream capture. */
+int tj_sort_keys_noalloc(const uint64_t* keys_in, uint64_t* keys_out, int64_t n, int32_t key_bits, void* stream);
+
 /* ----------------------------------------------------------------- misc */
 const char* tj_last_error_string(void);
 int tj_version(void);

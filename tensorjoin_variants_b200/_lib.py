@@ -27,7 +27,7 @@ EXPORTS = [
     "tj_join", "tj_result_count", "tj_result_stats", "tj_result_pairs", "tj_result_keys",
     "tj_result_neighbor_table", "tj_result_free", "tj_index_build", "tj_index_info", "tj_index_copy",
     "tj_index_free", "tj_join_batched", "tj_batch_offsets", "tj_batch_pairs", "tj_last_error_string",
-    "tj_version", "tj_device_sm_count", "tj_kernel_launches",
+    "tj_version", "tj_device_sm_count", "tj_kernel_launches", "tj_sort_keys_noalloc",
 ]
 
 
@@ -89,6 +89,8 @@ def lib() -> C.CDLL:
     L.tj_version.restype = C.c_int
     L.tj_device_sm_count.restype = C.c_int
     L.tj_kernel_launches.restype = C.c_int64
+    L.tj_sort_keys_noalloc.argtypes = [P, P, I64, I32, P]
+    L.tj_sort_keys_noalloc.restype = C.c_int
     for name in ("tj_join", "tj_result_stats", "tj_result_pairs", "tj_result_keys", "tj_result_neighbor_table",
                  "tj_index_build", "tj_index_info", "tj_index_copy", "tj_join_batched", "tj_batch_offsets",
                  "tj_batch_pairs"):

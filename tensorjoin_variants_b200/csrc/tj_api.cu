@@ -24,6 +24,7 @@ thread_local std::string g_last_error;
 }
 
 void fail(int code, const std::string& msg) { throw Error{code, msg}; }
+void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 void check_cuda(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return;

@@ -17,6 +17,7 @@ struct Error {
     std::string msg;
 };
 [[noreturn]] void fail(int code, const std::string& msg);
+void set_last_error(const std::string& msg);
 void check_cuda(cudaError_t e, const char* what);
 #define TJ_CUDA(x) ::tj::check_cuda((x), #x)
 
