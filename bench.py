@@ -46,8 +46,9 @@ METRIC = "dist_evals_per_s"
 UNIT = "pairs/s"
 WORKLOADS = {
     "factor512": dict(fn="factor512", screen="fp16", mode="rs"),
-    "mixture64": dict(fn="mixture64", screen="bf16", mode="rs"),
+    "mixture64": dict(fn="mixture64", screen="bf16x3", mode="rs"),
     "uniform16": dict(fn="uniform16", screen="plain", mode="upper"),
+    "int14x128": dict(fn="int14x128", screen="int8limb", mode="upper"),
 }
 
 
@@ -58,7 +59,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="factor512")
-    ap.add_argument("--screen", default=None, help="override the workload's screen (plain/bf16/fp16)")
+    ap.add_argument("--screen", default=None, help="override the workload's screen (plain/bf16/fp16/int8limb)")
     ap.add_argument("--n", type=int, default=0, help="rows per side (0 = the configuration's size)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 GPU baseline run")
     ap.add_argument("--no-e2e", action="store_true")
@@ -263,24 +264,31 @@ def main() -> None:
     peaks = measured_peaks()
     screen_ms = statistics.mean(s["ms_screen"] for s in stats)
     d = int(w.R.shape[1])
-    flops = 2.0 * d * pairs
+    # algorithmic ops per screened pair: 2 d (one 16-bit dot product) or 8 d (four int8 limb products)
+    flops = (8.0 if screen == "int8limb" else 6.0 if screen.endswith("x3") else 2.0) * d * pairs
+    peak_note = f"{peaks['source']} bf16_tflops_sustained (dense fp16 = bf16 rate)"
     if screen == "plain":
         achieved, unit, bound = flops / (screen_ms / 1000.0) / 1e12, "TFLOP/s", "simt"
         peak = None
+    elif screen == "int8limb":
+        achieved, unit, bound = flops / (screen_ms / 1000.0) / 1e12, "TOP/s", "tensor"
+        peak = 2.0 * peaks["tflops_sustained"]
+        peak_note = f"2 x {peaks['source']} bf16_tflops_sustained (dense int8 rate = 2 x bf16; no int8 measurement)"
     else:
         achieved, unit, bound = flops / (screen_ms / 1000.0) / 1e12, "TFLOP/s", "tensor"
         peak = peaks["tflops_sustained"]
-    roofline = {"bound": bound, "kernel": "screen_tc_kernel" if screen != "plain" else "plain_kernel",
+    kname = {"plain": "plain_kernel", "int8limb": "screen_i8_kernel"}.get(screen, "screen_tc_kernel")
+    roofline = {"bound": bound, "kernel": kname,
                 "achieved": achieved, "peak": peak, "unit": unit,
                 "frac": (achieved / peak) if peak else None,
-                "peak_source": f"{peaks['source']} bf16_tflops_sustained (dense fp16 = bf16 rate)",
-                "traffic": committed_traffic("screen_tc_kernel", args.workload),
+                "peak_source": peak_note,
+                "traffic": committed_traffic(kname, args.workload),
                 "screen_ms": screen_ms, "flops_per_launch": flops}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": screen if screen != "plain" else "f32", "data": "synthetic",
+        "vs_baseline": None, "dtype": {"plain": "f32", "int8limb": "s8"}.get(screen, screen), "data": "synthetic",
         "config": workload_config(args, w), "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
         "result_pairs": int(count), "stats": {k: st[k] for k in (
             "pairs_all", "pairs_screened", "tile_pairs", "screen_accept", "band", "refine_accept", "rare_checks",
@@ -293,7 +301,10 @@ def main() -> None:
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        resp = tj.join_result(R, S, eps2=T, mode=mode, screen="plain")
+        # int14 data run the plain path on exact FP32 copies (same predicate: d2 is exact in FP64)
+        Rp = R.float() if R.dtype == torch.int16 else R
+        Sp = None if S is None else (S.float() if S.dtype == torch.int16 else S)
+        resp = tj.join_result(Rp, Sp, eps2=T, mode=mode, screen="plain")
         ip, jp = resp.pairs()
         e1.record(stream)
         torch.cuda.synchronize()

@@ -56,6 +56,8 @@ extern "C" {
 #define TJ_SCREEN_BF16 1        /* tcgen05 BF16 x BF16 -> FP32 screen + certified band + FP64 refinement */
 #define TJ_SCREEN_FP16 2        /* tcgen05 FP16 x FP16 -> FP32 screen + certified band + FP64 refinement */
 #define TJ_SCREEN_INT8LIMB 3    /* int14 via two int8 limbs, exact INT32 tensor-core products (int16 input) */
+#define TJ_SCREEN_BF16X3 4      /* BF16 hi + lo operand limbs, 3 products per k into one FP32 accumulator */
+#define TJ_SCREEN_FP16X3 5      /* FP16 hi + lo operand limbs, 3 products per k into one FP32 accumulator */
 
 typedef struct tj_result tj_result;
 typedef struct tj_index tj_index;

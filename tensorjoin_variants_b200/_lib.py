@@ -20,7 +20,7 @@ ERRORS = {
 }
 DTYPE = {"f32": 0, "i16": 1}
 MODE = {"rs": 0, "upper": 1, "directed": 2}
-SCREEN = {"plain": 0, "bf16": 1, "fp16": 2, "int8limb": 3}
+SCREEN = {"plain": 0, "bf16": 1, "fp16": 2, "int8limb": 3, "bf16x3": 4, "fp16x3": 5}
 
 # Every symbol include/tensorjoin.h declares (checked by the CPU test suite).
 EXPORTS = [

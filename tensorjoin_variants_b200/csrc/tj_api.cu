@@ -155,7 +155,7 @@ struct Events {
 }  // namespace
 
 // Threshold constants of the certificate.
-JoinParams make_params(double T, int d, int kpad, long long nr, long long nc, bool self_join) {
+JoinParams make_params(double T, int d, int kpad, int split, long long nr, long long nc, bool self_join) {
     JoinParams jp;
     memset(&jp, 0, sizeof(jp));
     jp.T = T;
@@ -165,8 +165,11 @@ JoinParams make_params(double T, int d, int kpad, long long nr, long long nc, bo
     jp.Tm = T / (1.0 + g64) * (1.0 - 0x1p-50);
     jp.Tp = T / (1.0 - g64) * (1.0 + 0x1p-50);
     jp.gn = 2.0 * (double)(d + 2) * 0x1p-53;
-    jp.gmma = (double)(kpad + 64) * 0x1p-22;
-    jp.cabs = (double)(kpad + 64) * 0x1p-125;
+    // tensor-core accumulation premise: every FP32 accumulation step of the K exact products errs by at most
+    // 2 ulp of the running |sum| (2x the round-to-nearest bound, covering truncating alignment), + 64 steps slack
+    const double kacc = (double)kpad * (split ? 3.0 : 1.0);
+    jp.gmma = (kacc + 64.0) * 0x1p-22;
+    jp.cabs = (kacc + 64.0) * 0x1p-125;
     jp.key_off = 0;
     jp.n_rows = nr;
     jp.n_cols = nc;
@@ -241,7 +244,8 @@ void run_join(const void* R, long long nR, const void* S, long long nS, int d, i
         fail(TJ_ERR_UNSUPPORTED, "the int8-limb screen needs int16 (int14) input");
     if (dtype == TJ_DTYPE_I16 && screen == TJ_SCREEN_PLAIN)
         fail(TJ_ERR_UNSUPPORTED, "plain screen on int16 input is not provided; use TJ_SCREEN_INT8LIMB");
-    if (screen == TJ_SCREEN_INT8LIMB) fail(TJ_ERR_UNSUPPORTED, "int8-limb screen not built in this version");
+    if (screen == TJ_SCREEN_INT8LIMB && !(eps2 == std::floor(eps2) && eps2 < 0x1p62))
+        fail(TJ_ERR_INVALID, "the int8-limb screen needs an integer eps2 below 2^62");
     const int chunk_items = (opt && opt->chunk_items > 0) ? opt->chunk_items : 64;
 
     memset(&res->stats, 0, sizeof(res->stats));
@@ -260,27 +264,30 @@ void run_join(const void* R, long long nR, const void* S, long long nS, int d, i
     DBuf<Counters> ctr(1, st);
     launch(zero_counters, 1, 32, 0, st, ctr.p, 0);
     DBuf<FrameParams> fp(1, st);
+    DBuf<float> center((size_t)d, st);
     {
         const void* srcs[2] = {R, S};
         const long long ns[2] = {nR, nS};
-        compute_frame(srcs, ns, self ? 1 : 2, d, dtype, fp.p, st);
+        compute_frame(srcs, ns, self ? 1 : 2, d, dtype, fp.p, center.p, st);
     }
     Side sR, sS_;
     sR.src = R; sR.dtype = dtype; sR.n = nR; sR.d = d; sR.screen = screen;
-    prepare_side(sR, fp.p, st, &ctr.p->status);
+    prepare_side(sR, fp.p, center.p, st, &ctr.p->status);
     Side* pS = &sR;
     if (!self) {
         sS_.src = S; sS_.dtype = dtype; sS_.n = nS; sS_.d = d; sS_.screen = screen;
-        prepare_side(sS_, fp.p, st, &ctr.p->status);
+        prepare_side(sS_, fp.p, center.p, st, &ctr.p->status);
         pS = &sS_;
     }
     TileSet tR, tS;
     tile_stats(sR, kTileR, tR, st);
-    tile_stats(*pS, kTileS, tS, st);
+    const bool i8 = screen == TJ_SCREEN_INT8LIMB;
+    tile_stats(*pS, i8 ? 128 : kTileS, tS, st);
     ev.rec(1, st);
-    const JoinParams jp = make_params(eps2, d, sR.kpad, nR, nS, self);
+    const JoinParams jp = make_params(eps2, d, sR.kpad, sR.split, nR, nS, self);
     Candidates cand;
     build_candidates(tR, tS, jp.Tp, self, chunk_items, cand, st);
+    ev.rec(6, st);
     // distance evaluations of the candidate list (read back with the counters)
     launch(pairs_screened_kernel, num_sms() * 4, 256, 0, st, cand.chunks.p, cand.dev_counts.p + 1, cand.jlist.p,
                                                          tR.nvalid.p, tS.nvalid.p, &ctr.p->pad[0]);
@@ -301,9 +308,10 @@ void run_join(const void* R, long long nR, const void* S, long long nS, int d, i
         EmitBuffers eb{acc.p, cap, band.p, bcap, ctr.p};
         ev.rec(2, st);
         if (screen == TJ_SCREEN_PLAIN) screen_plain(g, eb, st);
+        else if (i8) screen_i8(g, eb, (long long)eps2, st);
         else screen_tc(g, eb, st);
         ev.rec(3, st);
-        refine_band(g, eb, st);
+        if (!i8) refine_band(g, eb, st);   // the int8-limb screen is exact: no band
         ev.rec(4, st);
         TJ_CUDA(cudaMemcpyAsync(&h, ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, st));
         TJ_CUDA(cudaStreamSynchronize(st));
@@ -350,7 +358,7 @@ void run_join(const void* R, long long nR, const void* S, long long nS, int d, i
     res->count = nvalid;
     S_.result_pairs = nvalid;
     S_.ms_index = ev.ms(0, 1);
-    S_.ms_candidates = ev.ms(1, 2) > 0 ? ev.ms(1, 2) : 0.0;
+    S_.ms_candidates = ev.ms(1, 6);
     S_.ms_screen = ev.ms(2, 3);
     S_.ms_refine = ev.ms(3, 4);
     S_.ms_sort = ev.ms(4, 5);
@@ -367,7 +375,7 @@ int tj_join(const void* R, int64_t nR, const void* S, int64_t nS, int32_t d, int
     if (!out) fail(TJ_ERR_INVALID, "out is null");
     *out = nullptr;
     if (mode < 0 || mode > 2) fail(TJ_ERR_INVALID, "unknown mode");
-    if (screen < 0 || screen > 3) fail(TJ_ERR_INVALID, "unknown screen");
+    if (screen < 0 || screen > 5) fail(TJ_ERR_INVALID, "unknown screen");
     if (dtype != TJ_DTYPE_F32 && dtype != TJ_DTYPE_I16) fail(TJ_ERR_INVALID, "unknown dtype");
     if (opt && opt->flags != 0) fail(TJ_ERR_INVALID, "options.flags must be 0");
     std::unique_ptr<tj_result> res(new tj_result());
@@ -439,15 +447,16 @@ int tj_index_build(const void* X, int64_t n, int32_t d, int32_t dtype, double ep
     DBuf<Counters> ctr(1, st);
     launch(zero_counters, 1, 32, 0, st, ctr.p, 0);
     DBuf<FrameParams> fp(1, st);
+    DBuf<float> center((size_t)d, st);
     const void* srcs[1] = {X};
     const long long ns[1] = {n};
-    compute_frame(srcs, ns, 1, d, dtype, fp.p, st);
+    compute_frame(srcs, ns, 1, d, dtype, fp.p, center.p, st);
     Side& s = ix->side;
     s.src = X; s.dtype = dtype; s.n = n; s.d = d; s.screen = kScreenPlain;
-    prepare_side(s, fp.p, st, &ctr.p->status);
+    prepare_side(s, fp.p, center.p, st, &ctr.p->status);
     tile_stats(s, kTileR, ix->t128, st);
     tile_stats(s, kTileS, ix->t256, st);
-    const JoinParams jp = make_params(eps2, d, 64, n, n, true);
+    const JoinParams jp = make_params(eps2, d, 64, 0, n, n, true);
     build_candidates(ix->t128, ix->t256, jp.Tp, true, 64, ix->cand, st);
     // cells: runs of equal Morton keys, prefix-sum offsets
     DBuf<uint32_t> flag((size_t)n, st), pos((size_t)n, st), ncell(1, st);

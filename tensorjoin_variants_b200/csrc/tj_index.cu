@@ -75,46 +75,50 @@ __global__ void __launch_bounds__(256) dim_stats_partial(const void* src, int dt
     }
 }
 
-// Deterministic reduction of the partials, variance ranking and frame parameters.
-__global__ void frame_finish(const float* pmin, const float* pmax, const double* psum, const double* psq, int nparts,
-                             long long ntot, int d, FrameParams* fp, float* var_ws, float* lo_ws, float* hi_ws) {
-    for (int k = threadIdx.x; k < d; k += blockDim.x) {
-        float mn = INFINITY, mx = -INFINITY;
-        double s = 0.0, q = 0.0;
-        for (int b = 0; b < nparts; ++b) {
-            const size_t o = (size_t)b * d + k;
-            mn = fminf(mn, pmin[o]);
-            mx = fmaxf(mx, pmax[o]);
-            s += psum[o];
-            q += psq[o];
-        }
-        const double mean = ntot ? s / (double)ntot : 0.0;
-        var_ws[k] = ntot ? (float)fmax(0.0, q / (double)ntot - mean * mean) : 0.f;
-        lo_ws[k] = mn;
-        hi_ws[k] = mx;
+// Deterministic reduction of the partials (one thread per dimension, fixed block order):
+// variance, range and the centre (per-dimension mean, FP32) used to centre the MMA operands.
+__global__ void dim_reduce(const float* pmin, const float* pmax, const double* psum, const double* psq, int nparts,
+                           long long ntot, int d, float* var_ws, float* lo_ws, float* hi_ws, float* center) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d) return;
+    float mn = INFINITY, mx = -INFINITY;
+    double s = 0.0, q = 0.0;
+    for (int b = 0; b < nparts; ++b) {
+        const size_t o = (size_t)b * d + k;
+        mn = fminf(mn, pmin[o]);
+        mx = fmaxf(mx, pmax[o]);
+        s += psum[o];
+        q += psq[o];
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int m = min(d, 8);
-        FrameParams f;
-        f.m = m;
-        f.bits = 32 / m;
-        for (int t = 0; t < m; ++t) {
-            int best = -1;
-            for (int k = 0; k < d; ++k) {
-                bool used = false;
-                for (int u = 0; u < t; ++u) used |= (f.dims[u] == k);
-                if (used) continue;
-                if (best < 0 || var_ws[k] > var_ws[best]) best = k;
-            }
-            f.dims[t] = best;
-            const float lo = lo_ws[best], hi = hi_ws[best];
-            const float range = (isfinite(lo) && isfinite(hi) && hi > lo) ? hi - lo : 1.f;
-            f.lo[t] = isfinite(lo) ? lo : 0.f;
-            f.inv_w[t] = (float)(1u << f.bits) / range;
+    const double mean = ntot ? s / (double)ntot : 0.0;
+    var_ws[k] = ntot ? (float)fmax(0.0, q / (double)ntot - mean * mean) : 0.f;
+    lo_ws[k] = mn;
+    hi_ws[k] = mx;
+    center[k] = isfinite(mean) ? (float)mean : 0.f;
+}
+
+// Pick the m = min(d, 8) highest-variance dimensions and their quantisation frame.
+__global__ void frame_pick(int d, const float* var_ws, const float* lo_ws, const float* hi_ws, FrameParams* fp) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int m = min(d, 8);
+    FrameParams f;
+    f.m = m;
+    f.bits = 32 / m;
+    for (int t = 0; t < m; ++t) {
+        int best = -1;
+        for (int k = 0; k < d; ++k) {
+            bool used = false;
+            for (int u = 0; u < t; ++u) used |= (f.dims[u] == k);
+            if (used) continue;
+            if (best < 0 || var_ws[k] > var_ws[best]) best = k;
         }
-        *fp = f;
+        f.dims[t] = best;
+        const float lo = lo_ws[best], hi = hi_ws[best];
+        const float range = (isfinite(lo) && isfinite(hi) && hi > lo) ? hi - lo : 1.f;
+        f.lo[t] = isfinite(lo) ? lo : 0.f;
+        f.inv_w[t] = (float)(1u << f.bits) / range;
     }
+    *fp = f;
 }
 
 __global__ void morton_keys(const void* src, int dtype, long long n, int d, const FrameParams* fpp, uint64_t* keys,
@@ -137,19 +141,40 @@ __global__ void morton_keys(const void* src, int dtype, long long n, int d, cons
     vals[r] = (uint32_t)r;
 }
 
+// Round to the 16-bit operand format; returns the rounded value as FP32 and its bit pattern.
+template <int kFmt>   // 1 = bf16, 0 = fp16
+TJ_DEV float round16(float v, uint16_t& bits) {
+    if (kFmt == 1) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        bits = __bfloat16_as_ushort(h);
+        return __bfloat162float(h);
+    }
+    const __half h = __float2half_rn(v);
+    bits = __half_as_ushort(h);
+    return __half2float(h);
+}
+
 // One warp per sorted row: operand conversion and certificate metadata.
-template <int kScreen>
+//   plain:      FP32 copy in sorted order, ||x||^2.
+//   16-bit:     x' = x - c (c the per-dimension centre; distances are translation invariant),
+//               z_hi = round16(x'), and with kSplit also z_lo = round16(x' - z_hi); operand row
+//               [z_hi (kpad) | z_lo (kpad)].  Metadata: A = ||x'||^2 (FP64), Y >= ||x'||,
+//               Z >= ||z_hi + z_lo||, Zl >= ||z_lo||, E >= ||x' - z_hi - z_lo||.
+//   int8 limbs: q = 128 h + l for int14 input, exact integer ||q||^2.
+template <int kScreen, int kSplit>
 __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kpad, long long rows_pad,
-                          const uint32_t* perm, uint16_t* op, int8_t* op8, float* xs, double* nrm2, float* nrm2f,
-                          float* zn, float* en, float* yn, long long* inorm, unsigned long long* status) {
+                          const uint32_t* perm, const float* center, uint16_t* op, int8_t* op8, float* xs,
+                          double* nrm2, float* nrm2f, float* zn, float* en, float* yn, float* zl, long long* inorm,
+                          unsigned long long* status) {
     const long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     if (r >= rows_pad) return;
     const bool real = r < n;
     const size_t orig = real ? (size_t)perm[r] : 0;
-    double sx = 0.0, sz = 0.0, se = 0.0;
+    double sx = 0.0, sz = 0.0, se = 0.0, sl = 0.0;
     long long sq = 0;
     bool bad = false, fp16_range = false;
+    const int opw = kSplit ? 2 * kpad : kpad;
     for (int k = lane; k < kpad; k += 32) {
         float x = 0.f;
         if (real && k < d) x = load_x(src, dtype, orig * d + k);
@@ -157,33 +182,34 @@ __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kp
         if (kScreen == kScreenPlain) {
             if (k < d) xs[(size_t)r * d + k] = x;
             sx += (double)x * x;
-        } else if (kScreen == kScreenBF16 || kScreen == kScreenFP16) {
-            float z;
-            uint16_t bits;
-            if (kScreen == kScreenBF16) {
-                const __nv_bfloat16 h = __float2bfloat16_rn(x);
-                z = __bfloat162float(h);
-                bits = __bfloat16_as_ushort(h);
-            } else {
-                if (fabsf(x) > 65504.f) fp16_range = true;
-                const __half h = __float2half_rn(x);
-                z = __half2float(h);
-                bits = __half_as_ushort(h);
-            }
-            op[(size_t)r * kpad + k] = bits;
-            const double xd = x, zd = z, ed = xd - zd;   // exact in FP64
-            sx += xd * xd;
-            sz += zd * zd;
-            se += ed * ed;
-        } else {   // int8 limbs of an int14 value: q = 128 h + l, h = floor((q + 64) / 128)
+        } else if (kScreen == kScreenInt8Limb) {   // q = 128 h + l, h = floor((q + 64) / 128)
             const int q = (int)x;
             if (q < -8192 || q > 8191) bad = true;
-            const int h = (q + 64 + 8192) / 128 - 64;   // floor division for q + 64 >= -8128
+            const int h = (q + 64 + 8192) / 128 - 64;
             const int l = q - 128 * h;
             op8[(size_t)r * (2 * kpad) + k] = (int8_t)h;
             op8[(size_t)r * (2 * kpad) + kpad + k] = (int8_t)l;
             sq += (long long)q * q;
             sx += (double)x * x;
+        } else {
+            constexpr int kFmt = (kScreen == kScreenBF16 || kScreen == kScreenBF16X3) ? 1 : 0;
+            const double xc = (k < d && real) ? (double)x - (double)center[k] : 0.0;
+            const float xf = (float)xc;
+            if (kFmt == 0 && fabsf(xf) > 65504.f) fp16_range = true;
+            uint16_t bh = 0, bl = 0;
+            const float zh = round16<kFmt>(xf, bh);
+            double z = (double)zh;
+            if (kSplit) {
+                const float zlo = round16<kFmt>((float)(xc - (double)zh), bl);
+                z += (double)zlo;
+                sl += (double)zlo * zlo;
+                op[(size_t)r * opw + kpad + k] = bl;
+            }
+            op[(size_t)r * opw + k] = bh;
+            const double ed = xc - z;
+            sx += xc * xc;
+            sz += z * z;
+            se += ed * ed;
         }
     }
 #pragma unroll
@@ -191,6 +217,7 @@ __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kp
         sx += __shfl_xor_sync(0xffffffffu, sx, o);
         sz += __shfl_xor_sync(0xffffffffu, sz, o);
         se += __shfl_xor_sync(0xffffffffu, se, o);
+        sl += __shfl_xor_sync(0xffffffffu, sl, o);
         sq += __shfl_xor_sync(0xffffffffu, sq, o);
     }
     bad = __any_sync(0xffffffffu, bad);
@@ -199,14 +226,17 @@ __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kp
         if (bad && real) atomicOr(status, (unsigned long long)kStatusBadInput);
         if (fp16_range && real) atomicOr(status, (unsigned long long)kStatusFp16Range);
         if (real && sx > 0x1p100) atomicOr(status, (unsigned long long)kStatusBadInput);
-        // FP64 sums of d non-negative exactly-representable squares: relative error <= (d+2) 2^-53
-        const double g = (double)(d + 2) * 0x1p-53;
+        // FP64 sums of d non-negative squares (each rounded once): relative error <= (d+2) 2^-53;
+        // x - c may round once more (2^-53 relative), absorbed by the extra 2^-50 terms.
+        const double g = (double)(d + 4) * 0x1p-53;
         const double up = (1.0 + 2.0 * g) * (1.0 + 0x1p-50);
         nrm2[r] = sx;
         nrm2f[r] = __double2float_rn(sx);
-        yn[r] = f32_up(sqrt(sx * up) * (1.0 + 0x1p-50));
+        const double ynorm = sqrt(sx * up) * (1.0 + 0x1p-50);
+        yn[r] = f32_up(ynorm);
         zn[r] = f32_up(sqrt(sz * up) * (1.0 + 0x1p-50));
-        en[r] = f32_up(sqrt(se * up) * (1.0 + 0x1p-50));
+        en[r] = f32_up(sqrt(se * up) * (1.0 + 0x1p-50) + 0x1p-50 * ynorm);
+        zl[r] = f32_up(sqrt(sl * up) * (1.0 + 0x1p-50));
         if (inorm) inorm[r] = sq;
     }
 }
@@ -215,12 +245,12 @@ __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kp
 __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dtype, long long n, int d, int tile,
                                                          int ntiles, const uint32_t* perm, const double* nrm2,
                                                          const float* nrm2f, const float* zn, const float* en,
-                                                         const float* yn, float* ctrT, float* loT, float* hiT,
-                                                         float* rad, float* maxZ, float* maxE, float* maxY,
-                                                         float* maxB, float* beta, uint32_t* nvalid,
-                                                         uint32_t* row0) {
+                                                         const float* yn, const float* zl, float* ctrT, float* loT,
+                                                         float* hiT, float* rad, float* maxZ, float* maxE,
+                                                         float* maxY, float* maxB, float* beta, float* maxZl,
+                                                         uint32_t* nvalid, uint32_t* row0) {
     extern __shared__ float s_ctr[];   // [d]
-    __shared__ float red[5][256];
+    __shared__ float red[6][256];
     const int t = blockIdx.x;
     const long long r0 = (long long)t * tile;
     const int nv = (int)min((long long)tile, n - r0);
@@ -257,13 +287,14 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
         rmax = fmax(rmax, s);
     }
     // row-bound maxima
-    float mz = 0.f, me = 0.f, my = 0.f, mb = 0.f, mbeta = 0.f;
+    float mz = 0.f, me = 0.f, my = 0.f, mb = 0.f, mbeta = 0.f, mzl = 0.f;
     for (int i = threadIdx.x; i < nv; i += blockDim.x) {
         const long long r = r0 + i;
         mz = fmaxf(mz, zn[r]);
         me = fmaxf(me, en[r]);
         my = fmaxf(my, yn[r]);
         mb = fmaxf(mb, nrm2f[r]);
+        mzl = fmaxf(mzl, zl[r]);
         const double bt = fabs((double)nrm2f[r] - nrm2[r]) + 2.0 * g * nrm2[r];
         mbeta = fmaxf(mbeta, f32_up(bt * (1.0 + 0x1p-40)));
     }
@@ -272,12 +303,13 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
     red[2][threadIdx.x] = my;
     red[3][threadIdx.x] = mb;
     red[4][threadIdx.x] = mbeta;
+    red[5][threadIdx.x] = mzl;
     __shared__ double rr[8];
     if (lane == 0) rr[warp] = rmax;
     __syncthreads();
     for (int s = 128; s > 0; s >>= 1) {
         if (threadIdx.x < s)
-            for (int q = 0; q < 5; ++q) red[q][threadIdx.x] = fmaxf(red[q][threadIdx.x], red[q][threadIdx.x + s]);
+            for (int q = 0; q < 6; ++q) red[q][threadIdx.x] = fmaxf(red[q][threadIdx.x], red[q][threadIdx.x + s]);
         __syncthreads();
     }
     if (threadIdx.x == 0) {
@@ -290,6 +322,7 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
         maxY[t] = red[2][0];
         maxB[t] = red[3][0];
         beta[t] = red[4][0];
+        maxZl[t] = red[5][0];
         nvalid[t] = (uint32_t)max(nv, 0);
         row0[t] = (uint32_t)r0;
     }
@@ -435,7 +468,7 @@ __global__ void chunk_emit(const uint64_t* keys, size_t cap, const uint32_t* tot
 // ------------------------------------------------------------------ host entry points
 
 void compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d, int dtype, FrameParams* fp,
-                   cudaStream_t st) {
+                   float* center, cudaStream_t st) {
     long long ntot = 0;
     for (int s = 0; s < nsrc; ++s) ntot += ns[s];
     const int parts = nsrc * kStatBlocks;
@@ -447,14 +480,18 @@ void compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d
         launch(dim_stats_partial, nb, 256, 0, st, srcs[s], dtype, ns[s], d, pmin.p, pmax.p, psum.p, psq.p,
                                               s * kStatBlocks);
     }
-    launch(frame_finish, 1, 256, 0, st, pmin.p, pmax.p, psum.p, psq.p, parts, ntot, d, fp, ws.p, ws.p + d,
-                                    ws.p + 2 * d);
+    launch(dim_reduce, (unsigned)((d + 127) / 128), 128, 0, st, pmin.p, pmax.p, psum.p, psq.p, parts, ntot, d, ws.p,
+           ws.p + d, ws.p + 2 * d, center);
+    launch(frame_pick, 1, 32, 0, st, d, ws.p, ws.p + d, ws.p + 2 * d, fp);
     TJ_CUDA(cudaGetLastError());
 }
 
-void prepare_side(Side& s, const FrameParams* fpd, cudaStream_t st, unsigned long long* status) {
+void prepare_side(Side& s, const FrameParams* fpd, const float* center, cudaStream_t st,
+                  unsigned long long* status) {
     const long long n = s.n;
-    s.kpad = (s.screen == kScreenInt8Limb) ? ((s.d + 127) / 128) * 128 : ((s.d + kBK - 1) / kBK) * kBK;
+    const bool i8 = s.screen == kScreenInt8Limb;
+    s.split = (s.screen == kScreenBF16X3 || s.screen == kScreenFP16X3) ? 1 : 0;
+    s.kpad = i8 ? ((s.d + 127) / 128) * 128 : ((s.d + kBK - 1) / kBK) * kBK;
     s.rows_pad = ((std::max<long long>(n, 1) + kTileS - 1) / kTileS) * kTileS;
     s.perm = DBuf<uint32_t>((size_t)std::max<long long>(n, 1), st);
     s.keys = DBuf<uint64_t>((size_t)std::max<long long>(n, 1), st);
@@ -463,12 +500,12 @@ void prepare_side(Side& s, const FrameParams* fpd, cudaStream_t st, unsigned lon
         DBuf<uint32_t> vtmp((size_t)n, st);
         DBuf<uint32_t> ws(radix_workspace_elems((size_t)n), st);
         launch(morton_keys, (unsigned)((n + 255) / 256), 256, 0, st, s.src, s.dtype, n, s.d, fpd, s.keys.p, s.perm.p);
-        TJ_CUDA(cudaGetLastError());
         radix_sort(s.keys.p, s.perm.p, ktmp.p, vtmp.p, (size_t)n, 32, ws.p, st);
     }
     const size_t rp = (size_t)s.rows_pad;
-    if (s.screen == kScreenBF16 || s.screen == kScreenFP16) s.op = DBuf<uint16_t>(rp * s.kpad, st);
-    if (s.screen == kScreenInt8Limb) {
+    const bool f16 = !i8 && s.screen != kScreenPlain;
+    if (f16) s.op = DBuf<uint16_t>(rp * (size_t)s.kpad * (s.split ? 2 : 1), st);
+    if (i8) {
         s.op8 = DBuf<int8_t>(rp * 2 * s.kpad, st);
         s.inorm = DBuf<long long>(rp, st);
     }
@@ -478,18 +515,20 @@ void prepare_side(Side& s, const FrameParams* fpd, cudaStream_t st, unsigned lon
     s.zn = DBuf<float>(rp, st);
     s.en = DBuf<float>(rp, st);
     s.yn = DBuf<float>(rp, st);
+    s.zl = DBuf<float>(rp, st);
     const unsigned blocks = (unsigned)((rp * 32 + 255) / 256);
-#define TJ_PREP(SCR)                                                                                             \
-    launch(prep_rows<SCR>, blocks, 256, 0, st, s.src, s.dtype, n, s.d, s.kpad, s.rows_pad, s.perm.p, s.op.p, s.op8.p, \
-                                           s.xs.p, s.nrm2.p, s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.inorm.p, status)
+#define TJ_PREP(SCR, SPLIT)                                                                                        \
+    launch(prep_rows<SCR, SPLIT>, blocks, 256, 0, st, s.src, s.dtype, n, s.d, s.kpad, s.rows_pad, s.perm.p, center, \
+           s.op.p, s.op8.p, s.xs.p, s.nrm2.p, s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.zl.p, s.inorm.p, status)
     switch (s.screen) {
-        case kScreenPlain: TJ_PREP(kScreenPlain); break;
-        case kScreenBF16: TJ_PREP(kScreenBF16); break;
-        case kScreenFP16: TJ_PREP(kScreenFP16); break;
-        default: TJ_PREP(kScreenInt8Limb); break;
+        case kScreenPlain: TJ_PREP(kScreenPlain, 0); break;
+        case kScreenBF16: TJ_PREP(kScreenBF16, 0); break;
+        case kScreenFP16: TJ_PREP(kScreenFP16, 0); break;
+        case kScreenBF16X3: TJ_PREP(kScreenBF16X3, 1); break;
+        case kScreenFP16X3: TJ_PREP(kScreenFP16X3, 1); break;
+        default: TJ_PREP(kScreenInt8Limb, 0); break;
     }
 #undef TJ_PREP
-    TJ_CUDA(cudaGetLastError());
 }
 
 void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st) {
@@ -506,6 +545,7 @@ void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st) {
     ts.maxY = DBuf<float>(nt, st);
     ts.maxB = DBuf<float>(nt, st);
     ts.beta = DBuf<float>(nt, st);
+    ts.maxZl = DBuf<float>(nt, st);
     ts.nvalid = DBuf<uint32_t>(nt, st);
     ts.row0 = DBuf<uint32_t>(nt, st);
     if (ts.ntiles == 0) return;
@@ -513,9 +553,9 @@ void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st) {
     if (smem > 48 * 1024)
         TJ_CUDA(cudaFuncSetAttribute(tile_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     launch(tile_stats_kernel, ts.ntiles, 256, smem, st, s.src, s.dtype, s.n, s.d, tile, ts.ntiles, s.perm.p, s.nrm2.p,
-                                                    s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, ts.ctrT.p, ts.loT.p,
+                                                    s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.zl.p, ts.ctrT.p, ts.loT.p,
                                                     ts.hiT.p, ts.rad.p, ts.maxZ.p, ts.maxE.p, ts.maxY.p, ts.maxB.p,
-                                                    ts.beta.p, ts.nvalid.p, ts.row0.p);
+                                                    ts.beta.p, ts.maxZl.p, ts.nvalid.p, ts.row0.p);
     TJ_CUDA(cudaGetLastError());
 }
 

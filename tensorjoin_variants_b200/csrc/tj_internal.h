@@ -56,7 +56,7 @@ int radix_passes(int bits);
 // ------------------------------------------------------------------ enums (mirror include/tensorjoin.h)
 enum DType { kF32 = 0, kI16 = 1 };
 enum Mode { kModeRS = 0, kModeUpper = 1, kModeDirected = 2 };
-enum Screen { kScreenPlain = 0, kScreenBF16 = 1, kScreenFP16 = 2, kScreenInt8Limb = 3 };
+enum Screen { kScreenPlain = 0, kScreenBF16 = 1, kScreenFP16 = 2, kScreenInt8Limb = 3, kScreenBF16X3 = 4, kScreenFP16X3 = 5 };
 
 // ------------------------------------------------------------------ prepared side (tj_index.cu)
 // A side of the join in Morton order: permutation, MMA operand and per-row certificate metadata.
@@ -67,18 +67,20 @@ struct Side {
     long long n = 0;             // rows
     int d = 0;
     int screen = kScreenBF16;
-    int kpad = 0;                // operand row length in elements (multiple of 64)
+    int kpad = 0;                // operand row length in elements (multiple of 64; int8: 128)
+    int split = 0;               // 1: operand rows are [z_hi | z_lo] (2 * kpad elements)
     long long rows_pad = 0;      // operand rows (multiple of 256)
     DBuf<uint32_t> perm;         // [n] sorted position -> original row
     DBuf<uint64_t> keys;         // [n] Morton keys (sorted)
-    DBuf<uint16_t> op;           // [rows_pad, kpad] bf16 / fp16 operand (screen != plain)
+    DBuf<uint16_t> op;           // [rows_pad, kpad or 2*kpad] bf16 / fp16 operand of x - centre
     DBuf<int8_t> op8;            // [rows_pad, 2*kpad] int8 limbs [hi | lo] (int8 limb screen)
     DBuf<float> xs;              // [rows_pad, d] FP32 rows in sorted order (plain screen)
     DBuf<double> nrm2;           // [rows_pad] sequential FP64 sum of squares of x
     DBuf<float> nrm2f;           // [rows_pad] FP32 nearest of nrm2
     DBuf<float> zn;              // [rows_pad] upper bound of ||z|| (z = operand row)
     DBuf<float> en;              // [rows_pad] upper bound of ||x - z||
-    DBuf<float> yn;              // [rows_pad] upper bound of ||x||
+    DBuf<float> yn;              // [rows_pad] upper bound of ||x - centre||
+    DBuf<float> zl;              // [rows_pad] upper bound of ||z_lo|| (0 without the split)
     DBuf<long long> inorm;       // [rows_pad] exact integer squared norms (int path)
 };
 
@@ -90,7 +92,7 @@ struct TileSet {
     DBuf<float> ctrT;      // [d][ntiles] centroid (transposed for coalesced candidate tests)
     DBuf<float> loT, hiT;  // [d][ntiles] exact per-dimension min / max
     DBuf<float> rad;       // [ntiles] upper bound of max ||x - centroid||
-    DBuf<float> maxZ, maxE, maxY, maxB, beta;  // [ntiles] maxima of the row bounds
+    DBuf<float> maxZ, maxE, maxY, maxB, beta, maxZl;  // [ntiles] maxima of the row bounds
     DBuf<uint32_t> nvalid;  // [ntiles] rows of the tile that are real points
     DBuf<uint32_t> row0;    // [ntiles] first sorted row of the tile
 };
@@ -117,8 +119,9 @@ struct FrameParams {
 
 // side preparation
 void compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d, int dtype, FrameParams* fp,
-                   cudaStream_t st);
-void prepare_side(Side& s, const FrameParams* fp_dev, cudaStream_t st, unsigned long long* status);
+                   float* center, cudaStream_t st);
+void prepare_side(Side& s, const FrameParams* fp_dev, const float* center, cudaStream_t st,
+                  unsigned long long* status);
 void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st);
 void build_candidates(const TileSet& tr, const TileSet& ts, double T, bool self_join, int chunk_items,
                       Candidates& c, cudaStream_t st);
@@ -143,6 +146,7 @@ struct JoinGeometry {
 
 void screen_tc(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st);
 void screen_plain(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st);
+void screen_i8(const JoinGeometry& g, const EmitBuffers& eb, long long T, cudaStream_t st);
 void refine_band(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st);
 void expand_directed(const uint64_t* upper, unsigned long long n_upper_slots, uint64_t* out, long long N,
                      cudaStream_t st);

@@ -14,47 +14,12 @@
 // the same FP64 refinement of band pairs.  It plays the role of the reference's
 // GDS-Join FP64 grid join / FP32-first control (adapters/gds_g2a/kernel.cu:314-386,
 // g15_strong_control_20260905/src/fp32_first.py:104-157).
+#include "tj_emit.cuh"
 #include "tj_internal.h"
 
 namespace tj {
 
 namespace {
-
-constexpr unsigned kEmitChunkP = 256;
-
-struct Appender {
-    unsigned long long base = 0;
-    unsigned used = 0, size = 0;
-    unsigned long long valid = 0;
-    TJ_DEV unsigned long long reserve(unsigned t, unsigned long long* reserved, uint64_t* buf, unsigned long long cap) {
-        if (used + t > size) {
-            pad(buf, cap);
-            const unsigned want = t > kEmitChunkP ? t : kEmitChunkP;
-            unsigned long long b = 0;
-            if (lane_id() == 0) b = atomicAdd(reserved, (unsigned long long)want);
-            base = __shfl_sync(0xffffffffu, b, 0);
-            used = 0;
-            size = want;
-        }
-        const unsigned long long r = base + used;
-        used += t;
-        valid += t;
-        return r;
-    }
-    TJ_DEV void pad(uint64_t* buf, unsigned long long cap) {
-        for (unsigned k = used + lane_id(); k < size; k += 32)
-            if (base + k < cap) buf[base + k] = kSentinel;
-        used = size;
-    }
-};
-
-TJ_DEV uint64_t key_of(const JoinParams& jp, uint32_t oi, uint32_t oj) {
-    if (jp.self_join) {
-        const uint32_t lo = oi < oj ? oi : oj, hi = oi < oj ? oj : oi;
-        return jp.key_off + (uint64_t)lo * (uint64_t)jp.n_cols + hi;
-    }
-    return jp.key_off + (uint64_t)oi * (uint64_t)jp.n_cols + oj;
-}
 
 // ------------------------------------------------------------------ plain FP32 join
 constexpr int kPT = 256;                // threads: 16 x 16
@@ -88,7 +53,7 @@ __global__ void __launch_bounds__(kPT, 1) plain_kernel(const PlainArgs a) {
     __shared__ float sS[kPK][kTileS + 1];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const unsigned nchunks = *a.nchunks;
-    Appender app_acc, app_band;
+    WarpAppender app_acc, app_band;
     unsigned long long n_items = 0, n_screen_acc = 0;
     for (unsigned c = blockIdx.x; c < nchunks; c += gridDim.x) {
         const uint4 ch = a.chunks[c];
@@ -155,7 +120,7 @@ __global__ void __launch_bounds__(kPT, 1) plain_kernel(const PlainArgs a) {
                         const int b = __ffs(mk) - 1;
                         mk &= mk - 1;
                         const unsigned row = (g * 2 + (b >> 4)) * 16 + ty, col = (b & 15) * 16 + tx;
-                        if (pos < a.acc_cap) a.acc[pos] = key_of(a.jp, a.r_perm[r0 + row], a.s_perm[c0 + col]);
+                        if (pos < a.acc_cap) a.acc[pos] = pair_key(a.jp, a.r_perm[r0 + row], a.s_perm[c0 + col]);
                         ++pos;
                     }
                     n_screen_acc += __popc(amask);
@@ -167,7 +132,7 @@ __global__ void __launch_bounds__(kPT, 1) plain_kernel(const PlainArgs a) {
                         const int b = __ffs(mk) - 1;
                         mk &= mk - 1;
                         const unsigned row = (g * 2 + (b >> 4)) * 16 + ty, col = (b & 15) * 16 + tx;
-                        if (pos < a.band_cap) a.band[pos] = key_of(a.jp, a.r_perm[r0 + row], a.s_perm[c0 + col]);
+                        if (pos < a.band_cap) a.band[pos] = pair_key(a.jp, a.r_perm[r0 + row], a.s_perm[c0 + col]);
                         ++pos;
                     }
                 }

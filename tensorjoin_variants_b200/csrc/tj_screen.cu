@@ -29,21 +29,29 @@
 //   warps 2-5: epilogue, warp w reads TMEM lanes 32*(w%4) .. +31 (one R row per thread)
 #include <cstdio>
 
+#include "tj_emit.cuh"
 #include "tj_internal.h"
 
 namespace tj {
 
 namespace {
 
-constexpr int kStages = 4;
 constexpr int kAccBufs = 2;
 constexpr int kEpiWarps = 4;
 constexpr int kScreenThreads = (2 + kEpiWarps) * 32;
 constexpr unsigned kABytes = kTileR * 128;          // 16 KB
 constexpr unsigned kBBytes = kTileS * 128;          // 32 KB
-constexpr unsigned kStageBytes = kABytes + kBBytes;  // 48 KB
-constexpr unsigned kEmitChunk = 256;
+// Stage = one 64-element k-block of A (128 rows) and B (256 rows); with the hi/lo split the
+// stage holds both limbs of both operands: [A_hi | A_lo | B_hi | B_lo].
+template <int kSplit> struct StageCfg {
+    static constexpr unsigned kBytes = (kSplit ? 2u : 1u) * (kABytes + kBBytes);   // 48 or 96 KB
+    static constexpr int kStages = kSplit ? 2 : 4;
+    static constexpr unsigned kAlo = kABytes;                    // offsets inside a split stage
+    static constexpr unsigned kBhi = kSplit ? 2u * kABytes : kABytes;
+    static constexpr unsigned kBlo = 2u * kABytes + kBBytes;
+};
 
+template <int kStages>
 struct ScreenCtl {
     uint64_t full[kStages];
     uint64_t empty[kStages];
@@ -56,7 +64,11 @@ struct ScreenCtl {
     float bt[2][kTileS];
 };
 
-constexpr size_t kScreenSmem = 1024 + (size_t)kStages * kStageBytes + sizeof(ScreenCtl);
+template <int kSplit>
+constexpr size_t screen_smem() {
+    return 1024 + (size_t)StageCfg<kSplit>::kStages * StageCfg<kSplit>::kBytes +
+           sizeof(ScreenCtl<StageCfg<kSplit>::kStages>);
+}
 
 struct ScreenArgs {
     const uint4* chunks;
@@ -69,6 +81,7 @@ struct ScreenArgs {
     const double* r_nrm2;
     const float* r_zn;
     const float* r_en;
+    const float* r_zl;
     // S side (columns of tile J)
     const uint32_t* s_row0;
     const uint32_t* s_nvalid;
@@ -78,12 +91,15 @@ struct ScreenArgs {
     const float* s_zn;
     const float* s_en;
     const float* s_yn;
+    const float* s_zl;
+    const float* sJ_maxZl;
     const float* sJ_maxZ;
     const float* sJ_maxE;
     const float* sJ_maxY;
     const float* sJ_maxB;
     const float* sJ_beta;
     int kblocks;
+    int kpad;
     unsigned idesc;
     JoinParams jp;
     uint64_t* acc;
@@ -93,52 +109,16 @@ struct ScreenArgs {
     Counters* ctr;
 };
 
-// Warp-level append into a per-warp reserved chunk of a global buffer.
-struct WarpAppender {
-    unsigned long long base = 0;
-    unsigned used = 0, size = 0;   // size == 0: no chunk yet
-    unsigned long long valid = 0;
-
-    // Reserve `t` (warp total) slots; returns the first slot for this warp's batch.
-    TJ_DEV unsigned long long reserve(unsigned t, unsigned long long* reserved, uint64_t* buf,
-                                      unsigned long long cap) {
-        const unsigned lane = lane_id();
-        if (used + t > size) {
-            pad(buf, cap);
-            const unsigned want = t > kEmitChunk ? t : kEmitChunk;
-            unsigned long long b = 0;
-            if (lane == 0) b = atomicAdd(reserved, (unsigned long long)want);
-            base = __shfl_sync(0xffffffffu, b, 0);
-            used = 0;
-            size = want;
-        }
-        const unsigned long long r = base + used;
-        used += t;
-        valid += t;
-        return r;
-    }
-    TJ_DEV void pad(uint64_t* buf, unsigned long long cap) {
-        for (unsigned k = used + lane_id(); k < size; k += 32)
-            if (base + k < cap) buf[base + k] = kSentinel;
-        used = size;
-    }
-};
-
-TJ_DEV uint64_t pair_key(const JoinParams& jp, uint32_t oi, uint32_t oj) {
-    if (jp.self_join) {
-        const uint32_t lo = oi < oj ? oi : oj, hi = oi < oj ? oj : oi;
-        return jp.key_off + (uint64_t)lo * (uint64_t)jp.n_cols + hi;
-    }
-    return jp.key_off + (uint64_t)oi * (uint64_t)jp.n_cols + oj;
-}
-
-template <int kFmt>   // 0 = fp16, 1 = bf16
+template <int kFmt, int kSplit>   // kFmt: 0 = fp16, 1 = bf16; kSplit: hi/lo operand limbs
 __global__ void __launch_bounds__(kScreenThreads, 1)
     screen_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      const ScreenArgs a) {
+    using Cfg = StageCfg<kSplit>;
+    constexpr int kStages = Cfg::kStages;
+    constexpr unsigned kStageBytes = Cfg::kBytes;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    ScreenCtl* ctl = (ScreenCtl*)(smem + (size_t)kStages * kStageBytes);
+    ScreenCtl<kStages>* ctl = (ScreenCtl<kStages>*)(smem + (size_t)kStages * kStageBytes);
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long* status = &a.ctr->status;
 
@@ -176,11 +156,15 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     const int srow = (int)a.s_row0[a.jlist[e]];
                     for (int kb = 0; kb < a.kblocks; ++kb) {
                         if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status)) { ok = false; break; }
-                        if (ctl->abort_flag) { ok = false; break; }
+                        if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         uint8_t* sa = smem + (size_t)stage * kStageBytes;
                         mbar_arrive_expect_tx(&ctl->full[stage], kStageBytes);
                         tma_load_2d(sa, &tmA, &ctl->full[stage], kb * kBK, rrow);
-                        tma_load_2d(sa + kABytes, &tmB, &ctl->full[stage], kb * kBK, srow);
+                        tma_load_2d(sa + Cfg::kBhi, &tmB, &ctl->full[stage], kb * kBK, srow);
+                        if (kSplit) {
+                            tma_load_2d(sa + Cfg::kAlo, &tmA, &ctl->full[stage], a.kpad + kb * kBK, rrow);
+                            tma_load_2d(sa + Cfg::kBlo, &tmB, &ctl->full[stage], a.kpad + kb * kBK, srow);
+                        }
                         if (++stage == kStages) { stage = 0; phase ^= 1; }
                     }
                 }
@@ -207,14 +191,18 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     const unsigned d_tmem = tmem + acc * kTileS;
                     for (int kb = 0; kb < a.kblocks; ++kb) {
                         if (!mbar_wait(&ctl->full[stage], phase, status)) { ok = false; break; }
-                        if (ctl->abort_flag) { ok = false; break; }
+                        if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         tc_fence_after();
                         const uint8_t* sa = smem + (size_t)stage * kStageBytes;
 #pragma unroll
                         for (int k = 0; k < kBK / 16; ++k) {
                             const uint64_t ad = desc_sw128(sa, k * 32);
-                            const uint64_t bd = desc_sw128(sa + kABytes, k * 32);
+                            const uint64_t bd = desc_sw128(sa + Cfg::kBhi, k * 32);
                             umma_f16(d_tmem, ad, bd, a.idesc, (kb | k) != 0 ? 1u : 0u);
+                            if (kSplit) {   // z.w ~ hi.hi + hi.lo + lo.hi, one FP32 accumulator
+                                umma_f16(d_tmem, ad, desc_sw128(sa + Cfg::kBlo, k * 32), a.idesc, 1u);
+                                umma_f16(d_tmem, desc_sw128(sa + Cfg::kAlo, k * 32), bd, a.idesc, 1u);
+                            }
                         }
                         umma_commit(&ctl->empty[stage]);
                         if (++stage == kStages) { stage = 0; phase ^= 1; }
@@ -247,6 +235,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             const double Ai = rvalid ? a.r_nrm2[rs] : 0.0;
             const double Zi = rvalid ? (double)a.r_zn[rs] : 0.0;
             const double Ei = rvalid ? (double)a.r_en[rs] : 0.0;
+            const double Zli = rvalid ? (double)a.r_zl[rs] : 0.0;
             for (unsigned e = ch.y; e < ch.z; ++e) {
                 const unsigned J = a.jlist[e];
                 const unsigned c0 = a.s_row0[J];
@@ -261,8 +250,8 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 float tau = -INFINITY;
                 if (rvalid) {
                     const double WJ = a.sJ_maxZ[J], FJ = a.sJ_maxE[J], YJ = a.sJ_maxY[J];
-                    const double BJ = a.sJ_maxB[J], betaJ = a.sJ_beta[J];
-                    const double RiJ = jp.gmma * Zi * WJ + jp.cabs + Ei * YJ + Zi * FJ;
+                    const double BJ = a.sJ_maxB[J], betaJ = a.sJ_beta[J], WlJ = a.sJ_maxZl[J];
+                    const double RiJ = jp.gmma * Zi * WJ + jp.cabs + Ei * YJ + Zi * FJ + Zli * WlJ;
                     const double PiJ = Zi * WJ * (1.0 + jp.gmma) + jp.cabs;
                     double t = jp.Tp - Ai + jp.gn * Ai + 0x1p-23 * (BJ + 2.0 * PiJ) + betaJ + 2.0 * RiJ;
                     t = t + fabs(t) * 0x1p-30 + 0x1p-1000;
@@ -302,7 +291,8 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                                 const double Bj = a.s_nrm2[cs];
                                 const double Wj = a.s_zn[cs], Fj = a.s_en[cs], Yj = a.s_yn[cs];
                                 const double s = Ai + Bj - 2.0 * p;
-                                const double R = jp.gmma * Zi * Wj + jp.cabs + Ei * Yj + Zi * Fj;
+                                const double R = jp.gmma * Zi * Wj + jp.cabs + Ei * Yj + Zi * Fj +
+                                                 Zli * (double)a.s_zl[cs];
                                 double m = 2.0 * R + jp.gn * (Ai + Bj) + 0x1p-50 * (Ai + Bj + 2.0 * fabs(p));
                                 m = m * (1.0 + 0x1p-40) + 0x1p-1000;
                                 if (s + m <= jp.Tm) amask |= 1u << k;
@@ -404,14 +394,15 @@ void make_tmap_2d(CUtensorMap* m, const void* base, long long rows, long long co
 void screen_tc(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st) {
     const Side& R = *g.R;
     const Side& S = *g.S;
-    if (R.screen != S.screen || (R.screen != kScreenBF16 && R.screen != kScreenFP16))
-        fail(-1, "screen_tc needs bf16 or fp16 operands on both sides");
-    if (R.kpad != S.kpad) fail(-1, "operand widths differ");
+    const bool bf = R.screen == kScreenBF16 || R.screen == kScreenBF16X3;
+    const bool ok = R.screen == S.screen && (bf || R.screen == kScreenFP16 || R.screen == kScreenFP16X3);
+    if (!ok) fail(-1, "screen_tc needs matching bf16 / fp16 operands on both sides");
+    if (R.kpad != S.kpad || R.split != S.split) fail(-1, "operand layouts differ");
     CUtensorMap tmA, tmB;
-    const CUtensorMapDataType dt =
-        R.screen == kScreenBF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
-    make_tmap_2d(&tmA, R.op.p, R.rows_pad, R.kpad, 2, kTileR, dt);
-    make_tmap_2d(&tmB, S.op.p, S.rows_pad, S.kpad, 2, kTileS, dt);
+    const CUtensorMapDataType dt = bf ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    const long long w = (long long)R.kpad * (R.split ? 2 : 1);
+    make_tmap_2d(&tmA, R.op.p, R.rows_pad, w, 2, kTileR, dt);
+    make_tmap_2d(&tmB, S.op.p, S.rows_pad, w, 2, kTileS, dt);
     ScreenArgs a;
     a.chunks = g.cand->chunks.p;
     a.nchunks = g.cand->dev_counts.p + 1;
@@ -422,6 +413,7 @@ void screen_tc(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st) {
     a.r_nrm2 = R.nrm2.p;
     a.r_zn = R.zn.p;
     a.r_en = R.en.p;
+    a.r_zl = R.zl.p;
     a.s_row0 = g.tS->row0.p;
     a.s_nvalid = g.tS->nvalid.p;
     a.s_perm = S.perm.p;
@@ -430,14 +422,16 @@ void screen_tc(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st) {
     a.s_zn = S.zn.p;
     a.s_en = S.en.p;
     a.s_yn = S.yn.p;
+    a.s_zl = S.zl.p;
+    a.sJ_maxZl = g.tS->maxZl.p;
     a.sJ_maxZ = g.tS->maxZ.p;
     a.sJ_maxE = g.tS->maxE.p;
     a.sJ_maxY = g.tS->maxY.p;
     a.sJ_maxB = g.tS->maxB.p;
     a.sJ_beta = g.tS->beta.p;
     a.kblocks = R.kpad / kBK;
-    const unsigned fmt = R.screen == kScreenBF16 ? 1u : 0u;
-    a.idesc = make_idesc(1u, fmt, kTileR, kTileS);
+    a.kpad = R.kpad;
+    a.idesc = make_idesc(1u, bf ? 1u : 0u, kTileR, kTileS);
     a.jp = g.jp;
     a.acc = eb.acc;
     a.acc_cap = eb.acc_cap;
@@ -445,16 +439,17 @@ void screen_tc(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st) {
     a.band_cap = eb.band_cap;
     a.ctr = eb.ctr;
     const int grid = num_sms();
-    if (fmt == 1) {
-        TJ_CUDA(cudaFuncSetAttribute(screen_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kScreenSmem));
-        launch(screen_tc_kernel<1>, grid, kScreenThreads, kScreenSmem, st, tmA, tmB, a);
-    } else {
-        TJ_CUDA(cudaFuncSetAttribute(screen_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kScreenSmem));
-        launch(screen_tc_kernel<0>, grid, kScreenThreads, kScreenSmem, st, tmA, tmB, a);
-    }
-    TJ_CUDA(cudaGetLastError());
+#define TJ_SCREEN(F, SP)                                                                                    \
+    do {                                                                                                    \
+        TJ_CUDA(cudaFuncSetAttribute(screen_tc_kernel<F, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     (int)screen_smem<SP>()));                                              \
+        launch(screen_tc_kernel<F, SP>, grid, kScreenThreads, screen_smem<SP>(), st, tmA, tmB, a);          \
+    } while (0)
+    if (bf && R.split) TJ_SCREEN(1, 1);
+    else if (bf) TJ_SCREEN(1, 0);
+    else if (R.split) TJ_SCREEN(0, 1);
+    else TJ_SCREEN(0, 0);
+#undef TJ_SCREEN
 }
 
 }  // namespace tj

@@ -1,0 +1,326 @@
+// Exact int14 screen on the tensor cores (tcgen05 kind::i8, sm_100a).
+//
+// Every int14 coordinate q in [-8192, 8191] is split into two signed int8 limbs
+// q = 128 h + l, h = floor((q + 64) / 128) in [-64, 64], l in [-64, 63].  For a tile
+// pair the kernel accumulates, exactly in INT32 TMEM accumulators,
+//     hh = sum h h',   x = sum (h l' + l h'),   ll = sum l l'
+// (|hh|, |ll| <= 4096 d, |x| <= 8192 d: no INT32 overflow for any order) and
+// recombines q.q' = 16384 hh + 128 x + ll in INT64, so d2 = |q|^2 + |q'|^2 - 2 q.q'
+// and the predicate d2 <= T are exact: there is no band and no refinement.
+// This is the reference's limb decomposition and exact recombination
+// (src/g9_tc_kernels.py:45-66 limb_dot; NUMERICS_G9_INT14.md:5-18), applied to the
+// whole screen instead of a refinement subset.
+//
+// Fast path: q.q' <= 16384 hh + M with M = 128 max|x| + max|ll| = d (128 * 8192 + 4096),
+// so a pair is certainly out when 32768 hh + 2M < |q|^2 + |q'|^2 - T.  With
+// a_i = floor((|q_i|^2 - T - 2M) / 2^15) and b_j = floor(|q_j|^2 / 2^15) this becomes the
+// integer test  hh - b_j < a_i  (two INT32 ops per pair).  Pairs failing it read x and ll
+// and take the exact INT64 test.
+//
+// TMEM: hh double-buffered (columns 0..255), x and ll single (256..511).  The UMMA
+// issuer runs the hh products of item n+1 while the epilogue still reads x / ll of item n.
+// Warp roles (320 threads): warp 0 TMA producer, warp 1 UMMA issuer, warps 2..9 epilogue
+// (warp w reads TMEM lanes 32*(w%4).. and columns 64*((w-2)/4)..).
+#include "tj_emit.cuh"
+#include "tj_internal.h"
+
+namespace tj {
+
+namespace {
+
+constexpr int kI8Stages = 3;
+constexpr int kI8Epi = 8;
+constexpr int kI8Threads = (2 + kI8Epi) * 32;
+constexpr int kI8N = 128;                        // S tile rows (UMMA N)
+constexpr unsigned kPart = 128u * 128u;          // one 128-row x 128-byte swizzled box (16 KB)
+constexpr unsigned kI8Stage = 4 * kPart;         // A_h, A_l, B_h, B_l
+constexpr unsigned kColHH0 = 0, kColX = 256, kColLL = 384;
+
+struct I8Ctl {
+    uint64_t full[kI8Stages];
+    uint64_t empty[kI8Stages];
+    uint64_t acc_full[2];
+    uint64_t hh_empty[2];
+    uint64_t xl_empty;
+    uint64_t drain;
+    unsigned tmem_base;
+    int abort_flag;
+    int acc_ok[2];
+    int bq[2][kI8N];       // floor(|q_j|^2 / 2^15), or a huge value for padding columns
+};
+
+constexpr size_t kI8Smem = 1024 + (size_t)kI8Stages * kI8Stage + sizeof(I8Ctl);
+
+struct I8Args {
+    const uint4* chunks;
+    const uint32_t* nchunks;
+    const uint32_t* jlist;
+    const uint32_t* r_row0;
+    const uint32_t* r_nvalid;
+    const uint32_t* r_perm;
+    const long long* r_norm;   // exact |q|^2
+    const uint32_t* s_row0;
+    const uint32_t* s_nvalid;
+    const uint32_t* s_perm;
+    const long long* s_norm;
+    int kblocks;               // kpad / 128
+    int kpad;
+    unsigned idesc;
+    long long T;               // integer threshold
+    long long twoM;            // 2 * bound on |128 x + ll|
+    JoinParams jp;
+    uint64_t* acc;
+    unsigned long long acc_cap;
+    Counters* ctr;
+};
+
+TJ_DEV int floor_shift15(long long v) { return (int)(v >> 15); }   // arithmetic shift = floor division
+
+__global__ void __launch_bounds__(kI8Threads, 1)
+    screen_i8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                     const I8Args a) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    I8Ctl* ctl = (I8Ctl*)(smem + (size_t)kI8Stages * kI8Stage);
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned long long* status = &a.ctr->status;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kI8Stages; ++s) {
+            mbar_init(&ctl->full[s], 1);
+            mbar_init(&ctl->empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&ctl->acc_full[b], 1);
+            mbar_init(&ctl->hh_empty[b], kI8Epi);
+        }
+        mbar_init(&ctl->xl_empty, kI8Epi);
+        mbar_init(&ctl->drain, 1);
+        ctl->abort_flag = 0;
+        fence_barrier_init();
+        prefetch_tmap(&tmA);
+        prefetch_tmap(&tmB);
+    }
+    if (warp == 1) tmem_alloc(&ctl->tmem_base, 512);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = ctl->tmem_base;
+    const unsigned nchunks = *a.nchunks;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            unsigned stage = 0, phase = 0;
+            bool ok = true;
+            for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
+                const uint4 ch = a.chunks[c];
+                const int rrow = (int)a.r_row0[ch.x];
+                for (unsigned e = ch.y; e < ch.z && ok; ++e) {
+                    const int srow = (int)a.s_row0[a.jlist[e]];
+                    for (int kb = 0; kb < a.kblocks; ++kb) {
+                        if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status)) { ok = false; break; }
+                        if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
+                        uint8_t* st = smem + (size_t)stage * kI8Stage;
+                        mbar_arrive_expect_tx(&ctl->full[stage], kI8Stage);
+                        tma_load_2d(st, &tmA, &ctl->full[stage], kb * 128, rrow);
+                        tma_load_2d(st + kPart, &tmA, &ctl->full[stage], a.kpad + kb * 128, rrow);
+                        tma_load_2d(st + 2 * kPart, &tmB, &ctl->full[stage], kb * 128, srow);
+                        tma_load_2d(st + 3 * kPart, &tmB, &ctl->full[stage], a.kpad + kb * 128, srow);
+                        if (++stage == kI8Stages) { stage = 0; phase ^= 1; }
+                    }
+                }
+            }
+            if (!ok) ctl->abort_flag = 1;
+            for (int s = 0; s < kI8Stages; ++s) {
+                const unsigned ph = ((unsigned)s < stage) ? phase : (phase ^ 1u);
+                mbar_wait(&ctl->full[s], ph, status, 1000000000ull);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            unsigned stage = 0, phase = 0;
+            unsigned long long n = 0;   // item counter of this CTA
+            bool ok = true;
+            for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
+                const uint4 ch = a.chunks[c];
+                for (unsigned e = ch.y; e < ch.z && ok; ++e, ++n) {
+                    const unsigned b = (unsigned)(n & 1);
+                    const unsigned use = (unsigned)((n >> 1) & 1);   // parity of this buffer's use
+                    if (!mbar_wait(&ctl->hh_empty[b], use ^ 1, status)) { ok = false; break; }
+                    tc_fence_after();
+                    const unsigned t_hh = tmem + kColHH0 + b * 128, t_x = tmem + kColX, t_ll = tmem + kColLL;
+                    for (int kb = 0; kb < a.kblocks; ++kb) {
+                        if (!mbar_wait(&ctl->full[stage], phase, status)) { ok = false; break; }
+                        if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
+                        tc_fence_after();
+                        const uint8_t* st = smem + (size_t)stage * kI8Stage;
+                        const uint8_t *Ah = st, *Al = st + kPart, *Bh = st + 2 * kPart, *Bl = st + 3 * kPart;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            umma_i8(t_hh, desc_sw128(Ah, k * 32), desc_sw128(Bh, k * 32), a.idesc, (kb | k) != 0);
+                        if (kb == 0) {   // x / ll of the previous item must have been read
+                            if (!mbar_wait(&ctl->xl_empty, (unsigned)(n & 1) ^ 1u, status)) { ok = false; break; }
+                            tc_fence_after();
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            umma_i8(t_x, desc_sw128(Ah, k * 32), desc_sw128(Bl, k * 32), a.idesc, (kb | k) != 0);
+                            umma_i8(t_x, desc_sw128(Al, k * 32), desc_sw128(Bh, k * 32), a.idesc, 1u);
+                            umma_i8(t_ll, desc_sw128(Al, k * 32), desc_sw128(Bl, k * 32), a.idesc, (kb | k) != 0);
+                        }
+                        umma_commit(&ctl->empty[stage]);
+                        if (++stage == kI8Stages) { stage = 0; phase ^= 1; }
+                    }
+                    if (!ok) break;
+                    umma_commit(&ctl->acc_full[b]);
+                }
+            }
+            if (!ok) ctl->abort_flag = 1;
+            umma_commit(&ctl->drain);
+            mbar_wait(&ctl->drain, 0, status, 1000000000ull);
+        }
+    } else {
+        const unsigned ew = warp - 2;                 // 0..7
+        const unsigned q = warp & 3;                  // TMEM lane quarter
+        const unsigned half = ew >> 2;                // column half (0: 0..63, 1: 64..127)
+        const unsigned et = threadIdx.x - 64;         // 0..255
+        const unsigned row = q * 32 + lane;
+        const JoinParams& jp = a.jp;
+        WarpAppender app;
+        unsigned long long n = 0, n_acc = 0, n_rare = 0, n_items = 0;
+        bool ok = true;
+        for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
+            const uint4 ch = a.chunks[c];
+            const unsigned I = ch.x;
+            const unsigned r0 = a.r_row0[I];
+            const bool rvalid = row < a.r_nvalid[I];
+            const unsigned rs = r0 + row;
+            const long long Ai = rvalid ? a.r_norm[rs] : 0;
+            const int ai = rvalid ? floor_shift15(Ai - a.T - a.twoM) : 0x7FFFFFFF;
+            for (unsigned e = ch.y; e < ch.z; ++e, ++n) {
+                const unsigned b = (unsigned)(n & 1), par = b;
+                const unsigned J = a.jlist[e];
+                const unsigned c0 = a.s_row0[J];
+                const unsigned nvJ = a.s_nvalid[J];
+                if (et < (unsigned)kI8N)
+                    ctl->bq[par][et] = et < nvJ ? floor_shift15(a.s_norm[c0 + et]) : 0x40000000;
+                if (et == 0)
+                    ctl->acc_ok[par] = mbar_wait(&ctl->acc_full[b], (unsigned)((n >> 1) & 1), status) ? 1 : 0;
+                asm volatile("bar.sync 1, 256;" ::: "memory");
+                if (!ctl->acc_ok[par]) { ok = false; break; }
+                tc_fence_after();
+                const int* bq = ctl->bq[par];
+                const unsigned lane_off = (q * 32u) << 16;
+#pragma unroll 1
+                for (int cb = 0; cb < 2; ++cb) {
+                    const unsigned col0 = half * 64 + cb * 32;
+                    uint32_t hh[32];
+                    tmem_ld32(tmem + lane_off + kColHH0 + b * 128 + col0, hh);
+                    tmem_ld_wait();
+                    int mx = -0x7FFFFFFF;
+#pragma unroll
+                    for (int k = 0; k < 32; ++k) mx = max(mx, (int)hh[k] - bq[col0 + k]);
+                    const bool cand = mx >= ai;
+                    if (!__any_sync(0xffffffffu, cand)) continue;
+                    uint32_t xv[32], lv[32];
+                    tmem_ld32(tmem + lane_off + kColX + col0, xv);
+                    tmem_ld32(tmem + lane_off + kColLL + col0, lv);
+                    tmem_ld_wait();
+                    uint32_t amask = 0;
+                    if (cand) {
+#pragma unroll
+                        for (int k = 0; k < 32; ++k) {
+                            if ((int)hh[k] - bq[col0 + k] < ai) continue;
+                            const unsigned cs = c0 + col0 + k;
+                            if (col0 + k >= nvJ) continue;
+                            if (jp.self_join && cs <= rs) continue;
+                            ++n_rare;
+                            const long long dot = (long long)(int)hh[k] * 16384ll + (long long)(int)xv[k] * 128ll +
+                                                  (long long)(int)lv[k];
+                            const long long d2 = Ai + a.s_norm[cs] - 2 * dot;
+                            if (d2 <= a.T) amask |= 1u << k;
+                        }
+                    }
+                    unsigned ta;
+                    const unsigned pa = warp_excl_scan(__popc(amask), ta);
+                    if (ta) {
+                        unsigned long long pos = app.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap) + pa;
+                        uint32_t mk = amask;
+                        while (mk) {
+                            const int k = __ffs(mk) - 1;
+                            mk &= mk - 1;
+                            const unsigned cs = c0 + col0 + k;
+                            if (pos < a.acc_cap) a.acc[pos] = pair_key(jp, a.r_perm[rs], a.s_perm[cs]);
+                            ++pos;
+                        }
+                        n_acc += __popc(amask);
+                    }
+                }
+                // this item's hh buffer and the shared x / ll are free again
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&ctl->hh_empty[b]);
+                    mbar_arrive(&ctl->xl_empty);
+                }
+                ++n_items;
+            }
+        }
+        if (!ok) ctl->abort_flag = 1;
+        app.pad(a.acc, a.acc_cap);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            n_acc += __shfl_xor_sync(0xffffffffu, n_acc, o);
+            n_rare += __shfl_xor_sync(0xffffffffu, n_rare, o);
+        }
+        if (lane == 0) {
+            if (app.valid) atomicAdd(&a.ctr->acc_valid, app.valid);
+            if (n_acc) atomicAdd(&a.ctr->screen_accept, n_acc);
+            if (n_rare) atomicAdd(&a.ctr->rare_checks, n_rare);
+            if (ew == 0 && n_items) atomicAdd(&a.ctr->items, n_items);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem, 512);
+}
+
+}  // namespace
+
+void make_tmap_2d(CUtensorMap* m, const void* base, long long rows, long long cols, int esize, int box_rows,
+                  CUtensorMapDataType dt);
+
+void screen_i8(const JoinGeometry& g, const EmitBuffers& eb, long long T, cudaStream_t st) {
+    const Side& R = *g.R;
+    const Side& S = *g.S;
+    if (R.screen != kScreenInt8Limb || S.screen != kScreenInt8Limb) fail(-1, "screen_i8 needs int8-limb sides");
+    CUtensorMap tmA, tmB;
+    make_tmap_2d(&tmA, R.op8.p, R.rows_pad, 2 * (long long)R.kpad, 1, 128, CU_TENSOR_MAP_DATA_TYPE_UINT8);
+    make_tmap_2d(&tmB, S.op8.p, S.rows_pad, 2 * (long long)S.kpad, 1, kI8N, CU_TENSOR_MAP_DATA_TYPE_UINT8);
+    I8Args a;
+    a.chunks = g.cand->chunks.p;
+    a.nchunks = g.cand->dev_counts.p + 1;
+    a.jlist = g.cand->jlist.p;
+    a.r_row0 = g.tR->row0.p;
+    a.r_nvalid = g.tR->nvalid.p;
+    a.r_perm = R.perm.p;
+    a.r_norm = R.inorm.p;
+    a.s_row0 = g.tS->row0.p;
+    a.s_nvalid = g.tS->nvalid.p;
+    a.s_perm = S.perm.p;
+    a.s_norm = S.inorm.p;
+    a.kblocks = R.kpad / 128;
+    a.kpad = R.kpad;
+    a.idesc = make_idesc(2u, 1u, 128, kI8N);
+    a.T = T;
+    a.twoM = 2ll * (long long)R.kpad * (128ll * 8192ll + 4096ll);
+    a.jp = g.jp;
+    a.acc = eb.acc;
+    a.acc_cap = eb.acc_cap;
+    a.ctr = eb.ctr;
+    TJ_CUDA(cudaFuncSetAttribute(screen_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kI8Smem));
+    launch(screen_i8_kernel, num_sms(), kI8Threads, kI8Smem, st, tmA, tmB, a);
+}
+
+}  // namespace tj

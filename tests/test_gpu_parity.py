@@ -19,7 +19,7 @@ from tensorjoin_variants_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
 G = json.loads((GOLDEN / "golden.json").read_text())
-FLOAT_SCREENS = ["plain", "bf16", "fp16"]
+FLOAT_SCREENS = ["plain", "bf16", "fp16", "bf16x3", "fp16x3"]
 
 
 def sha(a):
@@ -75,9 +75,11 @@ def test_mixture_rs_small(screen):
     k, st = gpu_keys(w.R, w.S, w.T, "rs", screen)
     assert_same(k, oracle_keys(w.R, w.S, w.T, "rs"), screen)
     assert st["pairs_screened"] <= w.candidate_pairs_all
+    if screen == "bf16x3":   # centred hi/lo operands keep the certified band narrow on clustered data
+        assert st["band"] <= 0.01 * st["pairs_screened"]
 
 
-@pytest.mark.parametrize("screen", ["fp16", "bf16", "plain"])
+@pytest.mark.parametrize("screen", FLOAT_SCREENS)
 def test_factor512_small(screen):
     w = W.factor512(n=3000, samples=1 << 16)
     k, st = gpu_keys(w.R, w.S, w.T, "rs", screen)
@@ -152,16 +154,18 @@ def test_bad_inputs_fail_closed():
         tj.self_join(X, 0.3)
     assert e.value.code == -3
     Y = torch.rand((500, 16), device="cuda") * 1e5
-    with pytest.raises(_lib.TJError) as e:
-        tj.self_join(Y, 0.3, screen="fp16")
-    assert e.value.code == -4
+    Y[:250] -= 2e5                   # centred values still beyond the FP16 range
+    for scr in ("fp16", "fp16x3"):
+        with pytest.raises(_lib.TJError) as e:
+            tj.self_join(Y, 0.3, screen=scr)
+        assert e.value.code == -4
     F = torch.rand((10, 4), device="cuda")
     with pytest.raises(_lib.TJError) as e:   # the int8-limb screen takes int14 data only
         tj.join_result(F, F, 0.1, mode="rs", screen="int8limb")
     assert e.value.code == -7
 
 
-@pytest.mark.parametrize("screen", ["bf16", "fp16"])
+@pytest.mark.parametrize("screen", ["bf16", "fp16", "bf16x3"])
 def test_metamorphic(screen):
     rng = np.random.default_rng(23)
     R = rng.standard_normal((1500, 40)).astype(np.float32)
@@ -215,3 +219,47 @@ def test_index_structure():
     assert np.all(keys[cs[:-1]][1:] != keys[cs[:-1]][:-1])
     tp = idx.tile_pairs.cpu().numpy()
     assert tp.shape[1] == 2 and len(tp) >= idx.n_tiles // 2
+
+
+# ---------------------------------------------------------------- int14 data, exact int8-limb screen
+@pytest.mark.parametrize("d", [128, 100, 200])
+def test_int14_self_join_exact(d):
+    w = W.int14x128(n=5000, d=d, samples=1 << 14)
+    for mode in ("upper", "directed"):
+        k, st = gpu_keys(w.R, None, w.T, mode, "int8limb")
+        assert_same(k, oracle.join_i16(w.R, None, w.T, mode), f"d={d} {mode}")
+        assert st["band"] == 0
+
+
+def test_int14_rs_ties_and_extremes():
+    rng = np.random.default_rng(31)
+    R = rng.integers(-8192, 8192, size=(1500, 128), dtype=np.int16)
+    S = rng.integers(-8192, 8192, size=(1700, 128), dtype=np.int16)
+    R[:8] = 8191
+    S[:8] = -8192
+    R[8:16] = -8192
+    S[8:16] = 8191
+    S[100:150] = R[200:250] + rng.integers(-1, 2, size=(50, 128)).astype(np.int16)
+    S[100:150] = np.clip(S[100:150], -8192, 8191)
+    d2 = ((R[200:250].astype(np.int64) - S[100:150].astype(np.int64)) ** 2).sum(1)
+    T = int(np.median(d2))      # several pairs sit exactly on the threshold
+    assert np.count_nonzero(d2 == T) >= 1
+    k, st = gpu_keys(R, S, T, "rs", "int8limb")
+    assert_same(k, oracle.join_i16(R, S, T, "rs"), "ties")
+    # the largest possible distance (all +8191 vs all -8192) decides exactly at its own value
+    Tmax = 128 * (8191 + 8192) ** 2
+    kx, _ = gpu_keys(R[:16], S[:16], Tmax, "rs", "int8limb")
+    assert_same(kx, oracle.join_i16(R[:16], S[:16], Tmax, "rs"), "extremes")
+    kx2, _ = gpu_keys(R[:16], S[:16], Tmax - 1, "rs", "int8limb")
+    assert_same(kx2, oracle.join_i16(R[:16], S[:16], Tmax - 1, "rs"), "extremes-1")
+
+
+def test_int14_rejects_out_of_range_and_fraction():
+    X = torch.full((300, 128), 9000, dtype=torch.int16, device="cuda")
+    with pytest.raises(_lib.TJError) as e:
+        tj.self_join(X, eps2=10, screen="int8limb")
+    assert e.value.code == -3
+    Y = torch.zeros((300, 128), dtype=torch.int16, device="cuda")
+    with pytest.raises(_lib.TJError) as e:
+        tj.self_join(Y, eps2=10.5, screen="int8limb")
+    assert e.value.code == -1
