@@ -127,6 +127,13 @@ TJ_DEV void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x,
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
         :: "r"(smem_u32(dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y) : "memory");
 }
+// Contiguous global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16),
+// completing on an mbarrier transaction count.
+TJ_DEV void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        :: "r"(smem_u32(dst)), "l"((uint64_t)src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
 TJ_DEV void prefetch_tmap(const CUtensorMap* map) {
     asm volatile("prefetch.tensormap [%0];" :: "l"((uint64_t)map) : "memory");
 }

@@ -24,10 +24,13 @@
 // that reproduces the oracle's summation order).
 //
 // Warp roles (192 threads, one CTA per SM, persistent over the chunk list):
-//   warp 0: TMA producer (one lane), 4-stage ring of {A k-block 16 KB, B k-block 32 KB}
+//   warp 0: TMA producer (one lane): a ring of k-block stages {A 128 rows, B 256 rows} and a
+//           ring of per-item column-metadata blocks (one 8 KB bulk copy per S tile), so the
+//           epilogue never waits on global memory inside an item
 //   warp 1: TMEM allocator + UMMA issuer (one lane), 2 accumulators x 256 columns
-//   warps 2-5: epilogue, warp w reads TMEM lanes 32*(w%4) .. +31 (one R row per thread)
-#include <cstdio>
+//   warps 2-5: epilogue, warp w reads TMEM lanes 32*(w%4) .. +31 (one R row per thread); the four
+//           warps run independently (no named barrier), synchronised only through mbarriers
+#include <algorithm>
 
 #include "tj_emit.cuh"
 #include "tj_internal.h"
@@ -41,6 +44,8 @@ constexpr int kEpiWarps = 4;
 constexpr int kScreenThreads = (2 + kEpiWarps) * 32;
 constexpr unsigned kABytes = kTileR * 128;          // 16 KB
 constexpr unsigned kBBytes = kTileS * 128;          // 32 KB
+constexpr int kMetaSlots = 3;
+
 // Stage = one 64-element k-block of A (128 rows) and B (256 rows); with the hi/lo split the
 // stage holds both limbs of both operands: [A_hi | A_lo | B_hi | B_lo].
 template <int kSplit> struct StageCfg {
@@ -51,23 +56,37 @@ template <int kSplit> struct StageCfg {
     static constexpr unsigned kBlo = 2u * kABytes + kBBytes;
 };
 
+// Column metadata of one S tile (256 sorted rows), structure of arrays, one bulk copy per item.
+struct ColMetaF {
+    float nrm2f[kTileS];   // FP32 nearest of ||y - c||^2; +inf for rows beyond the tile's points
+    float zn[kTileS];      // >= ||w||
+    float en[kTileS];      // >= ||y - c - w||
+    float yn[kTileS];      // >= ||y - c||
+    float zl[kTileS];      // >= ||w_lo||
+    uint32_t perm[kTileS]; // original row id
+    double nrm2[kTileS];   // ||y - c||^2 (FP64)
+    float WJ, FJ, YJ, BJ, betaJ, WlJ;   // tile maxima of zn, en, yn, nrm2f, |nrm2f - nrm2| bound, zl
+    uint32_t c0, nvJ;      // first sorted row, rows that are real points
+};
+static_assert(sizeof(ColMetaF) % 16 == 0, "bulk copies need 16-byte multiples");
+
 template <int kStages>
 struct ScreenCtl {
     uint64_t full[kStages];
     uint64_t empty[kStages];
     uint64_t acc_full[kAccBufs];
     uint64_t acc_empty[kAccBufs];
+    uint64_t meta_full[kMetaSlots];
+    uint64_t meta_empty[kMetaSlots];
     uint64_t drain;
     unsigned tmem_base;
     int abort_flag;
-    int acc_ok[2];   // per item parity, like bt: written after the previous item's barrier
-    float bt[2][kTileS];
 };
 
 template <int kSplit>
 constexpr size_t screen_smem() {
     return 1024 + (size_t)StageCfg<kSplit>::kStages * StageCfg<kSplit>::kBytes +
-           sizeof(ScreenCtl<StageCfg<kSplit>::kStages>);
+           (size_t)kMetaSlots * sizeof(ColMetaF) + sizeof(ScreenCtl<StageCfg<kSplit>::kStages>);
 }
 
 struct ScreenArgs {
@@ -82,22 +101,9 @@ struct ScreenArgs {
     const float* r_zn;
     const float* r_en;
     const float* r_zl;
-    // S side (columns of tile J)
+    // S side: per-tile column metadata blocks
+    const ColMetaF* s_meta;
     const uint32_t* s_row0;
-    const uint32_t* s_nvalid;
-    const uint32_t* s_perm;
-    const double* s_nrm2;
-    const float* s_nrm2f;
-    const float* s_zn;
-    const float* s_en;
-    const float* s_yn;
-    const float* s_zl;
-    const float* sJ_maxZl;
-    const float* sJ_maxZ;
-    const float* sJ_maxE;
-    const float* sJ_maxY;
-    const float* sJ_maxB;
-    const float* sJ_beta;
     int kblocks;
     int kpad;
     unsigned idesc;
@@ -109,6 +115,46 @@ struct ScreenArgs {
     Counters* ctr;
 };
 
+// r[k] for a runtime k without local memory: a fixed 31-select tree (the rare path's only way
+// to reach one accumulator value, keeping a single copy of its code).
+TJ_DEV uint32_t pick32(const uint32_t (&r)[32], int k) {
+    uint32_t a16[16], a8[8], a4[4], a2[2];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) a16[i] = (k & 16) ? r[i + 16] : r[i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a8[i] = (k & 8) ? a16[i + 8] : a16[i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a4[i] = (k & 4) ? a8[i + 4] : a8[i];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) a2[i] = (k & 2) ? a4[i + 2] : a4[i];
+    return (k & 1) ? a2[1] : a2[0];
+}
+
+// Pack the S-side row metadata into one ColMetaF block per 256-row tile.
+__global__ void __launch_bounds__(kTileS) build_col_meta(const uint32_t* row0, const uint32_t* nvalid,
+                                                          const uint32_t* perm, const double* nrm2,
+                                                          const float* nrm2f, const float* zn, const float* en,
+                                                          const float* yn, const float* zl, const float* maxZ,
+                                                          const float* maxE, const float* maxY, const float* maxB,
+                                                          const float* beta, const float* maxZl, ColMetaF* out) {
+    const unsigned J = blockIdx.x, t = threadIdx.x;
+    const unsigned c0 = row0[J], nv = nvalid[J];
+    ColMetaF& m = out[J];
+    const bool ok = t < nv;
+    const unsigned r = c0 + t;
+    m.nrm2f[t] = ok ? nrm2f[r] : INFINITY;
+    m.zn[t] = ok ? zn[r] : 0.f;
+    m.en[t] = ok ? en[r] : 0.f;
+    m.yn[t] = ok ? yn[r] : 0.f;
+    m.zl[t] = ok ? zl[r] : 0.f;
+    m.perm[t] = ok ? perm[r] : 0u;
+    m.nrm2[t] = ok ? nrm2[r] : 0.0;
+    if (t == 0) {
+        m.WJ = maxZ[J]; m.FJ = maxE[J]; m.YJ = maxY[J]; m.BJ = maxB[J]; m.betaJ = beta[J]; m.WlJ = maxZl[J];
+        m.c0 = c0; m.nvJ = nv;
+    }
+}
+
 template <int kFmt, int kSplit>   // kFmt: 0 = fp16, 1 = bf16; kSplit: hi/lo operand limbs
 __global__ void __launch_bounds__(kScreenThreads, 1)
     screen_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -118,7 +164,8 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
     constexpr unsigned kStageBytes = Cfg::kBytes;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    ScreenCtl<kStages>* ctl = (ScreenCtl<kStages>*)(smem + (size_t)kStages * kStageBytes);
+    ColMetaF* meta = (ColMetaF*)(smem + (size_t)kStages * kStageBytes);
+    ScreenCtl<kStages>* ctl = (ScreenCtl<kStages>*)(meta + kMetaSlots);
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long* status = &a.ctr->status;
 
@@ -130,6 +177,10 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         for (int b = 0; b < kAccBufs; ++b) {
             mbar_init(&ctl->acc_full[b], 1);
             mbar_init(&ctl->acc_empty[b], kEpiWarps);
+        }
+        for (int m = 0; m < kMetaSlots; ++m) {
+            mbar_init(&ctl->meta_full[m], 1);
+            mbar_init(&ctl->meta_empty[m], kEpiWarps);
         }
         mbar_init(&ctl->drain, 1);
         ctl->abort_flag = 0;
@@ -148,12 +199,18 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         // ------------------------------------------------------------ TMA producer
         if (lane == 0) {
             unsigned stage = 0, phase = 0;
+            unsigned long long n = 0;   // items issued
             bool ok = true;
             for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
                 const uint4 ch = a.chunks[c];
                 const int rrow = (int)a.r_row0[ch.x];
-                for (unsigned e = ch.y; e < ch.z && ok; ++e) {
-                    const int srow = (int)a.s_row0[a.jlist[e]];
+                for (unsigned e = ch.y; e < ch.z && ok; ++e, ++n) {
+                    const unsigned J = a.jlist[e];
+                    const int srow = (int)a.s_row0[J];
+                    const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
+                    if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status)) { ok = false; break; }
+                    mbar_arrive_expect_tx(&ctl->meta_full[slot], (unsigned)sizeof(ColMetaF));
+                    bulk_load(&meta[slot], a.s_meta + J, (unsigned)sizeof(ColMetaF), &ctl->meta_full[slot]);
                     for (int kb = 0; kb < a.kblocks; ++kb) {
                         if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
@@ -170,12 +227,15 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 }
             }
             if (!ok) ctl->abort_flag = 1;
-            // drain: the last load issued into each stage must have landed before exit
-            for (int k = 0; k < kStages; ++k) {
-                // stage s was last filled in phase (phase ^ 1) if s >= stage, else in phase `phase`
-                const unsigned s = (unsigned)k;
-                const unsigned ph = (s < stage) ? phase : (phase ^ 1u);
+            // drain: the last copy issued into every stage / metadata slot must land before exit
+            for (int s = 0; s < kStages; ++s) {
+                const unsigned ph = ((unsigned)s < stage) ? phase : (phase ^ 1u);
                 mbar_wait(&ctl->full[s], ph, status, 1000000000ull);
+            }
+            for (int s = 0; s < kMetaSlots; ++s) {
+                if (n <= (unsigned long long)s) continue;
+                const unsigned long long last = ((n - 1 - s) / kMetaSlots) * kMetaSlots + s;
+                mbar_wait(&ctl->meta_full[s], (unsigned)((last / kMetaSlots) & 1), status, 1000000000ull);
             }
         }
     } else if (warp == 1) {
@@ -219,12 +279,11 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
     } else {
         // ------------------------------------------------------------ epilogue
         const unsigned q = warp & 3;                 // TMEM lane quarter of this warp
-        const unsigned et = threadIdx.x - 64;        // 0..127 epilogue thread id
         const unsigned row = q * 32 + lane;          // R row within the tile
         const JoinParams& jp = a.jp;
         WarpAppender app_acc, app_band;
-        unsigned acc = 0, acc_phase = 0, par = 0;
-        unsigned long long n_screen_acc = 0, n_rare = 0, n_items = 0;
+        unsigned acc = 0, acc_phase = 0;
+        unsigned long long n = 0, n_screen_acc = 0, n_rare = 0, n_items = 0;
         bool ok = true;
         for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
             const uint4 ch = a.chunks[c];
@@ -236,109 +295,99 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             const double Zi = rvalid ? (double)a.r_zn[rs] : 0.0;
             const double Ei = rvalid ? (double)a.r_en[rs] : 0.0;
             const double Zli = rvalid ? (double)a.r_zl[rs] : 0.0;
-            for (unsigned e = ch.y; e < ch.z; ++e) {
-                const unsigned J = a.jlist[e];
-                const unsigned c0 = a.s_row0[J];
-                const unsigned nvJ = a.s_nvalid[J];
-                ctl->bt[par][et] = et < nvJ ? a.s_nrm2f[c0 + et] : INFINITY;
-                ctl->bt[par][et + 128] = et + 128 < nvJ ? a.s_nrm2f[c0 + et + 128] : INFINITY;
-                if (et == 0) ctl->acc_ok[par] = mbar_wait(&ctl->acc_full[acc], acc_phase, status) ? 1 : 0;
-                asm volatile("bar.sync 1, 128;" ::: "memory");
-                if (!ctl->acc_ok[par]) { ok = false; break; }
+            const uint32_t oi = rvalid ? a.r_perm[rs] : 0u;
+            for (unsigned e = ch.y; e < ch.z; ++e, ++n) {
+                const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
+                if (!mbar_wait(&ctl->meta_full[slot], mph, status) ||
+                    !mbar_wait(&ctl->acc_full[acc], acc_phase, status)) { ok = false; break; }
                 tc_fence_after();
+                const ColMetaF& m = meta[slot];
+                const unsigned c0 = m.c0;
                 // per-(row, S tile) fast threshold; every error term bounded by tile maxima
                 float tau = -INFINITY;
                 if (rvalid) {
-                    const double WJ = a.sJ_maxZ[J], FJ = a.sJ_maxE[J], YJ = a.sJ_maxY[J];
-                    const double BJ = a.sJ_maxB[J], betaJ = a.sJ_beta[J], WlJ = a.sJ_maxZl[J];
+                    const double WJ = m.WJ, FJ = m.FJ, YJ = m.YJ, BJ = m.BJ, betaJ = m.betaJ, WlJ = m.WlJ;
                     const double RiJ = jp.gmma * Zi * WJ + jp.cabs + Ei * YJ + Zi * FJ + Zli * WlJ;
                     const double PiJ = Zi * WJ * (1.0 + jp.gmma) + jp.cabs;
                     double t = jp.Tp - Ai + jp.gn * Ai + 0x1p-23 * (BJ + 2.0 * PiJ) + betaJ + 2.0 * RiJ;
                     t = t + fabs(t) * 0x1p-30 + 0x1p-1000;
                     tau = f32_up(t);
                 }
-                const float* bt = ctl->bt[par];
                 const unsigned tbase = tmem + ((q * 32u) << 16) + acc * kTileS;
 #pragma unroll 1
                 for (int cb = 0; cb < kTileS / 32; ++cb) {
+                    const int col0 = cb * 32;
                     uint32_t raw[32];
-                    tmem_ld32(tbase + cb * 32, raw);
+                    tmem_ld32(tbase + col0, raw);
                     tmem_ld_wait();
-                    if (cb == kTileS / 32 - 1) {
+                    if (cb == kTileS / 32 - 1) {   // accumulator fully read: hand it back to the MMA
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&ctl->acc_empty[acc]);
                     }
-                    float vmin = INFINITY;
+                    // fast path: one FMA and one compare per pair, candidates collected in a bit mask
+                    uint32_t cmask = 0;
 #pragma unroll
                     for (int k = 0; k < 32; ++k)
-                        vmin = fminf(vmin, fmaf(-2.f, __uint_as_float(raw[k]), bt[cb * 32 + k]));
-                    const bool cand = vmin <= tau;
-                    if (!__any_sync(0xffffffffu, cand)) continue;
-                    // ---------------- rare path: per-pair FP64 certificate
+                        cmask |= (fmaf(-2.f, __uint_as_float(raw[k]), m.nrm2f[col0 + k]) <= tau ? 1u : 0u) << k;
+                    if (jp.self_join && cmask) {   // keep sorted column > sorted row only
+                        const int lim = (int)rs - (int)(c0 + col0);   // columns k <= lim are not above the diagonal
+                        if (lim >= 31) cmask = 0;
+                        else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
+                    }
+                    if (!__any_sync(0xffffffffu, cmask != 0)) continue;
+                    // ---------------- rare path: per-pair FP64 certificate, operands from shared memory
                     uint32_t amask = 0, bmask = 0;
-                    if (cand) {
-#pragma unroll
-                        for (int k = 0; k < 32; ++k) {
-                            const float pk = __uint_as_float(raw[k]);
-                            const float v = fmaf(-2.f, pk, bt[cb * 32 + k]);
-                            if (v <= tau) {
-                                const unsigned col = cb * 32 + k;
-                                const unsigned cs = c0 + col;
-                                if (jp.self_join && cs <= rs) continue;
-                                ++n_rare;
-                                const double p = (double)pk;
-                                const double Bj = a.s_nrm2[cs];
-                                const double Wj = a.s_zn[cs], Fj = a.s_en[cs], Yj = a.s_yn[cs];
-                                const double s = Ai + Bj - 2.0 * p;
-                                const double R = jp.gmma * Zi * Wj + jp.cabs + Ei * Yj + Zi * Fj +
-                                                 Zli * (double)a.s_zl[cs];
-                                double m = 2.0 * R + jp.gn * (Ai + Bj) + 0x1p-50 * (Ai + Bj + 2.0 * fabs(p));
-                                m = m * (1.0 + 0x1p-40) + 0x1p-1000;
-                                if (s + m <= jp.Tm) amask |= 1u << k;
-                                else if (!(s - m > jp.Tp)) bmask |= 1u << k;
-                            }
-                        }
+                    uint32_t mk = cmask;
+                    while (mk) {
+                        const int k = __ffs(mk) - 1;
+                        mk &= mk - 1;
+                        ++n_rare;
+                        const int col = col0 + k;
+                        const double p = (double)__uint_as_float(pick32(raw, k));
+                        const double Bj = m.nrm2[col];
+                        const double sv = Ai + Bj - 2.0 * p;
+                        const double R = jp.gmma * Zi * (double)m.zn[col] + jp.cabs + Ei * (double)m.yn[col] +
+                                         Zi * (double)m.en[col] + Zli * (double)m.zl[col];
+                        double mm = 2.0 * R + jp.gn * (Ai + Bj) + 0x1p-50 * (Ai + Bj + 2.0 * fabs(p));
+                        mm = mm * (1.0 + 0x1p-40) + 0x1p-1000;
+                        if (sv + mm <= jp.Tm) amask |= 1u << k;
+                        else if (!(sv - mm > jp.Tp)) bmask |= 1u << k;
                     }
                     unsigned ta, tb;
                     const unsigned pa = warp_excl_scan(__popc(amask), ta);
                     const unsigned pb = warp_excl_scan(__popc(bmask), tb);
                     if (ta) {
-                        const unsigned long long base = app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap);
-                        unsigned long long pos = base + pa;
-                        uint32_t mk = amask;
-                        while (mk) {
-                            const int k = __ffs(mk) - 1;
-                            mk &= mk - 1;
-                            const unsigned cs = c0 + cb * 32 + k;
-                            if (pos < a.acc_cap) a.acc[pos] = pair_key(jp, a.r_perm[rs], a.s_perm[cs]);
+                        unsigned long long pos = app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap) + pa;
+                        uint32_t w = amask;
+                        while (w) {
+                            const int k = __ffs(w) - 1;
+                            w &= w - 1;
+                            if (pos < a.acc_cap) a.acc[pos] = pair_key(jp, oi, m.perm[col0 + k]);
                             ++pos;
                         }
                         n_screen_acc += __popc(amask);
                     }
                     if (tb) {
-                        const unsigned long long base =
-                            app_band.reserve(tb, &a.ctr->band_reserved, a.band, a.band_cap);
-                        unsigned long long pos = base + pb;
-                        uint32_t mk = bmask;
-                        while (mk) {
-                            const int k = __ffs(mk) - 1;
-                            mk &= mk - 1;
-                            const unsigned cs = c0 + cb * 32 + k;
-                            if (pos < a.band_cap) a.band[pos] = pair_key(jp, a.r_perm[rs], a.s_perm[cs]);
+                        unsigned long long pos = app_band.reserve(tb, &a.ctr->band_reserved, a.band, a.band_cap) + pb;
+                        uint32_t w = bmask;
+                        while (w) {
+                            const int k = __ffs(w) - 1;
+                            w &= w - 1;
+                            if (pos < a.band_cap) a.band[pos] = pair_key(jp, oi, m.perm[col0 + k]);
                             ++pos;
                         }
                     }
                 }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&ctl->meta_empty[slot]);   // this warp is done with the slot
                 ++n_items;
-                par ^= 1;
                 if (++acc == kAccBufs) { acc = 0; acc_phase ^= 1; }
             }
         }
         if (!ok) ctl->abort_flag = 1;
         app_acc.pad(a.acc, a.acc_cap);
         app_band.pad(a.band, a.band_cap);
-        // warp totals
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             n_screen_acc += __shfl_xor_sync(0xffffffffu, n_screen_acc, o);
@@ -414,21 +463,14 @@ void screen_tc(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st) {
     a.r_zn = R.zn.p;
     a.r_en = R.en.p;
     a.r_zl = R.zl.p;
-    a.s_row0 = g.tS->row0.p;
-    a.s_nvalid = g.tS->nvalid.p;
-    a.s_perm = S.perm.p;
-    a.s_nrm2 = S.nrm2.p;
-    a.s_nrm2f = S.nrm2f.p;
-    a.s_zn = S.zn.p;
-    a.s_en = S.en.p;
-    a.s_yn = S.yn.p;
-    a.s_zl = S.zl.p;
-    a.sJ_maxZl = g.tS->maxZl.p;
-    a.sJ_maxZ = g.tS->maxZ.p;
-    a.sJ_maxE = g.tS->maxE.p;
-    a.sJ_maxY = g.tS->maxY.p;
-    a.sJ_maxB = g.tS->maxB.p;
-    a.sJ_beta = g.tS->beta.p;
+    const TileSet& tS = *g.tS;
+    DBuf<ColMetaF> smeta((size_t)std::max(tS.ntiles, 1), st);
+    if (tS.ntiles > 0)
+        launch(build_col_meta, tS.ntiles, kTileS, 0, st, tS.row0.p, tS.nvalid.p, S.perm.p, S.nrm2.p, S.nrm2f.p,
+               S.zn.p, S.en.p, S.yn.p, S.zl.p, tS.maxZ.p, tS.maxE.p, tS.maxY.p, tS.maxB.p, tS.beta.p, tS.maxZl.p,
+               smeta.p);
+    a.s_meta = smeta.p;
+    a.s_row0 = tS.row0.p;
     a.kblocks = R.kpad / kBK;
     a.kpad = R.kpad;
     a.idesc = make_idesc(1u, bf ? 1u : 0u, kTileR, kTileS);

@@ -21,6 +21,8 @@
 // issuer runs the hh products of item n+1 while the epilogue still reads x / ll of item n.
 // Warp roles (320 threads): warp 0 TMA producer, warp 1 UMMA issuer, warps 2..9 epilogue
 // (warp w reads TMEM lanes 32*(w%4).. and columns 64*((w-2)/4)..).
+#include <algorithm>
+
 #include "tj_emit.cuh"
 #include "tj_internal.h"
 
@@ -36,20 +38,31 @@ constexpr unsigned kPart = 128u * 128u;          // one 128-row x 128-byte swizz
 constexpr unsigned kI8Stage = 4 * kPart;         // A_h, A_l, B_h, B_l
 constexpr unsigned kColHH0 = 0, kColX = 256, kColLL = 384;
 
+constexpr int kI8Meta = 3;
+
+// Column metadata of one 128-row S tile, loaded with one bulk copy per item.
+struct ColMetaI8 {
+    int bq[kI8N];           // floor(|q_j|^2 / 2^15); 2^30 for rows beyond the tile's points
+    uint32_t perm[kI8N];    // original row id
+    long long norm[kI8N];   // exact |q_j|^2
+    uint32_t c0, nvJ, pad0, pad1;
+};
+static_assert(sizeof(ColMetaI8) % 16 == 0, "bulk copies need 16-byte multiples");
+
 struct I8Ctl {
     uint64_t full[kI8Stages];
     uint64_t empty[kI8Stages];
     uint64_t acc_full[2];
     uint64_t hh_empty[2];
     uint64_t xl_empty;
+    uint64_t meta_full[kI8Meta];
+    uint64_t meta_empty[kI8Meta];
     uint64_t drain;
     unsigned tmem_base;
     int abort_flag;
-    int acc_ok[2];
-    int bq[2][kI8N];       // floor(|q_j|^2 / 2^15), or a huge value for padding columns
 };
 
-constexpr size_t kI8Smem = 1024 + (size_t)kI8Stages * kI8Stage + sizeof(I8Ctl);
+constexpr size_t kI8Smem = 1024 + (size_t)kI8Stages * kI8Stage + kI8Meta * sizeof(ColMetaI8) + sizeof(I8Ctl);
 
 struct I8Args {
     const uint4* chunks;
@@ -60,9 +73,7 @@ struct I8Args {
     const uint32_t* r_perm;
     const long long* r_norm;   // exact |q|^2
     const uint32_t* s_row0;
-    const uint32_t* s_nvalid;
-    const uint32_t* s_perm;
-    const long long* s_norm;
+    const ColMetaI8* s_meta;
     int kblocks;               // kpad / 128
     int kpad;
     unsigned idesc;
@@ -76,12 +87,26 @@ struct I8Args {
 
 TJ_DEV int floor_shift15(long long v) { return (int)(v >> 15); }   // arithmetic shift = floor division
 
+__global__ void __launch_bounds__(kI8N) build_col_meta_i8(const uint32_t* row0, const uint32_t* nvalid,
+                                                         const uint32_t* perm, const long long* norm,
+                                                         ColMetaI8* out) {
+    const unsigned J = blockIdx.x, t = threadIdx.x;
+    const unsigned c0 = row0[J], nv = nvalid[J];
+    ColMetaI8& m = out[J];
+    const bool ok = t < nv;
+    m.bq[t] = ok ? floor_shift15(norm[c0 + t]) : 0x40000000;
+    m.perm[t] = ok ? perm[c0 + t] : 0u;
+    m.norm[t] = ok ? norm[c0 + t] : 0ll;
+    if (t == 0) { m.c0 = c0; m.nvJ = nv; m.pad0 = m.pad1 = 0; }
+}
+
 __global__ void __launch_bounds__(kI8Threads, 1)
     screen_i8_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      const I8Args a) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    I8Ctl* ctl = (I8Ctl*)(smem + (size_t)kI8Stages * kI8Stage);
+    ColMetaI8* meta = (ColMetaI8*)(smem + (size_t)kI8Stages * kI8Stage);
+    I8Ctl* ctl = (I8Ctl*)(meta + kI8Meta);
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long* status = &a.ctr->status;
 
@@ -95,6 +120,10 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             mbar_init(&ctl->hh_empty[b], kI8Epi);
         }
         mbar_init(&ctl->xl_empty, kI8Epi);
+        for (int m = 0; m < kI8Meta; ++m) {
+            mbar_init(&ctl->meta_full[m], 1);
+            mbar_init(&ctl->meta_empty[m], kI8Epi);
+        }
         mbar_init(&ctl->drain, 1);
         ctl->abort_flag = 0;
         fence_barrier_init();
@@ -111,12 +140,18 @@ __global__ void __launch_bounds__(kI8Threads, 1)
     if (warp == 0) {
         if (lane == 0) {
             unsigned stage = 0, phase = 0;
+            unsigned long long n = 0;
             bool ok = true;
             for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
                 const uint4 ch = a.chunks[c];
                 const int rrow = (int)a.r_row0[ch.x];
-                for (unsigned e = ch.y; e < ch.z && ok; ++e) {
-                    const int srow = (int)a.s_row0[a.jlist[e]];
+                for (unsigned e = ch.y; e < ch.z && ok; ++e, ++n) {
+                    const unsigned J = a.jlist[e];
+                    const int srow = (int)a.s_row0[J];
+                    const unsigned slot = (unsigned)(n % kI8Meta), mph = (unsigned)((n / kI8Meta) & 1);
+                    if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status)) { ok = false; break; }
+                    mbar_arrive_expect_tx(&ctl->meta_full[slot], (unsigned)sizeof(ColMetaI8));
+                    bulk_load(&meta[slot], a.s_meta + J, (unsigned)sizeof(ColMetaI8), &ctl->meta_full[slot]);
                     for (int kb = 0; kb < a.kblocks; ++kb) {
                         if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
@@ -134,6 +169,11 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             for (int s = 0; s < kI8Stages; ++s) {
                 const unsigned ph = ((unsigned)s < stage) ? phase : (phase ^ 1u);
                 mbar_wait(&ctl->full[s], ph, status, 1000000000ull);
+            }
+            for (int s = 0; s < kI8Meta; ++s) {
+                if (n <= (unsigned long long)s) continue;
+                const unsigned long long last = ((n - 1 - s) / kI8Meta) * kI8Meta + s;
+                mbar_wait(&ctl->meta_full[s], (unsigned)((last / kI8Meta) & 1), status, 1000000000ull);
             }
         }
     } else if (warp == 1) {
@@ -183,7 +223,6 @@ __global__ void __launch_bounds__(kI8Threads, 1)
         const unsigned ew = warp - 2;                 // 0..7
         const unsigned q = warp & 3;                  // TMEM lane quarter
         const unsigned half = ew >> 2;                // column half (0: 0..63, 1: 64..127)
-        const unsigned et = threadIdx.x - 64;         // 0..255
         const unsigned row = q * 32 + lane;
         const JoinParams& jp = a.jp;
         WarpAppender app;
@@ -197,47 +236,42 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             const unsigned rs = r0 + row;
             const long long Ai = rvalid ? a.r_norm[rs] : 0;
             const int ai = rvalid ? floor_shift15(Ai - a.T - a.twoM) : 0x7FFFFFFF;
+            const uint32_t oi = rvalid ? a.r_perm[rs] : 0u;
             for (unsigned e = ch.y; e < ch.z; ++e, ++n) {
-                const unsigned b = (unsigned)(n & 1), par = b;
-                const unsigned J = a.jlist[e];
-                const unsigned c0 = a.s_row0[J];
-                const unsigned nvJ = a.s_nvalid[J];
-                if (et < (unsigned)kI8N)
-                    ctl->bq[par][et] = et < nvJ ? floor_shift15(a.s_norm[c0 + et]) : 0x40000000;
-                if (et == 0)
-                    ctl->acc_ok[par] = mbar_wait(&ctl->acc_full[b], (unsigned)((n >> 1) & 1), status) ? 1 : 0;
-                asm volatile("bar.sync 1, 256;" ::: "memory");
-                if (!ctl->acc_ok[par]) { ok = false; break; }
+                const unsigned b = (unsigned)(n & 1);
+                const unsigned slot = (unsigned)(n % kI8Meta), mph = (unsigned)((n / kI8Meta) & 1);
+                if (!mbar_wait(&ctl->meta_full[slot], mph, status) ||
+                    !mbar_wait(&ctl->acc_full[b], (unsigned)((n >> 1) & 1), status)) { ok = false; break; }
                 tc_fence_after();
-                const int* bq = ctl->bq[par];
+                const ColMetaI8& m = meta[slot];
+                const unsigned c0 = m.c0;
                 const unsigned lane_off = (q * 32u) << 16;
+                const unsigned col0 = half * 64;
 #pragma unroll 1
-                for (int cb = 0; cb < 2; ++cb) {
-                    const unsigned col0 = half * 64 + cb * 32;
-                    uint32_t hh[32];
-                    tmem_ld32(tmem + lane_off + kColHH0 + b * 128 + col0, hh);
+                for (int h = 0; h < 2; ++h) {
+                    const unsigned cc = col0 + h * 32;
+                    uint32_t hv[32];
+                    tmem_ld32(tmem + lane_off + kColHH0 + b * 128 + cc, hv);
                     tmem_ld_wait();
                     int mx = -0x7FFFFFFF;
 #pragma unroll
-                    for (int k = 0; k < 32; ++k) mx = max(mx, (int)hh[k] - bq[col0 + k]);
+                    for (int k = 0; k < 32; ++k) mx = max(mx, (int)hv[k] - m.bq[cc + k]);
                     const bool cand = mx >= ai;
                     if (!__any_sync(0xffffffffu, cand)) continue;
                     uint32_t xv[32], lv[32];
-                    tmem_ld32(tmem + lane_off + kColX + col0, xv);
-                    tmem_ld32(tmem + lane_off + kColLL + col0, lv);
+                    tmem_ld32(tmem + lane_off + kColX + cc, xv);
+                    tmem_ld32(tmem + lane_off + kColLL + cc, lv);
                     tmem_ld_wait();
                     uint32_t amask = 0;
                     if (cand) {
 #pragma unroll
                         for (int k = 0; k < 32; ++k) {
-                            if ((int)hh[k] - bq[col0 + k] < ai) continue;
-                            const unsigned cs = c0 + col0 + k;
-                            if (col0 + k >= nvJ) continue;
-                            if (jp.self_join && cs <= rs) continue;
+                            if ((int)hv[k] - m.bq[cc + k] < ai) continue;
+                            if (jp.self_join && c0 + cc + k <= rs) continue;
                             ++n_rare;
-                            const long long dot = (long long)(int)hh[k] * 16384ll + (long long)(int)xv[k] * 128ll +
-                                                  (long long)(int)lv[k];
-                            const long long d2 = Ai + a.s_norm[cs] - 2 * dot;
+                            const long long dot = (long long)(int)hv[k] * 16384ll +
+                                                  (long long)(int)xv[k] * 128ll + (long long)(int)lv[k];
+                            const long long d2 = Ai + m.norm[cc + k] - 2 * dot;
                             if (d2 <= a.T) amask |= 1u << k;
                         }
                     }
@@ -249,19 +283,19 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                         while (mk) {
                             const int k = __ffs(mk) - 1;
                             mk &= mk - 1;
-                            const unsigned cs = c0 + col0 + k;
-                            if (pos < a.acc_cap) a.acc[pos] = pair_key(jp, a.r_perm[rs], a.s_perm[cs]);
+                            if (pos < a.acc_cap) a.acc[pos] = pair_key(jp, oi, m.perm[cc + k]);
                             ++pos;
                         }
                         n_acc += __popc(amask);
                     }
                 }
-                // this item's hh buffer and the shared x / ll are free again
+                // this item's hh buffer, the shared x / ll and the metadata slot are free again
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) {
                     mbar_arrive(&ctl->hh_empty[b]);
                     mbar_arrive(&ctl->xl_empty);
+                    mbar_arrive(&ctl->meta_empty[slot]);
                 }
                 ++n_items;
             }
@@ -306,10 +340,12 @@ void screen_i8(const JoinGeometry& g, const EmitBuffers& eb, long long T, cudaSt
     a.r_nvalid = g.tR->nvalid.p;
     a.r_perm = R.perm.p;
     a.r_norm = R.inorm.p;
-    a.s_row0 = g.tS->row0.p;
-    a.s_nvalid = g.tS->nvalid.p;
-    a.s_perm = S.perm.p;
-    a.s_norm = S.inorm.p;
+    const TileSet& tS = *g.tS;
+    DBuf<ColMetaI8> smeta((size_t)std::max(tS.ntiles, 1), st);
+    if (tS.ntiles > 0)
+        launch(build_col_meta_i8, tS.ntiles, kI8N, 0, st, tS.row0.p, tS.nvalid.p, S.perm.p, S.inorm.p, smeta.p);
+    a.s_row0 = tS.row0.p;
+    a.s_meta = smeta.p;
     a.kblocks = R.kpad / 128;
     a.kpad = R.kpad;
     a.idesc = make_idesc(2u, 1u, 128, kI8N);
