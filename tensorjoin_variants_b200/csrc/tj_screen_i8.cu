@@ -87,6 +87,20 @@ struct I8Args {
 
 TJ_DEV int floor_shift15(long long v) { return (int)(v >> 15); }   // arithmetic shift = floor division
 
+// r[k] for a runtime k without local memory (fixed 31-select tree).
+TJ_DEV uint32_t pick32(const uint32_t (&r)[32], int k) {
+    uint32_t a16[16], a8[8], a4[4], a2[2];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) a16[i] = (k & 16) ? r[i + 16] : r[i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a8[i] = (k & 8) ? a16[i + 8] : a16[i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a4[i] = (k & 4) ? a8[i + 4] : a8[i];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) a2[i] = (k & 2) ? a4[i + 2] : a4[i];
+    return (k & 1) ? a2[1] : a2[0];
+}
+
 __global__ void __launch_bounds__(kI8N) build_col_meta_i8(const uint32_t* row0, const uint32_t* nvalid,
                                                          const uint32_t* perm, const long long* norm,
                                                          ColMetaI8* out) {
@@ -253,27 +267,28 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                     uint32_t hv[32];
                     tmem_ld32(tmem + lane_off + kColHH0 + b * 128 + cc, hv);
                     tmem_ld_wait();
-                    int mx = -0x7FFFFFFF;
+                    uint32_t cmask = 0;
 #pragma unroll
-                    for (int k = 0; k < 32; ++k) mx = max(mx, (int)hv[k] - m.bq[cc + k]);
-                    const bool cand = mx >= ai;
-                    if (!__any_sync(0xffffffffu, cand)) continue;
+                    for (int k = 0; k < 32; ++k) cmask |= ((int)hv[k] - m.bq[cc + k] >= ai ? 1u : 0u) << k;
+                    if (jp.self_join && cmask) {   // keep sorted column > sorted row only
+                        const int lim = (int)rs - (int)(c0 + cc);
+                        if (lim >= 31) cmask = 0;
+                        else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
+                    }
+                    if (!__any_sync(0xffffffffu, cmask != 0)) continue;
                     uint32_t xv[32], lv[32];
                     tmem_ld32(tmem + lane_off + kColX + cc, xv);
                     tmem_ld32(tmem + lane_off + kColLL + cc, lv);
                     tmem_ld_wait();
-                    uint32_t amask = 0;
-                    if (cand) {
-#pragma unroll
-                        for (int k = 0; k < 32; ++k) {
-                            if ((int)hv[k] - m.bq[cc + k] < ai) continue;
-                            if (jp.self_join && c0 + cc + k <= rs) continue;
-                            ++n_rare;
-                            const long long dot = (long long)(int)hv[k] * 16384ll +
-                                                  (long long)(int)xv[k] * 128ll + (long long)(int)lv[k];
-                            const long long d2 = Ai + m.norm[cc + k] - 2 * dot;
-                            if (d2 <= a.T) amask |= 1u << k;
-                        }
+                    uint32_t amask = 0, mk = cmask;
+                    while (mk) {   // exact INT64 test, one copy of the code
+                        const int k = __ffs(mk) - 1;
+                        mk &= mk - 1;
+                        ++n_rare;
+                        const long long dot = (long long)(int)pick32(hv, k) * 16384ll +
+                                              (long long)(int)pick32(xv, k) * 128ll + (long long)(int)pick32(lv, k);
+                        const long long d2 = Ai + m.norm[cc + k] - 2 * dot;
+                        if (d2 <= a.T) amask |= 1u << k;
                     }
                     unsigned ta;
                     const unsigned pa = warp_excl_scan(__popc(amask), ta);
