@@ -102,13 +102,13 @@ __global__ void cell_starts(const uint32_t* flag, const uint32_t* pos, long long
     if (i == 0) start[*ncells] = (uint32_t)n;
 }
 __global__ void pairs_screened_kernel(const uint4* chunks, const uint32_t* nchunks, const uint32_t* jlist,
-                                      const uint32_t* rnv, const uint32_t* snv, unsigned long long* out) {
+                                      const uint4* rtiles, const uint4* stiles, unsigned long long* out) {
     unsigned long long acc = 0;
     const unsigned n = *nchunks;
     for (unsigned c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         const uint4 ch = chunks[c];
-        const unsigned long long rv = rnv[ch.x];
-        for (unsigned e = ch.y; e < ch.z; ++e) acc += rv * snv[jlist[e]];
+        const unsigned long long rv = rtiles[ch.x].y;
+        for (unsigned e = ch.y; e < ch.z; ++e) acc += rv * stiles[jlist[e]].y;
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
@@ -188,10 +188,9 @@ struct tj_result {
     long long count = 0;
     long long n_rows = 0, n_cols = 0;
     tj_stats stats;
-    // batched mode
+    // batched mode (njoins > 1): per-join output ranges and key decoding tables
+    int njoins = 1;
     std::vector<int64_t> offsets;
-    std::vector<long long> join_cols;
-    std::vector<unsigned long long> join_keyoff;
     DBuf<unsigned long long> d_keyoff;
     DBuf<long long> d_cols;
 };
@@ -230,75 +229,261 @@ void check_status(unsigned long long status) {
     if (status & kStatusTmemAlloc) fail(TJ_ERR_CUDA, "tensor memory allocation failed");
 }
 
-void run_join(const void* R, long long nR, const void* S, long long nS, int d, int dtype, double eps2, int mode,
-              int screen, const tj_options* opt, tj_result* res, cudaStream_t st) {
-    const bool self = mode != TJ_MODE_RS;
-    if (self) { S = R; nS = nR; }
-    if ((nR > 0 && !R) || (nS > 0 && !S)) fail(TJ_ERR_INVALID, "null input pointer");
-    if (d <= 0 || nR < 0 || nS < 0) fail(TJ_ERR_INVALID, "invalid shape");
-    if (nR >= (1ll << 32) || nS >= (1ll << 32)) fail(TJ_ERR_INVALID, "more than 2^32 - 1 rows per side");
-    if (!(eps2 >= 0.0) || std::isinf(eps2)) fail(TJ_ERR_INVALID, "eps2 must be finite and >= 0");
-    if (dtype == TJ_DTYPE_I16 && screen != TJ_SCREEN_INT8LIMB && screen != TJ_SCREEN_PLAIN)
-        fail(TJ_ERR_UNSUPPORTED, "int16 input needs the int8-limb or plain screen");
-    if (dtype == TJ_DTYPE_F32 && screen == TJ_SCREEN_INT8LIMB)
-        fail(TJ_ERR_UNSUPPORTED, "the int8-limb screen needs int16 (int14) input");
-    if (dtype == TJ_DTYPE_I16 && screen == TJ_SCREEN_PLAIN)
-        fail(TJ_ERR_UNSUPPORTED, "plain screen on int16 input is not provided; use TJ_SCREEN_INT8LIMB");
-    if (screen == TJ_SCREEN_INT8LIMB && !(eps2 == std::floor(eps2) && eps2 < 0x1p62))
-        fail(TJ_ERR_INVALID, "the int8-limb screen needs an integer eps2 below 2^62");
-    const int chunk_items = (opt && opt->chunk_items > 0) ? opt->chunk_items : 64;
+struct JoinIn {
+    const void* R;
+    const void* S;
+    long long nR, nS;
+    int d;
+    double eps2;
+};
 
-    memset(&res->stats, 0, sizeof(res->stats));
-    res->n_rows = nR;
-    res->n_cols = nS;
+// One or many joins.  Joins are grouped into classes of equal d; each class gets one
+// concatenated, Morton-sorted side per operand (joins stay contiguous), global tile tables, one
+// block-diagonal candidate list and one persistent screen launch over all classes.
+void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen, const tj_options* opt,
+               tj_result* res, cudaStream_t st) {
+    const bool self = mode != TJ_MODE_RS;
+    const int nj = (int)joins.size();
+    if (nj < 1) fail(TJ_ERR_INVALID, "no joins");
+    if (self && nj != 1) fail(TJ_ERR_INVALID, "self-join modes take one join");
+    const bool i8 = screen == TJ_SCREEN_INT8LIMB;
+    if (i8 && nj != 1) fail(TJ_ERR_UNSUPPORTED, "the int8-limb screen runs one join at a time");
+    if (dtype == TJ_DTYPE_I16 && !i8) fail(TJ_ERR_UNSUPPORTED, "int16 input needs the int8-limb screen");
+    if (dtype == TJ_DTYPE_F32 && i8) fail(TJ_ERR_UNSUPPORTED, "the int8-limb screen needs int16 (int14) input");
+    long long total_r = 0;
+    for (const auto& j : joins) {
+        if ((j.nR > 0 && !j.R) || (j.nS > 0 && !j.S)) fail(TJ_ERR_INVALID, "null input pointer");
+        if (j.d <= 0 || j.nR < 0 || j.nS < 0) fail(TJ_ERR_INVALID, "invalid shape");
+        if (j.nR >= (1ll << 32) || j.nS >= (1ll << 32)) fail(TJ_ERR_INVALID, "more than 2^32 - 1 rows per side");
+        if (!(j.eps2 >= 0.0) || std::isinf(j.eps2)) fail(TJ_ERR_INVALID, "eps2 must be finite and >= 0");
+        if (i8 && !(j.eps2 == std::floor(j.eps2) && j.eps2 < 0x1p62))
+            fail(TJ_ERR_INVALID, "the int8-limb screen needs an integer eps2 below 2^62");
+        total_r += j.nR;
+    }
+    const int chunk_items = (opt && opt->chunk_items > 0) ? opt->chunk_items : 64;
+    const int esize = dtype == TJ_DTYPE_I16 ? 2 : 4;
     tj_stats& S_ = res->stats;
-    S_.n_rows = nR;
-    S_.n_cols = nS;
-    S_.pairs_all = self ? nR * (nR - 1) / 2 : nR * nS;
-    if (nR == 0 || nS == 0) {
+    memset(&S_, 0, sizeof(S_));
+    res->njoins = nj;
+    res->n_rows = nj == 1 ? joins[0].nR : total_r;
+    res->n_cols = nj == 1 ? (self ? joins[0].nR : joins[0].nS) : 0;
+    S_.n_rows = res->n_rows;
+    S_.n_cols = res->n_cols;
+
+    // key space: join k owns [key_off[k], key_off[k] + nR_k * nS_k)
+    std::vector<unsigned long long> key_off(nj);
+    std::vector<long long> ncols(nj);
+    unsigned long long kspace = 0;
+    for (int k = 0; k < nj; ++k) {
+        const long long nc = self ? joins[k].nR : joins[k].nS;
+        key_off[k] = kspace;
+        ncols[k] = nc;
+        kspace += (unsigned long long)joins[k].nR * (unsigned long long)nc;
+        S_.pairs_all += self ? joins[k].nR * (joins[k].nR - 1) / 2 : joins[k].nR * joins[k].nS;
+    }
+    // classes of equal d (joins with an empty side contribute no pairs and are skipped)
+    std::vector<int> cls_d;
+    std::vector<std::vector<int>> cls_j;
+    for (int k = 0; k < nj; ++k) {
+        if (joins[k].nR == 0 || (!self && joins[k].nS == 0)) continue;
+        int c = -1;
+        for (size_t q = 0; q < cls_d.size(); ++q)
+            if (cls_d[q] == joins[k].d) c = (int)q;
+        if (c < 0) {
+            if ((int)cls_d.size() == kMaxClass) fail(TJ_ERR_UNSUPPORTED, "at most 4 distinct dimensions per batch");
+            cls_d.push_back(joins[k].d);
+            cls_j.emplace_back();
+            c = (int)cls_d.size() - 1;
+        }
+        cls_j[c].push_back(k);
+    }
+    const int ncls = (int)cls_d.size();
+    if (ncls == 0) {
         res->count = 0;
+        if (nj > 1) res->offsets.assign(nj + 1, 0);
         return;
     }
     Events ev;
     ev.rec(0, st);
     DBuf<Counters> ctr(1, st);
     launch(zero_counters, 1, 32, 0, st, ctr.p, 0);
-    DBuf<FrameParams> fp(1, st);
-    DBuf<float> center((size_t)d, st);
-    {
-        const void* srcs[2] = {R, S};
-        const long long ns[2] = {nR, nS};
-        compute_frame(srcs, ns, self ? 1 : 2, d, dtype, fp.p, center.p, st);
-    }
-    Side sR, sS_;
-    sR.src = R; sR.dtype = dtype; sR.n = nR; sR.d = d; sR.screen = screen;
-    prepare_side(sR, fp.p, center.p, st, &ctr.p->status);
-    Side* pS = &sR;
-    if (!self) {
-        sS_.src = S; sS_.dtype = dtype; sS_.n = nS; sS_.d = d; sS_.screen = screen;
-        prepare_side(sS_, fp.p, center.p, st, &ctr.p->status);
-        pS = &sS_;
-    }
-    TileSet tR, tS;
-    tile_stats(sR, kTileR, tR, st);
-    const bool i8 = screen == TJ_SCREEN_INT8LIMB;
-    tile_stats(*pS, i8 ? 128 : kTileS, tS, st);
-    ev.rec(1, st);
-    const JoinParams jp = make_params(eps2, d, sR.kpad, sR.split, nR, nS, self);
-    Candidates cand;
-    build_candidates(tR, tS, jp.Tp, self, chunk_items, cand, st);
-    ev.rec(6, st);
-    // distance evaluations of the candidate list (read back with the counters)
-    launch(pairs_screened_kernel, num_sms() * 4, 256, 0, st, cand.chunks.p, cand.dev_counts.p + 1, cand.jlist.p,
-                                                         tR.nvalid.p, tS.nvalid.p, &ctr.p->pad[0]);
-    TJ_CUDA(cudaGetLastError());
-    ev.rec(2, st);
 
-    JoinGeometry g{&sR, pS, &tR, &tS, &cand, jp};
+    struct Cls {
+        Side R, S;
+        TileSet tR, tS;
+        DBuf<float> XR, XS, center;
+        DBuf<FrameParams> fp;
+        DBuf<long long> rowoffR, rowoffS;
+    };
+    std::vector<std::unique_ptr<Cls>> C(ncls);
+    std::vector<uint4> rtiles, stiles;
+    ScreenInput g;
+    g.ncls = ncls;
+    std::vector<JoinParams> jps(nj);
+    for (int k = 0; k < nj; ++k) memset(&jps[k], 0, sizeof(JoinParams));
+    const int stile = i8 ? 128 : kTileS;
+    for (int c = 0; c < ncls; ++c) {
+        C[c].reset(new Cls());
+        Cls& K = *C[c];
+        const int d = cls_d[c];
+        const auto& J = cls_j[c];
+        const int njc = (int)J.size();
+        std::vector<long long> roR(njc + 1, 0), roS(njc + 1, 0);
+        for (int q = 0; q < njc; ++q) {
+            roR[q + 1] = roR[q] + joins[J[q]].nR;
+            roS[q + 1] = roS[q] + (self ? joins[J[q]].nR : joins[J[q]].nS);
+        }
+        const void* srcR = joins[J[0]].R;
+        const void* srcS = self ? joins[J[0]].R : joins[J[0]].S;
+        if (njc > 1) {   // concatenate the class's joins (one copy per side)
+            std::vector<const void*> pr, ps;
+            std::vector<long long> nr, ns;
+            for (int q = 0; q < njc; ++q) {
+                pr.push_back(joins[J[q]].R); nr.push_back(joins[J[q]].nR);
+                ps.push_back(joins[J[q]].S); ns.push_back(joins[J[q]].nS);
+            }
+            K.XR = DBuf<float>((size_t)roR[njc] * d, st);
+            K.XS = DBuf<float>((size_t)roS[njc] * d, st);
+            gather_rows(pr, nr, d, esize, K.XR.p, st);
+            gather_rows(ps, ns, d, esize, K.XS.p, st);
+            srcR = K.XR.p;
+            srcS = K.XS.p;
+            K.rowoffR = DBuf<long long>((size_t)njc + 1, st);
+            K.rowoffS = DBuf<long long>((size_t)njc + 1, st);
+            TJ_CUDA(cudaMemcpyAsync(K.rowoffR.p, roR.data(), (njc + 1) * 8, cudaMemcpyHostToDevice, st));
+            TJ_CUDA(cudaMemcpyAsync(K.rowoffS.p, roS.data(), (njc + 1) * 8, cudaMemcpyHostToDevice, st));
+        }
+        K.fp = DBuf<FrameParams>(1, st);
+        K.center = DBuf<float>((size_t)d, st);
+        {
+            const void* srcs[2] = {srcR, srcS};
+            const long long ns[2] = {roR[njc], roS[njc]};
+            compute_frame(srcs, ns, self ? 1 : 2, d, dtype, K.fp.p, K.center.p, st);
+        }
+        K.R.src = srcR; K.R.dtype = dtype; K.R.n = roR[njc]; K.R.d = d; K.R.screen = screen;
+        K.R.njc = njc; K.R.d_rowoff = njc > 1 ? K.rowoffR.p : nullptr;
+        prepare_side(K.R, K.fp.p, K.center.p, st, &ctr.p->status);
+        compute_perm_local(K.R, st);
+        Side* pS = &K.R;
+        if (!self) {
+            K.S.src = srcS; K.S.dtype = dtype; K.S.n = roS[njc]; K.S.d = d; K.S.screen = screen;
+            K.S.njc = njc; K.S.d_rowoff = njc > 1 ? K.rowoffS.p : nullptr;
+            prepare_side(K.S, K.fp.p, K.center.p, st, &ctr.p->status);
+            compute_perm_local(K.S, st);
+            pS = &K.S;
+        }
+        // tile tables: tiles never span two joins; sorted rows of join q are [ro[q], ro[q+1])
+        g.rbase[c] = (int)rtiles.size();
+        g.sbase[c] = (int)stiles.size();
+        for (int q = 0; q < njc; ++q) {
+            const int k = J[q];
+            for (long long t = 0; t * kTileR < joins[k].nR; ++t) {
+                const uint32_t r0 = (uint32_t)(roR[q] + t * kTileR);
+                const uint32_t nv = (uint32_t)std::min<long long>(kTileR, joins[k].nR - t * kTileR);
+                K.tR.h_row0.push_back(r0); K.tR.h_nvalid.push_back(nv); K.tR.h_join.push_back((uint32_t)k);
+                rtiles.push_back(make_uint4(r0, nv, (unsigned)k, (unsigned)c));
+            }
+            const long long nsk = self ? joins[k].nR : joins[k].nS;
+            for (long long t = 0; t * stile < nsk; ++t) {
+                const uint32_t r0 = (uint32_t)(roS[q] + t * stile);
+                const uint32_t nv = (uint32_t)std::min<long long>(stile, nsk - t * stile);
+                K.tS.h_row0.push_back(r0); K.tS.h_nvalid.push_back(nv); K.tS.h_join.push_back((uint32_t)k);
+                stiles.push_back(make_uint4(r0, nv, (unsigned)k, (unsigned)c));
+            }
+        }
+        tile_stats(K.R, kTileR, K.tR, st);
+        tile_stats(*pS, stile, K.tS, st);
+        for (int q = 0; q < njc; ++q) {
+            const int k = J[q];
+            jps[k] = make_params(joins[k].eps2, d, K.R.kpad, K.R.split, joins[k].nR, ncols[k], self);
+            jps[k].key_off = key_off[k];
+        }
+        g.R[c] = &K.R;
+        g.S[c] = pS;
+        g.tR[c] = &K.tR;
+        g.tS[c] = &K.tS;
+    }
+    g.ntR_total = (int)rtiles.size();
+    g.ntS_total = (int)stiles.size();
+    g.njoins = nj;
+    g.jp0 = jps[0];
+    g.T_int = (long long)joins[0].eps2;
+    DBuf<uint4> d_rt((size_t)g.ntR_total, st), d_st((size_t)g.ntS_total, st);
+    DBuf<JoinParams> d_jps((size_t)nj, st);
+    DBuf<unsigned long long> d_koff((size_t)nj, st);
+    DBuf<long long> d_cols((size_t)nj, st);
+    DBuf<const void*> d_rsrc((size_t)nj, st), d_ssrc((size_t)nj, st);
+    std::vector<const void*> hr(nj), hs(nj);
+    for (int k = 0; k < nj; ++k) { hr[k] = joins[k].R; hs[k] = self ? joins[k].R : joins[k].S; }
+    TJ_CUDA(cudaMemcpyAsync(d_rt.p, rtiles.data(), rtiles.size() * sizeof(uint4), cudaMemcpyHostToDevice, st));
+    TJ_CUDA(cudaMemcpyAsync(d_st.p, stiles.data(), stiles.size() * sizeof(uint4), cudaMemcpyHostToDevice, st));
+    TJ_CUDA(cudaMemcpyAsync(d_jps.p, jps.data(), nj * sizeof(JoinParams), cudaMemcpyHostToDevice, st));
+    TJ_CUDA(cudaMemcpyAsync(d_koff.p, key_off.data(), nj * 8, cudaMemcpyHostToDevice, st));
+    TJ_CUDA(cudaMemcpyAsync(d_cols.p, ncols.data(), nj * 8, cudaMemcpyHostToDevice, st));
+    TJ_CUDA(cudaMemcpyAsync(d_rsrc.p, hr.data(), nj * sizeof(void*), cudaMemcpyHostToDevice, st));
+    TJ_CUDA(cudaMemcpyAsync(d_ssrc.p, hs.data(), nj * sizeof(void*), cudaMemcpyHostToDevice, st));
+    g.rtiles = d_rt.p;
+    g.stiles = d_st.p;
+    g.jps = d_jps.p;
+    g.key_off = d_koff.p;
+    g.rsrc = d_rsrc.p;
+    g.ssrc = d_ssrc.p;
+    ev.rec(1, st);
+
+    // candidate tile pairs (block-diagonal over joins) and execution chunks
+    Candidates cand;
+    if (nj == 1) {
+        build_candidates(*g.tR[0], *g.tS[0], jps[0].Tp, self, chunk_items, cand, st);
+    } else {
+        std::vector<CandClassView> views(ncls);
+        for (int c = 0; c < ncls; ++c) {
+            const TileSet& a = *g.tR[c];
+            const TileSet& b = *g.tS[c];
+            views[c] = CandClassView{a.ctrT.p, a.loT.p, a.hiT.p, a.rad.p, b.ctrT.p, b.loT.p, b.hiT.p, b.rad.p,
+                                     a.ntiles, b.ntiles, g.rbase[c], g.sbase[c], cls_d[c], 0};
+        }
+        std::vector<CandBlock> blocks;
+        std::vector<double> tps;
+        std::vector<uint32_t> rsb(g.ntR_total, 0);
+        int words = 1;
+        std::vector<int> jr0(nj, -1), js0(nj, -1), jnr(nj, 0), jns(nj, 0), jcls(nj, 0);
+        for (int i = 0; i < g.ntR_total; ++i) {
+            const int k = (int)rtiles[i].z;
+            if (jr0[k] < 0) jr0[k] = i;
+            ++jnr[k];
+            jcls[k] = (int)rtiles[i].w;
+        }
+        for (int i = 0; i < g.ntS_total; ++i) {
+            const int k = (int)stiles[i].z;
+            if (js0[k] < 0) js0[k] = i;
+            ++jns[k];
+        }
+        for (int k = 0; k < nj; ++k) {
+            if (jr0[k] < 0 || js0[k] < 0) continue;
+            words = std::max(words, (jns[k] + 31) / 32);
+            for (int t = 0; t < jnr[k]; t += 16) {
+                blocks.push_back(CandBlock{(uint32_t)(jr0[k] + t), (uint32_t)std::min(16, jnr[k] - t),
+                                           (uint32_t)js0[k], (uint32_t)jns[k], (uint32_t)jcls[k], 0u});
+                tps.push_back(jps[k].Tp);
+            }
+            for (int t = 0; t < jnr[k]; ++t) rsb[jr0[k] + t] = (uint32_t)js0[k];
+        }
+        build_candidates_batched(views, blocks, tps, g.ntR_total, words, chunk_items, rsb, cand, st);
+    }
+    g.cand = &cand;
+    launch(pairs_screened_kernel, num_sms() * 4, 256, 0, st, (const uint4*)cand.chunks.p,
+           (const uint32_t*)(cand.dev_counts.p + 1), (const uint32_t*)cand.jlist.p, (const uint4*)d_rt.p,
+           (const uint4*)d_st.p, &ctr.p->pad[0]);
+    ev.rec(6, st);
+
+    // screen + refine with overflow-and-retry
+    unsigned long long sum_max = 0;
+    for (const auto& j : joins) sum_max += (unsigned long long)std::max(j.nR, self ? j.nR : j.nS);
+    const unsigned long long per = nj == 1 ? 64ull : 24ull;
     unsigned long long cap = (opt && opt->initial_capacity > 0) ? (unsigned long long)opt->initial_capacity
-                                                                : std::max<unsigned long long>(1ull << 20,
-                                                                      64ull * (unsigned long long)std::max(nR, nS));
-    unsigned long long bcap = cap;
+                                                                : std::max<unsigned long long>(1ull << 20, per * sum_max);
+    unsigned long long bcap = (opt && opt->initial_capacity > 0) ? cap : std::max<unsigned long long>(1ull << 20,
+                                                                                                   cap / (nj == 1 ? 1 : 8));
     DBuf<uint64_t> acc, band;
     Counters h;
     for (int attempt = 0;; ++attempt) {
@@ -308,7 +493,7 @@ void run_join(const void* R, long long nR, const void* S, long long nS, int d, i
         EmitBuffers eb{acc.p, cap, band.p, bcap, ctr.p};
         ev.rec(2, st);
         if (screen == TJ_SCREEN_PLAIN) screen_plain(g, eb, st);
-        else if (i8) screen_i8(g, eb, (long long)eps2, st);
+        else if (i8) screen_i8(g, eb, st);
         else screen_tc(g, eb, st);
         ev.rec(3, st);
         if (!i8) refine_band(g, eb, st);   // the int8-limb screen is exact: no band
@@ -331,26 +516,34 @@ void run_join(const void* R, long long nR, const void* S, long long nS, int d, i
     S_.rare_checks = (int64_t)h.rare_checks;
     band.reset();
 
-    // canonical order: (directed expansion) + radix sort on the trimmed key width
+    // canonical order
     unsigned long long slots = h.acc_reserved;
     long long nvalid = (long long)h.acc_valid;
-    unsigned long long max_key = (unsigned long long)nR * (unsigned long long)nS;   // + 1 > any valid key
     DBuf<uint64_t> keys;
     if (mode == TJ_MODE_DIRECTED) {
-        const unsigned long long nk = 2 * slots + (unsigned long long)nR;
+        const long long N = joins[0].nR;
+        const unsigned long long nk = 2 * slots + (unsigned long long)N;
         keys = DBuf<uint64_t>(nk, st);
-        expand_directed(acc.p, slots, keys.p, nR, st);
+        expand_directed(acc.p, slots, keys.p, N, st);
         acc.reset();
         slots = nk;
-        nvalid = 2 * nvalid + nR;
+        nvalid = 2 * nvalid + N;
     } else {
         keys = std::move(acc);
     }
-    const int bits = bits_for(max_key);   // sentinel low bits (all ones) exceed every valid key
+    const int bits = bits_for(kspace);   // sentinel low bits (all ones) exceed every valid key
     if (slots > 1) {
         DBuf<uint64_t> ktmp(slots, st);
         DBuf<uint32_t> ws(radix_workspace_elems(slots), st);
         radix_sort(keys.p, nullptr, ktmp.p, nullptr, slots, bits, ws.p, st);
+    }
+    if (nj > 1) {
+        DBuf<long long> offs((size_t)nj + 1, st);
+        batch_offsets(keys.p, nvalid, d_koff.p, nj, offs.p, st);
+        res->offsets.resize(nj + 1);
+        TJ_CUDA(cudaMemcpyAsync(res->offsets.data(), offs.p, (nj + 1) * 8, cudaMemcpyDeviceToHost, st));
+        res->d_keyoff = std::move(d_koff);
+        res->d_cols = std::move(d_cols);
     }
     ev.rec(5, st);
     TJ_CUDA(cudaStreamSynchronize(st));
@@ -379,7 +572,9 @@ int tj_join(const void* R, int64_t nR, const void* S, int64_t nS, int32_t d, int
     if (dtype != TJ_DTYPE_F32 && dtype != TJ_DTYPE_I16) fail(TJ_ERR_INVALID, "unknown dtype");
     if (opt && opt->flags != 0) fail(TJ_ERR_INVALID, "options.flags must be 0");
     std::unique_ptr<tj_result> res(new tj_result());
-    run_join(R, nR, S, nS, d, dtype, eps2, mode, screen, opt, res.get(), (cudaStream_t)stream);
+    std::vector<JoinIn> js{JoinIn{R, (const void*)(mode == TJ_MODE_RS ? S : R), nR, mode == TJ_MODE_RS ? nS : nR,
+                                  d, eps2}};
+    run_batch(js, dtype, mode, screen, opt, res.get(), (cudaStream_t)stream);
     *out = res.release();
     return TJ_OK;
     TJ_API_END
@@ -398,7 +593,7 @@ int tj_result_pairs(const tj_result* res, int64_t* i_out, int64_t* j_out, void* 
     if (!res) fail(TJ_ERR_INVALID, "null result");
     if (res->count == 0) return TJ_OK;
     if (!i_out || !j_out) fail(TJ_ERR_INVALID, "null output");
-    if (!res->offsets.empty()) fail(TJ_ERR_INVALID, "batched result: use tj_batch_pairs");
+    if (res->njoins > 1) fail(TJ_ERR_INVALID, "batched result: use tj_batch_pairs");
     decode_pairs(res->keys.p, res->count, res->n_cols, i_out, j_out, (cudaStream_t)stream);
     return TJ_OK;
     TJ_API_END
@@ -418,7 +613,7 @@ int tj_result_keys(const tj_result* res, uint64_t* keys_out, void* stream) {
 int tj_result_neighbor_table(const tj_result* res, uint32_t* counts_out, int64_t* flat_out, void* stream) {
     TJ_API_BEGIN
     if (!res || !counts_out) fail(TJ_ERR_INVALID, "null argument");
-    if (!res->offsets.empty()) fail(TJ_ERR_INVALID, "batched result: not supported");
+    if (res->njoins > 1) fail(TJ_ERR_INVALID, "batched result: not supported");
     cudaStream_t st = (cudaStream_t)stream;
     TJ_CUDA(cudaMemsetAsync(counts_out, 0, (size_t)res->n_rows * 4, st));
     if (res->count > 0)
@@ -520,9 +715,21 @@ void tj_index_free(tj_index* idx) {
 
 int tj_join_batched(const tj_batch_join* joins, int32_t njoins, int32_t screen, const tj_options* opt,
                     tj_result** out, void* stream) {
-    (void)joins; (void)njoins; (void)screen; (void)opt; (void)out; (void)stream;
-    g_last_error = "batched joins are not built in this version";
-    return TJ_ERR_UNSUPPORTED;
+    TJ_API_BEGIN
+    if (!out || (njoins > 0 && !joins)) fail(TJ_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (njoins < 1) fail(TJ_ERR_INVALID, "njoins must be >= 1");
+    if (screen < 0 || screen > 5 || screen == TJ_SCREEN_INT8LIMB) fail(TJ_ERR_UNSUPPORTED, "batched joins take FP32 screens");
+    if (opt && opt->flags != 0) fail(TJ_ERR_INVALID, "options.flags must be 0");
+    std::vector<JoinIn> js((size_t)njoins);
+    for (int k = 0; k < njoins; ++k) js[k] = JoinIn{joins[k].R, joins[k].S, joins[k].nR, joins[k].nS, joins[k].d, joins[k].eps2};
+    std::unique_ptr<tj_result> res(new tj_result());
+    run_batch(js, TJ_DTYPE_F32, TJ_MODE_RS, screen, opt, res.get(), (cudaStream_t)stream);
+    if (res->offsets.empty()) res->offsets.assign((size_t)njoins + 1, res->count);   // one join: [0, count)
+    if (njoins == 1) res->offsets[0] = 0;
+    *out = res.release();
+    return TJ_OK;
+    TJ_API_END
 }
 
 int tj_batch_offsets(const tj_result* res, int64_t* offsets_host) {
@@ -533,9 +740,18 @@ int tj_batch_offsets(const tj_result* res, int64_t* offsets_host) {
 }
 
 int tj_batch_pairs(const tj_result* res, int64_t* i_out, int64_t* j_out, void* stream) {
-    (void)res; (void)i_out; (void)j_out; (void)stream;
-    g_last_error = "batched joins are not built in this version";
-    return TJ_ERR_UNSUPPORTED;
+    TJ_API_BEGIN
+    if (!res) fail(TJ_ERR_INVALID, "null result");
+    if (res->count == 0) return TJ_OK;
+    if (!i_out || !j_out) fail(TJ_ERR_INVALID, "null output");
+    if (res->njoins == 1) {
+        decode_pairs(res->keys.p, res->count, res->n_cols, i_out, j_out, (cudaStream_t)stream);
+        return TJ_OK;
+    }
+    decode_pairs_batched(res->keys.p, res->count, res->d_keyoff.p, res->d_cols.p, res->njoins, i_out, j_out,
+                         (cudaStream_t)stream);
+    return TJ_OK;
+    TJ_API_END
 }
 
 const char* tj_last_error_string(void) { return g_last_error.c_str(); }

@@ -121,8 +121,19 @@ __global__ void frame_pick(int d, const float* var_ws, const float* lo_ws, const
     *fp = f;
 }
 
+TJ_DEV int join_of_row(const long long* rowoff, int njc, long long r) {   // last j with rowoff[j] <= r
+    int lo = 0, hi = njc - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (rowoff[mid] <= r) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Morton key of the indexed dimensions; with several joins concatenated in one side the join
+// index goes above bit 32, so every join's rows stay contiguous after the sort.
 __global__ void morton_keys(const void* src, int dtype, long long n, int d, const FrameParams* fpp, uint64_t* keys,
-                            uint32_t* vals) {
+                            uint32_t* vals, const long long* rowoff, int njc) {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
     const FrameParams fp = *fpp;
@@ -137,8 +148,32 @@ __global__ void morton_keys(const void* src, int dtype, long long n, int d, cons
     uint64_t key = 0;
     for (int b = fp.bits - 1; b >= 0; --b)
         for (int t = 0; t < fp.m; ++t) key = (key << 1) | ((c[t] >> b) & 1u);
+    if (njc > 1) key |= (uint64_t)join_of_row(rowoff, njc, r) << 32;
     keys[r] = key;
     vals[r] = (uint32_t)r;
+}
+
+__global__ void perm_local_kernel(const uint64_t* keys, const uint32_t* perm, const long long* rowoff, long long n,
+                                  uint32_t* out) {
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) out[r] = (uint32_t)((long long)perm[r] - rowoff[keys[r] >> 32]);
+}
+
+// Concatenate many row-major matrices (one per join) into one: row r of the output comes from the
+// source whose row range contains r.
+__global__ void gather_rows_kernel(const void* const* srcs, const long long* rowoff, int nsrc, long long nrows,
+                                   int row_bytes, uint8_t* dst) {
+    const long long r = (long long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (r >= nrows) return;
+    const int j = join_of_row(rowoff, nsrc, r);
+    const uint8_t* src = (const uint8_t*)srcs[j] + (size_t)(r - rowoff[j]) * row_bytes;
+    uint8_t* out = dst + (size_t)r * row_bytes;
+    if ((row_bytes & 3) == 0 && (((uintptr_t)src | (uintptr_t)out) & 3) == 0) {
+        for (int b = (threadIdx.x & 31) * 4; b < row_bytes; b += 128)
+            *(uint32_t*)(out + b) = *(const uint32_t*)(src + b);
+    } else {
+        for (int b = threadIdx.x & 31; b < row_bytes; b += 32) out[b] = src[b];
+    }
 }
 
 // Round to the 16-bit operand format; returns the rounded value as FP32 and its bit pattern.
@@ -248,12 +283,14 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
                                                          const float* yn, const float* zl, float* ctrT, float* loT,
                                                          float* hiT, float* rad, float* maxZ, float* maxE,
                                                          float* maxY, float* maxB, float* beta, float* maxZl,
-                                                         uint32_t* nvalid, uint32_t* row0) {
+                                                         uint32_t* nvalid, uint32_t* row0, const uint32_t* row0_in,
+                                                         const uint32_t* nvalid_in) {
     extern __shared__ float s_ctr[];   // [d]
     __shared__ float red[6][256];
     const int t = blockIdx.x;
-    const long long r0 = (long long)t * tile;
-    const int nv = (int)min((long long)tile, n - r0);
+    const bool tabled = row0_in != nullptr;   // batched sides: tiles never span two joins
+    const long long r0 = tabled ? (long long)row0_in[t] : (long long)t * tile;
+    const int nv = tabled ? (int)nvalid_in[t] : (int)min((long long)tile, n - r0);
     const double g = (double)(d + 2) * 0x1p-53;
     // per-dimension centroid and bounding box
     for (int k = threadIdx.x; k < d; k += blockDim.x) {
@@ -323,8 +360,10 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
         maxB[t] = red[3][0];
         beta[t] = red[4][0];
         maxZl[t] = red[5][0];
-        nvalid[t] = (uint32_t)max(nv, 0);
-        row0[t] = (uint32_t)r0;
+        if (!tabled) {
+            nvalid[t] = (uint32_t)max(nv, 0);
+            row0[t] = (uint32_t)r0;
+        }
     }
 }
 
@@ -393,6 +432,68 @@ __global__ void __launch_bounds__(256) cand_test(const float* rctrT, const float
     }
 }
 
+// Batched candidate test: one block = up to kCandI R tiles of one join against all S tiles of
+// the same join (tiles of different joins never pair).  Same rigorous bounds as cand_test.
+template <int kCandI>
+__global__ void __launch_bounds__(256) cand_test_batched(const CandBlock* blocks, const CandClassView* views,
+                                                         const double* Tp_blk, uint32_t* bitmap, int words) {
+    extern __shared__ float sm[];   // [3][kCandI][d]
+    const CandBlock cb = blocks[blockIdx.x];
+    const CandClassView cv = views[cb.cls];
+    const int d = cv.d;
+    float* sc = sm;
+    float* slo = sm + kCandI * d;
+    float* shi = sm + 2 * kCandI * d;
+    const int iloc0 = (int)cb.i0 - cv.rbase;   // class-local R tile of the block's first tile
+    for (int e = threadIdx.x; e < kCandI * d; e += blockDim.x) {
+        const int ii = e / d, k = e % d;
+        const bool ok = ii < (int)cb.ni;
+        sc[e] = ok ? cv.rctrT[(size_t)k * cv.ntR + iloc0 + ii] : 0.f;
+        slo[e] = ok ? cv.rloT[(size_t)k * cv.ntR + iloc0 + ii] : 0.f;
+        shi[e] = ok ? cv.rhiT[(size_t)k * cv.ntR + iloc0 + ii] : 0.f;
+    }
+    __syncthreads();
+    const double Tp = Tp_blk[blockIdx.x];
+    const float f = 1.f - (float)(d + 8) * 0x1p-23f;
+    const float rtp = (float)(sqrt(Tp) * (1.0 + 0x1p-20));
+    const float tpf = (float)(Tp * (1.0 + 0x1p-20));
+    const unsigned lane = threadIdx.x & 31;
+    for (int j0 = 0; j0 < (int)cb.nj; j0 += blockDim.x) {
+        const int jl = j0 + threadIdx.x;          // S tile index inside the join
+        const bool jok = jl < (int)cb.nj;
+        const int js = (int)cb.j0 - cv.sbase + jl;   // class-local S tile
+        float ball[kCandI], box[kCandI];
+#pragma unroll
+        for (int ii = 0; ii < kCandI; ++ii) ball[ii] = box[ii] = 0.f;
+        if (jok) {
+            for (int k = 0; k < d; ++k) {
+                const float cj = cv.sctrT[(size_t)k * cv.ntS + js];
+                const float lj = cv.sloT[(size_t)k * cv.ntS + js];
+                const float hj = cv.shiT[(size_t)k * cv.ntS + js];
+#pragma unroll
+                for (int ii = 0; ii < kCandI; ++ii) {
+                    const float dc = sc[ii * d + k] - cj;
+                    ball[ii] = fmaf(dc, dc, ball[ii]);
+                    const float gap = fmaxf(fmaxf(lj - shi[ii * d + k], slo[ii * d + k] - hj), 0.f);
+                    box[ii] = fmaf(gap, gap, box[ii]);
+                }
+            }
+        }
+        const float rj = jok ? cv.srad[js] : 0.f;
+        for (int ii = 0; ii < kCandI; ++ii) {
+            bool keep = jok && ii < (int)cb.ni;
+            if (keep) {
+                const float lb_box = box[ii] * f;
+                const float lb_ball = sqrtf(ball[ii] * f) * (1.f - 0x1p-20f) - cv.rrad[iloc0 + ii] - rj;
+                if (lb_box > tpf || lb_ball > rtp) keep = false;
+            }
+            const unsigned bits = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0 && ii < (int)cb.ni && (jl >> 5) < words)
+                bitmap[(size_t)(cb.i0 + ii) * words + (jl >> 5)] = bits;
+        }
+    }
+}
+
 __global__ void cand_count(const uint32_t* bitmap, int words, int ntR, uint32_t* cnt) {
     const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
@@ -404,11 +505,13 @@ __global__ void cand_count(const uint32_t* bitmap, int words, int ntR, uint32_t*
     if (lane == 0) cnt[I] = c;
 }
 
-__global__ void cand_fill(const uint32_t* bitmap, int words, int ntR, const uint32_t* off, uint32_t* jlist) {
+__global__ void cand_fill(const uint32_t* bitmap, int words, int ntR, const uint32_t* off, uint32_t* jlist,
+                          const uint32_t* rtile_sbase) {
     const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     if (I >= ntR) return;
     uint32_t pos = off[I];
+    const uint32_t sb = rtile_sbase ? rtile_sbase[I] : 0u;   // batched: global id of the join's first S tile
     for (int w0 = 0; w0 < words; w0 += 32) {
         const int w = w0 + lane;
         const unsigned bits = w < words ? bitmap[(size_t)I * words + w] : 0u;
@@ -418,7 +521,7 @@ __global__ void cand_fill(const uint32_t* bitmap, int words, int ntR, const uint
         while (b) {
             const int bit = __ffs(b) - 1;
             b &= b - 1;
-            jlist[p++] = (uint32_t)(w * 32 + bit);
+            jlist[p++] = sb + (uint32_t)(w * 32 + bit);
         }
         pos += tot;
     }
@@ -499,9 +602,13 @@ void prepare_side(Side& s, const FrameParams* fpd, const float* center, cudaStre
         DBuf<uint64_t> ktmp((size_t)n, st);
         DBuf<uint32_t> vtmp((size_t)n, st);
         DBuf<uint32_t> ws(radix_workspace_elems((size_t)n), st);
-        launch(morton_keys, (unsigned)((n + 255) / 256), 256, 0, st, s.src, s.dtype, n, s.d, fpd, s.keys.p, s.perm.p);
-        radix_sort(s.keys.p, s.perm.p, ktmp.p, vtmp.p, (size_t)n, 32, ws.p, st);
+        launch(morton_keys, (unsigned)((n + 255) / 256), 256, 0, st, s.src, s.dtype, n, s.d, fpd, s.keys.p, s.perm.p,
+               s.d_rowoff, s.njc);
+        int jbits = 0;
+        while ((1 << jbits) < s.njc) ++jbits;
+        radix_sort(s.keys.p, s.perm.p, ktmp.p, vtmp.p, (size_t)n, 32 + jbits, ws.p, st);
     }
+    s.emit = s.perm.p;
     const size_t rp = (size_t)s.rows_pad;
     const bool f16 = !i8 && s.screen != kScreenPlain;
     if (f16) s.op = DBuf<uint16_t>(rp * (size_t)s.kpad * (s.split ? 2 : 1), st);
@@ -534,7 +641,8 @@ void prepare_side(Side& s, const FrameParams* fpd, const float* center, cudaStre
 void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st) {
     ts.tile = tile;
     ts.d = s.d;
-    ts.ntiles = (int)((s.n + tile - 1) / tile);
+    const bool tabled = !ts.h_row0.empty();
+    ts.ntiles = tabled ? (int)ts.h_row0.size() : (int)((s.n + tile - 1) / tile);
     const size_t nt = (size_t)std::max(ts.ntiles, 1);
     ts.ctrT = DBuf<float>(nt * s.d, st);
     ts.loT = DBuf<float>(nt * s.d, st);
@@ -549,14 +657,44 @@ void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st) {
     ts.nvalid = DBuf<uint32_t>(nt, st);
     ts.row0 = DBuf<uint32_t>(nt, st);
     if (ts.ntiles == 0) return;
+    if (tabled) {
+        TJ_CUDA(cudaMemcpyAsync(ts.row0.p, ts.h_row0.data(), nt * 4, cudaMemcpyHostToDevice, st));
+        TJ_CUDA(cudaMemcpyAsync(ts.nvalid.p, ts.h_nvalid.data(), nt * 4, cudaMemcpyHostToDevice, st));
+    }
     const size_t smem = (size_t)s.d * sizeof(float);
     if (smem > 48 * 1024)
         TJ_CUDA(cudaFuncSetAttribute(tile_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     launch(tile_stats_kernel, ts.ntiles, 256, smem, st, s.src, s.dtype, s.n, s.d, tile, ts.ntiles, s.perm.p, s.nrm2.p,
-                                                    s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.zl.p, ts.ctrT.p, ts.loT.p,
-                                                    ts.hiT.p, ts.rad.p, ts.maxZ.p, ts.maxE.p, ts.maxY.p, ts.maxB.p,
-                                                    ts.beta.p, ts.maxZl.p, ts.nvalid.p, ts.row0.p);
-    TJ_CUDA(cudaGetLastError());
+           s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.zl.p, ts.ctrT.p, ts.loT.p, ts.hiT.p, ts.rad.p, ts.maxZ.p, ts.maxE.p,
+           ts.maxY.p, ts.maxB.p, ts.beta.p, ts.maxZl.p, ts.nvalid.p, ts.row0.p,
+           tabled ? (const uint32_t*)ts.row0.p : (const uint32_t*)nullptr,
+           tabled ? (const uint32_t*)ts.nvalid.p : (const uint32_t*)nullptr);
+}
+
+void gather_rows(const std::vector<const void*>& srcs, const std::vector<long long>& rows, int d, int esize,
+                 void* dst, cudaStream_t st) {
+    const int ns = (int)srcs.size();
+    std::vector<long long> off(ns + 1, 0);
+    for (int k = 0; k < ns; ++k) off[k + 1] = off[k] + rows[k];
+    DBuf<const void*> dsrc((size_t)ns, st);
+    DBuf<long long> doff((size_t)ns + 1, st);
+    TJ_CUDA(cudaMemcpyAsync(dsrc.p, srcs.data(), ns * sizeof(void*), cudaMemcpyHostToDevice, st));
+    TJ_CUDA(cudaMemcpyAsync(doff.p, off.data(), (ns + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+    const long long n = off[ns];
+    if (n == 0) return;
+    launch(gather_rows_kernel, (unsigned)((n + 7) / 8), 256, 0, st, (const void* const*)dsrc.p,
+           (const long long*)doff.p, ns, n, d * esize, (uint8_t*)dst);
+}
+
+void compute_perm_local(Side& s, cudaStream_t st) {
+    if (s.njc <= 1 || s.n == 0) {
+        s.emit = s.perm.p;
+        return;
+    }
+    s.perm_local = DBuf<uint32_t>((size_t)s.n, st);
+    launch(perm_local_kernel, (unsigned)((s.n + 255) / 256), 256, 0, st, s.keys.p, s.perm.p, s.d_rowoff, s.n,
+           s.perm_local.p);
+    s.emit = s.perm_local.p;
 }
 
 void build_candidates(const TileSet& tr, const TileSet& ts, double Tp, bool self_join, int chunk_items,
@@ -589,7 +727,8 @@ void build_candidates(const TileSet& tr, const TileSet& ts, double Tp, bool self
     launch(cand_count, (unsigned)((ntR * 32 + 255) / 256), 256, 0, st, bitmap.p, words, ntR, c.cnt.p);
     DBuf<uint32_t> sws(scan_workspace_elems((size_t)ntR) + 4, st);
     exclusive_scan_u32(c.cnt.p, c.off.p, (size_t)ntR, c.dev_counts.p, sws.p, st);
-    launch(cand_fill, (unsigned)((ntR * 32 + 255) / 256), 256, 0, st, bitmap.p, words, ntR, c.off.p, c.jlist.p);
+    launch(cand_fill, (unsigned)((ntR * 32 + 255) / 256), 256, 0, st, bitmap.p, words, ntR, c.off.p, c.jlist.p,
+           (const uint32_t*)nullptr);
     // chunks: (w, I) order so that concurrently running CTAs share the same S window
     DBuf<uint32_t> nch((size_t)ntR, st), cbase((size_t)ntR, st);
     launch(chunk_counts, (unsigned)((ntR + 255) / 256), 256, 0, st, c.cnt.p, ntR, chunk_items, nch.p);
@@ -604,6 +743,59 @@ void build_candidates(const TileSet& tr, const TileSet& ts, double Tp, bool self
     launch(chunk_emit, (unsigned)((cap + 255) / 256), 256, 0, st, keys.p, cap, c.dev_counts.p + 1, c.cnt.p, c.off.p,
                                                                chunk_items, c.chunks.p);
     TJ_CUDA(cudaGetLastError());
+}
+
+void build_candidates_batched(const std::vector<CandClassView>& classes, const std::vector<CandBlock>& blocks,
+                              const std::vector<double>& Tp_per_block, int ntR_total, int words, int chunk_items,
+                              const std::vector<uint32_t>& rtile_sbase, Candidates& c, cudaStream_t st) {
+    const int ntR = ntR_total;
+    const int nb = (int)blocks.size();
+    c.cnt = DBuf<uint32_t>((size_t)std::max(ntR, 1), st);
+    c.off = DBuf<uint32_t>((size_t)std::max(ntR, 1), st);
+    c.dev_counts = DBuf<uint32_t>(2, st);
+    TJ_CUDA(cudaMemsetAsync(c.dev_counts.p, 0, 2 * sizeof(uint32_t), st));
+    size_t maxc = 0;
+    for (const auto& b : blocks) maxc += (size_t)b.ni * b.nj;
+    c.jlist = DBuf<uint32_t>(std::max<size_t>(maxc, 1), st);
+    c.chunks_cap = maxc / (size_t)chunk_items + (size_t)ntR + 1;
+    c.chunks = DBuf<uint4>(c.chunks_cap, st);
+    if (ntR == 0 || nb == 0) return;
+    int dmax = 1;
+    for (const auto& v : classes) dmax = std::max(dmax, v.d);
+    DBuf<CandBlock> dblk((size_t)nb, st);
+    DBuf<CandClassView> dview(classes.size(), st);
+    DBuf<double> dtp((size_t)nb, st);
+    DBuf<uint32_t> dsb((size_t)ntR, st);
+    TJ_CUDA(cudaMemcpyAsync(dblk.p, blocks.data(), nb * sizeof(CandBlock), cudaMemcpyHostToDevice, st));
+    TJ_CUDA(cudaMemcpyAsync(dview.p, classes.data(), classes.size() * sizeof(CandClassView), cudaMemcpyHostToDevice,
+                            st));
+    TJ_CUDA(cudaMemcpyAsync(dtp.p, Tp_per_block.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
+    TJ_CUDA(cudaMemcpyAsync(dsb.p, rtile_sbase.data(), ntR * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    DBuf<uint32_t> bitmap((size_t)ntR * words, st);
+    TJ_CUDA(cudaMemsetAsync(bitmap.p, 0, bitmap.bytes(), st));
+    const size_t smem = (size_t)3 * 16 * dmax * sizeof(float);
+    if (smem > 200 * 1024) fail(-7, "dimension too large for the batched candidate test");
+    TJ_CUDA(cudaFuncSetAttribute(cand_test_batched<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    launch(cand_test_batched<16>, nb, 256, smem, st, (const CandBlock*)dblk.p, (const CandClassView*)dview.p,
+           (const double*)dtp.p, bitmap.p, words);
+    launch(cand_count, (unsigned)((ntR * 32 + 255) / 256), 256, 0, st, bitmap.p, words, ntR, c.cnt.p);
+    DBuf<uint32_t> sws(scan_workspace_elems((size_t)ntR) + 4, st);
+    exclusive_scan_u32(c.cnt.p, c.off.p, (size_t)ntR, c.dev_counts.p, sws.p, st);
+    launch(cand_fill, (unsigned)((ntR * 32 + 255) / 256), 256, 0, st, bitmap.p, words, ntR, c.off.p, c.jlist.p,
+           (const uint32_t*)dsb.p);
+    DBuf<uint32_t> nch((size_t)ntR, st), cbase((size_t)ntR, st);
+    launch(chunk_counts, (unsigned)((ntR + 255) / 256), 256, 0, st, c.cnt.p, ntR, chunk_items, nch.p);
+    exclusive_scan_u32(nch.p, cbase.p, (size_t)ntR, c.dev_counts.p + 1, sws.p, st);
+    const size_t cap = c.chunks_cap;
+    DBuf<uint64_t> keys(cap, st), ktmp(cap, st);
+    DBuf<uint32_t> vals(cap, st), vtmp(cap, st);
+    launch(fill_keys_max, (unsigned)((cap + 255) / 256), 256, 0, st, keys.p, vals.p, (size_t)0, cap,
+           (const uint32_t*)(c.dev_counts.p + 1));
+    launch(chunk_keys, (unsigned)((ntR + 255) / 256), 256, 0, st, nch.p, cbase.p, ntR, cap, keys.p, vals.p);
+    DBuf<uint32_t> rws(radix_workspace_elems(cap), st);
+    radix_sort(keys.p, vals.p, ktmp.p, vtmp.p, cap, 48, rws.p, st);
+    launch(chunk_emit, (unsigned)((cap + 255) / 256), 256, 0, st, keys.p, cap, (const uint32_t*)(c.dev_counts.p + 1),
+           c.cnt.p, c.off.p, chunk_items, c.chunks.p);
 }
 
 }  // namespace tj

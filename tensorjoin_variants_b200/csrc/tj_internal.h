@@ -70,7 +70,11 @@ struct Side {
     int kpad = 0;                // operand row length in elements (multiple of 64; int8: 128)
     int split = 0;               // 1: operand rows are [z_hi | z_lo] (2 * kpad elements)
     long long rows_pad = 0;      // operand rows (multiple of 256)
-    DBuf<uint32_t> perm;         // [n] sorted position -> original row
+    DBuf<uint32_t> perm;         // [n] sorted position -> row of the side's source matrix
+    DBuf<uint32_t> perm_local;   // [n] sorted position -> row id inside its own join (batched sides)
+    const uint32_t* emit = nullptr;   // ids written into pair keys: perm (one join) or perm_local
+    const long long* d_rowoff = nullptr;   // device [njc + 1]: first source row of each join (batched)
+    int njc = 1;                 // joins concatenated in this side
     DBuf<uint64_t> keys;         // [n] Morton keys (sorted)
     DBuf<uint16_t> op;           // [rows_pad, kpad or 2*kpad] bf16 / fp16 operand of x - centre
     DBuf<int8_t> op8;            // [rows_pad, 2*kpad] int8 limbs [hi | lo] (int8 limb screen)
@@ -95,6 +99,7 @@ struct TileSet {
     DBuf<float> maxZ, maxE, maxY, maxB, beta, maxZl;  // [ntiles] maxima of the row bounds
     DBuf<uint32_t> nvalid;  // [ntiles] rows of the tile that are real points
     DBuf<uint32_t> row0;    // [ntiles] first sorted row of the tile
+    std::vector<uint32_t> h_row0, h_nvalid, h_join;   // host tile tables (batched sides; empty: uniform tiles)
 };
 
 // Candidate tile pairs grouped by R tile, cut into chunks scheduled J-window-major.
@@ -125,6 +130,23 @@ void prepare_side(Side& s, const FrameParams* fp_dev, const float* center, cudaS
 void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st);
 void build_candidates(const TileSet& tr, const TileSet& ts, double T, bool self_join, int chunk_items,
                       Candidates& c, cudaStream_t st);
+void gather_rows(const std::vector<const void*>& srcs, const std::vector<long long>& rows, int d, int esize,
+                 void* dst, cudaStream_t st);
+void compute_perm_local(Side& s, cudaStream_t st);
+
+// Candidate tile pairs of many joins at once (block-diagonal: tiles only pair within their join).
+struct CandBlock {              // one cand_test block: up to 16 R tiles of one join against all its S tiles
+    uint32_t i0, ni;            // first global R tile, tiles in the block
+    uint32_t j0, nj;            // first global S tile of the join, S tiles of the join
+    uint32_t cls, pad;          // class of the join (selects the tile statistics arrays)
+};
+struct CandClassView {          // tile statistics of one class, indexed by class-local tile ids
+    const float *rctrT, *rloT, *rhiT, *rrad, *sctrT, *sloT, *shiT, *srad;
+    int ntR, ntS, rbase, sbase, d, pad;
+};
+void build_candidates_batched(const std::vector<CandClassView>& classes, const std::vector<CandBlock>& blocks,
+                              const std::vector<double>& Tp_per_block, int ntR_total, int words, int chunk_items,
+                              const std::vector<uint32_t>& rtile_sbase, Candidates& c, cudaStream_t st);
 
 // ------------------------------------------------------------------ screen / refine / emit
 struct EmitBuffers {
@@ -135,23 +157,43 @@ struct EmitBuffers {
     Counters* ctr = nullptr;
 };
 
-struct JoinGeometry {
-    const Side* R;
-    const Side* S;
-    const TileSet* tR;
-    const TileSet* tS;
-    const Candidates* cand;
-    JoinParams jp;
+constexpr int kMaxClass = 4;
+
+// Everything a screen launch needs: up to kMaxClass classes (same d inside a class) of prepared
+// sides, global R / S tile tables (row0, nvalid, join, class), the global chunk list, per-join
+// parameters, and per-join source pointers for the FP64 refinement.
+struct ScreenInput {
+    int ncls = 0;
+    const Side* R[kMaxClass] = {};
+    const Side* S[kMaxClass] = {};
+    const TileSet* tR[kMaxClass] = {};
+    const TileSet* tS[kMaxClass] = {};
+    int rbase[kMaxClass] = {}, sbase[kMaxClass] = {};   // global tile id of each class's first tile
+    int ntR_total = 0, ntS_total = 0;
+    const uint4* rtiles = nullptr;      // device [ntR_total]: (row0 in class, nvalid, join, class)
+    const uint4* stiles = nullptr;      // device [ntS_total]
+    const Candidates* cand = nullptr;
+    const JoinParams* jps = nullptr;    // device [njoins]
+    int njoins = 0;
+    const unsigned long long* key_off = nullptr;   // device [njoins]: ascending key offsets
+    const void* const* rsrc = nullptr;  // device [njoins]: caller's R rows of each join
+    const void* const* ssrc = nullptr;  // device [njoins]
+    long long T_int = 0;                // integer threshold (int8-limb screen, single join)
+    JoinParams jp0{};                   // host copy of join 0's parameters (single-join kernels)
 };
 
-void screen_tc(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st);
-void screen_plain(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st);
-void screen_i8(const JoinGeometry& g, const EmitBuffers& eb, long long T, cudaStream_t st);
-void refine_band(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st);
+void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);
+void screen_plain(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);
+void screen_i8(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);
+void refine_band(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);
 void expand_directed(const uint64_t* upper, unsigned long long n_upper_slots, uint64_t* out, long long N,
                      cudaStream_t st);
 void decode_pairs(const uint64_t* keys, long long n, long long n_cols, int64_t* i_out, int64_t* j_out,
                   cudaStream_t st);
+void decode_pairs_batched(const uint64_t* keys, long long n, const unsigned long long* key_off,
+                          const long long* n_cols, int njoins, int64_t* i_out, int64_t* j_out, cudaStream_t st);
+void batch_offsets(const uint64_t* keys, long long n, const unsigned long long* key_off, int njoins,
+                   long long* offsets, cudaStream_t st);
 
 int num_sms();
 

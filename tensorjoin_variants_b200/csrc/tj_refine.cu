@@ -14,6 +14,9 @@
 // the same FP64 refinement of band pairs.  It plays the role of the reference's
 // GDS-Join FP64 grid join / FP32-first control (adapters/gds_g2a/kernel.cu:314-386,
 // g15_strong_control_20260905/src/fp32_first.py:104-157).
+#include <cstring>
+#include <vector>
+
 #include "tj_emit.cuh"
 #include "tj_internal.h"
 
@@ -26,21 +29,23 @@ constexpr int kPT = 256;                // threads: 16 x 16
 constexpr int kPR = 8, kPC = 16;        // micro-tile: 8 rows x 16 cols per thread
 constexpr int kPK = 16;                 // k chunk
 
+struct PlainClass {
+    const float* rx;     // [rows_pad, d] sorted FP32 rows (R side of the class)
+    const float* sx;     // [rows_pad, d] sorted FP32 rows (S side)
+    const uint32_t* r_emit;
+    const uint32_t* s_emit;
+    int d;
+};
+
 struct PlainArgs {
     const uint4* chunks;
     const uint32_t* nchunks;
     const uint32_t* jlist;
-    const float* rx;     // [rows_pad, d] sorted FP32 rows (R)
-    const float* sx;     // [rows_pad, d] sorted FP32 rows (S)
-    const uint32_t* r_row0;
-    const uint32_t* r_nvalid;
-    const uint32_t* r_perm;
-    const uint32_t* s_row0;
-    const uint32_t* s_nvalid;
-    const uint32_t* s_perm;
-    int d;
-    float tin, tout;     // certified-in / certified-out thresholds on the FP32 sum
-    JoinParams jp;
+    const uint4* rtiles;        // (row0, nvalid, join, class) per global R tile
+    const uint4* stiles;
+    const JoinParams* jps;
+    const float2* thr;          // per join: certified-in / certified-out thresholds on the FP32 sum
+    PlainClass cls[kMaxClass];
     uint64_t* acc;
     unsigned long long acc_cap;
     uint64_t* band;
@@ -57,28 +62,33 @@ __global__ void __launch_bounds__(kPT, 1) plain_kernel(const PlainArgs a) {
     unsigned long long n_items = 0, n_screen_acc = 0;
     for (unsigned c = blockIdx.x; c < nchunks; c += gridDim.x) {
         const uint4 ch = a.chunks[c];
-        const unsigned I = ch.x;
-        const unsigned r0 = a.r_row0[I], nvI = a.r_nvalid[I];
+        const uint4 rt = a.rtiles[ch.x];
+        const PlainClass& pc = a.cls[rt.w];
+        const JoinParams jp = a.jps[rt.z];
+        const float2 th = a.thr[rt.z];
+        const int d = pc.d;
+        const unsigned r0 = rt.x, nvI = rt.y;
         for (unsigned e = ch.y; e < ch.z; ++e) {
             const unsigned J = a.jlist[e];
-            const unsigned c0 = a.s_row0[J], nvJ = a.s_nvalid[J];
+            const uint4 stt = a.stiles[J];
+            const unsigned c0 = stt.x, nvJ = stt.y;
             float acc[kPR][kPC];
 #pragma unroll
             for (int i = 0; i < kPR; ++i)
 #pragma unroll
                 for (int j = 0; j < kPC; ++j) acc[i][j] = 0.f;
-            for (int k0 = 0; k0 < a.d; k0 += kPK) {
+            for (int k0 = 0; k0 < d; k0 += kPK) {
                 __syncthreads();
                 for (int idx = threadIdx.x; idx < kPK * kTileR; idx += kPT) {
                     const int r = idx / kPK, k = idx % kPK;
-                    sR[k][r] = (k0 + k < a.d) ? a.rx[(size_t)(r0 + r) * a.d + k0 + k] : 0.f;
+                    sR[k][r] = (k0 + k < d) ? pc.rx[(size_t)(r0 + r) * d + k0 + k] : 0.f;
                 }
                 for (int idx = threadIdx.x; idx < kPK * kTileS; idx += kPT) {
                     const int r = idx / kPK, k = idx % kPK;
-                    sS[k][r] = (k0 + k < a.d) ? a.sx[(size_t)(c0 + r) * a.d + k0 + k] : 0.f;
+                    sS[k][r] = (k0 + k < d) ? pc.sx[(size_t)(c0 + r) * d + k0 + k] : 0.f;
                 }
                 __syncthreads();
-                const int kmax = min(kPK, a.d - k0);
+                const int kmax = min(kPK, d - k0);
                 for (int k = 0; k < kmax; ++k) {
                     float rv[kPR], sv[kPC];
 #pragma unroll
@@ -105,9 +115,9 @@ __global__ void __launch_bounds__(kPT, 1) plain_kernel(const PlainArgs a) {
                         const int i = g * 2 + h;
                         const unsigned row = i * 16 + ty, col = j * 16 + tx;
                         const float s = acc[i][j];
-                        if (s > a.tout || row >= nvI || col >= nvJ) continue;
-                        if (a.jp.self_join && c0 + col <= r0 + row) continue;
-                        if (s <= a.tin) amask |= 1u << (h * 16 + j);
+                        if (s > th.y || row >= nvI || col >= nvJ) continue;
+                        if (jp.self_join && c0 + col <= r0 + row) continue;
+                        if (s <= th.x) amask |= 1u << (h * 16 + j);
                         else bmask |= 1u << (h * 16 + j);
                     }
                 unsigned ta, tb;
@@ -120,7 +130,7 @@ __global__ void __launch_bounds__(kPT, 1) plain_kernel(const PlainArgs a) {
                         const int b = __ffs(mk) - 1;
                         mk &= mk - 1;
                         const unsigned row = (g * 2 + (b >> 4)) * 16 + ty, col = (b & 15) * 16 + tx;
-                        if (pos < a.acc_cap) a.acc[pos] = pair_key(a.jp, a.r_perm[r0 + row], a.s_perm[c0 + col]);
+                        if (pos < a.acc_cap) a.acc[pos] = pair_key(jp, pc.r_emit[r0 + row], pc.s_emit[c0 + col]);
                         ++pos;
                     }
                     n_screen_acc += __popc(amask);
@@ -132,7 +142,7 @@ __global__ void __launch_bounds__(kPT, 1) plain_kernel(const PlainArgs a) {
                         const int b = __ffs(mk) - 1;
                         mk &= mk - 1;
                         const unsigned row = (g * 2 + (b >> 4)) * 16 + ty, col = (b & 15) * 16 + tx;
-                        if (pos < a.band_cap) a.band[pos] = pair_key(a.jp, a.r_perm[r0 + row], a.s_perm[c0 + col]);
+                        if (pos < a.band_cap) a.band[pos] = pair_key(jp, pc.r_emit[r0 + row], pc.s_emit[c0 + col]);
                         ++pos;
                     }
                 }
@@ -156,10 +166,11 @@ __global__ void __launch_bounds__(kPT, 1) plain_kernel(const PlainArgs a) {
 struct RefineArgs {
     const uint64_t* band;
     unsigned long long band_cap;
-    const float* R;       // caller's rows, original order
-    const float* S;
-    int d;
-    JoinParams jp;
+    const JoinParams* jps;              // per join
+    const unsigned long long* key_off;  // ascending key offset of each join
+    int njoins;
+    const void* const* rsrc;            // caller's rows of each join, original order
+    const void* const* ssrc;
     uint64_t* acc;
     unsigned long long acc_cap;
     Counters* ctr;
@@ -201,10 +212,18 @@ __global__ void refine_kernel(const RefineArgs a) {
         if (idx < n) {
             key = a.band[idx];
             if (key != kSentinel) {
-                const uint64_t local = key - a.jp.key_off;
-                const uint64_t i = local / (uint64_t)a.jp.n_cols, j = local - i * (uint64_t)a.jp.n_cols;
-                const double d2 = seq_d2(a.R + (size_t)i * a.d, a.S + (size_t)j * a.d, a.d);
-                ok = d2 <= a.jp.T;
+                int lo = 0, hi = a.njoins - 1;   // join owning the key: last offset <= key
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (a.key_off[mid] <= key) lo = mid; else hi = mid - 1;
+                }
+                const JoinParams& jp = a.jps[lo];
+                const uint64_t local = key - jp.key_off;
+                const uint64_t i = local / (uint64_t)jp.n_cols, j = local - i * (uint64_t)jp.n_cols;
+                const float* R = (const float*)a.rsrc[lo];
+                const float* S = (const float*)a.ssrc[lo];
+                const double d2 = seq_d2(R + (size_t)i * jp.d, S + (size_t)j * jp.d, jp.d);
+                ok = d2 <= jp.T;
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -250,58 +269,100 @@ __global__ void decode_kernel(const uint64_t* keys, long long n, long long n_col
     jo[t] = (int64_t)(k - i * (uint64_t)n_cols);
 }
 
+__global__ void decode_batched_kernel(const uint64_t* keys, long long n, const unsigned long long* key_off,
+                                     const long long* n_cols, int njoins, int64_t* io, int64_t* jo) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint64_t k = keys[t];
+    int lo = 0, hi = njoins - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (key_off[mid] <= k) lo = mid; else hi = mid - 1;
+    }
+    const uint64_t local = k - key_off[lo];
+    const uint64_t i = local / (uint64_t)n_cols[lo];
+    io[t] = (int64_t)i;
+    jo[t] = (int64_t)(local - i * (uint64_t)n_cols[lo]);
+}
+
+// offsets[k] = first position of a key >= key_off[k] in the sorted keys; offsets[njoins] = n.
+__global__ void batch_offsets_kernel(const uint64_t* keys, long long n, const unsigned long long* key_off,
+                                     int njoins, long long* offsets) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > njoins) return;
+    if (k == njoins) { offsets[k] = n; return; }
+    long long lo = 0, hi = n;
+    const uint64_t v = key_off[k];
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (keys[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    offsets[k] = lo;
+}
+
 }  // namespace
 
-void screen_plain(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st) {
-    const Side& R = *g.R;
-    const Side& S = *g.S;
-    if (R.screen != kScreenPlain || S.screen != kScreenPlain) fail(-1, "screen_plain needs FP32 sides");
+void screen_plain(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     PlainArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int c = 0; c < g.ncls; ++c) {
+        const Side& R = *g.R[c];
+        const Side& S = *g.S[c];
+        if (R.screen != kScreenPlain || S.screen != kScreenPlain) fail(-1, "screen_plain needs FP32 sides");
+        a.cls[c].rx = R.xs.p;
+        a.cls[c].sx = S.xs.p;
+        a.cls[c].r_emit = R.emit;
+        a.cls[c].s_emit = S.emit;
+        a.cls[c].d = R.d;
+    }
+    // per join: FP32 sum of d squared FP32 differences with FMA: |s - D| <= gamma_{d+2} D + d 2^-148 (u = 2^-24)
+    std::vector<JoinParams> hj((size_t)g.njoins);
+    TJ_CUDA(cudaMemcpyAsync(hj.data(), g.jps, g.njoins * sizeof(JoinParams), cudaMemcpyDeviceToHost, st));
+    TJ_CUDA(cudaStreamSynchronize(st));
+    std::vector<float2> th((size_t)g.njoins);
+    for (int k = 0; k < g.njoins; ++k) {
+        const double u = 0x1p-24, nu = (double)(hj[k].d + 4) * u;
+        const double gam = nu / (1.0 - nu);
+        const double tiny = (double)(hj[k].d + 4) * 0x1p-147;
+        const double tin = (hj[k].Tm - tiny) * (1.0 - gam) * (1.0 - 0x1p-30);
+        const double tout = (hj[k].Tp + tiny) * (1.0 + gam) * (1.0 + 0x1p-30) + tiny;
+        float fin = tin > 0 ? (float)tin : -1.f;   // nearest, then nudged to stay a lower bound
+        if (fin > 0 && (double)fin > tin) fin = nextafterf(fin, 0.f);
+        float fout = (float)tout;
+        if ((double)fout < tout) fout = nextafterf(fout, INFINITY);
+        th[k] = make_float2(fin, fout);
+    }
+    DBuf<float2> dth((size_t)g.njoins, st);
+    TJ_CUDA(cudaMemcpyAsync(dth.p, th.data(), g.njoins * sizeof(float2), cudaMemcpyHostToDevice, st));
     a.chunks = g.cand->chunks.p;
     a.nchunks = g.cand->dev_counts.p + 1;
     a.jlist = g.cand->jlist.p;
-    a.rx = R.xs.p;
-    a.sx = S.xs.p;
-    a.r_row0 = g.tR->row0.p;
-    a.r_nvalid = g.tR->nvalid.p;
-    a.r_perm = R.perm.p;
-    a.s_row0 = g.tS->row0.p;
-    a.s_nvalid = g.tS->nvalid.p;
-    a.s_perm = S.perm.p;
-    a.d = R.d;
-    // FP32 sum of d squared FP32 differences with FMA: |s - D| <= gamma_{d+2} D + d 2^-148 (u = 2^-24)
-    const double u = 0x1p-24, nu = (double)(R.d + 4) * u;
-    const double gam = nu / (1.0 - nu);
-    const double tiny = (double)(R.d + 4) * 0x1p-147;
-    const double tin = (g.jp.Tm - tiny) * (1.0 - gam) * (1.0 - 0x1p-30);
-    const double tout = (g.jp.Tp + tiny) * (1.0 + gam) * (1.0 + 0x1p-30) + tiny;
-    a.tin = tin > 0 ? (float)tin : -1.f;    // rounding to nearest then nudging down keeps it a lower bound
-    if (a.tin > 0 && (double)a.tin > tin) a.tin = nextafterf(a.tin, 0.f);
-    a.tout = (float)tout;
-    if ((double)a.tout < tout) a.tout = nextafterf(a.tout, INFINITY);
-    a.jp = g.jp;
+    a.rtiles = g.rtiles;
+    a.stiles = g.stiles;
+    a.jps = g.jps;
+    a.thr = dth.p;
     a.acc = eb.acc;
     a.acc_cap = eb.acc_cap;
     a.band = eb.band;
     a.band_cap = eb.band_cap;
     a.ctr = eb.ctr;
     launch(plain_kernel, num_sms() * 2, kPT, 0, st, a);
-    TJ_CUDA(cudaGetLastError());
+    TJ_CUDA(cudaStreamSynchronize(st));   // the host threshold table is uploaded from this frame
 }
 
-void refine_band(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st) {
+void refine_band(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     RefineArgs a;
     a.band = eb.band;
     a.band_cap = eb.band_cap;
-    a.R = (const float*)g.R->src;
-    a.S = (const float*)g.S->src;
-    a.d = g.R->d;
-    a.jp = g.jp;
+    a.jps = g.jps;
+    a.key_off = g.key_off;
+    a.njoins = g.njoins;
+    a.rsrc = g.rsrc;
+    a.ssrc = g.ssrc;
     a.acc = eb.acc;
     a.acc_cap = eb.acc_cap;
     a.ctr = eb.ctr;
     launch(refine_kernel, num_sms() * 8, 256, 0, st, a);
-    TJ_CUDA(cudaGetLastError());
 }
 
 void expand_directed(const uint64_t* upper, unsigned long long slots, uint64_t* out, long long N, cudaStream_t st) {
@@ -309,6 +370,18 @@ void expand_directed(const uint64_t* upper, unsigned long long slots, uint64_t* 
     if (n == 0) return;
     launch(expand_directed_kernel, (unsigned)((n + 255) / 256), 256, 0, st, upper, slots, out, N);
     TJ_CUDA(cudaGetLastError());
+}
+
+void decode_pairs_batched(const uint64_t* keys, long long n, const unsigned long long* key_off,
+                          const long long* n_cols, int njoins, int64_t* i_out, int64_t* j_out, cudaStream_t st) {
+    if (n <= 0) return;
+    launch(decode_batched_kernel, (unsigned)((n + 255) / 256), 256, 0, st, keys, n, key_off, n_cols, njoins, i_out,
+           j_out);
+}
+
+void batch_offsets(const uint64_t* keys, long long n, const unsigned long long* key_off, int njoins,
+                   long long* offsets, cudaStream_t st) {
+    launch(batch_offsets_kernel, (unsigned)((njoins + 1 + 255) / 256), 256, 0, st, keys, n, key_off, njoins, offsets);
 }
 
 void decode_pairs(const uint64_t* keys, long long n, long long n_cols, int64_t* i_out, int64_t* j_out,

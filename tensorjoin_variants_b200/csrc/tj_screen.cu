@@ -31,6 +31,7 @@
 //   warps 2-5: epilogue, warp w reads TMEM lanes 32*(w%4) .. +31 (one R row per thread); the four
 //           warps run independently (no named barrier), synchronised only through mbarriers
 #include <algorithm>
+#include <cstring>
 
 #include "tj_emit.cuh"
 #include "tj_internal.h"
@@ -89,25 +90,33 @@ constexpr size_t screen_smem() {
            (size_t)kMetaSlots * sizeof(ColMetaF) + sizeof(ScreenCtl<StageCfg<kSplit>::kStages>);
 }
 
-struct ScreenArgs {
-    const uint4* chunks;
-    const uint32_t* nchunks;   // device count
-    const uint32_t* jlist;
-    // R side (rows of tile I)
-    const uint32_t* r_row0;
-    const uint32_t* r_nvalid;
-    const uint32_t* r_perm;
+// Per-class pointers (a class = joins with the same d, one concatenated operand matrix per side).
+struct ScreenClassArgs {
+    const uint32_t* r_emit;   // id written into keys for each sorted R row
     const double* r_nrm2;
     const float* r_zn;
     const float* r_en;
     const float* r_zl;
-    // S side: per-tile column metadata blocks
-    const ColMetaF* s_meta;
-    const uint32_t* s_row0;
     int kblocks;
     int kpad;
+};
+
+struct TMaps {
+    CUtensorMap a[kMaxClass];
+    CUtensorMap b[kMaxClass];
+};
+
+struct ScreenArgs {
+    const uint4* chunks;       // (global R tile, jlist begin, jlist end, 0)
+    const uint32_t* nchunks;   // device count
+    const uint32_t* jlist;     // global S tile ids
+    const uint4* rtiles;       // (row0 in class operand, nvalid, join, class) per global R tile
+    const uint4* stiles;       // same per global S tile
+    const ColMetaF* s_meta;    // per global S tile
+    const JoinParams* jps;     // per join
+    ScreenClassArgs cls[kMaxClass];
+    int ncls;
     unsigned idesc;
-    JoinParams jp;
     uint64_t* acc;
     unsigned long long acc_cap;
     uint64_t* band;
@@ -157,8 +166,7 @@ __global__ void __launch_bounds__(kTileS) build_col_meta(const uint32_t* row0, c
 
 template <int kFmt, int kSplit>   // kFmt: 0 = fp16, 1 = bf16; kSplit: hi/lo operand limbs
 __global__ void __launch_bounds__(kScreenThreads, 1)
-    screen_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                     const ScreenArgs a) {
+    screen_tc_kernel(const __grid_constant__ TMaps tm, const ScreenArgs a) {
     using Cfg = StageCfg<kSplit>;
     constexpr int kStages = Cfg::kStages;
     constexpr unsigned kStageBytes = Cfg::kBytes;
@@ -185,8 +193,10 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         mbar_init(&ctl->drain, 1);
         ctl->abort_flag = 0;
         fence_barrier_init();
-        prefetch_tmap(&tmA);
-        prefetch_tmap(&tmB);
+        for (int c = 0; c < a.ncls; ++c) {
+            prefetch_tmap(&tm.a[c]);
+            prefetch_tmap(&tm.b[c]);
+        }
     }
     if (warp == 1) tmem_alloc(&ctl->tmem_base, 512);
     tc_fence_before();
@@ -203,24 +213,29 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             bool ok = true;
             for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
                 const uint4 ch = a.chunks[c];
-                const int rrow = (int)a.r_row0[ch.x];
+                const uint4 rt = a.rtiles[ch.x];
+                const int rrow = (int)rt.x;
+                const unsigned cls = rt.w;
+                const int kblocks = a.cls[cls].kblocks, kpad = a.cls[cls].kpad;
+                const CUtensorMap* mA = &tm.a[cls];
+                const CUtensorMap* mB = &tm.b[cls];
                 for (unsigned e = ch.y; e < ch.z && ok; ++e, ++n) {
                     const unsigned J = a.jlist[e];
-                    const int srow = (int)a.s_row0[J];
+                    const int srow = (int)a.stiles[J].x;
                     const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
                     if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status)) { ok = false; break; }
                     mbar_arrive_expect_tx(&ctl->meta_full[slot], (unsigned)sizeof(ColMetaF));
                     bulk_load(&meta[slot], a.s_meta + J, (unsigned)sizeof(ColMetaF), &ctl->meta_full[slot]);
-                    for (int kb = 0; kb < a.kblocks; ++kb) {
+                    for (int kb = 0; kb < kblocks; ++kb) {
                         if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         uint8_t* sa = smem + (size_t)stage * kStageBytes;
                         mbar_arrive_expect_tx(&ctl->full[stage], kStageBytes);
-                        tma_load_2d(sa, &tmA, &ctl->full[stage], kb * kBK, rrow);
-                        tma_load_2d(sa + Cfg::kBhi, &tmB, &ctl->full[stage], kb * kBK, srow);
+                        tma_load_2d(sa, mA, &ctl->full[stage], kb * kBK, rrow);
+                        tma_load_2d(sa + Cfg::kBhi, mB, &ctl->full[stage], kb * kBK, srow);
                         if (kSplit) {
-                            tma_load_2d(sa + Cfg::kAlo, &tmA, &ctl->full[stage], a.kpad + kb * kBK, rrow);
-                            tma_load_2d(sa + Cfg::kBlo, &tmB, &ctl->full[stage], a.kpad + kb * kBK, srow);
+                            tma_load_2d(sa + Cfg::kAlo, mA, &ctl->full[stage], kpad + kb * kBK, rrow);
+                            tma_load_2d(sa + Cfg::kBlo, mB, &ctl->full[stage], kpad + kb * kBK, srow);
                         }
                         if (++stage == kStages) { stage = 0; phase ^= 1; }
                     }
@@ -245,11 +260,12 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             bool ok = true;
             for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
                 const uint4 ch = a.chunks[c];
+                const int kblocks = a.cls[a.rtiles[ch.x].w].kblocks;
                 for (unsigned e = ch.y; e < ch.z && ok; ++e) {
                     if (!mbar_wait(&ctl->acc_empty[acc], acc_phase ^ 1, status)) { ok = false; break; }
                     tc_fence_after();
                     const unsigned d_tmem = tmem + acc * kTileS;
-                    for (int kb = 0; kb < a.kblocks; ++kb) {
+                    for (int kb = 0; kb < kblocks; ++kb) {
                         if (!mbar_wait(&ctl->full[stage], phase, status)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         tc_fence_after();
@@ -280,22 +296,23 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         // ------------------------------------------------------------ epilogue
         const unsigned q = warp & 3;                 // TMEM lane quarter of this warp
         const unsigned row = q * 32 + lane;          // R row within the tile
-        const JoinParams& jp = a.jp;
         WarpAppender app_acc, app_band;
         unsigned acc = 0, acc_phase = 0;
         unsigned long long n = 0, n_screen_acc = 0, n_rare = 0, n_items = 0;
         bool ok = true;
         for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
             const uint4 ch = a.chunks[c];
-            const unsigned I = ch.x;
-            const unsigned r0 = a.r_row0[I];
-            const bool rvalid = row < a.r_nvalid[I];
+            const uint4 rt = a.rtiles[ch.x];
+            const ScreenClassArgs& ca = a.cls[rt.w];
+            const JoinParams jp = a.jps[rt.z];
+            const unsigned r0 = rt.x;
+            const bool rvalid = row < rt.y;
             const unsigned rs = r0 + row;
-            const double Ai = rvalid ? a.r_nrm2[rs] : 0.0;
-            const double Zi = rvalid ? (double)a.r_zn[rs] : 0.0;
-            const double Ei = rvalid ? (double)a.r_en[rs] : 0.0;
-            const double Zli = rvalid ? (double)a.r_zl[rs] : 0.0;
-            const uint32_t oi = rvalid ? a.r_perm[rs] : 0u;
+            const double Ai = rvalid ? ca.r_nrm2[rs] : 0.0;
+            const double Zi = rvalid ? (double)ca.r_zn[rs] : 0.0;
+            const double Ei = rvalid ? (double)ca.r_en[rs] : 0.0;
+            const double Zli = rvalid ? (double)ca.r_zl[rs] : 0.0;
+            const uint32_t oi = rvalid ? ca.r_emit[rs] : 0u;
             for (unsigned e = ch.y; e < ch.z; ++e, ++n) {
                 const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
                 if (!mbar_wait(&ctl->meta_full[slot], mph, status) ||
@@ -440,41 +457,48 @@ void make_tmap_2d(CUtensorMap* m, const void* base, long long rows, long long co
     if (r != CUDA_SUCCESS) fail(-2, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
 }
 
-void screen_tc(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st) {
-    const Side& R = *g.R;
-    const Side& S = *g.S;
-    const bool bf = R.screen == kScreenBF16 || R.screen == kScreenBF16X3;
-    const bool ok = R.screen == S.screen && (bf || R.screen == kScreenFP16 || R.screen == kScreenFP16X3);
-    if (!ok) fail(-1, "screen_tc needs matching bf16 / fp16 operands on both sides");
-    if (R.kpad != S.kpad || R.split != S.split) fail(-1, "operand layouts differ");
-    CUtensorMap tmA, tmB;
-    const CUtensorMapDataType dt = bf ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
-    const long long w = (long long)R.kpad * (R.split ? 2 : 1);
-    make_tmap_2d(&tmA, R.op.p, R.rows_pad, w, 2, kTileR, dt);
-    make_tmap_2d(&tmB, S.op.p, S.rows_pad, w, 2, kTileS, dt);
+void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
+    if (g.ncls < 1 || g.ncls > kMaxClass) fail(-1, "screen_tc: bad class count");
+    const int scr = g.R[0]->screen;
+    const bool bf = scr == kScreenBF16 || scr == kScreenBF16X3;
+    const int split = g.R[0]->split;
+    TMaps tm;
+    memset(&tm, 0, sizeof(tm));
     ScreenArgs a;
+    memset(&a, 0, sizeof(a));
+    DBuf<ColMetaF> smeta((size_t)std::max(g.ntS_total, 1), st);
+    for (int c = 0; c < g.ncls; ++c) {
+        const Side& R = *g.R[c];
+        const Side& S = *g.S[c];
+        const bool ok = R.screen == scr && S.screen == scr && R.split == split && S.split == split &&
+                        (bf || scr == kScreenFP16 || scr == kScreenFP16X3) && R.kpad == S.kpad;
+        if (!ok) fail(-1, "screen_tc needs matching bf16 / fp16 operands on both sides of every class");
+        const CUtensorMapDataType dt = bf ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+        const long long w = (long long)R.kpad * (split ? 2 : 1);
+        make_tmap_2d(&tm.a[c], R.op.p, R.rows_pad, w, 2, kTileR, dt);
+        make_tmap_2d(&tm.b[c], S.op.p, S.rows_pad, w, 2, kTileS, dt);
+        const TileSet& tS = *g.tS[c];
+        if (tS.ntiles > 0)
+            launch(build_col_meta, tS.ntiles, kTileS, 0, st, tS.row0.p, tS.nvalid.p, S.emit, S.nrm2.p, S.nrm2f.p,
+                   S.zn.p, S.en.p, S.yn.p, S.zl.p, tS.maxZ.p, tS.maxE.p, tS.maxY.p, tS.maxB.p, tS.beta.p,
+                   tS.maxZl.p, smeta.p + g.sbase[c]);
+        a.cls[c].r_emit = R.emit;
+        a.cls[c].r_nrm2 = R.nrm2.p;
+        a.cls[c].r_zn = R.zn.p;
+        a.cls[c].r_en = R.en.p;
+        a.cls[c].r_zl = R.zl.p;
+        a.cls[c].kblocks = R.kpad / kBK;
+        a.cls[c].kpad = R.kpad;
+    }
     a.chunks = g.cand->chunks.p;
     a.nchunks = g.cand->dev_counts.p + 1;
     a.jlist = g.cand->jlist.p;
-    a.r_row0 = g.tR->row0.p;
-    a.r_nvalid = g.tR->nvalid.p;
-    a.r_perm = R.perm.p;
-    a.r_nrm2 = R.nrm2.p;
-    a.r_zn = R.zn.p;
-    a.r_en = R.en.p;
-    a.r_zl = R.zl.p;
-    const TileSet& tS = *g.tS;
-    DBuf<ColMetaF> smeta((size_t)std::max(tS.ntiles, 1), st);
-    if (tS.ntiles > 0)
-        launch(build_col_meta, tS.ntiles, kTileS, 0, st, tS.row0.p, tS.nvalid.p, S.perm.p, S.nrm2.p, S.nrm2f.p,
-               S.zn.p, S.en.p, S.yn.p, S.zl.p, tS.maxZ.p, tS.maxE.p, tS.maxY.p, tS.maxB.p, tS.beta.p, tS.maxZl.p,
-               smeta.p);
+    a.rtiles = g.rtiles;
+    a.stiles = g.stiles;
     a.s_meta = smeta.p;
-    a.s_row0 = tS.row0.p;
-    a.kblocks = R.kpad / kBK;
-    a.kpad = R.kpad;
+    a.jps = g.jps;
+    a.ncls = g.ncls;
     a.idesc = make_idesc(1u, bf ? 1u : 0u, kTileR, kTileS);
-    a.jp = g.jp;
     a.acc = eb.acc;
     a.acc_cap = eb.acc_cap;
     a.band = eb.band;
@@ -485,11 +509,11 @@ void screen_tc(const JoinGeometry& g, const EmitBuffers& eb, cudaStream_t st) {
     do {                                                                                                    \
         TJ_CUDA(cudaFuncSetAttribute(screen_tc_kernel<F, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                      (int)screen_smem<SP>()));                                              \
-        launch(screen_tc_kernel<F, SP>, grid, kScreenThreads, screen_smem<SP>(), st, tmA, tmB, a);          \
+        launch(screen_tc_kernel<F, SP>, grid, kScreenThreads, screen_smem<SP>(), st, tm, a);                \
     } while (0)
-    if (bf && R.split) TJ_SCREEN(1, 1);
+    if (bf && split) TJ_SCREEN(1, 1);
     else if (bf) TJ_SCREEN(1, 0);
-    else if (R.split) TJ_SCREEN(0, 1);
+    else if (split) TJ_SCREEN(0, 1);
     else TJ_SCREEN(0, 0);
 #undef TJ_SCREEN
 }

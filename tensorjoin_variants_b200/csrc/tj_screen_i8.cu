@@ -340,9 +340,10 @@ __global__ void __launch_bounds__(kI8Threads, 1)
 void make_tmap_2d(CUtensorMap* m, const void* base, long long rows, long long cols, int esize, int box_rows,
                   CUtensorMapDataType dt);
 
-void screen_i8(const JoinGeometry& g, const EmitBuffers& eb, long long T, cudaStream_t st) {
-    const Side& R = *g.R;
-    const Side& S = *g.S;
+void screen_i8(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
+    if (g.ncls != 1 || g.njoins != 1) fail(-7, "the int8-limb screen runs one join at a time");
+    const Side& R = *g.R[0];
+    const Side& S = *g.S[0];
     if (R.screen != kScreenInt8Limb || S.screen != kScreenInt8Limb) fail(-1, "screen_i8 needs int8-limb sides");
     CUtensorMap tmA, tmB;
     make_tmap_2d(&tmA, R.op8.p, R.rows_pad, 2 * (long long)R.kpad, 1, 128, CU_TENSOR_MAP_DATA_TYPE_UINT8);
@@ -351,22 +352,22 @@ void screen_i8(const JoinGeometry& g, const EmitBuffers& eb, long long T, cudaSt
     a.chunks = g.cand->chunks.p;
     a.nchunks = g.cand->dev_counts.p + 1;
     a.jlist = g.cand->jlist.p;
-    a.r_row0 = g.tR->row0.p;
-    a.r_nvalid = g.tR->nvalid.p;
-    a.r_perm = R.perm.p;
+    a.r_row0 = g.tR[0]->row0.p;
+    a.r_nvalid = g.tR[0]->nvalid.p;
+    a.r_perm = R.emit;
     a.r_norm = R.inorm.p;
-    const TileSet& tS = *g.tS;
+    const TileSet& tS = *g.tS[0];
     DBuf<ColMetaI8> smeta((size_t)std::max(tS.ntiles, 1), st);
     if (tS.ntiles > 0)
-        launch(build_col_meta_i8, tS.ntiles, kI8N, 0, st, tS.row0.p, tS.nvalid.p, S.perm.p, S.inorm.p, smeta.p);
+        launch(build_col_meta_i8, tS.ntiles, kI8N, 0, st, tS.row0.p, tS.nvalid.p, S.emit, S.inorm.p, smeta.p);
     a.s_row0 = tS.row0.p;
     a.s_meta = smeta.p;
     a.kblocks = R.kpad / 128;
     a.kpad = R.kpad;
     a.idesc = make_idesc(2u, 1u, 128, kI8N);
-    a.T = T;
+    a.T = g.T_int;
     a.twoM = 2ll * (long long)R.kpad * (128ll * 8192ll + 4096ll);
-    a.jp = g.jp;
+    a.jp = g.jp0;
     a.acc = eb.acc;
     a.acc_cap = eb.acc_cap;
     a.ctr = eb.ctr;

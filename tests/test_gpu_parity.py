@@ -263,3 +263,44 @@ def test_int14_rejects_out_of_range_and_fraction():
     with pytest.raises(_lib.TJError) as e:
         tj.self_join(Y, eps2=10.5, screen="int8limb")
     assert e.value.code == -1
+
+
+# ---------------------------------------------------------------- batched ragged joins (one persistent screen launch)
+def _ragged(njoins, seed, dims=(8, 32, 128), lo=50, hi=3000):
+    rng = np.random.default_rng(seed)
+    joins = []
+    for k in range(njoins):
+        nr = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        ns = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        d = int(rng.choice(dims))
+        centres = rng.random((8, d))
+        R = (centres[rng.integers(0, 8, nr)] + rng.standard_normal((nr, d)) * 0.05).astype(np.float32)
+        S = (centres[rng.integers(0, 8, ns)] + rng.standard_normal((ns, d)) * 0.05).astype(np.float32)
+        T = W.ragged_eps2(ns, d, 8, 0.05, 16)
+        joins.append((R, S, T))
+    return joins
+
+
+@pytest.mark.parametrize("screen", ["bf16x3", "fp16", "plain"])
+def test_batched_ragged_exact(screen):
+    joins = _ragged(40, 41)
+    joins.append((joins[0][0][:0], joins[1][1], 0.5))          # empty R side
+    joins.append((joins[2][0], joins[3][1][:1], joins[3][2]))  # single S row (d may differ: reuse S of same d)
+    joins[-1] = (joins[3][0], joins[3][1][:1], joins[3][2])
+    dev = [(torch.from_numpy(R).cuda(), torch.from_numpy(S).cuda(), float(np.sqrt(T))) for R, S, T in joins]
+    out = tj.join_batched(dev, screen=screen)
+    assert len(out) == len(joins)
+    for k, ((R, S, T), (i, j)) in enumerate(zip(joins, out)):
+        Tk = float(np.sqrt(T)) ** 2
+        want = oracle.join_f32(R, S, Tk, "rs") if len(R) and len(S) else np.empty(0, np.uint64)
+        got = i.cpu().numpy().astype(np.uint64) * np.uint64(max(len(S), 1)) + j.cpu().numpy().astype(np.uint64)
+        assert_same(got, want, f"{screen} join {k} d={R.shape[1]} {len(R)}x{len(S)}")
+
+
+def test_batched_equals_single_joins():
+    joins = _ragged(12, 42, dims=(32,))
+    dev = [(torch.from_numpy(R).cuda(), torch.from_numpy(S).cuda(), float(np.sqrt(T))) for R, S, T in joins]
+    out = tj.join_batched(dev, screen="bf16x3")
+    for (Rt, St, e), (i, j) in zip(dev, out):
+        i1, j1 = tj.join(Rt, St, e, screen="bf16x3")
+        assert torch.equal(i, i1) and torch.equal(j, j1)
