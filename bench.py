@@ -49,6 +49,7 @@ WORKLOADS = {
     "mixture64": dict(fn="mixture64", screen="bf16x3", mode="rs"),
     "uniform16": dict(fn="uniform16", screen="plain", mode="upper"),
     "int14x128": dict(fn="int14x128", screen="int8limb", mode="upper"),
+    "ragged4096": dict(fn="ragged4096", screen="bf16x3", mode="rs"),
 }
 
 
@@ -211,6 +212,9 @@ def main() -> None:
     spec = WORKLOADS[args.workload]
     screen = args.screen or spec["screen"]
     mode = spec["mode"]
+    if args.workload == "ragged4096":
+        ragged_bench(args, rank, world, screen, dist)
+        return
     w = make_workload(args.workload, args.n)
     R = torch.from_numpy(w.R).cuda()
     S = None if w.S is None else torch.from_numpy(w.S).cuda()
@@ -263,9 +267,8 @@ def main() -> None:
     # dominant kernel: the screen (tensor-core bound); algorithmic flops = 2 d per screened pair
     peaks = measured_peaks()
     screen_ms = statistics.mean(s["ms_screen"] for s in stats)
-    d = int(w.R.shape[1])
-    # algorithmic ops per screened pair: 2 d (one 16-bit dot product) or 8 d (four int8 limb products)
-    flops = (8.0 if screen == "int8limb" else 6.0 if screen.endswith("x3") else 2.0) * d * pairs
+    # algorithmic ops per screened pair, counted by the library: 2 d (16-bit), 6 d (hi/lo split), 8 d (int8 limbs)
+    flops = statistics.mean(s["screen_ops"] for s in stats) if screen != "plain" else 2.0 * w.R.shape[1] * pairs
     peak_note = f"{peaks['source']} bf16_tflops_sustained (dense fp16 = bf16 rate)"
     if screen == "plain":
         achieved, unit, bound = flops / (screen_ms / 1000.0) / 1e12, "TFLOP/s", "simt"
@@ -363,6 +366,141 @@ def main() -> None:
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------- config 5: batched ragged joins
+def ragged_device(joins=4096, lo=256, hi=65536, dims=(8, 32, 128), clusters=8, std=0.05, degree=16, seed=5,
+                  size_scale=1.0):
+    """Config-5 data drawn on the GPU (seeded torch CUDA generator): per dimension class one bulk draw,
+    every join a contiguous slice.  Same shapes and distributions as workloads.ragged4096."""
+    import torch
+    from tensorjoin_variants_b200 import workloads as W
+
+    rng = np.random.default_rng(seed)
+    nr = np.maximum(1, np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), joins)) * size_scale)).astype(np.int64)
+    ns = np.maximum(1, np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), joins)) * size_scale)).astype(np.int64)
+    dj = rng.choice(np.asarray(dims), joins)
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    out = [dict() for _ in range(joins)]
+    classes = []
+    for d in dims:
+        ks = np.flatnonzero(dj == d)
+        if len(ks) == 0:
+            continue
+        centres = torch.from_numpy(rng.random((len(ks), clusters, d)).astype(np.float32)).cuda()
+        for side, counts in (("R", nr[ks]), ("S", ns[ks])):
+            total = int(counts.sum())
+            owner = torch.from_numpy(np.repeat(np.arange(len(ks)), counts)).cuda()
+            label = torch.randint(0, clusters, (total,), generator=g, device="cuda")
+            X = torch.randn((total, d), generator=g, device="cuda") * std + centres[owner, label]
+            classes.append(X)
+            offs = np.concatenate([[0], np.cumsum(counts)])
+            for q, k in enumerate(ks):
+                out[k][side] = X[int(offs[q]):int(offs[q + 1])]
+    eps = [math.sqrt(W.ragged_eps2(int(ns[k]), int(dj[k]), clusters, std, degree)) for k in range(joins)]
+    return [(out[k]["R"], out[k]["S"], eps[k]) for k in range(joins)], classes
+
+
+def ragged_bench(args, rank, world, screen, dist):
+    import torch
+
+    import tensorjoin_variants_b200 as tj
+    from tensorjoin_variants_b200 import _lib
+
+    scale = args.n / 11_800 if args.n else 1.0   # --n sets the mean side length
+    joins, classes = ragged_device(size_scale=scale)
+    torch.cuda.synchronize()
+    nj = len(joins)
+    stream = torch.cuda.current_stream()
+
+    def step(scr):
+        return tj.join_batched_result(joins, screen=scr)
+
+    for _ in range(args.warmup):
+        r = step(screen)
+        del r
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
+    except Exception:
+        gpu_id = "0"
+    clocks = Clocks(gpu_id)
+    clocks.start()
+    time.sleep(0.3)
+    l0 = _lib.lib().tj_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    stats = []
+    for _ in range(args.steps):
+        r = step(screen)
+        stats.append(r.stats)
+        pairs_out = r.count
+        del r
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = _lib.lib().tj_kernel_launches() - l0
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    st = stats[-1]
+    pairs = st["pairs_screened"]
+    peaks = measured_peaks()
+    screen_ms = statistics.mean(s["ms_screen"] for s in stats)
+    ops = statistics.mean(s["screen_ops"] for s in stats)
+    achieved = ops / (screen_ms / 1000.0) / 1e12
+    peak = peaks["tflops_sustained"] if screen != "plain" else None
+    # per-join latency: a seeded sample of joins run one at a time through tj.join
+    rng = np.random.default_rng(11)
+    lat = []
+    for k in rng.choice(nj, size=min(128, nj), replace=False):
+        R, S, e = joins[int(k)]
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        i, j = tj.join(R, S, e, screen=screen)
+        b.record(stream)
+        torch.cuda.synchronize()
+        lat.append(a.elapsed_time(b))
+    line = {
+        "metric": METRIC, "value": world * pairs / (ms / 1000.0), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": screen, "data": "synthetic (seeded, drawn on the GPU)",
+        "config": {"workload": "ragged4096", "joins": nj, "rows_r": int(sum(j[0].shape[0] for j in joins)),
+                   "rows_s": int(sum(j[1].shape[0] for j in joins)), "dims": [8, 32, 128], "screen": screen,
+                   "mean_side": 11_800 * scale, "l2": "inputs larger than L2 (no flush needed)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "tensor" if screen != "plain" else "simt", "kernel": "screen_tc_kernel",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None,
+                     "peak_source": f"{peaks['source']} bf16_tflops_sustained", "traffic": None,
+                     "screen_ms": screen_ms, "flops_per_launch": ops},
+        "clocks": clk, "gpu_launches": int(launches), "result_pairs": int(pairs_out),
+        "batch": {"joins_per_s": nj / (ms / 1000.0), "ms_per_join_amortised": ms / nj,
+                  "single_join_latency_ms_p50": float(np.percentile(lat, 50)),
+                  "single_join_latency_ms_p99": float(np.percentile(lat, 99)), "latency_sample": len(lat)},
+        "stats": {k: st[k] for k in ("pairs_all", "pairs_screened", "tile_pairs", "screen_accept", "band",
+                                     "refine_accept", "result_pairs", "retries", "ms_index", "ms_candidates",
+                                     "ms_screen", "ms_refine", "ms_sort", "ms_total")},
+    }
+    if not args.no_plain and screen != "plain":
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rp = step("plain")
+        b.record(stream)
+        torch.cuda.synchronize()
+        r = step(screen)
+        same = bool(torch.equal(rp.keys(), r.keys()))
+        line["plain_gpu"] = {"ms_per_step": a.elapsed_time(b), "speedup_of_tc_path": a.elapsed_time(b) / ms,
+                             "identical_pair_set": same}
+        del rp, r
     if rank == 0:
         print(json.dumps(line), flush=True)
 

@@ -80,6 +80,7 @@ typedef struct tj_stats {
     int64_t result_pairs;         /* pairs in the output */
     int64_t retries;              /* capacity retries (overflow-and-retry passes) */
     double ms_index, ms_candidates, ms_screen, ms_refine, ms_sort, ms_total;   /* device time per stage */
+    double screen_ops;            /* algorithmic screen operations: per pair 2d (16-bit), 6d (hi/lo split), 8d (int8 limbs) */
 } tj_stats;
 
 /* ----------------------------------------------------------------- joins */

@@ -8,6 +8,7 @@ Public API (drop-in for the reference's join path):
     join_batched([(R,S,eps)])  -> per-join (i, j)
 All work runs in libtensorjoin.so (hand-written sm_100a CUDA behind a C ABI).
 """
-from .api import Index, Result, build_index, join, join_batched, join_result, self_join  # noqa: F401
+from .api import (BatchResult, Index, Result, build_index, join, join_batched, join_batched_result,  # noqa: F401
+                  join_result, self_join)
 
 __version__ = "0.1.0"

@@ -45,7 +45,7 @@ class Stats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "n_rows", "n_cols", "pairs_all", "tile_pairs", "pairs_screened", "screen_accept", "band",
         "refine_accept", "rare_checks", "result_pairs", "retries")] + [(n, C.c_double) for n in (
-        "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total")]
+        "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total", "screen_ops")]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -27,7 +27,8 @@ import torch
 from . import _lib
 from ._lib import MODE, SCREEN, check, lib
 
-__all__ = ["join", "self_join", "join_result", "build_index", "Result", "Index", "join_batched"]
+__all__ = ["join", "self_join", "join_result", "build_index", "Result", "Index", "join_batched",
+           "join_batched_result", "BatchResult"]
 
 
 def _stream_ptr() -> int:
@@ -204,8 +205,36 @@ def build_index(X, eps=None, *, eps2=None) -> Index:
     return Index(perm, keys, cs, tp, int(nt.value))
 
 
-def join_batched(joins, screen: str = "bf16"):
-    """Many independent R-S joins [(R, S, eps), ...] in one batched pass; returns [(i, j), ...]."""
+class BatchResult(Result):
+    """Result of a batched join: all joins' pairs in one sorted array plus per-join ranges."""
+
+    def __init__(self, handle, njoins: int, host: bool, keepalive=()):
+        super().__init__(handle, 0, 0, host, keepalive)
+        self.njoins = njoins
+
+    def offsets(self):
+        offs = (C.c_int64 * (self.njoins + 1))()
+        check(lib().tj_batch_offsets(self._h, offs))
+        return [int(v) for v in offs]
+
+    def pairs(self):
+        n = self.count
+        i = torch.empty(n, dtype=torch.int64, device="cuda")
+        j = torch.empty(n, dtype=torch.int64, device="cuda")
+        if n:
+            check(lib().tj_batch_pairs(self._h, C.c_void_p(i.data_ptr()), C.c_void_p(j.data_ptr()),
+                                       C.c_void_p(_stream_ptr())))
+        return self._out(i, j)
+
+    def split(self):
+        """[(i, j)] per join, in join order (local row ids of each join's R and S)."""
+        i, j = self.pairs()
+        o = self.offsets()
+        return [(i[o[k]:o[k + 1]], j[o[k]:o[k + 1]]) for k in range(self.njoins)]
+
+
+def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_items: int = 0) -> BatchResult:
+    """Run many independent R-S joins [(R, S, eps), ...] in one batched pass (one screen launch)."""
     descs = (_lib.BatchJoin * len(joins))()
     keep = []
     host = True
@@ -217,17 +246,12 @@ def join_batched(joins, screen: str = "bf16"):
         descs[k] = _lib.BatchJoin(Rt.data_ptr(), St.data_ptr(), Rt.shape[0], St.shape[0], Rt.shape[1], 0,
                                   _threshold(eps, None))
     h = C.c_void_p()
-    opt = _lib.Options(0, 0, 0)
+    opt = _lib.Options(int(capacity), int(chunk_items), 0)
     check(lib().tj_join_batched(descs, len(joins), SCREEN[screen], C.byref(opt), C.byref(h),
                                 C.c_void_p(_stream_ptr())))
-    res = Result(h, 0, 0, host, keepalive=tuple(keep))
-    offs = (C.c_int64 * (len(joins) + 1))()
-    check(lib().tj_batch_offsets(h, offs))
-    n = offs[len(joins)]
-    i = torch.empty(n, dtype=torch.int64, device="cuda")
-    j = torch.empty(n, dtype=torch.int64, device="cuda")
-    if n:
-        check(lib().tj_batch_pairs(h, C.c_void_p(i.data_ptr()), C.c_void_p(j.data_ptr()), C.c_void_p(_stream_ptr())))
-    if host:
-        i, j = i.cpu(), j.cpu()
-    return [(i[offs[k]:offs[k + 1]], j[offs[k]:offs[k + 1]]) for k in range(len(joins))]
+    return BatchResult(h, len(joins), host, keepalive=tuple(keep))
+
+
+def join_batched(joins, screen: str = "bf16", **kw):
+    """Many independent R-S joins [(R, S, eps), ...] in one batched pass; returns [(i, j), ...]."""
+    return join_batched_result(joins, screen=screen, **kw).split()

@@ -85,6 +85,10 @@ int num_sms() {
 // ------------------------------------------------------------------ helpers
 namespace {
 
+struct ScreenOps {
+    unsigned long long per_pair[kMaxClass];
+};
+
 __global__ void zero_counters(Counters* c, int emit_only) {
     unsigned long long* w = (unsigned long long*)c;
     const int n = emit_only ? 8 : (int)(sizeof(Counters) / 8);
@@ -101,17 +105,30 @@ __global__ void cell_starts(const uint32_t* flag, const uint32_t* pos, long long
     if (i < n && flag[i]) start[pos[i]] = (uint32_t)i;
     if (i == 0) start[*ncells] = (uint32_t)n;
 }
+// Distance evaluations of the candidate list (out[0]) and algorithmic screen operations (out[1]),
+// ops_per_pair[c] = 2 d (16-bit), 6 d (hi/lo split) or 8 d (int8 limbs) for class c.
 __global__ void pairs_screened_kernel(const uint4* chunks, const uint32_t* nchunks, const uint32_t* jlist,
-                                      const uint4* rtiles, const uint4* stiles, unsigned long long* out) {
-    unsigned long long acc = 0;
+                                      const uint4* rtiles, const uint4* stiles, const ScreenOps ops,
+                                      unsigned long long* out) {
+    unsigned long long acc = 0, aops = 0;
     const unsigned n = *nchunks;
     for (unsigned c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         const uint4 ch = chunks[c];
-        const unsigned long long rv = rtiles[ch.x].y;
-        for (unsigned e = ch.y; e < ch.z; ++e) acc += rv * stiles[jlist[e]].y;
+        const uint4 rt = rtiles[ch.x];
+        const unsigned long long rv = rt.y;
+        unsigned long long p = 0;
+        for (unsigned e = ch.y; e < ch.z; ++e) p += rv * stiles[jlist[e]].y;
+        acc += p;
+        aops += p * ops.per_pair[rt.w];
     }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+    for (int o = 16; o > 0; o >>= 1) {
+        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        aops += __shfl_xor_sync(0xffffffffu, aops, o);
+    }
+    if ((threadIdx.x & 31) == 0 && acc) {
+        atomicAdd(out, acc);
+        atomicAdd(out + 1, aops);
+    }
 }
 __global__ void tile_pair_list(const uint4* chunks, const uint32_t* nchunks, const uint32_t* jlist, uint32_t* out) {
     const unsigned n = *nchunks;
@@ -471,9 +488,13 @@ void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen
         build_candidates_batched(views, blocks, tps, g.ntR_total, words, chunk_items, rsb, cand, st);
     }
     g.cand = &cand;
+    ScreenOps sops;
+    memset(&sops, 0, sizeof(sops));
+    for (int c = 0; c < ncls; ++c)
+        sops.per_pair[c] = (unsigned long long)cls_d[c] * (i8 ? 8ull : (C[c]->R.split ? 6ull : 2ull));
     launch(pairs_screened_kernel, num_sms() * 4, 256, 0, st, (const uint4*)cand.chunks.p,
            (const uint32_t*)(cand.dev_counts.p + 1), (const uint32_t*)cand.jlist.p, (const uint4*)d_rt.p,
-           (const uint4*)d_st.p, &ctr.p->pad[0]);
+           (const uint4*)d_st.p, sops, &ctr.p->pad[0]);
     ev.rec(6, st);
 
     // screen + refine with overflow-and-retry
@@ -510,6 +531,7 @@ void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen
     }
     S_.tile_pairs = (int64_t)h.items;
     S_.pairs_screened = (int64_t)h.pad[0];
+    S_.screen_ops = (double)h.pad[1];
     S_.screen_accept = (int64_t)h.screen_accept;
     S_.band = (int64_t)h.band_valid;
     S_.refine_accept = (int64_t)h.refine_accept;

@@ -190,20 +190,41 @@ def ragged_eps2(n_s, d, clusters, std, degree):
 
 def ragged4096(joins=4096, lo=256, hi=65536, dims=(8, 32, 128), clusters=8, std=0.05, degree=16, seed=5,
                size_scale=1.0):
-    """Config 5: thousands of independent R-S joins with log-uniform sizes and d drawn from ``dims``."""
+    """Config 5: thousands of independent R-S joins with log-uniform sizes and d drawn from ``dims``.
+
+    Each join is an 8-cluster mixture (centres U[0,1)^d, isotropic std 0.05) on both sides.  Data are
+    drawn per dimension class in bulk and every join's R and S are contiguous slices of its class
+    arrays (``RaggedJoin.R`` / ``.S`` are views), so the whole batch also exists as a few large arrays
+    (``ragged_classes``) that can be moved to the device in one copy per class.
+    """
     rng = np.random.default_rng(seed)
-    out = []
-    for _ in range(joins):
-        nr = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))) * size_scale))
-        ns = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))) * size_scale))
-        nr, ns = max(1, nr), max(1, ns)
-        d = int(rng.choice(dims))
-        centres = rng.random((clusters, d))
-        R = _mixture(rng, nr, centres, std)
-        S = _mixture(rng, ns, centres, std)
-        T = ragged_eps2(ns, d, clusters, std, degree)
-        out.append(RaggedJoin(R, S, math.sqrt(T), T))
-    return out
+    nr = np.maximum(1, np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), joins)) * size_scale)).astype(np.int64)
+    ns = np.maximum(1, np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), joins)) * size_scale)).astype(np.int64)
+    dj = rng.choice(np.asarray(dims), joins)
+    out = [None] * joins
+    for d in dims:
+        ks = np.flatnonzero(dj == d)
+        if len(ks) == 0:
+            continue
+        centres = rng.random((len(ks), clusters, d)).astype(np.float32)
+        for side, counts in (("R", nr[ks]), ("S", ns[ks])):
+            total = int(counts.sum())
+            owner = np.repeat(np.arange(len(ks)), counts)
+            label = rng.integers(0, clusters, total)
+            X = rng.standard_normal((total, d), dtype=np.float32)
+            X *= np.float32(std)
+            X += centres[owner, label]
+            offs = np.concatenate([[0], np.cumsum(counts)])
+            for q, k in enumerate(ks):
+                part = X[offs[q]:offs[q + 1]]
+                if out[k] is None:
+                    out[k] = {}
+                out[k][side] = part
+    res = []
+    for k in range(joins):
+        T = ragged_eps2(int(ns[k]), int(dj[k]), clusters, std, degree)
+        res.append(RaggedJoin(out[k]["R"], out[k]["S"], math.sqrt(T), T))
+    return res
 
 
 CONFIGS = {
