@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
                                                          float* hiT, float* rad, float* maxZ, float* maxE,
                                                          float* maxY, float* maxB, float* beta, float* maxZl,
                                                          uint32_t* nvalid, uint32_t* row0, const uint32_t* row0_in,
-                                                         const uint32_t* nvalid_in) {
+                                                         const uint32_t* nvalid_in, int warp_rows) {
     extern __shared__ float s_ctr[];   // [d]
     __shared__ float red[6][256];
     const int t = blockIdx.x;
@@ -293,24 +293,61 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
     const int nv = tabled ? (int)nvalid_in[t] : (int)min((long long)tile, n - r0);
     const double g = (double)(d + 2) * 0x1p-53;
     // per-dimension centroid and bounding box
-    for (int k = threadIdx.x; k < d; k += blockDim.x) {
-        double s = 0.0;
-        float mn = INFINITY, mx = -INFINITY;
-        for (int i = 0; i < nv; ++i) {
-            const float v = load_x(src, dtype, (size_t)perm[r0 + i] * d + k);
-            s += v;
-            mn = fminf(mn, v);
-            mx = fmaxf(mx, v);
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp_rows) {
+        // warp w reads rows w, w+8, ... (coalesced across dimensions); per-warp partials in shared
+        // memory, combined over the 8 warps in a fixed order
+        double* psum = (double*)(s_ctr + ((d + 1) & ~1));   // [8][d]
+        float* pmin = (float*)(psum + 8 * d);               // [8][d]
+        float* pmax = pmin + 8 * d;                         // [8][d]
+        for (int k = lane; k < d; k += 32) {
+            psum[warp * d + k] = 0.0;
+            pmin[warp * d + k] = INFINITY;
+            pmax[warp * d + k] = -INFINITY;
         }
-        const float c = (float)(s / (double)max(nv, 1));
-        s_ctr[k] = c;
-        ctrT[(size_t)k * ntiles + t] = c;
-        loT[(size_t)k * ntiles + t] = mn;
-        hiT[(size_t)k * ntiles + t] = mx;
+        for (int i = warp; i < nv; i += 8) {
+            const size_t base = (size_t)perm[r0 + i] * d;
+            for (int k = lane; k < d; k += 32) {
+                const float v = load_x(src, dtype, base + k);
+                psum[warp * d + k] += v;
+                pmin[warp * d + k] = fminf(pmin[warp * d + k], v);
+                pmax[warp * d + k] = fmaxf(pmax[warp * d + k], v);
+            }
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < d; k += blockDim.x) {
+            double sm = 0.0;
+            float mn = INFINITY, mx = -INFINITY;
+            for (int w = 0; w < 8; ++w) {
+                sm += psum[w * d + k];
+                mn = fminf(mn, pmin[w * d + k]);
+                mx = fmaxf(mx, pmax[w * d + k]);
+            }
+            const float c = (float)(sm / (double)max(nv, 1));
+            s_ctr[k] = c;
+            ctrT[(size_t)k * ntiles + t] = c;
+            loT[(size_t)k * ntiles + t] = mn;
+            hiT[(size_t)k * ntiles + t] = mx;
+        }
+    } else {
+        for (int k = threadIdx.x; k < d; k += blockDim.x) {
+            double sm = 0.0;
+            float mn = INFINITY, mx = -INFINITY;
+            for (int i = 0; i < nv; ++i) {
+                const float v = load_x(src, dtype, (size_t)perm[r0 + i] * d + k);
+                sm += v;
+                mn = fminf(mn, v);
+                mx = fmaxf(mx, v);
+            }
+            const float c = (float)(sm / (double)max(nv, 1));
+            s_ctr[k] = c;
+            ctrT[(size_t)k * ntiles + t] = c;
+            loT[(size_t)k * ntiles + t] = mn;
+            hiT[(size_t)k * ntiles + t] = mx;
+        }
     }
     __syncthreads();
     // radius: warp per row, exact FP64 differences against the FP32 centroid
-    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double rmax = 0.0;
     for (int i = warp; i < nv; i += 8) {
         const size_t base = (size_t)perm[r0 + i] * d;
@@ -661,14 +698,18 @@ void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st) {
         TJ_CUDA(cudaMemcpyAsync(ts.row0.p, ts.h_row0.data(), nt * 4, cudaMemcpyHostToDevice, st));
         TJ_CUDA(cudaMemcpyAsync(ts.nvalid.p, ts.h_nvalid.data(), nt * 4, cudaMemcpyHostToDevice, st));
     }
-    const size_t smem = (size_t)s.d * sizeof(float);
+    // centroid [d] floats (rounded up to an even count) + per-warp partials (8 x d x (8 + 4 + 4) bytes)
+    const size_t base = (size_t)((s.d + 1) & ~1) * sizeof(float);
+    const size_t part = (size_t)8 * s.d * 16;
+    const int warp_rows = base + part <= 200 * 1024 ? 1 : 0;
+    const size_t smem = base + (warp_rows ? part : 0);
     if (smem > 48 * 1024)
         TJ_CUDA(cudaFuncSetAttribute(tile_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     launch(tile_stats_kernel, ts.ntiles, 256, smem, st, s.src, s.dtype, s.n, s.d, tile, ts.ntiles, s.perm.p, s.nrm2.p,
            s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.zl.p, ts.ctrT.p, ts.loT.p, ts.hiT.p, ts.rad.p, ts.maxZ.p, ts.maxE.p,
            ts.maxY.p, ts.maxB.p, ts.beta.p, ts.maxZl.p, ts.nvalid.p, ts.row0.p,
            tabled ? (const uint32_t*)ts.row0.p : (const uint32_t*)nullptr,
-           tabled ? (const uint32_t*)ts.nvalid.p : (const uint32_t*)nullptr);
+           tabled ? (const uint32_t*)ts.nvalid.p : (const uint32_t*)nullptr, warp_rows);
 }
 
 void gather_rows(const std::vector<const void*>& srcs, const std::vector<long long>& rows, int d, int esize,

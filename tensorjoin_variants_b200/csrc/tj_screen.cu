@@ -321,14 +321,19 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 const ColMetaF& m = meta[slot];
                 const unsigned c0 = m.c0;
                 // per-(row, S tile) fast threshold; every error term bounded by tile maxima
-                float tau = -INFINITY;
+                //   v > tau       =>  D > Tp  (certainly out)
+                //   v <= tau_in   =>  D <= Tm (certainly in)
+                float tau = -INFINITY, tau_in = -INFINITY;
                 if (rvalid) {
                     const double WJ = m.WJ, FJ = m.FJ, YJ = m.YJ, BJ = m.BJ, betaJ = m.betaJ, WlJ = m.WlJ;
                     const double RiJ = jp.gmma * Zi * WJ + jp.cabs + Ei * YJ + Zi * FJ + Zli * WlJ;
                     const double PiJ = Zi * WJ * (1.0 + jp.gmma) + jp.cabs;
-                    double t = jp.Tp - Ai + jp.gn * Ai + 0x1p-23 * (BJ + 2.0 * PiJ) + betaJ + 2.0 * RiJ;
-                    t = t + fabs(t) * 0x1p-30 + 0x1p-1000;
+                    const double slack = jp.gn * Ai + 0x1p-23 * (BJ + 2.0 * PiJ) + betaJ + 2.0 * RiJ;
+                    // the 2^-40 / 2^-50 terms exceed the FP64 rounding of these sums even under cancellation
+                    const double t = jp.Tp - Ai + slack * (1.0 + 0x1p-40) + 0x1p-50 * (jp.Tp + Ai) + 0x1p-1000;
                     tau = f32_up(t);
+                    const double ti = jp.Tm - Ai - slack * (1.0 + 0x1p-40) - 0x1p-50 * (jp.Tm + Ai) - 0x1p-1000;
+                    tau_in = f32_dn(ti);
                 }
                 const unsigned tbase = tmem + ((q * 32u) << 16) + acc * kTileS;
 #pragma unroll 1
@@ -353,9 +358,16 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
                     }
                     if (!__any_sync(0xffffffffu, cmask != 0)) continue;
-                    // ---------------- rare path: per-pair FP64 certificate, operands from shared memory
-                    uint32_t amask = 0, bmask = 0;
-                    uint32_t mk = cmask;
+                    // ---------------- rare path: certified FP32 accept, else per-pair FP64 certificate
+                    uint32_t inm = 0;
+                    if (cmask) {
+#pragma unroll
+                        for (int k = 0; k < 32; ++k)
+                            inm |= (fmaf(-2.f, __uint_as_float(raw[k]), m.nrm2f[col0 + k]) <= tau_in ? 1u : 0u) << k;
+                        inm &= cmask;
+                    }
+                    uint32_t amask = inm, bmask = 0;
+                    uint32_t mk = cmask & ~inm;
                     while (mk) {
                         const int k = __ffs(mk) - 1;
                         mk &= mk - 1;
