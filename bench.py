@@ -298,6 +298,16 @@ def main() -> None:
             "result_pairs", "retries", "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total")},
     }
     line["stats"]["refined_fraction"] = st["band"] / max(1, st["pairs_screened"])
+    if screen not in ("plain", "int8limb"):   # screen error vs sequential FP64 on 64 sampled tile pairs
+        rd = tj.join_result(R, S, eps2=T, mode=mode, screen=screen, screen_diag=True)
+        sd = rd.stats
+        line["screen_error"] = {"max_abs_err_d2": sd["screen_max_abs_err"],
+                                "max_err_over_certified_radius": sd["screen_err_over_bound"],
+                                "pairs_sampled": sd["screen_err_pairs"], "eps2": float(T),
+                                "band_pairs": sd["band"], "refined_fraction": sd["band"] / max(1, sd["pairs_screened"])}
+        del rd
+    elif screen == "int8limb":
+        line["screen_error"] = {"max_abs_err_d2": 0, "note": "exact integer screen (int8 limbs, INT64 recombination)"}
 
     # plain FP32 direct-difference GPU join over the same candidate tile pairs (the baseline to beat)
     if not args.no_plain and screen != "plain":

@@ -65,8 +65,12 @@ typedef struct tj_index tj_index;
 typedef struct tj_options {
     int64_t initial_capacity;   /* accept / band buffer slots for the first attempt (0: library default) */
     int32_t chunk_items;        /* tile pairs per scheduling chunk (0: 64) */
-    int32_t flags;              /* reserved, must be 0 */
+    int32_t flags;              /* TJ_FLAG_* bits */
 } tj_options;
+
+/* Sample tile pairs during the tensor-core screen and report the screen's distance error against
+ * sequential FP64 distances (tj_stats.screen_*).  Diagnostic: adds a sampling pass. */
+#define TJ_FLAG_SCREEN_DIAG 1
 
 typedef struct tj_stats {
     int64_t n_rows, n_cols;       /* |R|, |S| (self-join: N, N) */
@@ -81,6 +85,9 @@ typedef struct tj_stats {
     int64_t retries;              /* capacity retries (overflow-and-retry passes) */
     double ms_index, ms_candidates, ms_screen, ms_refine, ms_sort, ms_total;   /* device time per stage */
     double screen_ops;            /* algorithmic screen operations: per pair 2d (16-bit), 6d (hi/lo split), 8d (int8 limbs) */
+    double screen_max_abs_err;    /* TJ_FLAG_SCREEN_DIAG: max |(|x|^2 + |y|^2 - 2p) - d2_fp64| over the sampled pairs */
+    double screen_err_over_bound; /* TJ_FLAG_SCREEN_DIAG: max of that error divided by the certified radius */
+    int64_t screen_err_pairs;     /* TJ_FLAG_SCREEN_DIAG: sampled pairs */
 } tj_stats;
 
 /* ----------------------------------------------------------------- joins */

@@ -122,7 +122,7 @@ class Result:
         return self._out(counts, flat)
 
 
-def _run(R, S, eps, eps2, mode: str, screen: str, capacity: int, chunk_items: int) -> Result:
+def _run(R, S, eps, eps2, mode: str, screen: str, capacity: int, chunk_items: int, flags: int = 0) -> Result:
     if screen not in SCREEN:
         raise ValueError(f"screen must be one of {sorted(SCREEN)}")
     Rt, host = _as_device(R, screen == "int8limb")
@@ -137,7 +137,7 @@ def _run(R, S, eps, eps2, mode: str, screen: str, capacity: int, chunk_items: in
         St = Rt
     T = _threshold(eps, eps2)
     dtype = _lib.DTYPE["i16"] if Rt.dtype == torch.int16 else _lib.DTYPE["f32"]
-    opt = _lib.Options(int(capacity), int(chunk_items), 0)
+    opt = _lib.Options(int(capacity), int(chunk_items), int(flags))
     h = C.c_void_p()
     check(lib().tj_join(C.c_void_p(Rt.data_ptr()), Rt.shape[0], C.c_void_p(St.data_ptr()), St.shape[0],
                         Rt.shape[1], dtype, T, MODE[mode], SCREEN[screen], C.byref(opt), C.byref(h),
@@ -146,11 +146,15 @@ def _run(R, S, eps, eps2, mode: str, screen: str, capacity: int, chunk_items: in
 
 
 def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "bf16", capacity: int = 0,
-                chunk_items: int = 0) -> Result:
-    """Run a join and return the Result handle (pairs, keys, neighbour table, statistics)."""
+                chunk_items: int = 0, screen_diag: bool = False) -> Result:
+    """Run a join and return the Result handle (pairs, keys, neighbour table, statistics).
+
+    ``screen_diag=True`` also samples 64 tile pairs of the tensor-core screen and reports, in
+    ``stats``, the screen's largest distance error against sequential FP64 distances and that
+    error relative to the certified radius (must stay below 1)."""
     if mode not in MODE:
         raise ValueError(f"mode must be one of {sorted(MODE)}")
-    return _run(R, S, eps, eps2, mode, screen, capacity, chunk_items)
+    return _run(R, S, eps, eps2, mode, screen, capacity, chunk_items, _lib.FLAG_SCREEN_DIAG if screen_diag else 0)
 
 
 def join(R, S, eps=None, *, eps2=None, screen: str = "bf16", return_stats: bool = False, **kw):

@@ -497,6 +497,27 @@ void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen
            (const uint4*)d_st.p, sops, &ctr.p->pad[0]);
     ev.rec(6, st);
 
+    // optional screen-error sampling (tensor-core screens): 64 tile pairs spread over the candidate list
+    const bool diag = opt && (opt->flags & TJ_FLAG_SCREEN_DIAG) && screen != TJ_SCREEN_PLAIN && !i8;
+    DBuf<float> dump;
+    DBuf<uint4> dump_ids;
+    DBuf<unsigned long long> diag_out;
+    if (diag) {
+        uint32_t tot = 0;
+        TJ_CUDA(cudaMemcpyAsync(&tot, cand.dev_counts.p, 4, cudaMemcpyDeviceToHost, st));
+        TJ_CUDA(cudaStreamSynchronize(st));
+        g.dump_items = 64;
+        g.dump_every = std::max(1u, tot / g.dump_items);
+        dump = DBuf<float>((size_t)g.dump_items * kTileR * kTileS, st);
+        dump_ids = DBuf<uint4>(g.dump_items, st);
+        diag_out = DBuf<unsigned long long>(3, st);
+        TJ_CUDA(cudaMemsetAsync(dump_ids.p, 0, g.dump_items * sizeof(uint4), st));
+        TJ_CUDA(cudaMemsetAsync(diag_out.p, 0, 3 * 8, st));
+        g.dump = dump.p;
+        g.dump_ids = dump_ids.p;
+        g.diag_out = diag_out.p;
+    }
+
     // screen + refine with overflow-and-retry
     unsigned long long sum_max = 0;
     for (const auto& j : joins) sum_max += (unsigned long long)std::max(j.nR, self ? j.nR : j.nS);
@@ -532,6 +553,14 @@ void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen
     S_.tile_pairs = (int64_t)h.items;
     S_.pairs_screened = (int64_t)h.pad[0];
     S_.screen_ops = (double)h.pad[1];
+    if (diag) {
+        unsigned long long dv[3] = {0, 0, 0};
+        TJ_CUDA(cudaMemcpyAsync(dv, diag_out.p, sizeof(dv), cudaMemcpyDeviceToHost, st));
+        TJ_CUDA(cudaStreamSynchronize(st));
+        memcpy(&S_.screen_max_abs_err, &dv[0], 8);
+        memcpy(&S_.screen_err_over_bound, &dv[1], 8);
+        S_.screen_err_pairs = (int64_t)dv[2];
+    }
     S_.screen_accept = (int64_t)h.screen_accept;
     S_.band = (int64_t)h.band_valid;
     S_.refine_accept = (int64_t)h.refine_accept;
@@ -592,7 +621,7 @@ int tj_join(const void* R, int64_t nR, const void* S, int64_t nS, int32_t d, int
     if (mode < 0 || mode > 2) fail(TJ_ERR_INVALID, "unknown mode");
     if (screen < 0 || screen > 5) fail(TJ_ERR_INVALID, "unknown screen");
     if (dtype != TJ_DTYPE_F32 && dtype != TJ_DTYPE_I16) fail(TJ_ERR_INVALID, "unknown dtype");
-    if (opt && opt->flags != 0) fail(TJ_ERR_INVALID, "options.flags must be 0");
+    if (opt && (opt->flags & ~TJ_FLAG_SCREEN_DIAG)) fail(TJ_ERR_INVALID, "unknown option flags");
     std::unique_ptr<tj_result> res(new tj_result());
     std::vector<JoinIn> js{JoinIn{R, (const void*)(mode == TJ_MODE_RS ? S : R), nR, mode == TJ_MODE_RS ? nS : nR,
                                   d, eps2}};
@@ -742,7 +771,7 @@ int tj_join_batched(const tj_batch_join* joins, int32_t njoins, int32_t screen, 
     *out = nullptr;
     if (njoins < 1) fail(TJ_ERR_INVALID, "njoins must be >= 1");
     if (screen < 0 || screen > 5 || screen == TJ_SCREEN_INT8LIMB) fail(TJ_ERR_UNSUPPORTED, "batched joins take FP32 screens");
-    if (opt && opt->flags != 0) fail(TJ_ERR_INVALID, "options.flags must be 0");
+    if (opt && (opt->flags & ~TJ_FLAG_SCREEN_DIAG)) fail(TJ_ERR_INVALID, "unknown option flags");
     std::vector<JoinIn> js((size_t)njoins);
     for (int k = 0; k < njoins; ++k) js[k] = JoinIn{joins[k].R, joins[k].S, joins[k].nR, joins[k].nS, joins[k].d, joins[k].eps2};
     std::unique_ptr<tj_result> res(new tj_result());

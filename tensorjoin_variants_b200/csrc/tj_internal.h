@@ -180,6 +180,11 @@ struct ScreenInput {
     const void* const* ssrc = nullptr;  // device [njoins]
     long long T_int = 0;                // integer threshold (int8-limb screen, single join)
     JoinParams jp0{};                   // host copy of join 0's parameters (single-join kernels)
+    // screen-error diagnostics (tensor-core screens): sampled accumulators and the analysis result
+    float* dump = nullptr;              // [dump_items][128][256]
+    uint4* dump_ids = nullptr;          // [dump_items]
+    unsigned dump_every = 0, dump_items = 0;
+    unsigned long long* diag_out = nullptr;   // [3]: max |d2hat - d2| (double bits), max ratio to bound, pairs
 };
 
 void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);

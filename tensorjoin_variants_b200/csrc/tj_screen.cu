@@ -122,6 +122,11 @@ struct ScreenArgs {
     uint64_t* band;
     unsigned long long band_cap;
     Counters* ctr;
+    // diagnostics: tile pairs with jlist index % dump_every == 0 write their accumulators (p values)
+    float* dump;               // [dump_items][128][256], null when off
+    uint4* dump_ids;           // [dump_items]: (global R tile, global S tile, 1, 0)
+    unsigned dump_every;
+    unsigned dump_items;
 };
 
 // r[k] for a runtime k without local memory: a fixed 31-select tree (the rare path's only way
@@ -342,6 +347,13 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     uint32_t raw[32];
                     tmem_ld32(tbase + col0, raw);
                     tmem_ld_wait();
+                    if (a.dump && e % a.dump_every == 0 && e / a.dump_every < a.dump_items) {
+                        const size_t slotd = e / a.dump_every;
+                        float* out = a.dump + (slotd * kTileR + row) * kTileS + col0;
+#pragma unroll
+                        for (int k = 0; k < 32; ++k) out[k] = __uint_as_float(raw[k]);
+                        if (row == 0 && cb == 0) a.dump_ids[slotd] = make_uint4(ch.x, a.jlist[e], 1u, 0u);
+                    }
                     if (cb == kTileS / 32 - 1) {   // accumulator fully read: hand it back to the MMA
                         tc_fence_before();
                         __syncwarp();
@@ -436,6 +448,58 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
     if (warp == 1) tmem_dealloc(tmem, 512);
 }
 
+// Screen error of the sampled tile pairs: |d2hat - d2| with d2hat = A + B - 2p from the dumped
+// accumulator and d2 the sequential FP64 distance of the original rows, and its ratio to the
+// certificate's radius (2R + norm terms).  Non-negative doubles are maximised as their bit patterns.
+__global__ void __launch_bounds__(256) screen_error_kernel(const ScreenArgs a, const float* dump, const uint4* ids,
+                                                           const void* const* rsrc, const void* const* ssrc,
+                                                           unsigned long long* out) {
+    const uint4 id = ids[blockIdx.x];
+    if (id.z != 1) return;
+    const uint4 rt = a.rtiles[id.x];
+    const uint4 st = a.stiles[id.y];
+    const ScreenClassArgs& ca = a.cls[rt.w];
+    const JoinParams jp = a.jps[rt.z];
+    const ColMetaF& m = a.s_meta[id.y];
+    const float* Rrows = (const float*)rsrc[rt.z];
+    const float* Srows = (const float*)ssrc[rt.z];
+    double emax = 0.0, rmax = 0.0;
+    unsigned long long cnt = 0;
+    for (int e = threadIdx.x; e < kTileR * kTileS; e += blockDim.x) {
+        const int row = e / kTileS, col = e % kTileS;
+        if (row >= (int)rt.y || col >= (int)st.y) continue;
+        const unsigned rs = rt.x + row;
+        const double p = (double)dump[(size_t)blockIdx.x * kTileR * kTileS + e];
+        const double Ai = ca.r_nrm2[rs], Bj = m.nrm2[col];
+        const double d2hat = Ai + Bj - 2.0 * p;
+        const float* x = Rrows + (size_t)ca.r_emit[rs] * jp.d;
+        const float* y = Srows + (size_t)m.perm[col] * jp.d;
+        double d2 = 0.0;
+        for (int k = 0; k < jp.d; ++k) {
+            const double t = __dsub_rn((double)x[k], (double)y[k]);
+            d2 = __dadd_rn(d2, __dmul_rn(t, t));
+        }
+        const double Zi = ca.r_zn[rs], Ei = ca.r_en[rs], Zli = ca.r_zl[rs];
+        const double R = jp.gmma * Zi * (double)m.zn[col] + jp.cabs + Ei * (double)m.yn[col] +
+                         Zi * (double)m.en[col] + Zli * (double)m.zl[col];
+        const double bound = 2.0 * R + jp.gn * (Ai + Bj);
+        const double err = fabs(d2hat - d2);
+        emax = fmax(emax, err);
+        rmax = fmax(rmax, bound > 0 ? err / bound : 0.0);
+        ++cnt;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+        rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out, (unsigned long long)__double_as_longlong(emax));
+        atomicMax(out + 1, (unsigned long long)__double_as_longlong(rmax));
+        atomicAdd(out + 2, cnt);
+    }
+}
+
 // ------------------------------------------------------------------ host side
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -516,6 +580,10 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     a.band = eb.band;
     a.band_cap = eb.band_cap;
     a.ctr = eb.ctr;
+    a.dump = g.dump;
+    a.dump_ids = g.dump_ids;
+    a.dump_every = g.dump_every ? g.dump_every : 1u;
+    a.dump_items = g.dump ? g.dump_items : 0u;
     const int grid = num_sms();
 #define TJ_SCREEN(F, SP)                                                                                    \
     do {                                                                                                    \
@@ -528,6 +596,9 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     else if (split) TJ_SCREEN(0, 1);
     else TJ_SCREEN(0, 0);
 #undef TJ_SCREEN
+    if (g.dump && g.dump_items)
+        launch(screen_error_kernel, g.dump_items, 256, 0, st, a, (const float*)g.dump, (const uint4*)g.dump_ids,
+               g.rsrc, g.ssrc, g.diag_out);
 }
 
 }  // namespace tj

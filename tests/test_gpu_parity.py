@@ -304,3 +304,31 @@ def test_batched_equals_single_joins():
     for (Rt, St, e), (i, j) in zip(dev, out):
         i1, j1 = tj.join(Rt, St, e, screen="bf16x3")
         assert torch.equal(i, i1) and torch.equal(j, j1)
+
+
+@pytest.mark.parametrize("screen", ["bf16", "fp16", "bf16x3", "fp16x3"])
+def test_screen_error_within_certified_radius(screen):
+    """Sampled tensor-core accumulators: the distance estimate's error against sequential FP64 stays
+    inside the certified radius (the accumulation premise holds on these inputs), and the result is
+    unchanged by the diagnostic pass."""
+    for w in (W.factor512(n=4000, samples=1 << 15), W.mixture64(n=8000, samples=1 << 15)):
+        R, S = torch.from_numpy(w.R).cuda(), torch.from_numpy(w.S).cuda()
+        res = tj.join_result(R, S, eps2=w.T, screen=screen, screen_diag=True)
+        st = res.stats
+        assert st["screen_err_pairs"] > 0
+        assert 0.0 < st["screen_err_over_bound"] < 1.0, st
+        k = res.keys().cpu().numpy().view(np.uint64)
+        assert_same(k, oracle_keys(w.R, w.S, w.T, "rs"), screen)
+
+
+def test_threshold_ties_float():
+    """T equal to the oracle's exact distance of chosen pairs: those pairs are in, nothing else changes."""
+    rng = np.random.default_rng(51)
+    R = rng.standard_normal((600, 64)).astype(np.float32)
+    S = rng.standard_normal((700, 64)).astype(np.float32)
+    ii = rng.integers(0, 600, 6)
+    jj = rng.integers(0, 700, 6)
+    for T in oracle.pair_d2(R, S, ii, jj):
+        for screen in ("bf16", "fp16x3", "plain"):
+            k, _ = gpu_keys(R, S, float(T), "rs", screen)
+            assert_same(k, oracle_keys(R, S, float(T), "rs"), f"tie {screen}")
