@@ -245,16 +245,19 @@ def main() -> None:
     ev0.record(stream)
     stats = []
     count = 0
-    for _ in range(args.steps):
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for s_ in range(args.steps):
         res, i, j = step()
         stats.append(res.stats)
         count = res.count
         del res, i, j
+        marks[s_].record(stream)
     ev1.record(stream)
     torch.cuda.synchronize()
     launches = _lib.lib().tj_kernel_launches() - launches0
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1) / args.steps
+    step_ms = [(ev0 if k == 0 else marks[k - 1]).elapsed_time(marks[k]) for k in range(args.steps)]
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -293,7 +296,8 @@ def main() -> None:
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": {"plain": "f32", "int8limb": "s8"}.get(screen, screen), "data": "synthetic",
         "config": workload_config(args, w), "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
-        "result_pairs": int(count), "stats": {k: st[k] for k in (
+        "result_pairs": int(count), "step_ms": step_ms, "lib_ms_total": [s["ms_total"] for s in stats],
+        "stats": {k: st[k] for k in (
             "pairs_all", "pairs_screened", "tile_pairs", "screen_accept", "band", "refine_accept", "rare_checks",
             "result_pairs", "retries", "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total")},
     }
@@ -446,16 +450,19 @@ def ragged_bench(args, rank, world, screen, dist):
     torch.cuda.synchronize()
     e0.record(stream)
     stats = []
-    for _ in range(args.steps):
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for s_ in range(args.steps):
         r = step(screen)
         stats.append(r.stats)
         pairs_out = r.count
         del r
+        marks[s_].record(stream)
     e1.record(stream)
     torch.cuda.synchronize()
     launches = _lib.lib().tj_kernel_launches() - l0
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / args.steps
+    step_ms = [(e0 if k == 0 else marks[k - 1]).elapsed_time(marks[k]) for k in range(args.steps)]
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -492,6 +499,7 @@ def ragged_bench(args, rank, world, screen, dist):
                      "peak_source": f"{peaks['source']} bf16_tflops_sustained", "traffic": None,
                      "screen_ms": screen_ms, "flops_per_launch": ops},
         "clocks": clk, "gpu_launches": int(launches), "result_pairs": int(pairs_out),
+        "step_ms": step_ms, "lib_ms_total": [s["ms_total"] for s in stats],
         "batch": {"joins_per_s": nj / (ms / 1000.0), "ms_per_join_amortised": ms / nj,
                   "single_join_latency_ms_p50": float(np.percentile(lat, 50)),
                   "single_join_latency_ms_p99": float(np.percentile(lat, 99)), "latency_sample": len(lat)},

@@ -160,6 +160,19 @@ int tj_device_sm_count(void);
 /* Running total of kernels this library has launched in the process (audit of timed regions). */
 int64_t tj_kernel_launches(void);
 
+/* The current device's memory pool, from which every join's temporaries and results are drawn
+ * (stream-ordered; memory freed by one join is reused by the next).  No counterpart in the
+ * reference, whose scripts allocated through torch.
+ * tj_pool_usage: bytes the pool holds from the driver, bytes in live allocations, and the peak of
+ * the former (any pointer may be NULL).
+ * tj_pool_reserve: makes the pool hold at least `bytes` (one allocation and free on `stream`, then a
+ * synchronisation of `stream`), so that later joins need not map new device memory.
+ * tj_pool_trim: returns held memory above `keep_bytes` to the driver (memory of frees still pending
+ * on a stream is kept until they complete). */
+int tj_pool_usage(int64_t* reserved, int64_t* used, int64_t* reserved_high);
+int tj_pool_reserve(int64_t bytes, void* stream);
+int tj_pool_trim(int64_t keep_bytes);
+
 #ifdef __cplusplus
 }
 #endif

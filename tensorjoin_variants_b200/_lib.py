@@ -29,6 +29,7 @@ EXPORTS = [
     "tj_result_neighbor_table", "tj_result_free", "tj_index_build", "tj_index_info", "tj_index_copy",
     "tj_index_free", "tj_join_batched", "tj_batch_offsets", "tj_batch_pairs", "tj_last_error_string",
     "tj_version", "tj_device_sm_count", "tj_kernel_launches", "tj_sort_keys_noalloc",
+    "tj_pool_usage", "tj_pool_reserve", "tj_pool_trim",
 ]
 
 
@@ -93,6 +94,12 @@ def lib() -> C.CDLL:
     L.tj_kernel_launches.restype = C.c_int64
     L.tj_sort_keys_noalloc.argtypes = [P, P, I64, I32, P]
     L.tj_sort_keys_noalloc.restype = C.c_int
+    L.tj_pool_usage.argtypes = [C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]
+    L.tj_pool_usage.restype = C.c_int
+    L.tj_pool_reserve.argtypes = [I64, P]
+    L.tj_pool_reserve.restype = C.c_int
+    L.tj_pool_trim.argtypes = [I64]
+    L.tj_pool_trim.restype = C.c_int
     for name in ("tj_join", "tj_result_stats", "tj_result_pairs", "tj_result_keys", "tj_result_neighbor_table",
                  "tj_index_build", "tj_index_info", "tj_index_copy", "tj_join_batched", "tj_batch_offsets",
                  "tj_batch_pairs"):

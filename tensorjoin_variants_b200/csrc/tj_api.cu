@@ -6,6 +6,7 @@
 // overflow-and-retry pass of the reference, src/run_g2a_tensorjoin.py:329-378).
 // Everything else stays on the device in stream order; memory comes from a
 // private stream-ordered pool so repeated joins do not hit cudaMalloc.
+#include <chrono>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -56,9 +57,31 @@ cudaMemPool_t pool_for_current() {
 }
 }  // namespace
 
+// TJ_TRACE_ALLOC=<ms> in the environment logs, to stderr, every pool allocation whose host call
+// took longer than <ms> milliseconds, with the pool's reserved / used bytes afterwards.
+static double trace_alloc_ms() {
+    static const double v = [] {
+        const char* e = getenv("TJ_TRACE_ALLOC");
+        return e ? atof(e) : -1.0;
+    }();
+    return v;
+}
+
 void* dalloc(size_t bytes, cudaStream_t st) {
     void* p = nullptr;
+    const double lim = trace_alloc_ms();
+    const auto t0 = std::chrono::steady_clock::now();
     const cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool_for_current(), st);
+    if (lim >= 0.0) {
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms > lim) {
+            uint64_t res = 0, used = 0;
+            cudaMemPoolGetAttribute(pool_for_current(), cudaMemPoolAttrReservedMemCurrent, &res);
+            cudaMemPoolGetAttribute(pool_for_current(), cudaMemPoolAttrUsedMemCurrent, &used);
+            fprintf(stderr, "[tj alloc] %zu bytes took %.2f ms (pool reserved %llu MiB, used %llu MiB)\n", bytes, ms,
+                    (unsigned long long)(res >> 20), (unsigned long long)(used >> 20));
+        }
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         fail(TJ_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
@@ -74,6 +97,49 @@ namespace {
 std::atomic<long long> g_launches{0};
 }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+namespace {
+struct StageChunk {
+    uint8_t* p = nullptr;
+    size_t cap = 0, used = 0;
+};
+thread_local std::vector<StageChunk> g_stage;
+thread_local cudaEvent_t g_stage_done = nullptr;   // recorded after the latest staged copy
+thread_local bool g_stage_pending = false;
+}  // namespace
+
+// Makes every staging region reusable.  Waits for the last staged copy first (a call that failed
+// part-way may have left one in flight); on the normal path the join already synchronised, so the
+// wait returns at once.
+void stage_reset() {
+    if (g_stage_pending) {
+        TJ_CUDA(cudaEventSynchronize(g_stage_done));
+        g_stage_pending = false;
+    }
+    for (auto& c : g_stage) c.used = 0;
+}
+
+void upload(void* dev_dst, const void* host_src, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return;
+    const size_t need = (bytes + 255) & ~(size_t)255;
+    StageChunk* ch = nullptr;
+    for (auto& c : g_stage)
+        if (c.cap - c.used >= need) { ch = &c; break; }
+    if (!ch) {
+        StageChunk c;
+        c.cap = std::max<size_t>(need, (size_t)4 << 20);
+        TJ_CUDA(cudaMallocHost((void**)&c.p, c.cap));
+        g_stage.push_back(c);
+        ch = &g_stage.back();
+    }
+    uint8_t* src = ch->p + ch->used;
+    ch->used += need;
+    memcpy(src, host_src, bytes);
+    TJ_CUDA(cudaMemcpyAsync(dev_dst, src, bytes, cudaMemcpyHostToDevice, st));
+    if (!g_stage_done) TJ_CUDA(cudaEventCreateWithFlags(&g_stage_done, cudaEventDisableTiming));
+    TJ_CUDA(cudaEventRecord(g_stage_done, st));
+    g_stage_pending = true;
+}
 
 int num_sms() {
     int dev = 0;
@@ -320,6 +386,7 @@ void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen
         if (nj > 1) res->offsets.assign(nj + 1, 0);
         return;
     }
+    stage_reset();
     Events ev;
     ev.rec(0, st);
     DBuf<Counters> ctr(1, st);
@@ -359,16 +426,33 @@ void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen
                 pr.push_back(joins[J[q]].R); nr.push_back(joins[J[q]].nR);
                 ps.push_back(joins[J[q]].S); ns.push_back(joins[J[q]].nS);
             }
-            K.XR = DBuf<float>((size_t)roR[njc] * d, st);
-            K.XS = DBuf<float>((size_t)roS[njc] * d, st);
-            gather_rows(pr, nr, d, esize, K.XR.p, st);
-            gather_rows(ps, ns, d, esize, K.XS.p, st);
-            srcR = K.XR.p;
-            srcS = K.XS.p;
+            // joins whose rows already lie back to back in one array (views of one tensor) are used
+            // in place; otherwise the class's rows are gathered into one array
+            auto adjacent = [&](const std::vector<const void*>& p, const std::vector<long long>& n) {
+                for (size_t q = 0; q + 1 < p.size(); ++q)
+                    if ((const char*)p[q] + (size_t)n[q] * d * esize != (const char*)p[q + 1]) return false;
+                return true;
+            };
+            if (adjacent(pr, nr)) {
+                srcR = pr[0];
+            } else {
+                K.XR = DBuf<float>((size_t)roR[njc] * d, st);
+                gather_rows(pr, nr, d, esize, K.XR.p, st);
+                srcR = K.XR.p;
+            }
+            if (self) {
+                srcS = srcR;
+            } else if (adjacent(ps, ns)) {
+                srcS = ps[0];
+            } else {
+                K.XS = DBuf<float>((size_t)roS[njc] * d, st);
+                gather_rows(ps, ns, d, esize, K.XS.p, st);
+                srcS = K.XS.p;
+            }
             K.rowoffR = DBuf<long long>((size_t)njc + 1, st);
             K.rowoffS = DBuf<long long>((size_t)njc + 1, st);
-            TJ_CUDA(cudaMemcpyAsync(K.rowoffR.p, roR.data(), (njc + 1) * 8, cudaMemcpyHostToDevice, st));
-            TJ_CUDA(cudaMemcpyAsync(K.rowoffS.p, roS.data(), (njc + 1) * 8, cudaMemcpyHostToDevice, st));
+            upload(K.rowoffR.p, roR.data(), (njc + 1) * 8, st);
+            upload(K.rowoffS.p, roS.data(), (njc + 1) * 8, st);
         }
         K.fp = DBuf<FrameParams>(1, st);
         K.center = DBuf<float>((size_t)d, st);
@@ -432,16 +516,17 @@ void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen
     DBuf<const void*> d_rsrc((size_t)nj, st), d_ssrc((size_t)nj, st);
     std::vector<const void*> hr(nj), hs(nj);
     for (int k = 0; k < nj; ++k) { hr[k] = joins[k].R; hs[k] = self ? joins[k].R : joins[k].S; }
-    TJ_CUDA(cudaMemcpyAsync(d_rt.p, rtiles.data(), rtiles.size() * sizeof(uint4), cudaMemcpyHostToDevice, st));
-    TJ_CUDA(cudaMemcpyAsync(d_st.p, stiles.data(), stiles.size() * sizeof(uint4), cudaMemcpyHostToDevice, st));
-    TJ_CUDA(cudaMemcpyAsync(d_jps.p, jps.data(), nj * sizeof(JoinParams), cudaMemcpyHostToDevice, st));
-    TJ_CUDA(cudaMemcpyAsync(d_koff.p, key_off.data(), nj * 8, cudaMemcpyHostToDevice, st));
-    TJ_CUDA(cudaMemcpyAsync(d_cols.p, ncols.data(), nj * 8, cudaMemcpyHostToDevice, st));
-    TJ_CUDA(cudaMemcpyAsync(d_rsrc.p, hr.data(), nj * sizeof(void*), cudaMemcpyHostToDevice, st));
-    TJ_CUDA(cudaMemcpyAsync(d_ssrc.p, hs.data(), nj * sizeof(void*), cudaMemcpyHostToDevice, st));
+    upload(d_rt.p, rtiles.data(), rtiles.size() * sizeof(uint4), st);
+    upload(d_st.p, stiles.data(), stiles.size() * sizeof(uint4), st);
+    upload(d_jps.p, jps.data(), nj * sizeof(JoinParams), st);
+    upload(d_koff.p, key_off.data(), nj * 8, st);
+    upload(d_cols.p, ncols.data(), nj * 8, st);
+    upload(d_rsrc.p, hr.data(), nj * sizeof(void*), st);
+    upload(d_ssrc.p, hs.data(), nj * sizeof(void*), st);
     g.rtiles = d_rt.p;
     g.stiles = d_st.p;
     g.jps = d_jps.p;
+    g.h_jps = jps.data();
     g.key_off = d_koff.p;
     g.rsrc = d_rsrc.p;
     g.ssrc = d_ssrc.p;
@@ -689,6 +774,7 @@ int tj_index_build(const void* X, int64_t n, int32_t d, int32_t dtype, double ep
     if (n >= (1ll << 32)) fail(TJ_ERR_INVALID, "more than 2^32 - 1 rows");
     if (dtype != TJ_DTYPE_F32 && dtype != TJ_DTYPE_I16) fail(TJ_ERR_INVALID, "unknown dtype");
     cudaStream_t st = (cudaStream_t)stream;
+    stage_reset();
     std::unique_ptr<tj_index> ix(new tj_index());
     DBuf<Counters> ctr(1, st);
     launch(zero_counters, 1, 32, 0, st, ctr.p, 0);
@@ -817,6 +903,44 @@ int tj_device_sm_count(void) {
     } catch (...) {
         return -1;
     }
+}
+
+int tj_pool_usage(int64_t* reserved, int64_t* used, int64_t* reserved_high) {
+    TJ_API_BEGIN
+    cudaMemPool_t pool = pool_for_current();
+    uint64_t v = 0;
+    if (reserved) { TJ_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v)); *reserved = (int64_t)v; }
+    if (used) { TJ_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &v)); *used = (int64_t)v; }
+    if (reserved_high) {
+        TJ_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemHigh, &v));
+        *reserved_high = (int64_t)v;
+    }
+    return TJ_OK;
+    TJ_API_END
+}
+
+int tj_pool_reserve(int64_t bytes, void* stream) {
+    TJ_API_BEGIN
+    if (bytes < 0) fail(TJ_ERR_INVALID, "bytes must be >= 0");
+    cudaMemPool_t pool = pool_for_current();
+    uint64_t have = 0;
+    TJ_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &have));
+    if ((uint64_t)bytes > have) {
+        cudaStream_t st = (cudaStream_t)stream;
+        void* p = dalloc((size_t)bytes, st);
+        dfree(p, st);
+        TJ_CUDA(cudaStreamSynchronize(st));
+    }
+    return TJ_OK;
+    TJ_API_END
+}
+
+int tj_pool_trim(int64_t keep_bytes) {
+    TJ_API_BEGIN
+    if (keep_bytes < 0) fail(TJ_ERR_INVALID, "keep_bytes must be >= 0");
+    TJ_CUDA(cudaMemPoolTrimTo(pool_for_current(), (size_t)keep_bytes));
+    return TJ_OK;
+    TJ_API_END
 }
 
 }  // extern "C"

@@ -16,7 +16,7 @@ namespace tj {
 constexpr int kWarp = 32;
 constexpr int kTileR = 128;     // R-side tile rows (UMMA M)
 constexpr int kTileS = 256;     // S-side tile rows (UMMA N)
-constexpr int kBK = 64;         // 16-bit elements per k-block = one 128-byte swizzle row
+constexpr int kBK = 64;         // 16-bit elements per k-block = one 128-byte swizzle row (widest)
 constexpr uint64_t kSentinel = ~0ull;
 
 // Device status word bits (written with atomicOr, read by the host once per join).
@@ -199,6 +199,19 @@ TJ_DEV uint64_t desc_sw128(const void* smem_base, unsigned byte_off) {
     d |= (uint64_t)1u << 46;                        // descriptor version (sm_100)
     d |= (uint64_t)2u << 61;                        // layout: SWIZZLE_128B
     return d;
+}
+
+// The same descriptor for a K-major operand whose rows are `row_bytes` = 32, 64 or 128 bytes
+// (16, 32 or 64 16-bit elements), written by a TMA box of that width with the matching
+// CU_TENSOR_MAP_SWIZZLE_32B / 64B / 128B mode: atoms of 8 rows, stride byte offset 8 * row_bytes,
+// layout code 6 / 4 / 2.  The constant upper half is computed once on the host (desc_hi).
+__host__ __device__ constexpr uint32_t desc_hi_for_rows(unsigned row_bytes) {
+    return ((8u * row_bytes) >> 4) | (1u << 14) |
+           ((row_bytes == 32u ? 6u : row_bytes == 64u ? 4u : 2u) << 29);
+}
+TJ_DEV uint64_t desc_kmajor(const void* smem_base, unsigned byte_off, uint32_t desc_hi) {
+    const unsigned a = smem_u32(smem_base) + byte_off;
+    return ((uint64_t)desc_hi << 32) | (uint64_t)(1u << 16) | (uint64_t)((a >> 4) & 0x3FFFu);
 }
 
 // UMMA instruction descriptor (kind::f16 / kind::i8, dense, K-major A and B).

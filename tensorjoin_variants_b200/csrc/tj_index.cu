@@ -75,26 +75,40 @@ __global__ void __launch_bounds__(256) dim_stats_partial(const void* src, int dt
     }
 }
 
-// Deterministic reduction of the partials (one thread per dimension, fixed block order):
-// variance, range and the centre (per-dimension mean, FP32) used to centre the MMA operands.
-__global__ void dim_reduce(const float* pmin, const float* pmax, const double* psum, const double* psq, int nparts,
-                           long long ntot, int d, float* var_ws, float* lo_ws, float* hi_ws, float* center) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= d) return;
+// Deterministic reduction of the partials (one block per dimension, a fixed-shape tree over the
+// partial blocks): variance, range and the centre (per-dimension mean, FP32) used to centre the
+// MMA operands.
+__global__ void __launch_bounds__(256) dim_reduce(const float* pmin, const float* pmax, const double* psum,
+                                                  const double* psq, int nparts, long long ntot, int d,
+                                                  float* var_ws, float* lo_ws, float* hi_ws, float* center) {
+    __shared__ double ss[256], sq[256];
+    __shared__ float smn[256], smx[256];
+    const int k = blockIdx.x, t = threadIdx.x;
     float mn = INFINITY, mx = -INFINITY;
     double s = 0.0, q = 0.0;
-    for (int b = 0; b < nparts; ++b) {
+    for (int b = t; b < nparts; b += blockDim.x) {
         const size_t o = (size_t)b * d + k;
         mn = fminf(mn, pmin[o]);
         mx = fmaxf(mx, pmax[o]);
         s += psum[o];
         q += psq[o];
     }
-    const double mean = ntot ? s / (double)ntot : 0.0;
-    var_ws[k] = ntot ? (float)fmax(0.0, q / (double)ntot - mean * mean) : 0.f;
-    lo_ws[k] = mn;
-    hi_ws[k] = mx;
-    center[k] = isfinite(mean) ? (float)mean : 0.f;
+    ss[t] = s; sq[t] = q; smn[t] = mn; smx[t] = mx;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (t < w) {
+            ss[t] += ss[t + w]; sq[t] += sq[t + w];
+            smn[t] = fminf(smn[t], smn[t + w]); smx[t] = fmaxf(smx[t], smx[t + w]);
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        const double mean = ntot ? ss[0] / (double)ntot : 0.0;
+        var_ws[k] = ntot ? (float)fmax(0.0, sq[0] / (double)ntot - mean * mean) : 0.f;
+        lo_ws[k] = smn[0];
+        hi_ws[k] = smx[0];
+        center[k] = isfinite(mean) ? (float)mean : 0.f;
+    }
 }
 
 // Pick the m = min(d, 8) highest-variance dimensions and their quantisation frame.
@@ -620,7 +634,7 @@ void compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d
         launch(dim_stats_partial, nb, 256, 0, st, srcs[s], dtype, ns[s], d, pmin.p, pmax.p, psum.p, psq.p,
                                               s * kStatBlocks);
     }
-    launch(dim_reduce, (unsigned)((d + 127) / 128), 128, 0, st, pmin.p, pmax.p, psum.p, psq.p, parts, ntot, d, ws.p,
+    launch(dim_reduce, (unsigned)d, 256, 0, st, pmin.p, pmax.p, psum.p, psq.p, parts, ntot, d, ws.p,
            ws.p + d, ws.p + 2 * d, center);
     launch(frame_pick, 1, 32, 0, st, d, ws.p, ws.p + d, ws.p + 2 * d, fp);
     TJ_CUDA(cudaGetLastError());
@@ -631,7 +645,10 @@ void prepare_side(Side& s, const FrameParams* fpd, const float* center, cudaStre
     const long long n = s.n;
     const bool i8 = s.screen == kScreenInt8Limb;
     s.split = (s.screen == kScreenBF16X3 || s.screen == kScreenFP16X3) ? 1 : 0;
-    s.kpad = i8 ? ((s.d + 127) / 128) * 128 : ((s.d + kBK - 1) / kBK) * kBK;
+    // 16-bit operands: rows of 16 or 32 elements for small d (32- / 64-byte swizzle), else a
+    // multiple of 64 (128-byte swizzle); int8 limbs: a multiple of 128
+    s.kpad = i8 ? ((s.d + 127) / 128) * 128
+                : s.d <= 16 ? 16 : s.d <= 32 ? 32 : ((s.d + kBK - 1) / kBK) * kBK;
     s.rows_pad = ((std::max<long long>(n, 1) + kTileS - 1) / kTileS) * kTileS;
     s.perm = DBuf<uint32_t>((size_t)std::max<long long>(n, 1), st);
     s.keys = DBuf<uint64_t>((size_t)std::max<long long>(n, 1), st);
@@ -695,8 +712,8 @@ void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st) {
     ts.row0 = DBuf<uint32_t>(nt, st);
     if (ts.ntiles == 0) return;
     if (tabled) {
-        TJ_CUDA(cudaMemcpyAsync(ts.row0.p, ts.h_row0.data(), nt * 4, cudaMemcpyHostToDevice, st));
-        TJ_CUDA(cudaMemcpyAsync(ts.nvalid.p, ts.h_nvalid.data(), nt * 4, cudaMemcpyHostToDevice, st));
+        upload(ts.row0.p, ts.h_row0.data(), nt * 4, st);
+        upload(ts.nvalid.p, ts.h_nvalid.data(), nt * 4, st);
     }
     // centroid [d] floats (rounded up to an even count) + per-warp partials (8 x d x (8 + 4 + 4) bytes)
     const size_t base = (size_t)((s.d + 1) & ~1) * sizeof(float);
@@ -719,8 +736,8 @@ void gather_rows(const std::vector<const void*>& srcs, const std::vector<long lo
     for (int k = 0; k < ns; ++k) off[k + 1] = off[k] + rows[k];
     DBuf<const void*> dsrc((size_t)ns, st);
     DBuf<long long> doff((size_t)ns + 1, st);
-    TJ_CUDA(cudaMemcpyAsync(dsrc.p, srcs.data(), ns * sizeof(void*), cudaMemcpyHostToDevice, st));
-    TJ_CUDA(cudaMemcpyAsync(doff.p, off.data(), (ns + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+    upload(dsrc.p, srcs.data(), ns * sizeof(void*), st);
+    upload(doff.p, off.data(), (ns + 1) * sizeof(long long), st);
     const long long n = off[ns];
     if (n == 0) return;
     launch(gather_rows_kernel, (unsigned)((n + 7) / 8), 256, 0, st, (const void* const*)dsrc.p,
@@ -807,11 +824,10 @@ void build_candidates_batched(const std::vector<CandClassView>& classes, const s
     DBuf<CandClassView> dview(classes.size(), st);
     DBuf<double> dtp((size_t)nb, st);
     DBuf<uint32_t> dsb((size_t)ntR, st);
-    TJ_CUDA(cudaMemcpyAsync(dblk.p, blocks.data(), nb * sizeof(CandBlock), cudaMemcpyHostToDevice, st));
-    TJ_CUDA(cudaMemcpyAsync(dview.p, classes.data(), classes.size() * sizeof(CandClassView), cudaMemcpyHostToDevice,
-                            st));
-    TJ_CUDA(cudaMemcpyAsync(dtp.p, Tp_per_block.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
-    TJ_CUDA(cudaMemcpyAsync(dsb.p, rtile_sbase.data(), ntR * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    upload(dblk.p, blocks.data(), nb * sizeof(CandBlock), st);
+    upload(dview.p, classes.data(), classes.size() * sizeof(CandClassView), st);
+    upload(dtp.p, Tp_per_block.data(), nb * sizeof(double), st);
+    upload(dsb.p, rtile_sbase.data(), ntR * sizeof(uint32_t), st);
     DBuf<uint32_t> bitmap((size_t)ntR * words, st);
     TJ_CUDA(cudaMemsetAsync(bitmap.p, 0, bitmap.bytes(), st));
     const size_t smem = (size_t)3 * 16 * dmax * sizeof(float);

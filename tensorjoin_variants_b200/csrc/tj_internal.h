@@ -44,6 +44,12 @@ struct DBuf {
     size_t bytes() const { return n * sizeof(T); }
 };
 
+// Host -> device copy of a small host table through a per-thread pinned staging arena, so the copy
+// is asynchronous (a pageable source would make cudaMemcpyAsync wait for the stream).  Staging
+// regions are reused only after stage_reset(), which waits for the last staged copy.
+void upload(void* dev_dst, const void* host_src, size_t bytes, cudaStream_t st);
+void stage_reset();
+
 // ------------------------------------------------------------------ scan / sort (tj_sort.cu)
 size_t scan_workspace_elems(size_t n);
 void exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* total, uint32_t* ws,
@@ -174,6 +180,7 @@ struct ScreenInput {
     const uint4* stiles = nullptr;      // device [ntS_total]
     const Candidates* cand = nullptr;
     const JoinParams* jps = nullptr;    // device [njoins]
+    const JoinParams* h_jps = nullptr;  // host copy of the same table
     int njoins = 0;
     const unsigned long long* key_off = nullptr;   // device [njoins]: ascending key offsets
     const void* const* rsrc = nullptr;  // device [njoins]: caller's R rows of each join

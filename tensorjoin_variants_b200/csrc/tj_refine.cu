@@ -316,9 +316,8 @@ void screen_plain(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) 
         a.cls[c].d = R.d;
     }
     // per join: FP32 sum of d squared FP32 differences with FMA: |s - D| <= gamma_{d+2} D + d 2^-148 (u = 2^-24)
-    std::vector<JoinParams> hj((size_t)g.njoins);
-    TJ_CUDA(cudaMemcpyAsync(hj.data(), g.jps, g.njoins * sizeof(JoinParams), cudaMemcpyDeviceToHost, st));
-    TJ_CUDA(cudaStreamSynchronize(st));
+    const JoinParams* hj = g.h_jps;
+    if (!hj) fail(-1, "screen_plain needs the host join parameters");
     std::vector<float2> th((size_t)g.njoins);
     for (int k = 0; k < g.njoins; ++k) {
         const double u = 0x1p-24, nu = (double)(hj[k].d + 4) * u;
@@ -333,7 +332,7 @@ void screen_plain(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) 
         th[k] = make_float2(fin, fout);
     }
     DBuf<float2> dth((size_t)g.njoins, st);
-    TJ_CUDA(cudaMemcpyAsync(dth.p, th.data(), g.njoins * sizeof(float2), cudaMemcpyHostToDevice, st));
+    upload(dth.p, th.data(), g.njoins * sizeof(float2), st);
     a.chunks = g.cand->chunks.p;
     a.nchunks = g.cand->dev_counts.p + 1;
     a.jlist = g.cand->jlist.p;
@@ -347,7 +346,6 @@ void screen_plain(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) 
     a.band_cap = eb.band_cap;
     a.ctr = eb.ctr;
     launch(plain_kernel, num_sms() * 2, kPT, 0, st, a);
-    TJ_CUDA(cudaStreamSynchronize(st));   // the host threshold table is uploaded from this frame
 }
 
 void refine_band(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {

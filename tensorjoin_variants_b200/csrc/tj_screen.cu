@@ -28,8 +28,10 @@
 //           ring of per-item column-metadata blocks (one 8 KB bulk copy per S tile), so the
 //           epilogue never waits on global memory inside an item
 //   warp 1: TMEM allocator + UMMA issuer (one lane), 2 accumulators x 256 columns
-//   warps 2-5: epilogue, warp w reads TMEM lanes 32*(w%4) .. +31 (one R row per thread); the four
-//           warps run independently (no named barrier), synchronised only through mbarriers
+//   warps 2-9: epilogue, warp w reads TMEM lanes 32*(w%4) .. +31 (one R row per thread) and
+//           columns 128*((w-2)/4) .. +127 of the accumulator, so every SM sub-partition runs two
+//           epilogue warps that hide each other's TMEM and shared-memory latency; the eight warps
+//           run independently (no named barrier), synchronised only through mbarriers
 #include <algorithm>
 #include <cstring>
 
@@ -41,7 +43,7 @@ namespace tj {
 namespace {
 
 constexpr int kAccBufs = 2;
-constexpr int kEpiWarps = 4;
+constexpr int kEpiWarps = 8;                        // two per TMEM lane quarter (column halves)
 constexpr int kScreenThreads = (2 + kEpiWarps) * 32;
 constexpr unsigned kABytes = kTileR * 128;          // 16 KB
 constexpr unsigned kBBytes = kTileS * 128;          // 32 KB
@@ -97,8 +99,11 @@ struct ScreenClassArgs {
     const float* r_zn;
     const float* r_en;
     const float* r_zl;
-    int kblocks;
-    int kpad;
+    int kblocks;              // kpad / kbk
+    int kpad;                 // operand row length (16, 32 or a multiple of 64 elements)
+    int kbk;                  // elements per k-block: 16, 32 or 64 (32-, 64- or 128-byte swizzle)
+    unsigned tx_bytes;        // bytes one stage receives for this class
+    uint32_t desc_hi;         // upper half of the UMMA shared-memory descriptors
 };
 
 struct TMaps {
@@ -221,7 +226,8 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 const uint4 rt = a.rtiles[ch.x];
                 const int rrow = (int)rt.x;
                 const unsigned cls = rt.w;
-                const int kblocks = a.cls[cls].kblocks, kpad = a.cls[cls].kpad;
+                const int kblocks = a.cls[cls].kblocks, kpad = a.cls[cls].kpad, kbk = a.cls[cls].kbk;
+                const unsigned tx = a.cls[cls].tx_bytes;
                 const CUtensorMap* mA = &tm.a[cls];
                 const CUtensorMap* mB = &tm.b[cls];
                 for (unsigned e = ch.y; e < ch.z && ok; ++e, ++n) {
@@ -235,12 +241,12 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         uint8_t* sa = smem + (size_t)stage * kStageBytes;
-                        mbar_arrive_expect_tx(&ctl->full[stage], kStageBytes);
-                        tma_load_2d(sa, mA, &ctl->full[stage], kb * kBK, rrow);
-                        tma_load_2d(sa + Cfg::kBhi, mB, &ctl->full[stage], kb * kBK, srow);
+                        mbar_arrive_expect_tx(&ctl->full[stage], tx);
+                        tma_load_2d(sa, mA, &ctl->full[stage], kb * kbk, rrow);
+                        tma_load_2d(sa + Cfg::kBhi, mB, &ctl->full[stage], kb * kbk, srow);
                         if (kSplit) {
-                            tma_load_2d(sa + Cfg::kAlo, mA, &ctl->full[stage], kpad + kb * kBK, rrow);
-                            tma_load_2d(sa + Cfg::kBlo, mB, &ctl->full[stage], kpad + kb * kBK, srow);
+                            tma_load_2d(sa + Cfg::kAlo, mA, &ctl->full[stage], kpad + kb * kbk, rrow);
+                            tma_load_2d(sa + Cfg::kBlo, mB, &ctl->full[stage], kpad + kb * kbk, srow);
                         }
                         if (++stage == kStages) { stage = 0; phase ^= 1; }
                     }
@@ -265,7 +271,9 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             bool ok = true;
             for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
                 const uint4 ch = a.chunks[c];
-                const int kblocks = a.cls[a.rtiles[ch.x].w].kblocks;
+                const ScreenClassArgs& ca = a.cls[a.rtiles[ch.x].w];
+                const int kblocks = ca.kblocks, ksteps = ca.kbk / 16;
+                const uint32_t dh = ca.desc_hi;
                 for (unsigned e = ch.y; e < ch.z && ok; ++e) {
                     if (!mbar_wait(&ctl->acc_empty[acc], acc_phase ^ 1, status)) { ok = false; break; }
                     tc_fence_after();
@@ -277,12 +285,13 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         const uint8_t* sa = smem + (size_t)stage * kStageBytes;
 #pragma unroll
                         for (int k = 0; k < kBK / 16; ++k) {
-                            const uint64_t ad = desc_sw128(sa, k * 32);
-                            const uint64_t bd = desc_sw128(sa + Cfg::kBhi, k * 32);
+                            if (k >= ksteps) break;
+                            const uint64_t ad = desc_kmajor(sa, k * 32, dh);
+                            const uint64_t bd = desc_kmajor(sa + Cfg::kBhi, k * 32, dh);
                             umma_f16(d_tmem, ad, bd, a.idesc, (kb | k) != 0 ? 1u : 0u);
                             if (kSplit) {   // z.w ~ hi.hi + hi.lo + lo.hi, one FP32 accumulator
-                                umma_f16(d_tmem, ad, desc_sw128(sa + Cfg::kBlo, k * 32), a.idesc, 1u);
-                                umma_f16(d_tmem, desc_sw128(sa + Cfg::kAlo, k * 32), bd, a.idesc, 1u);
+                                umma_f16(d_tmem, ad, desc_kmajor(sa + Cfg::kBlo, k * 32, dh), a.idesc, 1u);
+                                umma_f16(d_tmem, desc_kmajor(sa + Cfg::kAlo, k * 32, dh), bd, a.idesc, 1u);
                             }
                         }
                         umma_commit(&ctl->empty[stage]);
@@ -300,7 +309,9 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
     } else {
         // ------------------------------------------------------------ epilogue
         const unsigned q = warp & 3;                 // TMEM lane quarter of this warp
+        const unsigned half = (warp - 2) >> 2;       // accumulator column half of this warp
         const unsigned row = q * 32 + lane;          // R row within the tile
+        constexpr int kCbPerWarp = kTileS / 32 / 2;
         WarpAppender app_acc, app_band;
         unsigned acc = 0, acc_phase = 0;
         unsigned long long n = 0, n_screen_acc = 0, n_rare = 0, n_items = 0;
@@ -342,7 +353,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 }
                 const unsigned tbase = tmem + ((q * 32u) << 16) + acc * kTileS;
 #pragma unroll 1
-                for (int cb = 0; cb < kTileS / 32; ++cb) {
+                for (int cb = half * kCbPerWarp; cb < (int)(half + 1) * kCbPerWarp; ++cb) {
                     const int col0 = cb * 32;
                     uint32_t raw[32];
                     tmem_ld32(tbase + col0, raw);
@@ -354,20 +365,35 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         for (int k = 0; k < 32; ++k) out[k] = __uint_as_float(raw[k]);
                         if (row == 0 && cb == 0) a.dump_ids[slotd] = make_uint4(ch.x, a.jlist[e], 1u, 0u);
                     }
-                    if (cb == kTileS / 32 - 1) {   // accumulator fully read: hand it back to the MMA
+                    if (cb == (int)(half + 1) * kCbPerWarp - 1) {   // this warp's part read: hand it back
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&ctl->acc_empty[acc]);
                     }
-                    // fast path: one FMA and one compare per pair, candidates collected in a bit mask
-                    uint32_t cmask = 0;
+                    // fast path: one FMA and one min per pair (four independent min chains); only a
+                    // 32-column group whose minimum passes the threshold builds the candidate mask
+                    const float4* nb4 = reinterpret_cast<const float4*>(&m.nrm2f[col0]);
+                    float vm[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
 #pragma unroll
-                    for (int k = 0; k < 32; ++k)
-                        cmask |= (fmaf(-2.f, __uint_as_float(raw[k]), m.nrm2f[col0 + k]) <= tau ? 1u : 0u) << k;
-                    if (jp.self_join && cmask) {   // keep sorted column > sorted row only
-                        const int lim = (int)rs - (int)(c0 + col0);   // columns k <= lim are not above the diagonal
-                        if (lim >= 31) cmask = 0;
-                        else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
+                    for (int k4 = 0; k4 < 8; ++k4) {
+                        const float4 b = nb4[k4];
+                        vm[0] = fminf(vm[0], fmaf(-2.f, __uint_as_float(raw[4 * k4 + 0]), b.x));
+                        vm[1] = fminf(vm[1], fmaf(-2.f, __uint_as_float(raw[4 * k4 + 1]), b.y));
+                        vm[2] = fminf(vm[2], fmaf(-2.f, __uint_as_float(raw[4 * k4 + 2]), b.z));
+                        vm[3] = fminf(vm[3], fmaf(-2.f, __uint_as_float(raw[4 * k4 + 3]), b.w));
+                    }
+                    const bool hit = fminf(fminf(vm[0], vm[1]), fminf(vm[2], vm[3])) <= tau;
+                    if (!__any_sync(0xffffffffu, hit)) continue;
+                    uint32_t cmask = 0;
+                    if (hit) {
+#pragma unroll
+                        for (int k = 0; k < 32; ++k)
+                            cmask |= (fmaf(-2.f, __uint_as_float(raw[k]), m.nrm2f[col0 + k]) <= tau ? 1u : 0u) << k;
+                        if (jp.self_join) {   // keep sorted column > sorted row only
+                            const int lim = (int)rs - (int)(c0 + col0);   // columns k <= lim: not above the diagonal
+                            if (lim >= 31) cmask = 0;
+                            else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
+                        }
                     }
                     if (!__any_sync(0xffffffffu, cmask != 0)) continue;
                     // ---------------- rare path: certified FP32 accept, else per-pair FP64 certificate
@@ -439,7 +465,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             if (app_band.valid) atomicAdd(&a.ctr->band_valid, app_band.valid);
             if (n_screen_acc) atomicAdd(&a.ctr->screen_accept, n_screen_acc);
             if (n_rare) atomicAdd(&a.ctr->rare_checks, n_rare);
-            if (q == 0 && n_items) atomicAdd(&a.ctr->items, n_items);
+            if (warp == 2 && n_items) atomicAdd(&a.ctr->items, n_items);
         }
     }
     tc_fence_before();
@@ -521,14 +547,19 @@ EncodeTiledFn encode_fn() {
 
 // 2-D tensor map over a row-major [rows, cols] matrix of `esize`-byte elements, box = 128 bytes x box_rows,
 // 128-byte swizzle (the UMMA K-major canonical layout).
+// 2-D tensor map over a row-major [rows, cols] matrix with boxes of box_rows x (box_bytes / esize)
+// elements, swizzled by the box row width (32, 64 or 128 bytes).
 void make_tmap_2d(CUtensorMap* m, const void* base, long long rows, long long cols, int esize, int box_rows,
-                  CUtensorMapDataType dt) {
+                  CUtensorMapDataType dt, int box_bytes) {
+    if (box_bytes != 32 && box_bytes != 64 && box_bytes != 128) fail(-1, "make_tmap_2d: box width");
     const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)cols * esize};
-    const cuuint32_t box[2] = {(cuuint32_t)(128 / esize), (cuuint32_t)box_rows};
+    const cuuint32_t box[2] = {(cuuint32_t)(box_bytes / esize), (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
+    const CUtensorMapSwizzle sw = box_bytes == 32 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                  : box_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
     const CUresult r = encode_fn()(m, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
-                                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) fail(-2, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
 }
@@ -551,8 +582,10 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
         if (!ok) fail(-1, "screen_tc needs matching bf16 / fp16 operands on both sides of every class");
         const CUtensorMapDataType dt = bf ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
         const long long w = (long long)R.kpad * (split ? 2 : 1);
-        make_tmap_2d(&tm.a[c], R.op.p, R.rows_pad, w, 2, kTileR, dt);
-        make_tmap_2d(&tm.b[c], S.op.p, S.rows_pad, w, 2, kTileS, dt);
+        const int kbk = std::min(R.kpad, kBK);
+        if (kbk != 16 && kbk != 32 && kbk != 64) fail(-1, "screen_tc: operand width");
+        make_tmap_2d(&tm.a[c], R.op.p, R.rows_pad, w, 2, kTileR, dt, 2 * kbk);
+        make_tmap_2d(&tm.b[c], S.op.p, S.rows_pad, w, 2, kTileS, dt, 2 * kbk);
         const TileSet& tS = *g.tS[c];
         if (tS.ntiles > 0)
             launch(build_col_meta, tS.ntiles, kTileS, 0, st, tS.row0.p, tS.nvalid.p, S.emit, S.nrm2.p, S.nrm2f.p,
@@ -563,8 +596,11 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
         a.cls[c].r_zn = R.zn.p;
         a.cls[c].r_en = R.en.p;
         a.cls[c].r_zl = R.zl.p;
-        a.cls[c].kblocks = R.kpad / kBK;
+        a.cls[c].kblocks = R.kpad / kbk;
         a.cls[c].kpad = R.kpad;
+        a.cls[c].kbk = kbk;
+        a.cls[c].tx_bytes = (unsigned)((split ? 2 : 1) * (kTileR + kTileS) * kbk * 2);
+        a.cls[c].desc_hi = desc_hi_for_rows(2u * (unsigned)kbk);
     }
     a.chunks = g.cand->chunks.p;
     a.nchunks = g.cand->dev_counts.p + 1;

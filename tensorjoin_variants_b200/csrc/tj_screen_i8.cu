@@ -23,6 +23,8 @@
 // (warp w reads TMEM lanes 32*(w%4).. and columns 64*((w-2)/4)..).
 #include <algorithm>
 
+#include <climits>
+
 #include "tj_emit.cuh"
 #include "tj_internal.h"
 
@@ -267,13 +269,29 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                     uint32_t hv[32];
                     tmem_ld32(tmem + lane_off + kColHH0 + b * 128 + cc, hv);
                     tmem_ld_wait();
-                    uint32_t cmask = 0;
+                    // fast path: one subtract and one max per pair (four independent chains); only a
+                    // 32-column group whose maximum reaches the threshold builds the candidate mask
+                    const int4* bq4 = reinterpret_cast<const int4*>(&m.bq[cc]);
+                    int vx[4] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN};
 #pragma unroll
-                    for (int k = 0; k < 32; ++k) cmask |= ((int)hv[k] - m.bq[cc + k] >= ai ? 1u : 0u) << k;
-                    if (jp.self_join && cmask) {   // keep sorted column > sorted row only
-                        const int lim = (int)rs - (int)(c0 + cc);
-                        if (lim >= 31) cmask = 0;
-                        else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
+                    for (int k4 = 0; k4 < 8; ++k4) {
+                        const int4 bb = bq4[k4];
+                        vx[0] = max(vx[0], (int)hv[4 * k4 + 0] - bb.x);
+                        vx[1] = max(vx[1], (int)hv[4 * k4 + 1] - bb.y);
+                        vx[2] = max(vx[2], (int)hv[4 * k4 + 2] - bb.z);
+                        vx[3] = max(vx[3], (int)hv[4 * k4 + 3] - bb.w);
+                    }
+                    const bool hit = max(max(vx[0], vx[1]), max(vx[2], vx[3])) >= ai;
+                    if (!__any_sync(0xffffffffu, hit)) continue;
+                    uint32_t cmask = 0;
+                    if (hit) {
+#pragma unroll
+                        for (int k = 0; k < 32; ++k) cmask |= ((int)hv[k] - m.bq[cc + k] >= ai ? 1u : 0u) << k;
+                        if (jp.self_join) {   // keep sorted column > sorted row only
+                            const int lim = (int)rs - (int)(c0 + cc);
+                            if (lim >= 31) cmask = 0;
+                            else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
+                        }
                     }
                     if (!__any_sync(0xffffffffu, cmask != 0)) continue;
                     uint32_t xv[32], lv[32];
@@ -338,7 +356,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
 }  // namespace
 
 void make_tmap_2d(CUtensorMap* m, const void* base, long long rows, long long cols, int esize, int box_rows,
-                  CUtensorMapDataType dt);
+                  CUtensorMapDataType dt, int box_bytes);
 
 void screen_i8(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     if (g.ncls != 1 || g.njoins != 1) fail(-7, "the int8-limb screen runs one join at a time");
@@ -346,8 +364,8 @@ void screen_i8(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     const Side& S = *g.S[0];
     if (R.screen != kScreenInt8Limb || S.screen != kScreenInt8Limb) fail(-1, "screen_i8 needs int8-limb sides");
     CUtensorMap tmA, tmB;
-    make_tmap_2d(&tmA, R.op8.p, R.rows_pad, 2 * (long long)R.kpad, 1, 128, CU_TENSOR_MAP_DATA_TYPE_UINT8);
-    make_tmap_2d(&tmB, S.op8.p, S.rows_pad, 2 * (long long)S.kpad, 1, kI8N, CU_TENSOR_MAP_DATA_TYPE_UINT8);
+    make_tmap_2d(&tmA, R.op8.p, R.rows_pad, 2 * (long long)R.kpad, 1, 128, CU_TENSOR_MAP_DATA_TYPE_UINT8, 128);
+    make_tmap_2d(&tmB, S.op8.p, S.rows_pad, 2 * (long long)S.kpad, 1, kI8N, CU_TENSOR_MAP_DATA_TYPE_UINT8, 128);
     I8Args a;
     a.chunks = g.cand->chunks.p;
     a.nchunks = g.cand->dev_counts.p + 1;

@@ -6,7 +6,8 @@
 //   1. per-block digit histogram (digit-major [256][blocks]),
 //   2. device-wide exclusive scan of that table,
 //   3. stable scatter: every warp ranks its keys round by round with
-//      __match_any_sync, warps are combined in order through shared counters.
+//      __match_any_sync, warps are combined in order through shared counters,
+//      the tile is regrouped by digit in shared memory and written out in runs.
 // Stability across passes makes the whole sort correct for any bit width.
 //
 // It replaces the CUB SortKeys call of the reference's output stage
@@ -118,19 +119,42 @@ __global__ void __launch_bounds__(kRsThreads) rs_hist(const uint64_t* keys, size
     hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
+// Block-wide exclusive scan of one value per thread (kRsThreads == 256 values).
+TJ_DEV uint32_t block_excl_scan_256(uint32_t v, uint32_t* warp_tot) {
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned tot;
+    const unsigned pre = warp_excl_scan(v, tot);
+    if (lane == 0) warp_tot[warp] = tot;
+    __syncthreads();
+    uint32_t off = 0;
+#pragma unroll
+    for (int w = 0; w < kRsWarps; ++w) off += (w < (int)warp) ? warp_tot[w] : 0u;
+    return off + pre;
+}
+
+// Stable scatter of one 4096-key tile.  Keys are ranked per warp (round by round with
+// __match_any_sync), the block's keys are regrouped by digit in shared memory, and then written
+// out in that order, so consecutive threads store consecutive addresses of one digit's run
+// (about 16 keys = 128 B per digit and tile for 8-bit digits) instead of scattered 8-byte words.
 template <bool kVals>
 __global__ void __launch_bounds__(kRsThreads) rs_scatter(const uint64_t* keys_in, const uint32_t* vals_in,
                                                         uint64_t* keys_out, uint32_t* vals_out, size_t n, int shift,
                                                         const uint32_t* offs, unsigned nblocks) {
+    extern __shared__ __align__(16) unsigned char rs_dyn[];
+    uint64_t* sk = (uint64_t*)rs_dyn;                      // [kRsTile] keys grouped by digit
+    uint32_t* sv = (uint32_t*)(rs_dyn + kRsTile * 8);      // [kRsTile] values (kVals)
     __shared__ uint32_t wcnt[kRsWarps][256];
-    __shared__ uint32_t gbase[256];
+    __shared__ uint32_t gbase[256];    // global start of each digit's run for this tile
+    __shared__ uint32_t lstart[256];   // tile-local start of each digit's run
+    __shared__ uint32_t wtot[kRsWarps];
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kRsWarps * 256; i += kRsThreads) (&wcnt[0][0])[i] = 0;
     gbase[threadIdx.x] = offs[(size_t)threadIdx.x * nblocks + blockIdx.x];
     __syncthreads();
 
     // warp w owns the contiguous run [w*512, (w+1)*512) of this block's tile; round r, lane l -> r*32 + l
-    const size_t wbase = (size_t)blockIdx.x * kRsTile + (size_t)warp * (kRsRounds * 32);
+    const size_t tbase = (size_t)blockIdx.x * kRsTile;
+    const size_t wbase = tbase + (size_t)warp * (kRsRounds * 32);
     uint64_t k[kRsRounds];
     uint32_t v[kRsRounds];
     uint32_t rank[kRsRounds];
@@ -154,7 +178,7 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter(const uint64_t* keys_in
         __syncwarp();
     }
     __syncthreads();
-    {   // exclusive prefix over warps for each digit
+    {   // exclusive prefix over warps for each digit, then over digits for the tile
         const unsigned dg = threadIdx.x;
         uint32_t run = 0;
 #pragma unroll
@@ -163,16 +187,26 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter(const uint64_t* keys_in
             wcnt[w][dg] = run;
             run += t;
         }
+        lstart[dg] = block_excl_scan_256(run, wtot);
     }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kRsRounds; ++r) {
         if (rank[r] != 0xFFFFFFFFu) {
             const unsigned dg = digit_of(k[r], shift);
-            const size_t pos = (size_t)gbase[dg] + wcnt[warp][dg] + rank[r];
-            keys_out[pos] = k[r];
-            if (kVals) vals_out[pos] = v[r];
+            const unsigned p = lstart[dg] + wcnt[warp][dg] + rank[r];
+            sk[p] = k[r];
+            if (kVals) sv[p] = v[r];
         }
+    }
+    __syncthreads();
+    const unsigned cnt = (unsigned)min((size_t)kRsTile, n - tbase);
+    for (unsigned p = threadIdx.x; p < cnt; p += kRsThreads) {
+        const uint64_t key = sk[p];
+        const unsigned dg = digit_of(key, shift);
+        const size_t pos = (size_t)gbase[dg] + (p - lstart[dg]);
+        keys_out[pos] = key;
+        if (kVals) vals_out[pos] = sv[p];
     }
 }
 
@@ -189,6 +223,10 @@ size_t radix_workspace_elems(size_t n) {
 void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp, size_t n, int bits,
                 uint32_t* ws, cudaStream_t st) {
     if (n <= 1 || bits <= 0) return;
+    if (n >= (1ull << 32)) fail(-1, "radix_sort: more than 2^32 - 1 keys");
+    const size_t dyn_k = (size_t)kRsTile * 8, dyn_kv = (size_t)kRsTile * 12;
+    TJ_CUDA(cudaFuncSetAttribute(rs_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_k));
+    if (vals) TJ_CUDA(cudaFuncSetAttribute(rs_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_kv));
     const unsigned nb = (unsigned)((n + kRsTile - 1) / kRsTile);
     const size_t h = 256 * (size_t)nb;
     uint32_t* hist = ws;
@@ -202,9 +240,9 @@ void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* va
         launch(rs_hist, nb, kRsThreads, 0, st, kin, n, shift, hist, nb);
         exclusive_scan_u32(hist, offs, h, nullptr, sws, st);
         if (vals)
-            launch(rs_scatter<true>, nb, kRsThreads, 0, st, kin, vin, kout, vout, n, shift, offs, nb);
+            launch(rs_scatter<true>, nb, kRsThreads, dyn_kv, st, kin, vin, kout, vout, n, shift, offs, nb);
         else
-            launch(rs_scatter<false>, nb, kRsThreads, 0, st, kin, nullptr, kout, nullptr, n, shift, offs, nb);
+            launch(rs_scatter<false>, nb, kRsThreads, dyn_k, st, kin, nullptr, kout, nullptr, n, shift, offs, nb);
         std::swap(kin, kout);
         std::swap(vin, vout);
     }

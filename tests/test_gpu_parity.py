@@ -3,6 +3,7 @@
 The tolerance is zero: the pair set is discrete and the FP64 refinement uses the
 oracle's summation order.  Pairs are compared as canonical uint64 keys.
 """
+import ctypes as C
 import hashlib
 import json
 from pathlib import Path
@@ -88,7 +89,7 @@ def test_factor512_small(screen):
 
 
 @pytest.mark.parametrize("screen", FLOAT_SCREENS)
-@pytest.mark.parametrize("d", [1, 3, 63, 65, 130])
+@pytest.mark.parametrize("d", [1, 3, 8, 16, 17, 31, 32, 33, 63, 65, 130])
 def test_ragged_dimensions(screen, d):
     rng = np.random.default_rng(100 + d)
     R = rng.standard_normal((700, d)).astype(np.float32)
@@ -311,7 +312,8 @@ def test_screen_error_within_certified_radius(screen):
     """Sampled tensor-core accumulators: the distance estimate's error against sequential FP64 stays
     inside the certified radius (the accumulation premise holds on these inputs), and the result is
     unchanged by the diagnostic pass."""
-    for w in (W.factor512(n=4000, samples=1 << 15), W.mixture64(n=8000, samples=1 << 15)):
+    for w in (W.factor512(n=4000, samples=1 << 15), W.mixture64(n=8000, samples=1 << 15),
+              W.mixture64(n=8000, d=32, samples=1 << 15), W.mixture64(n=8000, d=8, samples=1 << 15)):
         R, S = torch.from_numpy(w.R).cuda(), torch.from_numpy(w.S).cuda()
         res = tj.join_result(R, S, eps2=w.T, screen=screen, screen_diag=True)
         st = res.stats
@@ -332,3 +334,44 @@ def test_threshold_ties_float():
         for screen in ("bf16", "fp16x3", "plain"):
             k, _ = gpu_keys(R, S, float(T), "rs", screen)
             assert_same(k, oracle_keys(R, S, float(T), "rs"), f"tie {screen}")
+
+
+@pytest.mark.parametrize("screen", ["bf16x3", "plain"])
+def test_batched_views_of_one_array(screen):
+    """Joins given as back-to-back views of one device array per side (used in place, no gather)
+    give the same pairs as the same joins in separate arrays; a partly adjacent batch is gathered."""
+    joins = _ragged(16, 43, dims=(8, 32))
+    by_d = {}
+    for R, S, T in joins:
+        by_d.setdefault(R.shape[1], []).append((R, S, T))
+    views, separate = [], []
+    for d, js in by_d.items():
+        Rall = torch.from_numpy(np.concatenate([R for R, _, _ in js])).cuda()
+        Sall = torch.from_numpy(np.concatenate([S for _, S, _ in js])).cuda()
+        r0 = s0 = 0
+        for R, S, T in js:
+            views.append((Rall[r0:r0 + len(R)], Sall[s0:s0 + len(S)], float(np.sqrt(T))))
+            separate.append((torch.from_numpy(R).cuda(), torch.from_numpy(S).cuda(), float(np.sqrt(T))))
+            r0 += len(R)
+            s0 += len(S)
+    a = tj.join_batched(views, screen=screen)
+    b = tj.join_batched(separate, screen=screen)
+    mixed = [views[0], separate[1]] + views[2:]
+    c = tj.join_batched(mixed, screen=screen)
+    for (i, j), (i2, j2), (i3, j3) in zip(a, b, c):
+        assert torch.equal(i, i2) and torch.equal(j, j2)
+        assert torch.equal(i, i3) and torch.equal(j, j3)
+
+
+def test_pool_usage_and_reserve():
+    """The memory-pool entry points report sizes and grow the pool on request."""
+    L = _lib.lib()
+    r0, u0, h0 = C.c_int64(), C.c_int64(), C.c_int64()
+    assert L.tj_pool_usage(C.byref(r0), C.byref(u0), C.byref(h0)) == 0
+    want = r0.value + (256 << 20)
+    assert L.tj_pool_reserve(want, C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+    r1 = C.c_int64()
+    assert L.tj_pool_usage(C.byref(r1), None, None) == 0
+    assert r1.value >= want
+    assert L.tj_pool_trim(0) == 0
+    assert L.tj_pool_reserve(-1, None) != 0
