@@ -160,15 +160,17 @@ int tj_device_sm_count(void);
 /* Running total of kernels this library has launched in the process (audit of timed regions). */
 int64_t tj_kernel_launches(void);
 
-/* The current device's memory pool, from which every join's temporaries and results are drawn
- * (stream-ordered; memory freed by one join is reused by the next).  No counterpart in the
- * reference, whose scripts allocated through torch.
- * tj_pool_usage: bytes the pool holds from the driver, bytes in live allocations, and the peak of
- * the former (any pointer may be NULL).
+/* Device memory held by the library on the current device.  No counterpart in the reference,
+ * whose scripts allocated through torch.  A join takes its temporaries from a workspace owned by the
+ * calling host thread (one block per thread and device, grown to 1.25x the largest join seen), its
+ * result arrays from a cache of up to four buffers released by freed results, and everything else
+ * from a stream-ordered pool; a steady stream of similar joins therefore maps no new memory.
+ * tj_pool_usage: bytes held (pool reservation + this thread's workspace), bytes of the pool in live
+ * allocations (results alive or cached), and the pool's peak reservation (any pointer may be NULL).
  * tj_pool_reserve: makes the pool hold at least `bytes` (one allocation and free on `stream`, then a
- * synchronisation of `stream`), so that later joins need not map new device memory.
- * tj_pool_trim: returns held memory above `keep_bytes` to the driver (memory of frees still pending
- * on a stream is kept until they complete). */
+ * synchronisation of `stream`).
+ * tj_pool_trim: frees the cached result buffers and this thread's workspace, waits for the device,
+ * and returns pool memory above `keep_bytes` to the driver. */
 int tj_pool_usage(int64_t* reserved, int64_t* used, int64_t* reserved_high);
 int tj_pool_reserve(int64_t bytes, void* stream);
 int tj_pool_trim(int64_t keep_bytes);

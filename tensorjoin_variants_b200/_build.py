@@ -13,7 +13,7 @@ CSRC = PKG / "csrc"
 INCLUDE = PKG.parent / "include"
 OBJ = PKG / "_build"
 LIB = PKG / "libtensorjoin.so"
-SOURCES = ["tj_sort.cu", "tj_index.cu", "tj_screen.cu", "tj_screen_i8.cu", "tj_refine.cu", "tj_noalloc.cu", "tj_api.cu"]
+SOURCES = ["tj_memory.cu", "tj_sort.cu", "tj_index.cu", "tj_screen.cu", "tj_screen_i8.cu", "tj_refine.cu", "tj_noalloc.cu", "tj_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "-diag-suppress", "177", f"-I{INCLUDE}"]

@@ -33,65 +33,9 @@ void check_cuda(cudaError_t e, const char* what) {
     fail(code, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-// ------------------------------------------------------------------ memory pool
 namespace {
-std::mutex g_pool_mu;
-cudaMemPool_t g_pools[64] = {};
 int g_sms[64] = {};
-
-cudaMemPool_t pool_for_current() {
-    int dev = 0;
-    TJ_CUDA(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(g_pool_mu);
-    if (!g_pools[dev]) {
-        cudaMemPoolProps props;
-        memset(&props, 0, sizeof(props));
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = dev;
-        TJ_CUDA(cudaMemPoolCreate(&g_pools[dev], &props));
-        uint64_t thr = ~0ull;
-        TJ_CUDA(cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &thr));
-    }
-    return g_pools[dev];
-}
 }  // namespace
-
-// TJ_TRACE_ALLOC=<ms> in the environment logs, to stderr, every pool allocation whose host call
-// took longer than <ms> milliseconds, with the pool's reserved / used bytes afterwards.
-static double trace_alloc_ms() {
-    static const double v = [] {
-        const char* e = getenv("TJ_TRACE_ALLOC");
-        return e ? atof(e) : -1.0;
-    }();
-    return v;
-}
-
-void* dalloc(size_t bytes, cudaStream_t st) {
-    void* p = nullptr;
-    const double lim = trace_alloc_ms();
-    const auto t0 = std::chrono::steady_clock::now();
-    const cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool_for_current(), st);
-    if (lim >= 0.0) {
-        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-        if (ms > lim) {
-            uint64_t res = 0, used = 0;
-            cudaMemPoolGetAttribute(pool_for_current(), cudaMemPoolAttrReservedMemCurrent, &res);
-            cudaMemPoolGetAttribute(pool_for_current(), cudaMemPoolAttrUsedMemCurrent, &used);
-            fprintf(stderr, "[tj alloc] %zu bytes took %.2f ms (pool reserved %llu MiB, used %llu MiB)\n", bytes, ms,
-                    (unsigned long long)(res >> 20), (unsigned long long)(used >> 20));
-        }
-    }
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        fail(TJ_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
-    }
-    return p;
-}
-
-void dfree(void* p, cudaStream_t st) {
-    if (p) cudaFreeAsync(p, st);
-}
 
 namespace {
 std::atomic<long long> g_launches{0};
@@ -323,8 +267,8 @@ struct JoinIn {
 // One or many joins.  Joins are grouped into classes of equal d; each class gets one
 // concatenated, Morton-sorted side per operand (joins stay contiguous), global tile tables, one
 // block-diagonal candidate list and one persistent screen launch over all classes.
-void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen, const tj_options* opt,
-               tj_result* res, cudaStream_t st) {
+void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int screen, const tj_options* opt,
+                    tj_result* res, cudaStream_t st) {
     const bool self = mode != TJ_MODE_RS;
     const int nj = (int)joins.size();
     if (nj < 1) fail(TJ_ERR_INVALID, "no joins");
@@ -511,8 +455,13 @@ void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen
     g.T_int = (long long)joins[0].eps2;
     DBuf<uint4> d_rt((size_t)g.ntR_total, st), d_st((size_t)g.ntS_total, st);
     DBuf<JoinParams> d_jps((size_t)nj, st);
-    DBuf<unsigned long long> d_koff((size_t)nj, st);
-    DBuf<long long> d_cols((size_t)nj, st);
+    DBuf<unsigned long long> d_koff;
+    DBuf<long long> d_cols;
+    {
+        WorkspaceSuspend keep;   // key decoding tables stay with the result
+        d_koff = DBuf<unsigned long long>((size_t)nj, st);
+        d_cols = DBuf<long long>((size_t)nj, st);
+    }
     DBuf<const void*> d_rsrc((size_t)nj, st), d_ssrc((size_t)nj, st);
     std::vector<const void*> hr(nj), hs(nj);
     for (int k = 0; k < nj; ++k) { hr[k] = joins[k].R; hs[k] = self ? joins[k].R : joins[k].S; }
@@ -614,7 +563,7 @@ void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen
     DBuf<uint64_t> acc, band;
     Counters h;
     for (int attempt = 0;; ++attempt) {
-        acc = DBuf<uint64_t>(cap, st);
+        acc = DBuf<uint64_t>::result(cap, st);   // becomes the result's key array
         band = DBuf<uint64_t>(bcap, st);
         launch(zero_counters, 1, 32, 0, st, ctr.p, 1);
         EmitBuffers eb{acc.p, cap, band.p, bcap, ctr.p};
@@ -659,7 +608,7 @@ void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen
     if (mode == TJ_MODE_DIRECTED) {
         const long long N = joins[0].nR;
         const unsigned long long nk = 2 * slots + (unsigned long long)N;
-        keys = DBuf<uint64_t>(nk, st);
+        keys = DBuf<uint64_t>::result(nk, st);
         expand_directed(acc.p, slots, keys.p, N, st);
         acc.reset();
         slots = nk;
@@ -692,6 +641,13 @@ void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen
     S_.ms_refine = ev.ms(3, 4);
     S_.ms_sort = ev.ms(4, 5);
     S_.ms_total = ev.ms(0, 5);
+}
+
+// One join (or batch) with its temporaries in the calling thread's workspace.
+void run_batch(const std::vector<JoinIn>& joins, int dtype, int mode, int screen, const tj_options* opt,
+               tj_result* res, cudaStream_t st) {
+    WorkspaceScope ws(st);
+    run_batch_body(joins, dtype, mode, screen, opt, res, st);
 }
 
 }  // namespace
@@ -909,7 +865,10 @@ int tj_pool_usage(int64_t* reserved, int64_t* used, int64_t* reserved_high) {
     TJ_API_BEGIN
     cudaMemPool_t pool = pool_for_current();
     uint64_t v = 0;
-    if (reserved) { TJ_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v)); *reserved = (int64_t)v; }
+    if (reserved) {
+        TJ_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v));
+        *reserved = (int64_t)(v + workspace_bytes());
+    }
     if (used) { TJ_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &v)); *used = (int64_t)v; }
     if (reserved_high) {
         TJ_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemHigh, &v));
@@ -938,6 +897,8 @@ int tj_pool_reserve(int64_t bytes, void* stream) {
 int tj_pool_trim(int64_t keep_bytes) {
     TJ_API_BEGIN
     if (keep_bytes < 0) fail(TJ_ERR_INVALID, "keep_bytes must be >= 0");
+    release_cached(nullptr);
+    TJ_CUDA(cudaDeviceSynchronize());   // frees pending on any stream complete before the trim
     TJ_CUDA(cudaMemPoolTrimTo(pool_for_current(), (size_t)keep_bytes));
     return TJ_OK;
     TJ_API_END

@@ -21,26 +21,75 @@ void set_last_error(const std::string& msg);
 void check_cuda(cudaError_t e, const char* what);
 #define TJ_CUDA(x) ::tj::check_cuda((x), #x)
 
-// ------------------------------------------------------------------ stream-ordered device memory
+// ------------------------------------------------------------------ device memory (tj_memory.cu)
+// dalloc/dfree: while a WorkspaceScope is open on this thread and device, blocks come from the
+// join workspace (a stack reclaimed in free order; overflow goes to the pool); otherwise from the
+// stream-ordered pool.  Result buffers, which outlive the join, use result_alloc/result_release
+// (a small cache of released result buffers in front of the pool).
+cudaMemPool_t pool_for_current();
 void* dalloc(size_t bytes, cudaStream_t st);
 void dfree(void* p, cudaStream_t st);
+void* result_alloc(size_t bytes, cudaStream_t st, size_t* cap_out);
+void result_release(void* p, size_t cap, cudaStream_t st);
+void release_cached(cudaStream_t st);   // drop cached result buffers and this thread's workspace
+size_t workspace_bytes();               // this thread's workspace on the current device
+
+// Opens the join workspace for the lifetime of the object (one join, all work on stream `st`).
+// Closing it re-makes the workspace if the join needed more than it held.
+struct WorkspaceScope {
+    cudaStream_t st;
+    int dev;
+    explicit WorkspaceScope(cudaStream_t s);
+    ~WorkspaceScope();
+    WorkspaceScope(const WorkspaceScope&) = delete;
+    WorkspaceScope& operator=(const WorkspaceScope&) = delete;
+};
+// Allocations made while this object lives bypass the workspace (buffers that leave the join).
+struct WorkspaceSuspend {
+    int dev;
+    WorkspaceSuspend();
+    ~WorkspaceSuspend();
+    WorkspaceSuspend(const WorkspaceSuspend&) = delete;
+    WorkspaceSuspend& operator=(const WorkspaceSuspend&) = delete;
+};
 
 template <class T>
 struct DBuf {
     T* p = nullptr;
     size_t n = 0;
     cudaStream_t st = nullptr;
+    size_t rcap = 0;   // > 0: a result buffer of rcap bytes (goes back to the result cache)
     DBuf() = default;
     DBuf(size_t n_, cudaStream_t s) : n(n_), st(s) { p = n ? (T*)dalloc(n * sizeof(T), s) : nullptr; }
+    // a buffer that may leave the join as part of a result
+    static DBuf result(size_t n_, cudaStream_t s) {
+        DBuf b;
+        b.n = n_;
+        b.st = s;
+        b.p = (T*)result_alloc(n_ * sizeof(T), s, &b.rcap);
+        return b;
+    }
     DBuf(const DBuf&) = delete;
     DBuf& operator=(const DBuf&) = delete;
-    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), st(o.st) { o.p = nullptr; o.n = 0; }
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), st(o.st), rcap(o.rcap) { o.p = nullptr; o.n = 0; o.rcap = 0; }
     DBuf& operator=(DBuf&& o) noexcept {
-        if (this != &o) { reset(); p = o.p; n = o.n; st = o.st; o.p = nullptr; o.n = 0; }
+        if (this != &o) {
+            reset();
+            p = o.p; n = o.n; st = o.st; rcap = o.rcap;
+            o.p = nullptr; o.n = 0; o.rcap = 0;
+        }
         return *this;
     }
     ~DBuf() { reset(); }
-    void reset() { if (p) dfree(p, st); p = nullptr; n = 0; }
+    void reset() {
+        if (p) {
+            if (rcap) result_release(p, rcap, st);
+            else dfree(p, st);
+        }
+        p = nullptr;
+        n = 0;
+        rcap = 0;
+    }
     size_t bytes() const { return n * sizeof(T); }
 };
 

@@ -375,3 +375,49 @@ def test_pool_usage_and_reserve():
     assert r1.value >= want
     assert L.tj_pool_trim(0) == 0
     assert L.tj_pool_reserve(-1, None) != 0
+
+
+def test_results_alive_across_joins_and_sizes():
+    """Results held while later joins of other sizes run (workspace growth, result-buffer reuse)
+    keep their pairs; a freed result's buffer handed to a later join does not disturb it."""
+    ws = [W.mixture64(n=n, d=d, samples=1 << 14) for n, d in ((3000, 16), (12000, 64), (1500, 32))]
+    ws.append(ws[1])
+    want = [oracle_keys(w.R, w.S, w.T, "rs") for w in ws[:3]]
+    want.append(want[1])
+    held = []
+    for k, w in enumerate(ws):
+        res = tj.join_result(torch.from_numpy(w.R).cuda(), torch.from_numpy(w.S).cuda(), eps2=w.T, screen="bf16x3")
+        held.append(res)
+        if k == 1:
+            held[0] = None   # release the first result while others stay alive
+    for k in (1, 2, 3):
+        assert_same(held[k].keys().cpu().numpy().view(np.uint64), want[k], f"held {k}")
+
+
+def test_concurrent_host_threads():
+    """Two host threads joining at once on their own streams (one workspace per thread)."""
+    import threading
+    ws = [W.mixture64(n=6000, d=32, seed=s, samples=1 << 14) for s in (11, 12)]
+    want = [oracle_keys(w.R, w.S, w.T, "rs") for w in ws]
+    out = [None, None]
+    errs = []
+
+    def run(k):
+        try:
+            s = torch.cuda.Stream()
+            with torch.cuda.stream(s):
+                R, S = torch.from_numpy(ws[k].R).cuda(), torch.from_numpy(ws[k].S).cuda()
+                for _ in range(3):
+                    res = tj.join_result(R, S, eps2=ws[k].T, screen="bf16x3")
+                    out[k] = res.keys().cpu().numpy().view(np.uint64)
+        except Exception as e:   # surfaced below
+            errs.append(e)
+
+    th = [threading.Thread(target=run, args=(k,)) for k in (0, 1)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs, errs
+    for k in (0, 1):
+        assert_same(out[k], want[k], f"thread {k}")
