@@ -24,7 +24,7 @@ namespace tj {
 
 namespace {
 
-constexpr int kStatBlocks = 512;
+constexpr int kStatBlocks = 1184;   // 8 blocks of 256 threads per SM on 148 SMs
 
 TJ_DEV float load_x(const void* src, int dtype, size_t idx) {
     return dtype == kF32 ? ((const float*)src)[idx] : (float)((const int16_t*)src)[idx];
@@ -47,7 +47,20 @@ __global__ void __launch_bounds__(256) dim_stats_partial(const void* src, int dt
         float mn = INFINITY, mx = -INFINITY;
         double s = 0.0, q = 0.0;
         if (g < G && k < d) {
-            for (long long r = r0 + g; r < r1; r += G) {
+            long long r = r0 + g;
+            for (; r + 3 * G < r1; r += 4 * G) {   // four independent loads in flight per thread
+                float v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) v[u] = load_x(src, dtype, (size_t)(r + u * G) * d + k);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    mn = fminf(mn, v[u]);
+                    mx = fmaxf(mx, v[u]);
+                    s += v[u];
+                    q += (double)v[u] * v[u];
+                }
+            }
+            for (; r < r1; r += G) {
                 const float v = load_x(src, dtype, (size_t)r * d + k);
                 mn = fminf(mn, v);
                 mx = fmaxf(mx, v);
@@ -203,37 +216,38 @@ TJ_DEV float round16(float v, uint16_t& bits) {
     return __half2float(h);
 }
 
-// One warp per sorted row: operand conversion and certificate metadata.
+// One group of kL lanes per sorted row (a warp for wide rows, 4 or 8 lanes for rows of at most
+// 16 or 32 elements): operand conversion and certificate metadata.
 //   plain:      FP32 copy in sorted order, ||x||^2.
 //   16-bit:     x' = x - c (c the per-dimension centre; distances are translation invariant),
 //               z_hi = round16(x'), and with kSplit also z_lo = round16(x' - z_hi); operand row
 //               [z_hi (kpad) | z_lo (kpad)].  Metadata: A = ||x'||^2 (FP64), Y >= ||x'||,
 //               Z >= ||z_hi + z_lo||, Zl >= ||z_lo||, E >= ||x' - z_hi - z_lo||.
 //   int8 limbs: q = 128 h + l for int14 input, exact integer ||q||^2.
-template <int kScreen, int kSplit>
+template <int kScreen, int kSplit, int kL>   // kL lanes per row (4, 8 or 32): 32 / kL rows per warp
 __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kpad, long long rows_pad,
                           const uint32_t* perm, const float* center, uint16_t* op, int8_t* op8, float* xs,
                           double* nrm2, float* nrm2f, float* zn, float* en, float* yn, float* zl, long long* inorm,
                           unsigned long long* status) {
-    const long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const unsigned lane = threadIdx.x & 31;
-    if (r >= rows_pad) return;
-    const bool real = r < n;
+    const long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / kL;
+    const unsigned sub = threadIdx.x % kL;
+    const bool live = r < rows_pad;          // lanes past the end still take part in the shuffles
+    const bool real = live && r < n;
     const size_t orig = real ? (size_t)perm[r] : 0;
     double sx = 0.0, sz = 0.0, se = 0.0, sl = 0.0;
     long long sq = 0;
-    bool bad = false, fp16_range = false;
+    unsigned flags = 0;   // 1: bad input, 2: FP16 range
     const int opw = kSplit ? 2 * kpad : kpad;
-    for (int k = lane; k < kpad; k += 32) {
+    for (int k = sub; k < kpad && live; k += kL) {
         float x = 0.f;
         if (real && k < d) x = load_x(src, dtype, orig * d + k);
-        if (!isfinite(x)) { bad = true; x = 0.f; }
+        if (!isfinite(x)) { flags |= 1u; x = 0.f; }
         if (kScreen == kScreenPlain) {
             if (k < d) xs[(size_t)r * d + k] = x;
             sx += (double)x * x;
         } else if (kScreen == kScreenInt8Limb) {   // q = 128 h + l, h = floor((q + 64) / 128)
             const int q = (int)x;
-            if (q < -8192 || q > 8191) bad = true;
+            if (q < -8192 || q > 8191) flags |= 1u;
             const int h = (q + 64 + 8192) / 128 - 64;
             const int l = q - 128 * h;
             op8[(size_t)r * (2 * kpad) + k] = (int8_t)h;
@@ -244,7 +258,7 @@ __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kp
             constexpr int kFmt = (kScreen == kScreenBF16 || kScreen == kScreenBF16X3) ? 1 : 0;
             const double xc = (k < d && real) ? (double)x - (double)center[k] : 0.0;
             const float xf = (float)xc;
-            if (kFmt == 0 && fabsf(xf) > 65504.f) fp16_range = true;
+            if (kFmt == 0 && fabsf(xf) > 65504.f) flags |= 2u;
             uint16_t bh = 0, bl = 0;
             const float zh = round16<kFmt>(xf, bh);
             double z = (double)zh;
@@ -262,18 +276,17 @@ __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kp
         }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = kL / 2; o > 0; o >>= 1) {
         sx += __shfl_xor_sync(0xffffffffu, sx, o);
         sz += __shfl_xor_sync(0xffffffffu, sz, o);
         se += __shfl_xor_sync(0xffffffffu, se, o);
         sl += __shfl_xor_sync(0xffffffffu, sl, o);
         sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        flags |= __shfl_xor_sync(0xffffffffu, flags, o);
     }
-    bad = __any_sync(0xffffffffu, bad);
-    fp16_range = __any_sync(0xffffffffu, fp16_range);
-    if (lane == 0) {
-        if (bad && real) atomicOr(status, (unsigned long long)kStatusBadInput);
-        if (fp16_range && real) atomicOr(status, (unsigned long long)kStatusFp16Range);
+    if (sub == 0 && live) {
+        if ((flags & 1u) && real) atomicOr(status, (unsigned long long)kStatusBadInput);
+        if ((flags & 2u) && real) atomicOr(status, (unsigned long long)kStatusFp16Range);
         if (real && sx > 0x1p100) atomicOr(status, (unsigned long long)kStatusBadInput);
         // FP64 sums of d non-negative squares (each rounded once): relative error <= (d+2) 2^-53;
         // x - c may round once more (2^-53 relative), absorbed by the extra 2^-50 terms.
@@ -290,7 +303,8 @@ __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kp
     }
 }
 
-// Tile statistics: one block per tile.
+// Tile statistics: one block per tile; kL lanes per row (4, 8 or 32), 256 / kL rows at a time.
+template <int kL>
 __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dtype, long long n, int d, int tile,
                                                          int ntiles, const uint32_t* perm, const double* nrm2,
                                                          const float* nrm2f, const float* zn, const float* en,
@@ -308,31 +322,33 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
     const double g = (double)(d + 2) * 0x1p-53;
     // per-dimension centroid and bounding box
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int kNG = 256 / kL;                   // row groups per block
+    const int grp = threadIdx.x / kL, sub = threadIdx.x % kL;
     if (warp_rows) {
-        // warp w reads rows w, w+8, ... (coalesced across dimensions); per-warp partials in shared
-        // memory, combined over the 8 warps in a fixed order
-        double* psum = (double*)(s_ctr + ((d + 1) & ~1));   // [8][d]
-        float* pmin = (float*)(psum + 8 * d);               // [8][d]
-        float* pmax = pmin + 8 * d;                         // [8][d]
-        for (int k = lane; k < d; k += 32) {
-            psum[warp * d + k] = 0.0;
-            pmin[warp * d + k] = INFINITY;
-            pmax[warp * d + k] = -INFINITY;
+        // group q reads rows q, q + kNG, ... (coalesced across dimensions); per-group partials in
+        // shared memory, combined over the groups in a fixed order
+        double* psum = (double*)(s_ctr + ((d + 1) & ~1));   // [kNG][d]
+        float* pmin = (float*)(psum + kNG * d);             // [kNG][d]
+        float* pmax = pmin + kNG * d;                       // [kNG][d]
+        for (int k = sub; k < d; k += kL) {
+            psum[grp * d + k] = 0.0;
+            pmin[grp * d + k] = INFINITY;
+            pmax[grp * d + k] = -INFINITY;
         }
-        for (int i = warp; i < nv; i += 8) {
+        for (int i = grp; i < nv; i += kNG) {
             const size_t base = (size_t)perm[r0 + i] * d;
-            for (int k = lane; k < d; k += 32) {
+            for (int k = sub; k < d; k += kL) {
                 const float v = load_x(src, dtype, base + k);
-                psum[warp * d + k] += v;
-                pmin[warp * d + k] = fminf(pmin[warp * d + k], v);
-                pmax[warp * d + k] = fmaxf(pmax[warp * d + k], v);
+                psum[grp * d + k] += v;
+                pmin[grp * d + k] = fminf(pmin[grp * d + k], v);
+                pmax[grp * d + k] = fmaxf(pmax[grp * d + k], v);
             }
         }
         __syncthreads();
         for (int k = threadIdx.x; k < d; k += blockDim.x) {
             double sm = 0.0;
             float mn = INFINITY, mx = -INFINITY;
-            for (int w = 0; w < 8; ++w) {
+            for (int w = 0; w < kNG; ++w) {
                 sm += psum[w * d + k];
                 mn = fminf(mn, pmin[w * d + k]);
                 mx = fmaxf(mx, pmax[w * d + k]);
@@ -361,19 +377,25 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
         }
     }
     __syncthreads();
-    // radius: warp per row, exact FP64 differences against the FP32 centroid
+    // radius: kL lanes per row, exact FP64 differences against the FP32 centroid; the row loop is
+    // uniform across each warp so that every lane takes part in the shuffles
     double rmax = 0.0;
-    for (int i = warp; i < nv; i += 8) {
-        const size_t base = (size_t)perm[r0 + i] * d;
+    for (int i0 = warp * (32 / kL); i0 < nv; i0 += kNG) {
+        const int i = i0 + (int)(lane / kL);
         double s = 0.0;
-        for (int k = lane; k < d; k += 32) {
-            const double df = (double)load_x(src, dtype, base + k) - (double)s_ctr[k];
-            s += df * df;
+        if (i < nv) {
+            const size_t base = (size_t)perm[r0 + i] * d;
+            for (int k = sub; k < d; k += kL) {
+                const double df = (double)load_x(src, dtype, base + k) - (double)s_ctr[k];
+                s += df * df;
+            }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        for (int o = kL / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         rmax = fmax(rmax, s);
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
     // row-bound maxima
     float mz = 0.f, me = 0.f, my = 0.f, mb = 0.f, mbeta = 0.f, mzl = 0.f;
     for (int i = threadIdx.x; i < nv; i += blockDim.x) {
@@ -677,10 +699,17 @@ void prepare_side(Side& s, const FrameParams* fpd, const float* center, cudaStre
     s.en = DBuf<float>(rp, st);
     s.yn = DBuf<float>(rp, st);
     s.zl = DBuf<float>(rp, st);
-    const unsigned blocks = (unsigned)((rp * 32 + 255) / 256);
-#define TJ_PREP(SCR, SPLIT)                                                                                        \
-    launch(prep_rows<SCR, SPLIT>, blocks, 256, 0, st, s.src, s.dtype, n, s.d, s.kpad, s.rows_pad, s.perm.p, center, \
-           s.op.p, s.op8.p, s.xs.p, s.nrm2.p, s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.zl.p, s.inorm.p, status)
+    // lanes per row: 4 for rows of <= 16 elements, 8 for <= 32, else a warp
+#define TJ_PREP_L(SCR, SPLIT, L)                                                                                 \
+    launch(prep_rows<SCR, SPLIT, L>, (unsigned)((rp * L + 255) / 256), 256, 0, st, s.src, s.dtype, n, s.d, s.kpad, \
+           s.rows_pad, s.perm.p, center, s.op.p, s.op8.p, s.xs.p, s.nrm2.p, s.nrm2f.p, s.zn.p, s.en.p, s.yn.p,      \
+           s.zl.p, s.inorm.p, status)
+#define TJ_PREP(SCR, SPLIT)                                    \
+    do {                                                       \
+        if (s.kpad <= 16) TJ_PREP_L(SCR, SPLIT, 4);            \
+        else if (s.kpad <= 32) TJ_PREP_L(SCR, SPLIT, 8);       \
+        else TJ_PREP_L(SCR, SPLIT, 32);                        \
+    } while (0)
     switch (s.screen) {
         case kScreenPlain: TJ_PREP(kScreenPlain, 0); break;
         case kScreenBF16: TJ_PREP(kScreenBF16, 0); break;
@@ -690,6 +719,7 @@ void prepare_side(Side& s, const FrameParams* fpd, const float* center, cudaStre
         default: TJ_PREP(kScreenInt8Limb, 0); break;
     }
 #undef TJ_PREP
+#undef TJ_PREP_L
 }
 
 void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st) {
@@ -715,18 +745,24 @@ void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st) {
         upload(ts.row0.p, ts.h_row0.data(), nt * 4, st);
         upload(ts.nvalid.p, ts.h_nvalid.data(), nt * 4, st);
     }
-    // centroid [d] floats (rounded up to an even count) + per-warp partials (8 x d x (8 + 4 + 4) bytes)
+    // lanes per row as in prep_rows; centroid [d] floats (rounded up to an even count) + per-group
+    // partials (256 / kL groups x d x (8 + 4 + 4) bytes)
+    const int L = s.d <= 16 ? 4 : s.d <= 32 ? 8 : 32;
     const size_t base = (size_t)((s.d + 1) & ~1) * sizeof(float);
-    const size_t part = (size_t)8 * s.d * 16;
+    const size_t part = (size_t)(256 / L) * s.d * 16;
     const int warp_rows = base + part <= 200 * 1024 ? 1 : 0;
     const size_t smem = base + (warp_rows ? part : 0);
-    if (smem > 48 * 1024)
-        TJ_CUDA(cudaFuncSetAttribute(tile_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    launch(tile_stats_kernel, ts.ntiles, 256, smem, st, s.src, s.dtype, s.n, s.d, tile, ts.ntiles, s.perm.p, s.nrm2.p,
-           s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.zl.p, ts.ctrT.p, ts.loT.p, ts.hiT.p, ts.rad.p, ts.maxZ.p, ts.maxE.p,
-           ts.maxY.p, ts.maxB.p, ts.beta.p, ts.maxZl.p, ts.nvalid.p, ts.row0.p,
-           tabled ? (const uint32_t*)ts.row0.p : (const uint32_t*)nullptr,
-           tabled ? (const uint32_t*)ts.nvalid.p : (const uint32_t*)nullptr, warp_rows);
+    auto run = [&](auto kern) {
+        if (smem > 48 * 1024) TJ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        launch(kern, ts.ntiles, 256, smem, st, s.src, s.dtype, s.n, s.d, tile, ts.ntiles, s.perm.p, s.nrm2.p,
+               s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.zl.p, ts.ctrT.p, ts.loT.p, ts.hiT.p, ts.rad.p, ts.maxZ.p,
+               ts.maxE.p, ts.maxY.p, ts.maxB.p, ts.beta.p, ts.maxZl.p, ts.nvalid.p, ts.row0.p,
+               tabled ? (const uint32_t*)ts.row0.p : (const uint32_t*)nullptr,
+               tabled ? (const uint32_t*)ts.nvalid.p : (const uint32_t*)nullptr, warp_rows);
+    };
+    if (L == 4) run(tile_stats_kernel<4>);
+    else if (L == 8) run(tile_stats_kernel<8>);
+    else run(tile_stats_kernel<32>);
 }
 
 void gather_rows(const std::vector<const void*>& srcs, const std::vector<long long>& rows, int d, int esize,
