@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <string>
 #include <utility>
 #include <vector>
@@ -265,7 +266,18 @@ template <class... KArgs, class... Args>
 void launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
     k<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
     count_launch();
-    check_cuda(cudaGetLastError(), "kernel launch");
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {   // name the kernel's resources in the error
+        cudaFuncAttributes fa;
+        memset(&fa, 0, sizeof(fa));
+        cudaFuncGetAttributes(&fa, k);
+        cudaGetLastError();
+        fail(-2, std::string("kernel launch: ") + cudaGetErrorString(e) + " (block " +
+                     std::to_string(block.x * block.y * block.z) + " threads, " + std::to_string(smem) +
+                     " B dynamic shared; kernel: " + std::to_string(fa.numRegs) + " registers, max " +
+                     std::to_string(fa.maxThreadsPerBlock) + " threads, " + std::to_string(fa.sharedSizeBytes) +
+                     " B static shared, " + std::to_string(fa.maxDynamicSharedSizeBytes) + " B dynamic allowed)");
+    }
 }
 
 }  // namespace tj

@@ -370,40 +370,49 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&ctl->acc_empty[acc]);
                     }
-                    // fast path: one FMA and one min per pair (four independent min chains); only a
-                    // 32-column group whose minimum passes the threshold builds the candidate mask
+                    // fast path: one FMA and one min per pair, one min chain per 8-column group; only the
+                    // groups whose minimum passes tau (in any lane of the warp) are examined pair by pair
                     const float4* nb4 = reinterpret_cast<const float4*>(&m.nrm2f[col0]);
-                    float vm[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+                    float vm[4];
 #pragma unroll
-                    for (int k4 = 0; k4 < 8; ++k4) {
-                        const float4 b = nb4[k4];
-                        vm[0] = fminf(vm[0], fmaf(-2.f, __uint_as_float(raw[4 * k4 + 0]), b.x));
-                        vm[1] = fminf(vm[1], fmaf(-2.f, __uint_as_float(raw[4 * k4 + 1]), b.y));
-                        vm[2] = fminf(vm[2], fmaf(-2.f, __uint_as_float(raw[4 * k4 + 2]), b.z));
-                        vm[3] = fminf(vm[3], fmaf(-2.f, __uint_as_float(raw[4 * k4 + 3]), b.w));
+                    for (int g = 0; g < 4; ++g) {
+                        const float4 b0 = nb4[2 * g], b1 = nb4[2 * g + 1];
+                        const uint32_t* r8 = raw + 8 * g;
+                        float v = fmaf(-2.f, __uint_as_float(r8[0]), b0.x);
+                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[1]), b0.y));
+                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[2]), b0.z));
+                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[3]), b0.w));
+                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[4]), b1.x));
+                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[5]), b1.y));
+                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[6]), b1.z));
+                        vm[g] = fminf(v, fmaf(-2.f, __uint_as_float(r8[7]), b1.w));
                     }
-                    const bool hit = fminf(fminf(vm[0], vm[1]), fminf(vm[2], vm[3])) <= tau;
-                    if (!__any_sync(0xffffffffu, hit)) continue;
-                    uint32_t cmask = 0;
-                    if (hit) {
+                    const unsigned gmask = (vm[0] <= tau ? 1u : 0u) | (vm[1] <= tau ? 2u : 0u) |
+                                           (vm[2] <= tau ? 4u : 0u) | (vm[3] <= tau ? 8u : 0u);
+                    const unsigned gunion = __reduce_or_sync(0xffffffffu, gmask);
+                    if (!gunion) continue;
+                    // candidate (v <= tau) and certified-in (v <= tau_in) masks over the hit groups only
+                    uint32_t cmask = 0, inm = 0;
 #pragma unroll
-                        for (int k = 0; k < 32; ++k)
-                            cmask |= (fmaf(-2.f, __uint_as_float(raw[k]), m.nrm2f[col0 + k]) <= tau ? 1u : 0u) << k;
-                        if (jp.self_join) {   // keep sorted column > sorted row only
-                            const int lim = (int)rs - (int)(c0 + col0);   // columns k <= lim: not above the diagonal
-                            if (lim >= 31) cmask = 0;
-                            else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
+                    for (int g = 0; g < 4; ++g) {
+                        if (!(gunion & (1u << g))) continue;
+                        if (gmask & (1u << g)) {
+#pragma unroll
+                            for (int k = 8 * g; k < 8 * g + 8; ++k) {
+                                const float v = fmaf(-2.f, __uint_as_float(raw[k]), m.nrm2f[col0 + k]);
+                                cmask |= (v <= tau ? 1u : 0u) << k;
+                                inm |= (v <= tau_in ? 1u : 0u) << k;
+                            }
                         }
+                    }
+                    if (jp.self_join && cmask) {   // keep sorted column > sorted row only
+                        const int lim = (int)rs - (int)(c0 + col0);   // columns k <= lim: not above the diagonal
+                        if (lim >= 31) cmask = 0;
+                        else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
                     }
                     if (!__any_sync(0xffffffffu, cmask != 0)) continue;
                     // ---------------- rare path: certified FP32 accept, else per-pair FP64 certificate
-                    uint32_t inm = 0;
-                    if (cmask) {
-#pragma unroll
-                        for (int k = 0; k < 32; ++k)
-                            inm |= (fmaf(-2.f, __uint_as_float(raw[k]), m.nrm2f[col0 + k]) <= tau_in ? 1u : 0u) << k;
-                        inm &= cmask;
-                    }
+                    inm &= cmask;
                     uint32_t amask = inm, bmask = 0;
                     uint32_t mk = cmask & ~inm;
                     while (mk) {

@@ -269,29 +269,41 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                     uint32_t hv[32];
                     tmem_ld32(tmem + lane_off + kColHH0 + b * 128 + cc, hv);
                     tmem_ld_wait();
-                    // fast path: one subtract and one max per pair (four independent chains); only a
-                    // 32-column group whose maximum reaches the threshold builds the candidate mask
+                    // fast path: one subtract and one max per pair, one max chain per 8-column group; only
+                    // the groups whose maximum reaches the threshold (in any lane) are examined pair by pair
                     const int4* bq4 = reinterpret_cast<const int4*>(&m.bq[cc]);
-                    int vx[4] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN};
+                    int vx[4];
 #pragma unroll
-                    for (int k4 = 0; k4 < 8; ++k4) {
-                        const int4 bb = bq4[k4];
-                        vx[0] = max(vx[0], (int)hv[4 * k4 + 0] - bb.x);
-                        vx[1] = max(vx[1], (int)hv[4 * k4 + 1] - bb.y);
-                        vx[2] = max(vx[2], (int)hv[4 * k4 + 2] - bb.z);
-                        vx[3] = max(vx[3], (int)hv[4 * k4 + 3] - bb.w);
+                    for (int g = 0; g < 4; ++g) {
+                        const int4 b0 = bq4[2 * g], b1 = bq4[2 * g + 1];
+                        const uint32_t* h8 = hv + 8 * g;
+                        int v = (int)h8[0] - b0.x;
+                        v = max(v, (int)h8[1] - b0.y);
+                        v = max(v, (int)h8[2] - b0.z);
+                        v = max(v, (int)h8[3] - b0.w);
+                        v = max(v, (int)h8[4] - b1.x);
+                        v = max(v, (int)h8[5] - b1.y);
+                        v = max(v, (int)h8[6] - b1.z);
+                        vx[g] = max(v, (int)h8[7] - b1.w);
                     }
-                    const bool hit = max(max(vx[0], vx[1]), max(vx[2], vx[3])) >= ai;
-                    if (!__any_sync(0xffffffffu, hit)) continue;
+                    const unsigned gmask = (vx[0] >= ai ? 1u : 0u) | (vx[1] >= ai ? 2u : 0u) |
+                                           (vx[2] >= ai ? 4u : 0u) | (vx[3] >= ai ? 8u : 0u);
+                    const unsigned gunion = __reduce_or_sync(0xffffffffu, gmask);
+                    if (!gunion) continue;
                     uint32_t cmask = 0;
-                    if (hit) {
 #pragma unroll
-                        for (int k = 0; k < 32; ++k) cmask |= ((int)hv[k] - m.bq[cc + k] >= ai ? 1u : 0u) << k;
-                        if (jp.self_join) {   // keep sorted column > sorted row only
-                            const int lim = (int)rs - (int)(c0 + cc);
-                            if (lim >= 31) cmask = 0;
-                            else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
+                    for (int g = 0; g < 4; ++g) {
+                        if (!(gunion & (1u << g))) continue;
+                        if (gmask & (1u << g)) {
+#pragma unroll
+                            for (int k = 8 * g; k < 8 * g + 8; ++k)
+                                cmask |= ((int)hv[k] - m.bq[cc + k] >= ai ? 1u : 0u) << k;
                         }
+                    }
+                    if (jp.self_join && cmask) {   // keep sorted column > sorted row only
+                        const int lim = (int)rs - (int)(c0 + cc);
+                        if (lim >= 31) cmask = 0;
+                        else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
                     }
                     if (!__any_sync(0xffffffffu, cmask != 0)) continue;
                     uint32_t xv[32], lv[32];
