@@ -23,15 +23,16 @@
 // certificate: accept (emit), reject, or band (queued for the FP64 refinement
 // that reproduces the oracle's summation order).
 //
-// Warp roles (192 threads, one CTA per SM, persistent over the chunk list):
+// Warp roles (512 threads, one CTA per SM, persistent over the chunk list):
 //   warp 0: TMA producer (one lane): a ring of k-block stages {A 128 rows, B 256 rows} and a
 //           ring of per-item column-metadata blocks (one 8 KB bulk copy per S tile), so the
 //           epilogue never waits on global memory inside an item
 //   warp 1: TMEM allocator + UMMA issuer (one lane), 2 accumulators x 256 columns
-//   warps 2-9: epilogue, warp w reads TMEM lanes 32*(w%4) .. +31 (one R row per thread) and
-//           columns 128*((w-2)/4) .. +127 of the accumulator, so every SM sub-partition runs two
-//           epilogue warps that hide each other's TMEM and shared-memory latency; the eight warps
-//           run independently (no named barrier), synchronised only through mbarriers
+//   warps 4-15: epilogue, warp w reads TMEM lanes 32*(w%4) .. +31 (one R row per thread) and one
+//           third of the accumulator's columns (blocks of 32: [0,3), [3,6), [6,8) for (w-4)/4 = 0,1,2),
+//           so every SM sub-partition runs three epilogue warps that hide each other's latency; the
+//           twelve warps run independently (no named barrier), synchronised only through mbarriers
+//   warps 2-3: idle (they complete the first warpgroup)
 #include <algorithm>
 #include <cstring>
 
@@ -43,8 +44,9 @@ namespace tj {
 namespace {
 
 constexpr int kAccBufs = 2;
-constexpr int kEpiWarps = 8;                        // two per TMEM lane quarter (column halves)
-constexpr int kScreenThreads = (2 + kEpiWarps) * 32;
+constexpr int kEpiWarps = 12;                       // three per TMEM lane quarter (column thirds)
+constexpr int kEpiFirst = 4;                         // warps 0-3: TMA producer, UMMA issuer, two idle
+constexpr int kScreenThreads = (kEpiFirst + kEpiWarps) * 32;
 constexpr unsigned kABytes = kTileR * 128;          // 16 KB
 constexpr unsigned kBBytes = kTileS * 128;          // 32 KB
 constexpr int kMetaSlots = 3;
@@ -306,12 +308,13 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             umma_commit(&ctl->drain);
             mbar_wait(&ctl->drain, 0, status, 1000000000ull);
         }
-    } else {
+    } else if (warp >= kEpiFirst) {
         // ------------------------------------------------------------ epilogue
         const unsigned q = warp & 3;                 // TMEM lane quarter of this warp
-        const unsigned half = (warp - 2) >> 2;       // accumulator column half of this warp
-        const unsigned row = q * 32 + lane;          // R row within the tile
-        constexpr int kCbPerWarp = kTileS / 32 / 2;
+        const unsigned part = (warp - kEpiFirst) >> 2;   // accumulator column third of this warp
+        const unsigned row = q * 32 + lane;              // R row within the tile
+        // 32-column blocks of the 256-column accumulator: thirds [0, 3), [3, 6), [6, 8)
+        const int cb_begin = (int)part * 3, cb_end = part == 2 ? kTileS / 32 : (int)part * 3 + 3;
         WarpAppender app_acc, app_band;
         unsigned acc = 0, acc_phase = 0;
         unsigned long long n = 0, n_screen_acc = 0, n_rare = 0, n_items = 0;
@@ -320,14 +323,15 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             const uint4 ch = a.chunks[c];
             const uint4 rt = a.rtiles[ch.x];
             const ScreenClassArgs& ca = a.cls[rt.w];
-            const JoinParams jp = a.jps[rt.z];
+            const JoinParams& jp = a.jps[rt.z];   // read through L1 where used
             const unsigned r0 = rt.x;
             const bool rvalid = row < rt.y;
             const unsigned rs = r0 + row;
             const double Ai = rvalid ? ca.r_nrm2[rs] : 0.0;
-            const double Zi = rvalid ? (double)ca.r_zn[rs] : 0.0;
-            const double Ei = rvalid ? (double)ca.r_en[rs] : 0.0;
-            const double Zli = rvalid ? (double)ca.r_zl[rs] : 0.0;
+            // row bounds held as FP32 (exact in FP64, widened where used)
+            const float Zi = rvalid ? ca.r_zn[rs] : 0.f;
+            const float Ei = rvalid ? ca.r_en[rs] : 0.f;
+            const float Zli = rvalid ? ca.r_zl[rs] : 0.f;
             const uint32_t oi = rvalid ? ca.r_emit[rs] : 0u;
             for (unsigned e = ch.y; e < ch.z; ++e, ++n) {
                 const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
@@ -342,8 +346,9 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 float tau = -INFINITY, tau_in = -INFINITY;
                 if (rvalid) {
                     const double WJ = m.WJ, FJ = m.FJ, YJ = m.YJ, BJ = m.BJ, betaJ = m.betaJ, WlJ = m.WlJ;
-                    const double RiJ = jp.gmma * Zi * WJ + jp.cabs + Ei * YJ + Zi * FJ + Zli * WlJ;
-                    const double PiJ = Zi * WJ * (1.0 + jp.gmma) + jp.cabs;
+                    const double Zd = Zi, Ed = Ei, Zld = Zli;
+                    const double RiJ = jp.gmma * Zd * WJ + jp.cabs + Ed * YJ + Zd * FJ + Zld * WlJ;
+                    const double PiJ = Zd * WJ * (1.0 + jp.gmma) + jp.cabs;
                     const double slack = jp.gn * Ai + 0x1p-23 * (BJ + 2.0 * PiJ) + betaJ + 2.0 * RiJ;
                     // the 2^-40 / 2^-50 terms exceed the FP64 rounding of these sums even under cancellation
                     const double t = jp.Tp - Ai + slack * (1.0 + 0x1p-40) + 0x1p-50 * (jp.Tp + Ai) + 0x1p-1000;
@@ -353,7 +358,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 }
                 const unsigned tbase = tmem + ((q * 32u) << 16) + acc * kTileS;
 #pragma unroll 1
-                for (int cb = half * kCbPerWarp; cb < (int)(half + 1) * kCbPerWarp; ++cb) {
+                for (int cb = cb_begin; cb < cb_end; ++cb) {
                     const int col0 = cb * 32;
                     uint32_t raw[32];
                     tmem_ld32(tbase + col0, raw);
@@ -365,27 +370,26 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         for (int k = 0; k < 32; ++k) out[k] = __uint_as_float(raw[k]);
                         if (row == 0 && cb == 0) a.dump_ids[slotd] = make_uint4(ch.x, a.jlist[e], 1u, 0u);
                     }
-                    if (cb == (int)(half + 1) * kCbPerWarp - 1) {   // this warp's part read: hand it back
+                    if (cb == cb_end - 1) {   // this warp's part read: hand it back
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&ctl->acc_empty[acc]);
                     }
-                    // fast path: one FMA and one min per pair, one min chain per 8-column group; only the
-                    // groups whose minimum passes tau (in any lane of the warp) are examined pair by pair
+                    // fast path: v = fma(-2, p, B~) two pairs per packed FMA, folded by three-input mins
+                    // (one instruction per pair), one min chain per 8-column group; only the groups whose
+                    // minimum passes tau (in any lane of the warp) are examined pair by pair
                     const float4* nb4 = reinterpret_cast<const float4*>(&m.nrm2f[col0]);
                     float vm[4];
 #pragma unroll
                     for (int g = 0; g < 4; ++g) {
                         const float4 b0 = nb4[2 * g], b1 = nb4[2 * g + 1];
                         const uint32_t* r8 = raw + 8 * g;
-                        float v = fmaf(-2.f, __uint_as_float(r8[0]), b0.x);
-                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[1]), b0.y));
-                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[2]), b0.z));
-                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[3]), b0.w));
-                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[4]), b1.x));
-                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[5]), b1.y));
-                        v = fminf(v, fmaf(-2.f, __uint_as_float(r8[6]), b1.z));
-                        vm[g] = fminf(v, fmaf(-2.f, __uint_as_float(r8[7]), b1.w));
+                        float v0, v1, v2, v3, v4, v5, v6, v7;
+                        fma_m2_x2(__uint_as_float(r8[0]), __uint_as_float(r8[1]), b0.x, b0.y, v0, v1);
+                        fma_m2_x2(__uint_as_float(r8[2]), __uint_as_float(r8[3]), b0.z, b0.w, v2, v3);
+                        fma_m2_x2(__uint_as_float(r8[4]), __uint_as_float(r8[5]), b1.x, b1.y, v4, v5);
+                        fma_m2_x2(__uint_as_float(r8[6]), __uint_as_float(r8[7]), b1.z, b1.w, v6, v7);
+                        vm[g] = fmin3(fmin3(fmin3(v0, v1, v2), v3, v4), fminf(v5, v6), v7);
                     }
                     const unsigned gmask = (vm[0] <= tau ? 1u : 0u) | (vm[1] <= tau ? 2u : 0u) |
                                            (vm[2] <= tau ? 4u : 0u) | (vm[3] <= tau ? 8u : 0u);
@@ -423,16 +427,17 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         const double p = (double)__uint_as_float(pick32(raw, k));
                         const double Bj = m.nrm2[col];
                         const double sv = Ai + Bj - 2.0 * p;
-                        const double R = jp.gmma * Zi * (double)m.zn[col] + jp.cabs + Ei * (double)m.yn[col] +
-                                         Zi * (double)m.en[col] + Zli * (double)m.zl[col];
+                        const double R = jp.gmma * (double)Zi * (double)m.zn[col] + jp.cabs +
+                                         (double)Ei * (double)m.yn[col] + (double)Zi * (double)m.en[col] +
+                                         (double)Zli * (double)m.zl[col];
                         double mm = 2.0 * R + jp.gn * (Ai + Bj) + 0x1p-50 * (Ai + Bj + 2.0 * fabs(p));
                         mm = mm * (1.0 + 0x1p-40) + 0x1p-1000;
                         if (sv + mm <= jp.Tm) amask |= 1u << k;
                         else if (!(sv - mm > jp.Tp)) bmask |= 1u << k;
                     }
-                    unsigned ta, tb;
-                    const unsigned pa = warp_excl_scan(__popc(amask), ta);
-                    const unsigned pb = warp_excl_scan(__popc(bmask), tb);
+                    unsigned ta = 0, tb = 0, pa = 0, pb = 0;   // scans only for lists some lane appends to
+                    if (__any_sync(0xffffffffu, amask != 0)) pa = warp_excl_scan(__popc(amask), ta);
+                    if (__any_sync(0xffffffffu, bmask != 0)) pb = warp_excl_scan(__popc(bmask), tb);
                     if (ta) {
                         unsigned long long pos = app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap) + pa;
                         uint32_t w = amask;
@@ -474,7 +479,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             if (app_band.valid) atomicAdd(&a.ctr->band_valid, app_band.valid);
             if (n_screen_acc) atomicAdd(&a.ctr->screen_accept, n_screen_acc);
             if (n_rare) atomicAdd(&a.ctr->rare_checks, n_rare);
-            if (warp == 2 && n_items) atomicAdd(&a.ctr->items, n_items);
+            if (warp == kEpiFirst && n_items) atomicAdd(&a.ctr->items, n_items);
         }
     }
     tc_fence_before();
