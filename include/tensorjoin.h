@@ -71,6 +71,9 @@ typedef struct tj_options {
 /* Sample tile pairs during the tensor-core screen and report the screen's distance error against
  * sequential FP64 distances (tj_stats.screen_*).  Diagnostic: adds a sampling pass. */
 #define TJ_FLAG_SCREEN_DIAG 1
+/* Use the one-SM tensor-core screen even where the CTA-pair screen (cta_group::2, 256 x 256 tiles
+ * over two SMs; one join, rows of >= 256 elements, every tile pair a candidate) would run. */
+#define TJ_FLAG_SCREEN_1SM 2
 
 typedef struct tj_stats {
     int64_t n_rows, n_cols;       /* |R|, |S| (self-join: N, N) */
@@ -88,6 +91,7 @@ typedef struct tj_stats {
     double screen_max_abs_err;    /* TJ_FLAG_SCREEN_DIAG: max |(|x|^2 + |y|^2 - 2p) - d2_fp64| over the sampled pairs */
     double screen_err_over_bound; /* TJ_FLAG_SCREEN_DIAG: max of that error divided by the certified radius */
     int64_t screen_err_pairs;     /* TJ_FLAG_SCREEN_DIAG: sampled pairs */
+    int64_t screen_pair;          /* 1 if the CTA-pair tensor-core screen ran */
 } tj_stats;
 
 /* ----------------------------------------------------------------- joins */

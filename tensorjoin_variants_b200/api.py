@@ -146,15 +146,17 @@ def _run(R, S, eps, eps2, mode: str, screen: str, capacity: int, chunk_items: in
 
 
 def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "bf16", capacity: int = 0,
-                chunk_items: int = 0, screen_diag: bool = False) -> Result:
+                chunk_items: int = 0, screen_diag: bool = False, cta_pair: bool = True) -> Result:
     """Run a join and return the Result handle (pairs, keys, neighbour table, statistics).
 
     ``screen_diag=True`` also samples 64 tile pairs of the tensor-core screen and reports, in
     ``stats``, the screen's largest distance error against sequential FP64 distances and that
-    error relative to the certified radius (must stay below 1)."""
+    error relative to the certified radius (must stay below 1).  ``cta_pair=False`` keeps the
+    one-SM screen where the CTA-pair screen would run (``stats["screen_pair"]`` says which ran)."""
     if mode not in MODE:
         raise ValueError(f"mode must be one of {sorted(MODE)}")
-    return _run(R, S, eps, eps2, mode, screen, capacity, chunk_items, _lib.FLAG_SCREEN_DIAG if screen_diag else 0)
+    flags = (_lib.FLAG_SCREEN_DIAG if screen_diag else 0) | (0 if cta_pair else _lib.FLAG_SCREEN_1SM)
+    return _run(R, S, eps, eps2, mode, screen, capacity, chunk_items, flags)
 
 
 def join(R, S, eps=None, *, eps2=None, screen: str = "bf16", return_stats: bool = False, **kw):

@@ -476,6 +476,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     g.stiles = d_st.p;
     g.jps = d_jps.p;
     g.h_jps = jps.data();
+    g.allow_pair = !(opt && (opt->flags & TJ_FLAG_SCREEN_1SM));
     g.key_off = d_koff.p;
     g.rsrc = d_rsrc.p;
     g.ssrc = d_ssrc.p;
@@ -571,6 +572,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         if (screen == TJ_SCREEN_PLAIN) screen_plain(g, eb, st);
         else if (i8) screen_i8(g, eb, st);
         else screen_tc(g, eb, st);
+        S_.screen_pair = g.used_pair ? 1 : 0;
         ev.rec(3, st);
         if (!i8) refine_band(g, eb, st);   // the int8-limb screen is exact: no band
         ev.rec(4, st);
@@ -662,7 +664,7 @@ int tj_join(const void* R, int64_t nR, const void* S, int64_t nS, int32_t d, int
     if (mode < 0 || mode > 2) fail(TJ_ERR_INVALID, "unknown mode");
     if (screen < 0 || screen > 5) fail(TJ_ERR_INVALID, "unknown screen");
     if (dtype != TJ_DTYPE_F32 && dtype != TJ_DTYPE_I16) fail(TJ_ERR_INVALID, "unknown dtype");
-    if (opt && (opt->flags & ~TJ_FLAG_SCREEN_DIAG)) fail(TJ_ERR_INVALID, "unknown option flags");
+    if (opt && (opt->flags & ~(TJ_FLAG_SCREEN_DIAG | TJ_FLAG_SCREEN_1SM))) fail(TJ_ERR_INVALID, "unknown option flags");
     std::unique_ptr<tj_result> res(new tj_result());
     std::vector<JoinIn> js{JoinIn{R, (const void*)(mode == TJ_MODE_RS ? S : R), nR, mode == TJ_MODE_RS ? nS : nR,
                                   d, eps2}};
@@ -813,7 +815,7 @@ int tj_join_batched(const tj_batch_join* joins, int32_t njoins, int32_t screen, 
     *out = nullptr;
     if (njoins < 1) fail(TJ_ERR_INVALID, "njoins must be >= 1");
     if (screen < 0 || screen > 5 || screen == TJ_SCREEN_INT8LIMB) fail(TJ_ERR_UNSUPPORTED, "batched joins take FP32 screens");
-    if (opt && (opt->flags & ~TJ_FLAG_SCREEN_DIAG)) fail(TJ_ERR_INVALID, "unknown option flags");
+    if (opt && (opt->flags & ~(TJ_FLAG_SCREEN_DIAG | TJ_FLAG_SCREEN_1SM))) fail(TJ_ERR_INVALID, "unknown option flags");
     std::vector<JoinIn> js((size_t)njoins);
     for (int k = 0; k < njoins; ++k) js[k] = JoinIn{joins[k].R, joins[k].S, joins[k].nR, joins[k].nS, joins[k].d, joins[k].eps2};
     std::unique_ptr<tj_result> res(new tj_result());

@@ -64,6 +64,24 @@ TJ_DEV unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_sha
 TJ_DEV float f32_up(double x) { float r; asm("cvt.rp.f32.f64 %0, %1;" : "=f"(r) : "d"(x)); return r; }
 TJ_DEV float f32_dn(double x) { float r; asm("cvt.rm.f32.f64 %0, %1;" : "=f"(r) : "d"(x)); return r; }
 
+// v0 = fma(-2, p0, c0), v1 = fma(-2, p1, c1) as one packed FP32x2 FMA (sm_100), each lane rounded
+// exactly as the scalar fmaf.
+TJ_DEV void fma_m2_x2(float p0, float p1, float c0, float c1, float& v0, float& v1) {
+    asm("{\n\t.reg .b64 a, c, m, r;\n\t"
+        "mov.b64 a, {%2, %3};\n\t"
+        "mov.b64 c, {%4, %5};\n\t"
+        "mov.b64 m, {%6, %6};\n\t"
+        "fma.rn.f32x2 r, a, m, c;\n\t"
+        "mov.b64 {%0, %1}, r;\n\t}"
+        : "=f"(v0), "=f"(v1) : "f"(p0), "f"(p1), "f"(c0), "f"(c1), "f"(-2.0f));
+}
+// min of three floats in one instruction (sm_100); a NaN operand is ignored, as by fminf.
+TJ_DEV float fmin3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // exclusive warp prefix sum of v (all 32 lanes participate)
 TJ_DEV unsigned warp_excl_scan(unsigned v, unsigned& total) {
     unsigned x = v;
@@ -170,6 +188,76 @@ TJ_DEV void umma_i8(unsigned d_tmem, uint64_t adesc, uint64_t bdesc, unsigned id
 TJ_DEV void umma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                  :: "r"(smem_u32(bar)) : "memory");
+}
+
+// ---------------------------------------------------------------- CTA pairs (cta_group::2)
+TJ_DEV unsigned cluster_ctarank() { unsigned r; asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r)); return r; }
+// all threads of both CTAs of the cluster (release / acquire at cluster scope)
+TJ_DEV void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// shared::cluster address of the same shared variable in CTA `rank` of the cluster
+TJ_DEV unsigned mapa_shared(const void* p, unsigned rank) {
+    unsigned r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+    return r;
+}
+// arrive on an mbarrier of (possibly) another CTA of the cluster, releasing at cluster scope
+TJ_DEV void mbar_arrive_cluster(unsigned bar_cluster_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" :: "r"(bar_cluster_addr) : "memory");
+}
+TJ_DEV bool mbar_try_wait_cluster(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// bounded wait with cluster-scope acquire (a barrier that the other CTA of the pair arrives on)
+TJ_DEV bool mbar_wait_cluster(uint64_t* bar, unsigned parity, unsigned long long* status,
+                              unsigned long long limit_ns = kWaitLimitNs) {
+    for (int it = 0; it < 256; ++it)
+        if (mbar_try_wait_cluster(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (true) {
+        if (mbar_try_wait_cluster(bar, parity)) return true;
+        __nanosleep(64);
+        if (global_ns() - t0 > limit_ns) break;
+    }
+    atomicOr(status, (unsigned long long)kStatusWaitTimeout);
+    return false;
+}
+// TMA tile load into this CTA's shared memory whose completion is counted on an mbarrier of
+// either CTA of the pair (cta_group::2); no multicast.
+TJ_DEV void tma_load_2d_pair(void* dst, const CUtensorMap* map, unsigned bar_cluster_addr, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4}], [%2];"
+        :: "r"(smem_u32(dst)), "l"((uint64_t)map), "r"(bar_cluster_addr), "r"(x), "r"(y) : "memory");
+}
+TJ_DEV void tmem_alloc_pair(unsigned* dst_smem, unsigned ncols) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(dst_smem)), "r"(ncols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+TJ_DEV void tmem_dealloc_pair(unsigned taddr, unsigned ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(ncols) : "memory");
+}
+// D (both CTAs' TMEM) (+)= A (M = 256: 128 rows from each CTA) * B^T (N columns, half from each CTA)
+TJ_DEV void umma_f16_pair(unsigned d_tmem, uint64_t adesc, uint64_t bdesc, unsigned idesc, unsigned accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        :: "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+}
+// arrive once, on completion of this thread's prior pair MMAs, on the mbarrier at this offset in
+// every CTA of `cta_mask`
+TJ_DEV void umma_commit_pair_mc(uint64_t* bar, uint16_t cta_mask) {
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
+                 :: "r"(smem_u32(bar)), "h"(cta_mask) : "memory");
 }
 
 // 32 lanes x 32 consecutive 32-bit columns; thread t receives lane (base_lane + t).

@@ -236,6 +236,8 @@ struct ScreenInput {
     const void* const* rsrc = nullptr;  // device [njoins]: caller's R rows of each join
     const void* const* ssrc = nullptr;  // device [njoins]
     long long T_int = 0;                // integer threshold (int8-limb screen, single join)
+    bool allow_pair = true;             // the CTA-pair tensor-core screen may be used where it applies
+    mutable bool used_pair = false;     // set by screen_tc
     JoinParams jp0{};                   // host copy of join 0's parameters (single-join kernels)
     // screen-error diagnostics (tensor-core screens): sampled accumulators and the analysis result
     float* dump = nullptr;              // [dump_items][128][256]

@@ -88,10 +88,23 @@ struct ScreenCtl {
     int abort_flag;
 };
 
-template <int kSplit>
+// CTA pair (cta_group::2, 256 x 256 tile over two SMs): a stage holds this CTA's 128 A rows and its
+// 128-row half of B for one 64-element k-block; the pair's MMA reads A and B from both CTAs.
+struct StageCfgPair {
+    static constexpr unsigned kBytes = kABytes + kABytes;   // 32 KB
+    static constexpr int kStages = 6;
+    static constexpr unsigned kAlo = 0;
+    static constexpr unsigned kBhi = kABytes;
+    static constexpr unsigned kBlo = 0;
+};
+template <int kSplit, bool kPair> struct StageSel { using type = StageCfg<kSplit>; };
+template <> struct StageSel<0, true> { using type = StageCfgPair; };
+
+template <int kSplit, bool kPair>
 constexpr size_t screen_smem() {
-    return 1024 + (size_t)StageCfg<kSplit>::kStages * StageCfg<kSplit>::kBytes +
-           (size_t)kMetaSlots * sizeof(ColMetaF) + sizeof(ScreenCtl<StageCfg<kSplit>::kStages>);
+    using Cfg = typename StageSel<kSplit, kPair>::type;
+    return 1024 + (size_t)Cfg::kStages * Cfg::kBytes + (size_t)kMetaSlots * sizeof(ColMetaF) +
+           sizeof(ScreenCtl<Cfg::kStages>);
 }
 
 // Per-class pointers (a class = joins with the same d, one concatenated operand matrix per side).
@@ -124,6 +137,9 @@ struct ScreenArgs {
     ScreenClassArgs cls[kMaxClass];
     int ncls;
     unsigned idesc;
+    // CTA-pair mode: every (R tile, S tile) pair is a candidate; chunks are generated from the grid
+    unsigned idesc_pair;       // M = 256 instruction descriptor
+    unsigned ntR, ntS, nT;     // R tiles, S tiles, R tile pairs
     uint64_t* acc;
     unsigned long long acc_cap;
     uint64_t* band;
@@ -176,10 +192,37 @@ __global__ void __launch_bounds__(kTileS) build_col_meta(const uint32_t* row0, c
     }
 }
 
-template <int kFmt, int kSplit>   // kFmt: 0 = fp16, 1 = bf16; kSplit: hi/lo operand limbs
+// One work chunk: R tile, its table entry and a range of items (S tiles).  In CTA-pair mode chunk c
+// is (R tile pair t, S tiles [64 jc, 64 jc + 64)) with t = c mod nT; CTA `rank` of the pair takes R
+// tile 2t + rank (a tile past the end gets no valid rows) and item e is S tile e.
+template <bool kPair>
+TJ_DEV void chunk_at(const ScreenArgs& a, unsigned c, unsigned rank, unsigned& rtile, uint4& rt, unsigned& e0,
+                     unsigned& e1) {
+    if (!kPair) {
+        const uint4 ch = a.chunks[c];
+        rtile = ch.x;
+        rt = a.rtiles[ch.x];
+        e0 = ch.y;
+        e1 = ch.z;
+        return;
+    }
+    const unsigned t = c % a.nT, jc = c / a.nT;
+    e0 = jc * 64u;
+    e1 = min(e0 + 64u, a.ntS);
+    rtile = 2u * t + rank;
+    if (rtile < a.ntR) {
+        rt = a.rtiles[rtile];
+    } else {
+        const uint4 r0 = a.rtiles[2u * t];
+        rt = make_uint4(r0.x + (unsigned)kTileR, 0u, r0.z, r0.w);
+    }
+}
+
+// kFmt: 0 = fp16, 1 = bf16; kSplit: hi/lo operand limbs; kPair: CTA-pair MMA (cta_group::2, no split)
+template <int kFmt, int kSplit, bool kPair>
 __global__ void __launch_bounds__(kScreenThreads, 1)
     screen_tc_kernel(const __grid_constant__ TMaps tm, const ScreenArgs a) {
-    using Cfg = StageCfg<kSplit>;
+    using Cfg = typename StageSel<kSplit, kPair>::type;
     constexpr int kStages = Cfg::kStages;
     constexpr unsigned kStageBytes = Cfg::kBytes;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -188,6 +231,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
     ScreenCtl<kStages>* ctl = (ScreenCtl<kStages>*)(meta + kMetaSlots);
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long* status = &a.ctr->status;
+    const unsigned rank = kPair ? cluster_ctarank() : 0u;   // 0: the pair's MMA-issuing CTA
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -196,7 +240,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         }
         for (int b = 0; b < kAccBufs; ++b) {
             mbar_init(&ctl->acc_full[b], 1);
-            mbar_init(&ctl->acc_empty[b], kEpiWarps);
+            mbar_init(&ctl->acc_empty[b], kPair ? 2 * kEpiWarps : kEpiWarps);   // pair: both CTAs' warps
         }
         for (int m = 0; m < kMetaSlots; ++m) {
             mbar_init(&ctl->meta_full[m], 1);
@@ -210,12 +254,18 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             prefetch_tmap(&tm.b[c]);
         }
     }
-    if (warp == 1) tmem_alloc(&ctl->tmem_base, 512);
+    if (warp == 1) {
+        if (kPair) tmem_alloc_pair(&ctl->tmem_base, 512);
+        else tmem_alloc(&ctl->tmem_base, 512);
+    }
     tc_fence_before();
-    __syncthreads();
+    if (kPair) cluster_sync();   // the peer's barriers are initialised before any remote arrival
+    else __syncthreads();
     tc_fence_after();
     const unsigned tmem = ctl->tmem_base;
-    const unsigned nchunks = *a.nchunks;
+    const unsigned nchunks = kPair ? a.nT * ((a.ntS + 63u) / 64u) : *a.nchunks;
+    const unsigned cfirst = kPair ? (blockIdx.x >> 1) : blockIdx.x;
+    const unsigned cstride = kPair ? (gridDim.x >> 1) : gridDim.x;
 
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
@@ -223,18 +273,19 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             unsigned stage = 0, phase = 0;
             unsigned long long n = 0;   // items issued
             bool ok = true;
-            for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
-                const uint4 ch = a.chunks[c];
-                const uint4 rt = a.rtiles[ch.x];
+            for (unsigned c = cfirst; c < nchunks && ok; c += cstride) {
+                unsigned rtile, e0, e1;
+                uint4 rt;
+                chunk_at<kPair>(a, c, rank, rtile, rt, e0, e1);
                 const int rrow = (int)rt.x;
                 const unsigned cls = rt.w;
                 const int kblocks = a.cls[cls].kblocks, kpad = a.cls[cls].kpad, kbk = a.cls[cls].kbk;
                 const unsigned tx = a.cls[cls].tx_bytes;
                 const CUtensorMap* mA = &tm.a[cls];
                 const CUtensorMap* mB = &tm.b[cls];
-                for (unsigned e = ch.y; e < ch.z && ok; ++e, ++n) {
-                    const unsigned J = a.jlist[e];
-                    const int srow = (int)a.stiles[J].x;
+                for (unsigned e = e0; e < e1 && ok; ++e, ++n) {
+                    const unsigned J = kPair ? e : a.jlist[e];
+                    const int srow = (int)a.stiles[J].x + (int)(rank * kTileR);   // pair: this CTA's half
                     const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
                     if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status)) { ok = false; break; }
                     mbar_arrive_expect_tx(&ctl->meta_full[slot], (unsigned)sizeof(ColMetaF));
@@ -243,9 +294,16 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         uint8_t* sa = smem + (size_t)stage * kStageBytes;
-                        mbar_arrive_expect_tx(&ctl->full[stage], tx);
-                        tma_load_2d(sa, mA, &ctl->full[stage], kb * kbk, rrow);
-                        tma_load_2d(sa + Cfg::kBhi, mB, &ctl->full[stage], kb * kbk, srow);
+                        if (kPair) {   // both CTAs' copies complete on the MMA CTA's barrier
+                            const unsigned fb = mapa_shared(&ctl->full[stage], 0);
+                            if (rank == 0) mbar_arrive_expect_tx(&ctl->full[stage], 2 * tx);
+                            tma_load_2d_pair(sa, mA, fb, kb * kbk, rrow);
+                            tma_load_2d_pair(sa + Cfg::kBhi, mB, fb, kb * kbk, srow);
+                        } else {
+                            mbar_arrive_expect_tx(&ctl->full[stage], tx);
+                            tma_load_2d(sa, mA, &ctl->full[stage], kb * kbk, rrow);
+                            tma_load_2d(sa + Cfg::kBhi, mB, &ctl->full[stage], kb * kbk, srow);
+                        }
                         if (kSplit) {
                             tma_load_2d(sa + Cfg::kAlo, mA, &ctl->full[stage], kpad + kb * kbk, rrow);
                             tma_load_2d(sa + Cfg::kBlo, mB, &ctl->full[stage], kpad + kb * kbk, srow);
@@ -255,8 +313,10 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 }
             }
             if (!ok) ctl->abort_flag = 1;
-            // drain: the last copy issued into every stage / metadata slot must land before exit
-            for (int s = 0; s < kStages; ++s) {
+            // drain: the last copy issued into every stage / metadata slot must land before exit (in
+            // the pair the MMA CTA's barriers count both CTAs' copies; the final cluster barrier
+            // follows the last MMA, which consumed them)
+            for (int s = 0; s < kStages && rank == 0; ++s) {
                 const unsigned ph = ((unsigned)s < stage) ? phase : (phase ^ 1u);
                 mbar_wait(&ctl->full[s], ph, status, 1000000000ull);
             }
@@ -267,17 +327,21 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             }
         }
     } else if (warp == 1) {
-        // ------------------------------------------------------------ UMMA issuer
-        if (lane == 0) {
+        // ------------------------------------------------------------ UMMA issuer (pair: CTA 0 only)
+        if (lane == 0 && rank == 0) {
             unsigned stage = 0, phase = 0, acc = 0, acc_phase = 0;
             bool ok = true;
-            for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
-                const uint4 ch = a.chunks[c];
-                const ScreenClassArgs& ca = a.cls[a.rtiles[ch.x].w];
+            for (unsigned c = cfirst; c < nchunks && ok; c += cstride) {
+                unsigned rtile, e0, e1;
+                uint4 rt;
+                chunk_at<kPair>(a, c, 0u, rtile, rt, e0, e1);
+                const ScreenClassArgs& ca = a.cls[rt.w];
                 const int kblocks = ca.kblocks, ksteps = ca.kbk / 16;
                 const uint32_t dh = ca.desc_hi;
-                for (unsigned e = ch.y; e < ch.z && ok; ++e) {
-                    if (!mbar_wait(&ctl->acc_empty[acc], acc_phase ^ 1, status)) { ok = false; break; }
+                for (unsigned e = e0; e < e1 && ok; ++e) {
+                    const bool got = kPair ? mbar_wait_cluster(&ctl->acc_empty[acc], acc_phase ^ 1, status)
+                                           : mbar_wait(&ctl->acc_empty[acc], acc_phase ^ 1, status);
+                    if (!got) { ok = false; break; }
                     tc_fence_after();
                     const unsigned d_tmem = tmem + acc * kTileS;
                     for (int kb = 0; kb < kblocks; ++kb) {
@@ -290,22 +354,26 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                             if (k >= ksteps) break;
                             const uint64_t ad = desc_kmajor(sa, k * 32, dh);
                             const uint64_t bd = desc_kmajor(sa + Cfg::kBhi, k * 32, dh);
-                            umma_f16(d_tmem, ad, bd, a.idesc, (kb | k) != 0 ? 1u : 0u);
+                            if (kPair) umma_f16_pair(d_tmem, ad, bd, a.idesc_pair, (kb | k) != 0 ? 1u : 0u);
+                            else umma_f16(d_tmem, ad, bd, a.idesc, (kb | k) != 0 ? 1u : 0u);
                             if (kSplit) {   // z.w ~ hi.hi + hi.lo + lo.hi, one FP32 accumulator
                                 umma_f16(d_tmem, ad, desc_kmajor(sa + Cfg::kBlo, k * 32, dh), a.idesc, 1u);
                                 umma_f16(d_tmem, desc_kmajor(sa + Cfg::kAlo, k * 32, dh), bd, a.idesc, 1u);
                             }
                         }
-                        umma_commit(&ctl->empty[stage]);
+                        if (kPair) umma_commit_pair_mc(&ctl->empty[stage], 0x3);   // frees the stage in both CTAs
+                        else umma_commit(&ctl->empty[stage]);
                         if (++stage == kStages) { stage = 0; phase ^= 1; }
                     }
                     if (!ok) break;
-                    umma_commit(&ctl->acc_full[acc]);
+                    if (kPair) umma_commit_pair_mc(&ctl->acc_full[acc], 0x3);   // both CTAs' epilogues
+                    else umma_commit(&ctl->acc_full[acc]);
                     if (++acc == kAccBufs) { acc = 0; acc_phase ^= 1; }
                 }
             }
             if (!ok) ctl->abort_flag = 1;
-            umma_commit(&ctl->drain);
+            if (kPair) umma_commit_pair_mc(&ctl->drain, 0x1);
+            else umma_commit(&ctl->drain);
             mbar_wait(&ctl->drain, 0, status, 1000000000ull);
         }
     } else if (warp >= kEpiFirst) {
@@ -319,9 +387,10 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         unsigned acc = 0, acc_phase = 0;
         unsigned long long n = 0, n_screen_acc = 0, n_rare = 0, n_items = 0;
         bool ok = true;
-        for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
-            const uint4 ch = a.chunks[c];
-            const uint4 rt = a.rtiles[ch.x];
+        for (unsigned c = cfirst; c < nchunks && ok; c += cstride) {
+            unsigned rtile, e0, e1;
+            uint4 rt;
+            chunk_at<kPair>(a, c, rank, rtile, rt, e0, e1);
             const ScreenClassArgs& ca = a.cls[rt.w];
             const JoinParams& jp = a.jps[rt.z];   // read through L1 where used
             const unsigned r0 = rt.x;
@@ -333,7 +402,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             const float Ei = rvalid ? ca.r_en[rs] : 0.f;
             const float Zli = rvalid ? ca.r_zl[rs] : 0.f;
             const uint32_t oi = rvalid ? ca.r_emit[rs] : 0u;
-            for (unsigned e = ch.y; e < ch.z; ++e, ++n) {
+            for (unsigned e = e0; e < e1; ++e, ++n) {
                 const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
                 if (!mbar_wait(&ctl->meta_full[slot], mph, status) ||
                     !mbar_wait(&ctl->acc_full[acc], acc_phase, status)) { ok = false; break; }
@@ -368,12 +437,15 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         float* out = a.dump + (slotd * kTileR + row) * kTileS + col0;
 #pragma unroll
                         for (int k = 0; k < 32; ++k) out[k] = __uint_as_float(raw[k]);
-                        if (row == 0 && cb == 0) a.dump_ids[slotd] = make_uint4(ch.x, a.jlist[e], 1u, 0u);
+                        if (row == 0 && cb == 0) a.dump_ids[slotd] = make_uint4(rtile, a.jlist[e], 1u, 0u);
                     }
                     if (cb == cb_end - 1) {   // this warp's part read: hand it back
                         tc_fence_before();
                         __syncwarp();
-                        if (lane == 0) mbar_arrive(&ctl->acc_empty[acc]);
+                        if (lane == 0) {
+                            if (kPair) mbar_arrive_cluster(mapa_shared(&ctl->acc_empty[acc], 0));
+                            else mbar_arrive(&ctl->acc_empty[acc]);
+                        }
                     }
                     // fast path: v = fma(-2, p, B~) two pairs per packed FMA, folded by three-input mins
                     // (one instruction per pair), one min chain per 8-column group; only the groups whose
@@ -483,9 +555,13 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         }
     }
     tc_fence_before();
-    __syncthreads();
+    if (kPair) cluster_sync();   // the pair's last MMA (which read both CTAs' stages) has completed
+    else __syncthreads();
     tc_fence_after();
-    if (warp == 1) tmem_dealloc(tmem, 512);
+    if (warp == 1) {
+        if (kPair) tmem_dealloc_pair(tmem, 512);
+        else tmem_dealloc(tmem, 512);
+    }
 }
 
 // Screen error of the sampled tile pairs: |d2hat - d2| with d2hat = A + B - 2p from the dumped
@@ -587,6 +663,17 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     memset(&tm, 0, sizeof(tm));
     ScreenArgs a;
     memset(&a, 0, sizeof(a));
+    // CTA-pair screen (cta_group::2): one join, no split, rows of at least 256 elements (MMA-bound)
+    // and every tile pair a candidate (checked on the device count: one 4-byte read-back)
+    bool pair = g.allow_pair && g.ncls == 1 && g.njoins == 1 && !split && !g.dump && !g.jp0.self_join &&
+                g.R[0]->kpad >= 256 && g.tR[0]->ntiles > 0 && g.tS[0]->ntiles > 0;
+    if (pair) {
+        uint32_t tot = 0;
+        TJ_CUDA(cudaMemcpyAsync(&tot, g.cand->dev_counts.p, sizeof(tot), cudaMemcpyDeviceToHost, st));
+        TJ_CUDA(cudaStreamSynchronize(st));
+        pair = (unsigned long long)tot == (unsigned long long)g.tR[0]->ntiles * (unsigned long long)g.tS[0]->ntiles;
+    }
+    g.used_pair = pair;
     DBuf<ColMetaF> smeta((size_t)std::max(g.ntS_total, 1), st);
     for (int c = 0; c < g.ncls; ++c) {
         const Side& R = *g.R[c];
@@ -599,7 +686,7 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
         const int kbk = std::min(R.kpad, kBK);
         if (kbk != 16 && kbk != 32 && kbk != 64) fail(-1, "screen_tc: operand width");
         make_tmap_2d(&tm.a[c], R.op.p, R.rows_pad, w, 2, kTileR, dt, 2 * kbk);
-        make_tmap_2d(&tm.b[c], S.op.p, S.rows_pad, w, 2, kTileS, dt, 2 * kbk);
+        make_tmap_2d(&tm.b[c], S.op.p, S.rows_pad, w, 2, pair ? kTileR : kTileS, dt, 2 * kbk);
         const TileSet& tS = *g.tS[c];
         if (tS.ntiles > 0)
             launch(build_col_meta, tS.ntiles, kTileS, 0, st, tS.row0.p, tS.nvalid.p, S.emit, S.nrm2.p, S.nrm2f.p,
@@ -613,7 +700,8 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
         a.cls[c].kblocks = R.kpad / kbk;
         a.cls[c].kpad = R.kpad;
         a.cls[c].kbk = kbk;
-        a.cls[c].tx_bytes = (unsigned)((split ? 2 : 1) * (kTileR + kTileS) * kbk * 2);
+        a.cls[c].tx_bytes = pair ? (unsigned)(2 * kTileR * kbk * 2)   // this CTA's A rows + B half
+                                 : (unsigned)((split ? 2 : 1) * (kTileR + kTileS) * kbk * 2);
         a.cls[c].desc_hi = desc_hi_for_rows(2u * (unsigned)kbk);
     }
     a.chunks = g.cand->chunks.p;
@@ -625,6 +713,10 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     a.jps = g.jps;
     a.ncls = g.ncls;
     a.idesc = make_idesc(1u, bf ? 1u : 0u, kTileR, kTileS);
+    a.idesc_pair = make_idesc(1u, bf ? 1u : 0u, 2 * kTileR, kTileS);
+    a.ntR = (unsigned)g.tR[0]->ntiles;
+    a.ntS = (unsigned)g.tS[0]->ntiles;
+    a.nT = (a.ntR + 1) / 2;
     a.acc = eb.acc;
     a.acc_cap = eb.acc_cap;
     a.band = eb.band;
@@ -635,13 +727,36 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     a.dump_every = g.dump_every ? g.dump_every : 1u;
     a.dump_items = g.dump ? g.dump_items : 0u;
     const int grid = num_sms();
-#define TJ_SCREEN(F, SP)                                                                                    \
-    do {                                                                                                    \
-        TJ_CUDA(cudaFuncSetAttribute(screen_tc_kernel<F, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                     (int)screen_smem<SP>()));                                              \
-        launch(screen_tc_kernel<F, SP>, grid, kScreenThreads, screen_smem<SP>(), st, tm, a);                \
+#define TJ_SCREEN(F, SP)                                                                                      \
+    do {                                                                                                      \
+        TJ_CUDA(cudaFuncSetAttribute(screen_tc_kernel<F, SP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                     (int)screen_smem<SP, false>()));                                         \
+        launch(screen_tc_kernel<F, SP, false>, grid, kScreenThreads, screen_smem<SP, false>(), st, tm, a);   \
     } while (0)
-    if (bf && split) TJ_SCREEN(1, 1);
+    if (pair) {
+        auto kern = bf ? screen_tc_kernel<1, 0, true> : screen_tc_kernel<0, 0, true>;
+        const size_t smem = screen_smem<0, true>();
+        TJ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        cudaLaunchConfig_t cfg;
+        memset(&cfg, 0, sizeof(cfg));
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.blockDim = dim3(kScreenThreads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cfg.gridDim = dim3((unsigned)(grid & ~1));
+        int nclusters = 0;
+        TJ_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg));
+        if (nclusters < 1) fail(-2, "screen_tc: no CTA pair fits on the device");
+        cfg.gridDim = dim3((unsigned)(2 * std::min(nclusters, grid / 2)));
+        count_launch();
+        TJ_CUDA(cudaLaunchKernelEx(&cfg, kern, tm, a));
+    } else if (bf && split) TJ_SCREEN(1, 1);
     else if (bf) TJ_SCREEN(1, 0);
     else if (split) TJ_SCREEN(0, 1);
     else TJ_SCREEN(0, 0);

@@ -421,3 +421,23 @@ def test_concurrent_host_threads():
     assert not errs, errs
     for k in (0, 1):
         assert_same(out[k], want[k], f"thread {k}")
+
+
+@pytest.mark.parametrize("screen", ["fp16", "bf16"])
+@pytest.mark.parametrize("shape", [(2000, 1500, 512), (300, 700, 256), (1100, 257, 320)])
+def test_cta_pair_screen(screen, shape):
+    """The CTA-pair screen (cta_group::2, 256 x 256 tiles over two SMs) gives the oracle's pairs,
+    including an odd number of 128-row R tiles and S sides that are not a multiple of 256 rows."""
+    nr, ns, d = shape
+    rng = np.random.default_rng(nr + ns + d)
+    R = (rng.standard_normal((nr, d)) / np.sqrt(d)).astype(np.float32)
+    S = (rng.standard_normal((ns, d)) / np.sqrt(d)).astype(np.float32)
+    T = float(np.quantile(((R[:60, None, :].astype(np.float64) - S[None, :300, :]) ** 2).sum(-1), 0.01))
+    want = oracle_keys(R, S, T, "rs")
+    Rt, St = torch.from_numpy(R).cuda(), torch.from_numpy(S).cuda()
+    res = tj.join_result(Rt, St, eps2=T, screen=screen)
+    assert res.stats["screen_pair"] == 1, res.stats
+    assert_same(res.keys().cpu().numpy().view(np.uint64), want, f"pair {screen} {shape}")
+    one = tj.join_result(Rt, St, eps2=T, screen=screen, cta_pair=False)
+    assert one.stats["screen_pair"] == 0
+    assert_same(one.keys().cpu().numpy().view(np.uint64), want, f"one-SM {screen} {shape}")
