@@ -124,6 +124,17 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
 
 
+def max_over_ranks(x: float, world: int, dist, device: str = "cuda") -> float:
+    """The largest of every rank's `x` (all ranks call this at the same point)."""
+    if world <= 1:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -258,10 +269,8 @@ def main() -> None:
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1) / args.steps
     step_ms = [(ev0 if k == 0 else marks[k - 1]).elapsed_time(marks[k]) for k in range(args.steps)]
+    ms = max_over_ranks(ms, world, dist)
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     st = stats[-1]
     pairs = st["pairs_screened"]
@@ -352,10 +361,7 @@ def main() -> None:
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1) / k_e2e
-        if world > 1:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(ems, world, dist)
         h2d = Rh.numel() * Rh.element_size() + (0 if Sh is None else Sh.numel() * Sh.element_size())
         line["e2e"] = {"value": world * pairs / (ems / 1000.0), "unit": UNIT, "ms_per_step": ems,
                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(16 * len(ih)),
@@ -463,10 +469,7 @@ def ragged_bench(args, rank, world, screen, dist):
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / args.steps
     step_ms = [(e0 if k == 0 else marks[k - 1]).elapsed_time(marks[k]) for k in range(args.steps)]
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, dist)
     st = stats[-1]
     pairs = st["pairs_screened"]
     peaks = measured_peaks()
@@ -519,6 +522,9 @@ def ragged_bench(args, rank, world, screen, dist):
         line["plain_gpu"] = {"ms_per_step": a.elapsed_time(b), "speedup_of_tc_path": a.elapsed_time(b) / ms,
                              "identical_pair_set": same}
         del rp, r
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
