@@ -43,7 +43,7 @@ namespace tj {
 
 namespace {
 
-constexpr int kAccBufs = 2;
+constexpr int kAccMax = 4;   // TMEM accumulators: one-SM kernel 4 x 128 columns, CTA pair 2 x 256
 constexpr int kEpiWarps = 12;                       // three per TMEM lane quarter (column thirds)
 constexpr int kEpiFirst = 4;                         // warps 0-3: TMA producer, UMMA issuer, two idle
 constexpr int kScreenThreads = (kEpiFirst + kEpiWarps) * 32;
@@ -79,8 +79,8 @@ template <int kStages>
 struct ScreenCtl {
     uint64_t full[kStages];
     uint64_t empty[kStages];
-    uint64_t acc_full[kAccBufs];
-    uint64_t acc_empty[kAccBufs];
+    uint64_t acc_full[kAccMax];
+    uint64_t acc_empty[kAccMax];
     uint64_t meta_full[kMetaSlots];
     uint64_t meta_empty[kMetaSlots];
     uint64_t drain;
@@ -238,13 +238,14 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             mbar_init(&ctl->full[s], 1);
             mbar_init(&ctl->empty[s], 1);
         }
-        for (int b = 0; b < kAccBufs; ++b) {
+        for (int b = 0; b < kAccMax; ++b) {
             mbar_init(&ctl->acc_full[b], 1);
-            mbar_init(&ctl->acc_empty[b], kPair ? 2 * kEpiWarps : kEpiWarps);   // pair: both CTAs' warps
+            // pair: the 12 epilogue warps of both CTAs; one SM: the 4 warps of one epilogue group
+            mbar_init(&ctl->acc_empty[b], kPair ? 2 * kEpiWarps : 4);
         }
         for (int m = 0; m < kMetaSlots; ++m) {
             mbar_init(&ctl->meta_full[m], 1);
-            mbar_init(&ctl->meta_empty[m], kEpiWarps);
+            mbar_init(&ctl->meta_empty[m], kPair ? kEpiWarps : 8);   // one SM: the two groups of an item
         }
         mbar_init(&ctl->drain, 1);
         ctl->abort_flag = 0;
@@ -330,6 +331,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         // ------------------------------------------------------------ UMMA issuer (pair: CTA 0 only)
         if (lane == 0 && rank == 0) {
             unsigned stage = 0, phase = 0, acc = 0, acc_phase = 0;
+            unsigned long long n_mma = 0;   // items issued
             bool ok = true;
             for (unsigned c = cfirst; c < nchunks && ok; c += cstride) {
                 unsigned rtile, e0, e1;
@@ -338,12 +340,21 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 const ScreenClassArgs& ca = a.cls[rt.w];
                 const int kblocks = ca.kblocks, ksteps = ca.kbk / 16;
                 const uint32_t dh = ca.desc_hi;
-                for (unsigned e = e0; e < e1 && ok; ++e) {
-                    const bool got = kPair ? mbar_wait_cluster(&ctl->acc_empty[acc], acc_phase ^ 1, status)
-                                           : mbar_wait(&ctl->acc_empty[acc], acc_phase ^ 1, status);
+                for (unsigned e = e0; e < e1 && ok; ++e, ++n_mma) {
+                    // one SM: item n fills accumulators 2n mod 4 and 2n+1 mod 4 (its two 128-column halves)
+                    const unsigned b0 = kPair ? acc : (unsigned)((2 * n_mma) & 3), b1 = (b0 + 1) & 3;
+                    bool got;
+                    if (kPair) {
+                        got = mbar_wait_cluster(&ctl->acc_empty[acc], acc_phase ^ 1, status);
+                    } else {
+                        got = mbar_wait(&ctl->acc_empty[b0], (unsigned)(((2 * n_mma) >> 2) & 1) ^ 1u, status) &&
+                              mbar_wait(&ctl->acc_empty[b1], (unsigned)(((2 * n_mma + 1) >> 2) & 1) ^ 1u, status);
+                    }
                     if (!got) { ok = false; break; }
                     tc_fence_after();
-                    const unsigned d_tmem = tmem + acc * kTileS;
+                    const unsigned d_tmem = tmem + acc * kTileS;                 // pair: 256 columns
+                    const unsigned d0 = tmem + b0 * 128u, d1 = tmem + b1 * 128u;  // one SM: 2 x 128
+                    const unsigned bhalf = 256u * (unsigned)ca.kbk;              // bytes of 128 B rows
                     for (int kb = 0; kb < kblocks; ++kb) {
                         if (!mbar_wait(&ctl->full[stage], phase, status)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
@@ -352,13 +363,22 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
 #pragma unroll
                         for (int k = 0; k < kBK / 16; ++k) {
                             if (k >= ksteps) break;
+                            const unsigned accum = (kb | k) != 0 ? 1u : 0u;
                             const uint64_t ad = desc_kmajor(sa, k * 32, dh);
-                            const uint64_t bd = desc_kmajor(sa + Cfg::kBhi, k * 32, dh);
-                            if (kPair) umma_f16_pair(d_tmem, ad, bd, a.idesc_pair, (kb | k) != 0 ? 1u : 0u);
-                            else umma_f16(d_tmem, ad, bd, a.idesc, (kb | k) != 0 ? 1u : 0u);
-                            if (kSplit) {   // z.w ~ hi.hi + hi.lo + lo.hi, one FP32 accumulator
-                                umma_f16(d_tmem, ad, desc_kmajor(sa + Cfg::kBlo, k * 32, dh), a.idesc, 1u);
-                                umma_f16(d_tmem, desc_kmajor(sa + Cfg::kAlo, k * 32, dh), bd, a.idesc, 1u);
+                            if (kPair) {
+                                umma_f16_pair(d_tmem, ad, desc_kmajor(sa + Cfg::kBhi, k * 32, dh), a.idesc_pair, accum);
+                            } else {
+#pragma unroll
+                                for (int h = 0; h < 2; ++h) {
+                                    const unsigned dd = h ? d1 : d0;
+                                    const uint64_t bd = desc_kmajor(sa + Cfg::kBhi + h * bhalf, k * 32, dh);
+                                    umma_f16(dd, ad, bd, a.idesc, accum);
+                                    if (kSplit) {   // z.w ~ hi.hi + hi.lo + lo.hi, one FP32 accumulator
+                                        umma_f16(dd, ad, desc_kmajor(sa + Cfg::kBlo + h * bhalf, k * 32, dh), a.idesc,
+                                                 1u);
+                                        umma_f16(dd, desc_kmajor(sa + Cfg::kAlo, k * 32, dh), bd, a.idesc, 1u);
+                                    }
+                                }
                             }
                         }
                         if (kPair) umma_commit_pair_mc(&ctl->empty[stage], 0x3);   // frees the stage in both CTAs
@@ -366,11 +386,16 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         if (++stage == kStages) { stage = 0; phase ^= 1; }
                     }
                     if (!ok) break;
-                    if (kPair) umma_commit_pair_mc(&ctl->acc_full[acc], 0x3);   // both CTAs' epilogues
-                    else umma_commit(&ctl->acc_full[acc]);
-                    if (++acc == kAccBufs) { acc = 0; acc_phase ^= 1; }
+                    if (kPair) {
+                        umma_commit_pair_mc(&ctl->acc_full[acc], 0x3);   // both CTAs' epilogues
+                        if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+                    } else {
+                        umma_commit(&ctl->acc_full[b0]);
+                        umma_commit(&ctl->acc_full[b1]);
+                    }
                 }
             }
+            if (!kPair && n_mma) atomicAdd(&a.ctr->items, n_mma);
             if (!ok) ctl->abort_flag = 1;
             if (kPair) umma_commit_pair_mc(&ctl->drain, 0x1);
             else umma_commit(&ctl->drain);
@@ -379,10 +404,13 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
     } else if (warp >= kEpiFirst) {
         // ------------------------------------------------------------ epilogue
         const unsigned q = warp & 3;                 // TMEM lane quarter of this warp
-        const unsigned part = (warp - kEpiFirst) >> 2;   // accumulator column third of this warp
+        const unsigned part = (warp - kEpiFirst) >> 2;   // pair: column third; one SM: epilogue group
         const unsigned row = q * 32 + lane;              // R row within the tile
-        // 32-column blocks of the 256-column accumulator: thirds [0, 3), [3, 6), [6, 8)
-        const int cb_begin = (int)part * 3, cb_end = part == 2 ? kTileS / 32 : (int)part * 3 + 3;
+        // pair: 32-column blocks of the 256-column accumulator, thirds [0, 3), [3, 6), [6, 8);
+        // one SM: all four blocks of a 128-column half-item (sub-item s = 2 item + half, taken by
+        // group s mod 3, accumulator s mod 4)
+        const int cb_begin = kPair ? (int)part * 3 : 0;
+        const int cb_end = kPair ? (part == 2 ? kTileS / 32 : (int)part * 3 + 3) : 4;
         WarpAppender app_acc, app_band;
         unsigned acc = 0, acc_phase = 0;
         unsigned long long n = 0, n_screen_acc = 0, n_rare = 0, n_items = 0;
@@ -402,10 +430,19 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             const float Ei = rvalid ? ca.r_en[rs] : 0.f;
             const float Zli = rvalid ? ca.r_zl[rs] : 0.f;
             const uint32_t oi = rvalid ? ca.r_emit[rs] : 0u;
-            for (unsigned e = e0; e < e1; ++e, ++n) {
+            for (unsigned e = e0; e < e1 && ok; ++e, ++n) {
+              for (unsigned h = 0; h < (kPair ? 1u : 2u); ++h) {
+                unsigned colbase = 0, b = acc, bph = acc_phase;
+                if (!kPair) {
+                    const unsigned long long sub = 2 * n + h;
+                    if ((unsigned)(sub % 3) != part) continue;
+                    colbase = h * 128u;
+                    b = (unsigned)(sub & 3);
+                    bph = (unsigned)((sub >> 2) & 1);
+                }
                 const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
                 if (!mbar_wait(&ctl->meta_full[slot], mph, status) ||
-                    !mbar_wait(&ctl->acc_full[acc], acc_phase, status)) { ok = false; break; }
+                    !mbar_wait(&ctl->acc_full[b], bph, status)) { ok = false; break; }
                 tc_fence_after();
                 const ColMetaF& m = meta[slot];
                 const unsigned c0 = m.c0;
@@ -425,26 +462,26 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     const double ti = jp.Tm - Ai - slack * (1.0 + 0x1p-40) - 0x1p-50 * (jp.Tm + Ai) - 0x1p-1000;
                     tau_in = f32_dn(ti);
                 }
-                const unsigned tbase = tmem + ((q * 32u) << 16) + acc * kTileS;
+                const unsigned tbase = tmem + ((q * 32u) << 16) + (kPair ? b * kTileS : b * 128u);
 #pragma unroll 1
                 for (int cb = cb_begin; cb < cb_end; ++cb) {
-                    const int col0 = cb * 32;
+                    const int col0 = (int)colbase + cb * 32;   // column of the S tile
                     uint32_t raw[32];
-                    tmem_ld32(tbase + col0, raw);
+                    tmem_ld32(tbase + cb * 32, raw);
                     tmem_ld_wait();
                     if (a.dump && e % a.dump_every == 0 && e / a.dump_every < a.dump_items) {
                         const size_t slotd = e / a.dump_every;
                         float* out = a.dump + (slotd * kTileR + row) * kTileS + col0;
 #pragma unroll
                         for (int k = 0; k < 32; ++k) out[k] = __uint_as_float(raw[k]);
-                        if (row == 0 && cb == 0) a.dump_ids[slotd] = make_uint4(rtile, a.jlist[e], 1u, 0u);
+                        if (row == 0 && col0 == 0) a.dump_ids[slotd] = make_uint4(rtile, a.jlist[e], 1u, 0u);
                     }
                     if (cb == cb_end - 1) {   // this warp's part read: hand it back
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) {
-                            if (kPair) mbar_arrive_cluster(mapa_shared(&ctl->acc_empty[acc], 0));
-                            else mbar_arrive(&ctl->acc_empty[acc]);
+                            if (kPair) mbar_arrive_cluster(mapa_shared(&ctl->acc_empty[b], 0));
+                            else mbar_arrive(&ctl->acc_empty[b]);
                         }
                     }
                     // fast path: v = fma(-2, p, B~) two pairs per packed FMA, folded by three-input mins
@@ -535,7 +572,8 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&ctl->meta_empty[slot]);   // this warp is done with the slot
                 ++n_items;
-                if (++acc == kAccBufs) { acc = 0; acc_phase ^= 1; }
+                if (kPair && ++acc == 2) { acc = 0; acc_phase ^= 1; }
+              }
             }
         }
         if (!ok) ctl->abort_flag = 1;
@@ -551,7 +589,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             if (app_band.valid) atomicAdd(&a.ctr->band_valid, app_band.valid);
             if (n_screen_acc) atomicAdd(&a.ctr->screen_accept, n_screen_acc);
             if (n_rare) atomicAdd(&a.ctr->rare_checks, n_rare);
-            if (warp == kEpiFirst && n_items) atomicAdd(&a.ctr->items, n_items);
+            if (kPair && warp == kEpiFirst && n_items) atomicAdd(&a.ctr->items, n_items);
         }
     }
     tc_fence_before();
@@ -712,7 +750,7 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     a.s_meta = smeta.p;
     a.jps = g.jps;
     a.ncls = g.ncls;
-    a.idesc = make_idesc(1u, bf ? 1u : 0u, kTileR, kTileS);
+    a.idesc = make_idesc(1u, bf ? 1u : 0u, kTileR, 128u);   // one SM: 128-column half-items
     a.idesc_pair = make_idesc(1u, bf ? 1u : 0u, 2 * kTileR, kTileS);
     a.ntR = (unsigned)g.tR[0]->ntiles;
     a.ntS = (unsigned)g.tS[0]->ntiles;
