@@ -254,6 +254,8 @@ __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kp
             op8[(size_t)r * (2 * kpad) + kpad + k] = (int8_t)l;
             sq += (long long)q * q;
             sx += (double)x * x;
+            sz += (double)(h * h);   // |h|^2 and |l|^2 exactly (small integers): zn, zl bound the limb norms
+            sl += (double)(l * l);
         } else {
             constexpr int kFmt = (kScreen == kScreenBF16 || kScreen == kScreenBF16X3) ? 1 : 0;
             const double xc = (k < d && real) ? (double)x - (double)center[k] : 0.0;

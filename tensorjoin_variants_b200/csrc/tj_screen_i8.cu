@@ -11,11 +11,15 @@
 // (src/g9_tc_kernels.py:45-66 limb_dot; NUMERICS_G9_INT14.md:5-18), applied to the
 // whole screen instead of a refinement subset.
 //
-// Fast path: q.q' <= 16384 hh + M with M = 128 max|x| + max|ll| = d (128 * 8192 + 4096),
-// so a pair is certainly out when 32768 hh + 2M < |q|^2 + |q'|^2 - T.  With
-// a_i = floor((|q_i|^2 - T - 2M) / 2^15) and b_j = floor(|q_j|^2 / 2^15) this becomes the
-// integer test  hh - b_j < a_i  (two INT32 ops per pair).  Pairs failing it read x and ll
-// and take the exact INT64 test.
+// Fast path: q.q' <= 16384 hh + M with M >= |128 x + ll|.  By Cauchy-Schwarz on the limb vectors,
+// |x| <= |h||l'| + |l||h'| and |ll| <= |l||l'|, so per (row i, S tile J)
+//     M_iJ = 128 (|h_i| L_J + |l_i| H_J) + |l_i| L_J,   H_J, L_J = tile maxima of |h'|, |l'|
+// (FP32 upper bounds of the norms, the sum taken in FP64 and rounded up to an integer), and a pair
+// is certainly out when 32768 hh + 2 M_iJ < |q|^2 + |q'|^2 - T.  With
+// a_iJ = floor((|q_i|^2 - T - 2 M_iJ) / 2^15) and b_j = floor(|q_j|^2 / 2^15) this is the integer
+// test  hh - b_j < a_iJ  (two INT32 ops per pair).  Pairs failing it read x and ll and take the
+// exact INT64 test.  (The data-independent bound M = d (128 * 8192 + 4096) is ~3x looser on
+// uniform int14 rows and sent ~10x more pairs to the exact test.)
 //
 // TMEM: hh double-buffered (columns 0..255), x and ll single (256..511).  The UMMA
 // issuer runs the hh products of item n+1 while the epilogue still reads x / ll of item n.
@@ -47,7 +51,8 @@ struct ColMetaI8 {
     int bq[kI8N];           // floor(|q_j|^2 / 2^15); 2^30 for rows beyond the tile's points
     uint32_t perm[kI8N];    // original row id
     long long norm[kI8N];   // exact |q_j|^2
-    uint32_t c0, nvJ, pad0, pad1;
+    uint32_t c0, nvJ;
+    float HJ, LJ;           // >= max |h'|, max |l'| over the tile's rows
 };
 static_assert(sizeof(ColMetaI8) % 16 == 0, "bulk copies need 16-byte multiples");
 
@@ -74,13 +79,14 @@ struct I8Args {
     const uint32_t* r_nvalid;
     const uint32_t* r_perm;
     const long long* r_norm;   // exact |q|^2
+    const float* r_hn;         // >= |h| per row
+    const float* r_ln;         // >= |l| per row
     const uint32_t* s_row0;
     const ColMetaI8* s_meta;
     int kblocks;               // kpad / 128
     int kpad;
     unsigned idesc;
     long long T;               // integer threshold
-    long long twoM;            // 2 * bound on |128 x + ll|
     JoinParams jp;
     uint64_t* acc;
     unsigned long long acc_cap;
@@ -105,7 +111,7 @@ TJ_DEV uint32_t pick32(const uint32_t (&r)[32], int k) {
 
 __global__ void __launch_bounds__(kI8N) build_col_meta_i8(const uint32_t* row0, const uint32_t* nvalid,
                                                          const uint32_t* perm, const long long* norm,
-                                                         ColMetaI8* out) {
+                                                         const float* maxH, const float* maxL, ColMetaI8* out) {
     const unsigned J = blockIdx.x, t = threadIdx.x;
     const unsigned c0 = row0[J], nv = nvalid[J];
     ColMetaI8& m = out[J];
@@ -113,7 +119,7 @@ __global__ void __launch_bounds__(kI8N) build_col_meta_i8(const uint32_t* row0, 
     m.bq[t] = ok ? floor_shift15(norm[c0 + t]) : 0x40000000;
     m.perm[t] = ok ? perm[c0 + t] : 0u;
     m.norm[t] = ok ? norm[c0 + t] : 0ll;
-    if (t == 0) { m.c0 = c0; m.nvJ = nv; m.pad0 = m.pad1 = 0; }
+    if (t == 0) { m.c0 = c0; m.nvJ = nv; m.HJ = maxH[J]; m.LJ = maxL[J]; }
 }
 
 __global__ void __launch_bounds__(kI8Threads, 1)
@@ -251,7 +257,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             const bool rvalid = row < a.r_nvalid[I];
             const unsigned rs = r0 + row;
             const long long Ai = rvalid ? a.r_norm[rs] : 0;
-            const int ai = rvalid ? floor_shift15(Ai - a.T - a.twoM) : 0x7FFFFFFF;
+            const double hi_n = rvalid ? (double)a.r_hn[rs] : 0.0, li_n = rvalid ? (double)a.r_ln[rs] : 0.0;
             const uint32_t oi = rvalid ? a.r_perm[rs] : 0u;
             for (unsigned e = ch.y; e < ch.z; ++e, ++n) {
                 const unsigned b = (unsigned)(n & 1);
@@ -261,6 +267,15 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                 tc_fence_after();
                 const ColMetaI8& m = meta[slot];
                 const unsigned c0 = m.c0;
+                // a_iJ with M_iJ >= |128 x + ll| for this row and S tile (every term non-negative;
+                // the 2^-40 factor and +2 cover the FP64 rounding of the sum and of the ceil)
+                int ai = 0x7FFFFFFF;
+                if (rvalid) {
+                    const double HJ = m.HJ, LJ = m.LJ;
+                    const double Md = (128.0 * (hi_n * LJ + li_n * HJ) + li_n * LJ) * (1.0 + 0x1p-40) + 2.0;
+                    const long long M = (long long)ceil(Md);
+                    ai = floor_shift15(Ai - a.T - 2 * M);
+                }
                 const unsigned lane_off = (q * 32u) << 16;
                 const unsigned col0 = half * 64;
 #pragma unroll 1
@@ -386,17 +401,19 @@ void screen_i8(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     a.r_nvalid = g.tR[0]->nvalid.p;
     a.r_perm = R.emit;
     a.r_norm = R.inorm.p;
+    a.r_hn = R.zn.p;   // the int8-limb preparation stores |h| and |l| upper bounds in zn / zl
+    a.r_ln = R.zl.p;
     const TileSet& tS = *g.tS[0];
     DBuf<ColMetaI8> smeta((size_t)std::max(tS.ntiles, 1), st);
     if (tS.ntiles > 0)
-        launch(build_col_meta_i8, tS.ntiles, kI8N, 0, st, tS.row0.p, tS.nvalid.p, S.emit, S.inorm.p, smeta.p);
+        launch(build_col_meta_i8, tS.ntiles, kI8N, 0, st, tS.row0.p, tS.nvalid.p, S.emit, S.inorm.p, tS.maxZ.p,
+               tS.maxZl.p, smeta.p);
     a.s_row0 = tS.row0.p;
     a.s_meta = smeta.p;
     a.kblocks = R.kpad / 128;
     a.kpad = R.kpad;
     a.idesc = make_idesc(2u, 1u, 128, kI8N);
     a.T = g.T_int;
-    a.twoM = 2ll * (long long)R.kpad * (128ll * 8192ll + 4096ll);
     a.jp = g.jp0;
     a.acc = eb.acc;
     a.acc_cap = eb.acc_cap;
