@@ -17,21 +17,31 @@
 // premise; here the kernel owns its accumulation, so the premise is stated for
 // tcgen05 and checked by the screen-error diagnostics.
 //
-// Fast path (every pair): v = fma(-2, p, B~_j) in FP32 and one compare against a
-// per-(row, S tile) threshold tau_i that absorbs every error term; v > tau_i
-// proves the FP64 oracle value exceeds T.  The rare remainder gets a per-pair FP64
-// certificate: accept (emit), reject, or band (queued for the FP64 refinement
-// that reproduces the oracle's summation order).
+// Fast path (every pair): v = fma(-2, p, B~_j) in FP32 (two pairs per packed FP32x2 FMA) folded by
+// three-input mins per 8-column group, and one compare of each group minimum against a
+// per-(row, S tile) threshold tau_i that absorbs every error term; v > tau_i proves the FP64
+// oracle value exceeds T.  Groups that pass get per-pair masks: certified FP32 accept, else a
+// per-pair FP64 certificate: accept (emit), reject, or band (queued for the FP64 refinement that
+// reproduces the oracle's summation order).
 //
-// Warp roles (512 threads, one CTA per SM, persistent over the chunk list):
-//   warp 0: TMA producer (one lane): a ring of k-block stages {A 128 rows, B 256 rows} and a
-//           ring of per-item column-metadata blocks (one 8 KB bulk copy per S tile), so the
-//           epilogue never waits on global memory inside an item
-//   warp 1: TMEM allocator + UMMA issuer (one lane), 2 accumulators x 256 columns
-//   warps 4-15: epilogue, warp w reads TMEM lanes 32*(w%4) .. +31 (one R row per thread) and one
-//           third of the accumulator's columns (blocks of 32: [0,3), [3,6), [6,8) for (w-4)/4 = 0,1,2),
-//           so every SM sub-partition runs three epilogue warps that hide each other's latency; the
-//           twelve warps run independently (no named barrier), synchronised only through mbarriers
+// Two forms of the same kernel (512 threads, one CTA per SM, persistent over the chunk list):
+//   one SM (kPair = false): an item is a 128-row R tile x 256-row S tile, issued as two 128-column
+//           half-items (M = 128, N = 128 UMMA) into four TMEM accumulators of 128 columns; half-item
+//           s = 2 item + h goes to accumulator s mod 4 and to epilogue group s mod 3, so the three
+//           groups work on different half-items at once and the MMA can run up to two items ahead
+//   CTA pair (kPair = true, cta_group::2, clusters of 2 SMs, dense single joins with rows of
+//           >= 256 elements): an item is a 256 x 256 tile; each CTA loads its 128 A rows and its
+//           128-row half of B, CTA 0 issues M = 256 UMMAs into both CTAs' TMEM (2 accumulators of
+//           256 columns), stage and accumulator barriers are signalled to both CTAs (tcgen05.commit
+//           multicast) and the epilogue warps of both CTAs release accumulators on CTA 0's barrier
+//
+// Warp roles:
+//   warp 0: TMA producer (one lane): a ring of k-block stages and a ring of per-item column-metadata
+//           blocks (one 8 KB bulk copy per S tile), so the epilogue never waits on global memory
+//   warp 1: TMEM allocator + UMMA issuer (one lane; in the pair, CTA 0's)
+//   warps 4-15: epilogue, warp w reads TMEM lanes 32*(w%4) .. +31 (one R row per thread); one SM:
+//           group (w-4)/4 takes whole half-items (4 blocks of 32 columns); pair: column thirds of every
+//           item (blocks [0,3), [3,6), [6,8)).  Warps synchronise only through mbarriers.
 //   warps 2-3: idle (they complete the first warpgroup)
 #include <algorithm>
 #include <cstring>
