@@ -311,6 +311,11 @@ def main() -> None:
             "result_pairs", "retries", "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total")},
     }
     line["stats"]["refined_fraction"] = st["band"] / max(1, st["pairs_screened"])
+    # the other rates of the metric family: all-pairs equivalent (|R||S| or N(N-1)/2 per second)
+    # and emitted result pairs per second, whole job
+    line["rates"] = {"all_pairs_equivalent_per_s": world * st["pairs_all"] / (ms / 1000.0),
+                     "result_pairs_per_s": world * int(count) / (ms / 1000.0),
+                     "pair_space_pruned_fraction": max(0.0, 1.0 - st["pairs_screened"] / max(1, st["pairs_all"]))}
     if screen not in ("plain", "int8limb"):   # screen error vs sequential FP64 on 64 sampled tile pairs
         rd = tj.join_result(R, S, eps2=T, mode=mode, screen=screen, screen_diag=True)
         sd = rd.stats
