@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--screen", default=None, help="override the workload's screen (plain/bf16/fp16/int8limb)")
     ap.add_argument("--n", type=int, default=0, help="rows per side (0 = the configuration's size)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 GPU baseline run")
+    ap.add_argument("--index-frame", default="auto", choices=["auto", "axes", "pca"],
+                    help="cells the rows are sorted by before tiling (default: the library's choice)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=128, help="R rows in the CPU baseline sample")
@@ -232,7 +234,7 @@ def main() -> None:
     T = w.T
 
     def step():
-        res = tj.join_result(R, S, eps2=T, mode=mode, screen=screen)
+        res = tj.join_result(R, S, eps2=T, mode=mode, screen=screen, index_frame=args.index_frame)
         i, j = res.pairs()
         return res, i, j
 
@@ -308,7 +310,8 @@ def main() -> None:
         "result_pairs": int(count), "step_ms": step_ms, "lib_ms_total": [s["ms_total"] for s in stats],
         "stats": {k: st[k] for k in (
             "pairs_all", "pairs_screened", "tile_pairs", "screen_accept", "band", "refine_accept", "rare_checks",
-            "result_pairs", "retries", "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total")},
+            "result_pairs", "retries", "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total",
+            "index_frame")},
     }
     line["stats"]["refined_fraction"] = st["band"] / max(1, st["pairs_screened"])
     # the other rates of the metric family: all-pairs equivalent (|R||S| or N(N-1)/2 per second)

@@ -74,6 +74,14 @@ typedef struct tj_options {
 /* Use the one-SM tensor-core screen even where the CTA-pair screen (cta_group::2, 256 x 256 tiles
  * over two SMs; one join, rows of >= 256 elements, every tile pair a candidate) would run. */
 #define TJ_FLAG_SCREEN_1SM 2
+/* Index frame: the cells rows are sorted by before they are cut into tiles.  By default a single
+ * join with 9 <= d <= 128 and at least 2^17 rows in all uses cells over the top 8 principal
+ * directions of a sampled covariance; every other join uses cells over the 8 highest-variance
+ * input dimensions.  FRAME_AXES forces the input-dimension cells, FRAME_PCA the principal-direction
+ * cells wherever 9 <= d <= 128 (any size, packed joins included).  The frame only changes which
+ * rows share a tile, never the pairs.  Setting both is an error. */
+#define TJ_FLAG_FRAME_AXES 4
+#define TJ_FLAG_FRAME_PCA 8
 
 typedef struct tj_stats {
     int64_t n_rows, n_cols;       /* |R|, |S| (self-join: N, N) */
@@ -92,6 +100,8 @@ typedef struct tj_stats {
     double screen_err_over_bound; /* TJ_FLAG_SCREEN_DIAG: max of that error divided by the certified radius */
     int64_t screen_err_pairs;     /* TJ_FLAG_SCREEN_DIAG: sampled pairs */
     int64_t screen_pair;          /* 1 if the CTA-pair tensor-core screen ran */
+    int64_t index_frame;          /* 1 if the index cells were over principal directions, 0 if over
+                                     input dimensions */
 } tj_stats;
 
 /* ----------------------------------------------------------------- joins */

@@ -23,6 +23,8 @@ MODE = {"rs": 0, "upper": 1, "directed": 2}
 SCREEN = {"plain": 0, "bf16": 1, "fp16": 2, "int8limb": 3, "bf16x3": 4, "fp16x3": 5}
 FLAG_SCREEN_DIAG = 1
 FLAG_SCREEN_1SM = 2
+FLAG_FRAME_AXES = 4
+FLAG_FRAME_PCA = 8
 
 # Every symbol include/tensorjoin.h declares (checked by the CPU test suite).
 EXPORTS = [
@@ -49,7 +51,8 @@ class Stats(C.Structure):
         "n_rows", "n_cols", "pairs_all", "tile_pairs", "pairs_screened", "screen_accept", "band",
         "refine_accept", "rare_checks", "result_pairs", "retries")] + [(n, C.c_double) for n in (
         "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total", "screen_ops",
-        "screen_max_abs_err", "screen_err_over_bound")] + [("screen_err_pairs", C.c_int64), ("screen_pair", C.c_int64)]
+        "screen_max_abs_err", "screen_err_over_bound")] + [("screen_err_pairs", C.c_int64), ("screen_pair", C.c_int64),
+                                                   ("index_frame", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

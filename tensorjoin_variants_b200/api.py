@@ -145,17 +145,27 @@ def _run(R, S, eps, eps2, mode: str, screen: str, capacity: int, chunk_items: in
     return Result(h, Rt.shape[0], St.shape[0] if mode == "rs" else Rt.shape[0], host, keepalive=(Rt, St))
 
 
+FRAME_FLAGS = {"auto": 0, "axes": _lib.FLAG_FRAME_AXES, "pca": _lib.FLAG_FRAME_PCA}
+
+
 def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "bf16", capacity: int = 0,
-                chunk_items: int = 0, screen_diag: bool = False, cta_pair: bool = True) -> Result:
+                chunk_items: int = 0, screen_diag: bool = False, cta_pair: bool = True,
+                index_frame: str = "auto") -> Result:
     """Run a join and return the Result handle (pairs, keys, neighbour table, statistics).
 
     ``screen_diag=True`` also samples 64 tile pairs of the tensor-core screen and reports, in
     ``stats``, the screen's largest distance error against sequential FP64 distances and that
     error relative to the certified radius (must stay below 1).  ``cta_pair=False`` keeps the
-    one-SM screen where the CTA-pair screen would run (``stats["screen_pair"]`` says which ran)."""
+    one-SM screen where the CTA-pair screen would run (``stats["screen_pair"]`` says which ran).
+    ``index_frame`` picks the cells rows are sorted by before tiling: "auto", "axes" (the 8
+    highest-variance input dimensions) or "pca" (the top 8 principal directions, 9 <= d <= 128);
+    ``stats["index_frame"]`` is 1 where the principal-direction cells were used."""
     if mode not in MODE:
         raise ValueError(f"mode must be one of {sorted(MODE)}")
+    if index_frame not in FRAME_FLAGS:
+        raise ValueError(f"index_frame must be one of {sorted(FRAME_FLAGS)}")
     flags = (_lib.FLAG_SCREEN_DIAG if screen_diag else 0) | (0 if cta_pair else _lib.FLAG_SCREEN_1SM)
+    flags |= FRAME_FLAGS[index_frame]
     return _run(R, S, eps, eps2, mode, screen, capacity, chunk_items, flags)
 
 

@@ -264,6 +264,14 @@ struct JoinIn {
     double eps2;
 };
 
+void check_flags(const tj_options* opt) {
+    if (!opt) return;
+    const int known = TJ_FLAG_SCREEN_DIAG | TJ_FLAG_SCREEN_1SM | TJ_FLAG_FRAME_AXES | TJ_FLAG_FRAME_PCA;
+    if (opt->flags & ~known) fail(TJ_ERR_INVALID, "unknown option flags");
+    if ((opt->flags & TJ_FLAG_FRAME_AXES) && (opt->flags & TJ_FLAG_FRAME_PCA))
+        fail(TJ_ERR_INVALID, "TJ_FLAG_FRAME_AXES and TJ_FLAG_FRAME_PCA exclude each other");
+}
+
 // One or many joins.  Joins are grouped into classes of equal d; each class gets one
 // concatenated, Morton-sorted side per operand (joins stay contiguous), global tile tables, one
 // block-diagonal candidate list and one persistent screen launch over all classes.
@@ -341,6 +349,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         TileSet tR, tS;
         DBuf<float> XR, XS, center;
         DBuf<FrameParams> fp;
+        bool pca_frame = false;   // cells over principal directions (else input dimensions)
         DBuf<long long> rowoffR, rowoffS;
     };
     std::vector<std::unique_ptr<Cls>> C(ncls);
@@ -403,17 +412,24 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         {
             const void* srcs[2] = {srcR, srcS};
             const long long ns[2] = {roR[njc], roS[njc]};
-            compute_frame(srcs, ns, self ? 1 : 2, d, dtype, K.fp.p, K.center.p, st);
+            // packed joins keep input-dimension cells unless asked otherwise: one covariance pooled
+            // over many joins mostly describes how the joins differ, not how each one's rows spread
+            const int flags = opt ? opt->flags : 0;
+            const int fm = (flags & TJ_FLAG_FRAME_AXES) ? kFrameAxes
+                         : (flags & TJ_FLAG_FRAME_PCA) ? kFramePca
+                         : njc == 1 ? kFrameAuto : kFrameAxes;
+            K.pca_frame = compute_frame(srcs, ns, self ? 1 : 2, d, dtype, fm, K.fp.p, K.center.p, st);
+            if (K.pca_frame) S_.index_frame = 1;
         }
         K.R.src = srcR; K.R.dtype = dtype; K.R.n = roR[njc]; K.R.d = d; K.R.screen = screen;
         K.R.njc = njc; K.R.d_rowoff = njc > 1 ? K.rowoffR.p : nullptr;
-        prepare_side(K.R, K.fp.p, K.center.p, st, &ctr.p->status);
+        prepare_side(K.R, K.fp.p, K.pca_frame, K.center.p, st, &ctr.p->status);
         compute_perm_local(K.R, st);
         Side* pS = &K.R;
         if (!self) {
             K.S.src = srcS; K.S.dtype = dtype; K.S.n = roS[njc]; K.S.d = d; K.S.screen = screen;
             K.S.njc = njc; K.S.d_rowoff = njc > 1 ? K.rowoffS.p : nullptr;
-            prepare_side(K.S, K.fp.p, K.center.p, st, &ctr.p->status);
+            prepare_side(K.S, K.fp.p, K.pca_frame, K.center.p, st, &ctr.p->status);
             compute_perm_local(K.S, st);
             pS = &K.S;
         }
@@ -664,7 +680,7 @@ int tj_join(const void* R, int64_t nR, const void* S, int64_t nS, int32_t d, int
     if (mode < 0 || mode > 2) fail(TJ_ERR_INVALID, "unknown mode");
     if (screen < 0 || screen > 5) fail(TJ_ERR_INVALID, "unknown screen");
     if (dtype != TJ_DTYPE_F32 && dtype != TJ_DTYPE_I16) fail(TJ_ERR_INVALID, "unknown dtype");
-    if (opt && (opt->flags & ~(TJ_FLAG_SCREEN_DIAG | TJ_FLAG_SCREEN_1SM))) fail(TJ_ERR_INVALID, "unknown option flags");
+    check_flags(opt);
     std::unique_ptr<tj_result> res(new tj_result());
     std::vector<JoinIn> js{JoinIn{R, (const void*)(mode == TJ_MODE_RS ? S : R), nR, mode == TJ_MODE_RS ? nS : nR,
                                   d, eps2}};
@@ -740,10 +756,10 @@ int tj_index_build(const void* X, int64_t n, int32_t d, int32_t dtype, double ep
     DBuf<float> center((size_t)d, st);
     const void* srcs[1] = {X};
     const long long ns[1] = {n};
-    compute_frame(srcs, ns, 1, d, dtype, fp.p, center.p, st);
+    const bool pca_frame = compute_frame(srcs, ns, 1, d, dtype, kFrameAuto, fp.p, center.p, st);
     Side& s = ix->side;
     s.src = X; s.dtype = dtype; s.n = n; s.d = d; s.screen = kScreenPlain;
-    prepare_side(s, fp.p, center.p, st, &ctr.p->status);
+    prepare_side(s, fp.p, pca_frame, center.p, st, &ctr.p->status);
     tile_stats(s, kTileR, ix->t128, st);
     tile_stats(s, kTileS, ix->t256, st);
     const JoinParams jp = make_params(eps2, d, 64, 0, n, n, true);
@@ -815,7 +831,7 @@ int tj_join_batched(const tj_batch_join* joins, int32_t njoins, int32_t screen, 
     *out = nullptr;
     if (njoins < 1) fail(TJ_ERR_INVALID, "njoins must be >= 1");
     if (screen < 0 || screen > 5 || screen == TJ_SCREEN_INT8LIMB) fail(TJ_ERR_UNSUPPORTED, "batched joins take FP32 screens");
-    if (opt && (opt->flags & ~(TJ_FLAG_SCREEN_DIAG | TJ_FLAG_SCREEN_1SM))) fail(TJ_ERR_INVALID, "unknown option flags");
+    check_flags(opt);
     std::vector<JoinIn> js((size_t)njoins);
     for (int k = 0; k < njoins; ++k) js[k] = JoinIn{joins[k].R, joins[k].S, joins[k].nR, joins[k].nS, joins[k].d, joins[k].eps2};
     std::unique_ptr<tj_result> res(new tj_result());

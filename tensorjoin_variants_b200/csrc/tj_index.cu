@@ -127,25 +127,26 @@ __global__ void __launch_bounds__(256) dim_reduce(const float* pmin, const float
 // Pick the m = min(d, 8) highest-variance dimensions and their quantisation frame.
 __global__ void frame_pick(int d, const float* var_ws, const float* lo_ws, const float* hi_ws, FrameParams* fp) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const int m = min(d, 8);
-    FrameParams f;
-    f.m = m;
-    f.bits = 32 / m;
+    const int m = min(d, 8), bits = 32 / m;
+    int dims[8];
     for (int t = 0; t < m; ++t) {
         int best = -1;
         for (int k = 0; k < d; ++k) {
             bool used = false;
-            for (int u = 0; u < t; ++u) used |= (f.dims[u] == k);
+            for (int u = 0; u < t; ++u) used |= (dims[u] == k);
             if (used) continue;
             if (best < 0 || var_ws[k] > var_ws[best]) best = k;
         }
-        f.dims[t] = best;
+        dims[t] = best;
         const float lo = lo_ws[best], hi = hi_ws[best];
         const float range = (isfinite(lo) && isfinite(hi) && hi > lo) ? hi - lo : 1.f;
-        f.lo[t] = isfinite(lo) ? lo : 0.f;
-        f.inv_w[t] = (float)(1u << f.bits) / range;
+        fp->dims[t] = best;
+        fp->lo[t] = isfinite(lo) ? lo : 0.f;
+        fp->inv_w[t] = (float)(1u << bits) / range;
     }
-    *fp = f;
+    fp->m = m;
+    fp->bits = bits;
+    fp->pca = 0;
 }
 
 TJ_DEV int join_of_row(const long long* rowoff, int njc, long long r) {   // last j with rowoff[j] <= r
@@ -157,24 +158,324 @@ TJ_DEV int join_of_row(const long long* rowoff, int njc, long long r) {   // las
     return lo;
 }
 
-// Morton key of the indexed dimensions; with several joins concatenated in one side the join
+// Principal-component frame (the PCA-ordered layout): covariance of up to kPcaSamples evenly
+// spaced rows of all sources, top m = 8 directions by subspace iteration, cells over the
+// projections y_k = (x - c) . v_k quantised on their range over the sampled rows.  The frame only
+// decides which rows share a tile; every bound and result stays exact.
+constexpr int kCovBlocks = 256;
+constexpr long long kPcaSamples = 16384;
+constexpr int kPcaRounds = 8;
+
+// Per-block partial covariance (d x d, FP32, rows in a fixed order), d <= kPcaMaxD.
+__global__ void __launch_bounds__(256) cov_partial(const void* const* srcs, const long long* offs, int nsrc,
+                                                   long long stride, long long nsamp, int d, int dtype,
+                                                   const float* center, float* partial) {
+    __shared__ float y[32][kPcaMaxD];
+    const int dd = d * d;
+    float acc[64];
+#pragma unroll
+    for (int u = 0; u < 64; ++u) acc[u] = 0.f;
+    const long long per = (nsamp + gridDim.x - 1) / gridDim.x;
+    const long long s0 = (long long)blockIdx.x * per, s1 = min(nsamp, s0 + per);
+    for (long long sb = s0; sb < s1; sb += 32) {
+        const int rows = (int)min(32ll, s1 - sb);
+        for (int e = threadIdx.x; e < 32 * d; e += 256) {
+            const int rr = e / d, k = e % d;
+            float v = 0.f;
+            if (rr < rows) {
+                const long long g = (sb + rr) * stride;   // row index over the concatenated sources
+                int src = 0;
+                while (src + 1 < nsrc && offs[src + 1] <= g) ++src;
+                v = load_x(srcs[src], dtype, (size_t)(g - offs[src]) * d + k) - center[k];
+                if (!isfinite(v)) v = 0.f;
+            }
+            y[rr][k] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 64; ++u) {
+            const int e = threadIdx.x + u * 256;
+            if (e < dd) {
+                const int i = e / d, j = e % d;
+                float a = acc[u];
+                for (int rr = 0; rr < rows; ++rr) a = fmaf(y[rr][i], y[rr][j], a);
+                acc[u] = a;
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 64; ++u) {
+        const int e = threadIdx.x + u * 256;
+        if (e < dd) partial[(size_t)blockIdx.x * dd + e] = acc[u];
+    }
+}
+
+// Sum of the per-block partial covariances, in block order (one thread per entry).
+__global__ void cov_reduce(const float* partial, int nparts, int dd, float* C) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= dd) return;
+    float a = 0.f;
+    for (int b = 0; b < nparts; ++b) a += partial[(size_t)b * dd + e];
+    C[e] = a;
+}
+
+TJ_DEV float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Top m = 8 principal directions of C by kPcaRounds rounds of V <- orth(C V) from a fixed start,
+// C scaled by 1 / trace(C) first.  Each round: W = C V on all threads, the 8 x 8 Gram matrix
+// G = W^T W by the warps, its Cholesky factor G = L L^T (FP64, one thread), then V = W L^-T
+// (Cholesky QR).  Should G lose definiteness the previous V is kept: the frame only orders rows.
+static_assert(kPcaMaxD == 128, "the Morton projection loads rows in four 32-column blocks");
+__global__ void __launch_bounds__(256) pca_frame(const float* Cg, int d, FrameParams* fp) {
+    extern __shared__ float sm[];
+    __shared__ float G[8][8], Li[8][8];
+    __shared__ float s_scale;
+    __shared__ int s_ok;
+    float* C = sm;                   // [d][d]
+    float* V = C + d * d;            // [8][d]
+    float* W = V + 8 * d;            // [8][d]
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nwarps = blockDim.x >> 5, dd = d * d, m = 8;
+    if (t < 32) {
+        float tr = 0.f;
+        for (int i = lane; i < d; i += 32) tr += Cg[i * d + i];
+        tr = warp_sum_f(tr);
+        if (lane == 0) s_scale = (tr > 0.f && isfinite(tr)) ? 1.f / tr : 0.f;
+    }
+    __syncthreads();
+    const float scale = s_scale;
+    for (int e = t; e < dd; e += blockDim.x) C[e] = Cg[e] * scale;
+    for (int e = t; e < m * d; e += blockDim.x) {   // deterministic, linearly independent start
+        const int k = e / d, j = e % d;
+        V[e] = (j % m == k ? 1.f : 0.f) + 0.001f * (float)((j * 7 + k * 13) % 17);
+    }
+    __syncthreads();
+    for (int it = 0; it < kPcaRounds && scale > 0.f; ++it) {
+        for (int e = t; e < m * d; e += blockDim.x) {   // W = C V (C is symmetric: read its columns)
+            const int k = e / d, i = e % d;
+            float a = 0.f;
+            for (int j = 0; j < d; ++j) a = fmaf(C[j * d + i], V[k * d + j], a);
+            W[e] = a;
+        }
+        __syncthreads();
+        for (int e = warp; e < 64; e += nwarps) {       // G = W^T W
+            const int k = e >> 3, u = e & 7;
+            float a = 0.f;
+            for (int j = lane; j < d; j += 32) a = fmaf(W[k * d + j], W[u * d + j], a);
+            a = warp_sum_f(a);
+            if (lane == 0) G[k][u] = a;
+        }
+        __syncthreads();
+        if (t == 0) {   // L = chol(G), Li = L^-1 (lower triangular), FP64
+            double L[8][8] = {}, I[8][8] = {};
+            bool ok = true;
+            for (int k = 0; k < 8 && ok; ++k) {
+                for (int u = 0; u <= k; ++u) {
+                    double v = 0.5 * ((double)G[k][u] + (double)G[u][k]);
+                    for (int q = 0; q < u; ++q) v -= L[k][q] * L[u][q];
+                    if (u == k) {
+                        if (!(v > 1e-30)) { ok = false; break; }
+                        L[k][k] = sqrt(v);
+                    } else {
+                        L[k][u] = v / L[u][u];
+                    }
+                }
+            }
+            if (ok) {
+                for (int c = 0; c < 8; ++c) {
+                    for (int k = c; k < 8; ++k) {
+                        double v = k == c ? 1.0 : 0.0;
+                        for (int q = c; q < k; ++q) v -= L[k][q] * I[q][c];
+                        I[k][c] = v / L[k][k];
+                    }
+                }
+                for (int k = 0; k < 8; ++k)
+                    for (int u = 0; u < 8; ++u) Li[k][u] = (float)I[k][u];
+            }
+            s_ok = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        for (int e = t; e < m * d; e += blockDim.x) {   // V[:, k] = sum_{u <= k} W[:, u] Li[k][u]
+            const int k = e / d, i = e % d;
+            float a = 0.f;
+            for (int u = 0; u <= k; ++u) a = fmaf(W[u * d + i], Li[k][u], a);
+            V[e] = a;
+        }
+        __syncthreads();
+    }
+    for (int e = t; e < m * d; e += blockDim.x) fp->V[e] = V[e];
+    if (t == 0) {
+        fp->m = m;
+        fp->bits = 32 / m;
+        fp->pca = 1;
+        for (int k = 0; k < m; ++k) fp->dims[k] = -1;
+    }
+}
+
+// Projections of one row onto the frame's 8 directions, computed by a whole warp: coalesced reads
+// of the row, butterfly sums; every lane returns the full sums.
+TJ_DEV void project8_warp(const void* src, int dtype, size_t row, int d, const float* center, const float* V,
+                          int lane, float (&y)[8]) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) y[k] = 0.f;
+    for (int j = lane; j < d; j += 32) {
+        const float xv = load_x(src, dtype, row * d + j) - center[j];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) y[k] = fmaf(xv, V[k * d + j], y[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) y[k] = warp_sum_f(y[k]);
+}
+
+// Range of each projection over the same sampled rows (one warp per row): per-block minima and
+// maxima (out[block][k] = min, out[block][8 + k] = max), reduced by pca_range_finish.  Cells span
+// the sampled range; rows outside it fall into the edge cells.
+__global__ void __launch_bounds__(256) proj_range_partial(const void* const* srcs, const long long* offs, int nsrc,
+                                                          long long stride, long long nsamp, int d, int dtype,
+                                                          const float* center, const FrameParams* fp, float* out) {
+    __shared__ float smn[8][256], smx[8][256];
+    float mn[8], mx[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { mn[k] = INFINITY; mx[k] = -INFINITY; }
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = (long long)gridDim.x * (blockDim.x / 32);
+    for (long long sidx = (long long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); sidx < nsamp;
+         sidx += nwarps) {
+        const long long g = sidx * stride;
+        int src = 0;
+        while (src + 1 < nsrc && offs[src + 1] <= g) ++src;
+        float y[8];
+        project8_warp(srcs[src], dtype, (size_t)(g - offs[src]), d, center, fp->V, lane, y);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (isfinite(y[k])) { mn[k] = fminf(mn[k], y[k]); mx[k] = fmaxf(mx[k], y[k]); }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { smn[k][threadIdx.x] = mn[k]; smx[k][threadIdx.x] = mx[k]; }
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                smn[k][threadIdx.x] = fminf(smn[k][threadIdx.x], smn[k][threadIdx.x + w]);
+                smx[k][threadIdx.x] = fmaxf(smx[k][threadIdx.x], smx[k][threadIdx.x + w]);
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 8) {
+        out[blockIdx.x * 16 + threadIdx.x] = smn[threadIdx.x][0];
+        out[blockIdx.x * 16 + 8 + threadIdx.x] = smx[threadIdx.x][0];
+    }
+}
+
+__global__ void pca_range_finish(const float* part, int nparts, FrameParams* fp) {
+    const int k = threadIdx.x;
+    if (k >= 8) return;
+    float lo = INFINITY, hi = -INFINITY;
+    for (int b = 0; b < nparts; ++b) {
+        lo = fminf(lo, part[b * 16 + k]);
+        hi = fmaxf(hi, part[b * 16 + 8 + k]);
+    }
+    const bool ok = isfinite(lo) && isfinite(hi) && hi > lo;
+    fp->lo[k] = ok ? lo : 0.f;
+    fp->inv_w[k] = (float)(1u << fp->bits) / (ok ? hi - lo : 1.f);
+}
+
+TJ_DEV uint64_t morton_interleave(const unsigned* c, int m, int bits) {
+    uint64_t key = 0;
+    for (int b = bits - 1; b >= 0; --b)
+        for (int t = 0; t < m; ++t) key = (key << 1) | ((c[t] >> b) & 1u);
+    return key;
+}
+
+// Morton key of the input-dimension cells; with several joins concatenated in one side the join
 // index goes above bit 32, so every join's rows stay contiguous after the sort.
 __global__ void morton_keys(const void* src, int dtype, long long n, int d, const FrameParams* fpp, uint64_t* keys,
                             uint32_t* vals, const long long* rowoff, int njc) {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
-    const FrameParams fp = *fpp;
-    const unsigned maxc = (1u << fp.bits) - 1u;
+    const int m = fpp->m, bits = fpp->bits;
+    const unsigned maxc = (1u << bits) - 1u;
     unsigned c[16];
-    for (int t = 0; t < fp.m; ++t) {
-        const float v = load_x(src, dtype, (size_t)r * d + fp.dims[t]);
-        float q = (v - fp.lo[t]) * fp.inv_w[t];
+    for (int t = 0; t < m; ++t) {
+        const float v = load_x(src, dtype, (size_t)r * d + fpp->dims[t]);
+        float q = (v - fpp->lo[t]) * fpp->inv_w[t];
         q = fminf(fmaxf(q, 0.f), (float)maxc);
         c[t] = isfinite(q) ? (unsigned)q : 0u;
     }
-    uint64_t key = 0;
-    for (int b = fp.bits - 1; b >= 0; --b)
-        for (int t = 0; t < fp.m; ++t) key = (key << 1) | ((c[t] >> b) & 1u);
+    uint64_t key = morton_interleave(c, m, bits);
+    if (njc > 1) key |= (uint64_t)join_of_row(rowoff, njc, r) << 32;
+    keys[r] = key;
+    vals[r] = (uint32_t)r;
+}
+
+// Morton key of the principal-direction cells.  Each warp projects its 32 rows four at a time:
+// all of a group's row loads issue together (coalesced, four 32-column blocks), then one
+// reduce-scatter over the 4 x 8 partial sums (31 shuffles; lane L ends with row L / 8, direction
+// L % 8), routed through shared memory to the row's lane.  Launched with 256 threads.
+__global__ void __launch_bounds__(256, 3) morton_keys_pca(const void* src, int dtype, long long n, int d,
+                                                          const FrameParams* fpp, uint64_t* keys, uint32_t* vals,
+                                                          const long long* rowoff, int njc, const float* center) {
+    __shared__ float ybuf[8][32][9];
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long w0 = r - lane;
+    for (int q0 = 0; q0 < 32 && w0 + q0 < n; q0 += 4) {   // warp-uniform bound: every lane shuffles
+        float a[32];   // a[u * 8 + t]: row q0 + u, direction t
+#pragma unroll
+        for (int e = 0; e < 32; ++e) a[e] = 0.f;
+        float xv[4][4];   // [column block jj][row u]
+#pragma unroll
+        for (int jj = 0; jj < kPcaMaxD / 32; ++jj) {
+            const int j = lane + 32 * jj;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                xv[jj][u] = (j < d && w0 + q0 + u < n) ? load_x(src, dtype, (size_t)(w0 + q0 + u) * d + j) : 0.f;
+        }
+#pragma unroll
+        for (int jj = 0; jj < kPcaMaxD / 32; ++jj) {
+            const int j = lane + 32 * jj;
+            if (j < d) {
+                const float cj = center[j];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    const float v = fpp->V[t * d + j];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) a[u * 8 + t] = fmaf(xv[jj][u] - cj, v, a[u * 8 + t]);
+                }
+            }
+        }
+        // reduce-scatter: at width h, lanes with bit h set keep the upper half of the entries
+#pragma unroll
+        for (int h = 16; h >= 1; h >>= 1) {
+            const bool up = (lane & h) != 0;
+#pragma unroll
+            for (int e = 0; e < h; ++e) {
+                const float send = up ? a[e] : a[e + h];
+                const float keep = up ? a[e + h] : a[e];
+                a[e] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+            }
+        }
+        ybuf[wib][q0 + (lane >> 3)][lane & 7] = a[0];
+    }
+    __syncwarp();
+    if (r >= n) return;
+    const int bits = fpp->bits;
+    const unsigned maxc = (1u << bits) - 1u;
+    unsigned c[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        float q = (ybuf[wib][lane][t] - fpp->lo[t]) * fpp->inv_w[t];
+        q = fminf(fmaxf(q, 0.f), (float)maxc);
+        c[t] = isfinite(q) ? (unsigned)q : 0u;
+    }
+    uint64_t key = morton_interleave(c, 8, bits);
     if (njc > 1) key |= (uint64_t)join_of_row(rowoff, njc, r) << 32;
     keys[r] = key;
     vals[r] = (uint32_t)r;
@@ -645,8 +946,8 @@ __global__ void chunk_emit(const uint64_t* keys, size_t cap, const uint32_t* tot
 
 // ------------------------------------------------------------------ host entry points
 
-void compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d, int dtype, FrameParams* fp,
-                   float* center, cudaStream_t st) {
+bool compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d, int dtype, int frame_mode,
+                   FrameParams* fp, float* center, cudaStream_t st) {
     long long ntot = 0;
     for (int s = 0; s < nsrc; ++s) ntot += ns[s];
     const int parts = nsrc * kStatBlocks;
@@ -660,11 +961,38 @@ void compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d
     }
     launch(dim_reduce, (unsigned)d, 256, 0, st, pmin.p, pmax.p, psum.p, psq.p, parts, ntot, d, ws.p,
            ws.p + d, ws.p + 2 * d, center);
-    launch(frame_pick, 1, 32, 0, st, d, ws.p, ws.p + d, ws.p + 2 * d, fp);
+    const bool pca = frame_mode != kFrameAxes && d >= 9 && d <= kPcaMaxD && ntot > 0 &&
+                     (frame_mode == kFramePca || ntot >= kPcaMinRows);
+    if (pca) {   // principal-component cells
+        const long long stride = std::max(1ll, ntot / kPcaSamples);
+        const long long nsamp = (ntot + stride - 1) / stride;   // (nsamp - 1) * stride < ntot
+        std::vector<long long> offs(nsrc + 1, 0);
+        for (int s = 0; s < nsrc; ++s) offs[s + 1] = offs[s] + ns[s];
+        DBuf<const void*> dsrc((size_t)nsrc, st);
+        DBuf<long long> doff((size_t)nsrc + 1, st);
+        upload(dsrc.p, srcs, nsrc * sizeof(void*), st);
+        upload(doff.p, offs.data(), (nsrc + 1) * sizeof(long long), st);
+        DBuf<float> part((size_t)kCovBlocks * d * d, st);   // >= kCovBlocks * 16 floats (d >= 9)
+        DBuf<float> cov((size_t)d * d, st);
+        launch(cov_partial, kCovBlocks, 256, 0, st, (const void* const*)dsrc.p, (const long long*)doff.p, nsrc,
+               stride, nsamp, d, dtype, (const float*)center, part.p);
+        launch(cov_reduce, (unsigned)((d * d + 255) / 256), 256, 0, st, (const float*)part.p, kCovBlocks, d * d,
+               cov.p);
+        const size_t smem = (size_t)(d * d + 16 * d) * sizeof(float);
+        if (smem > 48 * 1024)
+            TJ_CUDA(cudaFuncSetAttribute(pca_frame, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        launch(pca_frame, 1, 256, smem, st, (const float*)cov.p, d, fp);
+        launch(proj_range_partial, kCovBlocks, 256, 0, st, (const void* const*)dsrc.p, (const long long*)doff.p,
+               nsrc, stride, nsamp, d, dtype, (const float*)center, (const FrameParams*)fp, part.p);
+        launch(pca_range_finish, 1, 32, 0, st, (const float*)part.p, kCovBlocks, fp);
+    } else {
+        launch(frame_pick, 1, 32, 0, st, d, ws.p, ws.p + d, ws.p + 2 * d, fp);
+    }
     TJ_CUDA(cudaGetLastError());
+    return pca;
 }
 
-void prepare_side(Side& s, const FrameParams* fpd, const float* center, cudaStream_t st,
+void prepare_side(Side& s, const FrameParams* fpd, bool pca_frame, const float* center, cudaStream_t st,
                   unsigned long long* status) {
     const long long n = s.n;
     const bool i8 = s.screen == kScreenInt8Limb;
@@ -680,8 +1008,12 @@ void prepare_side(Side& s, const FrameParams* fpd, const float* center, cudaStre
         DBuf<uint64_t> ktmp((size_t)n, st);
         DBuf<uint32_t> vtmp((size_t)n, st);
         DBuf<uint32_t> ws(radix_workspace_elems((size_t)n), st);
-        launch(morton_keys, (unsigned)((n + 255) / 256), 256, 0, st, s.src, s.dtype, n, s.d, fpd, s.keys.p, s.perm.p,
-               s.d_rowoff, s.njc);
+        if (pca_frame)
+            launch(morton_keys_pca, (unsigned)((n + 255) / 256), 256, 0, st, s.src, s.dtype, n, s.d, fpd, s.keys.p,
+                   s.perm.p, s.d_rowoff, s.njc, center);
+        else
+            launch(morton_keys, (unsigned)((n + 255) / 256), 256, 0, st, s.src, s.dtype, n, s.d, fpd, s.keys.p,
+                   s.perm.p, s.d_rowoff, s.njc);
         int jbits = 0;
         while ((1 << jbits) < s.njc) ++jbits;
         radix_sort(s.keys.p, s.perm.p, ktmp.p, vtmp.p, (size_t)n, 32 + jbits, ws.p, st);

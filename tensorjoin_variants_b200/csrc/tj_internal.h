@@ -170,18 +170,28 @@ struct Candidates {
     size_t chunks_cap = 0;
 };
 
+constexpr int kPcaMaxD = 128;   // principal-component frames for 9 <= d <= kPcaMaxD
 struct FrameParams {
-    int m = 0;               // indexed dimensions
+    int m = 0;               // indexed dimensions (or principal directions)
     int bits = 0;            // bits per indexed dimension
-    int dims[16] = {0};
+    int pca = 0;             // 1: cells over the projections onto the top m principal directions
+    int dims[16] = {0};      // pca == 0: the indexed input dimensions
     float lo[16] = {0};
     float inv_w[16] = {0};
+    float V[8 * kPcaMaxD] = {0};   // pca == 1: direction k is V[k * d .. k * d + d)
 };
 
 // side preparation
-void compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d, int dtype, FrameParams* fp,
-                   float* center, cudaStream_t st);
-void prepare_side(Side& s, const FrameParams* fp_dev, const float* center, cudaStream_t st,
+// Index frame shared by both sides: cells over the m = min(d, 8) highest-variance input
+// dimensions, or cells over the top 8 principal directions of a sampled covariance
+// (kFramePca: whenever 9 <= d <= kPcaMaxD; kFrameAuto: also needs kPcaMinRows rows in all). The
+// return value says whether the principal-component frame was built. Also writes the
+// per-dimension centre.
+constexpr int kFrameAuto = 0, kFrameAxes = 1, kFramePca = 2;
+constexpr long long kPcaMinRows = 1ll << 17;   // below this the frame's fixed cost is not repaid
+bool compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d, int dtype, int frame_mode,
+                   FrameParams* fp, float* center, cudaStream_t st);
+void prepare_side(Side& s, const FrameParams* fp_dev, bool pca_frame, const float* center, cudaStream_t st,
                   unsigned long long* status);
 void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st);
 void build_candidates(const TileSet& tr, const TileSet& ts, double T, bool self_join, int chunk_items,

@@ -441,3 +441,62 @@ def test_cta_pair_screen(screen, shape):
     one = tj.join_result(Rt, St, eps2=T, screen=screen, cta_pair=False)
     assert one.stats["screen_pair"] == 0
     assert_same(one.keys().cpu().numpy().view(np.uint64), want, f"one-SM {screen} {shape}")
+
+
+_PCA_CASE = {}
+
+
+def _pca_case():
+    """2,000 x 130,000 rows of the 64-d mixture: 132,000 rows in all, enough for the automatic
+    principal-direction index frame (the oracle takes a few seconds; computed once)."""
+    if not _PCA_CASE:
+        w = W.mixture64(n=130000, samples=1 << 14)
+        R = np.ascontiguousarray(w.R[:2000])
+        _PCA_CASE.update(R=R, S=w.S, T=w.T, want=oracle_keys(R, w.S, w.T, "rs"))
+    return _PCA_CASE
+
+
+@pytest.mark.parametrize("screen", ["plain", "fp16", "bf16x3"])
+def test_principal_direction_frame_auto(screen):
+    """A single join with enough rows picks the principal-direction cells; the pairs stay the
+    oracle's, and forcing the input-dimension cells gives the same pairs."""
+    c = _pca_case()
+    k, st = gpu_keys(c["R"], c["S"], c["T"], "rs", screen)
+    assert st["index_frame"] == 1, st
+    assert_same(k, c["want"], f"pca {screen}")
+    k2, st2 = gpu_keys(c["R"], c["S"], c["T"], "rs", screen, index_frame="axes")
+    assert st2["index_frame"] == 0
+    assert_same(k2, c["want"], f"axes {screen}")
+    small = W.mixture64(n=6000, samples=1 << 14)   # below the row threshold: input-dimension cells
+    _, st3 = gpu_keys(small.R, small.S, small.T, "rs", screen)
+    assert st3["index_frame"] == 0
+
+
+@pytest.mark.parametrize("screen", FLOAT_SCREENS)
+@pytest.mark.parametrize("d", [9, 16, 33, 64, 128])
+def test_principal_direction_frame_forced(screen, d):
+    """index_frame="pca" at small sizes, R-S and both self-join modes, against the oracle."""
+    rng = np.random.default_rng(300 + d)
+    centres = rng.random((6, d))
+    R = (centres[rng.integers(0, 6, 1500)] + 0.05 * rng.standard_normal((1500, d))).astype(np.float32)
+    S = (centres[rng.integers(0, 6, 2300)] + 0.05 * rng.standard_normal((2300, d))).astype(np.float32)
+    T = float(np.quantile(((R[:60, None, :].astype(np.float64) - S[None, :400, :]) ** 2).sum(-1), 0.02))
+    k, st = gpu_keys(R, S, T, "rs", screen, index_frame="pca")
+    assert st["index_frame"] == 1
+    assert_same(k, oracle_keys(R, S, T, "rs"), f"pca rs {screen} d={d}")
+    for mode in ("upper", "directed"):
+        k, st = gpu_keys(S, None, T, mode, screen, index_frame="pca")
+        assert st["index_frame"] == 1
+        assert_same(k, oracle_keys(S, None, T, mode), f"pca {mode} {screen} d={d}")
+
+
+def test_frame_flags_exclusive():
+    """Both frame flags at once is an invalid argument (rejected before any device work)."""
+    R = torch.rand(300, 16, device="cuda")
+    with pytest.raises(ValueError):
+        tj.join_result(R, R, eps2=0.1, index_frame="both")
+    opt = _lib.Options(0, 0, _lib.FLAG_FRAME_AXES | _lib.FLAG_FRAME_PCA)
+    h = C.c_void_p()
+    rc = _lib.lib().tj_join(C.c_void_p(R.data_ptr()), 300, C.c_void_p(R.data_ptr()), 300, 16, _lib.DTYPE["f32"],
+                            0.1, _lib.MODE["rs"], _lib.SCREEN["bf16"], C.byref(opt), C.byref(h), None)
+    assert rc != 0 and not h.value
