@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 GPU baseline run")
     ap.add_argument("--index-frame", default="auto", choices=["auto", "axes", "pca"],
                     help="cells the rows are sorted by before tiling (default: the library's choice)")
+    ap.add_argument("--band-fp32", action="store_true", help="certified FP32 band stage before the FP64 terminal")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=128, help="R rows in the CPU baseline sample")
@@ -234,7 +235,8 @@ def main() -> None:
     T = w.T
 
     def step():
-        res = tj.join_result(R, S, eps2=T, mode=mode, screen=screen, index_frame=args.index_frame)
+        res = tj.join_result(R, S, eps2=T, mode=mode, screen=screen, index_frame=args.index_frame,
+                             band_fp32=args.band_fp32)
         i, j = res.pairs()
         return res, i, j
 
@@ -311,7 +313,7 @@ def main() -> None:
         "stats": {k: st[k] for k in (
             "pairs_all", "pairs_screened", "tile_pairs", "screen_accept", "band", "refine_accept", "rare_checks",
             "result_pairs", "retries", "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total",
-            "index_frame")},
+            "index_frame", "band_fp64")},
     }
     line["stats"]["refined_fraction"] = st["band"] / max(1, st["pairs_screened"])
     # the other rates of the metric family: all-pairs equivalent (|R||S| or N(N-1)/2 per second)
@@ -444,7 +446,7 @@ def ragged_bench(args, rank, world, screen, dist):
     stream = torch.cuda.current_stream()
 
     def step(scr):
-        return tj.join_batched_result(joins, screen=scr)
+        return tj.join_batched_result(joins, screen=scr, band_fp32=args.band_fp32)
 
     for _ in range(args.warmup):
         r = step(screen)
@@ -516,7 +518,7 @@ def ragged_bench(args, rank, world, screen, dist):
                   "single_join_latency_ms_p99": float(np.percentile(lat, 99)), "latency_sample": len(lat)},
         "stats": {k: st[k] for k in ("pairs_all", "pairs_screened", "tile_pairs", "screen_accept", "band",
                                      "refine_accept", "result_pairs", "retries", "ms_index", "ms_candidates",
-                                     "ms_screen", "ms_refine", "ms_sort", "ms_total")},
+                                     "ms_screen", "ms_refine", "ms_sort", "ms_total", "band_fp64")},
     }
     if not args.no_plain and screen != "plain":
         torch.cuda.synchronize()

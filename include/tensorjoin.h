@@ -82,6 +82,11 @@ typedef struct tj_options {
  * rows share a tile, never the pairs.  Setting both is an error. */
 #define TJ_FLAG_FRAME_AXES 4
 #define TJ_FLAG_FRAME_PCA 8
+/* Certified FP32 band stage: every band pair is first decided, where it can be, by an FP32 sum of
+ * squared FP32 differences against thresholds that bound its rounding error; only the pairs it
+ * cannot decide go on to the sequential FP64 terminal (tj_stats.band_fp64 counts them).  The
+ * pairs are the same either way.  No effect on the plain and int8-limb screens. */
+#define TJ_FLAG_BAND_FP32 16
 
 typedef struct tj_stats {
     int64_t n_rows, n_cols;       /* |R|, |S| (self-join: N, N) */
@@ -102,6 +107,7 @@ typedef struct tj_stats {
     int64_t screen_pair;          /* 1 if the CTA-pair tensor-core screen ran */
     int64_t index_frame;          /* 1 if the index cells were over principal directions, 0 if over
                                      input dimensions */
+    int64_t band_fp64;            /* band pairs decided by the FP64 terminal */
 } tj_stats;
 
 /* ----------------------------------------------------------------- joins */

@@ -25,6 +25,7 @@ FLAG_SCREEN_DIAG = 1
 FLAG_SCREEN_1SM = 2
 FLAG_FRAME_AXES = 4
 FLAG_FRAME_PCA = 8
+FLAG_BAND_FP32 = 16
 
 # Every symbol include/tensorjoin.h declares (checked by the CPU test suite).
 EXPORTS = [
@@ -52,7 +53,7 @@ class Stats(C.Structure):
         "refine_accept", "rare_checks", "result_pairs", "retries")] + [(n, C.c_double) for n in (
         "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total", "screen_ops",
         "screen_max_abs_err", "screen_err_over_bound")] + [("screen_err_pairs", C.c_int64), ("screen_pair", C.c_int64),
-                                                   ("index_frame", C.c_int64)]
+                                                   ("index_frame", C.c_int64), ("band_fp64", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -150,7 +150,7 @@ FRAME_FLAGS = {"auto": 0, "axes": _lib.FLAG_FRAME_AXES, "pca": _lib.FLAG_FRAME_P
 
 def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "bf16", capacity: int = 0,
                 chunk_items: int = 0, screen_diag: bool = False, cta_pair: bool = True,
-                index_frame: str = "auto") -> Result:
+                index_frame: str = "auto", band_fp32: bool = False) -> Result:
     """Run a join and return the Result handle (pairs, keys, neighbour table, statistics).
 
     ``screen_diag=True`` also samples 64 tile pairs of the tensor-core screen and reports, in
@@ -159,13 +159,15 @@ def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "b
     one-SM screen where the CTA-pair screen would run (``stats["screen_pair"]`` says which ran).
     ``index_frame`` picks the cells rows are sorted by before tiling: "auto", "axes" (the 8
     highest-variance input dimensions) or "pca" (the top 8 principal directions, 9 <= d <= 128);
-    ``stats["index_frame"]`` is 1 where the principal-direction cells were used."""
+    ``stats["index_frame"]`` is 1 where the principal-direction cells were used.
+    ``band_fp32=True`` decides band pairs by a certified FP32 sum first and sends only the rest to
+    the FP64 terminal (``stats["band_fp64"]`` counts those)."""
     if mode not in MODE:
         raise ValueError(f"mode must be one of {sorted(MODE)}")
     if index_frame not in FRAME_FLAGS:
         raise ValueError(f"index_frame must be one of {sorted(FRAME_FLAGS)}")
     flags = (_lib.FLAG_SCREEN_DIAG if screen_diag else 0) | (0 if cta_pair else _lib.FLAG_SCREEN_1SM)
-    flags |= FRAME_FLAGS[index_frame]
+    flags |= FRAME_FLAGS[index_frame] | (_lib.FLAG_BAND_FP32 if band_fp32 else 0)
     return _run(R, S, eps, eps2, mode, screen, capacity, chunk_items, flags)
 
 
@@ -249,8 +251,13 @@ class BatchResult(Result):
         return [(i[o[k]:o[k + 1]], j[o[k]:o[k + 1]]) for k in range(self.njoins)]
 
 
-def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_items: int = 0) -> BatchResult:
-    """Run many independent R-S joins [(R, S, eps), ...] in one batched pass (one screen launch)."""
+def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_items: int = 0,
+                        index_frame: str = "auto", band_fp32: bool = False) -> BatchResult:
+    """Run many independent R-S joins [(R, S, eps), ...] in one batched pass (one screen launch).
+    ``index_frame`` and ``band_fp32`` as in ``join_result`` (packed joins keep input-dimension
+    cells under "auto")."""
+    if index_frame not in FRAME_FLAGS:
+        raise ValueError(f"index_frame must be one of {sorted(FRAME_FLAGS)}")
     descs = (_lib.BatchJoin * len(joins))()
     keep = []
     host = True
@@ -262,7 +269,8 @@ def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_it
         descs[k] = _lib.BatchJoin(Rt.data_ptr(), St.data_ptr(), Rt.shape[0], St.shape[0], Rt.shape[1], 0,
                                   _threshold(eps, None))
     h = C.c_void_p()
-    opt = _lib.Options(int(capacity), int(chunk_items), 0)
+    flags = FRAME_FLAGS[index_frame] | (_lib.FLAG_BAND_FP32 if band_fp32 else 0)
+    opt = _lib.Options(int(capacity), int(chunk_items), flags)
     check(lib().tj_join_batched(descs, len(joins), SCREEN[screen], C.byref(opt), C.byref(h),
                                 C.c_void_p(_stream_ptr())))
     return BatchResult(h, len(joins), host, keepalive=tuple(keep))

@@ -266,7 +266,8 @@ struct JoinIn {
 
 void check_flags(const tj_options* opt) {
     if (!opt) return;
-    const int known = TJ_FLAG_SCREEN_DIAG | TJ_FLAG_SCREEN_1SM | TJ_FLAG_FRAME_AXES | TJ_FLAG_FRAME_PCA;
+    const int known = TJ_FLAG_SCREEN_DIAG | TJ_FLAG_SCREEN_1SM | TJ_FLAG_FRAME_AXES | TJ_FLAG_FRAME_PCA |
+                      TJ_FLAG_BAND_FP32;
     if (opt->flags & ~known) fail(TJ_ERR_INVALID, "unknown option flags");
     if ((opt->flags & TJ_FLAG_FRAME_AXES) && (opt->flags & TJ_FLAG_FRAME_PCA))
         fail(TJ_ERR_INVALID, "TJ_FLAG_FRAME_AXES and TJ_FLAG_FRAME_PCA exclude each other");
@@ -550,6 +551,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
 
     // optional screen-error sampling (tensor-core screens): 64 tile pairs spread over the candidate list
     const bool diag = opt && (opt->flags & TJ_FLAG_SCREEN_DIAG) && screen != TJ_SCREEN_PLAIN && !i8;
+    const bool band_fp32 = opt && (opt->flags & TJ_FLAG_BAND_FP32);
     DBuf<float> dump;
     DBuf<uint4> dump_ids;
     DBuf<unsigned long long> diag_out;
@@ -590,7 +592,9 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         else screen_tc(g, eb, st);
         S_.screen_pair = g.used_pair ? 1 : 0;
         ev.rec(3, st);
-        if (!i8) refine_band(g, eb, st);   // the int8-limb screen is exact: no band
+        // the int8-limb screen is exact: no band; the plain screen's band is already the FP32
+        // stage's undecided set
+        if (!i8) refine_band(g, eb, band_fp32 && screen != TJ_SCREEN_PLAIN, st);
         ev.rec(4, st);
         TJ_CUDA(cudaMemcpyAsync(&h, ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, st));
         TJ_CUDA(cudaStreamSynchronize(st));
@@ -617,6 +621,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     S_.band = (int64_t)h.band_valid;
     S_.refine_accept = (int64_t)h.refine_accept;
     S_.rare_checks = (int64_t)h.rare_checks;
+    S_.band_fp64 = (int64_t)h.band_fp64;
     band.reset();
 
     // canonical order

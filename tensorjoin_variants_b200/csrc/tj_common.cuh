@@ -38,7 +38,8 @@ struct Counters {
     unsigned long long rare_checks;    // pairs that reached the per-pair FP64 certificate
     unsigned long long items;          // tile pairs screened
     unsigned long long status;         // kStatus* bits
-    unsigned long long pad[7];
+    unsigned long long band_fp64;      // band pairs that reached the FP64 terminal
+    unsigned long long pad[6];
 };
 
 // Per-join parameters (batched mode has one per join; a single join uses one entry).

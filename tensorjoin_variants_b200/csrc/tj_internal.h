@@ -259,7 +259,8 @@ struct ScreenInput {
 void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);
 void screen_plain(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);
 void screen_i8(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);
-void refine_band(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);
+// FP64 terminal for the band; fp32_stage puts the certified FP32 band stage in front of it.
+void refine_band(const ScreenInput& g, const EmitBuffers& eb, bool fp32_stage, cudaStream_t st);
 void expand_directed(const uint64_t* upper, unsigned long long n_upper_slots, uint64_t* out, long long N,
                      cudaStream_t st);
 void decode_pairs(const uint64_t* keys, long long n, long long n_cols, int64_t* i_out, int64_t* j_out,

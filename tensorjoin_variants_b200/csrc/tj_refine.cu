@@ -174,7 +174,32 @@ struct RefineArgs {
     uint64_t* acc;
     unsigned long long acc_cap;
     Counters* ctr;
+    const float2* thr;                  // per join FP32-sum thresholds (the FP32 band stage)
 };
+
+// FP32 sum of squared FP32 differences in four FMA chains (tree depth <= d / 4 + 2), the FP32
+// band stage's value; certified against the FP64 oracle by fp32_sum_thresholds.
+TJ_DEV float fp32_d2(const float* x, const float* y, int d) {
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    if ((d & 3) == 0 && ((((uintptr_t)x) | ((uintptr_t)y)) & 15) == 0) {
+        const float4* x4 = (const float4*)x;
+        const float4* y4 = (const float4*)y;
+        for (int k = 0; k < d / 4; ++k) {
+            const float4 a = __ldg(x4 + k), b = __ldg(y4 + k);
+            float t;
+            t = a.x - b.x; a0 = fmaf(t, t, a0);
+            t = a.y - b.y; a1 = fmaf(t, t, a1);
+            t = a.z - b.z; a2 = fmaf(t, t, a2);
+            t = a.w - b.w; a3 = fmaf(t, t, a3);
+        }
+    } else {
+        for (int k = 0; k < d; ++k) {
+            const float t = __ldg(x + k) - __ldg(y + k);
+            a0 = fmaf(t, t, a0);
+        }
+    }
+    return (a0 + a1) + (a2 + a3);
+}
 
 TJ_DEV double seq_d2(const float* x, const float* y, int d) {
     double acc = 0.0;
@@ -198,11 +223,14 @@ TJ_DEV double seq_d2(const float* x, const float* y, int d) {
     return acc;
 }
 
+// Band pairs -> accept buffer.  kFp32: each pair is first decided, where it can be, by the
+// certified FP32 sum (the FP32 band stage); only the rest pay the sequential FP64 terminal.
+template <bool kFp32>
 __global__ void refine_kernel(const RefineArgs a) {
     const unsigned long long n = min(a.ctr->band_reserved, a.band_cap);
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     const unsigned long long start = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long n_acc = 0;
+    unsigned long long n_acc = 0, n_fp64 = 0;
     // loop count is warp-uniform so the ballot below is well formed
     const unsigned long long warp_start = start & ~31ull;
     for (unsigned long long w = warp_start; w < n; w += stride) {
@@ -220,10 +248,19 @@ __global__ void refine_kernel(const RefineArgs a) {
                 const JoinParams& jp = a.jps[lo];
                 const uint64_t local = key - jp.key_off;
                 const uint64_t i = local / (uint64_t)jp.n_cols, j = local - i * (uint64_t)jp.n_cols;
-                const float* R = (const float*)a.rsrc[lo];
-                const float* S = (const float*)a.ssrc[lo];
-                const double d2 = seq_d2(R + (size_t)i * jp.d, S + (size_t)j * jp.d, jp.d);
-                ok = d2 <= jp.T;
+                const float* x = (const float*)a.rsrc[lo] + (size_t)i * jp.d;
+                const float* y = (const float*)a.ssrc[lo] + (size_t)j * jp.d;
+                bool decided = false;
+                if (kFp32) {
+                    const float s = fp32_d2(x, y, jp.d);
+                    const float2 th = a.thr[lo];
+                    if (s <= th.x) { ok = true; decided = true; }
+                    else if (s > th.y) { decided = true; }
+                }
+                if (!decided) {
+                    ok = seq_d2(x, y, jp.d) <= jp.T;
+                    ++n_fp64;
+                }
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -242,6 +279,9 @@ __global__ void refine_kernel(const RefineArgs a) {
         atomicAdd(&a.ctr->acc_valid, n_acc);
         atomicAdd(&a.ctr->refine_accept, n_acc);
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n_fp64 += __shfl_xor_sync(0xffffffffu, n_fp64, o);
+    if (lane_id() == 0 && n_fp64) atomicAdd(&a.ctr->band_fp64, n_fp64);
 }
 
 // ------------------------------------------------------------------ canonical output helpers
@@ -302,22 +342,13 @@ __global__ void batch_offsets_kernel(const uint64_t* keys, long long n, const un
 
 }  // namespace
 
-void screen_plain(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
-    PlainArgs a;
-    memset(&a, 0, sizeof(a));
-    for (int c = 0; c < g.ncls; ++c) {
-        const Side& R = *g.R[c];
-        const Side& S = *g.S[c];
-        if (R.screen != kScreenPlain || S.screen != kScreenPlain) fail(-1, "screen_plain needs FP32 sides");
-        a.cls[c].rx = R.xs.p;
-        a.cls[c].sx = S.xs.p;
-        a.cls[c].r_emit = R.emit;
-        a.cls[c].s_emit = S.emit;
-        a.cls[c].d = R.d;
-    }
-    // per join: FP32 sum of d squared FP32 differences with FMA: |s - D| <= gamma_{d+2} D + d 2^-148 (u = 2^-24)
+// Per join, thresholds on an FP32 sum s of the d squared FP32 differences (FMA accumulation, any
+// summation tree of depth <= d + 2): s <= x certifies the FP64 oracle value <= T, s > y certifies
+// it > T.  |s - D| <= gamma_{d+4} D + (d + 4) 2^-147 with u = 2^-24 (one rounding in each
+// difference, one in each FMA or add along the tree, subnormal products absolutely).
+static void fp32_sum_thresholds(const ScreenInput& g, float2* dst, cudaStream_t st) {
     const JoinParams* hj = g.h_jps;
-    if (!hj) fail(-1, "screen_plain needs the host join parameters");
+    if (!hj) fail(-1, "the FP32 thresholds need the host join parameters");
     std::vector<float2> th((size_t)g.njoins);
     for (int k = 0; k < g.njoins; ++k) {
         const double u = 0x1p-24, nu = (double)(hj[k].d + 4) * u;
@@ -331,8 +362,24 @@ void screen_plain(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) 
         if ((double)fout < tout) fout = nextafterf(fout, INFINITY);
         th[k] = make_float2(fin, fout);
     }
+    upload(dst, th.data(), g.njoins * sizeof(float2), st);
+}
+
+void screen_plain(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
+    PlainArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int c = 0; c < g.ncls; ++c) {
+        const Side& R = *g.R[c];
+        const Side& S = *g.S[c];
+        if (R.screen != kScreenPlain || S.screen != kScreenPlain) fail(-1, "screen_plain needs FP32 sides");
+        a.cls[c].rx = R.xs.p;
+        a.cls[c].sx = S.xs.p;
+        a.cls[c].r_emit = R.emit;
+        a.cls[c].s_emit = S.emit;
+        a.cls[c].d = R.d;
+    }
     DBuf<float2> dth((size_t)g.njoins, st);
-    upload(dth.p, th.data(), g.njoins * sizeof(float2), st);
+    fp32_sum_thresholds(g, dth.p, st);
     a.chunks = g.cand->chunks.p;
     a.nchunks = g.cand->dev_counts.p + 1;
     a.jlist = g.cand->jlist.p;
@@ -348,7 +395,7 @@ void screen_plain(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) 
     launch(plain_kernel, num_sms() * 2, kPT, 0, st, a);
 }
 
-void refine_band(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
+void refine_band(const ScreenInput& g, const EmitBuffers& eb, bool fp32_stage, cudaStream_t st) {
     RefineArgs a;
     a.band = eb.band;
     a.band_cap = eb.band_cap;
@@ -360,7 +407,15 @@ void refine_band(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     a.acc = eb.acc;
     a.acc_cap = eb.acc_cap;
     a.ctr = eb.ctr;
-    launch(refine_kernel, num_sms() * 8, 256, 0, st, a);
+    a.thr = nullptr;
+    if (fp32_stage) {
+        DBuf<float2> dth((size_t)g.njoins, st);
+        fp32_sum_thresholds(g, dth.p, st);
+        a.thr = dth.p;
+        launch(refine_kernel<true>, num_sms() * 8, 256, 0, st, a);
+    } else {
+        launch(refine_kernel<false>, num_sms() * 8, 256, 0, st, a);
+    }
 }
 
 void expand_directed(const uint64_t* upper, unsigned long long slots, uint64_t* out, long long N, cudaStream_t st) {

@@ -27,5 +27,14 @@ def test_library_exports_every_declared_symbol():
 
 def test_structs_match_header_layout():
     assert ctypes.sizeof(_lib.Options) == 16
-    assert ctypes.sizeof(_lib.Stats) == 11 * 8 + 9 * 8 + 8 + 8 + 8
+    assert ctypes.sizeof(_lib.Stats) == 11 * 8 + 9 * 8 + 8 + 8 + 8 + 8
     assert ctypes.sizeof(_lib.BatchJoin) == 48
+
+
+def test_flag_constants_match_header():
+    text = HEADER.read_text()
+    flags = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define TJ_FLAG_([A-Z0-9_]+) (\d+)", text)}
+    assert flags, "no TJ_FLAG_* defines found"
+    for name, value in flags.items():
+        assert getattr(_lib, "FLAG_" + name) == value, name
+    assert len(set(flags.values())) == len(flags)

@@ -500,3 +500,42 @@ def test_frame_flags_exclusive():
     rc = _lib.lib().tj_join(C.c_void_p(R.data_ptr()), 300, C.c_void_p(R.data_ptr()), 300, 16, _lib.DTYPE["f32"],
                             0.1, _lib.MODE["rs"], _lib.SCREEN["bf16"], C.byref(opt), C.byref(h), None)
     assert rc != 0 and not h.value
+
+
+@pytest.mark.parametrize("screen", ["bf16", "fp16", "bf16x3", "fp16x3"])
+def test_fp32_band_stage(screen):
+    """The certified FP32 band stage decides most band pairs without FP64 and changes no pair:
+    R-S and both self-join modes, several d, ties at the threshold."""
+    cases = []
+    w = W.mixture64(n=6000, samples=1 << 14)
+    cases.append((w.R, w.S, w.T, "rs"))
+    f = W.factor512(n=2500, samples=1 << 14)
+    cases.append((f.R, f.S, f.T, "rs"))
+    rng = np.random.default_rng(77)
+    for d in (3, 17, 130):
+        X = rng.standard_normal((1800, d)).astype(np.float32)
+        X[1500:1600] = X[:100]                      # d2 == 0 pairs
+        T = float(np.quantile(((X[:50, None, :].astype(np.float64) - X[None, 50:400, :]) ** 2).sum(-1), 0.01))
+        cases.append((X, None, T, "upper"))
+        cases.append((X, None, T, "directed"))
+    for R, S, T, mode in cases:
+        want = oracle_keys(R, S, T, mode)
+        k0, st0 = gpu_keys(R, S, T, mode, screen)
+        k1, st1 = gpu_keys(R, S, T, mode, screen, band_fp32=True)
+        label = f"{screen} {mode} d={R.shape[1]}"
+        assert_same(k0, want, label + " fp64-only")
+        assert_same(k1, want, label + " fp32 stage")
+        assert st0["band_fp64"] == st0["band"], st0
+        assert st1["band_fp64"] <= st1["band"], st1
+
+
+def test_fp32_band_stage_batched():
+    joins = _ragged(24, 43)
+    dev = [(torch.from_numpy(R).cuda(), torch.from_numpy(S).cuda(), float(np.sqrt(T))) for R, S, T in joins]
+    res = tj.join_batched_result(dev, screen="bf16", band_fp32=True)
+    assert res.stats["band_fp64"] <= res.stats["band"]
+    for k, ((R, S, T), (i, j)) in enumerate(zip(joins, res.split())):
+        Tk = float(np.sqrt(T)) ** 2
+        want = oracle.join_f32(R, S, Tk, "rs") if len(R) and len(S) else np.empty(0, np.uint64)
+        got = i.cpu().numpy().astype(np.uint64) * np.uint64(max(len(S), 1)) + j.cpu().numpy().astype(np.uint64)
+        assert_same(got, want, f"fp32 stage join {k}")
