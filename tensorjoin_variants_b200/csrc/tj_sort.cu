@@ -99,7 +99,6 @@ void exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* t
 namespace {
 
 constexpr int kRsThreads = 256;
-constexpr int kRsWarps = kRsThreads / 32;
 constexpr int kRsRounds = 16;                         // keys per thread
 constexpr int kRsTile = kRsThreads * kRsRounds;       // 4096 keys per block
 
@@ -111,16 +110,28 @@ __global__ void __launch_bounds__(kRsThreads) rs_hist(const uint64_t* keys, size
     h[threadIdx.x] = 0;
     __syncthreads();
     const size_t base = (size_t)blockIdx.x * kRsTile;
+    unsigned dg[kRsRounds];   // all loads in flight before the shared-memory counting
+#pragma unroll
     for (int r = 0; r < kRsRounds; ++r) {
         const size_t i = base + (size_t)r * kRsThreads + threadIdx.x;
-        if (i < n) atomicAdd(&h[digit_of(keys[i], shift)], 1u);
+        dg[r] = i < n ? digit_of(keys[i], shift) : 256u;
     }
+#pragma unroll
+    for (int r = 0; r < kRsRounds; ++r)
+        if (dg[r] < 256u) atomicAdd(&h[dg[r]], 1u);
     __syncthreads();
     hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// Block-wide exclusive scan of one value per thread (kRsThreads == 256 values).
-TJ_DEV uint32_t block_excl_scan_256(uint32_t v, uint32_t* warp_tot) {
+// The scatter runs 512 threads over the same 4096-key tile (8 keys per thread): twice the warps
+// of the histogram kernel, to hide the latency of its load, rank and regroup phases.
+constexpr int kScThreads = 512;
+constexpr int kScWarps = kScThreads / 32;
+constexpr int kScRounds = kRsTile / kScThreads;       // 8 keys per thread
+
+// Block-wide exclusive scan of one value per thread over kWarps warps (every thread calls it).
+template <int kWarps>
+TJ_DEV uint32_t block_excl_scan(uint32_t v, uint32_t* warp_tot) {
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned tot;
     const unsigned pre = warp_excl_scan(v, tot);
@@ -128,7 +139,7 @@ TJ_DEV uint32_t block_excl_scan_256(uint32_t v, uint32_t* warp_tot) {
     __syncthreads();
     uint32_t off = 0;
 #pragma unroll
-    for (int w = 0; w < kRsWarps; ++w) off += (w < (int)warp) ? warp_tot[w] : 0u;
+    for (int w = 0; w < kWarps; ++w) off += (w < (int)warp) ? warp_tot[w] : 0u;
     return off + pre;
 }
 
@@ -137,34 +148,35 @@ TJ_DEV uint32_t block_excl_scan_256(uint32_t v, uint32_t* warp_tot) {
 // out in that order, so consecutive threads store consecutive addresses of one digit's run
 // (about 16 keys = 128 B per digit and tile for 8-bit digits) instead of scattered 8-byte words.
 template <bool kVals>
-__global__ void __launch_bounds__(kRsThreads) rs_scatter(const uint64_t* keys_in, const uint32_t* vals_in,
+__global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) rs_scatter(const uint64_t* keys_in, const uint32_t* vals_in,
                                                         uint64_t* keys_out, uint32_t* vals_out, size_t n, int shift,
                                                         const uint32_t* offs, unsigned nblocks) {
     extern __shared__ __align__(16) unsigned char rs_dyn[];
     uint64_t* sk = (uint64_t*)rs_dyn;                      // [kRsTile] keys grouped by digit
     uint32_t* sv = (uint32_t*)(rs_dyn + kRsTile * 8);      // [kRsTile] values (kVals)
-    __shared__ uint32_t wcnt[kRsWarps][256];
-    __shared__ uint32_t gbase[256];    // global start of each digit's run for this tile
-    __shared__ uint32_t lstart[256];   // tile-local start of each digit's run
-    __shared__ uint32_t wtot[kRsWarps];
+    __shared__ uint32_t wcnt[kScWarps][256];   // per warp and digit: count, then tile-local start
+    __shared__ uint32_t gdelta[256];   // global start minus tile-local start of each digit's run (mod 2^32)
+    __shared__ uint32_t wtot[kScWarps];
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < kRsWarps * 256; i += kRsThreads) (&wcnt[0][0])[i] = 0;
-    gbase[threadIdx.x] = offs[(size_t)threadIdx.x * nblocks + blockIdx.x];
+    for (int i = threadIdx.x; i < kScWarps * 256; i += kScThreads) (&wcnt[0][0])[i] = 0;
+    const uint32_t gbase = threadIdx.x < 256 ? offs[(size_t)threadIdx.x * nblocks + blockIdx.x] : 0u;
     __syncthreads();
 
-    // warp w owns the contiguous run [w*512, (w+1)*512) of this block's tile; round r, lane l -> r*32 + l
+    // warp w owns the contiguous run [w*256, (w+1)*256) of this block's tile; round r, lane l -> r*32 + l
     const size_t tbase = (size_t)blockIdx.x * kRsTile;
-    const size_t wbase = tbase + (size_t)warp * (kRsRounds * 32);
-    uint64_t k[kRsRounds];
-    uint32_t v[kRsRounds];
-    uint32_t rank[kRsRounds];
+    const size_t wbase = tbase + (size_t)warp * (kScRounds * 32);
+    uint64_t k[kScRounds];
+    uint32_t v[kScRounds];
+    uint32_t rank[kScRounds];
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
-    for (int r = 0; r < kRsRounds; ++r) {
+    for (int r = 0; r < kScRounds; ++r) {
         const size_t i = wbase + (size_t)r * 32 + lane;
-        const bool ok = i < n;
-        k[r] = ok ? keys_in[i] : 0ull;
-        if (kVals) v[r] = ok ? vals_in[i] : 0u;
+        k[r] = i < n ? keys_in[i] : 0ull;
+    }
+#pragma unroll
+    for (int r = 0; r < kScRounds; ++r) {
+        const bool ok = wbase + (size_t)r * 32 + lane < n;
         const unsigned valid = __ballot_sync(0xffffffffu, ok);
         rank[r] = 0xFFFFFFFFu;
         if (ok) {
@@ -177,34 +189,48 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter(const uint64_t* keys_in
         }
         __syncwarp();
     }
+    if (kVals) {   // values load while the block meets at the barrier (fewer live registers above)
+#pragma unroll
+        for (int r = 0; r < kScRounds; ++r) {
+            const size_t i = wbase + (size_t)r * 32 + lane;
+            v[r] = i < n ? vals_in[i] : 0u;
+        }
+    }
     __syncthreads();
-    {   // exclusive prefix over warps for each digit, then over digits for the tile
+    {   // per digit (threads 0..255): total over warps, tile-local start by a block scan, then each
+        // warp's start of that digit's run (one shared read per key in the regroup below)
         const unsigned dg = threadIdx.x;
         uint32_t run = 0;
+        if (dg < 256) {
 #pragma unroll
-        for (int w = 0; w < kRsWarps; ++w) {
-            const uint32_t t = wcnt[w][dg];
-            wcnt[w][dg] = run;
-            run += t;
+            for (int w = 0; w < kScWarps; ++w) run += wcnt[w][dg];
         }
-        lstart[dg] = block_excl_scan_256(run, wtot);
+        const uint32_t ls = block_excl_scan<kScWarps>(run, wtot);
+        if (dg < 256) {
+            uint32_t at = ls;
+#pragma unroll
+            for (int w = 0; w < kScWarps; ++w) {
+                const uint32_t t = wcnt[w][dg];
+                wcnt[w][dg] = at;
+                at += t;
+            }
+            gdelta[dg] = gbase - ls;
+        }
     }
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < kRsRounds; ++r) {
+    for (int r = 0; r < kScRounds; ++r) {
         if (rank[r] != 0xFFFFFFFFu) {
-            const unsigned dg = digit_of(k[r], shift);
-            const unsigned p = lstart[dg] + wcnt[warp][dg] + rank[r];
+            const unsigned p = wcnt[warp][digit_of(k[r], shift)] + rank[r];
             sk[p] = k[r];
             if (kVals) sv[p] = v[r];
         }
     }
     __syncthreads();
     const unsigned cnt = (unsigned)min((size_t)kRsTile, n - tbase);
-    for (unsigned p = threadIdx.x; p < cnt; p += kRsThreads) {
+    for (unsigned p = threadIdx.x; p < cnt; p += kScThreads) {
         const uint64_t key = sk[p];
-        const unsigned dg = digit_of(key, shift);
-        const size_t pos = (size_t)gbase[dg] + (p - lstart[dg]);
+        const size_t pos = (size_t)(uint32_t)(gdelta[digit_of(key, shift)] + p);
         keys_out[pos] = key;
         if (kVals) vals_out[pos] = sv[p];
     }
@@ -226,7 +252,11 @@ void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* va
     if (n >= (1ull << 32)) fail(-1, "radix_sort: more than 2^32 - 1 keys");
     const size_t dyn_k = (size_t)kRsTile * 8, dyn_kv = (size_t)kRsTile * 12;
     TJ_CUDA(cudaFuncSetAttribute(rs_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_k));
-    if (vals) TJ_CUDA(cudaFuncSetAttribute(rs_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_kv));
+    TJ_CUDA(cudaFuncSetAttribute(rs_scatter<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    if (vals) {
+        TJ_CUDA(cudaFuncSetAttribute(rs_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_kv));
+        TJ_CUDA(cudaFuncSetAttribute(rs_scatter<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    }
     const unsigned nb = (unsigned)((n + kRsTile - 1) / kRsTile);
     const size_t h = 256 * (size_t)nb;
     uint32_t* hist = ws;
@@ -240,9 +270,9 @@ void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* va
         launch(rs_hist, nb, kRsThreads, 0, st, kin, n, shift, hist, nb);
         exclusive_scan_u32(hist, offs, h, nullptr, sws, st);
         if (vals)
-            launch(rs_scatter<true>, nb, kRsThreads, dyn_kv, st, kin, vin, kout, vout, n, shift, offs, nb);
+            launch(rs_scatter<true>, nb, kScThreads, dyn_kv, st, kin, vin, kout, vout, n, shift, offs, nb);
         else
-            launch(rs_scatter<false>, nb, kRsThreads, dyn_k, st, kin, nullptr, kout, nullptr, n, shift, offs, nb);
+            launch(rs_scatter<false>, nb, kScThreads, dyn_k, st, kin, nullptr, kout, nullptr, n, shift, offs, nb);
         std::swap(kin, kout);
         std::swap(vin, vout);
     }
