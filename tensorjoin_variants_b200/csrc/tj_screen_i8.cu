@@ -21,7 +21,9 @@
 // exact INT64 test.  (The data-independent bound M = d (128 * 8192 + 4096) is ~3x looser on
 // uniform int14 rows and sent ~10x more pairs to the exact test.)
 //
-// TMEM: hh double-buffered (columns 0..255), x and ll single (256..511).  The UMMA
+// TMEM: hh double-buffered (columns 0..255), x and ll single (256..511).  The hh products of an
+// item are committed on their own barrier before its x / ll products are issued, so the epilogue's
+// fast path (hh only) overlaps the x / ll products; the rare path waits for them.  The UMMA
 // issuer runs the hh products of item n+1 while the epilogue still reads x / ll of item n.
 // Warp roles (320 threads): warp 0 TMA producer, warp 1 UMMA issuer, warps 2..9 epilogue
 // (warp w reads TMEM lanes 32*(w%4).. and columns 64*((w-2)/4)..).
@@ -62,6 +64,7 @@ struct I8Ctl {
     uint64_t acc_full[2];
     uint64_t hh_empty[2];
     uint64_t xl_empty;
+    uint64_t xl_full;      // x and ll of the current item are in TMEM
     uint64_t meta_full[kI8Meta];
     uint64_t meta_empty[kI8Meta];
     uint64_t drain;
@@ -142,6 +145,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             mbar_init(&ctl->hh_empty[b], kI8Epi);
         }
         mbar_init(&ctl->xl_empty, kI8Epi);
+        mbar_init(&ctl->xl_full, 1);
         for (int m = 0; m < kI8Meta; ++m) {
             mbar_init(&ctl->meta_full[m], 1);
             mbar_init(&ctl->meta_empty[m], kI8Epi);
@@ -220,6 +224,9 @@ __global__ void __launch_bounds__(kI8Threads, 1)
 #pragma unroll
                         for (int k = 0; k < 4; ++k)
                             umma_i8(t_hh, desc_sw128(Ah, k * 32), desc_sw128(Bh, k * 32), a.idesc, (kb | k) != 0);
+                        // hh is complete after the last k-block's hh products: release it to the
+                        // epilogue now, so its fast path overlaps this item's x / ll products
+                        if (kb == a.kblocks - 1) umma_commit(&ctl->acc_full[b]);
                         if (kb == 0) {   // x / ll of the previous item must have been read
                             if (!mbar_wait(&ctl->xl_empty, (unsigned)(n & 1) ^ 1u, status)) { ok = false; break; }
                             tc_fence_after();
@@ -234,7 +241,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                         if (++stage == kI8Stages) { stage = 0; phase ^= 1; }
                     }
                     if (!ok) break;
-                    umma_commit(&ctl->acc_full[b]);
+                    umma_commit(&ctl->xl_full);
                 }
             }
             if (!ok) ctl->abort_flag = 1;
@@ -278,6 +285,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                 }
                 const unsigned lane_off = (q * 32u) << 16;
                 const unsigned col0 = half * 64;
+                bool xl_seen = false;
 #pragma unroll 1
                 for (int h = 0; h < 2; ++h) {
                     const unsigned cc = col0 + h * 32;
@@ -321,6 +329,14 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                         else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
                     }
                     if (!__any_sync(0xffffffffu, cmask != 0)) continue;
+                    // every epilogue warp observes each phase of xl_full (here, or at the end of the
+                    // item), so the parity below names this item's products and no other
+                    if (!xl_seen) {
+                        const bool xl_ok = mbar_wait(&ctl->xl_full, (unsigned)(n & 1), status);
+                        if (!__all_sync(0xffffffffu, xl_ok)) { ok = false; break; }   // warp-uniform exit
+                        xl_seen = true;
+                    }
+                    tc_fence_after();
                     uint32_t xv[32], lv[32];
                     tmem_ld32(tmem + lane_off + kColX + cc, xv);
                     tmem_ld32(tmem + lane_off + kColLL + cc, lv);
@@ -349,6 +365,11 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                         n_acc += __popc(amask);
                     }
                 }
+                if (ok && !xl_seen) {
+                    const bool xl_ok = mbar_wait(&ctl->xl_full, (unsigned)(n & 1), status);
+                    ok = __all_sync(0xffffffffu, xl_ok);
+                }
+                if (!ok) break;
                 // this item's hh buffer, the shared x / ll and the metadata slot are free again
                 tc_fence_before();
                 __syncwarp();
