@@ -1,0 +1,93 @@
+"""Autotuner host logic on the CPU (selection, keys, persistence) and, on a GPU, tuned joins
+that give the oracle's pairs and reuse the table."""
+import json
+
+import numpy as np
+import pytest
+
+from tensorjoin_variants_b200 import autotune as A
+
+
+def test_candidates_cover_only_what_applies():
+    c512 = A.candidates(512, "fp16", "rs")
+    assert {c.cta_pair for c in c512} == {True, False}
+    assert {c.index_frame for c in c512} == {"auto"}            # d > 128: no principal-direction cells
+    assert {c.band_fp32 for c in c512} == {False, True}
+    assert {c.chunk_items for c in c512} == set(A.CHUNK_ITEMS)
+    c64 = A.candidates(64, "bf16x3", "upper")
+    assert {c.cta_pair for c in c64} == {True}                  # self-join / d < 256: one-SM screen only
+    assert {c.index_frame for c in c64} == {"axes", "pca"}
+    ci = A.candidates(128, "int8limb", "upper")
+    assert {c.band_fp32 for c in ci} == {False}                 # exact screen: no band
+    assert len(set(c512)) == len(c512)
+
+
+def test_tune_key_buckets():
+    k = A.tune_key(64, "f32", "bf16x3", "rs", 1 << 20, 1 << 20, 15.0)
+    assert k == "d64/f32/bf16x3/rs/space2^40/sel2^4"
+    assert A.tune_key(64, "f32", "bf16x3", "rs", 1 << 20, 1 << 20, 16.5) == k   # same bucket
+    assert A.tune_key(64, "f32", "bf16x3", "rs", 1 << 20, 1 << 20, 0.0).endswith("sel2^0")
+    assert A.tune_key(64, "f32", "bf16x3", "rs", 1 << 21, 1 << 20, 15.0) != k
+
+
+def test_pick_fastest_by_best_time_and_ties_to_first():
+    cands = [A.Choice(chunk_items=c) for c in (16, 64, 256)]
+    times = {16: [5.0, 4.0], 64: [3.0, 3.5], 256: [3.0, 9.0]}
+    calls = {c: 0 for c in (16, 64, 256)}
+
+    def runner(ch):
+        k = ch.chunk_items
+        t = times[k][calls[k]]
+        calls[k] += 1
+        return t, 1234
+
+    best, timings, count = A.Tuner.pick(cands, runner, reps=2)
+    assert best.chunk_items == 64 and count == 1234
+    assert len(timings) == 3 and min(timings.values()) == 3.0
+    assert all(v == 2 for v in calls.values())
+
+
+def test_pick_rejects_a_choice_that_changes_the_pairs():
+    cands = [A.Choice(chunk_items=16), A.Choice(chunk_items=64)]
+    with pytest.raises(RuntimeError):
+        A.Tuner.pick(cands, lambda ch: (1.0, 10 if ch.chunk_items == 16 else 11), reps=1)
+
+
+def test_table_persists(tmp_path):
+    path = str(tmp_path / "tune.json")
+    t = A.Tuner(path)
+    choice = A.Choice(cta_pair=False, chunk_items=256, index_frame="pca", band_fp32=True)
+    t.record("d64/f32/bf16/rs/space2^30/sel2^3", choice, {"x": 1.5})
+    again = A.Tuner(path)
+    assert again.lookup("d64/f32/bf16/rs/space2^30/sel2^3") == choice
+    assert again.lookup("missing") is None
+    assert json.load(open(path))["d64/f32/bf16/rs/space2^30/sel2^3"]["ms"] == {"x": 1.5}
+
+
+@pytest.mark.gpu
+def test_tuned_join_matches_oracle_and_reuses_the_table(tmp_path):
+    import torch
+
+    import oracle
+    from tensorjoin_variants_b200 import workloads as W
+
+    w = W.mixture64(n=9000, samples=1 << 14)
+    R, S = torch.from_numpy(w.R).cuda(), torch.from_numpy(w.S).cuda()
+    tuner = A.Tuner(str(tmp_path / "t.json"))
+    n_tunes = []
+    orig = tuner.tune
+
+    def counting_tune(*a, **k):
+        n_tunes.append(1)
+        return orig(*a, **k)
+
+    tuner.tune = counting_tune
+    want = oracle.join_f32(w.R, w.S, w.T, "rs")
+    for _ in range(2):
+        res = tuner.join(R, S, eps2=w.T, screen="bf16x3", sample_rows=2048)
+        got = res.keys().cpu().numpy().view(np.uint64)
+        assert np.array_equal(got, want)
+    assert len(n_tunes) == 1                       # the second join found its key in the table
+    X = torch.from_numpy(w.R[:4000]).cuda()
+    res = tuner.join(X, None, eps2=w.T, mode="upper", screen="fp16", sample_rows=1024)
+    assert np.array_equal(res.keys().cpu().numpy().view(np.uint64), oracle.join_f32(w.R[:4000], None, w.T, "upper"))
