@@ -539,9 +539,19 @@ __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kp
     long long sq = 0;
     unsigned flags = 0;   // 1: bad input, 2: FP16 range
     const int opw = kSplit ? 2 * kpad : kpad;
-    for (int k = sub; k < kpad && live; k += kL) {
-        float x = 0.f;
-        if (real && k < d) x = load_x(src, dtype, orig * d + k);
+    constexpr int kU = 4;   // elements per lane whose loads are issued together
+    for (int k0 = sub; k0 < kpad && live; k0 += kU * kL) {
+      float xv[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+          const int k = k0 + u * kL;
+          xv[u] = (real && k < d) ? load_x(src, dtype, orig * d + k) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int k = k0 + u * kL;
+        if (k >= kpad) break;
+        float x = xv[u];
         if (!isfinite(x)) { flags |= 1u; x = 0.f; }
         if (kScreen == kScreenPlain) {
             if (k < d) xs[(size_t)r * d + k] = x;
@@ -577,6 +587,7 @@ __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kp
             sz += z * z;
             se += ed * ed;
         }
+      }
     }
 #pragma unroll
     for (int o = kL / 2; o > 0; o >>= 1) {
@@ -638,13 +649,31 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
             pmin[grp * d + k] = INFINITY;
             pmax[grp * d + k] = -INFINITY;
         }
-        for (int i = grp; i < nv; i += kNG) {
-            const size_t base = (size_t)perm[r0 + i] * d;
+        constexpr int kU = 4;   // rows of a group whose loads are issued together
+        for (int i = grp; i < nv; i += kU * kNG) {
+            size_t base[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int ii = i + u * kNG;
+                base[u] = ii < nv ? (size_t)perm[r0 + ii] * d : 0;
+            }
             for (int k = sub; k < d; k += kL) {
-                const float v = load_x(src, dtype, base + k);
-                psum[grp * d + k] += v;
-                pmin[grp * d + k] = fminf(pmin[grp * d + k], v);
-                pmax[grp * d + k] = fmaxf(pmax[grp * d + k], v);
+                float v[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) v[u] = i + u * kNG < nv ? load_x(src, dtype, base[u] + k) : 0.f;
+                double sm = psum[grp * d + k];
+                float mn = pmin[grp * d + k], mx = pmax[grp * d + k];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    if (i + u * kNG < nv) {
+                        sm += v[u];
+                        mn = fminf(mn, v[u]);
+                        mx = fmaxf(mx, v[u]);
+                    }
+                }
+                psum[grp * d + k] = sm;
+                pmin[grp * d + k] = mn;
+                pmax[grp * d + k] = mx;
             }
         }
         __syncthreads();
@@ -683,19 +712,35 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
     // radius: kL lanes per row, exact FP64 differences against the FP32 centroid; the row loop is
     // uniform across each warp so that every lane takes part in the shuffles
     double rmax = 0.0;
-    for (int i0 = warp * (32 / kL); i0 < nv; i0 += kNG) {
-        const int i = i0 + (int)(lane / kL);
-        double s = 0.0;
-        if (i < nv) {
-            const size_t base = (size_t)perm[r0 + i] * d;
-            for (int k = sub; k < d; k += kL) {
-                const double df = (double)load_x(src, dtype, base + k) - (double)s_ctr[k];
-                s += df * df;
+    constexpr int kRU = 2;   // rows per lane group whose loads are issued together
+    for (int i0 = warp * (32 / kL); i0 < nv; i0 += kRU * kNG) {
+        double s[kRU];
+        size_t base[kRU];
+        bool ok[kRU];
+#pragma unroll
+        for (int u = 0; u < kRU; ++u) {
+            const int i = i0 + u * kNG + (int)(lane / kL);
+            ok[u] = i < nv;
+            base[u] = ok[u] ? (size_t)perm[r0 + i] * d : 0;
+            s[u] = 0.0;
+        }
+        for (int k = sub; k < d; k += kL) {
+            float v[kRU];
+#pragma unroll
+            for (int u = 0; u < kRU; ++u) v[u] = ok[u] ? load_x(src, dtype, base[u] + k) : 0.f;
+            const double c = (double)s_ctr[k];
+#pragma unroll
+            for (int u = 0; u < kRU; ++u) {
+                const double df = (double)v[u] - c;
+                if (ok[u]) s[u] += df * df;
             }
         }
 #pragma unroll
-        for (int o = kL / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        rmax = fmax(rmax, s);
+        for (int u = 0; u < kRU; ++u) {
+#pragma unroll
+            for (int o = kL / 2; o > 0; o >>= 1) s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
+            rmax = fmax(rmax, s[u]);
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
