@@ -236,6 +236,95 @@ __global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) rs_scatter(const ui
     }
 }
 
+// Whole sort of a small array (n <= kSmallSort) in one CTA: per pass a histogram of all keys and
+// its scan give each digit's start, then the 4096-key chunks are ranked in order exactly as in
+// rs_scatter (16 warps, __match_any_sync) and written to their final positions; the running digit
+// starts carry stability across chunks.  Keys ping-pong through global memory (L2-resident at this
+// size); __syncthreads orders each pass's writes before the next pass's reads within the block.
+// One launch replaces the four to five launches per pass of the multi-block path.
+constexpr unsigned kSmallSort = 16384;
+
+template <bool kVals>
+__global__ void __launch_bounds__(kScThreads) rs_small(uint64_t* keys, uint32_t* vals, uint64_t* ktmp,
+                                                      uint32_t* vtmp, unsigned n, int passes) {
+    __shared__ uint32_t wcnt[kScWarps][256];
+    __shared__ uint32_t base[256];     // this pass: next output position of each digit
+    __shared__ uint32_t wtot[kScWarps];
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
+    const unsigned lt = (1u << lane) - 1u;
+    uint64_t *kin = keys, *kout = ktmp;
+    uint32_t *vin = vals, *vout = vtmp;
+    for (int pass = 0; pass < passes; ++pass) {
+        const int shift = 8 * pass;
+        if (t < 256) base[t] = 0;
+        __syncthreads();
+        for (unsigned i = t; i < n; i += kScThreads) atomicAdd(&base[digit_of(kin[i], shift)], 1u);
+        __syncthreads();
+        const uint32_t cnt = t < 256 ? base[t] : 0u;
+        const uint32_t ex = block_excl_scan<kScWarps>(cnt, wtot);
+        __syncthreads();                       // every thread has read base[] for its count
+        if (t < 256) base[t] = ex;
+        for (unsigned c0 = 0; c0 < n; c0 += kRsTile) {
+            for (int i = t; i < kScWarps * 256; i += kScThreads) (&wcnt[0][0])[i] = 0;
+            __syncthreads();
+            const unsigned wbase = c0 + warp * (kScRounds * 32);
+            uint64_t k[kScRounds];
+            uint32_t rank[kScRounds];
+#pragma unroll
+            for (int r = 0; r < kScRounds; ++r) {
+                const unsigned i = wbase + r * 32 + lane;
+                k[r] = i < n ? kin[i] : 0ull;
+            }
+#pragma unroll
+            for (int r = 0; r < kScRounds; ++r) {
+                const bool ok = wbase + r * 32 + lane < n;
+                const unsigned valid = __ballot_sync(0xffffffffu, ok);
+                rank[r] = 0xFFFFFFFFu;
+                if (ok) {
+                    const unsigned dg = digit_of(k[r], shift);
+                    const unsigned peers = __match_any_sync(valid, dg);
+                    const unsigned prev = wcnt[warp][dg];
+                    rank[r] = prev + __popc(peers & lt);
+                    __syncwarp(valid);
+                    if ((peers & lt) == 0) wcnt[warp][dg] = prev + __popc(peers);
+                }
+                __syncwarp();
+            }
+            __syncthreads();
+            if (t < 256) {   // each warp's start of digit t in this chunk; advance the digit's start
+                uint32_t at = base[t];
+#pragma unroll
+                for (int w = 0; w < kScWarps; ++w) {
+                    const uint32_t c = wcnt[w][t];
+                    wcnt[w][t] = at;
+                    at += c;
+                }
+                base[t] = at;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < kScRounds; ++r) {
+                if (rank[r] != 0xFFFFFFFFu) {
+                    const unsigned i = wbase + r * 32 + lane;
+                    const unsigned pos = wcnt[warp][digit_of(k[r], shift)] + rank[r];
+                    kout[pos] = k[r];
+                    if (kVals) vout[pos] = vin[i];
+                }
+            }
+            __syncthreads();   // wcnt is reused by the next chunk
+        }
+        uint64_t* tk = kin; kin = kout; kout = tk;
+        uint32_t* tv = vin; vin = vout; vout = tv;
+        __syncthreads();       // this pass's writes are read by the next pass
+    }
+    if (kin != keys) {         // odd number of passes: the result is in the temporaries
+        for (unsigned i = t; i < n; i += kScThreads) {
+            keys[i] = kin[i];
+            if (kVals) vals[i] = vin[i];
+        }
+    }
+}
+
 }  // namespace
 
 size_t radix_workspace_elems(size_t n) {
@@ -250,6 +339,15 @@ void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* va
                 uint32_t* ws, cudaStream_t st) {
     if (n <= 1 || bits <= 0) return;
     if (n >= (1ull << 32)) fail(-1, "radix_sort: more than 2^32 - 1 keys");
+    if (n <= kSmallSort) {
+        const int passes = (bits + 7) / 8;
+        if (vals)
+            launch(rs_small<true>, 1, kScThreads, 0, st, keys, vals, keys_tmp, vals_tmp, (unsigned)n, passes);
+        else
+            launch(rs_small<false>, 1, kScThreads, 0, st, keys, (uint32_t*)nullptr, keys_tmp, (uint32_t*)nullptr,
+                   (unsigned)n, passes);
+        return;
+    }
     const size_t dyn_k = (size_t)kRsTile * 8, dyn_kv = (size_t)kRsTile * 12;
     TJ_CUDA(cudaFuncSetAttribute(rs_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_k));
     TJ_CUDA(cudaFuncSetAttribute(rs_scatter<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
