@@ -513,6 +513,8 @@ def ragged_bench(args, rank, world, screen, dist):
                      "screen_ms": screen_ms, "flops_per_launch": ops},
         "clocks": clk, "gpu_launches": int(launches), "result_pairs": int(pairs_out),
         "step_ms": step_ms, "lib_ms_total": [s["ms_total"] for s in stats],
+        "stage_ms_per_step": [{k[3:]: round(s[k], 3) for k in ("ms_index", "ms_candidates", "ms_screen", "ms_refine",
+                                                               "ms_sort")} for s in stats],
         "batch": {"joins_per_s": nj / (ms / 1000.0), "ms_per_join_amortised": ms / nj,
                   "single_join_latency_ms_p50": float(np.percentile(lat, 50)),
                   "single_join_latency_ms_p99": float(np.percentile(lat, 99)), "latency_sample": len(lat)},

@@ -83,6 +83,12 @@ TJ_DEV float fmin3(float a, float b, float c) {
     return r;
 }
 
+TJ_DEV float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // exclusive warp prefix sum of v (all 32 lanes participate)
 TJ_DEV unsigned warp_excl_scan(unsigned v, unsigned& total) {
     unsigned x = v;

@@ -43,6 +43,7 @@
 //           group (w-4)/4 takes whole half-items (4 blocks of 32 columns); pair: column thirds of every
 //           item (blocks [0,3), [3,6), [6,8)).  Warps synchronise only through mbarriers.
 //   warps 2-3: idle (they complete the first warpgroup)
+#include <cstddef>
 #include <algorithm>
 #include <cstring>
 
@@ -80,10 +81,12 @@ struct ColMetaF {
     float zl[kTileS];      // >= ||w_lo||
     uint32_t perm[kTileS]; // original row id
     double nrm2[kTileS];   // ||y - c||^2 (FP64)
+    float gminB[kTileS / 8];   // per 8-column group: min of nrm2f (the group-wise fast test)
     float WJ, FJ, YJ, BJ, betaJ, WlJ;   // tile maxima of zn, en, yn, nrm2f, |nrm2f - nrm2| bound, zl
     uint32_t c0, nvJ;      // first sorted row, rows that are real points
 };
 static_assert(sizeof(ColMetaF) % 16 == 0, "bulk copies need 16-byte multiples");
+static_assert(offsetof(ColMetaF, gminB) % 16 == 0, "group minima are read four at a time");
 
 template <int kStages>
 struct ScreenCtl {
@@ -116,6 +119,8 @@ constexpr size_t screen_smem() {
     return 1024 + (size_t)Cfg::kStages * Cfg::kBytes + (size_t)kMetaSlots * sizeof(ColMetaF) +
            sizeof(ScreenCtl<Cfg::kStages>);
 }
+static_assert(screen_smem<0, false>() <= 232448 && screen_smem<1, false>() <= 232448 &&
+              screen_smem<0, true>() <= 232448, "227 KB of shared memory per CTA at most");
 
 // Per-class pointers (a class = joins with the same d, one concatenated operand matrix per side).
 struct ScreenClassArgs {
@@ -196,6 +201,11 @@ __global__ void __launch_bounds__(kTileS) build_col_meta(const uint32_t* row0, c
     m.zl[t] = ok ? zl[r] : 0.f;
     m.perm[t] = ok ? perm[r] : 0u;
     m.nrm2[t] = ok ? nrm2[r] : 0.0;
+    float gb = ok ? nrm2f[r] : INFINITY;   // min over the 8 columns t & ~7 .. (t | 7)
+    gb = fminf(gb, __shfl_xor_sync(0xffffffffu, gb, 1));
+    gb = fminf(gb, __shfl_xor_sync(0xffffffffu, gb, 2));
+    gb = fminf(gb, __shfl_xor_sync(0xffffffffu, gb, 4));
+    if ((t & 7) == 0) m.gminB[t >> 3] = gb;
     if (t == 0) {
         m.WJ = maxZ[J]; m.FJ = maxE[J]; m.YJ = maxY[J]; m.BJ = maxB[J]; m.betaJ = beta[J]; m.WlJ = maxZl[J];
         m.c0 = c0; m.nvJ = nv;
@@ -494,22 +504,43 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                             else mbar_arrive(&ctl->acc_empty[b]);
                         }
                     }
-                    // fast path: v = fma(-2, p, B~) two pairs per packed FMA, folded by three-input mins
-                    // (one instruction per pair), one min chain per 8-column group; only the groups whose
-                    // minimum passes tau (in any lane of the warp) are examined pair by pair
-                    const float4* nb4 = reinterpret_cast<const float4*>(&m.nrm2f[col0]);
                     float vm[4];
+                    if (kPair) {
+                        // dense joins (CTA pair): one test per 8-column group, w = fma(-2, max p, min B~),
+                        // a lower bound of every pair's v = fma(-2, p, B~) in the group with the same
+                        // magnitude bounds (so the same rounding allowance in tau); four three-input maxes
+                        // and one FMA per 8 pairs
+                        const float4 gb = *reinterpret_cast<const float4*>(&m.gminB[col0 >> 3]);
+                        const float gbv[4] = {gb.x, gb.y, gb.z, gb.w};
 #pragma unroll
-                    for (int g = 0; g < 4; ++g) {
-                        const float4 b0 = nb4[2 * g], b1 = nb4[2 * g + 1];
-                        const uint32_t* r8 = raw + 8 * g;
-                        float v0, v1, v2, v3, v4, v5, v6, v7;
-                        fma_m2_x2(__uint_as_float(r8[0]), __uint_as_float(r8[1]), b0.x, b0.y, v0, v1);
-                        fma_m2_x2(__uint_as_float(r8[2]), __uint_as_float(r8[3]), b0.z, b0.w, v2, v3);
-                        fma_m2_x2(__uint_as_float(r8[4]), __uint_as_float(r8[5]), b1.x, b1.y, v4, v5);
-                        fma_m2_x2(__uint_as_float(r8[6]), __uint_as_float(r8[7]), b1.z, b1.w, v6, v7);
-                        vm[g] = fmin3(fmin3(fmin3(v0, v1, v2), v3, v4), fminf(v5, v6), v7);
+                        for (int g = 0; g < 4; ++g) {
+                            const uint32_t* r8 = raw + 8 * g;
+                            const float pm = fmax3(fmax3(fmax3(__uint_as_float(r8[0]), __uint_as_float(r8[1]),
+                                                               __uint_as_float(r8[2])),
+                                                         __uint_as_float(r8[3]), __uint_as_float(r8[4])),
+                                                   fmaxf(__uint_as_float(r8[5]), __uint_as_float(r8[6])),
+                                                   __uint_as_float(r8[7]));
+                            vm[g] = fmaf(-2.f, pm, gbv[g]);
+                        }
+                    } else {
+                        // v = fma(-2, p, B~) two pairs per packed FMA, folded by three-input mins (one
+                        // instruction per pair), one min chain per 8-column group: exact per column, which
+                        // matters where the norms vary inside a group (clustered data)
+                        const float4* nb4 = reinterpret_cast<const float4*>(&m.nrm2f[col0]);
+#pragma unroll
+                        for (int g = 0; g < 4; ++g) {
+                            const float4 b0 = nb4[2 * g], b1 = nb4[2 * g + 1];
+                            const uint32_t* r8 = raw + 8 * g;
+                            float v0, v1, v2, v3, v4, v5, v6, v7;
+                            fma_m2_x2(__uint_as_float(r8[0]), __uint_as_float(r8[1]), b0.x, b0.y, v0, v1);
+                            fma_m2_x2(__uint_as_float(r8[2]), __uint_as_float(r8[3]), b0.z, b0.w, v2, v3);
+                            fma_m2_x2(__uint_as_float(r8[4]), __uint_as_float(r8[5]), b1.x, b1.y, v4, v5);
+                            fma_m2_x2(__uint_as_float(r8[6]), __uint_as_float(r8[7]), b1.z, b1.w, v6, v7);
+                            vm[g] = fmin3(fmin3(fmin3(v0, v1, v2), v3, v4), fminf(v5, v6), v7);
+                        }
                     }
+                    // only the groups whose value passes tau (in any lane of the warp) are examined pair
+                    // by pair
                     const unsigned gmask = (vm[0] <= tau ? 1u : 0u) | (vm[1] <= tau ? 2u : 0u) |
                                            (vm[2] <= tau ? 4u : 0u) | (vm[3] <= tau ? 8u : 0u);
                     const unsigned gunion = __reduce_or_sync(0xffffffffu, gmask);
