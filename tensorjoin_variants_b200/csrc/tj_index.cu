@@ -124,29 +124,43 @@ __global__ void __launch_bounds__(256) dim_reduce(const float* pmin, const float
     }
 }
 
-// Pick the m = min(d, 8) highest-variance dimensions and their quantisation frame.
-__global__ void frame_pick(int d, const float* var_ws, const float* lo_ws, const float* hi_ws, FrameParams* fp) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const int m = min(d, 8), bits = 32 / m;
+// Pick the m = min(d, 8) highest-variance dimensions and their quantisation frame (one warp: each
+// round a lane-strided scan and a warp arg-max, ties to the lowest dimension).
+__global__ void __launch_bounds__(32) frame_pick(int d, const float* var_ws, const float* lo_ws, const float* hi_ws,
+                                                 FrameParams* fp) {
+    const int lane = threadIdx.x, m = min(d, 8), bits = 32 / m;
     int dims[8];
     for (int t = 0; t < m; ++t) {
         int best = -1;
-        for (int k = 0; k < d; ++k) {
+        float bv = 0.f;
+        for (int k = lane; k < d; k += 32) {
             bool used = false;
             for (int u = 0; u < t; ++u) used |= (dims[u] == k);
             if (used) continue;
-            if (best < 0 || var_ws[k] > var_ws[best]) best = k;
+            if (best < 0 || var_ws[k] > bv) { best = k; bv = var_ws[k]; }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {   // arg-max over lanes; no candidate < any candidate
+            const int ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const bool take = ob >= 0 && (best < 0 || ov > bv || (ov == bv && ob < best));
+            if (take) { best = ob; bv = ov; }
         }
         dims[t] = best;
+    }
+    if (lane < m) {
+        const int best = dims[lane];
         const float lo = lo_ws[best], hi = hi_ws[best];
         const float range = (isfinite(lo) && isfinite(hi) && hi > lo) ? hi - lo : 1.f;
-        fp->dims[t] = best;
-        fp->lo[t] = isfinite(lo) ? lo : 0.f;
-        fp->inv_w[t] = (float)(1u << bits) / range;
+        fp->dims[lane] = best;
+        fp->lo[lane] = isfinite(lo) ? lo : 0.f;
+        fp->inv_w[lane] = (float)(1u << bits) / range;
     }
-    fp->m = m;
-    fp->bits = bits;
-    fp->pca = 0;
+    if (lane == 0) {
+        fp->m = m;
+        fp->bits = bits;
+        fp->pca = 0;
+    }
 }
 
 TJ_DEV int join_of_row(const long long* rowoff, int njc, long long r) {   // last j with rowoff[j] <= r

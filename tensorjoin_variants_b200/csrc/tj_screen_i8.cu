@@ -28,6 +28,7 @@
 // Warp roles (320 threads): warp 0 TMA producer, warp 1 UMMA issuer, warps 2..9 epilogue
 // (warp w reads TMEM lanes 32*(w%4).. and columns 64*((w-2)/4)..).
 #include <algorithm>
+#include <cstddef>
 
 #include <climits>
 
@@ -53,10 +54,12 @@ struct ColMetaI8 {
     int bq[kI8N];           // floor(|q_j|^2 / 2^15); 2^30 for rows beyond the tile's points
     uint32_t perm[kI8N];    // original row id
     long long norm[kI8N];   // exact |q_j|^2
+    int gminb[kI8N / 8];    // per 8-column group: min of bq (the group-wise fast test)
     uint32_t c0, nvJ;
     float HJ, LJ;           // >= max |h'|, max |l'| over the tile's rows
 };
 static_assert(sizeof(ColMetaI8) % 16 == 0, "bulk copies need 16-byte multiples");
+static_assert(offsetof(ColMetaI8, gminb) % 16 == 0, "group minima are read four at a time");
 
 struct I8Ctl {
     uint64_t full[kI8Stages];
@@ -119,7 +122,13 @@ __global__ void __launch_bounds__(kI8N) build_col_meta_i8(const uint32_t* row0, 
     const unsigned c0 = row0[J], nv = nvalid[J];
     ColMetaI8& m = out[J];
     const bool ok = t < nv;
-    m.bq[t] = ok ? floor_shift15(norm[c0 + t]) : 0x40000000;
+    const int bq = ok ? floor_shift15(norm[c0 + t]) : 0x40000000;
+    m.bq[t] = bq;
+    int gb = bq;   // min over the 8 columns t & ~7 .. (t | 7)
+    gb = min(gb, __shfl_xor_sync(0xffffffffu, gb, 1));
+    gb = min(gb, __shfl_xor_sync(0xffffffffu, gb, 2));
+    gb = min(gb, __shfl_xor_sync(0xffffffffu, gb, 4));
+    if ((t & 7) == 0) m.gminb[t >> 3] = gb;
     m.perm[t] = ok ? perm[c0 + t] : 0u;
     m.norm[t] = ok ? norm[c0 + t] : 0ll;
     if (t == 0) { m.c0 = c0; m.nvJ = nv; m.HJ = maxH[J]; m.LJ = maxL[J]; }
@@ -292,22 +301,19 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                     uint32_t hv[32];
                     tmem_ld32(tmem + lane_off + kColHH0 + b * 128 + cc, hv);
                     tmem_ld_wait();
-                    // fast path: one subtract and one max per pair, one max chain per 8-column group; only
-                    // the groups whose maximum reaches the threshold (in any lane) are examined pair by pair
-                    const int4* bq4 = reinterpret_cast<const int4*>(&m.bq[cc]);
+                    // fast path, one integer test per 8-column group: hh_j - b_j <= max hh - min b, so
+                    // max hh - min b < a_iJ proves every pair of the group out (seven maxes and one
+                    // subtract per 8 pairs); only the groups that reach the threshold (in any lane) are
+                    // examined pair by pair
+                    const int4 gb = *reinterpret_cast<const int4*>(&m.gminb[cc >> 3]);
+                    const int gbv[4] = {gb.x, gb.y, gb.z, gb.w};
                     int vx[4];
 #pragma unroll
                     for (int g = 0; g < 4; ++g) {
-                        const int4 b0 = bq4[2 * g], b1 = bq4[2 * g + 1];
                         const uint32_t* h8 = hv + 8 * g;
-                        int v = (int)h8[0] - b0.x;
-                        v = max(v, (int)h8[1] - b0.y);
-                        v = max(v, (int)h8[2] - b0.z);
-                        v = max(v, (int)h8[3] - b0.w);
-                        v = max(v, (int)h8[4] - b1.x);
-                        v = max(v, (int)h8[5] - b1.y);
-                        v = max(v, (int)h8[6] - b1.z);
-                        vx[g] = max(v, (int)h8[7] - b1.w);
+                        const int m01 = max((int)h8[0], (int)h8[1]), m23 = max((int)h8[2], (int)h8[3]);
+                        const int m45 = max((int)h8[4], (int)h8[5]), m67 = max((int)h8[6], (int)h8[7]);
+                        vx[g] = max(max(m01, m23), max(m45, m67)) - gbv[g];
                     }
                     const unsigned gmask = (vx[0] >= ai ? 1u : 0u) | (vx[1] >= ai ? 2u : 0u) |
                                            (vx[2] >= ai ? 4u : 0u) | (vx[3] >= ai ? 8u : 0u);
