@@ -22,9 +22,11 @@
 // uniform int14 rows and sent ~10x more pairs to the exact test.)
 //
 // TMEM: hh double-buffered (columns 0..255), x and ll single (256..511).  The hh products of an
-// item are committed on their own barrier before its x / ll products are issued, so the epilogue's
-// fast path (hh only) overlaps the x / ll products; the rare path waits for them.  The UMMA
-// issuer runs the hh products of item n+1 while the epilogue still reads x / ll of item n.
+// item are committed on their own barrier, and the epilogue's fast path (hh only) runs first; each
+// epilogue warp then says whether any of its pairs needs the exact test, and with one k-block per
+// item (d <= 128) the UMMA issuer computes x / ll only for items where one does (after issuing the
+// next item's hh products), so most items cost one limb product instead of four.  With several
+// k-blocks x / ll are computed with hh.
 // Warp roles (320 threads): warp 0 TMA producer, warp 1 UMMA issuer, warps 2..9 epilogue
 // (warp w reads TMEM lanes 32*(w%4).. and columns 64*((w-2)/4)..).
 #include <algorithm>
@@ -67,12 +69,14 @@ struct I8Ctl {
     uint64_t acc_full[2];
     uint64_t hh_empty[2];
     uint64_t xl_empty;
-    uint64_t xl_full;      // x and ll of the current item are in TMEM
+    uint64_t xl_full;      // x and ll of the current item are in TMEM (or were skipped)
+    uint64_t xl_dec;       // every epilogue warp has said whether it needs x and ll of the item
     uint64_t meta_full[kI8Meta];
     uint64_t meta_empty[kI8Meta];
     uint64_t drain;
     unsigned tmem_base;
     int abort_flag;
+    int need[2];           // item parity: some epilogue warp needs x and ll
 };
 
 constexpr size_t kI8Smem = 1024 + (size_t)kI8Stages * kI8Stage + kI8Meta * sizeof(ColMetaI8) + sizeof(I8Ctl);
@@ -155,6 +159,8 @@ __global__ void __launch_bounds__(kI8Threads, 1)
         }
         mbar_init(&ctl->xl_empty, kI8Epi);
         mbar_init(&ctl->xl_full, 1);
+        mbar_init(&ctl->xl_dec, kI8Epi);
+        ctl->need[0] = ctl->need[1] = 0;
         for (int m = 0; m < kI8Meta; ++m) {
             mbar_init(&ctl->meta_full[m], 1);
             mbar_init(&ctl->meta_empty[m], kI8Epi);
@@ -216,6 +222,36 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             unsigned stage = 0, phase = 0;
             unsigned long long n = 0;   // item counter of this CTA
             bool ok = true;
+            // One k-block per item (d <= 128): the x / ll products are issued lazily, only when an
+            // epilogue warp's fast test leaves a pair for the exact test.  The item's operand stage
+            // is held until that decision, which is taken after the next item's hh products are
+            // issued, so the tensor pipe keeps working meanwhile.  Several k-blocks: x / ll are
+            // issued with hh (their stages cannot all be held).
+            const bool lazy = a.kblocks == 1;
+            bool pending = false;
+            unsigned long long pn = 0;
+            unsigned pstage = 0;
+            auto resolve = [&](unsigned long long mi, unsigned si) -> bool {
+                if (!mbar_wait(&ctl->xl_dec, (unsigned)(mi & 1), status)) return false;
+                volatile int* need = &ctl->need[mi & 1];
+                const int needed = *need;
+                *need = 0;   // the item two ahead writes it only after this resolve (acc_full order)
+                if (needed) {
+                    tc_fence_after();
+                    const uint8_t* st = smem + (size_t)si * kI8Stage;
+                    const uint8_t *Ah = st, *Al = st + kPart, *Bh = st + 2 * kPart, *Bl = st + 3 * kPart;
+                    const unsigned t_x = tmem + kColX, t_ll = tmem + kColLL;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        umma_i8(t_x, desc_sw128(Ah, k * 32), desc_sw128(Bl, k * 32), a.idesc, k != 0);
+                        umma_i8(t_x, desc_sw128(Al, k * 32), desc_sw128(Bh, k * 32), a.idesc, 1u);
+                        umma_i8(t_ll, desc_sw128(Al, k * 32), desc_sw128(Bl, k * 32), a.idesc, k != 0);
+                    }
+                }
+                umma_commit(&ctl->xl_full);
+                umma_commit(&ctl->empty[si]);
+                return true;
+            };
             for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
                 const uint4 ch = a.chunks[c];
                 for (unsigned e = ch.y; e < ch.z && ok; ++e, ++n) {
@@ -224,6 +260,22 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                     if (!mbar_wait(&ctl->hh_empty[b], use ^ 1, status)) { ok = false; break; }
                     tc_fence_after();
                     const unsigned t_hh = tmem + kColHH0 + b * 128, t_x = tmem + kColX, t_ll = tmem + kColLL;
+                    if (lazy) {
+                        if (!mbar_wait(&ctl->full[stage], phase, status)) { ok = false; break; }
+                        if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
+                        tc_fence_after();
+                        const uint8_t* st = smem + (size_t)stage * kI8Stage;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            umma_i8(t_hh, desc_sw128(st, k * 32), desc_sw128(st + 2 * kPart, k * 32), a.idesc, k != 0);
+                        umma_commit(&ctl->acc_full[b]);
+                        if (pending && !resolve(pn, pstage)) { ok = false; break; }
+                        pending = true;
+                        pn = n;
+                        pstage = stage;
+                        if (++stage == kI8Stages) { stage = 0; phase ^= 1; }
+                        continue;
+                    }
                     for (int kb = 0; kb < a.kblocks; ++kb) {
                         if (!mbar_wait(&ctl->full[stage], phase, status)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
@@ -253,6 +305,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                     umma_commit(&ctl->xl_full);
                 }
             }
+            if (ok && pending) ok = resolve(pn, pstage);
             if (!ok) ctl->abort_flag = 1;
             umma_commit(&ctl->drain);
             mbar_wait(&ctl->drain, 0, status, 1000000000ull);
@@ -294,7 +347,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                 }
                 const unsigned lane_off = (q * 32u) << 16;
                 const unsigned col0 = half * 64;
-                bool xl_seen = false;
+                uint32_t cms[2] = {0u, 0u};   // pairs left for the exact test, per 32-column block
 #pragma unroll 1
                 for (int h = 0; h < 2; ++h) {
                     const unsigned cc = col0 + h * 32;
@@ -334,16 +387,28 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                         if (lim >= 31) cmask = 0;
                         else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
                     }
+                    cms[h] = cmask;
+                }
+                // tell the MMA issuer whether this item's x / ll products are needed at all (it skips
+                // them when no warp needs them), then wait for them, or for the skip, in every warp:
+                // each epilogue warp observes every phase of xl_full, so the parity names this item
+                const bool any = __any_sync(0xffffffffu, (cms[0] | cms[1]) != 0);
+                if (lane == 0) {
+                    if (any) atomicOr(&ctl->need[n & 1], 1);
+                    mbar_arrive(&ctl->xl_dec);
+                }
+                {
+                    const bool xl_ok = mbar_wait(&ctl->xl_full, (unsigned)(n & 1), status);
+                    if (!__all_sync(0xffffffffu, xl_ok)) { ok = false; break; }   // warp-uniform exit
+                }
+                tc_fence_after();
+#pragma unroll 1
+                for (int h = 0; h < 2 && any; ++h) {
+                    const uint32_t cmask = cms[h];
                     if (!__any_sync(0xffffffffu, cmask != 0)) continue;
-                    // every epilogue warp observes each phase of xl_full (here, or at the end of the
-                    // item), so the parity below names this item's products and no other
-                    if (!xl_seen) {
-                        const bool xl_ok = mbar_wait(&ctl->xl_full, (unsigned)(n & 1), status);
-                        if (!__all_sync(0xffffffffu, xl_ok)) { ok = false; break; }   // warp-uniform exit
-                        xl_seen = true;
-                    }
-                    tc_fence_after();
-                    uint32_t xv[32], lv[32];
+                    const unsigned cc = col0 + h * 32;
+                    uint32_t hv[32], xv[32], lv[32];
+                    tmem_ld32(tmem + lane_off + kColHH0 + b * 128 + cc, hv);
                     tmem_ld32(tmem + lane_off + kColX + cc, xv);
                     tmem_ld32(tmem + lane_off + kColLL + cc, lv);
                     tmem_ld_wait();
@@ -370,10 +435,6 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                         }
                         n_acc += __popc(amask);
                     }
-                }
-                if (ok && !xl_seen) {
-                    const bool xl_ok = mbar_wait(&ctl->xl_full, (unsigned)(n & 1), status);
-                    ok = __all_sync(0xffffffffu, xl_ok);
                 }
                 if (!ok) break;
                 // this item's hh buffer, the shared x / ll and the metadata slot are free again
