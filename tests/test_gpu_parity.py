@@ -208,15 +208,16 @@ def test_neighbor_table_matches_pairs():
     assert torch.equal(flat, j)
 
 
-def test_index_structure():
-    w = W.mixture64(n=20000, samples=1 << 14)
+@pytest.mark.parametrize("n", [20000, 140000])   # 140,000 rows: principal-direction cells
+def test_index_structure(n):
+    w = W.mixture64(n=n, samples=1 << 14)
     idx = tj.build_index(torch.from_numpy(w.R).cuda(), w.eps)
     perm = idx.perm.cpu().numpy()
-    assert np.array_equal(np.sort(perm), np.arange(20000))
+    assert np.array_equal(np.sort(perm), np.arange(n))
     keys = idx.keys.cpu().numpy()
     assert np.all(keys[1:] >= keys[:-1])
     cs = idx.cell_start.cpu().numpy()
-    assert cs[0] == 0 and cs[-1] == 20000 and np.all(np.diff(cs) > 0)
+    assert cs[0] == 0 and cs[-1] == n and np.all(np.diff(cs) > 0)
     assert np.all(keys[cs[:-1]][1:] != keys[cs[:-1]][:-1])
     tp = idx.tile_pairs.cpu().numpy()
     assert tp.shape[1] == 2 and len(tp) >= idx.n_tiles // 2
