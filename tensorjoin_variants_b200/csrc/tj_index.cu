@@ -1,6 +1,6 @@
-// Index build: Morton-sorted grid over the highest-variance dimensions, per-row
-// certificate metadata and low-precision MMA operands, tile statistics, and the
-// candidate tile-pair list with its execution chunks.
+// Index build: Morton-sorted grid over the highest-variance dimensions or over the top
+// principal directions, per-row certificate metadata and low-precision MMA operands, tile
+// statistics, and the candidate tile-pair list with its execution chunks.
 //
 // Reference semantics (restated, not ported):
 //  * grid index: GDS-Join's per-dimension cells over NUMINDEXEDDIM variance-ordered
@@ -8,6 +8,9 @@
 //    getLinearID_nDimensions, :891-948 generateNDGridDimensions).  Here the cell
 //    coordinates are interleaved into a Morton key and points are radix-sorted by it
 //    on the GPU instead of a CPU std::set (main.cu:690-857).
+//  * principal-direction layout: the PCA-sorted block layout of the block-feasibility study
+//    (tensorjoin_20260908_block_feasibility/src/geometry.py:15-32 projection and layout), built
+//    here on the GPU from a sampled covariance and used only to order rows into tiles.
 //  * candidate list: the tile-pair schedule of the scripted joins
 //    (src/run_g2b_tensorjoin_public.py:211-215, np.triu_indices for self-joins) pruned
 //    with conservative block lower bounds, ball and axis-aligned box
