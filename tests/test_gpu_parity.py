@@ -228,9 +228,14 @@ def test_index_structure(n):
 def test_int14_self_join_exact(d):
     w = W.int14x128(n=5000, d=d, samples=1 << 14)
     for mode in ("upper", "directed"):
+        want = oracle.join_i16(w.R, None, w.T, mode)
         k, st = gpu_keys(w.R, None, w.T, mode, "int8limb")
-        assert_same(k, oracle.join_i16(w.R, None, w.T, mode), f"d={d} {mode}")
+        assert_same(k, want, f"d={d} {mode}")
         assert st["band"] == 0
+        # the full-size int14 join takes principal-direction cells (2M rows): same pairs here
+        k, st = gpu_keys(w.R, None, w.T, mode, "int8limb", index_frame="pca")
+        assert_same(k, want, f"d={d} {mode} pca")
+        assert st["index_frame"] == 1
 
 
 def test_int14_rs_ties_and_extremes():
