@@ -101,6 +101,15 @@ class Clocks:
                  "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        # nvidia-smi's start-up (driver queries of every GPU) can hold up this process's CUDA calls
+        # for hundreds of ms: let it write its first sample before the timed region begins
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+            self.file.flush()
+            if os.path.getsize(self.file.name) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self) -> dict:
         if self.proc is None:

@@ -666,7 +666,7 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
             pmin[grp * d + k] = INFINITY;
             pmax[grp * d + k] = -INFINITY;
         }
-        constexpr int kU = 4;   // rows of a group whose loads are issued together
+        constexpr int kU = 8;   // rows of a group whose loads are issued together
         for (int i = grp; i < nv; i += kU * kNG) {
             size_t base[kU];
 #pragma unroll
@@ -729,7 +729,7 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
     // radius: kL lanes per row, exact FP64 differences against the FP32 centroid; the row loop is
     // uniform across each warp so that every lane takes part in the shuffles
     double rmax = 0.0;
-    constexpr int kRU = 2;   // rows per lane group whose loads are issued together
+    constexpr int kRU = 4;   // rows per lane group whose loads are issued together
     for (int i0 = warp * (32 / kL); i0 < nv; i0 += kRU * kNG) {
         double s[kRU];
         size_t base[kRU];
