@@ -105,7 +105,7 @@ class Clocks:
         # nvidia-smi's start-up (driver queries of every GPU) can hold up this process's CUDA calls
         # for hundreds of ms: let it write its first sample before the timed region begins
         t0 = time.time()
-        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+        while time.time() - t0 < 2.0 and self.proc.poll() is None:   # bounded: output may be buffered
             self.file.flush()
             if os.path.getsize(self.file.name) > 0:
                 break
