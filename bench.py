@@ -531,6 +531,15 @@ def ragged_bench(args, rank, world, screen, dist):
                                      "refine_accept", "result_pairs", "retries", "ms_index", "ms_candidates",
                                      "ms_screen", "ms_refine", "ms_sort", "ms_total", "band_fp64")},
     }
+    line["stats"]["refined_fraction"] = st["band"] / max(1, st["pairs_screened"])
+    if screen != "plain":   # sampled screen error against FP64, outside the timed region
+        rd = tj.join_batched_result(joins, screen=screen, screen_diag=True)
+        sd = rd.stats
+        line["screen_error"] = {"max_abs_err_d2": sd["screen_max_abs_err"],
+                                "max_err_over_certified_radius": sd["screen_err_over_bound"],
+                                "pairs_sampled": sd["screen_err_pairs"], "band_pairs": sd["band"],
+                                "refined_fraction": sd["band"] / max(1, sd["pairs_screened"])}
+        del rd
     if not args.no_plain and screen != "plain":
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

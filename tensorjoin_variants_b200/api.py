@@ -261,10 +261,11 @@ class BatchResult(Result):
 
 
 def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_items: int = 0,
-                        index_frame: str = "auto", band_fp32: bool = False) -> BatchResult:
+                        index_frame: str = "auto", band_fp32: bool = False,
+                        screen_diag: bool = False) -> BatchResult:
     """Run many independent R-S joins [(R, S, eps), ...] in one batched pass (one screen launch).
-    ``index_frame`` and ``band_fp32`` as in ``join_result`` (packed joins keep input-dimension
-    cells under "auto")."""
+    ``index_frame``, ``band_fp32`` and ``screen_diag`` as in ``join_result`` (packed joins keep
+    input-dimension cells under "auto")."""
     if index_frame not in FRAME_FLAGS:
         raise ValueError(f"index_frame must be one of {sorted(FRAME_FLAGS)}")
     descs = (_lib.BatchJoin * len(joins))()
@@ -279,6 +280,7 @@ def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_it
                                   _threshold(eps, None))
     h = C.c_void_p()
     flags = FRAME_FLAGS[index_frame] | (_lib.FLAG_BAND_FP32 if band_fp32 else 0)
+    flags |= _lib.FLAG_SCREEN_DIAG if screen_diag else 0
     opt = _lib.Options(int(capacity), int(chunk_items), flags)
     check(lib().tj_join_batched(descs, len(joins), SCREEN[screen], C.byref(opt), C.byref(h),
                                 C.c_void_p(_stream_ptr())))

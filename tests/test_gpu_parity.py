@@ -545,3 +545,17 @@ def test_fp32_band_stage_batched():
         want = oracle.join_f32(R, S, Tk, "rs") if len(R) and len(S) else np.empty(0, np.uint64)
         got = i.cpu().numpy().astype(np.uint64) * np.uint64(max(len(S), 1)) + j.cpu().numpy().astype(np.uint64)
         assert_same(got, want, f"fp32 stage join {k}")
+
+
+def test_batched_screen_error_within_certified_radius():
+    """The sampled screen error of a batched pass (several dimension classes) stays inside the
+    certified radius, and the diagnostic pass changes no pair."""
+    joins = _ragged(16, 44)
+    dev = [(torch.from_numpy(R).cuda(), torch.from_numpy(S).cuda(), float(np.sqrt(T))) for R, S, T in joins]
+    for screen in ("bf16", "bf16x3"):
+        res = tj.join_batched_result(dev, screen=screen, screen_diag=True)
+        st = res.stats
+        assert st["screen_err_pairs"] > 0
+        assert st["screen_err_over_bound"] < 1.0, st
+        plain = tj.join_batched_result(dev, screen=screen)
+        assert torch.equal(res.keys(), plain.keys())
