@@ -615,21 +615,28 @@ __global__ void prep_rows(const void* src, int dtype, long long n, int d, int kp
         sq += __shfl_xor_sync(0xffffffffu, sq, o);
         flags |= __shfl_xor_sync(0xffffffffu, flags, o);
     }
+    // FP64 sums of d non-negative squares (each rounded once): relative error <= (d+2) 2^-53;
+    // x - c may round once more (2^-53 relative), absorbed by the extra 2^-50 terms.
+    // The four norm bounds of a row are taken by its first four lanes, one square root each in the
+    // same instruction stream (every lane computes one; kL >= 4), instead of four in a row on one lane.
+    static_assert(kL >= 4, "four lanes per row take the four norm bounds");
+    const double g = (double)(d + 4) * 0x1p-53;
+    const double up = (1.0 + 2.0 * g) * (1.0 + 0x1p-50);
+    const unsigned task = sub & 3u;   // 0: |x - c|, 1: |w|, 2: |x - c - w|, 3: |w_lo|
+    const double v = task == 0 ? sx : task == 1 ? sz : task == 2 ? se : sl;
+    double rt = sqrt(v * up) * (1.0 + 0x1p-50);
+    const double ynorm = __shfl_sync(0xffffffffu, rt, (int)((threadIdx.x & 31u) & ~(unsigned)(kL - 1)));
+    if (task == 2) rt += 0x1p-50 * ynorm;
+    if (live && sub < 4) {
+        float* dst = task == 0 ? yn : task == 1 ? zn : task == 2 ? en : zl;
+        dst[r] = f32_up(rt);
+    }
     if (sub == 0 && live) {
         if ((flags & 1u) && real) atomicOr(status, (unsigned long long)kStatusBadInput);
         if ((flags & 2u) && real) atomicOr(status, (unsigned long long)kStatusFp16Range);
         if (real && sx > 0x1p100) atomicOr(status, (unsigned long long)kStatusBadInput);
-        // FP64 sums of d non-negative squares (each rounded once): relative error <= (d+2) 2^-53;
-        // x - c may round once more (2^-53 relative), absorbed by the extra 2^-50 terms.
-        const double g = (double)(d + 4) * 0x1p-53;
-        const double up = (1.0 + 2.0 * g) * (1.0 + 0x1p-50);
         nrm2[r] = sx;
         nrm2f[r] = __double2float_rn(sx);
-        const double ynorm = sqrt(sx * up) * (1.0 + 0x1p-50);
-        yn[r] = f32_up(ynorm);
-        zn[r] = f32_up(sqrt(sz * up) * (1.0 + 0x1p-50));
-        en[r] = f32_up(sqrt(se * up) * (1.0 + 0x1p-50) + 0x1p-50 * ynorm);
-        zl[r] = f32_up(sqrt(sl * up) * (1.0 + 0x1p-50));
         if (inorm) inorm[r] = sq;
     }
 }
