@@ -816,8 +816,7 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
         auto kern = bf ? screen_tc_kernel<1, 0, true> : screen_tc_kernel<0, 0, true>;
         const size_t smem = screen_smem<0, true>();
         TJ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        cudaLaunchConfig_t cfg;
-        memset(&cfg, 0, sizeof(cfg));
+        cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = 2;
