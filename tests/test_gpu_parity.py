@@ -559,3 +559,12 @@ def test_batched_screen_error_within_certified_radius():
         assert st["screen_err_over_bound"] < 1.0, st
         plain = tj.join_batched_result(dev, screen=screen)
         assert torch.equal(res.keys(), plain.keys())
+
+
+def test_int14_many_items_exact():
+    """Many tile pairs per CTA (30,000 rows, d = 128): the on-demand x / ll products and their
+    hand-off between the epilogue warps and the UMMA issuer give the oracle's pairs."""
+    w = W.int14x128(n=30000, samples=1 << 14)
+    k, st = gpu_keys(w.R, None, w.T, "upper", "int8limb")
+    assert_same(k, oracle.join_i16(w.R, None, w.T, "upper"), "int14 n=30000")
+    assert st["tile_pairs"] > 148 * 40
