@@ -348,12 +348,14 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                 const unsigned lane_off = (q * 32u) << 16;
                 const unsigned col0 = half * 64;
                 uint32_t cms[2] = {0u, 0u};   // pairs left for the exact test, per 32-column block
-#pragma unroll 1
+                uint32_t hv2[2][32];          // both blocks' hh loads in flight together
+                tmem_ld32(tmem + lane_off + kColHH0 + b * 128 + col0, hv2[0]);
+                tmem_ld32(tmem + lane_off + kColHH0 + b * 128 + col0 + 32, hv2[1]);
+                tmem_ld_wait();
+#pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const unsigned cc = col0 + h * 32;
-                    uint32_t hv[32];
-                    tmem_ld32(tmem + lane_off + kColHH0 + b * 128 + cc, hv);
-                    tmem_ld_wait();
+                    const uint32_t (&hv)[32] = hv2[h];
                     // fast path, one integer test per 8-column group: hh_j - b_j <= max hh - min b, so
                     // max hh - min b < a_iJ proves every pair of the group out (seven maxes and one
                     // subtract per 8 pairs); only the groups that reach the threshold (in any lane) are
