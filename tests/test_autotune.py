@@ -91,3 +91,38 @@ def test_tuned_join_matches_oracle_and_reuses_the_table(tmp_path):
     X = torch.from_numpy(w.R[:4000]).cuda()
     res = tuner.join(X, None, eps2=w.T, mode="upper", screen="fp16", sample_rows=1024)
     assert np.array_equal(res.keys().cpu().numpy().view(np.uint64), oracle.join_f32(w.R[:4000], None, w.T, "upper"))
+
+
+def test_tuner_join_flow_with_a_fake_library(monkeypatch, tmp_path):
+    """Host flow of Tuner.join on the CPU: the selectivity probe, tuning on a miss (every candidate
+    timed, the fastest kept under both the probe's and the tuning sample's keys), reuse on a hit,
+    and the final join run with the chosen options."""
+    import torch
+
+    calls = []
+
+    class FakeResult:
+        def __init__(self, R, S, kw):
+            rows = R.shape[0]
+            self.count = rows * 12                                   # 12 result pairs per row
+            ms = 5.0 if kw.get("chunk_items") == 256 and kw.get("index_frame") == "pca" else 9.0
+            self.stats = {"ms_total": ms, "result_pairs": self.count}
+
+    def fake_join_result(R, S, eps2=None, mode="rs", screen="bf16", **kw):
+        calls.append((R.shape[0], kw))
+        return FakeResult(R, S, kw)
+
+    monkeypatch.setattr(A.api, "join_result", fake_join_result)
+    monkeypatch.setattr(A.api, "_as_device", lambda x, allow_int16: (x, False))
+    R = torch.zeros((50000, 64))
+    S = torch.zeros((60000, 64))
+    tuner = A.Tuner(str(tmp_path / "t.json"))
+    tuner.join(R, S, eps2=0.1, screen="bf16x3", sample_rows=1024)
+    final_kw = calls[-1][1]
+    assert calls[-1][0] == 50000 and final_kw["chunk_items"] == 256 and final_kw["index_frame"] == "pca"
+    n_first = len(calls)
+    assert n_first == 1 + 2 * len(A.candidates(64, "bf16x3", "rs")) + 1   # probe, tuning, join
+    tuner.join(R, S, eps2=0.1, screen="bf16x3", sample_rows=1024)
+    assert len(calls) == n_first + 2                                      # probe and join only
+    key = A.tune_key(64, "f32", "bf16x3", "rs", 50000, 60000, 12.0)
+    assert tuner.lookup(key) == A.Choice(True, 256, "pca", False)
