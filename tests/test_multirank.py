@@ -33,7 +33,7 @@ def _worker(rank, world, port, out):
 
 def test_max_over_ranks_gloo():
     port = _free_port()
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()   # no fork of a process that holds threads
     mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
     assert out[0] == 15.0 and out[1] == 15.0
 
