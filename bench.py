@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Benchmark of the certified exact epsilon-join on B200.
 
-Default workload (N=1): the high-dimensional R-S join, |R| = |S| = 500,000, d = 512,
-rank-32 factor model + N(0, 0.1^2) noise, rows L2-normalised, eps for ~8 neighbours,
+Headline workload (N=1): the high-dimensional R-S join, |R| = |S| = 500,000, d = 512,
+rank-32 factor model + N(0, 0.1^2), rows L2-normalised, eps for ~8 neighbours,
 FP16 tensor-core screen + certified band + FP64 refinement, pair set bit-exact to the
 FP64 oracle.  This is the configuration the >= 5x target against the plain FP32
 direct-difference GPU join is stated on.  Data are seeded synthetic arrays with
@@ -18,6 +18,13 @@ metric: distance evaluations per second (candidate pairs screened / step time),
         whole job over all ranks; ms_per_step is the join wall time.
 e2e:    the same metric through the public API with host (pinned) inputs and host
         outputs: H2D of R and S and D2H of the (i, j) result inside the timed region.
+parity: after the timed steps, complete result rows of a seeded sample of R rows are
+        recomputed by the CPU oracle (FP64 sequential k, or exact int64) against all of S
+        and compared key for key with the GPU result restricted to those rows, and every
+        emitted pair's distance is recomputed by the oracle and checked against T.
+configs: the default run (N=1) also measures the other four configurations (mixture,
+        int14 self-join, ragged batch, 20k x 16 plain grid), each with its own timing,
+        clocks, roofline, plain-GPU comparison, end-to-end time, CPU baseline and parity audit.
 --impl reference: the reference's own exact CPU path (SciPy cdist 'sqeuclidean' on
         FP64-widened rows + <= T, all host cores) on a bounded row sample per step.
 Multi-GPU: one process per GPU (torchrun), independent replicas of the workload
@@ -45,12 +52,13 @@ sys.path.insert(0, str(ROOT))
 METRIC = "dist_evals_per_s"
 UNIT = "pairs/s"
 WORKLOADS = {
-    "factor512": dict(fn="factor512", screen="fp16", mode="rs"),
-    "mixture64": dict(fn="mixture64", screen="bf16x3", mode="rs"),
-    "uniform16": dict(fn="uniform16", screen="plain", mode="upper"),
-    "int14x128": dict(fn="int14x128", screen="int8limb", mode="upper"),
-    "ragged4096": dict(fn="ragged4096", screen="bf16x3", mode="rs"),
+    "factor512": dict(fn="factor512", screen="fp16", mode="rs", audit_rows=1024),
+    "mixture64": dict(fn="mixture64", screen="bf16x3", mode="rs", audit_rows=2048),
+    "uniform16": dict(fn="uniform16", screen="plain", mode="upper", audit_rows=0),   # 0: exhaustive
+    "int14x128": dict(fn="int14x128", screen="int8limb", mode="upper", audit_rows=2048),
+    "ragged4096": dict(fn="ragged4096", screen="bf16x3", mode="rs", audit_rows=64),   # joins checked
 }
+SUB_CONFIGS = ["mixture64", "int14x128", "ragged4096", "uniform16"]
 
 
 def parse():
@@ -68,6 +76,10 @@ def parse():
     ap.add_argument("--band-fp32", action="store_true", help="certified FP32 band stage before the FP64 terminal")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle audit after the timed steps")
+    ap.add_argument("--configs", default="auto", choices=["auto", "none"],
+                    help="auto: a default single-GPU run also measures the other configurations")
+    ap.add_argument("--sub-steps", type=int, default=5, help="timed steps of each other configuration")
     ap.add_argument("--cpu-rows", type=int, default=128, help="R rows in the CPU baseline sample")
     ap.add_argument("--ref-rows", type=int, default=48, help="R rows per step of --impl reference")
     return ap.parse_args()
@@ -89,7 +101,7 @@ class Clocks:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: str):
         self.idx = gpu_index
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.proc = None
@@ -110,6 +122,7 @@ class Clocks:
             if os.path.getsize(self.file.name) > 0:
                 break
             time.sleep(0.02)
+        time.sleep(0.3)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -136,6 +149,15 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
 
 
+def gpu_uuid() -> str:
+    import torch
+
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
+    except Exception:
+        return str(torch.cuda.current_device())
+
+
 def max_over_ranks(x: float, world: int, dist, device: str = "cuda") -> float:
     """The largest of every rank's `x` (all ranks call this at the same point)."""
     if world <= 1:
@@ -156,6 +178,38 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "tflops": 1590.0, "tflops_sustained": 1400.0, "source": "fallback"}
 
 
+_INT8_PEAK = None
+
+
+def int8_peak_tops() -> dict:
+    """Dense INT8 tensor throughput of this GPU, measured here: torch._int_mm (a cuBLAS int8 GEMM,
+    int32 accumulate) at 8192^3, 10 timed launches after 3 warm-ups, CUDA events.  Only the
+    denominator of the int8 screen's roofline fraction; the screen never calls it."""
+    global _INT8_PEAK
+    if _INT8_PEAK is not None:
+        return _INT8_PEAK
+    import torch
+
+    n = 8192
+    a = torch.randint(-127, 127, (n, n), dtype=torch.int8, device="cuda")
+    b = torch.randint(-127, 127, (n, n), dtype=torch.int8, device="cuda").t()
+    for _ in range(3):
+        torch._int_mm(a, b)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    reps = 10
+    for _ in range(reps):
+        torch._int_mm(a, b)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    _INT8_PEAK = {"tops": 2.0 * n ** 3 / (ms / 1000.0) / 1e12, "ms": ms,
+                  "source": "measured here: torch._int_mm int8 GEMM 8192^3, burst"}
+    del a, b
+    torch.cuda.empty_cache()
+    return _INT8_PEAK
+
+
 def committed_traffic(kernel: str, workload: str):
     """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/traffic.txt)."""
     p = ROOT / "profiles" / "traffic.txt"
@@ -169,6 +223,60 @@ def committed_traffic(kernel: str, workload: str):
             except ValueError:
                 return None
     return None
+
+
+# ---------------------------------------------------------------------- oracle audit
+def _keys_np(keys_t) -> np.ndarray:
+    return keys_t.cpu().numpy().view(np.uint64)
+
+
+def parity_audit(R: np.ndarray, S: np.ndarray | None, T, mode: str, keys: np.ndarray, rows: int,
+                 seed: int = 2024) -> dict:
+    """Audit one GPU result against the CPU oracle (outside every timed region).
+
+    (i) complete rows: a seeded sample of `rows` R rows (all rows when rows == 0) joined by the
+        oracle against all of S; the GPU keys that touch those rows must be exactly that set
+        (self-joins: every pair with either end in the sample, i < j);
+    (ii) every emitted pair: its distance recomputed by the oracle must be <= T.
+    Pairs are canonical keys i * n_cols + j."""
+    import oracle
+
+    t0 = time.perf_counter()
+    is_int = R.dtype == np.int16
+    Sx = R if S is None else S
+    n_cols = Sx.shape[0]
+    nc = np.uint64(n_cols)
+    gi = (keys // nc).astype(np.int64)
+    gj = (keys % nc).astype(np.int64)
+    rng = np.random.default_rng(seed)
+    if rows <= 0 or rows >= R.shape[0]:
+        sample = np.arange(R.shape[0], dtype=np.int64)
+    else:
+        sample = np.sort(rng.choice(R.shape[0], rows, replace=False)).astype(np.int64)
+    sub = R[sample]
+    part = oracle.join_i16(sub, Sx, int(T), "rs") if is_int else oracle.join_f32(sub, Sx, float(T), "rs")
+    ii = sample[(part // nc).astype(np.int64)]
+    jj = (part % nc).astype(np.int64)
+    if mode == "rs":
+        want = ii.astype(np.uint64) * nc + jj.astype(np.uint64)
+        sel = np.isin(gi, sample)
+    else:   # self-join (upper): the neighbours of a sampled point on either side of the diagonal
+        keep = jj != ii
+        lo, hi = np.minimum(ii[keep], jj[keep]), np.maximum(ii[keep], jj[keep])
+        want = np.unique(lo.astype(np.uint64) * nc + hi.astype(np.uint64))
+        sel = np.isin(gi, sample) | np.isin(gj, sample)
+    got = np.unique(keys[sel])
+    want = np.unique(want)
+    missing = int(np.setdiff1d(want, got, assume_unique=True).size)
+    extra = int(np.setdiff1d(got, want, assume_unique=True).size)
+    d2 = oracle.pair_d2_mt(R, Sx, gi, gj)
+    over = int(np.count_nonzero(d2 > T))
+    dup = int(keys.size - np.unique(keys).size) if keys.size < (1 << 27) else None
+    return {"rows_checked": int(sample.size), "pairs_checked": int(want.size), "emitted_rechecked": int(keys.size),
+            "missing": missing, "extra": extra, "emitted_over_T": over, "duplicates": dup,
+            "mismatches": missing + extra + over + (dup or 0),
+            "oracle": ("exact int64" if is_int else "FP64 sequential-k") + f" C oracle, {oracle.default_threads()} "
+                      "host threads", "seconds": round(time.perf_counter() - t0, 2)}
 
 
 # ---------------------------------------------------------------------- reference arm
@@ -192,7 +300,7 @@ def reference_arm(args, rank: int) -> None:
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.mean(timed),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args, w),
+        "config": workload_config(args.workload, args.screen, args.gpus, w),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
                          "sample": f"scipy.spatial.distance.cdist(R64, S64, 'sqeuclidean') <= T (the reference's "
                                    f"exact CPU path) on {rows} seeded R rows x all {len(S)} S rows per step, "
@@ -203,45 +311,81 @@ def reference_arm(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
-def workload_config(args, w) -> dict:
-    spec = WORKLOADS[args.workload]
+def workload_config(name: str, screen: str | None, gpus: int, w) -> dict:
+    spec = WORKLOADS[name]
     S = w.R if w.S is None else w.S
-    return {"workload": args.workload, "n_rows": int(w.R.shape[0]), "n_cols": int(S.shape[0]),
-            "d": int(w.R.shape[1]), "mode": spec["mode"], "screen": args.screen or spec["screen"],
+    return {"workload": name, "n_rows": int(w.R.shape[0]), "n_cols": int(S.shape[0]),
+            "d": int(w.R.shape[1]), "mode": spec["mode"], "screen": screen or spec["screen"],
             "eps": w.eps, "eps2": float(w.T), "target_degree": w.target_degree,
-            "l2": "inputs larger than L2 (no flush needed)", "parallelism": f"replicas x{args.gpus}"}
+            "l2": "inputs larger than L2 (no flush needed)" if w.R.nbytes > (128 << 20)
+            else "inputs smaller than L2: every step re-reads them from L2 (no flush); reported as is",
+            "parallelism": f"replicas x{gpus}"}
 
 
-# ---------------------------------------------------------------------- our arm
-def main() -> None:
-    args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        reference_arm(args, rank)
-        return
+def screen_roofline(screen: str, d: int, pairs: int, screen_ms: float, issued_ops: float, peaks: dict) -> dict:
+    """Roofline of the screen kernel: algorithmic ops (2 d per pair; int8 limbs 8 d per pair, the count
+    the scope table fixes) and the ops the kernel actually issues, each over the same kernel time."""
+    secs = screen_ms / 1000.0
+    if screen == "plain":
+        ach = 2.0 * d * pairs / secs / 1e12
+        return {"bound": "simt", "kernel": "plain_kernel", "achieved": ach, "peak": None, "unit": "TFLOP/s",
+                "frac": None, "screen_ms": screen_ms, "flops_per_launch": 2.0 * d * pairs}
+    if screen == "int8limb":
+        p8 = int8_peak_tops()
+        alg = 8.0 * d * pairs
+        ach, iss = alg / secs / 1e12, issued_ops / secs / 1e12
+        return {"bound": "tensor", "kernel": "screen_i8_kernel", "achieved": ach, "peak": p8["tops"],
+                "unit": "TOP/s", "frac": ach / p8["tops"], "frac_algorithmic": ach / p8["tops"],
+                "achieved_issued": iss, "frac_issued": iss / p8["tops"], "peak_source": p8["source"],
+                "screen_ms": screen_ms, "ops_per_launch": alg, "issued_ops_per_launch": issued_ops}
+    peak = peaks["tflops_sustained"]
+    alg = 2.0 * d * pairs
+    ach, iss = alg / secs / 1e12, issued_ops / secs / 1e12
+    return {"bound": "tensor", "kernel": "screen_tc_kernel", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+            "frac": ach / peak, "frac_algorithmic": ach / peak, "achieved_issued": iss, "frac_issued": iss / peak,
+            "peak_source": f"{peaks['source']} bf16_tflops_sustained (dense fp16 = bf16 rate)",
+            "screen_ms": screen_ms, "flops_per_launch": alg, "issued_flops_per_launch": issued_ops}
 
+
+def issued_screen_ops(screen: str, st: dict, d: int) -> float:
+    """Tensor-core operations the screen issued: 2 d per screened pair (6 d with the hi/lo split; the
+    int8-limb screen reports its own count, which depends on how many items needed the low limbs)."""
+    if screen == "int8limb":
+        return float(st.get("screen_ops_issued") or st["screen_ops"])
+    return (6.0 if screen in ("bf16x3", "fp16x3") else 2.0) * d * st["pairs_screened"]
+
+
+def cpu_baseline_leg(R: np.ndarray, S: np.ndarray, T, rows: int, full_pairs: int) -> dict:
+    import oracle
+
+    rows = min(rows, R.shape[0])
+    rng = np.random.default_rng(7)
+    sample = R[np.sort(rng.choice(R.shape[0], rows, replace=False))]
+    procs = len(os.sched_getaffinity(0))
+    cp, secs, _ = oracle.scipy_rate(sample.astype(np.float32), S.astype(np.float32), T, procs, rows_per_task=2,
+                                    repeats=1, context="spawn")
+    rate = cp / secs[0]
+    return {"value": rate, "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": f"scipy cdist sqeuclidean (the reference's exact CPU path), {rows} seeded R "
+                      f"rows x all {len(S)} S rows, {procs} spawned processes, "
+                      f"{secs[0]:.1f} s; full join extrapolated {full_pairs / rate:.0f} s"}
+
+
+# ---------------------------------------------------------------------- one single-join configuration
+def bench_single(name: str, args, steps: int, warmup: int, rank: int, world: int, dist, headline: bool) -> dict:
     import torch
-    import torch.distributed as dist
 
     import tensorjoin_variants_b200 as tj
     from tensorjoin_variants_b200 import _lib
 
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-    spec = WORKLOADS[args.workload]
-    screen = args.screen or spec["screen"]
+    spec = WORKLOADS[name]
+    screen = (args.screen if headline else None) or spec["screen"]
     mode = spec["mode"]
-    if args.workload == "ragged4096":
-        ragged_bench(args, rank, world, screen, dist)
-        return
-    w = make_workload(args.workload, args.n)
+    w = make_workload(name, args.n if headline else 0)
     R = torch.from_numpy(w.R).cuda()
     S = None if w.S is None else torch.from_numpy(w.S).cuda()
     T = w.T
+    d = int(w.R.shape[1])
 
     def step():
         res = tj.join_result(R, S, eps2=T, mode=mode, screen=screen, index_frame=args.index_frame,
@@ -249,19 +393,14 @@ def main() -> None:
         i, j = res.pairs()
         return res, i, j
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         res, i, j = step()
         del res, i, j
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    try:
-        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
-    except Exception:
-        gpu_id = str(local)
-    clocks = Clocks(gpu_id)
+    clocks = Clocks(gpu_uuid())
     clocks.start()
-    time.sleep(0.3)
     launches0 = _lib.lib().tj_kernel_launches()
     stream = torch.cuda.current_stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -269,8 +408,8 @@ def main() -> None:
     ev0.record(stream)
     stats = []
     count = 0
-    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    for s_ in range(args.steps):
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for s_ in range(steps):
         res, i, j = step()
         stats.append(res.stats)
         count = res.count
@@ -280,53 +419,32 @@ def main() -> None:
     torch.cuda.synchronize()
     launches = _lib.lib().tj_kernel_launches() - launches0
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    step_ms = [(ev0 if k == 0 else marks[k - 1]).elapsed_time(marks[k]) for k in range(args.steps)]
+    ms = ev0.elapsed_time(ev1) / steps
+    step_ms = [(ev0 if k == 0 else marks[k - 1]).elapsed_time(marks[k]) for k in range(steps)]
     ms = max_over_ranks(ms, world, dist)
     if world > 1:
         dist.barrier()
     st = stats[-1]
     pairs = st["pairs_screened"]
     value = world * pairs / (ms / 1000.0)
-
-    # dominant kernel: the screen (tensor-core bound); algorithmic flops = 2 d per screened pair
     peaks = measured_peaks()
     screen_ms = statistics.mean(s["ms_screen"] for s in stats)
-    # algorithmic ops per screened pair, counted by the library: 2 d (16-bit), 6 d (hi/lo split), 8 d (int8 limbs)
-    flops = statistics.mean(s["screen_ops"] for s in stats) if screen != "plain" else 2.0 * w.R.shape[1] * pairs
-    peak_note = f"{peaks['source']} bf16_tflops_sustained (dense fp16 = bf16 rate)"
-    if screen == "plain":
-        achieved, unit, bound = flops / (screen_ms / 1000.0) / 1e12, "TFLOP/s", "simt"
-        peak = None
-    elif screen == "int8limb":
-        achieved, unit, bound = flops / (screen_ms / 1000.0) / 1e12, "TOP/s", "tensor"
-        peak = 2.0 * peaks["tflops_sustained"]
-        peak_note = f"2 x {peaks['source']} bf16_tflops_sustained (dense int8 rate = 2 x bf16; no int8 measurement)"
-    else:
-        achieved, unit, bound = flops / (screen_ms / 1000.0) / 1e12, "TFLOP/s", "tensor"
-        peak = peaks["tflops_sustained"]
-    kname = {"plain": "plain_kernel", "int8limb": "screen_i8_kernel"}.get(screen, "screen_tc_kernel")
-    roofline = {"bound": bound, "kernel": kname,
-                "achieved": achieved, "peak": peak, "unit": unit,
-                "frac": (achieved / peak) if peak else None,
-                "peak_source": peak_note,
-                "traffic": committed_traffic(kname, args.workload),
-                "screen_ms": screen_ms, "flops_per_launch": flops}
-
+    roofline = screen_roofline(screen, d, pairs, screen_ms, issued_screen_ops(screen, st, d), peaks)
+    if headline:
+        roofline["traffic"] = committed_traffic(roofline["kernel"], name)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": {"plain": "f32", "int8limb": "s8"}.get(screen, screen), "data": "synthetic",
-        "config": workload_config(args, w), "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
-        "result_pairs": int(count), "step_ms": step_ms, "lib_ms_total": [s["ms_total"] for s in stats],
+        "config": workload_config(name, screen, world, w), "roofline": roofline, "clocks": clk,
+        "gpu_launches": int(launches), "result_pairs": int(count), "step_ms": step_ms,
+        "lib_ms_total": [s["ms_total"] for s in stats],
         "stats": {k: st[k] for k in (
             "pairs_all", "pairs_screened", "tile_pairs", "screen_accept", "band", "refine_accept", "rare_checks",
             "result_pairs", "retries", "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total",
             "index_frame", "band_fp64")},
     }
     line["stats"]["refined_fraction"] = st["band"] / max(1, st["pairs_screened"])
-    # the other rates of the metric family: all-pairs equivalent (|R||S| or N(N-1)/2 per second)
-    # and emitted result pairs per second, whole job
     line["rates"] = {"all_pairs_equivalent_per_s": world * st["pairs_all"] / (ms / 1000.0),
                      "result_pairs_per_s": world * int(count) / (ms / 1000.0),
                      "pair_space_pruned_fraction": max(0.0, 1.0 - st["pairs_screened"] / max(1, st["pairs_all"]))}
@@ -341,6 +459,12 @@ def main() -> None:
     elif screen == "int8limb":
         line["screen_error"] = {"max_abs_err_d2": 0, "note": "exact integer screen (int8 limbs, INT64 recombination)"}
 
+    # the GPU result once more, for the plain comparison and the oracle audit
+    res = tj.join_result(R, S, eps2=T, mode=mode, screen=screen, index_frame=args.index_frame,
+                         band_fp32=args.band_fp32)
+    keys_t = res.keys()
+    del res
+
     # plain FP32 direct-difference GPU join over the same candidate tile pairs (the baseline to beat)
     if not args.no_plain and screen != "plain":
         torch.cuda.synchronize()
@@ -350,19 +474,16 @@ def main() -> None:
         Rp = R.float() if R.dtype == torch.int16 else R
         Sp = None if S is None else (S.float() if S.dtype == torch.int16 else S)
         resp = tj.join_result(Rp, Sp, eps2=T, mode=mode, screen="plain")
-        ip, jp = resp.pairs()
+        kp = resp.keys()
         e1.record(stream)
         torch.cuda.synchronize()
         pms = e0.elapsed_time(e1)
-        same = resp.count == count
-        if same and count:
-            res, i, j = step()
-            same = bool(torch.equal(i, ip) and torch.equal(j, jp))
-            del res, i, j
         line["plain_gpu"] = {"ms_per_step": pms, "value": world * resp.stats["pairs_screened"] / (pms / 1000.0),
-                             "speedup_of_tc_path": pms / ms, "identical_pair_set": same,
-                             "ms_screen": resp.stats["ms_screen"]}
-        del resp, ip, jp
+                             "speedup_of_tc_path": pms / ms, "identical_pair_set": bool(torch.equal(kp, keys_t)),
+                             "ms_screen": resp.stats["ms_screen"],
+                             "note": "one run; the same index, candidates, refinement and sort as the "
+                                     "tensor-core path, only the screen differs"}
+        del resp, kp, Rp, Sp
 
     # end to end through the public API with host buffers (pinned inputs, host outputs)
     if not args.no_e2e:
@@ -370,10 +491,10 @@ def main() -> None:
         Sh = None if w.S is None else torch.from_numpy(w.S).pin_memory()
         fn = (lambda: tj.join(Rh, Sh, eps2=T, screen=screen)) if mode == "rs" else \
             (lambda: tj.self_join(Rh, eps2=T, mode=mode, screen=screen))
-        for _ in range(max(3, args.warmup)):   # warm-up: the pinned host buffers reach the allocator's cache
+        for _ in range(max(3, warmup)):   # warm-up: the pinned host buffers reach the allocator's cache
             ih, jh = fn()
         torch.cuda.synchronize()
-        k_e2e = max(1, min(args.steps, 3))
+        k_e2e = max(1, min(steps, 3))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(k_e2e):
@@ -385,29 +506,19 @@ def main() -> None:
         h2d = Rh.numel() * Rh.element_size() + (0 if Sh is None else Sh.numel() * Sh.element_size())
         line["e2e"] = {"value": world * pairs / (ems / 1000.0), "unit": UNIT, "ms_per_step": ems,
                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(16 * len(ih)),
-                       "api": "tensorjoin_variants_b200.join(host pinned R, S) -> host (i, j)"}
+                       "api": ("tensorjoin_variants_b200.join" if mode == "rs" else "tensorjoin_variants_b200.self_join")
+                              + "(host pinned inputs) -> host (i, j)"}
+        del Rh, Sh, ih, jh
 
-    # CPU baseline: the reference's exact CPU path on a bounded sample (rank 0 only)
-    if rank == 0 and not args.no_cpu and world == 1:
-        import oracle
-
-        rows = min(args.cpu_rows, w.R.shape[0])
-        rng = np.random.default_rng(7)
-        sample = w.R[np.sort(rng.choice(w.R.shape[0], rows, replace=False))]
-        Sn = w.R if w.S is None else w.S
-        procs = len(os.sched_getaffinity(0))
-        cp, secs, _ = oracle.scipy_rate(sample, Sn, T, procs, rows_per_task=2, repeats=1, context="spawn")
-        rate = cp / secs[0]
-        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": procs, "kind": "reference",
-                                "sample": f"scipy cdist sqeuclidean (the reference's exact CPU path), {rows} seeded R "
-                                          f"rows x all {len(Sn)} S rows, {procs} spawned processes, "
-                                          f"{secs[0]:.1f} s; full join extrapolated "
-                                          f"{w.candidate_pairs_all / rate:.0f} s"}
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    keys = _keys_np(keys_t)
+    del keys_t, R, S
+    torch.cuda.synchronize()
+    if rank == 0 and world == 1 and not args.no_parity:
+        line["parity"] = parity_audit(w.R, w.S, T, mode, keys, spec["audit_rows"])
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline_leg(w.R, w.R if w.S is None else w.S, T, args.cpu_rows,
+                                                w.candidate_pairs_all)
+    return line
 
 
 # ---------------------------------------------------------------------- config 5: batched ragged joins
@@ -443,13 +554,43 @@ def ragged_device(joins=4096, lo=256, hi=65536, dims=(8, 32, 128), clusters=8, s
     return [(out[k]["R"], out[k]["S"], eps[k]) for k in range(joins)], classes
 
 
-def ragged_bench(args, rank, world, screen, dist):
+def ragged_audit(joins, result, count: int, seed: int = 2025) -> dict:
+    """`count` seeded joins of the batch, each checked exhaustively by the CPU oracle against the
+    batch result's range for that join (local (i, j) keys i * |S| + j)."""
+    import oracle
+
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(seed)
+    pick = np.sort(rng.choice(len(joins), size=min(count, len(joins)), replace=False))
+    parts = result.split()
+    mism, pairs, evals = 0, 0, 0
+    worst = None
+    for k in pick:
+        R, S, e = joins[int(k)]
+        Rn, Sn = R.cpu().numpy(), S.cpu().numpy()
+        i, j = parts[int(k)]
+        got = i.cpu().numpy().astype(np.uint64) * np.uint64(Sn.shape[0]) + j.cpu().numpy().astype(np.uint64)
+        want = oracle.join_f32(Rn, Sn, e * e, "rs")
+        bad = int(np.setdiff1d(got, want).size + np.setdiff1d(want, got).size) if not np.array_equal(got, want) else 0
+        if bad and worst is None:
+            worst = int(k)
+        mism += bad
+        pairs += int(want.size)
+        evals += int(Rn.shape[0]) * int(Sn.shape[0])
+    return {"joins_checked": int(len(pick)), "pairs_checked": pairs, "pair_evaluations": evals,
+            "mismatches": mism, "first_bad_join": worst,
+            "oracle": f"FP64 sequential-k C oracle, exhaustive per join, {oracle.default_threads()} host threads",
+            "seconds": round(time.perf_counter() - t0, 2)}
+
+
+def bench_ragged(args, steps: int, warmup: int, rank, world, dist, headline: bool) -> dict:
     import torch
 
     import tensorjoin_variants_b200 as tj
     from tensorjoin_variants_b200 import _lib
 
-    scale = args.n / 11_800 if args.n else 1.0   # --n sets the mean side length
+    screen = (args.screen if headline else None) or WORKLOADS["ragged4096"]["screen"]
+    scale = (args.n / 11_800 if args.n else 1.0) if headline else 1.0   # --n sets the mean side length
     joins, classes = ragged_device(size_scale=scale)
     torch.cuda.synchronize()
     nj = len(joins)
@@ -458,26 +599,21 @@ def ragged_bench(args, rank, world, screen, dist):
     def step(scr):
         return tj.join_batched_result(joins, screen=scr, band_fp32=args.band_fp32)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         r = step(screen)
         del r
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    try:
-        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
-    except Exception:
-        gpu_id = "0"
-    clocks = Clocks(gpu_id)
+    clocks = Clocks(gpu_uuid())
     clocks.start()
-    time.sleep(0.3)
     l0 = _lib.lib().tj_kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
     stats = []
-    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    for s_ in range(args.steps):
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for s_ in range(steps):
         r = step(screen)
         stats.append(r.stats)
         pairs_out = r.count
@@ -487,16 +623,26 @@ def ragged_bench(args, rank, world, screen, dist):
     torch.cuda.synchronize()
     launches = _lib.lib().tj_kernel_launches() - l0
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    step_ms = [(e0 if k == 0 else marks[k - 1]).elapsed_time(marks[k]) for k in range(args.steps)]
+    ms = e0.elapsed_time(e1) / steps
+    step_ms = [(e0 if k == 0 else marks[k - 1]).elapsed_time(marks[k]) for k in range(steps)]
     ms = max_over_ranks(ms, world, dist)
     st = stats[-1]
     pairs = st["pairs_screened"]
     peaks = measured_peaks()
     screen_ms = statistics.mean(s["ms_screen"] for s in stats)
-    ops = statistics.mean(s["screen_ops"] for s in stats)
-    achieved = ops / (screen_ms / 1000.0) / 1e12
+    # algorithmic flops 2 d per pair summed over the joins' classes: from the library's count of
+    # issued ops, which is 6 d per pair with the hi/lo split and 2 d without
+    issued = statistics.mean(s["screen_ops"] for s in stats)
+    alg = issued / 3.0 if screen in ("bf16x3", "fp16x3") else issued
+    secs = screen_ms / 1000.0
     peak = peaks["tflops_sustained"] if screen != "plain" else None
+    roof = {"bound": "tensor" if screen != "plain" else "simt", "kernel": "screen_tc_kernel",
+            "achieved": alg / secs / 1e12, "peak": peak, "unit": "TFLOP/s",
+            "frac": (alg / secs / 1e12) / peak if peak else None,
+            "frac_algorithmic": (alg / secs / 1e12) / peak if peak else None,
+            "achieved_issued": issued / secs / 1e12, "frac_issued": (issued / secs / 1e12) / peak if peak else None,
+            "peak_source": f"{peaks['source']} bf16_tflops_sustained", "traffic": None,
+            "screen_ms": screen_ms, "flops_per_launch": alg, "issued_flops_per_launch": issued}
     # per-join latency: a seeded sample of joins run one at a time through tj.join
     rng = np.random.default_rng(11)
     lat = []
@@ -510,18 +656,13 @@ def ragged_bench(args, rank, world, screen, dist):
         lat.append(a.elapsed_time(b))
     line = {
         "metric": METRIC, "value": world * pairs / (ms / 1000.0), "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "steps": steps, "warmup": warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": screen, "data": "synthetic (seeded, drawn on the GPU)",
         "config": {"workload": "ragged4096", "joins": nj, "rows_r": int(sum(j[0].shape[0] for j in joins)),
                    "rows_s": int(sum(j[1].shape[0] for j in joins)), "dims": [8, 32, 128], "screen": screen,
                    "mean_side": 11_800 * scale, "l2": "inputs larger than L2 (no flush needed)",
                    "parallelism": f"replicas x{world}"},
-        "roofline": {"bound": "tensor" if screen != "plain" else "simt", "kernel": "screen_tc_kernel",
-                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None,
-                     "peak_source": f"{peaks['source']} bf16_tflops_sustained", "traffic": None,
-                     "screen_ms": screen_ms, "flops_per_launch": ops},
-        "clocks": clk, "gpu_launches": int(launches), "result_pairs": int(pairs_out),
+        "roofline": roof, "clocks": clk, "gpu_launches": int(launches), "result_pairs": int(pairs_out),
         "step_ms": step_ms, "lib_ms_total": [s["ms_total"] for s in stats],
         "stage_ms_per_step": [{k[3:]: round(s[k], 3) for k in ("ms_index", "ms_candidates", "ms_screen", "ms_refine",
                                                                "ms_sort")} for s in stats],
@@ -541,6 +682,7 @@ def ragged_bench(args, rank, world, screen, dist):
                                 "pairs_sampled": sd["screen_err_pairs"], "band_pairs": sd["band"],
                                 "refined_fraction": sd["band"] / max(1, sd["pairs_screened"])}
         del rd
+    r = step(screen)
     if not args.no_plain and screen != "plain":
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -548,11 +690,82 @@ def ragged_bench(args, rank, world, screen, dist):
         rp = step("plain")
         b.record(stream)
         torch.cuda.synchronize()
-        r = step(screen)
-        same = bool(torch.equal(rp.keys(), r.keys()))
         line["plain_gpu"] = {"ms_per_step": a.elapsed_time(b), "speedup_of_tc_path": a.elapsed_time(b) / ms,
-                             "identical_pair_set": same}
-        del rp, r
+                             "identical_pair_set": bool(torch.equal(rp.keys(), r.keys()))}
+        del rp
+    if not args.no_e2e:   # host-resident batch: every join's rows from pinned host memory, pairs back to the host
+        hj = [(Rd.cpu().pin_memory(), Sd.cpu().pin_memory(), e) for Rd, Sd, e in joins]
+        for _ in range(max(1, min(warmup, 2))):
+            tj.join_batched_result(hj, screen=screen).pairs()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        k_e2e = 2
+        for _ in range(k_e2e):
+            ih, jh = tj.join_batched_result(hj, screen=screen).pairs()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ems = a.elapsed_time(b) / k_e2e
+        h2d = sum(x.numel() * 4 + y.numel() * 4 for x, y, _ in hj)
+        line["e2e"] = {"value": world * pairs / (ems / 1000.0), "unit": UNIT, "ms_per_step": ems,
+                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(16 * len(ih)),
+                       "api": "tensorjoin_variants_b200.join_batched_result(host pinned joins).pairs() -> host (i, j)"}
+        del hj
+    if rank == 0 and world == 1 and not args.no_parity:
+        line["parity"] = ragged_audit(joins, r, WORKLOADS["ragged4096"]["audit_rows"])
+    if rank == 0 and world == 1 and not args.no_cpu:   # the reference's CPU path on one seeded join's rows
+        k = int(np.random.default_rng(7).integers(nj))
+        Rn, Sn, e = joins[k][0].cpu().numpy(), joins[k][1].cpu().numpy(), joins[k][2]
+        cb = cpu_baseline_leg(Rn, Sn, e * e, args.cpu_rows, int(st["pairs_all"]))
+        cb["sample"] += f" (join {k} of the batch; extrapolated to the batch's {int(st['pairs_all'])} pairs)"
+        line["cpu_baseline"] = cb
+    del r
+    return line
+
+
+# ---------------------------------------------------------------------- main
+def main() -> None:
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from tensorjoin_variants_b200 import _lib
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    if args.workload == "ragged4096":
+        line = bench_ragged(args, args.steps, args.warmup, rank, world, dist, True)
+    else:
+        line = bench_single(args.workload, args, args.steps, args.warmup, rank, world, dist, True)
+    # the other configurations under the same clock (default single-GPU run only)
+    run_subs = args.configs == "auto" and world == 1 and args.workload == "factor512" and not args.n and \
+        not args.screen
+    if run_subs:
+        subs = {}
+        sub_steps, sub_warm = max(1, min(args.steps, args.sub_steps)), max(3, min(args.warmup, 3))
+        for name in SUB_CONFIGS:
+            _lib.lib().tj_pool_trim(0)
+            torch.cuda.empty_cache()
+            t0 = time.time()
+            try:
+                if name == "ragged4096":
+                    rec = bench_ragged(args, sub_steps, sub_warm, rank, world, dist, False)
+                else:
+                    rec = bench_single(name, args, sub_steps, sub_warm, rank, world, dist, False)
+            except Exception as exc:   # report the failure in the line; the headline stands
+                rec = {"error": f"{type(exc).__name__}: {exc}"}
+            rec["wall_s"] = round(time.time() - t0, 1)
+            subs[name] = rec
+        line["configs"] = subs
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -87,6 +87,20 @@ typedef struct tj_options {
  * cannot decide go on to the sequential FP64 terminal (tj_stats.band_fp64 counts them).  The
  * pairs are the same either way.  No effect on the plain and int8-limb screens. */
 #define TJ_FLAG_BAND_FP32 16
+/* int8-limb screen: issue all four limb products (hh, hl + lh, ll) on the tensor cores and decide
+ * every pair exactly inside the screen (no band).  By default, for rows of up to 256 elements, the
+ * screen issues only the high-limb product hh, bounds the low-limb terms by Cauchy-Schwarz, decides
+ * each candidate by an exact INT64 interval test, and sends the few undecided pairs to the exact
+ * integer refinement (tj_stats.band).  The pairs are the same either way. */
+#define TJ_FLAG_I8_FOUR_PRODUCTS 32
+/* Guard regions: 512 words of a fixed pattern (every byte -17, the reference's fill for retained
+ * buffers) right after the part of the accept, band, result-key and sort buffers that a stage may
+ * write, checked after the stage; an overwritten guard fails the join with TJ_ERR_CUDA.  A bounds
+ * check in place of a memory sanitizer; costs four tiny launches per stage. */
+#define TJ_FLAG_GUARDS 64
+/* Keep the screen's own decisions in the result: its certified accepts and its band, before the
+ * refinement, each sorted (tj_result_stage_keys).  For auditing each stage against an oracle. */
+#define TJ_FLAG_STAGE_KEYS 128
 
 typedef struct tj_stats {
     int64_t n_rows, n_cols;       /* |R|, |S| (self-join: N, N) */
@@ -108,6 +122,8 @@ typedef struct tj_stats {
     int64_t index_frame;          /* 1 if the index cells were over principal directions, 0 if over
                                      input dimensions */
     int64_t band_fp64;            /* band pairs decided by the FP64 terminal */
+    double screen_ops_issued;     /* tensor-core operations the screen issued: 2 M N K per MMA over every
+                                     tile pair it ran (padded rows, columns and K included) */
 } tj_stats;
 
 /* ----------------------------------------------------------------- joins */
@@ -125,6 +141,13 @@ int tj_result_stats(const tj_result* res, tj_stats* out);
 int tj_result_pairs(const tj_result* res, int64_t* i_out, int64_t* j_out, void* stream);
 /* Sorted canonical keys i * n_cols + j (uint64 device array of tj_result_count() elements). */
 int tj_result_keys(const tj_result* res, uint64_t* keys_out, void* stream);
+/* TJ_FLAG_STAGE_KEYS results: stage 0 = the pairs the screen accepted by its certificate alone,
+ * stage 1 = the band it passed to the refinement, as sorted canonical keys (self-joins: i < j, the
+ * screen's form, also in directed mode).  *count receives the number of keys; keys_out (device,
+ * *count elements) may be NULL to query the count.  No counterpart in the reference as an API; it
+ * serves the per-stage audit the reference ran against its oracle
+ * (src/run_g2a_tensorjoin.py:384-469). */
+int tj_result_stage_keys(const tj_result* res, int32_t stage, uint64_t* keys_out, int64_t* count, void* stream);
 /* GDS-style neighbour table: counts[n_rows] (uint32, device) and the flat j list (int64, device). */
 int tj_result_neighbor_table(const tj_result* res, uint32_t* counts_out, int64_t* flat_out, void* stream);
 void tj_result_free(tj_result* res);
@@ -174,6 +197,14 @@ int tj_batch_pairs(const tj_result* res, int64_t* i_out, int64_t* j_out, void* s
 int tj_sort_keys_noalloc(const uint64_t* keys_in, uint64_t* keys_out, int64_t n, int32_t key_bits, void* stream);
 
 /* ----------------------------------------------------------------- misc */
+/* Every wait inside the screen kernels is bounded: a kernel whose wait runs out sets a status bit,
+ * lets its copies and tensor-core operations in flight finish (each of those waits bounded by 1 s),
+ * frees its tensor memory and returns, and the join fails with TJ_ERR_TIMEOUT; the context stays
+ * usable.  This sets the limit of the pipeline waits (between the copy, MMA and epilogue roles) for
+ * joins started on the calling thread, in nanoseconds; 0 restores the default of 4 s.  No
+ * counterpart in the reference (its kernels have no bounded waits).  Meant for tests of the timeout
+ * path: a limit below the pipeline's normal latency makes joins fail. */
+int tj_set_wait_limit(int64_t ns);
 const char* tj_last_error_string(void);
 int tj_version(void);
 int tj_device_sm_count(void);

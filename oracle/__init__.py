@@ -62,8 +62,13 @@ def lib():
         L.oracle_pair_d2_f32.argtypes = [P, P, C.c_int, P, P, C.c_int64, P]
         L.oracle_row_counts_f32.argtypes = [P, C.c_int64, P, C.c_int64, C.c_int, C.c_double, P, C.c_int64, P]
         L.oracle_row_counts_f32.restype = C.c_int
+        L.oracle_pair_d2_f32_mt.argtypes = [P, P, C.c_int, P, P, C.c_int64, P, C.c_int]
+        L.oracle_pair_d2_f32_mt.restype = C.c_int
+        L.oracle_pair_d2_i16_mt.argtypes = [P, P, C.c_int, P, P, C.c_int64, P, C.c_int]
+        L.oracle_pair_d2_i16_mt.restype = C.c_int
         L.oracle_abi_version.restype = C.c_int
-        assert L.oracle_abi_version() == 1
+        if L.oracle_abi_version() != 2:
+            raise RuntimeError(f"{LIB_PATH} is a stale build: run oracle.build()")
         _lib = L
     return _lib
 
@@ -116,6 +121,28 @@ def pair_d2(R: np.ndarray, S: np.ndarray, i: np.ndarray, j: np.ndarray) -> np.nd
     out = np.empty(len(i), dtype=np.float64)
     lib().oracle_pair_d2_f32(R.ctypes.data, S.ctypes.data, R.shape[1], i.ctypes.data, j.ctypes.data, len(i),
                              out.ctypes.data)
+    return out
+
+
+def pair_d2_mt(R: np.ndarray, S: np.ndarray, i: np.ndarray, j: np.ndarray, threads: int | None = None) -> np.ndarray:
+    """Squared distances of explicit pairs (R[i], S[j]) over host threads: sequential-order FP64 for
+    FP32 rows (float64 result), exact int64 for int16 rows (int64 result)."""
+    is_int = np.asarray(R).dtype == np.int16
+    dt = np.int16 if is_int else np.float32
+    R = np.ascontiguousarray(R, dtype=dt)
+    S = np.ascontiguousarray(S, dtype=dt)
+    i = np.ascontiguousarray(i, dtype=np.int64)
+    j = np.ascontiguousarray(j, dtype=np.int64)
+    if len(i) != len(j):
+        raise ValueError("i and j differ in length")
+    if len(i) and (i.min() < 0 or i.max() >= R.shape[0] or j.min() < 0 or j.max() >= S.shape[0]):
+        raise IndexError("pair index out of range")
+    out = np.empty(len(i), dtype=np.int64 if is_int else np.float64)
+    fn = lib().oracle_pair_d2_i16_mt if is_int else lib().oracle_pair_d2_f32_mt
+    rc = fn(R.ctypes.data, S.ctypes.data, R.shape[1], i.ctypes.data, j.ctypes.data, len(i), out.ctypes.data,
+            threads or default_threads())
+    if rc != 0:
+        raise RuntimeError(f"oracle failed with code {rc}")
     return out
 
 

@@ -70,11 +70,14 @@ static inline double seq_d2_f32(const float *x, const float *y, int d) {
     return acc;
 }
 
-static inline int64_t seq_d2_i16(const int16_t *x, const int16_t *y, int d) {
+/* Exact integer squared distance of two int16 rows in int64 (any int16 values: |x - y| <= 65535,
+ * so each difference fits int32 and its square int64).  Integer addition is associative, so the
+ * order of the sum does not matter and the compiler may vectorise it across k. */
+static inline int64_t exact_d2_i16(const int16_t *x, const int16_t *y, int d) {
     int64_t acc = 0;
     for (int k = 0; k < d; ++k) {
-        int64_t t = (int64_t)x[k] - (int64_t)y[k];
-        acc += t * t;
+        const int32_t t = (int32_t)x[k] - (int32_t)y[k];
+        acc += (int64_t)t * (int64_t)t;
     }
     return acc;
 }
@@ -93,65 +96,96 @@ typedef struct {
     keybuf out;
 } job_t;
 
-#define JB 8
+#define JB 8   /* S rows per block (transposed to k-major doubles) */
+#define RB 16  /* R rows per block: each S block is loaded once per R block */
 
+/* Four independent FP64 lanes (GCC vector extension): lane-wise IEEE operations, each lane one
+ * pair's own accumulator, so the vectorisation is across pairs and never reorders a sum. */
+typedef double v4d __attribute__((vector_size(32)));
+
+static int cmp_u64(const void *a, const void *b) {
+    const uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+    return x < y ? -1 : x > y;
+}
+
+/* acc[r][jj] = sequential-k sum of (x_r[k] - blk[k][jj])^2 for two R rows and the JB S rows of blk. */
+static inline void block_sums(const double *x0, const double *x1, const double *blk, int d, double out[2][JB]) {
+    v4d a00 = {0, 0, 0, 0}, a01 = a00, a10 = a00, a11 = a00;
+    for (int k = 0; k < d; ++k) {
+        v4d b0, b1;
+        memcpy(&b0, blk + (size_t)k * JB, sizeof(v4d));
+        memcpy(&b1, blk + (size_t)k * JB + 4, sizeof(v4d));
+        const v4d u = {x0[k], x0[k], x0[k], x0[k]};
+        const v4d w = {x1[k], x1[k], x1[k], x1[k]};
+        v4d t;
+        t = u - b0; t = t * t; a00 = a00 + t;
+        t = u - b1; t = t * t; a01 = a01 + t;
+        t = w - b0; t = t * t; a10 = a10 + t;
+        t = w - b1; t = t * t; a11 = a11 + t;
+    }
+    memcpy(out[0], &a00, sizeof(v4d));
+    memcpy(out[0] + 4, &a01, sizeof(v4d));
+    memcpy(out[1], &a10, sizeof(v4d));
+    memcpy(out[1] + 4, &a11, sizeof(v4d));
+}
+
+/*
+ * Rows [row0, row1) of R against S.  Blocks of RB R rows sweep S in blocks of JB rows, so S is
+ * streamed from memory once per R block instead of once per R row; every pair still has its own
+ * accumulator and its own sequential k order (the blocking changes which pairs are computed
+ * together, never how one pair's sum is formed).  Keys of an R block are sorted before the next
+ * block starts, so each thread's output stays ascending.
+ *
+ * int16 rows run through the same FP64 lanes: every difference (|t| <= 65535), square (< 2^32) and
+ * partial sum (< d 2^32 <= 2^53 for d <= 2^21) is an integer that FP64 holds exactly, so the sum is
+ * the exact integer squared distance, compared with the integer threshold after conversion.
+ */
 static void *worker(void *arg) {
     job_t *jb = (job_t *)arg;
     const int d = jb->d;
-    if (!jb->is_int) {
-        const float *R = (const float *)jb->R;
-        const float *S = (const float *)jb->S;
-        double *blk = (double *)malloc((size_t)d * JB * sizeof(double));
-        double *xr = (double *)malloc((size_t)d * sizeof(double));
-        if (!blk || !xr) { free(blk); free(xr); jb->out.failed = 1; return NULL; }
-        for (int64_t i = jb->row0; i < jb->row1; ++i) {
-            const float *x = R + (size_t)i * d;
-            for (int k = 0; k < d; ++k) xr[k] = (double)x[k];
-            int64_t j0 = (jb->mode == 1) ? i + 1 : 0;
-            for (int64_t jb0 = j0; jb0 < jb->nS; jb0 += JB) {
-                int nb = (int)((jb->nS - jb0) < JB ? (jb->nS - jb0) : JB);
-                if (nb == JB) {
-                    /* transpose eight S rows to k-major doubles: acc[jj] keeps its own sequential k order */
-                    for (int jj = 0; jj < JB; ++jj) {
-                        const float *y = S + (size_t)(jb0 + jj) * d;
-                        for (int k = 0; k < d; ++k) blk[(size_t)k * JB + jj] = (double)y[k];
-                    }
-                    double acc[JB];
-                    for (int jj = 0; jj < JB; ++jj) acc[jj] = 0.0;
-                    for (int k = 0; k < d; ++k) {
-                        const double xv = xr[k];
-                        const double *bk = blk + (size_t)k * JB;
-                        for (int jj = 0; jj < JB; ++jj) {
-                            double t = xv - bk[jj];
-                            double sq = t * t;
-                            acc[jj] = acc[jj] + sq;
-                        }
-                    }
-                    for (int jj = 0; jj < JB; ++jj)
-                        if (acc[jj] <= jb->T) kb_push(&jb->out, (uint64_t)i * (uint64_t)jb->nS + (uint64_t)(jb0 + jj));
-                } else {
+    const int64_t nS = jb->nS;
+    double *blk = (double *)malloc((size_t)d * JB * sizeof(double));
+    double *xr = (double *)malloc((size_t)d * (RB + 1) * sizeof(double));
+    if (!blk || !xr) {
+        free(blk); free(xr);
+        jb->out.failed = 1;
+        return NULL;
+    }
+    for (int64_t i0 = jb->row0; i0 < jb->row1; i0 += RB) {
+        const int nr = (int)((jb->row1 - i0) < RB ? (jb->row1 - i0) : RB);
+        const int64_t mark = jb->out.n;
+        for (int r = 0; r < nr; ++r)
+            for (int k = 0; k < d; ++k)
+                xr[(size_t)r * d + k] = jb->is_int ? (double)((const int16_t *)jb->R)[(size_t)(i0 + r) * d + k]
+                                                   : (double)((const float *)jb->R)[(size_t)(i0 + r) * d + k];
+        for (int k = 0; k < d; ++k) xr[(size_t)nr * d + k] = 0.0;   /* partner of an odd last row */
+        const int64_t jstart = (jb->mode == 1) ? i0 + 1 : 0;
+        for (int64_t jb0 = jstart; jb0 < nS; jb0 += JB) {
+            const int nb = (int)((nS - jb0) < JB ? (nS - jb0) : JB);
+            for (int jj = 0; jj < JB; ++jj) {
+                const size_t row = (size_t)(jb0 + (jj < nb ? jj : 0)) * d;
+                for (int k = 0; k < d; ++k)
+                    blk[(size_t)k * JB + jj] = jb->is_int ? (double)((const int16_t *)jb->S)[row + k]
+                                                          : (double)((const float *)jb->S)[row + k];
+            }
+            for (int r = 0; r < nr; r += 2) {
+                double acc[2][JB];
+                block_sums(xr + (size_t)r * d, xr + (size_t)(r + 1) * d, blk, d, acc);
+                for (int h = 0; h < 2 && r + h < nr; ++h) {
+                    const int64_t i = i0 + r + h;
                     for (int jj = 0; jj < nb; ++jj) {
-                        const float *y = S + (size_t)(jb0 + jj) * d;
-                        if (seq_d2_f32(x, y, d) <= jb->T)
-                            kb_push(&jb->out, (uint64_t)i * (uint64_t)jb->nS + (uint64_t)(jb0 + jj));
+                        const int64_t j = jb0 + jj;
+                        if (jb->mode == 1 && j <= i) continue;
+                        const int in = jb->is_int ? ((int64_t)acc[h][jj] <= jb->Ti) : (acc[h][jj] <= jb->T);
+                        if (in) kb_push(&jb->out, (uint64_t)i * (uint64_t)nS + (uint64_t)j);
                     }
                 }
             }
         }
-        free(blk);
-        free(xr);
-    } else {
-        const int16_t *R = (const int16_t *)jb->R;
-        const int16_t *S = (const int16_t *)jb->S;
-        for (int64_t i = jb->row0; i < jb->row1; ++i) {
-            const int16_t *x = R + (size_t)i * d;
-            int64_t j0 = (jb->mode == 1) ? i + 1 : 0;
-            for (int64_t j = j0; j < jb->nS; ++j) {
-                if (seq_d2_i16(x, S + (size_t)j * d, d) <= jb->Ti)
-                    kb_push(&jb->out, (uint64_t)i * (uint64_t)jb->nS + (uint64_t)j);
-            }
-        }
+        if (jb->out.n - mark > 1)
+            qsort(jb->out.keys + mark, (size_t)(jb->out.n - mark), sizeof(uint64_t), cmp_u64);
     }
+    free(blk); free(xr);
     return NULL;
 }
 
@@ -243,6 +277,62 @@ void oracle_pair_d2_f32(const float *R, const float *S, int d, const int64_t *ii
     for (int64_t p = 0; p < n; ++p) out[p] = seq_d2_f32(R + (size_t)ii[p] * d, S + (size_t)jj[p] * d, d);
 }
 
+/* The same for many pairs over `nthreads` threads (contiguous pair ranges), FP32 or int16 rows
+ * (int16: exact int64 squared distances). */
+typedef struct {
+    const void *R, *S;
+    int d, is_int;
+    const int64_t *ii, *jj;
+    int64_t p0, p1;
+    void *out;
+} pair_job_t;
+
+static void *pair_worker(void *arg) {
+    pair_job_t *j = (pair_job_t *)arg;
+    const int d = j->d;
+    if (!j->is_int) {
+        const float *R = (const float *)j->R, *S = (const float *)j->S;
+        double *o = (double *)j->out;
+        for (int64_t p = j->p0; p < j->p1; ++p) o[p] = seq_d2_f32(R + (size_t)j->ii[p] * d, S + (size_t)j->jj[p] * d, d);
+    } else {
+        const int16_t *R = (const int16_t *)j->R, *S = (const int16_t *)j->S;
+        int64_t *o = (int64_t *)j->out;
+        for (int64_t p = j->p0; p < j->p1; ++p) o[p] = exact_d2_i16(R + (size_t)j->ii[p] * d, S + (size_t)j->jj[p] * d, d);
+    }
+    return NULL;
+}
+
+static int pair_run(const void *R, const void *S, int d, int is_int, const int64_t *ii, const int64_t *jj,
+                    int64_t n, void *out, int nthreads) {
+    if (d <= 0 || n < 0) return -2;
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    if (n < (int64_t)nthreads * 1024) nthreads = 1;
+    pair_job_t *jobs = (pair_job_t *)calloc((size_t)nthreads, sizeof(pair_job_t));
+    pthread_t *th = (pthread_t *)calloc((size_t)nthreads, sizeof(pthread_t));
+    if (!jobs || !th) { free(jobs); free(th); return -1; }
+    for (int t = 0; t < nthreads; ++t) {
+        pair_job_t j = {R, S, d, is_int, ii, jj, n * t / nthreads, n * (t + 1) / nthreads, out};
+        jobs[t] = j;
+    }
+    for (int t = 1; t < nthreads; ++t) pthread_create(&th[t], NULL, pair_worker, &jobs[t]);
+    pair_worker(&jobs[0]);
+    for (int t = 1; t < nthreads; ++t) pthread_join(th[t], NULL);
+    free(jobs);
+    free(th);
+    return 0;
+}
+
+int oracle_pair_d2_f32_mt(const float *R, const float *S, int d, const int64_t *ii, const int64_t *jj, int64_t n,
+                          double *out, int nthreads) {
+    return pair_run(R, S, d, 0, ii, jj, n, out, nthreads);
+}
+
+int oracle_pair_d2_i16_mt(const int16_t *R, const int16_t *S, int d, const int64_t *ii, const int64_t *jj, int64_t n,
+                          int64_t *out, int nthreads) {
+    return pair_run(R, S, d, 1, ii, jj, n, out, nthreads);
+}
+
 /* Per-row counts of neighbours (row-major scan, no key materialisation); used for large-sample audits. */
 int oracle_row_counts_f32(const float *R, int64_t nR, const float *S, int64_t nS, int d, double T,
                           const int64_t *rows, int64_t nrows, int64_t *counts) {
@@ -257,4 +347,4 @@ int oracle_row_counts_f32(const float *R, int64_t nR, const float *S, int64_t nS
 }
 
 /* Version tag so Python can check it loaded the expected build. */
-int oracle_abi_version(void) { return 1; }
+int oracle_abi_version(void) { return 2; }

@@ -26,6 +26,9 @@ FLAG_SCREEN_1SM = 2
 FLAG_FRAME_AXES = 4
 FLAG_FRAME_PCA = 8
 FLAG_BAND_FP32 = 16
+FLAG_I8_FOUR_PRODUCTS = 32
+FLAG_GUARDS = 64
+FLAG_STAGE_KEYS = 128
 
 # Every symbol include/tensorjoin.h declares (checked by the CPU test suite).
 EXPORTS = [
@@ -33,7 +36,7 @@ EXPORTS = [
     "tj_result_neighbor_table", "tj_result_free", "tj_index_build", "tj_index_info", "tj_index_copy",
     "tj_index_free", "tj_join_batched", "tj_batch_offsets", "tj_batch_pairs", "tj_last_error_string",
     "tj_version", "tj_device_sm_count", "tj_kernel_launches", "tj_sort_keys_noalloc",
-    "tj_pool_usage", "tj_pool_reserve", "tj_pool_trim",
+    "tj_pool_usage", "tj_pool_reserve", "tj_pool_trim", "tj_set_wait_limit", "tj_result_stage_keys",
 ]
 
 
@@ -53,7 +56,8 @@ class Stats(C.Structure):
         "refine_accept", "rare_checks", "result_pairs", "retries")] + [(n, C.c_double) for n in (
         "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total", "screen_ops",
         "screen_max_abs_err", "screen_err_over_bound")] + [("screen_err_pairs", C.c_int64), ("screen_pair", C.c_int64),
-                                                   ("index_frame", C.c_int64), ("band_fp64", C.c_int64)]
+                                                   ("index_frame", C.c_int64), ("band_fp64", C.c_int64),
+                                                   ("screen_ops_issued", C.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -105,6 +109,10 @@ def lib() -> C.CDLL:
     L.tj_pool_reserve.restype = C.c_int
     L.tj_pool_trim.argtypes = [I64]
     L.tj_pool_trim.restype = C.c_int
+    L.tj_set_wait_limit.argtypes = [I64]
+    L.tj_set_wait_limit.restype = C.c_int
+    L.tj_result_stage_keys.argtypes = [P, I32, P, C.POINTER(I64), P]
+    L.tj_result_stage_keys.restype = C.c_int
     for name in ("tj_join", "tj_result_stats", "tj_result_pairs", "tj_result_keys", "tj_result_neighbor_table",
                  "tj_index_build", "tj_index_info", "tj_index_copy", "tj_join_batched", "tj_batch_offsets",
                  "tj_batch_pairs"):

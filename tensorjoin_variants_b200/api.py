@@ -122,6 +122,17 @@ class Result:
             check(lib().tj_result_keys(self._h, C.c_void_p(k.data_ptr()), C.c_void_p(_stream_ptr())))
         return self._out(k)[0]
 
+    def stage_keys(self, stage: int):
+        """The screen's own decisions (join run with ``stage_keys=True``): stage 0 = pairs it accepted
+        by its certificate alone, stage 1 = its band, as sorted canonical keys (i < j for self-joins)."""
+        n = C.c_int64()
+        check(lib().tj_result_stage_keys(self._h, int(stage), None, C.byref(n), C.c_void_p(_stream_ptr())))
+        k = torch.empty(n.value, dtype=torch.int64, device="cuda")
+        if n.value:
+            check(lib().tj_result_stage_keys(self._h, int(stage), C.c_void_p(k.data_ptr()), C.byref(n),
+                                             C.c_void_p(_stream_ptr())))
+        return self._out(k)[0]
+
     def neighbor_table(self):
         """GDS-style output: neighbour counts per row and the flat, row-ordered neighbour list."""
         counts = torch.empty(self.n_rows, dtype=torch.int32, device="cuda")
@@ -159,7 +170,8 @@ FRAME_FLAGS = {"auto": 0, "axes": _lib.FLAG_FRAME_AXES, "pca": _lib.FLAG_FRAME_P
 
 def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "bf16", capacity: int = 0,
                 chunk_items: int = 0, screen_diag: bool = False, cta_pair: bool = True,
-                index_frame: str = "auto", band_fp32: bool = False) -> Result:
+                index_frame: str = "auto", band_fp32: bool = False, i8_four_products: bool = False,
+                guards: bool = False, stage_keys: bool = False) -> Result:
     """Run a join and return the Result handle (pairs, keys, neighbour table, statistics).
 
     ``screen_diag=True`` also samples 64 tile pairs of the tensor-core screen and reports, in
@@ -170,13 +182,19 @@ def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "b
     highest-variance input dimensions) or "pca" (the top 8 principal directions, 9 <= d <= 128);
     ``stats["index_frame"]`` is 1 where the principal-direction cells were used.
     ``band_fp32=True`` decides band pairs by a certified FP32 sum first and sends only the rest to
-    the FP64 terminal (``stats["band_fp64"]`` counts those)."""
+    the FP64 terminal (``stats["band_fp64"]`` counts those).  ``i8_four_products=True`` makes the
+    int8-limb screen issue all four limb products and decide every pair inside the screen, instead of
+    the high-limb product plus an exact integer refinement of the undecided band.  ``guards=True``
+    checks guard regions after every output buffer (an overwrite fails the join); ``stage_keys=True``
+    keeps the screen's certified accepts and its band for ``Result.stage_keys``."""
     if mode not in MODE:
         raise ValueError(f"mode must be one of {sorted(MODE)}")
     if index_frame not in FRAME_FLAGS:
         raise ValueError(f"index_frame must be one of {sorted(FRAME_FLAGS)}")
     flags = (_lib.FLAG_SCREEN_DIAG if screen_diag else 0) | (0 if cta_pair else _lib.FLAG_SCREEN_1SM)
     flags |= FRAME_FLAGS[index_frame] | (_lib.FLAG_BAND_FP32 if band_fp32 else 0)
+    flags |= _lib.FLAG_I8_FOUR_PRODUCTS if i8_four_products else 0
+    flags |= (_lib.FLAG_GUARDS if guards else 0) | (_lib.FLAG_STAGE_KEYS if stage_keys else 0)
     return _run(R, S, eps, eps2, mode, screen, capacity, chunk_items, flags)
 
 

@@ -39,8 +39,10 @@ int g_sms[64] = {};
 
 namespace {
 std::atomic<long long> g_launches{0};
+thread_local unsigned long long g_wait_ns = kWaitLimitNs;   // pipeline wait limit of this thread's joins
 }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long pipeline_wait_ns() { return g_wait_ns; }
 
 namespace {
 struct StageChunk {
@@ -96,14 +98,30 @@ int num_sms() {
 namespace {
 
 struct ScreenOps {
-    unsigned long long per_pair[kMaxClass];
+    unsigned long long per_pair[kMaxClass];   // algorithmic operations per screened pair
+    double per_item[kMaxClass];               // tensor-core operations issued per tile pair
 };
 
 __global__ void zero_counters(Counters* c, int emit_only) {
     unsigned long long* w = (unsigned long long*)c;
-    const int n = emit_only ? 8 : (int)(sizeof(Counters) / 8);
+    const int n = emit_only ? kCountersPerAttempt : (int)(sizeof(Counters) / 8);
     for (int i = threadIdx.x; i < n; i += blockDim.x) w[i] = 0;
 }
+
+// Guard regions (TJ_FLAG_GUARDS): kGuardSlots words of a fixed pattern written right after the
+// part of an output buffer a stage may write, and checked after the stage.  The pattern is -17 in
+// every byte, the reference's fill for its retained buffers.
+constexpr unsigned long long kGuardSlots = 512;
+constexpr uint64_t kGuardWord = 0xEFEFEFEFEFEFEFEFull;
+__global__ void guard_fill(uint64_t* p) {
+    for (unsigned i = threadIdx.x; i < kGuardSlots; i += blockDim.x) p[i] = kGuardWord;
+}
+__global__ void guard_check(const uint64_t* p, Counters* c) {
+    bool bad = false;
+    for (unsigned i = threadIdx.x; i < kGuardSlots; i += blockDim.x) bad |= p[i] != kGuardWord;
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&c->status, (unsigned long long)kStatusGuard);
+}
+__global__ void snapshot_reserved(Counters* c) { c->screen_reserved = c->acc_reserved; }
 
 __global__ void cell_flags(const uint64_t* keys, long long n, uint32_t* flag) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -115,12 +133,13 @@ __global__ void cell_starts(const uint32_t* flag, const uint32_t* pos, long long
     if (i < n && flag[i]) start[pos[i]] = (uint32_t)i;
     if (i == 0) start[*ncells] = (uint32_t)n;
 }
-// Distance evaluations of the candidate list (out[0]) and algorithmic screen operations (out[1]),
-// ops_per_pair[c] = 2 d (16-bit), 6 d (hi/lo split) or 8 d (int8 limbs) for class c.
+// Distance evaluations of the candidate list (out[0] = pairs_screened), algorithmic screen operations
+// (out[1], ops_per_pair[c] = 2 d (16-bit), 6 d (hi/lo split) or 8 d (int8 limbs) for class c) and tile
+// pairs per class (out[2 + c] = class_items[c], for the issued-operation count).
 __global__ void pairs_screened_kernel(const uint4* chunks, const uint32_t* nchunks, const uint32_t* jlist,
                                       const uint4* rtiles, const uint4* stiles, const ScreenOps ops,
                                       unsigned long long* out) {
-    unsigned long long acc = 0, aops = 0;
+    unsigned long long acc = 0, aops = 0, items[kMaxClass] = {0, 0, 0, 0};
     const unsigned n = *nchunks;
     for (unsigned c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         const uint4 ch = chunks[c];
@@ -130,14 +149,21 @@ __global__ void pairs_screened_kernel(const uint4* chunks, const uint32_t* nchun
         for (unsigned e = ch.y; e < ch.z; ++e) p += rv * stiles[jlist[e]].y;
         acc += p;
         aops += p * ops.per_pair[rt.w];
+#pragma unroll
+        for (int q = 0; q < kMaxClass; ++q) items[q] += rt.w == (unsigned)q ? ch.z - ch.y : 0u;
     }
     for (int o = 16; o > 0; o >>= 1) {
         acc += __shfl_xor_sync(0xffffffffu, acc, o);
         aops += __shfl_xor_sync(0xffffffffu, aops, o);
+#pragma unroll
+        for (int q = 0; q < kMaxClass; ++q) items[q] += __shfl_xor_sync(0xffffffffu, items[q], o);
     }
     if ((threadIdx.x & 31) == 0 && acc) {
         atomicAdd(out, acc);
         atomicAdd(out + 1, aops);
+#pragma unroll
+        for (int q = 0; q < kMaxClass; ++q)
+            if (items[q]) atomicAdd(out + 2 + q, items[q]);
     }
 }
 __global__ void tile_pair_list(const uint4* chunks, const uint32_t* nchunks, const uint32_t* jlist, uint32_t* out) {
@@ -213,6 +239,9 @@ using namespace tj;
 struct tj_result {
     DBuf<uint64_t> keys;       // sorted canonical keys (first `count` valid)
     long long count = 0;
+    // TJ_FLAG_STAGE_KEYS: the screen's certified accepts (0) and its band (1), sorted, first stage_n valid
+    DBuf<uint64_t> stage[2];
+    long long stage_n[2] = {0, 0};
     long long n_rows = 0, n_cols = 0;
     tj_stats stats;
     // batched mode (njoins > 1): per-join output ranges and key decoding tables
@@ -254,6 +283,7 @@ void check_status(unsigned long long status) {
     if (status & kStatusBadInput) fail(TJ_ERR_INPUT, "input contains NaN/Inf or a row norm beyond 2^50");
     if (status & kStatusFp16Range) fail(TJ_ERR_RANGE, "input magnitude exceeds the FP16 range; use the BF16 screen");
     if (status & kStatusTmemAlloc) fail(TJ_ERR_CUDA, "tensor memory allocation failed");
+    if (status & kStatusGuard) fail(TJ_ERR_CUDA, "a guard region after an output buffer was overwritten");
 }
 
 struct JoinIn {
@@ -267,7 +297,7 @@ struct JoinIn {
 void check_flags(const tj_options* opt) {
     if (!opt) return;
     const int known = TJ_FLAG_SCREEN_DIAG | TJ_FLAG_SCREEN_1SM | TJ_FLAG_FRAME_AXES | TJ_FLAG_FRAME_PCA |
-                      TJ_FLAG_BAND_FP32;
+                      TJ_FLAG_BAND_FP32 | TJ_FLAG_I8_FOUR_PRODUCTS | TJ_FLAG_GUARDS | TJ_FLAG_STAGE_KEYS;
     if (opt->flags & ~known) fail(TJ_ERR_INVALID, "unknown option flags");
     if ((opt->flags & TJ_FLAG_FRAME_AXES) && (opt->flags & TJ_FLAG_FRAME_PCA))
         fail(TJ_ERR_INVALID, "TJ_FLAG_FRAME_AXES and TJ_FLAG_FRAME_PCA exclude each other");
@@ -494,6 +524,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     g.jps = d_jps.p;
     g.h_jps = jps.data();
     g.allow_pair = !(opt && (opt->flags & TJ_FLAG_SCREEN_1SM));
+    g.i8_four_products = opt && (opt->flags & TJ_FLAG_I8_FOUR_PRODUCTS);
     g.key_off = d_koff.p;
     g.rsrc = d_rsrc.p;
     g.ssrc = d_ssrc.p;
@@ -542,11 +573,15 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     g.cand = &cand;
     ScreenOps sops;
     memset(&sops, 0, sizeof(sops));
-    for (int c = 0; c < ncls; ++c)
+    for (int c = 0; c < ncls; ++c) {
         sops.per_pair[c] = (unsigned long long)cls_d[c] * (i8 ? 8ull : (C[c]->R.split ? 6ull : 2ull));
+        // one tile pair issues 2 M N K per product: 128 x 256 (16-bit, 3 products with the split) or
+        // 128 x 128 (int8: the high-limb screen issues hh only)
+        sops.per_item[c] = 2.0 * kTileR * (double)stile * (double)C[c]->R.kpad * (C[c]->R.split ? 3.0 : 1.0);
+    }
     launch(pairs_screened_kernel, num_sms() * 4, 256, 0, st, (const uint4*)cand.chunks.p,
            (const uint32_t*)(cand.dev_counts.p + 1), (const uint32_t*)cand.jlist.p, (const uint4*)d_rt.p,
-           (const uint4*)d_st.p, sops, &ctr.p->pad[0]);
+           (const uint4*)d_st.p, sops, &ctr.p->pairs_screened);
     ev.rec(6, st);
 
     // optional screen-error sampling (tensor-core screens): 64 tile pairs spread over the candidate list
@@ -579,12 +614,19 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
                                                                 : std::max<unsigned long long>(1ull << 20, per * sum_max);
     unsigned long long bcap = (opt && opt->initial_capacity > 0) ? cap : std::max<unsigned long long>(1ull << 20,
                                                                                                    cap / (nj == 1 ? 1 : 8));
+    const bool guards = opt && (opt->flags & TJ_FLAG_GUARDS);
+    const bool stage_keys = opt && (opt->flags & TJ_FLAG_STAGE_KEYS);
+    const unsigned long long gs = guards ? kGuardSlots : 0;
     DBuf<uint64_t> acc, band;
     Counters h;
     for (int attempt = 0;; ++attempt) {
-        acc = DBuf<uint64_t>::result(cap, st);   // becomes the result's key array
-        band = DBuf<uint64_t>(bcap, st);
+        acc = DBuf<uint64_t>::result(cap + gs, st);   // becomes the result's key array
+        band = DBuf<uint64_t>(bcap + gs, st);
         launch(zero_counters, 1, 32, 0, st, ctr.p, 1);
+        if (guards) {
+            launch(guard_fill, 1, 256, 0, st, acc.p + cap);
+            launch(guard_fill, 1, 256, 0, st, band.p + bcap);
+        }
         EmitBuffers eb{acc.p, cap, band.p, bcap, ctr.p};
         ev.rec(2, st);
         if (screen == TJ_SCREEN_PLAIN) screen_plain(g, eb, st);
@@ -592,10 +634,15 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         else screen_tc(g, eb, st);
         S_.screen_pair = g.used_pair ? 1 : 0;
         ev.rec(3, st);
-        // the int8-limb screen is exact: no band; the plain screen's band is already the FP32
-        // stage's undecided set
-        if (!i8) refine_band(g, eb, band_fp32 && screen != TJ_SCREEN_PLAIN, st);
+        if (stage_keys) launch(snapshot_reserved, 1, 1, 0, st, ctr.p);
+        // the four-product int8-limb screen is exact: no band; the plain screen's band is already the
+        // FP32 stage's undecided set
+        if (!i8 || i8_high_limb_screen(g)) refine_band(g, eb, band_fp32 && screen != TJ_SCREEN_PLAIN && !i8, st);
         ev.rec(4, st);
+        if (guards) {
+            launch(guard_check, 1, 256, 0, st, (const uint64_t*)(acc.p + cap), ctr.p);
+            launch(guard_check, 1, 256, 0, st, (const uint64_t*)(band.p + bcap), ctr.p);
+        }
         TJ_CUDA(cudaMemcpyAsync(&h, ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, st));
         TJ_CUDA(cudaStreamSynchronize(st));
         check_status(h.status);
@@ -607,8 +654,11 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         bcap = std::max(bcap * 2, h.band_reserved + h.band_reserved / 4 + 4096);
     }
     S_.tile_pairs = (int64_t)h.items;
-    S_.pairs_screened = (int64_t)h.pad[0];
-    S_.screen_ops = (double)h.pad[1];
+    S_.pairs_screened = (int64_t)h.pairs_screened;
+    S_.screen_ops = (double)h.screen_ops;
+    for (int c = 0; c < ncls; ++c) S_.screen_ops_issued += (double)h.class_items[c] * sops.per_item[c];
+    if (i8 && !i8_high_limb_screen(g))   // the four-product screen: hl + lh and ll for the items that took them
+        S_.screen_ops_issued += 3.0 * (double)h.xl_items * sops.per_item[0];
     if (diag) {
         unsigned long long dv[3] = {0, 0, 0};
         TJ_CUDA(cudaMemcpyAsync(dv, diag_out.p, sizeof(dv), cudaMemcpyDeviceToHost, st));
@@ -622,6 +672,24 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     S_.refine_accept = (int64_t)h.refine_accept;
     S_.rare_checks = (int64_t)h.rare_checks;
     S_.band_fp64 = (int64_t)h.band_fp64;
+    if (stage_keys) {   // the screen's own decisions, sorted (self-joins: the screen's i < j form)
+        WorkspaceSuspend keep;
+        const unsigned long long n0 = std::min(h.screen_reserved, cap), n1 = std::min(h.band_reserved, bcap);
+        const uint64_t* src[2] = {acc.p, band.p};
+        const unsigned long long ns[2] = {n0, n1};
+        res->stage_n[0] = (long long)h.screen_accept;
+        res->stage_n[1] = (long long)h.band_valid;
+        for (int q = 0; q < 2; ++q) {
+            res->stage[q] = DBuf<uint64_t>(std::max(ns[q], 1ull), st);
+            if (!ns[q]) continue;
+            TJ_CUDA(cudaMemcpyAsync(res->stage[q].p, src[q], ns[q] * 8, cudaMemcpyDeviceToDevice, st));
+            if (ns[q] > 1) {
+                DBuf<uint64_t> t(ns[q], st);
+                DBuf<uint32_t> w(radix_workspace_elems(ns[q]), st);
+                radix_sort(res->stage[q].p, nullptr, t.p, nullptr, ns[q], 64, w.p, st);
+            }
+        }
+    }
     band.reset();
 
     // canonical order
@@ -631,7 +699,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     if (mode == TJ_MODE_DIRECTED) {
         const long long N = joins[0].nR;
         const unsigned long long nk = 2 * slots + (unsigned long long)N;
-        keys = DBuf<uint64_t>::result(nk, st);
+        keys = DBuf<uint64_t>::result(nk + gs, st);
         expand_directed(acc.p, slots, keys.p, N, st);
         acc.reset();
         slots = nk;
@@ -640,11 +708,15 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         keys = std::move(acc);
     }
     const int bits = bits_for(kspace);   // sentinel low bits (all ones) exceed every valid key
+    if (guards) launch(guard_fill, 1, 256, 0, st, keys.p + slots);   // keys holds >= slots + gs words
     if (slots > 1) {
-        DBuf<uint64_t> ktmp(slots, st);
+        DBuf<uint64_t> ktmp(slots + gs, st);
         DBuf<uint32_t> ws(radix_workspace_elems(slots), st);
+        if (guards) launch(guard_fill, 1, 256, 0, st, ktmp.p + slots);
         radix_sort(keys.p, nullptr, ktmp.p, nullptr, slots, bits, ws.p, st);
+        if (guards) launch(guard_check, 1, 256, 0, st, (const uint64_t*)(ktmp.p + slots), ctr.p);
     }
+    if (guards) launch(guard_check, 1, 256, 0, st, (const uint64_t*)(keys.p + slots), ctr.p);
     if (nj > 1) {
         DBuf<long long> offs((size_t)nj + 1, st);
         batch_offsets(keys.p, nvalid, d_koff.p, nj, offs.p, st);
@@ -654,7 +726,11 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         res->d_cols = std::move(d_cols);
     }
     ev.rec(5, st);
+    unsigned long long status_after = 0;
+    if (guards)
+        TJ_CUDA(cudaMemcpyAsync(&status_after, &ctr.p->status, 8, cudaMemcpyDeviceToHost, st));
     TJ_CUDA(cudaStreamSynchronize(st));
+    check_status(status_after);
     res->keys = std::move(keys);
     res->count = nvalid;
     S_.result_pairs = nvalid;
@@ -721,6 +797,19 @@ int tj_result_keys(const tj_result* res, uint64_t* keys_out, void* stream) {
     if (!keys_out) fail(TJ_ERR_INVALID, "null output");
     TJ_CUDA(cudaMemcpyAsync(keys_out, res->keys.p, (size_t)res->count * 8, cudaMemcpyDeviceToDevice,
                             (cudaStream_t)stream));
+    return TJ_OK;
+    TJ_API_END
+}
+
+int tj_result_stage_keys(const tj_result* res, int32_t stage, uint64_t* keys_out, int64_t* count, void* stream) {
+    TJ_API_BEGIN
+    if (!res || !count) fail(TJ_ERR_INVALID, "null argument");
+    if (stage != 0 && stage != 1) fail(TJ_ERR_INVALID, "stage must be 0 (screen accepts) or 1 (band)");
+    if (!res->stage[stage].p) fail(TJ_ERR_INVALID, "the join did not keep its stage keys (TJ_FLAG_STAGE_KEYS)");
+    *count = res->stage_n[stage];
+    if (keys_out && res->stage_n[stage] > 0)
+        TJ_CUDA(cudaMemcpyAsync(keys_out, res->stage[stage].p, (size_t)res->stage_n[stage] * 8,
+                                cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
     return TJ_OK;
     TJ_API_END
 }
@@ -868,6 +957,12 @@ int tj_batch_pairs(const tj_result* res, int64_t* i_out, int64_t* j_out, void* s
                          (cudaStream_t)stream);
     return TJ_OK;
     TJ_API_END
+}
+
+int tj_set_wait_limit(int64_t ns) {
+    if (ns < 0) { g_last_error = "the wait limit must be >= 0"; return TJ_ERR_INVALID; }
+    g_wait_ns = ns == 0 ? kWaitLimitNs : (unsigned long long)ns;
+    return TJ_OK;
 }
 
 const char* tj_last_error_string(void) { return g_last_error.c_str(); }

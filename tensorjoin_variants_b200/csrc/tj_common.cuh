@@ -25,9 +25,11 @@ enum : unsigned {
     kStatusBadInput = 1u << 1,      // NaN / Inf / out-of-range magnitude in an input row
     kStatusTmemAlloc = 1u << 2,     // TMEM allocation returned an unexpected address
     kStatusFp16Range = 1u << 3,     // |x| too large for an FP16 operand
+    kStatusGuard = 1u << 4,         // a guard region after an output buffer was overwritten
 };
 
-// Counters block shared by the screen, refine and emit stages (device memory, u64 each).
+// Counters block shared by the screen, refine and emit stages (device memory, u64 each).  The first
+// kCountersPerAttempt words restart with every screen attempt (capacity retries rerun the screen).
 struct Counters {
     unsigned long long acc_reserved;   // slots reserved in the accept buffer (incl. sentinel padding)
     unsigned long long acc_valid;      // accepted pairs written (screen + refine)
@@ -37,10 +39,16 @@ struct Counters {
     unsigned long long refine_accept;  // accepted by FP64 refinement
     unsigned long long rare_checks;    // pairs that reached the per-pair FP64 certificate
     unsigned long long items;          // tile pairs screened
-    unsigned long long status;         // kStatus* bits
     unsigned long long band_fp64;      // band pairs that reached the FP64 terminal
-    unsigned long long pad[6];
+    unsigned long long xl_items;       // int8 four-product screen: items that took the low-limb products
+    unsigned long long status;         // kStatus* bits
+    unsigned long long pairs_screened; // distance evaluations of the candidate list
+    unsigned long long screen_ops;     // algorithmic screen operations of the candidate list
+    unsigned long long class_items[4]; // candidate tile pairs per class
+    unsigned long long screen_reserved;  // acc_reserved after the screen, before the refinement appends
+    unsigned long long pad[2];
 };
+constexpr int kCountersPerAttempt = 10;
 
 // Per-join parameters (batched mode has one per join; a single join uses one entry).
 struct JoinParams {
@@ -131,10 +139,14 @@ TJ_DEV unsigned long long global_ns() {
 }
 // Bounded wait: gives up after `limit_ns` of wall time, sets the timeout bit and returns false.
 // Every wait in every kernel of this library goes through here, so no kernel can spin forever.
+// Limits of a millisecond or more first spin 256 times without reading the clock; shorter limits
+// (set through tj_set_wait_limit, for tests of the timeout path) start the clock at once.
 constexpr unsigned long long kWaitLimitNs = 4000000000ull;   // 4 s
+constexpr unsigned long long kDrainLimitNs = 1000000000ull;  // waits for a CTA's own copies in flight
 TJ_DEV bool mbar_wait(uint64_t* bar, unsigned parity, unsigned long long* status,
                       unsigned long long limit_ns = kWaitLimitNs) {
-    for (int it = 0; it < 256; ++it)
+    const int spins = limit_ns >= 1000000ull ? 256 : 1;
+    for (int it = 0; it < spins; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (true) {
@@ -225,7 +237,8 @@ TJ_DEV bool mbar_try_wait_cluster(uint64_t* bar, unsigned parity) {
 // bounded wait with cluster-scope acquire (a barrier that the other CTA of the pair arrives on)
 TJ_DEV bool mbar_wait_cluster(uint64_t* bar, unsigned parity, unsigned long long* status,
                               unsigned long long limit_ns = kWaitLimitNs) {
-    for (int it = 0; it < 256; ++it)
+    const int spins = limit_ns >= 1000000ull ? 256 : 1;
+    for (int it = 0; it < spins; ++it)
         if (mbar_try_wait_cluster(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (true) {

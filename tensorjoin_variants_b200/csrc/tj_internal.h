@@ -247,6 +247,7 @@ struct ScreenInput {
     const void* const* ssrc = nullptr;  // device [njoins]
     long long T_int = 0;                // integer threshold (int8-limb screen, single join)
     bool allow_pair = true;             // the CTA-pair tensor-core screen may be used where it applies
+    bool i8_four_products = false;      // int8-limb screen: all four limb products (exact in the kernel)
     mutable bool used_pair = false;     // set by screen_tc
     JoinParams jp0{};                   // host copy of join 0's parameters (single-join kernels)
     // screen-error diagnostics (tensor-core screens): sampled accumulators and the analysis result
@@ -259,6 +260,9 @@ struct ScreenInput {
 void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);
 void screen_plain(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);
 void screen_i8(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);
+// true when screen_i8 runs the high-limb screen (hh products only; undecided pairs go to the band
+// and the exact integer refinement), false for the four-product screen (exact, no band)
+bool i8_high_limb_screen(const ScreenInput& g);
 // FP64 terminal for the band; fp32_stage puts the certified FP32 band stage in front of it.
 void refine_band(const ScreenInput& g, const EmitBuffers& eb, bool fp32_stage, cudaStream_t st);
 void expand_directed(const uint64_t* upper, unsigned long long n_upper_slots, uint64_t* out, long long N,
@@ -271,6 +275,8 @@ void batch_offsets(const uint64_t* keys, long long n, const unsigned long long* 
                    long long* offsets, cudaStream_t st);
 
 int num_sms();
+// limit of the screen kernels' pipeline waits for joins started on the calling thread (tj_set_wait_limit)
+unsigned long long pipeline_wait_ns();
 
 // Every kernel of the library is launched through launch(): it checks the launch and counts it
 // (tj_kernel_launches() reports the running total, used to audit what ran inside a timed region).

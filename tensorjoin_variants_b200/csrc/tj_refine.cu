@@ -175,6 +175,8 @@ struct RefineArgs {
     unsigned long long acc_cap;
     Counters* ctr;
     const float2* thr;                  // per join FP32-sum thresholds (the FP32 band stage)
+    int is_int;                         // int16 (int14) rows: exact integer distances against T_int
+    long long T_int;
 };
 
 // FP32 sum of squared FP32 differences in four FMA chains (tree depth <= d / 4 + 2), the FP32
@@ -223,6 +225,32 @@ TJ_DEV double seq_d2(const float* x, const float* y, int d) {
     return acc;
 }
 
+// Exact squared distance of two int16 rows in int64: each difference fits int32 and its square
+// int64, so no order of the sum can round (the oracle's exact integer predicate).
+TJ_DEV long long exact_d2_i16(const int16_t* x, const int16_t* y, int d) {
+    long long acc = 0;
+    if ((d & 7) == 0 && ((((uintptr_t)x) | ((uintptr_t)y)) & 15) == 0) {
+        const int4* x4 = (const int4*)x;
+        const int4* y4 = (const int4*)y;
+        for (int k = 0; k < d / 8; ++k) {
+            const int4 a = __ldg(x4 + k), b = __ldg(y4 + k);
+            const int av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int t0 = (int)(short)(av[u] & 0xffff) - (int)(short)(bv[u] & 0xffff);
+                const int t1 = (av[u] >> 16) - (bv[u] >> 16);
+                acc += (long long)t0 * t0 + (long long)t1 * t1;
+            }
+        }
+    } else {
+        for (int k = 0; k < d; ++k) {
+            const int t = (int)__ldg(x + k) - (int)__ldg(y + k);
+            acc += (long long)t * t;
+        }
+    }
+    return acc;
+}
+
 // Band pairs -> accept buffer.  kFp32: each pair is first decided, where it can be, by the
 // certified FP32 sum (the FP32 band stage); only the rest pay the sequential FP64 terminal.
 template <bool kFp32>
@@ -248,6 +276,11 @@ __global__ void refine_kernel(const RefineArgs a) {
                 const JoinParams& jp = a.jps[lo];
                 const uint64_t local = key - jp.key_off;
                 const uint64_t i = local / (uint64_t)jp.n_cols, j = local - i * (uint64_t)jp.n_cols;
+                if (a.is_int) {   // int14 rows: the exact integer predicate decides every pair
+                    const int16_t* xi = (const int16_t*)a.rsrc[lo] + (size_t)i * jp.d;
+                    const int16_t* yi = (const int16_t*)a.ssrc[lo] + (size_t)j * jp.d;
+                    ok = exact_d2_i16(xi, yi, jp.d) <= a.T_int;
+                } else {
                 const float* x = (const float*)a.rsrc[lo] + (size_t)i * jp.d;
                 const float* y = (const float*)a.ssrc[lo] + (size_t)j * jp.d;
                 bool decided = false;
@@ -260,6 +293,7 @@ __global__ void refine_kernel(const RefineArgs a) {
                 if (!decided) {
                     ok = seq_d2(x, y, jp.d) <= jp.T;
                     ++n_fp64;
+                }
                 }
             }
         }
@@ -408,7 +442,10 @@ void refine_band(const ScreenInput& g, const EmitBuffers& eb, bool fp32_stage, c
     a.acc_cap = eb.acc_cap;
     a.ctr = eb.ctr;
     a.thr = nullptr;
-    if (fp32_stage) {
+    a.is_int = g.R[0]->dtype == kI16 ? 1 : 0;
+    a.T_int = g.T_int;
+    if (a.is_int && g.njoins != 1) fail(-7, "int16 band refinement runs one join at a time");
+    if (fp32_stage && !a.is_int) {
         DBuf<float2> dth((size_t)g.njoins, st);
         fp32_sum_thresholds(g, dth.p, st);
         a.thr = dth.p;

@@ -92,6 +92,7 @@ template <int kStages>
 struct ScreenCtl {
     uint64_t full[kStages];
     uint64_t empty[kStages];
+    uint64_t armed[kStages];   // CTA pair, in CTA 1: CTA 0 has armed this stage's phase of its full barrier
     uint64_t acc_full[kAccMax];
     uint64_t acc_empty[kAccMax];
     uint64_t meta_full[kMetaSlots];
@@ -165,6 +166,7 @@ struct ScreenArgs {
     uint4* dump_ids;           // [dump_items]: (global R tile, global S tile, 1, 0)
     unsigned dump_every;
     unsigned dump_items;
+    unsigned long long wait_ns;   // limit of every pipeline wait (drains keep kDrainLimitNs)
 };
 
 // r[k] for a runtime k without local memory: a fixed 31-select tree (the rare path's only way
@@ -257,6 +259,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         for (int s = 0; s < kStages; ++s) {
             mbar_init(&ctl->full[s], 1);
             mbar_init(&ctl->empty[s], 1);
+            mbar_init(&ctl->armed[s], 1);
         }
         for (int b = 0; b < kAccMax; ++b) {
             mbar_init(&ctl->acc_full[b], 1);
@@ -308,16 +311,25 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     const unsigned J = kPair ? e : a.jlist[e];
                     const int srow = (int)a.stiles[J].x + (int)(rank * kTileR);   // pair: this CTA's half
                     const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
-                    if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status)) { ok = false; break; }
+                    if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status, a.wait_ns)) { ok = false; break; }
                     mbar_arrive_expect_tx(&ctl->meta_full[slot], (unsigned)sizeof(ColMetaF));
                     bulk_load(&meta[slot], a.s_meta + J, (unsigned)sizeof(ColMetaF), &ctl->meta_full[slot]);
                     for (int kb = 0; kb < kblocks; ++kb) {
-                        if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status)) { ok = false; break; }
+                        if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status, a.wait_ns)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         uint8_t* sa = smem + (size_t)stage * kStageBytes;
                         if (kPair) {   // both CTAs' copies complete on the MMA CTA's barrier
+                            // CTA 1 copies only into phases CTA 0 has armed (CTA 0 tells it through CTA 1's
+                            // `armed` barrier), so every copy of the pair lands in a phase CTA 0 waits for
+                            // before the pair exits, also when one CTA gives up early
                             const unsigned fb = mapa_shared(&ctl->full[stage], 0);
-                            if (rank == 0) mbar_arrive_expect_tx(&ctl->full[stage], 2 * tx);
+                            if (rank == 0) {
+                                mbar_arrive_expect_tx(&ctl->full[stage], 2 * tx);
+                                mbar_arrive_cluster(mapa_shared(&ctl->armed[stage], 1));
+                            } else if (!mbar_wait(&ctl->armed[stage], phase, status, a.wait_ns)) {
+                                ok = false;
+                                break;
+                            }
                             tma_load_2d_pair(sa, mA, fb, kb * kbk, rrow);
                             tma_load_2d_pair(sa + Cfg::kBhi, mB, fb, kb * kbk, srow);
                         } else {
@@ -335,16 +347,16 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             }
             if (!ok) ctl->abort_flag = 1;
             // drain: the last copy issued into every stage / metadata slot must land before exit (in
-            // the pair the MMA CTA's barriers count both CTAs' copies; the final cluster barrier
-            // follows the last MMA, which consumed them)
+            // the pair the MMA CTA's barriers count both CTAs' copies and CTA 1 copies only into phases
+            // CTA 0 armed, so CTA 0's drain covers them; the final cluster barrier follows it)
             for (int s = 0; s < kStages && rank == 0; ++s) {
                 const unsigned ph = ((unsigned)s < stage) ? phase : (phase ^ 1u);
-                mbar_wait(&ctl->full[s], ph, status, 1000000000ull);
+                mbar_wait(&ctl->full[s], ph, status, kDrainLimitNs);
             }
             for (int s = 0; s < kMetaSlots; ++s) {
                 if (n <= (unsigned long long)s) continue;
                 const unsigned long long last = ((n - 1 - s) / kMetaSlots) * kMetaSlots + s;
-                mbar_wait(&ctl->meta_full[s], (unsigned)((last / kMetaSlots) & 1), status, 1000000000ull);
+                mbar_wait(&ctl->meta_full[s], (unsigned)((last / kMetaSlots) & 1), status, kDrainLimitNs);
             }
         }
     } else if (warp == 1) {
@@ -365,10 +377,12 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     const unsigned b0 = kPair ? acc : (unsigned)((2 * n_mma) & 3), b1 = (b0 + 1) & 3;
                     bool got;
                     if (kPair) {
-                        got = mbar_wait_cluster(&ctl->acc_empty[acc], acc_phase ^ 1, status);
+                        got = mbar_wait_cluster(&ctl->acc_empty[acc], acc_phase ^ 1, status, a.wait_ns);
                     } else {
-                        got = mbar_wait(&ctl->acc_empty[b0], (unsigned)(((2 * n_mma) >> 2) & 1) ^ 1u, status) &&
-                              mbar_wait(&ctl->acc_empty[b1], (unsigned)(((2 * n_mma + 1) >> 2) & 1) ^ 1u, status);
+                        got = mbar_wait(&ctl->acc_empty[b0], (unsigned)(((2 * n_mma) >> 2) & 1) ^ 1u, status,
+                                        a.wait_ns) &&
+                              mbar_wait(&ctl->acc_empty[b1], (unsigned)(((2 * n_mma + 1) >> 2) & 1) ^ 1u, status,
+                                        a.wait_ns);
                     }
                     if (!got) { ok = false; break; }
                     tc_fence_after();
@@ -376,7 +390,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     const unsigned d0 = tmem + b0 * 128u, d1 = tmem + b1 * 128u;  // one SM: 2 x 128
                     const unsigned bhalf = 256u * (unsigned)ca.kbk;              // bytes of 128 B rows
                     for (int kb = 0; kb < kblocks; ++kb) {
-                        if (!mbar_wait(&ctl->full[stage], phase, status)) { ok = false; break; }
+                        if (!mbar_wait(&ctl->full[stage], phase, status, a.wait_ns)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         tc_fence_after();
                         const uint8_t* sa = smem + (size_t)stage * kStageBytes;
@@ -419,7 +433,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             if (!ok) ctl->abort_flag = 1;
             if (kPair) umma_commit_pair_mc(&ctl->drain, 0x1);
             else umma_commit(&ctl->drain);
-            mbar_wait(&ctl->drain, 0, status, 1000000000ull);
+            mbar_wait(&ctl->drain, 0, status, kDrainLimitNs);
         }
     } else if (warp >= kEpiFirst) {
         // ------------------------------------------------------------ epilogue
@@ -461,8 +475,11 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     bph = (unsigned)((sub >> 2) & 1);
                 }
                 const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
-                if (!mbar_wait(&ctl->meta_full[slot], mph, status) ||
-                    !mbar_wait(&ctl->acc_full[b], bph, status)) { ok = false; break; }
+                {   // warp-uniform: the TMEM loads below are warp-collective
+                    const bool got = mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns) &&
+                                     mbar_wait(&ctl->acc_full[b], bph, status, a.wait_ns);
+                    if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
+                }
                 tc_fence_after();
                 const ColMetaF& m = meta[slot];
                 const unsigned c0 = m.c0;
@@ -805,6 +822,7 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     a.dump_ids = g.dump_ids;
     a.dump_every = g.dump_every ? g.dump_every : 1u;
     a.dump_items = g.dump ? g.dump_items : 0u;
+    a.wait_ns = pipeline_wait_ns();
     const int grid = num_sms();
 #define TJ_SCREEN(F, SP)                                                                                      \
     do {                                                                                                      \

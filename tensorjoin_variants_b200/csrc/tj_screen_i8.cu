@@ -101,9 +101,20 @@ struct I8Args {
     uint64_t* acc;
     unsigned long long acc_cap;
     Counters* ctr;
+    unsigned long long wait_ns;   // limit of every pipeline wait (drains keep kDrainLimitNs)
 };
 
 TJ_DEV int floor_shift15(long long v) { return (int)(v >> 15); }   // arithmetic shift = floor division
+// a_iJ = floor(v / 2^15) clamped to [-2^30, 2^31 - 1]: |hh - b_j| < 2^30 for every d the screen takes,
+// so the clamp never turns a candidate into a rejection (a huge T makes every real pair a candidate)
+TJ_DEV int clamp_shift15(long long v) {
+    const long long f = v >> 15;
+    return f < -(1ll << 30) ? -(1 << 30) : f > 0x7FFFFFFFll ? 0x7FFFFFFF : (int)f;
+}
+// columns of a 32-column block at and beyond the tile's valid count carry no point
+TJ_DEV uint32_t valid_cols(unsigned nv, unsigned cc) {
+    return nv >= cc + 32 ? 0xFFFFFFFFu : nv > cc ? ((1u << (nv - cc)) - 1u) : 0u;
+}
 
 // r[k] for a runtime k without local memory (fixed 31-select tree).
 TJ_DEV uint32_t pick32(const uint32_t (&r)[32], int k) {
@@ -190,11 +201,11 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                     const unsigned J = a.jlist[e];
                     const int srow = (int)a.s_row0[J];
                     const unsigned slot = (unsigned)(n % kI8Meta), mph = (unsigned)((n / kI8Meta) & 1);
-                    if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status)) { ok = false; break; }
+                    if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status, a.wait_ns)) { ok = false; break; }
                     mbar_arrive_expect_tx(&ctl->meta_full[slot], (unsigned)sizeof(ColMetaI8));
                     bulk_load(&meta[slot], a.s_meta + J, (unsigned)sizeof(ColMetaI8), &ctl->meta_full[slot]);
                     for (int kb = 0; kb < a.kblocks; ++kb) {
-                        if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status)) { ok = false; break; }
+                        if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status, a.wait_ns)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         uint8_t* st = smem + (size_t)stage * kI8Stage;
                         mbar_arrive_expect_tx(&ctl->full[stage], kI8Stage);
@@ -209,12 +220,12 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             if (!ok) ctl->abort_flag = 1;
             for (int s = 0; s < kI8Stages; ++s) {
                 const unsigned ph = ((unsigned)s < stage) ? phase : (phase ^ 1u);
-                mbar_wait(&ctl->full[s], ph, status, 1000000000ull);
+                mbar_wait(&ctl->full[s], ph, status, kDrainLimitNs);
             }
             for (int s = 0; s < kI8Meta; ++s) {
                 if (n <= (unsigned long long)s) continue;
                 const unsigned long long last = ((n - 1 - s) / kI8Meta) * kI8Meta + s;
-                mbar_wait(&ctl->meta_full[s], (unsigned)((last / kI8Meta) & 1), status, 1000000000ull);
+                mbar_wait(&ctl->meta_full[s], (unsigned)((last / kI8Meta) & 1), status, kDrainLimitNs);
             }
         }
     } else if (warp == 1) {
@@ -231,12 +242,14 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             bool pending = false;
             unsigned long long pn = 0;
             unsigned pstage = 0;
+            unsigned long long n_xl = 0;   // items that took the low-limb products
             auto resolve = [&](unsigned long long mi, unsigned si) -> bool {
-                if (!mbar_wait(&ctl->xl_dec, (unsigned)(mi & 1), status)) return false;
+                if (!mbar_wait(&ctl->xl_dec, (unsigned)(mi & 1), status, a.wait_ns)) return false;
                 volatile int* need = &ctl->need[mi & 1];
                 const int needed = *need;
                 *need = 0;   // the item two ahead writes it only after this resolve (acc_full order)
                 if (needed) {
+                    ++n_xl;
                     tc_fence_after();
                     const uint8_t* st = smem + (size_t)si * kI8Stage;
                     const uint8_t *Ah = st, *Al = st + kPart, *Bh = st + 2 * kPart, *Bl = st + 3 * kPart;
@@ -257,11 +270,11 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                 for (unsigned e = ch.y; e < ch.z && ok; ++e, ++n) {
                     const unsigned b = (unsigned)(n & 1);
                     const unsigned use = (unsigned)((n >> 1) & 1);   // parity of this buffer's use
-                    if (!mbar_wait(&ctl->hh_empty[b], use ^ 1, status)) { ok = false; break; }
+                    if (!mbar_wait(&ctl->hh_empty[b], use ^ 1, status, a.wait_ns)) { ok = false; break; }
                     tc_fence_after();
                     const unsigned t_hh = tmem + kColHH0 + b * 128, t_x = tmem + kColX, t_ll = tmem + kColLL;
                     if (lazy) {
-                        if (!mbar_wait(&ctl->full[stage], phase, status)) { ok = false; break; }
+                        if (!mbar_wait(&ctl->full[stage], phase, status, a.wait_ns)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         tc_fence_after();
                         const uint8_t* st = smem + (size_t)stage * kI8Stage;
@@ -277,7 +290,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                         continue;
                     }
                     for (int kb = 0; kb < a.kblocks; ++kb) {
-                        if (!mbar_wait(&ctl->full[stage], phase, status)) { ok = false; break; }
+                        if (!mbar_wait(&ctl->full[stage], phase, status, a.wait_ns)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         tc_fence_after();
                         const uint8_t* st = smem + (size_t)stage * kI8Stage;
@@ -289,7 +302,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                         // epilogue now, so its fast path overlaps this item's x / ll products
                         if (kb == a.kblocks - 1) umma_commit(&ctl->acc_full[b]);
                         if (kb == 0) {   // x / ll of the previous item must have been read
-                            if (!mbar_wait(&ctl->xl_empty, (unsigned)(n & 1) ^ 1u, status)) { ok = false; break; }
+                            if (!mbar_wait(&ctl->xl_empty, (unsigned)(n & 1) ^ 1u, status, a.wait_ns)) { ok = false; break; }
                             tc_fence_after();
                         }
 #pragma unroll
@@ -306,9 +319,11 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                 }
             }
             if (ok && pending) ok = resolve(pn, pstage);
+            if (!lazy) n_xl = n;
+            if (n_xl) atomicAdd(&a.ctr->xl_items, n_xl);
             if (!ok) ctl->abort_flag = 1;
             umma_commit(&ctl->drain);
-            mbar_wait(&ctl->drain, 0, status, 1000000000ull);
+            mbar_wait(&ctl->drain, 0, status, kDrainLimitNs);
         }
     } else {
         const unsigned ew = warp - 2;                 // 0..7
@@ -331,8 +346,11 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             for (unsigned e = ch.y; e < ch.z; ++e, ++n) {
                 const unsigned b = (unsigned)(n & 1);
                 const unsigned slot = (unsigned)(n % kI8Meta), mph = (unsigned)((n / kI8Meta) & 1);
-                if (!mbar_wait(&ctl->meta_full[slot], mph, status) ||
-                    !mbar_wait(&ctl->acc_full[b], (unsigned)((n >> 1) & 1), status)) { ok = false; break; }
+                {   // warp-uniform: the TMEM loads below are warp-collective
+                    const bool got = mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns) &&
+                                     mbar_wait(&ctl->acc_full[b], (unsigned)((n >> 1) & 1), status, a.wait_ns);
+                    if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
+                }
                 tc_fence_after();
                 const ColMetaI8& m = meta[slot];
                 const unsigned c0 = m.c0;
@@ -343,7 +361,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                     const double HJ = m.HJ, LJ = m.LJ;
                     const double Md = (128.0 * (hi_n * LJ + li_n * HJ) + li_n * LJ) * (1.0 + 0x1p-40) + 2.0;
                     const long long M = (long long)ceil(Md);
-                    ai = floor_shift15(Ai - a.T - 2 * M);
+                    ai = clamp_shift15(Ai - a.T - 2 * M);
                 }
                 const unsigned lane_off = (q * 32u) << 16;
                 const unsigned col0 = half * 64;
@@ -384,6 +402,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                                 cmask |= ((int)hv[k] - m.bq[cc + k] >= ai ? 1u : 0u) << k;
                         }
                     }
+                    cmask &= valid_cols(m.nvJ, cc);
                     if (jp.self_join && cmask) {   // keep sorted column > sorted row only
                         const int lim = (int)rs - (int)(c0 + cc);
                         if (lim >= 31) cmask = 0;
@@ -400,7 +419,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
                     mbar_arrive(&ctl->xl_dec);
                 }
                 {
-                    const bool xl_ok = mbar_wait(&ctl->xl_full, (unsigned)(n & 1), status);
+                    const bool xl_ok = mbar_wait(&ctl->xl_full, (unsigned)(n & 1), status, a.wait_ns);
                     if (!__all_sync(0xffffffffu, xl_ok)) { ok = false; break; }   // warp-uniform exit
                 }
                 tc_fence_after();
@@ -470,6 +489,324 @@ __global__ void __launch_bounds__(kI8Threads, 1)
     if (warp == 1) tmem_dealloc(tmem, 512);
 }
 
+// ------------------------------------------------------------------ high-limb screen
+// One tensor-core product per pair: hh = sum h h' (exact INT32), and the rest of q.q' bounded,
+// |128 x + ll| <= M_iJ (Cauchy-Schwarz on the limb vectors, as above).  Every pair whose interval
+//     [A_i + B_j - 32768 hh - 2 M_iJ,  A_i + B_j - 32768 hh + 2 M_iJ]
+// lies above T is out (the group fast test, then the same integer test per pair), one that lies at
+// or below T is in (exact INT64 test per candidate), and the rest go to the band buffer, where the
+// integer refinement decides them from the int16 rows.  Only the h limbs are loaded, and the R
+// tile's limbs stay resident in shared memory for all items of a chunk (only S tiles stream), so an
+// item costs 16 KB of L2 traffic and kpad / 32 MMAs.
+// Warp roles (384 threads): warp 0 TMA producer, warp 1 TMEM allocator + UMMA issuer, warps 2-3
+// idle, warps 4..11 epilogue (warp w reads TMEM lanes 32 (w % 4).. and columns 64 ((w - 4) / 4)..).
+constexpr int kHHStages = 6;                      // S k-blocks in flight (16 KB each)
+constexpr int kHHMaxKb = 2;                       // resident R k-blocks (kpad <= 256)
+constexpr int kHHAcc = 4;                         // TMEM accumulators of 128 columns
+constexpr int kHHEpi = 8;
+constexpr int kHHEpiFirst = 4;
+constexpr int kHHThreads = (kHHEpiFirst + kHHEpi) * 32;
+constexpr unsigned kHHABytes = kHHMaxKb * kPart;  // one resident R tile
+
+struct HHCtl {
+    uint64_t a_full[2];
+    uint64_t a_empty[2];
+    uint64_t full[kHHStages];
+    uint64_t empty[kHHStages];
+    uint64_t acc_full[kHHAcc];
+    uint64_t acc_empty[kHHAcc];
+    uint64_t meta_full[kI8Meta];
+    uint64_t meta_empty[kI8Meta];
+    uint64_t drain;
+    unsigned tmem_base;
+    int abort_flag;
+};
+
+constexpr size_t kHHSmem = 1024 + 2 * (size_t)kHHABytes + (size_t)kHHStages * kPart + kI8Meta * sizeof(ColMetaI8) +
+                           sizeof(HHCtl);
+static_assert(kHHSmem <= 232448, "227 KB of shared memory per CTA at most");
+
+struct HHArgs {
+    I8Args b;                  // tile tables, row data, threshold, output (as the four-product screen)
+    uint64_t* band;
+    unsigned long long band_cap;
+};
+
+__global__ void __launch_bounds__(kHHThreads, 1)
+    screen_i8_hh_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                        const HHArgs ha) {
+    const I8Args& a = ha.b;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* abuf = smem;                                       // 2 x kHHABytes
+    uint8_t* bbuf = smem + 2 * (size_t)kHHABytes;               // kHHStages x kPart
+    ColMetaI8* meta = (ColMetaI8*)(bbuf + (size_t)kHHStages * kPart);
+    HHCtl* ctl = (HHCtl*)(meta + kI8Meta);
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned long long* status = &a.ctr->status;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&ctl->a_full[i], 1);
+            mbar_init(&ctl->a_empty[i], 1);
+        }
+        for (int s = 0; s < kHHStages; ++s) {
+            mbar_init(&ctl->full[s], 1);
+            mbar_init(&ctl->empty[s], 1);
+        }
+        for (int b = 0; b < kHHAcc; ++b) {
+            mbar_init(&ctl->acc_full[b], 1);
+            mbar_init(&ctl->acc_empty[b], kHHEpi);
+        }
+        for (int m = 0; m < kI8Meta; ++m) {
+            mbar_init(&ctl->meta_full[m], 1);
+            mbar_init(&ctl->meta_empty[m], kHHEpi);
+        }
+        mbar_init(&ctl->drain, 1);
+        ctl->abort_flag = 0;
+        fence_barrier_init();
+        prefetch_tmap(&tmA);
+        prefetch_tmap(&tmB);
+    }
+    if (warp == 1) tmem_alloc(&ctl->tmem_base, 512);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = ctl->tmem_base;
+    const unsigned nchunks = *a.nchunks;
+    const int kblocks = a.kblocks;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA producer
+        if (lane == 0) {
+            unsigned stage = 0, phase = 0;
+            unsigned long long n = 0, nc = 0;   // items, chunks issued
+            bool ok = true;
+            for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x, ++nc) {
+                const uint4 ch = a.chunks[c];
+                const int rrow = (int)a.r_row0[ch.x];
+                const unsigned ab = (unsigned)(nc & 1);
+                if (!mbar_wait(&ctl->a_empty[ab], (unsigned)((nc >> 1) & 1) ^ 1u, status, a.wait_ns)) { ok = false; break; }
+                mbar_arrive_expect_tx(&ctl->a_full[ab], (unsigned)kblocks * kPart);
+                for (int kb = 0; kb < kblocks; ++kb)
+                    tma_load_2d(abuf + ab * kHHABytes + kb * kPart, &tmA, &ctl->a_full[ab], kb * 128, rrow);
+                for (unsigned e = ch.y; e < ch.z && ok; ++e, ++n) {
+                    const unsigned J = a.jlist[e];
+                    const int srow = (int)a.s_row0[J];
+                    const unsigned slot = (unsigned)(n % kI8Meta), mph = (unsigned)((n / kI8Meta) & 1);
+                    if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status, a.wait_ns)) { ok = false; break; }
+                    mbar_arrive_expect_tx(&ctl->meta_full[slot], (unsigned)sizeof(ColMetaI8));
+                    bulk_load(&meta[slot], a.s_meta + J, (unsigned)sizeof(ColMetaI8), &ctl->meta_full[slot]);
+                    for (int kb = 0; kb < kblocks; ++kb) {
+                        if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status, a.wait_ns)) { ok = false; break; }
+                        if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
+                        mbar_arrive_expect_tx(&ctl->full[stage], kPart);
+                        tma_load_2d(bbuf + (size_t)stage * kPart, &tmB, &ctl->full[stage], kb * 128, srow);
+                        if (++stage == kHHStages) { stage = 0; phase ^= 1; }
+                    }
+                }
+            }
+            if (!ok) ctl->abort_flag = 1;
+            // drain: the last copy issued into every buffer lands before exit
+            for (int s = 0; s < kHHStages; ++s) {
+                const unsigned ph = ((unsigned)s < stage) ? phase : (phase ^ 1u);
+                mbar_wait(&ctl->full[s], ph, status, kDrainLimitNs);
+            }
+            for (unsigned ab = 0; ab < 2; ++ab) {
+                if (nc <= ab) continue;
+                const unsigned long long last = ((nc - 1 - ab) / 2) * 2 + ab;
+                mbar_wait(&ctl->a_full[ab], (unsigned)((last >> 1) & 1), status, kDrainLimitNs);
+            }
+            for (int s = 0; s < kI8Meta; ++s) {
+                if (n <= (unsigned long long)s) continue;
+                const unsigned long long last = ((n - 1 - s) / kI8Meta) * kI8Meta + s;
+                mbar_wait(&ctl->meta_full[s], (unsigned)((last / kI8Meta) & 1), status, kDrainLimitNs);
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ UMMA issuer
+        if (lane == 0) {
+            unsigned stage = 0, phase = 0;
+            unsigned long long n = 0, nc = 0;
+            bool ok = true;
+            for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x, ++nc) {
+                const uint4 ch = a.chunks[c];
+                const unsigned ab = (unsigned)(nc & 1);
+                if (!mbar_wait(&ctl->a_full[ab], (unsigned)((nc >> 1) & 1), status, a.wait_ns)) { ok = false; break; }
+                tc_fence_after();
+                const uint8_t* A = abuf + ab * kHHABytes;
+                for (unsigned e = ch.y; e < ch.z && ok; ++e, ++n) {
+                    const unsigned b = (unsigned)(n & (kHHAcc - 1));
+                    if (!mbar_wait(&ctl->acc_empty[b], (unsigned)((n / kHHAcc) & 1) ^ 1u, status, a.wait_ns)) { ok = false; break; }
+                    tc_fence_after();
+                    const unsigned d_tmem = tmem + b * 128u;
+                    for (int kb = 0; kb < kblocks; ++kb) {
+                        if (!mbar_wait(&ctl->full[stage], phase, status, a.wait_ns)) { ok = false; break; }
+                        if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
+                        tc_fence_after();
+                        const uint8_t* B = bbuf + (size_t)stage * kPart;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            umma_i8(d_tmem, desc_sw128(A + kb * kPart, k * 32), desc_sw128(B, k * 32), a.idesc,
+                                    (kb | k) != 0);
+                        umma_commit(&ctl->empty[stage]);
+                        if (++stage == kHHStages) { stage = 0; phase ^= 1; }
+                    }
+                    if (!ok) break;
+                    umma_commit(&ctl->acc_full[b]);
+                }
+                umma_commit(&ctl->a_empty[ab]);   // the R tile is free once this chunk's MMAs complete
+            }
+            if (n) atomicAdd(&a.ctr->items, n);
+            if (!ok) ctl->abort_flag = 1;
+            umma_commit(&ctl->drain);
+            mbar_wait(&ctl->drain, 0, status, kDrainLimitNs);
+        }
+    } else if (warp >= kHHEpiFirst) {
+        // ------------------------------------------------------------ epilogue
+        const unsigned ew = warp - kHHEpiFirst;        // 0..7
+        const unsigned q = warp & 3;                   // TMEM lane quarter
+        const unsigned col0 = (ew >> 2) * 64;          // column half
+        const unsigned row = q * 32 + lane;
+        const unsigned lane_off = (q * 32u) << 16;
+        const JoinParams& jp = a.jp;
+        WarpAppender app_acc, app_band;
+        unsigned long long n = 0, n_acc = 0, n_rare = 0;
+        bool ok = true;
+        for (unsigned c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
+            const uint4 ch = a.chunks[c];
+            const unsigned I = ch.x;
+            const unsigned r0 = a.r_row0[I];
+            const bool rvalid = row < a.r_nvalid[I];
+            const unsigned rs = r0 + row;
+            const long long Ai = rvalid ? a.r_norm[rs] : 0;
+            const double hi_n = rvalid ? (double)a.r_hn[rs] : 0.0, li_n = rvalid ? (double)a.r_ln[rs] : 0.0;
+            const uint32_t oi = rvalid ? a.r_perm[rs] : 0u;
+            for (unsigned e = ch.y; e < ch.z; ++e, ++n) {
+                const unsigned b = (unsigned)(n & (kHHAcc - 1));
+                const unsigned slot = (unsigned)(n % kI8Meta), mph = (unsigned)((n / kI8Meta) & 1);
+                {   // warp-uniform: the TMEM loads below are warp-collective
+                    const bool got = mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns) &&
+                                     mbar_wait(&ctl->acc_full[b], (unsigned)((n / kHHAcc) & 1), status, a.wait_ns);
+                    if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
+                }
+                tc_fence_after();
+                uint32_t hv2[2][32];
+                tmem_ld32(tmem + lane_off + b * 128 + col0, hv2[0]);
+                tmem_ld32(tmem + lane_off + b * 128 + col0 + 32, hv2[1]);
+                const ColMetaI8& m = meta[slot];
+                const unsigned c0 = m.c0;
+                // M_iJ >= |128 x + ll| for this row and S tile (every term non-negative; the 2^-40 factor
+                // and +2 cover the FP64 rounding of the sum and of the ceil); a_iJ as in the header
+                int ai = 0x7FFFFFFF;
+                long long M = 0;
+                if (rvalid) {
+                    const double HJ = m.HJ, LJ = m.LJ;
+                    const double Md = (128.0 * (hi_n * LJ + li_n * HJ) + li_n * LJ) * (1.0 + 0x1p-40) + 2.0;
+                    M = (long long)ceil(Md);
+                    ai = clamp_shift15(Ai - a.T - 2 * M);
+                }
+                tmem_ld_wait();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&ctl->acc_empty[b]);   // the accumulator is in registers
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const unsigned cc = col0 + h * 32;
+                    const uint32_t (&hv)[32] = hv2[h];
+                    // group fast test: hh_j - b_j <= max hh - min b over 8 columns, so
+                    // max hh - min b < a_iJ proves the whole group out
+                    const int4 gb = *reinterpret_cast<const int4*>(&m.gminb[cc >> 3]);
+                    const int gbv[4] = {gb.x, gb.y, gb.z, gb.w};
+                    int vx[4];
+#pragma unroll
+                    for (int g = 0; g < 4; ++g) {
+                        const uint32_t* h8 = hv + 8 * g;
+                        const int m01 = max((int)h8[0], (int)h8[1]), m23 = max((int)h8[2], (int)h8[3]);
+                        const int m45 = max((int)h8[4], (int)h8[5]), m67 = max((int)h8[6], (int)h8[7]);
+                        vx[g] = max(max(m01, m23), max(m45, m67)) - gbv[g];
+                    }
+                    const unsigned gmask = (vx[0] >= ai ? 1u : 0u) | (vx[1] >= ai ? 2u : 0u) |
+                                           (vx[2] >= ai ? 4u : 0u) | (vx[3] >= ai ? 8u : 0u);
+                    const unsigned gunion = __reduce_or_sync(0xffffffffu, gmask);
+                    if (!gunion) continue;
+                    uint32_t cmask = 0;
+#pragma unroll
+                    for (int g = 0; g < 4; ++g) {
+                        if (!(gunion & (1u << g))) continue;
+                        if (gmask & (1u << g)) {
+#pragma unroll
+                            for (int k = 8 * g; k < 8 * g + 8; ++k)
+                                cmask |= ((int)hv[k] - m.bq[cc + k] >= ai ? 1u : 0u) << k;
+                        }
+                    }
+                    cmask &= valid_cols(m.nvJ, cc);
+                    if (jp.self_join && cmask) {   // keep sorted column > sorted row only
+                        const int lim = (int)rs - (int)(c0 + cc);
+                        if (lim >= 31) cmask = 0;
+                        else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
+                    }
+                    if (!__any_sync(0xffffffffu, cmask != 0)) continue;
+                    // candidates: exact INT64 interval test, in / out / band
+                    uint32_t amask = 0, bmask = 0, mk = cmask;
+                    while (mk) {
+                        const int k = __ffs(mk) - 1;
+                        mk &= mk - 1;
+                        ++n_rare;
+                        const long long mid = Ai + m.norm[cc + k] - 32768ll * (long long)(int)pick32(hv, k);
+                        if (mid + 2 * M <= a.T) amask |= 1u << k;
+                        else if (mid - 2 * M <= a.T) bmask |= 1u << k;
+                    }
+                    unsigned ta = 0, tb = 0, pa = 0, pb = 0;
+                    if (__any_sync(0xffffffffu, amask != 0)) pa = warp_excl_scan(__popc(amask), ta);
+                    if (__any_sync(0xffffffffu, bmask != 0)) pb = warp_excl_scan(__popc(bmask), tb);
+                    if (ta) {
+                        unsigned long long pos = app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap) + pa;
+                        uint32_t w = amask;
+                        while (w) {
+                            const int k = __ffs(w) - 1;
+                            w &= w - 1;
+                            if (pos < a.acc_cap) a.acc[pos] = pair_key(jp, oi, m.perm[cc + k]);
+                            ++pos;
+                        }
+                        n_acc += __popc(amask);
+                    }
+                    if (tb) {
+                        unsigned long long pos = app_band.reserve(tb, &a.ctr->band_reserved, ha.band, ha.band_cap) + pb;
+                        uint32_t w = bmask;
+                        while (w) {
+                            const int k = __ffs(w) - 1;
+                            w &= w - 1;
+                            if (pos < ha.band_cap) ha.band[pos] = pair_key(jp, oi, m.perm[cc + k]);
+                            ++pos;
+                        }
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&ctl->meta_empty[slot]);
+            }
+        }
+        if (!ok) ctl->abort_flag = 1;
+        app_acc.pad(a.acc, a.acc_cap);
+        app_band.pad(ha.band, ha.band_cap);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            n_acc += __shfl_xor_sync(0xffffffffu, n_acc, o);
+            n_rare += __shfl_xor_sync(0xffffffffu, n_rare, o);
+        }
+        if (lane == 0) {
+            if (app_acc.valid) atomicAdd(&a.ctr->acc_valid, app_acc.valid);
+            if (app_band.valid) atomicAdd(&a.ctr->band_valid, app_band.valid);
+            if (n_acc) atomicAdd(&a.ctr->screen_accept, n_acc);
+            if (n_rare) atomicAdd(&a.ctr->rare_checks, n_rare);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem, 512);
+}
+
 }  // namespace
 
 void make_tmap_2d(CUtensorMap* m, const void* base, long long rows, long long cols, int esize, int box_rows,
@@ -508,8 +845,22 @@ void screen_i8(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     a.acc = eb.acc;
     a.acc_cap = eb.acc_cap;
     a.ctr = eb.ctr;
+    a.wait_ns = pipeline_wait_ns();
+    if (i8_high_limb_screen(g)) {
+        HHArgs ha;
+        ha.b = a;
+        ha.band = eb.band;
+        ha.band_cap = eb.band_cap;
+        TJ_CUDA(cudaFuncSetAttribute(screen_i8_hh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHHSmem));
+        launch(screen_i8_hh_kernel, num_sms(), kHHThreads, kHHSmem, st, tmA, tmB, ha);
+        return;
+    }
     TJ_CUDA(cudaFuncSetAttribute(screen_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kI8Smem));
     launch(screen_i8_kernel, num_sms(), kI8Threads, kI8Smem, st, tmA, tmB, a);
+}
+
+bool i8_high_limb_screen(const ScreenInput& g) {
+    return !g.i8_four_products && g.R[0]->kpad <= kHHMaxKb * 128;
 }
 
 }  // namespace tj

@@ -28,8 +28,11 @@ def sha(a):
 
 
 def gpu_keys(R, S, T, mode, screen, **kw):
+    """Keys of one GPU join; every parity join runs with guard regions after its output buffers
+    (an out-of-bounds write fails the join)."""
     Rt = torch.from_numpy(np.ascontiguousarray(R)).cuda()
     St = None if S is None else torch.from_numpy(np.ascontiguousarray(S)).cuda()
+    kw.setdefault("guards", True)
     res = tj.join_result(Rt, St, eps2=T, mode=mode, screen=screen, **kw)
     k = res.keys().cpu().numpy().view(np.uint64)
     i, j = res.pairs()
@@ -224,21 +227,28 @@ def test_index_structure(n):
 
 
 # ---------------------------------------------------------------- int14 data, exact int8-limb screen
-@pytest.mark.parametrize("d", [128, 100, 200])
-def test_int14_self_join_exact(d):
+@pytest.mark.parametrize("four", [False, True])
+@pytest.mark.parametrize("d", [128, 100, 200, 300])
+def test_int14_self_join_exact(d, four):
+    """Both int8-limb screens (high-limb product + exact integer band refinement, or all four limb
+    products decided in the kernel) against the exact integer oracle; d = 300 exceeds the high-limb
+    screen's resident R tile, so it takes the four-product screen either way."""
     w = W.int14x128(n=5000, d=d, samples=1 << 14)
     for mode in ("upper", "directed"):
         want = oracle.join_i16(w.R, None, w.T, mode)
-        k, st = gpu_keys(w.R, None, w.T, mode, "int8limb")
-        assert_same(k, want, f"d={d} {mode}")
-        assert st["band"] == 0
+        k, st = gpu_keys(w.R, None, w.T, mode, "int8limb", i8_four_products=four)
+        assert_same(k, want, f"d={d} {mode} four={four}")
+        if four or d > 256:
+            assert st["band"] == 0
+        assert st["screen_ops_issued"] > 0
         # the full-size int14 join takes principal-direction cells (2M rows): same pairs here
-        k, st = gpu_keys(w.R, None, w.T, mode, "int8limb", index_frame="pca")
-        assert_same(k, want, f"d={d} {mode} pca")
+        k, st = gpu_keys(w.R, None, w.T, mode, "int8limb", index_frame="pca", i8_four_products=four)
+        assert_same(k, want, f"d={d} {mode} pca four={four}")
         assert st["index_frame"] == (1 if d <= 128 else 0)   # principal directions up to d = 128
 
 
-def test_int14_rs_ties_and_extremes():
+@pytest.mark.parametrize("four", [False, True])
+def test_int14_rs_ties_and_extremes(four):
     rng = np.random.default_rng(31)
     R = rng.integers(-8192, 8192, size=(1500, 128), dtype=np.int16)
     S = rng.integers(-8192, 8192, size=(1700, 128), dtype=np.int16)
@@ -251,14 +261,21 @@ def test_int14_rs_ties_and_extremes():
     d2 = ((R[200:250].astype(np.int64) - S[100:150].astype(np.int64)) ** 2).sum(1)
     T = int(np.median(d2))      # several pairs sit exactly on the threshold
     assert np.count_nonzero(d2 == T) >= 1
-    k, st = gpu_keys(R, S, T, "rs", "int8limb")
+    k, st = gpu_keys(R, S, T, "rs", "int8limb", i8_four_products=four)
     assert_same(k, oracle.join_i16(R, S, T, "rs"), "ties")
     # the largest possible distance (all +8191 vs all -8192) decides exactly at its own value
     Tmax = 128 * (8191 + 8192) ** 2
-    kx, _ = gpu_keys(R[:16], S[:16], Tmax, "rs", "int8limb")
+    kx, _ = gpu_keys(R[:16], S[:16], Tmax, "rs", "int8limb", i8_four_products=four)
     assert_same(kx, oracle.join_i16(R[:16], S[:16], Tmax, "rs"), "extremes")
-    kx2, _ = gpu_keys(R[:16], S[:16], Tmax - 1, "rs", "int8limb")
+    kx2, _ = gpu_keys(R[:16], S[:16], Tmax - 1, "rs", "int8limb", i8_four_products=four)
     assert_same(kx2, oracle.join_i16(R[:16], S[:16], Tmax - 1, "rs"), "extremes-1")
+    # a threshold far above every distance (2^61) accepts every pair; 0 accepts exact duplicates only
+    kh, _ = gpu_keys(R[:300], S[:200], 1 << 61, "rs", "int8limb", i8_four_products=four)
+    assert len(kh) == 300 * 200
+    S0 = S.copy()
+    S0[5] = R[7]
+    k0, _ = gpu_keys(R, S0, 0, "rs", "int8limb", i8_four_products=four)
+    assert_same(k0, oracle.join_i16(R, S0, 0, "rs"), "T = 0")
 
 
 def test_int14_rejects_out_of_range_and_fraction():
@@ -561,10 +578,12 @@ def test_batched_screen_error_within_certified_radius():
         assert torch.equal(res.keys(), plain.keys())
 
 
-def test_int14_many_items_exact():
-    """Many tile pairs per CTA (30,000 rows, d = 128): the on-demand x / ll products and their
-    hand-off between the epilogue warps and the UMMA issuer give the oracle's pairs."""
+@pytest.mark.parametrize("four", [False, True])
+def test_int14_many_items_exact(four):
+    """Many tile pairs per CTA (30,000 rows, d = 128): the four-product screen's on-demand x / ll
+    products and their hand-off between the epilogue warps and the UMMA issuer, and the high-limb
+    screen's resident R tiles over whole chunks and its four accumulators, give the oracle's pairs."""
     w = W.int14x128(n=30000, samples=1 << 14)
-    k, st = gpu_keys(w.R, None, w.T, "upper", "int8limb")
+    k, st = gpu_keys(w.R, None, w.T, "upper", "int8limb", i8_four_products=four)
     assert_same(k, oracle.join_i16(w.R, None, w.T, "upper"), "int14 n=30000")
     assert st["tile_pairs"] > 148 * 40
