@@ -682,6 +682,18 @@ def bench_ragged(args, steps: int, warmup: int, rank, world, dist, headline: boo
                                 "pairs_sampled": sd["screen_err_pairs"], "band_pairs": sd["band"],
                                 "refined_fraction": sd["band"] / max(1, sd["pairs_screened"])}
         del rd
+    if screen != "plain":   # per-join spans inside one batched screen launch, and the CTAs' idle tail
+        rt_ = tj.join_batched_result(joins, screen=screen, screen_times=True)
+        stt = rt_.stats
+        line["batch"].update({"in_batch_join_span_ms_p50": stt["join_span_ms_p50"],
+                              "in_batch_join_span_ms_p99": stt["join_span_ms_p99"],
+                              "in_batch_join_span_ms_max": stt["join_span_ms_max"],
+                              "screen_cta_tail_ms": stt["screen_cta_tail_ms"],
+                              "screen_ms_with_stamps": stt["ms_screen"],
+                              "note": "spans: first chunk start to last chunk end of each join inside the screen "
+                                      "launch (%globaltimer, an untimed extra run); tail: spread of the CTAs' end "
+                                      "times"})
+        del rt_
     r = step(screen)
     if not args.no_plain and screen != "plain":
         torch.cuda.synchronize()

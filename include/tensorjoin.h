@@ -101,6 +101,10 @@ typedef struct tj_options {
 /* Keep the screen's own decisions in the result: its certified accepts and its band, before the
  * refinement, each sorted (tj_result_stage_keys).  For auditing each stage against an oracle. */
 #define TJ_FLAG_STAGE_KEYS 128
+/* Tensor-core screens: record %globaltimer stamps of every join's first chunk start and last chunk
+ * end and of every CTA's start and end, and report their spread (tj_stats.join_span_ms_*,
+ * screen_cta_tail_ms).  Diagnostic: one atomic per chunk and epilogue warp. */
+#define TJ_FLAG_SCREEN_TIMES 256
 
 typedef struct tj_stats {
     int64_t n_rows, n_cols;       /* |R|, |S| (self-join: N, N) */
@@ -110,7 +114,9 @@ typedef struct tj_stats {
     int64_t screen_accept;        /* pairs accepted by the certified screen alone */
     int64_t band;                 /* pairs sent to FP64 refinement */
     int64_t refine_accept;        /* band pairs accepted by FP64 refinement */
-    int64_t rare_checks;          /* pairs that reached the per-pair FP64 certificate in the screen */
+    int64_t rare_checks;          /* pairs that passed the screen's fast test without a certified accept
+                                     (16-bit screens: the band the screen emits; int8-limb screens: the
+                                     candidates that took the exact INT64 test) */
     int64_t result_pairs;         /* pairs in the output */
     int64_t retries;              /* capacity retries (overflow-and-retry passes) */
     double ms_index, ms_candidates, ms_screen, ms_refine, ms_sort, ms_total;   /* device time per stage */
@@ -124,6 +130,11 @@ typedef struct tj_stats {
     int64_t band_fp64;            /* band pairs decided by the FP64 terminal */
     double screen_ops_issued;     /* tensor-core operations the screen issued: 2 M N K per MMA over every
                                      tile pair it ran (padded rows, columns and K included) */
+    /* TJ_FLAG_SCREEN_TIMES: spread of the CTAs' end times (the idle tail of the persistent screen), and
+     * the median, 99th percentile and largest time from a join's first chunk start to its last chunk
+     * end inside the screen launch */
+    double screen_cta_tail_ms;
+    double join_span_ms_p50, join_span_ms_p99, join_span_ms_max;
 } tj_stats;
 
 /* ----------------------------------------------------------------- joins */
@@ -186,14 +197,16 @@ int tj_batch_pairs(const tj_result* res, int64_t* i_out, int64_t* j_out, void* s
 /* ----------------------------------------------------------------- allocation-free sort */
 
 /* Sort n uint64 keys ascending by their low key_bits bits (1..64) into keys_out (device arrays;
- * keys_out may equal keys_in) without allocating any device memory.  No counterpart in the
+ * keys_out may equal keys_in, or must not overlap it at all: a partial overlap returns
+ * TJ_ERR_INVALID) without allocating any device memory.  No counterpart in the
  * reference: it is the canonical-order radix sort of this library, offered for callers that
  * cannot allocate at the call site (a fixed arena owned by the host engine, HBM reserved by
  * another allocator, or no allocation latency allowed between launches).  Its scratch is a
  * file-scope device array of about 9 MiB held by every GPU that loads the library; n is limited
  * to 1,048,576 keys (larger n returns TJ_ERR_INVALID).  All calls on a device share that array:
- * calls that overlap on the GPU race and must be serialised by the caller.  The first call on a
- * device resolves the array's address (cudaGetSymbolAddress); make it before any stream capture. */
+ * calls that overlap on the GPU race and must be serialised by the caller.  The first non-empty call
+ * in a CUDA context resolves the array's address in that context (cudaGetSymbolAddress, cached per
+ * context); make it before any stream capture.  n == 0 returns at once. */
 int tj_sort_keys_noalloc(const uint64_t* keys_in, uint64_t* keys_out, int64_t n, int32_t key_bits, void* stream);
 
 /* ----------------------------------------------------------------- misc */

@@ -29,6 +29,7 @@ FLAG_BAND_FP32 = 16
 FLAG_I8_FOUR_PRODUCTS = 32
 FLAG_GUARDS = 64
 FLAG_STAGE_KEYS = 128
+FLAG_SCREEN_TIMES = 256
 
 # Every symbol include/tensorjoin.h declares (checked by the CPU test suite).
 EXPORTS = [
@@ -57,7 +58,8 @@ class Stats(C.Structure):
         "ms_index", "ms_candidates", "ms_screen", "ms_refine", "ms_sort", "ms_total", "screen_ops",
         "screen_max_abs_err", "screen_err_over_bound")] + [("screen_err_pairs", C.c_int64), ("screen_pair", C.c_int64),
                                                    ("index_frame", C.c_int64), ("band_fp64", C.c_int64),
-                                                   ("screen_ops_issued", C.c_double)]
+                                                   ("screen_ops_issued", C.c_double)] + [
+        (n, C.c_double) for n in ("screen_cta_tail_ms", "join_span_ms_p50", "join_span_ms_p99", "join_span_ms_max")]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -171,7 +171,7 @@ FRAME_FLAGS = {"auto": 0, "axes": _lib.FLAG_FRAME_AXES, "pca": _lib.FLAG_FRAME_P
 def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "bf16", capacity: int = 0,
                 chunk_items: int = 0, screen_diag: bool = False, cta_pair: bool = True,
                 index_frame: str = "auto", band_fp32: bool = False, i8_four_products: bool = False,
-                guards: bool = False, stage_keys: bool = False) -> Result:
+                guards: bool = False, stage_keys: bool = False, screen_times: bool = False) -> Result:
     """Run a join and return the Result handle (pairs, keys, neighbour table, statistics).
 
     ``screen_diag=True`` also samples 64 tile pairs of the tensor-core screen and reports, in
@@ -195,6 +195,7 @@ def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "b
     flags |= FRAME_FLAGS[index_frame] | (_lib.FLAG_BAND_FP32 if band_fp32 else 0)
     flags |= _lib.FLAG_I8_FOUR_PRODUCTS if i8_four_products else 0
     flags |= (_lib.FLAG_GUARDS if guards else 0) | (_lib.FLAG_STAGE_KEYS if stage_keys else 0)
+    flags |= _lib.FLAG_SCREEN_TIMES if screen_times else 0
     return _run(R, S, eps, eps2, mode, screen, capacity, chunk_items, flags)
 
 
@@ -280,10 +281,12 @@ class BatchResult(Result):
 
 def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_items: int = 0,
                         index_frame: str = "auto", band_fp32: bool = False,
-                        screen_diag: bool = False) -> BatchResult:
+                        screen_diag: bool = False, screen_times: bool = False, guards: bool = False) -> BatchResult:
     """Run many independent R-S joins [(R, S, eps), ...] in one batched pass (one screen launch).
-    ``index_frame``, ``band_fp32`` and ``screen_diag`` as in ``join_result`` (packed joins keep
-    input-dimension cells under "auto")."""
+    ``index_frame``, ``band_fp32``, ``screen_diag`` and ``guards`` as in ``join_result`` (packed joins
+    keep input-dimension cells under "auto").  ``screen_times=True`` stamps each join's first and last
+    chunk inside the screen launch and each CTA's end (``stats["join_span_ms_p50"]``, ``_p99``,
+    ``_max`` and ``stats["screen_cta_tail_ms"]``)."""
     if index_frame not in FRAME_FLAGS:
         raise ValueError(f"index_frame must be one of {sorted(FRAME_FLAGS)}")
     descs = (_lib.BatchJoin * len(joins))()
@@ -299,6 +302,7 @@ def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_it
     h = C.c_void_p()
     flags = FRAME_FLAGS[index_frame] | (_lib.FLAG_BAND_FP32 if band_fp32 else 0)
     flags |= _lib.FLAG_SCREEN_DIAG if screen_diag else 0
+    flags |= (_lib.FLAG_SCREEN_TIMES if screen_times else 0) | (_lib.FLAG_GUARDS if guards else 0)
     opt = _lib.Options(int(capacity), int(chunk_items), flags)
     check(lib().tj_join_batched(descs, len(joins), SCREEN[screen], C.byref(opt), C.byref(h),
                                 C.c_void_p(_stream_ptr())))

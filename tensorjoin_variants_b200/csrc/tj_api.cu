@@ -6,6 +6,7 @@
 // overflow-and-retry pass of the reference, src/run_g2a_tensorjoin.py:329-378).
 // Everything else stays on the device in stream order; memory comes from a
 // private stream-ordered pool so repeated joins do not hit cudaMalloc.
+#include <algorithm>
 #include <chrono>
 #include <atomic>
 #include <cmath>
@@ -297,7 +298,8 @@ struct JoinIn {
 void check_flags(const tj_options* opt) {
     if (!opt) return;
     const int known = TJ_FLAG_SCREEN_DIAG | TJ_FLAG_SCREEN_1SM | TJ_FLAG_FRAME_AXES | TJ_FLAG_FRAME_PCA |
-                      TJ_FLAG_BAND_FP32 | TJ_FLAG_I8_FOUR_PRODUCTS | TJ_FLAG_GUARDS | TJ_FLAG_STAGE_KEYS;
+                      TJ_FLAG_BAND_FP32 | TJ_FLAG_I8_FOUR_PRODUCTS | TJ_FLAG_GUARDS | TJ_FLAG_STAGE_KEYS |
+                      TJ_FLAG_SCREEN_TIMES;
     if (opt->flags & ~known) fail(TJ_ERR_INVALID, "unknown option flags");
     if ((opt->flags & TJ_FLAG_FRAME_AXES) && (opt->flags & TJ_FLAG_FRAME_PCA))
         fail(TJ_ERR_INVALID, "TJ_FLAG_FRAME_AXES and TJ_FLAG_FRAME_PCA exclude each other");
@@ -617,12 +619,25 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     const bool guards = opt && (opt->flags & TJ_FLAG_GUARDS);
     const bool stage_keys = opt && (opt->flags & TJ_FLAG_STAGE_KEYS);
     const unsigned long long gs = guards ? kGuardSlots : 0;
+    const bool times = opt && (opt->flags & TJ_FLAG_SCREEN_TIMES) && screen != TJ_SCREEN_PLAIN && !i8;
+    DBuf<unsigned long long> join_t, cta_t;
+    if (times) {
+        join_t = DBuf<unsigned long long>(2 * (size_t)nj, st);
+        cta_t = DBuf<unsigned long long>(2 * (size_t)num_sms(), st);
+        g.join_t = join_t.p;
+        g.cta_t = cta_t.p;
+    }
     DBuf<uint64_t> acc, band;
     Counters h;
     for (int attempt = 0;; ++attempt) {
         acc = DBuf<uint64_t>::result(cap + gs, st);   // becomes the result's key array
         band = DBuf<uint64_t>(bcap + gs, st);
         launch(zero_counters, 1, 32, 0, st, ctr.p, 1);
+        if (times) {   // first starts: all ones (atomicMin), last ends and CTA stamps: zero
+            TJ_CUDA(cudaMemsetAsync(join_t.p, 0xFF, (size_t)nj * 8, st));
+            TJ_CUDA(cudaMemsetAsync(join_t.p + nj, 0, (size_t)nj * 8, st));
+            TJ_CUDA(cudaMemsetAsync(cta_t.p, 0, cta_t.bytes(), st));
+        }
         if (guards) {
             launch(guard_fill, 1, 256, 0, st, acc.p + cap);
             launch(guard_fill, 1, 256, 0, st, band.p + bcap);
@@ -666,6 +681,26 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         memcpy(&S_.screen_max_abs_err, &dv[0], 8);
         memcpy(&S_.screen_err_over_bound, &dv[1], 8);
         S_.screen_err_pairs = (int64_t)dv[2];
+    }
+    if (times) {
+        std::vector<unsigned long long> jt(2 * (size_t)nj), ct(cta_t.n);
+        TJ_CUDA(cudaMemcpyAsync(jt.data(), join_t.p, jt.size() * 8, cudaMemcpyDeviceToHost, st));
+        TJ_CUDA(cudaMemcpyAsync(ct.data(), cta_t.p, ct.size() * 8, cudaMemcpyDeviceToHost, st));
+        TJ_CUDA(cudaStreamSynchronize(st));
+        std::vector<double> span;
+        for (int k = 0; k < nj; ++k)
+            if (jt[nj + k] && jt[k] != ~0ull && jt[nj + k] >= jt[k]) span.push_back((double)(jt[nj + k] - jt[k]) * 1e-6);
+        std::sort(span.begin(), span.end());
+        if (!span.empty()) {
+            auto pct = [&](double p) { return span[std::min(span.size() - 1, (size_t)(p * (double)(span.size() - 1) + 0.5))]; };
+            S_.join_span_ms_p50 = pct(0.5);
+            S_.join_span_ms_p99 = pct(0.99);
+            S_.join_span_ms_max = span.back();
+        }
+        unsigned long long lo = ~0ull, hi = 0;
+        for (size_t b = 0; b + 1 < ct.size(); b += 2)
+            if (ct[b + 1]) { lo = std::min(lo, ct[b + 1]); hi = std::max(hi, ct[b + 1]); }
+        if (hi >= lo && hi) S_.screen_cta_tail_ms = (double)(hi - lo) * 1e-6;
     }
     S_.screen_accept = (int64_t)h.screen_accept;
     S_.band = (int64_t)h.band_valid;

@@ -46,7 +46,8 @@ struct Counters {
     unsigned long long screen_ops;     // algorithmic screen operations of the candidate list
     unsigned long long class_items[4]; // candidate tile pairs per class
     unsigned long long screen_reserved;  // acc_reserved after the screen, before the refinement appends
-    unsigned long long pad[2];
+    unsigned long long chunk_next;       // work queue of the one-SM screen: chunks taken beyond the first wave
+    unsigned long long pad[1];
 };
 constexpr int kCountersPerAttempt = 10;
 

@@ -255,6 +255,10 @@ struct ScreenInput {
     uint4* dump_ids = nullptr;          // [dump_items]
     unsigned dump_every = 0, dump_items = 0;
     unsigned long long* diag_out = nullptr;   // [3]: max |d2hat - d2| (double bits), max ratio to bound, pairs
+    // TJ_FLAG_SCREEN_TIMES (tensor-core screens): per-join first-start / last-end and per-CTA start / end
+    // %globaltimer stamps, null when off
+    unsigned long long* join_t = nullptr;     // [2 njoins]
+    unsigned long long* cta_t = nullptr;      // [2 * grid]
 };
 
 void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);

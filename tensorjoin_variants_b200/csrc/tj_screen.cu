@@ -98,9 +98,14 @@ struct ScreenCtl {
     uint64_t meta_full[kMetaSlots];
     uint64_t meta_empty[kMetaSlots];
     uint64_t drain;
+    uint64_t cfull[4];          // one SM: chunk ring (the producer takes chunks from the device queue)
+    uint64_t cempty[4];
+    unsigned cring[4];
     unsigned tmem_base;
     int abort_flag;
 };
+constexpr int kChunkRing = 4;
+constexpr unsigned kNoChunk = 0xFFFFFFFFu;
 
 // CTA pair (cta_group::2, 256 x 256 tile over two SMs): a stage holds this CTA's 128 A rows and its
 // 128-row half of B for one 64-element k-block; the pair's MMA reads A and B from both CTAs.
@@ -167,21 +172,37 @@ struct ScreenArgs {
     unsigned dump_every;
     unsigned dump_items;
     unsigned long long wait_ns;   // limit of every pipeline wait (drains keep kDrainLimitNs)
+    // TJ_FLAG_SCREEN_TIMES: %globaltimer of each join's first chunk start (join_t[j], atomicMin) and
+    // last chunk end (join_t[njoins + j], atomicMax), and each CTA's start and end (cta_t[2 b], [2 b + 1])
+    unsigned long long* join_t;
+    unsigned long long* cta_t;
+    unsigned njoins;
 };
 
-// r[k] for a runtime k without local memory: a fixed 31-select tree (the rare path's only way
-// to reach one accumulator value, keeping a single copy of its code).
-TJ_DEV uint32_t pick32(const uint32_t (&r)[32], int k) {
-    uint32_t a16[16], a8[8], a4[4], a2[2];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) a16[i] = (k & 16) ? r[i + 16] : r[i];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) a8[i] = (k & 8) ? a16[i + 8] : a16[i];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) a4[i] = (k & 4) ? a8[i + 4] : a8[i];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) a2[i] = (k & 2) ? a4[i + 2] : a4[i];
-    return (k & 1) ? a2[1] : a2[0];
+// One SM: the producer publishes the chunks it takes from the queue in a ring of kChunkRing slots;
+// the UMMA issuer and every epilogue warp read them in the same order (kNoChunk ends the sequence).
+// Its waits are bounded like every other pipeline wait.
+template <int kStages>
+TJ_DEV bool publish_chunk(ScreenCtl<kStages>* ctl, unsigned long long q, unsigned c, unsigned long long* status,
+                          unsigned long long wait_ns) {
+    const unsigned slot = (unsigned)(q % kChunkRing), ph = (unsigned)((q / kChunkRing) & 1);
+    if (!mbar_wait(&ctl->cempty[slot], ph ^ 1u, status, wait_ns)) return false;
+    *(volatile unsigned*)&ctl->cring[slot] = c;
+    mbar_arrive(&ctl->cfull[slot]);   // release: the slot's value is visible to every reader
+    return true;
+}
+// warp-collective in the epilogue warps (every lane reads; lane 0 frees the slot), one lane elsewhere
+template <int kStages>
+TJ_DEV bool take_chunk(ScreenCtl<kStages>* ctl, unsigned long long q, unsigned& c, unsigned long long* status,
+                       unsigned long long wait_ns, bool warp_collective) {
+    const unsigned slot = (unsigned)(q % kChunkRing), ph = (unsigned)((q / kChunkRing) & 1);
+    bool got = mbar_wait(&ctl->cfull[slot], ph, status, wait_ns);
+    if (warp_collective) got = __all_sync(0xffffffffu, got);
+    if (!got) return false;
+    c = *(volatile unsigned*)&ctl->cring[slot];
+    if (warp_collective) __syncwarp();
+    if (!warp_collective || lane_id() == 0) mbar_arrive(&ctl->cempty[slot]);
+    return true;
 }
 
 // Pack the S-side row metadata into one ColMetaF block per 256-row tile.
@@ -271,6 +292,10 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             mbar_init(&ctl->meta_empty[m], kPair ? kEpiWarps : 8);   // one SM: the two groups of an item
         }
         mbar_init(&ctl->drain, 1);
+        for (int r = 0; r < kChunkRing; ++r) {
+            mbar_init(&ctl->cfull[r], 1);
+            mbar_init(&ctl->cempty[r], 1 + kEpiWarps);   // the UMMA issuer and every epilogue warp
+        }
         ctl->abort_flag = 0;
         fence_barrier_init();
         for (int c = 0; c < a.ncls; ++c) {
@@ -290,6 +315,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
     const unsigned nchunks = kPair ? a.nT * ((a.ntS + 63u) / 64u) : *a.nchunks;
     const unsigned cfirst = kPair ? (blockIdx.x >> 1) : blockIdx.x;
     const unsigned cstride = kPair ? (gridDim.x >> 1) : gridDim.x;
+    if (a.cta_t && threadIdx.x == 0) a.cta_t[2 * blockIdx.x] = global_ns();
 
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
@@ -297,10 +323,21 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             unsigned stage = 0, phase = 0;
             unsigned long long n = 0;   // items issued
             bool ok = true;
-            for (unsigned c = cfirst; c < nchunks && ok; c += cstride) {
+            for (unsigned long long qc = 0;; ++qc) {
+                unsigned c;
+                if (kPair) {   // the two CTAs of a pair walk the same static sequence
+                    c = cfirst + (unsigned)qc * cstride;
+                    if (c >= nchunks || !ok) break;
+                } else {       // first wave by CTA index, then the device queue
+                    c = qc == 0 ? blockIdx.x : gridDim.x + (unsigned)atomicAdd(&a.ctr->chunk_next, 1ull);
+                    const bool end = !ok || c >= nchunks;
+                    if (!publish_chunk(ctl, qc, end ? kNoChunk : c, status, a.wait_ns)) { ok = false; break; }
+                    if (end) break;
+                }
                 unsigned rtile, e0, e1;
                 uint4 rt;
                 chunk_at<kPair>(a, c, rank, rtile, rt, e0, e1);
+                if (a.join_t) atomicMin(&a.join_t[rt.z], global_ns());
                 const int rrow = (int)rt.x;
                 const unsigned cls = rt.w;
                 const int kblocks = a.cls[cls].kblocks, kpad = a.cls[cls].kpad, kbk = a.cls[cls].kbk;
@@ -365,7 +402,16 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             unsigned stage = 0, phase = 0, acc = 0, acc_phase = 0;
             unsigned long long n_mma = 0;   // items issued
             bool ok = true;
-            for (unsigned c = cfirst; c < nchunks && ok; c += cstride) {
+            for (unsigned long long qc = 0;; ++qc) {
+                unsigned c;
+                if (kPair) {
+                    c = cfirst + (unsigned)qc * cstride;
+                    if (c >= nchunks || !ok) break;
+                } else {
+                    if (!ok) break;
+                    if (!take_chunk(ctl, qc, c, status, a.wait_ns, false)) { ok = false; break; }
+                    if (c == kNoChunk) break;
+                }
                 unsigned rtile, e0, e1;
                 uint4 rt;
                 chunk_at<kPair>(a, c, 0u, rtile, rt, e0, e1);
@@ -449,7 +495,16 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         unsigned acc = 0, acc_phase = 0;
         unsigned long long n = 0, n_screen_acc = 0, n_rare = 0, n_items = 0;
         bool ok = true;
-        for (unsigned c = cfirst; c < nchunks && ok; c += cstride) {
+        for (unsigned long long qc = 0;; ++qc) {
+            unsigned c;
+            if (kPair) {
+                c = cfirst + (unsigned)qc * cstride;
+                if (c >= nchunks || !ok) break;
+            } else {
+                if (!ok) break;
+                if (!take_chunk(ctl, qc, c, status, a.wait_ns, true)) { ok = false; break; }
+                if (c == kNoChunk) break;
+            }
             unsigned rtile, e0, e1;
             uint4 rt;
             chunk_at<kPair>(a, c, rank, rtile, rt, e0, e1);
@@ -500,8 +555,15 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     tau_in = f32_dn(ti);
                 }
                 const unsigned tbase = tmem + ((q * 32u) << 16) + (kPair ? b * kTileS : b * 128u);
-#pragma unroll 1
-                for (int cb = cb_begin; cb < cb_end; ++cb) {
+                // phase 1: every 32-column block of this warp's part is read from TMEM and tested; a
+                // lane keeps, per block, the mask of its candidates (v <= tau) and of the certified
+                // accepts among them (v <= tau_in).  No warp-collective step runs here, and the
+                // accumulator is handed back as soon as the last block is in registers.
+                uint32_t cmk[4] = {0u, 0u, 0u, 0u}, imk[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int cb = cb_begin + i;
+                    if (cb >= cb_end) break;
                     const int col0 = (int)colbase + cb * 32;   // column of the S tile
                     uint32_t raw[32];
                     tmem_ld32(tbase + cb * 32, raw);
@@ -556,74 +618,71 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                             vm[g] = fmin3(fmin3(fmin3(v0, v1, v2), v3, v4), fminf(v5, v6), v7);
                         }
                     }
-                    // only the groups whose value passes tau (in any lane of the warp) are examined pair
-                    // by pair
-                    const unsigned gmask = (vm[0] <= tau ? 1u : 0u) | (vm[1] <= tau ? 2u : 0u) |
-                                           (vm[2] <= tau ? 4u : 0u) | (vm[3] <= tau ? 8u : 0u);
-                    const unsigned gunion = __reduce_or_sync(0xffffffffu, gmask);
-                    if (!gunion) continue;
-                    // candidate (v <= tau) and certified-in (v <= tau_in) masks over the hit groups only
-                    uint32_t cmask = 0, inm = 0;
+                    // only the groups whose value passes tau in this lane are examined pair by pair
+                    uint32_t cm = 0, im = 0;
 #pragma unroll
                     for (int g = 0; g < 4; ++g) {
-                        if (!(gunion & (1u << g))) continue;
-                        if (gmask & (1u << g)) {
+                        if (vm[g] <= tau) {
 #pragma unroll
                             for (int k = 8 * g; k < 8 * g + 8; ++k) {
                                 const float v = fmaf(-2.f, __uint_as_float(raw[k]), m.nrm2f[col0 + k]);
-                                cmask |= (v <= tau ? 1u : 0u) << k;
-                                inm |= (v <= tau_in ? 1u : 0u) << k;
+                                cm |= (v <= tau ? 1u : 0u) << k;
+                                im |= (v <= tau_in ? 1u : 0u) << k;
                             }
                         }
                     }
-                    if (jp.self_join && cmask) {   // keep sorted column > sorted row only
+                    if (jp.self_join && cm) {   // keep sorted column > sorted row only
                         const int lim = (int)rs - (int)(c0 + col0);   // columns k <= lim: not above the diagonal
-                        if (lim >= 31) cmask = 0;
-                        else if (lim >= 0) cmask &= ~((2u << lim) - 1u);
+                        if (lim >= 31) cm = 0;
+                        else if (lim >= 0) cm &= ~((2u << lim) - 1u);
                     }
-                    if (!__any_sync(0xffffffffu, cmask != 0)) continue;
-                    // ---------------- rare path: certified FP32 accept, else per-pair FP64 certificate
-                    inm &= cmask;
-                    uint32_t amask = inm, bmask = 0;
-                    uint32_t mk = cmask & ~inm;
-                    while (mk) {
-                        const int k = __ffs(mk) - 1;
-                        mk &= mk - 1;
-                        ++n_rare;
-                        const int col = col0 + k;
-                        const double p = (double)__uint_as_float(pick32(raw, k));
-                        const double Bj = m.nrm2[col];
-                        const double sv = Ai + Bj - 2.0 * p;
-                        const double R = jp.gmma * (double)Zi * (double)m.zn[col] + jp.cabs +
-                                         (double)Ei * (double)m.yn[col] + (double)Zi * (double)m.en[col] +
-                                         (double)Zli * (double)m.zl[col];
-                        double mm = 2.0 * R + jp.gn * (Ai + Bj) + 0x1p-50 * (Ai + Bj + 2.0 * fabs(p));
-                        mm = mm * (1.0 + 0x1p-40) + 0x1p-1000;
-                        if (sv + mm <= jp.Tm) amask |= 1u << k;
-                        else if (!(sv - mm > jp.Tp)) bmask |= 1u << k;
-                    }
-                    unsigned ta = 0, tb = 0, pa = 0, pb = 0;   // scans only for lists some lane appends to
-                    if (__any_sync(0xffffffffu, amask != 0)) pa = warp_excl_scan(__popc(amask), ta);
-                    if (__any_sync(0xffffffffu, bmask != 0)) pb = warp_excl_scan(__popc(bmask), tb);
+                    cmk[i] = cm;
+                    imk[i] = im & cm;
+                }
+                // phase 2: one warp scan for the part's certified accepts and band pairs together
+                // (accepts in the low 16 bits, band in the high 16: at most 128 of each per lane), one
+                // reservation per list, then each lane writes its pairs' canonical keys
+                unsigned na = 0, nb = 0;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    na += __popc(imk[i]);
+                    nb += __popc(cmk[i] & ~imk[i]);
+                }
+                const unsigned packed = na | (nb << 16);
+                if (__any_sync(0xffffffffu, packed != 0)) {
+                    unsigned tot;
+                    const unsigned pre = warp_excl_scan(packed, tot);
+                    const unsigned ta = tot & 0xFFFFu, tb = tot >> 16;
+                    n_screen_acc += na;
+                    n_rare += nb;
                     if (ta) {
-                        unsigned long long pos = app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap) + pa;
-                        uint32_t w = amask;
-                        while (w) {
-                            const int k = __ffs(w) - 1;
-                            w &= w - 1;
-                            if (pos < a.acc_cap) a.acc[pos] = pair_key(jp, oi, m.perm[col0 + k]);
-                            ++pos;
+                        unsigned long long pos =
+                            app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap) + (pre & 0xFFFFu);
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            uint32_t w = imk[i];
+                            const int col0 = (int)colbase + (cb_begin + i) * 32;
+                            while (w) {
+                                const int k = __ffs(w) - 1;
+                                w &= w - 1;
+                                if (pos < a.acc_cap) a.acc[pos] = pair_key(jp, oi, m.perm[col0 + k]);
+                                ++pos;
+                            }
                         }
-                        n_screen_acc += __popc(amask);
                     }
                     if (tb) {
-                        unsigned long long pos = app_band.reserve(tb, &a.ctr->band_reserved, a.band, a.band_cap) + pb;
-                        uint32_t w = bmask;
-                        while (w) {
-                            const int k = __ffs(w) - 1;
-                            w &= w - 1;
-                            if (pos < a.band_cap) a.band[pos] = pair_key(jp, oi, m.perm[col0 + k]);
-                            ++pos;
+                        unsigned long long pos =
+                            app_band.reserve(tb, &a.ctr->band_reserved, a.band, a.band_cap) + (pre >> 16);
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            uint32_t w = cmk[i] & ~imk[i];
+                            const int col0 = (int)colbase + (cb_begin + i) * 32;
+                            while (w) {
+                                const int k = __ffs(w) - 1;
+                                w &= w - 1;
+                                if (pos < a.band_cap) a.band[pos] = pair_key(jp, oi, m.perm[col0 + k]);
+                                ++pos;
+                            }
                         }
                     }
                 }
@@ -633,6 +692,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 if (kPair && ++acc == 2) { acc = 0; acc_phase ^= 1; }
               }
             }
+            if (a.join_t && lane == 0) atomicMax(&a.join_t[a.njoins + rt.z], global_ns());
         }
         if (!ok) ctl->abort_flag = 1;
         app_acc.pad(a.acc, a.acc_cap);
@@ -658,6 +718,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         if (kPair) tmem_dealloc_pair(tmem, 512);
         else tmem_dealloc(tmem, 512);
     }
+    if (a.cta_t && threadIdx.x == 0) a.cta_t[2 * blockIdx.x + 1] = global_ns();
 }
 
 // Screen error of the sampled tile pairs: |d2hat - d2| with d2hat = A + B - 2p from the dumped
@@ -823,6 +884,10 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     a.dump_every = g.dump_every ? g.dump_every : 1u;
     a.dump_items = g.dump ? g.dump_items : 0u;
     a.wait_ns = pipeline_wait_ns();
+    a.join_t = g.join_t;
+    a.cta_t = g.cta_t;
+    a.njoins = (unsigned)g.njoins;
+    TJ_CUDA(cudaMemsetAsync(&eb.ctr->chunk_next, 0, sizeof(unsigned long long), st));
     const int grid = num_sms();
 #define TJ_SCREEN(F, SP)                                                                                      \
     do {                                                                                                      \

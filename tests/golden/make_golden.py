@@ -1,4 +1,8 @@
-"""Generate the golden fixtures under tests/golden/ (run in a container that has the reference tree).
+"""Generate the golden fixtures under tests/golden/ (run where the reference tree is available).
+
+Usage: python tests/golden/make_golden.py --reference <path of the tensorjoin-variants checkout>
+(or set TJ_REFERENCE_ROOT).  The fixture is read from
+<reference>/tensorjoin_20260902_certified_exact_join/adapters/gds_g2a/test_dat.txt.
 
 1. ``gds_test_dat_f32.npy``: GDS-Join's shipped 2-D test set
    (tensorjoin_20260902_certified_exact_join/adapters/gds_g2a/test_dat.txt,
@@ -13,9 +17,11 @@
 """
 from __future__ import annotations
 
+import argparse
 import ctypes
 import hashlib
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -23,7 +29,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF = Path("/root/reference/tensorjoin_20260902_certified_exact_join")
+PROJECT = "tensorjoin_20260902_certified_exact_join"
 
 
 def parse_gds(path: Path) -> np.ndarray:
@@ -42,11 +48,18 @@ def sha(a: np.ndarray) -> str:
 
 
 def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("TJ_REFERENCE_ROOT"),
+                    help="root of the reference checkout (or TJ_REFERENCE_ROOT)")
+    args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference or set TJ_REFERENCE_ROOT")
+    ref = Path(args.reference) / PROJECT
     sys.path.insert(0, str(ROOT))
     import oracle
     from tensorjoin_variants_b200 import workloads as W
 
-    X = parse_gds(REF / "adapters/gds_g2a/test_dat.txt")
+    X = parse_gds(ref / "adapters/gds_g2a/test_dat.txt")
     assert X.shape == (100_000, 2)
     np.save(HERE / "gds_test_dat_f32.npy", X)
     directed = oracle.join_f32(X, None, 1.0, "directed")

@@ -59,3 +59,21 @@ def test_noalloc_sort_in_place_and_limits():
     big = torch.zeros(MAX_KEYS + 1, dtype=torch.int64, device="cuda")
     assert _noalloc_sort(big, big, MAX_KEYS + 1, 40) == -1   # beyond the stated maximum: rejected
     assert b"maximum" in _lib.lib().tj_last_error_string()
+    # partly overlapping input and output ranges are rejected (the same array or disjoint ones only)
+    assert _noalloc_sort(big[:1000], big[500:1500], 1000, 40) == -1
+    assert b"overlap" in _lib.lib().tj_last_error_string()
+    assert _noalloc_sort(big, big, 0, 40) == 0                # empty: nothing to do
+
+
+@pytest.mark.parametrize("n", [1, 16384, 16385, MAX_KEYS])
+def test_noalloc_sort_sizes(n):
+    """The one-block path's limit (16,384 keys) on both sides, a single key, and exactly the maximum
+    (the ping-pong buffer full, the histogram and scan area at its largest), out of place."""
+    rng = np.random.default_rng(n)
+    keys = rng.integers(0, 1 << 40, size=n, dtype=np.int64)
+    t = torch.from_numpy(keys).cuda()
+    out = torch.empty_like(t)
+    assert _noalloc_sort(t, out, n, 40) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), np.sort(keys))
+    assert np.array_equal(t.cpu().numpy(), keys)   # the input is left as it was
