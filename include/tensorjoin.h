@@ -66,6 +66,12 @@ typedef struct tj_options {
     int64_t initial_capacity;   /* accept / band buffer slots for the first attempt (0: library default) */
     int32_t chunk_items;        /* tile pairs per scheduling chunk (0: 64) */
     int32_t flags;              /* TJ_FLAG_* bits */
+    /* Tile-shape knobs of the 16-bit tensor-core screens (0: the library's choice; the pairs never
+     * change): k_block = elements of K per pipeline stage (64, 32 or 16; must divide the padded row
+     * length, which is a multiple of 64 for d > 32), stages = operand stages in flight (2 up to the
+     * compiled 4, or 6 on the CTA pair; the hi/lo split compiles 2). */
+    int32_t k_block;
+    int32_t stages;
 } tj_options;
 
 /* Sample tile pairs during the tensor-core screen and report the screen's distance error against
@@ -105,11 +111,17 @@ typedef struct tj_options {
  * end and of every CTA's start and end, and report their spread (tj_stats.join_span_ms_*,
  * screen_cta_tail_ms).  Diagnostic: one atomic per chunk and epilogue warp. */
 #define TJ_FLAG_SCREEN_TIMES 256
+/* One-SM 16-bit screens: issue both 128-row halves of every candidate tile pair.  By default each
+ * half of a candidate's 256-row S tile is first tested against the R tile (the candidate test's
+ * bounds on the half's own statistics) and only live halves are issued, packed densely into the
+ * screen's MMA and epilogue pipeline.  The pairs are the same either way. */
+#define TJ_FLAG_WHOLE_TILES 512
 
 typedef struct tj_stats {
     int64_t n_rows, n_cols;       /* |R|, |S| (self-join: N, N) */
     int64_t pairs_all;            /* |R||S| (R-S) or N(N-1)/2 (self-join) */
-    int64_t tile_pairs;           /* candidate tile pairs screened (128 x 256 each) */
+    int64_t tile_pairs;           /* candidate tile pairs screened (128 x 256 each; one-SM 16-bit screens:
+                                     those with a live 128-row half) */
     int64_t pairs_screened;       /* distance evaluations: sum over tile pairs of valid rows x valid cols */
     int64_t screen_accept;        /* pairs accepted by the certified screen alone */
     int64_t band;                 /* pairs sent to FP64 refinement */

@@ -30,6 +30,7 @@ FLAG_I8_FOUR_PRODUCTS = 32
 FLAG_GUARDS = 64
 FLAG_STAGE_KEYS = 128
 FLAG_SCREEN_TIMES = 256
+FLAG_WHOLE_TILES = 512
 
 # Every symbol include/tensorjoin.h declares (checked by the CPU test suite).
 EXPORTS = [
@@ -48,7 +49,8 @@ class TJError(RuntimeError):
 
 
 class Options(C.Structure):
-    _fields_ = [("initial_capacity", C.c_int64), ("chunk_items", C.c_int32), ("flags", C.c_int32)]
+    _fields_ = [("initial_capacity", C.c_int64), ("chunk_items", C.c_int32), ("flags", C.c_int32),
+                ("k_block", C.c_int32), ("stages", C.c_int32)]
 
 
 class Stats(C.Structure):

@@ -142,7 +142,8 @@ class Result:
         return self._out(counts, flat)
 
 
-def _run(R, S, eps, eps2, mode: str, screen: str, capacity: int, chunk_items: int, flags: int = 0) -> Result:
+def _run(R, S, eps, eps2, mode: str, screen: str, capacity: int, chunk_items: int, flags: int = 0,
+         k_block: int = 0, stages: int = 0) -> Result:
     if screen not in SCREEN:
         raise ValueError(f"screen must be one of {sorted(SCREEN)}")
     Rt, host = _as_device(R, screen == "int8limb")
@@ -157,7 +158,7 @@ def _run(R, S, eps, eps2, mode: str, screen: str, capacity: int, chunk_items: in
         St = Rt
     T = _threshold(eps, eps2)
     dtype = _lib.DTYPE["i16"] if Rt.dtype == torch.int16 else _lib.DTYPE["f32"]
-    opt = _lib.Options(int(capacity), int(chunk_items), int(flags))
+    opt = _lib.Options(int(capacity), int(chunk_items), int(flags), int(k_block), int(stages))
     h = C.c_void_p()
     check(lib().tj_join(C.c_void_p(Rt.data_ptr()), Rt.shape[0], C.c_void_p(St.data_ptr()), St.shape[0],
                         Rt.shape[1], dtype, T, MODE[mode], SCREEN[screen], C.byref(opt), C.byref(h),
@@ -171,7 +172,8 @@ FRAME_FLAGS = {"auto": 0, "axes": _lib.FLAG_FRAME_AXES, "pca": _lib.FLAG_FRAME_P
 def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "bf16", capacity: int = 0,
                 chunk_items: int = 0, screen_diag: bool = False, cta_pair: bool = True,
                 index_frame: str = "auto", band_fp32: bool = False, i8_four_products: bool = False,
-                guards: bool = False, stage_keys: bool = False, screen_times: bool = False) -> Result:
+                guards: bool = False, stage_keys: bool = False, screen_times: bool = False,
+                k_block: int = 0, stages: int = 0, half_pack: bool = True) -> Result:
     """Run a join and return the Result handle (pairs, keys, neighbour table, statistics).
 
     ``screen_diag=True`` also samples 64 tile pairs of the tensor-core screen and reports, in
@@ -186,21 +188,45 @@ def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "b
     int8-limb screen issue all four limb products and decide every pair inside the screen, instead of
     the high-limb product plus an exact integer refinement of the undecided band.  ``guards=True``
     checks guard regions after every output buffer (an overwrite fails the join); ``stage_keys=True``
-    keeps the screen's certified accepts and its band for ``Result.stage_keys``."""
+    keeps the screen's certified accepts and its band for ``Result.stage_keys``.  ``k_block`` (16, 32
+    or 64 elements of K per stage) and ``stages`` (operand stages in flight) are tile-shape knobs of
+    the 16-bit screens for the autotuner; 0 keeps the library's choice.  ``half_pack=False`` makes
+    the one-SM screen issue both 128-row halves of every candidate tile pair (by default dead halves
+    are dropped after a half-tile bound test).  ``screen="auto"`` takes the
+    screen and knobs from the committed B200 tuning table (``autotune.default_table``) for this
+    workload's key (d, size, selectivity measured on a 512-row probe), BF16 hi/lo on a miss."""
     if mode not in MODE:
         raise ValueError(f"mode must be one of {sorted(MODE)}")
     if index_frame not in FRAME_FLAGS:
         raise ValueError(f"index_frame must be one of {sorted(FRAME_FLAGS)}")
+    if screen == "auto":   # the committed tuning table's choice for this workload (library defaults on a miss)
+        from . import autotune
+
+        choice, _ = autotune.default_table().choose(R, S, _threshold(eps, eps2), mode, "auto", tune_on_miss=False)
+        kw = choice.kwargs()
+        return join_result(R, S, eps2=_threshold(eps, eps2), mode=mode, screen=choice.screen_for("bf16x3"),
+                           capacity=capacity, chunk_items=chunk_items or kw["chunk_items"], screen_diag=screen_diag,
+                           cta_pair=cta_pair and kw["cta_pair"],
+                           index_frame=index_frame if index_frame != "auto" else kw["index_frame"],
+                           band_fp32=band_fp32 or kw["band_fp32"], guards=guards, stage_keys=stage_keys,
+                           screen_times=screen_times, k_block=k_block or kw["k_block"], stages=stages or kw["stages"])
     flags = (_lib.FLAG_SCREEN_DIAG if screen_diag else 0) | (0 if cta_pair else _lib.FLAG_SCREEN_1SM)
     flags |= FRAME_FLAGS[index_frame] | (_lib.FLAG_BAND_FP32 if band_fp32 else 0)
     flags |= _lib.FLAG_I8_FOUR_PRODUCTS if i8_four_products else 0
     flags |= (_lib.FLAG_GUARDS if guards else 0) | (_lib.FLAG_STAGE_KEYS if stage_keys else 0)
     flags |= _lib.FLAG_SCREEN_TIMES if screen_times else 0
-    return _run(R, S, eps, eps2, mode, screen, capacity, chunk_items, flags)
+    flags |= 0 if half_pack else _lib.FLAG_WHOLE_TILES
+    return _run(R, S, eps, eps2, mode, screen, capacity, chunk_items, flags, k_block, stages)
 
 
 def join(R, S, eps=None, *, eps2=None, screen: str = "bf16", return_stats: bool = False, **kw):
-    """R-S epsilon-join: sorted (i, j) with FP64 direct-difference distance <= eps."""
+    """R-S epsilon-join: sorted (i, j) with FP64 direct-difference distance <= eps
+    (``screen="auto"``: the tuned choice, see ``join_result``)."""
+    if screen == "auto":
+        res = join_result(R, S, eps, eps2=eps2, mode="rs", screen="auto", capacity=kw.get("capacity", 0),
+                          chunk_items=kw.get("chunk_items", 0))
+        i, j = res.pairs()
+        return (i, j, res.stats) if return_stats else (i, j)
     res = _run(R, S, eps, eps2, "rs", screen, kw.get("capacity", 0), kw.get("chunk_items", 0))
     i, j = res.pairs()
     return (i, j, res.stats) if return_stats else (i, j)
@@ -281,7 +307,9 @@ class BatchResult(Result):
 
 def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_items: int = 0,
                         index_frame: str = "auto", band_fp32: bool = False,
-                        screen_diag: bool = False, screen_times: bool = False, guards: bool = False) -> BatchResult:
+                        screen_diag: bool = False, screen_times: bool = False, guards: bool = False,
+                        k_block: int = 0, stages: int = 0, cta_pair: bool = True,
+                        half_pack: bool = True) -> BatchResult:
     """Run many independent R-S joins [(R, S, eps), ...] in one batched pass (one screen launch).
     ``index_frame``, ``band_fp32``, ``screen_diag`` and ``guards`` as in ``join_result`` (packed joins
     keep input-dimension cells under "auto").  ``screen_times=True`` stamps each join's first and last
@@ -303,7 +331,9 @@ def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_it
     flags = FRAME_FLAGS[index_frame] | (_lib.FLAG_BAND_FP32 if band_fp32 else 0)
     flags |= _lib.FLAG_SCREEN_DIAG if screen_diag else 0
     flags |= (_lib.FLAG_SCREEN_TIMES if screen_times else 0) | (_lib.FLAG_GUARDS if guards else 0)
-    opt = _lib.Options(int(capacity), int(chunk_items), flags)
+    flags |= 0 if cta_pair else _lib.FLAG_SCREEN_1SM
+    flags |= 0 if half_pack else _lib.FLAG_WHOLE_TILES
+    opt = _lib.Options(int(capacity), int(chunk_items), flags, int(k_block), int(stages))
     check(lib().tj_join_batched(descs, len(joins), SCREEN[screen], C.byref(opt), C.byref(h),
                                 C.c_void_p(_stream_ptr())))
     return BatchResult(h, len(joins), host, keepalive=tuple(keep))

@@ -1,61 +1,107 @@
-"""Autotuner for the join's run-time choices, keyed by (d, dtype, screen, mode, size, selectivity).
+"""Autotuner over the join's tile shapes and variants, keyed by (d, dtype, screen, mode, size, selectivity).
 
-The kernels' tile shapes are fixed at compile time (128 x 256 items, or 256 x 256 on a CTA pair;
-16-, 32- or 64-element k-blocks by d; stage counts by screen), so what is left to choose per
-workload is which of those variants runs and how the work is cut:
+What it chooses, per workload (every choice gives the same pair set; only the time differs):
 
-* ``cta_pair``     -- the 2-SM (cta_group::2) screen or the one-SM screen, where both apply;
-* ``chunk_items``  -- tile pairs per scheduling chunk of the persistent screen;
+* ``screen``       -- the screen's operand format when the caller asks for ``screen="auto"``:
+                      BF16 or FP16, single or hi/lo-split (x3) operands;
+* ``cta_pair``     -- BM x BN: 256 x 256 tiles on a CTA pair (cta_group::2) or 128 x 256 on one SM;
+* ``k_block``      -- BK: elements of K per pipeline stage (64, 32 or 16);
+* ``stages``       -- operand stages in flight (2 up to the compiled count);
+* ``i8_four_products`` -- limb count of the int14 screen: the high-limb product only (undecided
+                      pairs refined exactly) or all four limb products decided in the kernel;
+* ``chunk_items``  -- tile pairs per chunk of the persistent screen's work queue;
 * ``index_frame``  -- cells over input dimensions or over principal directions;
 * ``band_fp32``    -- the certified FP32 band stage in front of the FP64 terminal.
 
-``Tuner.tune`` times every applicable combination on an evenly spaced row sample of the caller's
-data (the library's own per-stage device times, best of ``reps``), keeps the fastest, and stores it
-under a key built from d, dtype, screen, mode, the log2 size of the pair space and the log2
-selectivity (result pairs per row) measured on the sample.  ``Tuner.join`` estimates the
-selectivity on a small sample, looks the key up (tuning on a miss) and runs the full join with the
-chosen options.  Every choice gives the same pair set; only the time differs.  The table can be
-saved to and loaded from a JSON file.
+The space is searched coordinate by coordinate in the order above: each dimension's values are
+timed with the others held at the best so far (the library's own device time of the whole join,
+best of ``reps``, on an evenly spaced row sample of the caller's data), so a tuning costs about
+twenty sample joins instead of the product of all options.  Every timed choice must give the same
+pair count.  The result is stored under a key of d, dtype, requested screen, mode, the log2 size
+of the pair space and the log2 selectivity (result pairs per row); tables persist as JSON.
+
+``default_table()`` is the table committed with the package (``tuned_b200.json``, produced by
+``python -m tensorjoin_variants_b200.autotune`` on a B200 over the five benchmark configurations);
+``api.join(..., screen="auto")`` and ``Tuner.join`` consult it before tuning.
 
 The reference has no autotuner (its kernels state "no autotuned configurations",
 tensorjoin_20260902_certified_exact_join/two_gate_campaign_20260908/src/g2_kernels.py:1).
 """
 from __future__ import annotations
 
-import itertools
 import json
 import math
 import os
 import threading
-from dataclasses import asdict, dataclass
+from dataclasses import asdict, dataclass, replace
+from pathlib import Path
 from typing import Callable
 
 import torch
 
 from . import api
+from ._lib import TJError
+
+DEFAULT_TABLE = Path(__file__).resolve().parent / "tuned_b200.json"
+FLOAT_SCREENS = ("bf16x3", "fp16x3", "bf16", "fp16")
 
 
 @dataclass(frozen=True)
 class Choice:
+    screen: str = ""              # "": the screen the caller asked for
     cta_pair: bool = True
+    k_block: int = 0              # 0: by d (64 for rows of more than 32 elements)
+    stages: int = 0               # 0: every compiled stage
+    i8_four_products: bool = False
     chunk_items: int = 0          # 0: the library default (64)
     index_frame: str = "auto"
     band_fp32: bool = False
 
     def kwargs(self) -> dict:
-        return dict(cta_pair=self.cta_pair, chunk_items=self.chunk_items, index_frame=self.index_frame,
-                    band_fp32=self.band_fp32)
+        kw = dict(cta_pair=self.cta_pair, chunk_items=self.chunk_items, index_frame=self.index_frame,
+                  band_fp32=self.band_fp32, k_block=self.k_block, stages=self.stages,
+                  i8_four_products=self.i8_four_products)
+        return kw
+
+    def screen_for(self, requested: str) -> str:
+        return self.screen or requested
 
 
 CHUNK_ITEMS = (16, 64, 256)
 
 
+def dimensions(d: int, screen: str, mode: str) -> list[tuple[str, list]]:
+    """Per dimension, the values that change what runs for this (d, requested screen, mode); the
+    first value of each list is the library's default."""
+    kpad = 16 if d <= 16 else 32 if d <= 32 else 64 * ((d + 63) // 64)
+    dims: list[tuple[str, list]] = []
+    if screen == "auto":
+        dims.append(("screen", list(FLOAT_SCREENS)))
+    float_screen = screen != "int8limb" and screen != "plain"
+    if float_screen and mode == "rs" and d >= 256:
+        dims.append(("cta_pair", [True, False]))
+    if screen == "int8limb" and kpad <= 256:
+        dims.append(("i8_four_products", [False, True]))
+    if float_screen:
+        kbs = [0] + [k for k in (32, 16) if k < min(kpad, 64) and kpad % k == 0]
+        if len(kbs) > 1:
+            dims.append(("k_block", kbs))
+        dims.append(("stages", [0, 3, 2]))
+    dims.append(("chunk_items", [0] + [c for c in CHUNK_ITEMS if c != 64]))
+    if 9 <= d <= 128:
+        dims.append(("index_frame", ["axes", "pca"]))
+    if float_screen:
+        dims.append(("band_fp32", [False, True]))
+    return dims
+
+
 def candidates(d: int, screen: str, mode: str) -> list[Choice]:
-    """Every combination whose options change what runs for this (d, screen, mode)."""
-    pairs = [True, False] if (mode == "rs" and d >= 256 and screen in ("bf16", "fp16")) else [True]
-    frames = ["axes", "pca"] if 9 <= d <= 128 else ["auto"]
-    bands = [False, True] if screen in ("bf16", "fp16", "bf16x3", "fp16x3") else [False]
-    return [Choice(p, c, f, b) for p, c, f, b in itertools.product(pairs, CHUNK_ITEMS, frames, bands)]
+    """Every single-coordinate variation of the default choice (the first sweep of the search)."""
+    out = [Choice()]
+    for name, values in dimensions(d, screen, mode):
+        for v in values[1:]:
+            out.append(replace(Choice(), **{name: v}))
+    return out
 
 
 def tune_key(d: int, dtype: str, screen: str, mode: str, n_rows: int, n_cols: int, per_row: float) -> str:
@@ -73,11 +119,23 @@ def _sample_rows(X: torch.Tensor, k: int) -> torch.Tensor:
     return X.index_select(0, idx).contiguous()
 
 
+_DEFAULT = None
+
+
+def default_table() -> "Tuner":
+    """The committed B200 table (read-only use; empty if the file is absent)."""
+    global _DEFAULT
+    if _DEFAULT is None:
+        _DEFAULT = Tuner(str(DEFAULT_TABLE) if DEFAULT_TABLE.exists() else None, read_only=True)
+    return _DEFAULT
+
+
 class Tuner:
     """Per-key table of the fastest ``Choice``; thread-safe; optional JSON persistence."""
 
-    def __init__(self, path: str | None = None):
+    def __init__(self, path: str | None = None, read_only: bool = False):
         self.path = path
+        self.read_only = read_only
         self.table: dict[str, dict] = {}
         self._lock = threading.Lock()
         if path and os.path.exists(path):
@@ -93,7 +151,7 @@ class Tuner:
     def record(self, key: str, best: Choice, timings: dict[str, float]) -> None:
         with self._lock:
             self.table[key] = {"choice": asdict(best), "ms": timings}
-            if self.path:
+            if self.path and not self.read_only:
                 tmp = self.path + ".tmp"
                 with open(tmp, "w") as f:
                     json.dump(self.table, f, indent=1, sort_keys=True)
@@ -101,16 +159,20 @@ class Tuner:
 
     # ---------------------------------------------------------------- measuring
     @staticmethod
-    def pick(cands: list[Choice], runner: Callable[[Choice], tuple[float, int]], reps: int = 2):
-        """Run every candidate ``reps`` times through ``runner`` (-> (ms, result pairs)); the
-        fastest by its best time wins, ties to the earlier candidate.  Returns (best, timings,
-        result pairs of the first run)."""
+    def pick(cands: list[Choice], runner: Callable[[Choice], tuple[float, int]], reps: int = 2,
+             count: int | None = None):
+        """Run every candidate ``reps`` times through ``runner`` (-> (ms, result pairs), or None when
+        the choice cannot run on this data); the fastest by its best time wins, ties to the earlier
+        candidate.  Returns (best, timings, result pairs)."""
         timings: dict[str, float] = {}
-        best, best_ms, count = None, math.inf, None
+        best, best_ms = None, math.inf
         for c in cands:
             ms = math.inf
             for _ in range(max(1, reps)):
-                t, n = runner(c)
+                r = runner(c)
+                if r is None:
+                    break
+                t, n = r
                 if count is None:
                     count = n
                 elif n != count:
@@ -119,12 +181,32 @@ class Tuner:
             timings[json.dumps(asdict(c), sort_keys=True)] = ms
             if ms < best_ms:
                 best, best_ms = c, ms
+        if best is None:
+            raise RuntimeError("no candidate could run")
+        return best, timings, count or 0
+
+    @classmethod
+    def search(cls, d: int, screen: str, mode: str, runner: Callable[[Choice], tuple[float, int] | None],
+               reps: int = 2):
+        """Coordinate search: each dimension's values timed with the others at the best so far."""
+        best = Choice()
+        timings: dict[str, float] = {}
+        count = None
+        for name, values in dimensions(d, screen, mode):
+            cands = [replace(best, **{name: v}) for v in values]
+            best, t, count = cls.pick(cands, runner, reps, count)
+            timings.update(t)
         return best, timings, count or 0
 
     @staticmethod
     def _device_runner(R, S, eps2, mode, screen):
         def run(c: Choice):
-            res = api.join_result(R, S, eps2=eps2, mode=mode, screen=screen, **c.kwargs())
+            try:
+                res = api.join_result(R, S, eps2=eps2, mode=mode, screen=c.screen_for(screen), **c.kwargs())
+            except TJError as e:
+                if e.code in (-4, -7):   # FP16 range exceeded / combination not supported: skip
+                    return None
+                raise
             st = res.stats
             return float(st["ms_total"]), int(st["result_pairs"])
         return run
@@ -140,14 +222,12 @@ class Tuner:
 
     def tune(self, R, S, eps2: float, mode: str = "rs", screen: str = "bf16", sample_rows: int = 4096,
              reps: int = 2) -> tuple[Choice, str, dict]:
-        """Time every applicable choice on a row sample and record the fastest; returns
-        (choice, key, timings in ms per choice)."""
+        """Search the choices on a row sample and record the fastest; returns (choice, key, timings)."""
         Rt, _ = api._as_device(R, screen == "int8limb")
         St = None if S is None else api._as_device(S, screen == "int8limb")[0]
         Rs, Ss, scale = self._sample(Rt, St, mode, sample_rows)
         d = Rt.shape[1]
-        best, timings, count = self.pick(candidates(d, screen, mode),
-                                         self._device_runner(Rs, Ss, eps2, mode, screen), reps)
+        best, timings, count = self.search(d, screen, mode, self._device_runner(Rs, Ss, eps2, mode, screen), reps)
         per_row = count / max(1, Rs.shape[0]) * scale
         key = tune_key(d, _dtype(Rt), screen, mode, Rt.shape[0], Rt.shape[0] if St is None else St.shape[0], per_row)
         self.record(key, best, timings)
@@ -158,25 +238,99 @@ class Tuner:
         Rt, _ = api._as_device(R, screen == "int8limb")
         St = None if S is None else api._as_device(S, screen == "int8limb")[0]
         Rs, Ss, scale = self._sample(Rt, St, mode, probe_rows)
-        res = api.join_result(Rs, Ss, eps2=eps2, mode=mode, screen=screen)
+        probe = "bf16x3" if screen == "auto" else screen
+        res = api.join_result(Rs, Ss, eps2=eps2, mode=mode, screen=probe)
         per_row = res.count / max(1, Rs.shape[0]) * scale
         return tune_key(Rt.shape[1], _dtype(Rt), screen, mode, Rt.shape[0],
                         Rt.shape[0] if St is None else St.shape[0], per_row)
+
+    def choose(self, R, S, eps2: float, mode: str, screen: str, sample_rows: int = 4096,
+               tune_on_miss: bool = True) -> tuple[Choice, str]:
+        """The choice for this join: this table, then the committed default table, then (on a miss)
+        a tuning run on a sample, or the library defaults when tuning is off."""
+        key = self.key_for(R, S, eps2, mode, screen)
+        choice = self.lookup(key)
+        if choice is None and self is not default_table():
+            choice = default_table().lookup(key)
+        if choice is None:
+            if not tune_on_miss:
+                return Choice(screen="bf16x3" if screen == "auto" else ""), key
+            # the tuning sample may bucket its selectivity differently: keep both keys
+            choice, _, timings = self.tune(R, S, eps2, mode, screen, sample_rows)
+            self.record(key, choice, timings)
+        return choice, key
 
     def join(self, R, S=None, eps=None, *, eps2=None, mode: str = "rs", screen: str = "bf16",
              sample_rows: int = 4096) -> api.Result:
         """Run the join with the table's choice for its key, tuning first on a miss."""
         T = api._threshold(eps, eps2)
-        key = self.key_for(R, S, T, mode, screen)
-        choice = self.lookup(key)
-        if choice is None:   # the tuning sample may bucket its selectivity differently: keep both keys
-            choice, _, timings = self.tune(R, S, T, mode, screen, sample_rows)
-            self.record(key, choice, timings)
-        return api.join_result(R, S, eps2=T, mode=mode, screen=screen, **choice.kwargs())
+        choice, _ = self.choose(R, S, T, mode, screen, sample_rows)
+        return api.join_result(R, S, eps2=T, mode=mode, screen=choice.screen_for(screen), **choice.kwargs())
+
+    # ---------------------------------------------------------------- batched joins
+    def join_batched(self, joins, screen: str = "bf16x3", sample_joins: int = 64, reps: int = 2):
+        """Tuned batched join: the choice is searched on a seeded sample of the batch's joins (the
+        batch's own mix of sizes and dimensions), keyed by the dimensions present, the requested
+        screen, the number of joins and the log2 of the batch's pair space."""
+        dims = sorted({int(j[0].shape[1]) for j in joins})
+        space = sum(int(j[0].shape[0]) * int(j[1].shape[0]) for j in joins)
+        key = (f"batch/d{'-'.join(map(str, dims))}/f32/{screen}/joins2^{int(round(math.log2(max(1, len(joins)))))}"
+               f"/space2^{int(round(math.log2(max(1, space))))}")
+        choice = self.lookup(key) or default_table().lookup(key)
+        if choice is None:
+            g = torch.Generator().manual_seed(len(joins))
+            idx = torch.randperm(len(joins), generator=g)[:sample_joins].tolist()
+            sample = [joins[i] for i in sorted(idx)]
+
+            def run(c: Choice):
+                kw = c.kwargs()
+                kw.pop("i8_four_products")
+                try:
+                    res = api.join_batched_result(sample, screen=c.screen_for(screen), **kw)
+                except TJError as e:
+                    if e.code in (-4, -7):
+                        return None
+                    raise
+                return float(res.stats["ms_total"]), int(res.stats["result_pairs"])
+
+            best, timings, _ = self.search(max(dims), screen, "rs", run, reps)
+            self.record(key, best, timings)
+            choice = best
+        kw = choice.kwargs()
+        kw.pop("i8_four_products")
+        return api.join_batched_result(joins, screen=choice.screen_for(screen), **kw), choice
 
 
 def _dtype(t: torch.Tensor) -> str:
     return "i16" if t.dtype == torch.int16 else "f32"
 
 
-__all__ = ["Choice", "Tuner", "candidates", "tune_key", "CHUNK_ITEMS"]
+def _produce(path: str, sample_rows: int) -> None:
+    """Tune the five benchmark configurations (seeded synthetic data of their shapes) on this GPU
+    and write the table to `path`."""
+    from . import workloads as W
+
+    t = Tuner(path)
+    jobs = [("factor512", "fp16", "rs"), ("factor512", "auto", "rs"), ("mixture64", "bf16x3", "rs"),
+            ("mixture64", "auto", "rs"), ("int14x128", "int8limb", "upper"), ("uniform16", "plain", "upper")]
+    for name, screen, mode in jobs:
+        w = getattr(W, name)()
+        R = torch.from_numpy(w.R).cuda()
+        S = None if w.S is None else torch.from_numpy(w.S).cuda()
+        choice, key = t.choose(R, S, float(w.T), mode, screen, sample_rows)
+        print(f"{name} {screen}: {key} -> {choice}", flush=True)
+        del R, S
+    print(json.dumps(t.table, indent=1, sort_keys=True))
+
+
+if __name__ == "__main__":
+    import argparse
+
+    ap = argparse.ArgumentParser(description="tune the benchmark configurations and write a table")
+    ap.add_argument("--out", default=str(DEFAULT_TABLE))
+    ap.add_argument("--sample-rows", type=int, default=8192)
+    a = ap.parse_args()
+    _produce(a.out, a.sample_rows)
+
+
+__all__ = ["Choice", "Tuner", "candidates", "dimensions", "tune_key", "default_table", "CHUNK_ITEMS"]

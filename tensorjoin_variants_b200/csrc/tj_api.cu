@@ -138,7 +138,7 @@ __global__ void cell_starts(const uint32_t* flag, const uint32_t* pos, long long
 // (out[1], ops_per_pair[c] = 2 d (16-bit), 6 d (hi/lo split) or 8 d (int8 limbs) for class c) and tile
 // pairs per class (out[2 + c] = class_items[c], for the issued-operation count).
 __global__ void pairs_screened_kernel(const uint4* chunks, const uint32_t* nchunks, const uint32_t* jlist,
-                                      const uint4* rtiles, const uint4* stiles, const ScreenOps ops,
+                                      const uint4* rtiles, const uint4* stiles, const ScreenOps ops, int half,
                                       unsigned long long* out) {
     unsigned long long acc = 0, aops = 0, items[kMaxClass] = {0, 0, 0, 0};
     const unsigned n = *nchunks;
@@ -146,12 +146,23 @@ __global__ void pairs_screened_kernel(const uint4* chunks, const uint32_t* nchun
         const uint4 ch = chunks[c];
         const uint4 rt = rtiles[ch.x];
         const unsigned long long rv = rt.y;
-        unsigned long long p = 0;
-        for (unsigned e = ch.y; e < ch.z; ++e) p += rv * stiles[jlist[e]].y;
+        unsigned long long p = 0, hi = 0;   // hi: 128-column half-items issued
+        for (unsigned e = ch.y; e < ch.z; ++e) {
+            const uint32_t je = jlist[e];
+            const unsigned nv = stiles[je & kJMask].y;
+            if (!half) {
+                p += rv * nv;
+                hi += 2;
+                continue;
+            }
+            const unsigned m = je >> 30;
+            if (m & 1u) { p += rv * min(nv, 128u); ++hi; }
+            if (m & 2u) { p += rv * (nv > 128u ? nv - 128u : 0u); ++hi; }
+        }
         acc += p;
         aops += p * ops.per_pair[rt.w];
 #pragma unroll
-        for (int q = 0; q < kMaxClass; ++q) items[q] += rt.w == (unsigned)q ? ch.z - ch.y : 0u;
+        for (int q = 0; q < kMaxClass; ++q) items[q] += rt.w == (unsigned)q ? hi : 0u;
     }
     for (int o = 16; o > 0; o >>= 1) {
         acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -299,10 +310,13 @@ void check_flags(const tj_options* opt) {
     if (!opt) return;
     const int known = TJ_FLAG_SCREEN_DIAG | TJ_FLAG_SCREEN_1SM | TJ_FLAG_FRAME_AXES | TJ_FLAG_FRAME_PCA |
                       TJ_FLAG_BAND_FP32 | TJ_FLAG_I8_FOUR_PRODUCTS | TJ_FLAG_GUARDS | TJ_FLAG_STAGE_KEYS |
-                      TJ_FLAG_SCREEN_TIMES;
+                      TJ_FLAG_SCREEN_TIMES | TJ_FLAG_WHOLE_TILES;
     if (opt->flags & ~known) fail(TJ_ERR_INVALID, "unknown option flags");
     if ((opt->flags & TJ_FLAG_FRAME_AXES) && (opt->flags & TJ_FLAG_FRAME_PCA))
         fail(TJ_ERR_INVALID, "TJ_FLAG_FRAME_AXES and TJ_FLAG_FRAME_PCA exclude each other");
+    if (opt->k_block != 0 && opt->k_block != 16 && opt->k_block != 32 && opt->k_block != 64)
+        fail(TJ_ERR_INVALID, "k_block must be 0, 16, 32 or 64");
+    if (opt->stages != 0 && (opt->stages < 2 || opt->stages > 6)) fail(TJ_ERR_INVALID, "stages must be 0 or 2..6");
 }
 
 // One or many joins.  Joins are grouped into classes of equal d; each class gets one
@@ -380,6 +394,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     struct Cls {
         Side R, S;
         TileSet tR, tS;
+        TileSet tSh;   // 128-row halves of the S tiles (half-tile masks of the one-SM screen)
         DBuf<float> XR, XS, center;
         DBuf<FrameParams> fp;
         bool pca_frame = false;   // cells over principal directions (else input dimensions)
@@ -527,6 +542,8 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     g.h_jps = jps.data();
     g.allow_pair = !(opt && (opt->flags & TJ_FLAG_SCREEN_1SM));
     g.i8_four_products = opt && (opt->flags & TJ_FLAG_I8_FOUR_PRODUCTS);
+    g.k_block = opt ? opt->k_block : 0;
+    g.stages = opt ? opt->stages : 0;
     g.key_off = d_koff.p;
     g.rsrc = d_rsrc.p;
     g.ssrc = d_ssrc.p;
@@ -577,13 +594,38 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     memset(&sops, 0, sizeof(sops));
     for (int c = 0; c < ncls; ++c) {
         sops.per_pair[c] = (unsigned long long)cls_d[c] * (i8 ? 8ull : (C[c]->R.split ? 6ull : 2ull));
-        // one tile pair issues 2 M N K per product: 128 x 256 (16-bit, 3 products with the split) or
-        // 128 x 128 (int8: the high-limb screen issues hh only)
-        sops.per_item[c] = 2.0 * kTileR * (double)stile * (double)C[c]->R.kpad * (C[c]->R.split ? 3.0 : 1.0);
+        // one half-item issues 2 M N K per product: 128 x 128 (16-bit, 3 products with the split; a
+        // tile pair is two half-items) or 128 x 128 x 1/2 (int8: an item is one 128 x 128 tile pair,
+        // counted as two halves, of which the high-limb screen issues hh only)
+        sops.per_item[c] = 2.0 * kTileR * 128.0 * (double)C[c]->R.kpad * (C[c]->R.split ? 3.0 : 1.0) *
+                           (i8 ? 0.5 : 1.0);
+    }
+    // live 128-row halves of every candidate for the one-SM 16-bit screen (joins the CTA-pair screen
+    // is likely to take skip this: that screen walks the whole tile grid)
+    const bool tc16 = !i8 && screen != TJ_SCREEN_PLAIN;
+    const bool likely_pair = g.allow_pair && ncls == 1 && nj == 1 && !self && !C[0]->R.split && C[0]->R.kpad >= 256;
+    const bool diag_req = opt && (opt->flags & TJ_FLAG_SCREEN_DIAG) && tc16;   // samples whole tile pairs
+    g.half_packed = tc16 && !likely_pair && !diag_req && !(opt && (opt->flags & TJ_FLAG_WHOLE_TILES));
+    if (g.half_packed) {
+        std::vector<HalfView> hv(ncls);
+        for (int c = 0; c < ncls; ++c) {
+            Cls& K = *C[c];
+            TileSet& H = K.tSh;
+            for (size_t t = 0; t < K.tS.h_row0.size(); ++t)
+                for (uint32_t h = 0; h < 2; ++h) {
+                    const uint32_t nv = K.tS.h_nvalid[t];
+                    H.h_row0.push_back(K.tS.h_row0[t] + 128u * h);
+                    H.h_nvalid.push_back(nv > 128u * h ? std::min(128u, nv - 128u * h) : 0u);
+                }
+            tile_stats(*g.S[c], 128, H, st);
+            hv[c] = HalfView{K.tR.ctrT.p, K.tR.loT.p, K.tR.hiT.p, K.tR.rad.p, H.ctrT.p, H.loT.p, H.hiT.p, H.rad.p,
+                             H.nvalid.p, K.tR.ntiles, H.ntiles, g.rbase[c], g.sbase[c], cls_d[c], 0};
+        }
+        half_masks(hv, cand, g.ntR_total, d_rt.p, d_jps.p, self, st);
     }
     launch(pairs_screened_kernel, num_sms() * 4, 256, 0, st, (const uint4*)cand.chunks.p,
            (const uint32_t*)(cand.dev_counts.p + 1), (const uint32_t*)cand.jlist.p, (const uint4*)d_rt.p,
-           (const uint4*)d_st.p, sops, &ctr.p->pairs_screened);
+           (const uint4*)d_st.p, sops, g.half_packed ? 1 : 0, &ctr.p->pairs_screened);
     ev.rec(6, st);
 
     // optional screen-error sampling (tensor-core screens): 64 tile pairs spread over the candidate list
@@ -673,7 +715,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     S_.screen_ops = (double)h.screen_ops;
     for (int c = 0; c < ncls; ++c) S_.screen_ops_issued += (double)h.class_items[c] * sops.per_item[c];
     if (i8 && !i8_high_limb_screen(g))   // the four-product screen: hl + lh and ll for the items that took them
-        S_.screen_ops_issued += 3.0 * (double)h.xl_items * sops.per_item[0];
+        S_.screen_ops_issued += 3.0 * (double)h.xl_items * 2.0 * kTileR * 128.0 * (double)C[0]->R.kpad;
     if (diag) {
         unsigned long long dv[3] = {0, 0, 0};
         TJ_CUDA(cudaMemcpyAsync(dv, diag_out.p, sizeof(dv), cudaMemcpyDeviceToHost, st));

@@ -1011,6 +1011,60 @@ __global__ void chunk_emit(const uint64_t* keys, size_t cap, const uint32_t* tot
     chunks[i] = make_uint4(I, b, e, 0);
 }
 
+// Half-tile masks for the one-SM tensor-core screen.  A candidate (R tile I, S tile J) of 128 x 256
+// rows is issued as two 128-column half-items; this tests each 128-row half of S tile J against R
+// tile I with cand_test's rigorous ball and box bounds (on the halves' own statistics) and stores the
+// live halves in bits 30-31 of the jlist entry.  The screen then issues and tests only live halves,
+// packing them densely into its MMA and epilogue pipeline; an entry whose halves are both dead is
+// skipped.  One block per R tile, threads over its candidate entries.
+__global__ void __launch_bounds__(256) half_mask_kernel(const uint32_t* cnt, const uint32_t* off, uint32_t* jlist,
+                                                        const uint4* rtiles, const JoinParams* jps,
+                                                        const HalfView* views, int self_join) {
+    extern __shared__ float hm_sm[];   // [3][d]: R tile centroid, low, high
+    const int I = blockIdx.x;
+    const uint4 rt = rtiles[I];
+    const HalfView v = views[rt.w];
+    const int d = v.d;
+    const int il = I - v.rbase;   // class-local R tile
+    for (int k = threadIdx.x; k < d; k += blockDim.x) {
+        hm_sm[k] = v.rctrT[(size_t)k * v.ntR + il];
+        hm_sm[d + k] = v.rloT[(size_t)k * v.ntR + il];
+        hm_sm[2 * d + k] = v.rhiT[(size_t)k * v.ntR + il];
+    }
+    __syncthreads();
+    const double Tp = jps[rt.z].Tp;
+    const float f = 1.f - (float)(d + 8) * 0x1p-23f;
+    const float rtp = (float)(sqrt(Tp) * (1.0 + 0x1p-20));
+    const float tpf = (float)(Tp * (1.0 + 0x1p-20));
+    const float ri = v.rrad[il];
+    const uint32_t e0 = off[I], e1 = e0 + cnt[I];
+    for (uint32_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const uint32_t J = jlist[e] & 0x3FFFFFFFu;
+        unsigned mask = 0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int hl = 2 * ((int)J - v.sbase) + h;   // class-local half tile
+            if (hl >= v.ntH || v.hnv[hl] == 0) continue;
+            if (self_join) {   // some sorted column of the half must exceed some sorted row of the tile
+                const long long maxcol = (long long)hl * 128 + 127;
+                if (maxcol <= (long long)il * 128) continue;
+            }
+            float ball = 0.f, box = 0.f;
+            for (int k = 0; k < d; ++k) {
+                const float dc = hm_sm[k] - v.hctrT[(size_t)k * v.ntH + hl];
+                ball = fmaf(dc, dc, ball);
+                const float gap = fmaxf(fmaxf(v.hloT[(size_t)k * v.ntH + hl] - hm_sm[2 * d + k],
+                                              hm_sm[d + k] - v.hhiT[(size_t)k * v.ntH + hl]), 0.f);
+                box = fmaf(gap, gap, box);
+            }
+            const float lb_box = box * f;
+            const float lb_ball = sqrtf(ball * f) * (1.f - 0x1p-20f) - ri - v.hrad[hl];
+            if (!(lb_box > tpf || lb_ball > rtp)) mask |= 1u << h;
+        }
+        jlist[e] = J | (mask << 30);
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ host entry points
@@ -1240,6 +1294,20 @@ void build_candidates(const TileSet& tr, const TileSet& ts, double Tp, bool self
     launch(chunk_emit, (unsigned)((cap + 255) / 256), 256, 0, st, keys.p, cap, c.dev_counts.p + 1, c.cnt.p, c.off.p,
                                                                chunk_items, c.chunks.p);
     TJ_CUDA(cudaGetLastError());
+}
+
+void half_masks(const std::vector<HalfView>& views, const Candidates& c, int ntR_total, const uint4* rtiles,
+                const JoinParams* jps, bool self_join, cudaStream_t st) {
+    if (ntR_total == 0 || views.empty()) return;
+    int dmax = 1;
+    for (const auto& v : views) dmax = std::max(dmax, v.d);
+    DBuf<HalfView> dv(views.size(), st);
+    upload(dv.p, views.data(), views.size() * sizeof(HalfView), st);
+    const size_t smem = (size_t)3 * dmax * sizeof(float);
+    if (smem > 48 * 1024)
+        TJ_CUDA(cudaFuncSetAttribute(half_mask_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    launch(half_mask_kernel, (unsigned)ntR_total, 256, smem, st, (const uint32_t*)c.cnt.p, (const uint32_t*)c.off.p,
+           c.jlist.p, rtiles, jps, (const HalfView*)dv.p, self_join ? 1 : 0);
 }
 
 void build_candidates_batched(const std::vector<CandClassView>& classes, const std::vector<CandBlock>& blocks,

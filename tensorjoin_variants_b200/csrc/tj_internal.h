@@ -214,6 +214,19 @@ void build_candidates_batched(const std::vector<CandClassView>& classes, const s
                               const std::vector<double>& Tp_per_block, int ntR_total, int words, int chunk_items,
                               const std::vector<uint32_t>& rtile_sbase, Candidates& c, cudaStream_t st);
 
+// Half-tile masks (one-SM tensor-core screen): R tile statistics and 128-row S half-tile statistics
+// of one class, class-local indices; ntH = 2 x the class's 256-row S tiles.
+struct HalfView {
+    const float *rctrT, *rloT, *rhiT, *rrad;
+    const float *hctrT, *hloT, *hhiT, *hrad;
+    const uint32_t* hnv;   // [ntH] rows of each half that are real points
+    int ntR, ntH, rbase, sbase, d, pad;
+};
+// Marks the live 128-row halves of every candidate's S tile in bits 30-31 of its jlist entry.
+void half_masks(const std::vector<HalfView>& views, const Candidates& c, int ntR_total, const uint4* rtiles,
+                const JoinParams* jps, bool self_join, cudaStream_t st);
+constexpr uint32_t kJMask = 0x3FFFFFFFu;   // jlist entry: S tile id in the low 30 bits
+
 // ------------------------------------------------------------------ screen / refine / emit
 struct EmitBuffers {
     uint64_t* acc = nullptr;   // accept keys
@@ -248,6 +261,9 @@ struct ScreenInput {
     long long T_int = 0;                // integer threshold (int8-limb screen, single join)
     bool allow_pair = true;             // the CTA-pair tensor-core screen may be used where it applies
     bool i8_four_products = false;      // int8-limb screen: all four limb products (exact in the kernel)
+    bool half_packed = false;           // jlist entries carry live-half masks (one-SM 16-bit screens)
+    int k_block = 0;                    // 16-bit screens: elements per k-block (16 / 32 / 64; 0: by d)
+    int stages = 0;                     // 16-bit screens: operand stages in flight (0: all compiled)
     mutable bool used_pair = false;     // set by screen_tc
     JoinParams jp0{};                   // host copy of join 0's parameters (single-join kernels)
     // screen-error diagnostics (tensor-core screens): sampled accumulators and the analysis result

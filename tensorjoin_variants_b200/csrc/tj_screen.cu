@@ -138,7 +138,8 @@ struct ScreenClassArgs {
     int kblocks;              // kpad / kbk
     int kpad;                 // operand row length (16, 32 or a multiple of 64 elements)
     int kbk;                  // elements per k-block: 16, 32 or 64 (32-, 64- or 128-byte swizzle)
-    unsigned tx_bytes;        // bytes one stage receives for this class
+    unsigned tx_bytes;        // bytes one stage receives for this class (CTA pair)
+    unsigned tx_a, tx_h;      // one SM: bytes of a stage's A part and of one 128-row B half (with the split)
     uint32_t desc_hi;         // upper half of the UMMA shared-memory descriptors
 };
 
@@ -177,6 +178,8 @@ struct ScreenArgs {
     unsigned long long* join_t;
     unsigned long long* cta_t;
     unsigned njoins;
+    int nstages;                  // operand stages in the ring (<= the compiled count; a tuning knob)
+    int half;                     // one SM: jlist entries carry live-half masks in bits 30-31
 };
 
 // One SM: the producer publishes the chunks it takes from the queue in a ring of kChunkRing slots;
@@ -289,7 +292,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         }
         for (int m = 0; m < kMetaSlots; ++m) {
             mbar_init(&ctl->meta_full[m], 1);
-            mbar_init(&ctl->meta_empty[m], kPair ? kEpiWarps : 8);   // one SM: the two groups of an item
+            mbar_init(&ctl->meta_empty[m], kEpiWarps);   // every epilogue warp passes every item
         }
         mbar_init(&ctl->drain, 1);
         for (int r = 0; r < kChunkRing; ++r) {
@@ -313,6 +316,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
     tc_fence_after();
     const unsigned tmem = ctl->tmem_base;
     const unsigned nchunks = kPair ? a.nT * ((a.ntS + 63u) / 64u) : *a.nchunks;
+    const int nst = (a.nstages >= 2 && a.nstages <= kStages) ? a.nstages : kStages;
     const unsigned cfirst = kPair ? (blockIdx.x >> 1) : blockIdx.x;
     const unsigned cstride = kPair ? (gridDim.x >> 1) : gridDim.x;
     if (a.cta_t && threadIdx.x == 0) a.cta_t[2 * blockIdx.x] = global_ns();
@@ -344,8 +348,14 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 const unsigned tx = a.cls[cls].tx_bytes;
                 const CUtensorMap* mA = &tm.a[cls];
                 const CUtensorMap* mB = &tm.b[cls];
-                for (unsigned e = e0; e < e1 && ok; ++e, ++n) {
-                    const unsigned J = kPair ? e : a.jlist[e];
+                for (unsigned e = e0; e < e1 && ok; ++e) {
+                    unsigned J = e, hm = 3u;   // one SM: live 128-row halves of the S tile
+                    if (!kPair) {
+                        const uint32_t je = a.jlist[e];
+                        J = je & kJMask;
+                        if (a.half) hm = je >> 30;
+                        if (!hm) continue;
+                    }
                     const int srow = (int)a.stiles[J].x + (int)(rank * kTileR);   // pair: this CTA's half
                     const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
                     if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status, a.wait_ns)) { ok = false; break; }
@@ -369,24 +379,31 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                             }
                             tma_load_2d_pair(sa, mA, fb, kb * kbk, rrow);
                             tma_load_2d_pair(sa + Cfg::kBhi, mB, fb, kb * kbk, srow);
-                        } else {
-                            mbar_arrive_expect_tx(&ctl->full[stage], tx);
+                        } else {   // A, then each live 128-row half of B (hi, and lo with the split)
+                            const unsigned bhalf = 256u * (unsigned)kbk;
+                            mbar_arrive_expect_tx(&ctl->full[stage],
+                                                  a.cls[cls].tx_a + (unsigned)__popc(hm) * a.cls[cls].tx_h);
                             tma_load_2d(sa, mA, &ctl->full[stage], kb * kbk, rrow);
-                            tma_load_2d(sa + Cfg::kBhi, mB, &ctl->full[stage], kb * kbk, srow);
+                            if (kSplit) tma_load_2d(sa + Cfg::kAlo, mA, &ctl->full[stage], kpad + kb * kbk, rrow);
+#pragma unroll
+                            for (int h = 0; h < 2; ++h) {
+                                if (!((hm >> h) & 1u)) continue;
+                                tma_load_2d(sa + Cfg::kBhi + h * bhalf, mB, &ctl->full[stage], kb * kbk, srow + h * 128);
+                                if (kSplit)
+                                    tma_load_2d(sa + Cfg::kBlo + h * bhalf, mB, &ctl->full[stage], kpad + kb * kbk,
+                                                srow + h * 128);
+                            }
                         }
-                        if (kSplit) {
-                            tma_load_2d(sa + Cfg::kAlo, mA, &ctl->full[stage], kpad + kb * kbk, rrow);
-                            tma_load_2d(sa + Cfg::kBlo, mB, &ctl->full[stage], kpad + kb * kbk, srow);
-                        }
-                        if (++stage == kStages) { stage = 0; phase ^= 1; }
+                        if (++stage == nst) { stage = 0; phase ^= 1; }
                     }
+                    ++n;
                 }
             }
             if (!ok) ctl->abort_flag = 1;
             // drain: the last copy issued into every stage / metadata slot must land before exit (in
             // the pair the MMA CTA's barriers count both CTAs' copies and CTA 1 copies only into phases
             // CTA 0 armed, so CTA 0's drain covers them; the final cluster barrier follows it)
-            for (int s = 0; s < kStages && rank == 0; ++s) {
+            for (int s = 0; s < nst && rank == 0; ++s) {
                 const unsigned ph = ((unsigned)s < stage) ? phase : (phase ^ 1u);
                 mbar_wait(&ctl->full[s], ph, status, kDrainLimitNs);
             }
@@ -401,6 +418,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         if (lane == 0 && rank == 0) {
             unsigned stage = 0, phase = 0, acc = 0, acc_phase = 0;
             unsigned long long n_mma = 0;   // items issued
+            unsigned ns = 0;                // one SM: half-items issued
             bool ok = true;
             for (unsigned long long qc = 0;; ++qc) {
                 unsigned c;
@@ -418,22 +436,31 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 const ScreenClassArgs& ca = a.cls[rt.w];
                 const int kblocks = ca.kblocks, ksteps = ca.kbk / 16;
                 const uint32_t dh = ca.desc_hi;
-                for (unsigned e = e0; e < e1 && ok; ++e, ++n_mma) {
-                    // one SM: item n fills accumulators 2n mod 4 and 2n+1 mod 4 (its two 128-column halves)
-                    const unsigned b0 = kPair ? acc : (unsigned)((2 * n_mma) & 3), b1 = (b0 + 1) & 3;
-                    bool got;
+                for (unsigned e = e0; e < e1 && ok; ++e) {
+                    unsigned hm = 3u;   // one SM: live 128-row halves of the item's S tile
+                    if (!kPair && a.half) {
+                        hm = a.jlist[e] >> 30;
+                        if (!hm) continue;
+                    }
+                    // one SM: live half h takes the next half-item s = ns, ns + 1, ... (accumulator s mod 4)
+                    unsigned bh[2] = {0u, 0u};
+                    bool got = true;
                     if (kPair) {
                         got = mbar_wait_cluster(&ctl->acc_empty[acc], acc_phase ^ 1, status, a.wait_ns);
                     } else {
-                        got = mbar_wait(&ctl->acc_empty[b0], (unsigned)(((2 * n_mma) >> 2) & 1) ^ 1u, status,
-                                        a.wait_ns) &&
-                              mbar_wait(&ctl->acc_empty[b1], (unsigned)(((2 * n_mma + 1) >> 2) & 1) ^ 1u, status,
-                                        a.wait_ns);
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            if (!((hm >> h) & 1u)) continue;
+                            bh[h] = (unsigned)(ns & 3);
+                            got = got && mbar_wait(&ctl->acc_empty[bh[h]], (unsigned)((ns >> 2) & 1) ^ 1u, status,
+                                                   a.wait_ns);
+                            ++ns;
+                        }
                     }
                     if (!got) { ok = false; break; }
                     tc_fence_after();
                     const unsigned d_tmem = tmem + acc * kTileS;                 // pair: 256 columns
-                    const unsigned d0 = tmem + b0 * 128u, d1 = tmem + b1 * 128u;  // one SM: 2 x 128
+                    const unsigned d0 = tmem + bh[0] * 128u, d1 = tmem + bh[1] * 128u;   // one SM: 2 x 128
                     const unsigned bhalf = 256u * (unsigned)ca.kbk;              // bytes of 128 B rows
                     for (int kb = 0; kb < kblocks; ++kb) {
                         if (!mbar_wait(&ctl->full[stage], phase, status, a.wait_ns)) { ok = false; break; }
@@ -450,6 +477,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                             } else {
 #pragma unroll
                                 for (int h = 0; h < 2; ++h) {
+                                    if (!((hm >> h) & 1u)) continue;
                                     const unsigned dd = h ? d1 : d0;
                                     const uint64_t bd = desc_kmajor(sa + Cfg::kBhi + h * bhalf, k * 32, dh);
                                     umma_f16(dd, ad, bd, a.idesc, accum);
@@ -463,16 +491,17 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         }
                         if (kPair) umma_commit_pair_mc(&ctl->empty[stage], 0x3);   // frees the stage in both CTAs
                         else umma_commit(&ctl->empty[stage]);
-                        if (++stage == kStages) { stage = 0; phase ^= 1; }
+                        if (++stage == nst) { stage = 0; phase ^= 1; }
                     }
                     if (!ok) break;
                     if (kPair) {
                         umma_commit_pair_mc(&ctl->acc_full[acc], 0x3);   // both CTAs' epilogues
                         if (++acc == 2) { acc = 0; acc_phase ^= 1; }
                     } else {
-                        umma_commit(&ctl->acc_full[b0]);
-                        umma_commit(&ctl->acc_full[b1]);
+                        if (hm & 1u) umma_commit(&ctl->acc_full[bh[0]]);
+                        if (hm & 2u) umma_commit(&ctl->acc_full[bh[1]]);
                     }
+                    ++n_mma;
                 }
             }
             if (!kPair && n_mma) atomicAdd(&a.ctr->items, n_mma);
@@ -493,7 +522,8 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         const int cb_end = kPair ? (part == 2 ? kTileS / 32 : (int)part * 3 + 3) : 4;
         WarpAppender app_acc, app_band;
         unsigned acc = 0, acc_phase = 0;
-        unsigned long long n = 0, n_screen_acc = 0, n_rare = 0, n_items = 0;
+        unsigned long long n_screen_acc = 0, n_rare = 0, n_items = 0;
+        unsigned n = 0, ns = 0;   // items, and (one SM) half-items passed: the UMMA issuer's numbering
         bool ok = true;
         for (unsigned long long qc = 0;; ++qc) {
             unsigned c;
@@ -519,20 +549,31 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             const float Ei = rvalid ? ca.r_en[rs] : 0.f;
             const float Zli = rvalid ? ca.r_zl[rs] : 0.f;
             const uint32_t oi = rvalid ? ca.r_emit[rs] : 0u;
-            for (unsigned e = e0; e < e1 && ok; ++e, ++n) {
+            for (unsigned e = e0; e < e1 && ok; ++e) {
+              unsigned hm = 3u;   // one SM: live 128-row halves of the item's S tile
+              if (!kPair && a.half) {
+                  hm = a.jlist[e] >> 30;
+                  if (!hm) continue;
+              }
+              // every epilogue warp passes every item's metadata slot (and releases it), also when its
+              // group takes none of the item's half-items
+              const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
+              if (!__all_sync(0xffffffffu, mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns))) {
+                  ok = false;
+                  break;
+              }
               for (unsigned h = 0; h < (kPair ? 1u : 2u); ++h) {
                 unsigned colbase = 0, b = acc, bph = acc_phase;
-                if (!kPair) {
-                    const unsigned long long sub = 2 * n + h;
+                if (!kPair) {   // live half h is half-item ns: group ns mod 3, accumulator ns mod 4
+                    if (!((hm >> h) & 1u)) continue;
+                    const unsigned sub = ns++;
                     if ((unsigned)(sub % 3) != part) continue;
                     colbase = h * 128u;
                     b = (unsigned)(sub & 3);
                     bph = (unsigned)((sub >> 2) & 1);
                 }
-                const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
                 {   // warp-uniform: the TMEM loads below are warp-collective
-                    const bool got = mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns) &&
-                                     mbar_wait(&ctl->acc_full[b], bph, status, a.wait_ns);
+                    const bool got = mbar_wait(&ctl->acc_full[b], bph, status, a.wait_ns);
                     if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
                 }
                 tc_fence_after();
@@ -573,7 +614,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         float* out = a.dump + (slotd * kTileR + row) * kTileS + col0;
 #pragma unroll
                         for (int k = 0; k < 32; ++k) out[k] = __uint_as_float(raw[k]);
-                        if (row == 0 && col0 == 0) a.dump_ids[slotd] = make_uint4(rtile, a.jlist[e], 1u, 0u);
+                        if (row == 0 && col0 == 0) a.dump_ids[slotd] = make_uint4(rtile, a.jlist[e] & kJMask, 1u, 0u);
                     }
                     if (cb == cb_end - 1) {   // this warp's part read: hand it back
                         tc_fence_before();
@@ -686,11 +727,12 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         }
                     }
                 }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&ctl->meta_empty[slot]);   // this warp is done with the slot
                 ++n_items;
                 if (kPair && ++acc == 2) { acc = 0; acc_phase ^= 1; }
               }
+              __syncwarp();
+              if (lane == 0) mbar_arrive(&ctl->meta_empty[slot]);   // this warp is done with the slot
+              ++n;
             }
             if (a.join_t && lane == 0) atomicMax(&a.join_t[a.njoins + rt.z], global_ns());
         }
@@ -840,10 +882,11 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
         if (!ok) fail(-1, "screen_tc needs matching bf16 / fp16 operands on both sides of every class");
         const CUtensorMapDataType dt = bf ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
         const long long w = (long long)R.kpad * (split ? 2 : 1);
-        const int kbk = std::min(R.kpad, kBK);
+        int kbk = std::min(R.kpad, kBK);
+        if (g.k_block && g.k_block < kbk && R.kpad % g.k_block == 0) kbk = g.k_block;   // tuning knob
         if (kbk != 16 && kbk != 32 && kbk != 64) fail(-1, "screen_tc: operand width");
         make_tmap_2d(&tm.a[c], R.op.p, R.rows_pad, w, 2, kTileR, dt, 2 * kbk);
-        make_tmap_2d(&tm.b[c], S.op.p, S.rows_pad, w, 2, pair ? kTileR : kTileS, dt, 2 * kbk);
+        make_tmap_2d(&tm.b[c], S.op.p, S.rows_pad, w, 2, kTileR, dt, 2 * kbk);   // 128-row boxes (halves)
         const TileSet& tS = *g.tS[c];
         if (tS.ntiles > 0)
             launch(build_col_meta, tS.ntiles, kTileS, 0, st, tS.row0.p, tS.nvalid.p, S.emit, S.nrm2.p, S.nrm2f.p,
@@ -857,8 +900,9 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
         a.cls[c].kblocks = R.kpad / kbk;
         a.cls[c].kpad = R.kpad;
         a.cls[c].kbk = kbk;
-        a.cls[c].tx_bytes = pair ? (unsigned)(2 * kTileR * kbk * 2)   // this CTA's A rows + B half
-                                 : (unsigned)((split ? 2 : 1) * (kTileR + kTileS) * kbk * 2);
+        a.cls[c].tx_bytes = (unsigned)(2 * kTileR * kbk * 2);   // CTA pair: this CTA's A rows + B half
+        a.cls[c].tx_a = (unsigned)((split ? 2 : 1) * kTileR * kbk * 2);
+        a.cls[c].tx_h = (unsigned)((split ? 2 : 1) * 128 * kbk * 2);
         a.cls[c].desc_hi = desc_hi_for_rows(2u * (unsigned)kbk);
     }
     a.chunks = g.cand->chunks.p;
@@ -886,6 +930,8 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     a.wait_ns = pipeline_wait_ns();
     a.join_t = g.join_t;
     a.cta_t = g.cta_t;
+    a.nstages = g.stages;
+    a.half = g.half_packed ? 1 : 0;
     a.njoins = (unsigned)g.njoins;
     TJ_CUDA(cudaMemsetAsync(&eb.ctr->chunk_next, 0, sizeof(unsigned long long), st));
     const int grid = num_sms();

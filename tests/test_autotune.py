@@ -8,18 +8,46 @@ import pytest
 from tensorjoin_variants_b200 import autotune as A
 
 
-def test_candidates_cover_only_what_applies():
-    c512 = A.candidates(512, "fp16", "rs")
-    assert {c.cta_pair for c in c512} == {True, False}
-    assert {c.index_frame for c in c512} == {"auto"}            # d > 128: no principal-direction cells
-    assert {c.band_fp32 for c in c512} == {False, True}
-    assert {c.chunk_items for c in c512} == set(A.CHUNK_ITEMS)
-    c64 = A.candidates(64, "bf16x3", "upper")
-    assert {c.cta_pair for c in c64} == {True}                  # self-join / d < 256: one-SM screen only
-    assert {c.index_frame for c in c64} == {"axes", "pca"}
-    ci = A.candidates(128, "int8limb", "upper")
-    assert {c.band_fp32 for c in ci} == {False}                 # exact screen: no band
-    assert len(set(c512)) == len(c512)
+def test_dimensions_cover_only_what_applies():
+    d512 = dict(A.dimensions(512, "fp16", "rs"))
+    assert d512["cta_pair"] == [True, False]                    # BM x BN: CTA pair or one SM
+    assert d512["k_block"] == [0, 32, 16] and d512["stages"] == [0, 3, 2]
+    assert "index_frame" not in d512                            # d > 128: no principal-direction cells
+    assert d512["band_fp32"] == [False, True]
+    assert set(d512["chunk_items"]) == {0, 16, 256}
+    d64 = dict(A.dimensions(64, "bf16x3", "upper"))
+    assert "cta_pair" not in d64                                # self-join / d < 256: one-SM screen only
+    assert d64["index_frame"] == ["axes", "pca"]
+    d8 = dict(A.dimensions(8, "bf16", "rs"))
+    assert "k_block" not in d8                                  # a 16-element row has one k-block size
+    di = dict(A.dimensions(128, "int8limb", "upper"))
+    assert di["i8_four_products"] == [False, True]              # limb count of the int14 screen
+    assert "band_fp32" not in di and "k_block" not in di
+    assert "i8_four_products" not in dict(A.dimensions(300, "int8limb", "upper"))   # rows > 256: four products
+    da = dict(A.dimensions(64, "auto", "rs"))
+    assert da["screen"] == list(A.FLOAT_SCREENS)                # operand format chosen by the tuner
+    c = A.candidates(64, "bf16x3", "rs")
+    assert c[0] == A.Choice() and len(set(c)) == len(c)
+
+
+def test_coordinate_search_keeps_each_dimensions_best():
+    """Each dimension's best is kept while the next one is searched; interactions add up."""
+    def runner(ch):
+        ms = 10.0 - (2.0 if ch.chunk_items == 256 else 0.0) - (1.5 if ch.index_frame == "pca" else 0.0)
+        ms -= 0.5 if ch.stages == 3 else 0.0
+        return ms, 77
+    best, timings, count = A.Tuner.search(64, "bf16x3", "rs", runner, reps=1)
+    assert (best.chunk_items, best.index_frame, best.stages) == (256, "pca", 3)
+    assert count == 77 and min(timings.values()) == 6.0
+
+
+def test_search_skips_choices_that_cannot_run():
+    def runner(ch):
+        if ch.screen.startswith("fp16"):
+            return None                                         # e.g. FP16 range exceeded
+        return (1.0 if ch.screen == "bf16" else 2.0), 5
+    best, _, _ = A.Tuner.search(64, "auto", "rs", runner, reps=1)
+    assert best.screen == "bf16"
 
 
 def test_tune_key_buckets():
@@ -56,7 +84,8 @@ def test_pick_rejects_a_choice_that_changes_the_pairs():
 def test_table_persists(tmp_path):
     path = str(tmp_path / "tune.json")
     t = A.Tuner(path)
-    choice = A.Choice(cta_pair=False, chunk_items=256, index_frame="pca", band_fp32=True)
+    choice = A.Choice(screen="fp16", cta_pair=False, k_block=32, stages=3, chunk_items=256, index_frame="pca",
+                      band_fp32=True)
     t.record("d64/f32/bf16/rs/space2^30/sel2^3", choice, {"x": 1.5})
     again = A.Tuner(path)
     assert again.lookup("d64/f32/bf16/rs/space2^30/sel2^3") == choice
@@ -105,7 +134,7 @@ def test_tuner_join_flow_with_a_fake_library(monkeypatch, tmp_path):
         def __init__(self, R, S, kw):
             rows = R.shape[0]
             self.count = rows * 12                                   # 12 result pairs per row
-            ms = 5.0 if kw.get("chunk_items") == 256 and kw.get("index_frame") == "pca" else 9.0
+            ms = 9.0 - (2.0 if kw.get("chunk_items") == 256 else 0.0) - (2.0 if kw.get("index_frame") == "pca" else 0.0)
             self.stats = {"ms_total": ms, "result_pairs": self.count}
 
     def fake_join_result(R, S, eps2=None, mode="rs", screen="bf16", **kw):
@@ -121,8 +150,9 @@ def test_tuner_join_flow_with_a_fake_library(monkeypatch, tmp_path):
     final_kw = calls[-1][1]
     assert calls[-1][0] == 50000 and final_kw["chunk_items"] == 256 and final_kw["index_frame"] == "pca"
     n_first = len(calls)
-    assert n_first == 1 + 2 * len(A.candidates(64, "bf16x3", "rs")) + 1   # probe, tuning, join
+    n_search = sum(len(v) for _, v in A.dimensions(64, "bf16x3", "rs"))
+    assert n_first == 1 + 2 * n_search + 1                                # probe, tuning (2 reps), join
     tuner.join(R, S, eps2=0.1, screen="bf16x3", sample_rows=1024)
     assert len(calls) == n_first + 2                                      # probe and join only
     key = A.tune_key(64, "f32", "bf16x3", "rs", 50000, 60000, 12.0)
-    assert tuner.lookup(key) == A.Choice(True, 256, "pca", False)
+    assert tuner.lookup(key) == A.Choice(chunk_items=256, index_frame="pca")

@@ -229,3 +229,43 @@ def test_accumulation_premise(screen):
           f"max |d2hat - d2| = {st['screen_max_abs_err']:.3e}")
     assert ratio < 1.0, st
     assert np.array_equal(_np(res.keys()), oracle.join_f32(R, S, T, "rs"))
+
+
+# ---------------------------------------------------------------- half-tile packing and tile-shape knobs
+@pytest.mark.parametrize("screen", ["bf16x3", "fp16", "bf16"])
+def test_half_packing_same_pairs_fewer_evaluations(screen):
+    """Dropping dead 128-row halves of candidate tile pairs (the default) gives the oracle's pairs with
+    no more distance evaluations than screening whole tile pairs; the tile-shape knobs (k-block,
+    stages) give the same pairs too."""
+    R, S, T, mode = case("mixture64")
+    want = oracle.join_f32(R, S, T, mode)
+    packed = _join(R, S, T, mode, screen)
+    whole = _join(R, S, T, mode, screen, half_pack=False)
+    assert np.array_equal(_np(packed.keys()), want)
+    assert np.array_equal(_np(whole.keys()), want)
+    assert packed.stats["pairs_screened"] <= whole.stats["pairs_screened"]
+    assert packed.stats["screen_ops_issued"] <= whole.stats["screen_ops_issued"]
+    for kb, stg in ((32, 0), (16, 3), (0, 2)):
+        r = _join(R, S, T, mode, screen, k_block=kb, stages=stg)
+        assert np.array_equal(_np(r.keys()), want), (kb, stg)
+
+
+def test_half_packing_self_join_and_batched():
+    R, S, T, mode = case("uniform16")
+    want = oracle.join_f32(R, None, T, "upper")
+    for hp in (True, False):
+        assert np.array_equal(_np(_join(R, None, T, "upper", "bf16x3", half_pack=hp).keys()), want)
+    rng = np.random.default_rng(78)
+    joins = []
+    for k in range(20):
+        d = (8, 32, 128)[k % 3]
+        c = rng.random((8, d))
+        Rk = (c[rng.integers(0, 8, 700)] + rng.standard_normal((700, d)) * 0.05).astype(np.float32)
+        Sk = (c[rng.integers(0, 8, 1900)] + rng.standard_normal((1900, d)) * 0.05).astype(np.float32)
+        joins.append((Rk, Sk, W.ragged_eps2(1900, d, 8, 0.05, 16)))
+    dev = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(), float(np.sqrt(t))) for a, b, t in joins]
+    for hp in (True, False):
+        out = tj.join_batched(dev, screen="bf16x3", half_pack=hp, guards=True)
+        for (Rk, Sk, t), (i, j), (_, _, e) in zip(joins, out, dev):
+            got = i.cpu().numpy().astype(np.uint64) * np.uint64(Sk.shape[0]) + j.cpu().numpy().astype(np.uint64)
+            assert np.array_equal(got, oracle.join_f32(Rk, Sk, e * e, "rs"))
