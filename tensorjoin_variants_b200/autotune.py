@@ -5,6 +5,7 @@ What it chooses, per workload (every choice gives the same pair set; only the ti
 * ``screen``       -- the screen's operand format when the caller asks for ``screen="auto"``:
                       BF16 or FP16, single or hi/lo-split (x3) operands;
 * ``cta_pair``     -- BM x BN: 256 x 256 tiles on a CTA pair (cta_group::2) or 128 x 256 on one SM;
+* ``half_pack``    -- one SM: 128 x 128 half-items with dead halves dropped, or whole 128 x 256 items;
 * ``k_block``      -- BK: elements of K per pipeline stage (64, 32 or 16);
 * ``stages``       -- operand stages in flight (2 up to the compiled count);
 * ``i8_four_products`` -- limb count of the int14 screen: the high-limb product only (undecided
@@ -50,6 +51,7 @@ FLOAT_SCREENS = ("bf16x3", "fp16x3", "bf16", "fp16")
 class Choice:
     screen: str = ""              # "": the screen the caller asked for
     cta_pair: bool = True
+    half_pack: bool = True        # one-SM screen: dead 128-row halves of candidate tile pairs dropped
     k_block: int = 0              # 0: by d (64 for rows of more than 32 elements)
     stages: int = 0               # 0: every compiled stage
     i8_four_products: bool = False
@@ -60,7 +62,7 @@ class Choice:
     def kwargs(self) -> dict:
         kw = dict(cta_pair=self.cta_pair, chunk_items=self.chunk_items, index_frame=self.index_frame,
                   band_fp32=self.band_fp32, k_block=self.k_block, stages=self.stages,
-                  i8_four_products=self.i8_four_products)
+                  i8_four_products=self.i8_four_products, half_pack=self.half_pack)
         return kw
 
     def screen_for(self, requested: str) -> str:
@@ -80,6 +82,8 @@ def dimensions(d: int, screen: str, mode: str) -> list[tuple[str, list]]:
     float_screen = screen != "int8limb" and screen != "plain"
     if float_screen and mode == "rs" and d >= 256:
         dims.append(("cta_pair", [True, False]))
+    if float_screen:
+        dims.append(("half_pack", [True, False]))
     if screen == "int8limb" and kpad <= 256:
         dims.append(("i8_four_products", [False, True]))
     if float_screen:
