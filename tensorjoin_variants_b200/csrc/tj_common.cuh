@@ -124,6 +124,10 @@ TJ_DEV void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
 TJ_DEV void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
 }
+// `count` arrivals at once
+TJ_DEV void mbar_arrive_cnt(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
 TJ_DEV bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     unsigned ok;
     asm volatile(

@@ -92,7 +92,6 @@ template <int kStages>
 struct ScreenCtl {
     uint64_t full[kStages];
     uint64_t empty[kStages];
-    uint64_t armed[kStages];   // CTA pair, in CTA 1: CTA 0 has armed this stage's phase of its full barrier
     uint64_t acc_full[kAccMax];
     uint64_t acc_empty[kAccMax];
     uint64_t meta_full[kMetaSlots];
@@ -283,7 +282,6 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         for (int s = 0; s < kStages; ++s) {
             mbar_init(&ctl->full[s], 1);
             mbar_init(&ctl->empty[s], 1);
-            mbar_init(&ctl->armed[s], 1);
         }
         for (int b = 0; b < kAccMax; ++b) {
             mbar_init(&ctl->acc_full[b], 1);
@@ -292,7 +290,9 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         }
         for (int m = 0; m < kMetaSlots; ++m) {
             mbar_init(&ctl->meta_full[m], 1);
-            mbar_init(&ctl->meta_empty[m], kEpiWarps);   // every epilogue warp passes every item
+            // pair: the 12 epilogue warps; one SM: the 8 warps of the item's two half-items (4 warps
+            // arriving twice where only one half is live)
+            mbar_init(&ctl->meta_empty[m], kPair ? kEpiWarps : 8);
         }
         mbar_init(&ctl->drain, 1);
         for (int r = 0; r < kChunkRing; ++r) {
@@ -366,17 +366,8 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         uint8_t* sa = smem + (size_t)stage * kStageBytes;
                         if (kPair) {   // both CTAs' copies complete on the MMA CTA's barrier
-                            // CTA 1 copies only into phases CTA 0 has armed (CTA 0 tells it through CTA 1's
-                            // `armed` barrier), so every copy of the pair lands in a phase CTA 0 waits for
-                            // before the pair exits, also when one CTA gives up early
                             const unsigned fb = mapa_shared(&ctl->full[stage], 0);
-                            if (rank == 0) {
-                                mbar_arrive_expect_tx(&ctl->full[stage], 2 * tx);
-                                mbar_arrive_cluster(mapa_shared(&ctl->armed[stage], 1));
-                            } else if (!mbar_wait(&ctl->armed[stage], phase, status, a.wait_ns)) {
-                                ok = false;
-                                break;
-                            }
+                            if (rank == 0) mbar_arrive_expect_tx(&ctl->full[stage], 2 * tx);
                             tma_load_2d_pair(sa, mA, fb, kb * kbk, rrow);
                             tma_load_2d_pair(sa + Cfg::kBhi, mB, fb, kb * kbk, srow);
                         } else {   // A, then each live 128-row half of B (hi, and lo with the split)
@@ -400,12 +391,16 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 }
             }
             if (!ok) ctl->abort_flag = 1;
-            // drain: the last copy issued into every stage / metadata slot must land before exit (in
-            // the pair the MMA CTA's barriers count both CTAs' copies and CTA 1 copies only into phases
-            // CTA 0 armed, so CTA 0's drain covers them; the final cluster barrier follows it)
-            for (int s = 0; s < nst && rank == 0; ++s) {
+            // drain: the last copy issued into every stage / metadata slot must land before exit.  In
+            // the pair the stage barriers live in CTA 0 and count both CTAs' copies: CTA 0 waits for
+            // the phases it armed, and CTA 1, which cannot see them, waits for its own stages to be
+            // released by the pair's MMA (its `empty` barriers, signalled after the MMA that read
+            // the copy); where the MMA stopped early these waits run out after kDrainLimitNs each,
+            // long after any copy issued has landed.  The final cluster barrier follows both.
+            for (int s = 0; s < nst; ++s) {
                 const unsigned ph = ((unsigned)s < stage) ? phase : (phase ^ 1u);
-                mbar_wait(&ctl->full[s], ph, status, kDrainLimitNs);
+                if (rank == 0) mbar_wait(&ctl->full[s], ph, status, kDrainLimitNs);
+                else if (n > 0) mbar_wait(&ctl->empty[s], ph, status, kDrainLimitNs);
             }
             for (int s = 0; s < kMetaSlots; ++s) {
                 if (n <= (unsigned long long)s) continue;
@@ -555,13 +550,10 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                   hm = a.jlist[e] >> 30;
                   if (!hm) continue;
               }
-              // every epilogue warp passes every item's metadata slot (and releases it), also when its
-              // group takes none of the item's half-items
+              // the item's metadata slot is read and released only by the warps whose group takes one
+              // of its half-items (consecutive half-items go to different groups)
               const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
-              if (!__all_sync(0xffffffffu, mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns))) {
-                  ok = false;
-                  break;
-              }
+              const unsigned meta_arrivals = (!kPair && __popc(hm) == 1) ? 2u : 1u;
               for (unsigned h = 0; h < (kPair ? 1u : 2u); ++h) {
                 unsigned colbase = 0, b = acc, bph = acc_phase;
                 if (!kPair) {   // live half h is half-item ns: group ns mod 3, accumulator ns mod 4
@@ -573,7 +565,8 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     bph = (unsigned)((sub >> 2) & 1);
                 }
                 {   // warp-uniform: the TMEM loads below are warp-collective
-                    const bool got = mbar_wait(&ctl->acc_full[b], bph, status, a.wait_ns);
+                    const bool got = mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns) &&
+                                     mbar_wait(&ctl->acc_full[b], bph, status, a.wait_ns);
                     if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
                 }
                 tc_fence_after();
@@ -727,11 +720,11 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         }
                     }
                 }
+                __syncwarp();
+                if (lane == 0) mbar_arrive_cnt(&ctl->meta_empty[slot], meta_arrivals);   // done with the slot
                 ++n_items;
                 if (kPair && ++acc == 2) { acc = 0; acc_phase ^= 1; }
               }
-              __syncwarp();
-              if (lane == 0) mbar_arrive(&ctl->meta_empty[slot]);   // this warp is done with the slot
               ++n;
             }
             if (a.join_t && lane == 0) atomicMax(&a.join_t[a.njoins + rt.z], global_ns());
@@ -744,11 +737,15 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             n_screen_acc += __shfl_xor_sync(0xffffffffu, n_screen_acc, o);
             n_rare += __shfl_xor_sync(0xffffffffu, n_rare, o);
         }
-        if (lane == 0) {
-            if (app_acc.valid) atomicAdd(&a.ctr->acc_valid, app_acc.valid);
-            if (app_band.valid) atomicAdd(&a.ctr->band_valid, app_band.valid);
-            if (n_screen_acc) atomicAdd(&a.ctr->screen_accept, n_screen_acc);
-            if (n_rare) atomicAdd(&a.ctr->rare_checks, n_rare);
+        if (lane == 0) {   // the screen's accepts and band pairs are exactly what the appenders wrote
+            if (n_screen_acc) {
+                atomicAdd(&a.ctr->acc_valid, n_screen_acc);
+                atomicAdd(&a.ctr->screen_accept, n_screen_acc);
+            }
+            if (n_rare) {
+                atomicAdd(&a.ctr->band_valid, n_rare);
+                atomicAdd(&a.ctr->rare_checks, n_rare);
+            }
             if (kPair && warp == kEpiFirst && n_items) atomicAdd(&a.ctr->items, n_items);
         }
     }

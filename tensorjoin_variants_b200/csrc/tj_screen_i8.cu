@@ -498,12 +498,15 @@ __global__ void __launch_bounds__(kI8Threads, 1)
 // integer refinement decides them from the int16 rows.  Only the h limbs are loaded, and the R
 // tile's limbs stay resident in shared memory for all items of a chunk (only S tiles stream), so an
 // item costs 16 KB of L2 traffic and kpad / 32 MMAs.
-// Warp roles (384 threads): warp 0 TMA producer, warp 1 TMEM allocator + UMMA issuer, warps 2-3
-// idle, warps 4..11 epilogue (warp w reads TMEM lanes 32 (w % 4).. and columns 64 ((w - 4) / 4)..).
+// Warp roles (512 threads): warp 0 TMA producer, warp 1 TMEM allocator + UMMA issuer, warps 2-3
+// idle, warps 4..15 epilogue in three groups of four that take alternate items (warp w reads TMEM
+// lanes 32 (w % 4).., all 128 columns in two passes of 64), so three warps per SM sub-partition
+// overlap their items' latency.
 constexpr int kHHStages = 6;                      // S k-blocks in flight (16 KB each)
 constexpr int kHHMaxKb = 2;                       // resident R k-blocks (kpad <= 256)
 constexpr int kHHAcc = 4;                         // TMEM accumulators of 128 columns
-constexpr int kHHEpi = 8;
+constexpr int kHHEpi = 12;                        // three groups of four warps, taking alternate items
+constexpr int kHHGroups = kHHEpi / 4;
 constexpr int kHHEpiFirst = 4;
 constexpr int kHHThreads = (kHHEpiFirst + kHHEpi) * 32;
 constexpr unsigned kHHABytes = kHHMaxKb * kPart;  // one resident R tile
@@ -556,11 +559,11 @@ __global__ void __launch_bounds__(kHHThreads, 1)
         }
         for (int b = 0; b < kHHAcc; ++b) {
             mbar_init(&ctl->acc_full[b], 1);
-            mbar_init(&ctl->acc_empty[b], kHHEpi);
+            mbar_init(&ctl->acc_empty[b], 4);   // the four warps of the item's epilogue group
         }
         for (int m = 0; m < kI8Meta; ++m) {
             mbar_init(&ctl->meta_full[m], 1);
-            mbar_init(&ctl->meta_empty[m], kHHEpi);
+            mbar_init(&ctl->meta_empty[m], 4);
         }
         mbar_init(&ctl->drain, 1);
         ctl->abort_flag = 0;
@@ -664,9 +667,8 @@ __global__ void __launch_bounds__(kHHThreads, 1)
         }
     } else if (warp >= kHHEpiFirst) {
         // ------------------------------------------------------------ epilogue
-        const unsigned ew = warp - kHHEpiFirst;        // 0..7
+        const unsigned group = (warp - kHHEpiFirst) >> 2;   // item n goes to group n mod 3
         const unsigned q = warp & 3;                   // TMEM lane quarter
-        const unsigned col0 = (ew >> 2) * 64;          // column half
         const unsigned row = q * 32 + lane;
         const unsigned lane_off = (q * 32u) << 16;
         const JoinParams& jp = a.jp;
@@ -683,6 +685,7 @@ __global__ void __launch_bounds__(kHHThreads, 1)
             const double hi_n = rvalid ? (double)a.r_hn[rs] : 0.0, li_n = rvalid ? (double)a.r_ln[rs] : 0.0;
             const uint32_t oi = rvalid ? a.r_perm[rs] : 0u;
             for (unsigned e = ch.y; e < ch.z; ++e, ++n) {
+                if ((unsigned)(n % kHHGroups) != group) continue;
                 const unsigned b = (unsigned)(n & (kHHAcc - 1));
                 const unsigned slot = (unsigned)(n % kI8Meta), mph = (unsigned)((n / kI8Meta) & 1);
                 {   // warp-uniform: the TMEM loads below are warp-collective
@@ -692,8 +695,8 @@ __global__ void __launch_bounds__(kHHThreads, 1)
                 }
                 tc_fence_after();
                 uint32_t hv2[2][32];
-                tmem_ld32(tmem + lane_off + b * 128 + col0, hv2[0]);
-                tmem_ld32(tmem + lane_off + b * 128 + col0 + 32, hv2[1]);
+                tmem_ld32(tmem + lane_off + b * 128, hv2[0]);
+                tmem_ld32(tmem + lane_off + b * 128 + 32, hv2[1]);
                 const ColMetaI8& m = meta[slot];
                 const unsigned c0 = m.c0;
                 // M_iJ >= |128 x + ll| for this row and S tile (every term non-negative; the 2^-40 factor
@@ -707,12 +710,21 @@ __global__ void __launch_bounds__(kHHThreads, 1)
                     ai = clamp_shift15(Ai - a.T - 2 * M);
                 }
                 tmem_ld_wait();
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&ctl->acc_empty[b]);   // the accumulator is in registers
+                // the warp's 128 columns in two passes of 64 (the second pass's loads hand the
+                // accumulator back once they are in registers)
+#pragma unroll 1
+                for (int pass = 0; pass < 2; ++pass) {
+                if (pass == 1) {
+                    tmem_ld32(tmem + lane_off + b * 128 + 64, hv2[0]);
+                    tmem_ld32(tmem + lane_off + b * 128 + 96, hv2[1]);
+                    tmem_ld_wait();
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&ctl->acc_empty[b]);   // the accumulator is in registers
+                }
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const unsigned cc = col0 + h * 32;
+                    const unsigned cc = pass * 64 + h * 32;
                     const uint32_t (&hv)[32] = hv2[h];
                     // group fast test: hh_j - b_j <= max hh - min b over 8 columns, so
                     // max hh - min b < a_iJ proves the whole group out
@@ -781,6 +793,7 @@ __global__ void __launch_bounds__(kHHThreads, 1)
                             ++pos;
                         }
                     }
+                }
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&ctl->meta_empty[slot]);
