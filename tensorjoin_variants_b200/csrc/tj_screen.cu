@@ -564,12 +564,10 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     b = (unsigned)(sub & 3);
                     bph = (unsigned)((sub >> 2) & 1);
                 }
-                {   // warp-uniform: the TMEM loads below are warp-collective
-                    const bool got = mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns) &&
-                                     mbar_wait(&ctl->acc_full[b], bph, status, a.wait_ns);
-                    if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
+                if (!__all_sync(0xffffffffu, mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns))) {
+                    ok = false;
+                    break;
                 }
-                tc_fence_after();
                 const ColMetaF& m = meta[slot];
                 const unsigned c0 = m.c0;
                 // per-(row, S tile) fast threshold; every error term bounded by tile maxima
@@ -588,6 +586,13 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     const double ti = jp.Tm - Ai - slack * (1.0 + 0x1p-40) - 0x1p-50 * (jp.Tm + Ai) - 0x1p-1000;
                     tau_in = f32_dn(ti);
                 }
+                // the thresholds above need only the metadata: the accumulator is awaited after them
+                // (warp-uniform: the TMEM loads below are warp-collective)
+                if (!__all_sync(0xffffffffu, mbar_wait(&ctl->acc_full[b], bph, status, a.wait_ns))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
                 const unsigned tbase = tmem + ((q * 32u) << 16) + (kPair ? b * kTileS : b * 128u);
                 // phase 1: every 32-column block of this warp's part is read from TMEM and tested; a
                 // lane keeps, per block, the mask of its candidates (v <= tau) and of the certified
