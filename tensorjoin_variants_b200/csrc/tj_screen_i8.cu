@@ -688,19 +688,15 @@ __global__ void __launch_bounds__(kHHThreads, 1)
                 if ((unsigned)(n % kHHGroups) != group) continue;
                 const unsigned b = (unsigned)(n & (kHHAcc - 1));
                 const unsigned slot = (unsigned)(n % kI8Meta), mph = (unsigned)((n / kI8Meta) & 1);
-                {   // warp-uniform: the TMEM loads below are warp-collective
-                    const bool got = mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns) &&
-                                     mbar_wait(&ctl->acc_full[b], (unsigned)((n / kHHAcc) & 1), status, a.wait_ns);
-                    if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
+                if (!__all_sync(0xffffffffu, mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns))) {
+                    ok = false;
+                    break;
                 }
-                tc_fence_after();
-                uint32_t hv2[2][32];
-                tmem_ld32(tmem + lane_off + b * 128, hv2[0]);
-                tmem_ld32(tmem + lane_off + b * 128 + 32, hv2[1]);
                 const ColMetaI8& m = meta[slot];
                 const unsigned c0 = m.c0;
                 // M_iJ >= |128 x + ll| for this row and S tile (every term non-negative; the 2^-40 factor
-                // and +2 cover the FP64 rounding of the sum and of the ceil); a_iJ as in the header
+                // and +2 cover the FP64 rounding of the sum and of the ceil); a_iJ as in the header.
+                // Only the metadata is needed: the accumulator is awaited after this.
                 int ai = 0x7FFFFFFF;
                 long long M = 0;
                 if (rvalid) {
@@ -709,6 +705,16 @@ __global__ void __launch_bounds__(kHHThreads, 1)
                     M = (long long)ceil(Md);
                     ai = clamp_shift15(Ai - a.T - 2 * M);
                 }
+                // warp-uniform: the TMEM loads below are warp-collective
+                if (!__all_sync(0xffffffffu, mbar_wait(&ctl->acc_full[b], (unsigned)((n / kHHAcc) & 1), status,
+                                                       a.wait_ns))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                uint32_t hv2[2][32];
+                tmem_ld32(tmem + lane_off + b * 128, hv2[0]);
+                tmem_ld32(tmem + lane_off + b * 128 + 32, hv2[1]);
                 tmem_ld_wait();
                 // the warp's 128 columns in two passes of 64 (the second pass's loads hand the
                 // accumulator back once they are in registers)
