@@ -407,6 +407,15 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     std::vector<JoinParams> jps(nj);
     for (int k = 0; k < nj; ++k) memset(&jps[k], 0, sizeof(JoinParams));
     const int stile = i8 ? 128 : kTileS;
+    // live 128-row halves of every candidate for the one-SM 16-bit screen (joins the CTA-pair screen
+    // is likely to take skip this: that screen walks the whole tile grid; such joins have rows of
+    // more than 192 elements, kpad >= 256, and no hi/lo split)
+    const bool tc16 = !i8 && screen != TJ_SCREEN_PLAIN;
+    const bool split_screen = screen == TJ_SCREEN_BF16X3 || screen == TJ_SCREEN_FP16X3;
+    const bool allow_pair = !(opt && (opt->flags & TJ_FLAG_SCREEN_1SM));
+    const bool likely_pair = allow_pair && ncls == 1 && nj == 1 && !self && !split_screen && cls_d[0] > 192;
+    const bool diag_req = opt && (opt->flags & TJ_FLAG_SCREEN_DIAG) && tc16;   // samples whole tile pairs
+    const bool half_packed = tc16 && !likely_pair && !diag_req && !(opt && (opt->flags & TJ_FLAG_WHOLE_TILES));
     for (int c = 0; c < ncls; ++c) {
         C[c].reset(new Cls());
         Cls& K = *C[c];
@@ -469,18 +478,6 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
             K.pca_frame = compute_frame(srcs, ns, self ? 1 : 2, d, dtype, fm, K.fp.p, K.center.p, st);
             if (K.pca_frame) S_.index_frame = 1;
         }
-        K.R.src = srcR; K.R.dtype = dtype; K.R.n = roR[njc]; K.R.d = d; K.R.screen = screen;
-        K.R.njc = njc; K.R.d_rowoff = njc > 1 ? K.rowoffR.p : nullptr;
-        prepare_side(K.R, K.fp.p, K.pca_frame, K.center.p, st, &ctr.p->status);
-        compute_perm_local(K.R, st);
-        Side* pS = &K.R;
-        if (!self) {
-            K.S.src = srcS; K.S.dtype = dtype; K.S.n = roS[njc]; K.S.d = d; K.S.screen = screen;
-            K.S.njc = njc; K.S.d_rowoff = njc > 1 ? K.rowoffS.p : nullptr;
-            prepare_side(K.S, K.fp.p, K.pca_frame, K.center.p, st, &ctr.p->status);
-            compute_perm_local(K.S, st);
-            pS = &K.S;
-        }
         // tile tables: tiles never span two joins; sorted rows of join q are [ro[q], ro[q+1])
         g.rbase[c] = (int)rtiles.size();
         g.sbase[c] = (int)stiles.size();
@@ -499,6 +496,25 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
                 K.tS.h_row0.push_back(r0); K.tS.h_nvalid.push_back(nv); K.tS.h_join.push_back((uint32_t)k);
                 stiles.push_back(make_uint4(r0, nv, (unsigned)k, (unsigned)c));
             }
+        }
+        // operands and tile statistics (one fused pass per side where the side allows it: the R
+        // tiling, or for a self-join the S tiling; the S tiling brings its 128-row halves along when
+        // the screen packs half-tiles)
+        TileSet* halves = half_packed ? &K.tSh : nullptr;
+        K.R.src = srcR; K.R.dtype = dtype; K.R.n = roR[njc]; K.R.d = d; K.R.screen = screen;
+        K.R.njc = njc; K.R.d_rowoff = njc > 1 ? K.rowoffR.p : nullptr;
+        if (self)
+            prepare_side(K.R, K.fp.p, K.pca_frame, K.center.p, st, &ctr.p->status, &K.tS, stile, halves);
+        else
+            prepare_side(K.R, K.fp.p, K.pca_frame, K.center.p, st, &ctr.p->status, &K.tR, kTileR);
+        compute_perm_local(K.R, st);
+        Side* pS = &K.R;
+        if (!self) {
+            K.S.src = srcS; K.S.dtype = dtype; K.S.n = roS[njc]; K.S.d = d; K.S.screen = screen;
+            K.S.njc = njc; K.S.d_rowoff = njc > 1 ? K.rowoffS.p : nullptr;
+            prepare_side(K.S, K.fp.p, K.pca_frame, K.center.p, st, &ctr.p->status, &K.tS, stile, halves);
+            compute_perm_local(K.S, st);
+            pS = &K.S;
         }
         tile_stats(K.R, kTileR, K.tR, st);
         tile_stats(*pS, stile, K.tS, st);
@@ -540,7 +556,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     g.stiles = d_st.p;
     g.jps = d_jps.p;
     g.h_jps = jps.data();
-    g.allow_pair = !(opt && (opt->flags & TJ_FLAG_SCREEN_1SM));
+    g.allow_pair = allow_pair;
     g.i8_four_products = opt && (opt->flags & TJ_FLAG_I8_FOUR_PRODUCTS);
     g.k_block = opt ? opt->k_block : 0;
     g.stages = opt ? opt->stages : 0;
@@ -600,24 +616,21 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         sops.per_item[c] = 2.0 * kTileR * 128.0 * (double)C[c]->R.kpad * (C[c]->R.split ? 3.0 : 1.0) *
                            (i8 ? 0.5 : 1.0);
     }
-    // live 128-row halves of every candidate for the one-SM 16-bit screen (joins the CTA-pair screen
-    // is likely to take skip this: that screen walks the whole tile grid)
-    const bool tc16 = !i8 && screen != TJ_SCREEN_PLAIN;
-    const bool likely_pair = g.allow_pair && ncls == 1 && nj == 1 && !self && !C[0]->R.split && C[0]->R.kpad >= 256;
-    const bool diag_req = opt && (opt->flags & TJ_FLAG_SCREEN_DIAG) && tc16;   // samples whole tile pairs
-    g.half_packed = tc16 && !likely_pair && !diag_req && !(opt && (opt->flags & TJ_FLAG_WHOLE_TILES));
+    g.half_packed = half_packed;
     if (g.half_packed) {
         std::vector<HalfView> hv(ncls);
         for (int c = 0; c < ncls; ++c) {
             Cls& K = *C[c];
             TileSet& H = K.tSh;
-            for (size_t t = 0; t < K.tS.h_row0.size(); ++t)
-                for (uint32_t h = 0; h < 2; ++h) {
-                    const uint32_t nv = K.tS.h_nvalid[t];
-                    H.h_row0.push_back(K.tS.h_row0[t] + 128u * h);
-                    H.h_nvalid.push_back(nv > 128u * h ? std::min(128u, nv - 128u * h) : 0u);
-                }
-            tile_stats(*g.S[c], 128, H, st);
+            if (!H.built) {   // halves not made by the fused operand pass
+                for (size_t t = 0; t < K.tS.h_row0.size(); ++t)
+                    for (uint32_t h = 0; h < 2; ++h) {
+                        const uint32_t nv = K.tS.h_nvalid[t];
+                        H.h_row0.push_back(K.tS.h_row0[t] + 128u * h);
+                        H.h_nvalid.push_back(nv > 128u * h ? std::min(128u, nv - 128u * h) : 0u);
+                    }
+                tile_stats(*g.S[c], 128, H, st);
+            }
             hv[c] = HalfView{K.tR.ctrT.p, K.tR.loT.p, K.tR.hiT.p, K.tR.rad.p, H.ctrT.p, H.loT.p, H.hiT.p, H.rad.p,
                              H.nvalid.p, K.tR.ntiles, H.ntiles, g.rbase[c], g.sbase[c], cls_d[c], 0};
         }
@@ -763,7 +776,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
             if (ns[q] > 1) {
                 DBuf<uint64_t> t(ns[q], st);
                 DBuf<uint32_t> w(radix_workspace_elems(ns[q]), st);
-                radix_sort(res->stage[q].p, nullptr, t.p, nullptr, ns[q], 64, w.p, st);
+                radix_sort(res->stage[q].p, nullptr, t.p, nullptr, ns[q], 64, w.p, st, &ctr.p->status);
             }
         }
     }
@@ -790,7 +803,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         DBuf<uint64_t> ktmp(slots + gs, st);
         DBuf<uint32_t> ws(radix_workspace_elems(slots), st);
         if (guards) launch(guard_fill, 1, 256, 0, st, ktmp.p + slots);
-        radix_sort(keys.p, nullptr, ktmp.p, nullptr, slots, bits, ws.p, st);
+        radix_sort(keys.p, nullptr, ktmp.p, nullptr, slots, bits, ws.p, st, &ctr.p->status);
         if (guards) launch(guard_check, 1, 256, 0, st, (const uint64_t*)(ktmp.p + slots), ctr.p);
     }
     if (guards) launch(guard_check, 1, 256, 0, st, (const uint64_t*)(keys.p + slots), ctr.p);

@@ -812,6 +812,322 @@ __global__ void __launch_bounds__(256) tile_stats_kernel(const void* src, int dt
     }
 }
 
+// Outputs of the fused kernel for one tile granularity.
+struct TileOut {
+    float *ctrT, *loT, *hiT, *rad, *maxZ, *maxE, *maxY, *maxB, *beta, *maxZl;
+    uint32_t *nvalid, *row0;
+    int ntiles;
+};
+
+// Operand preparation and tile statistics in one pass, for 16-bit screens over FP32 rows with
+// d % 4 == 0 and kpad = 4 kL <= 128 (one block per tile of 128 or 256 sorted rows; kL lanes per row,
+// each lane four consecutive elements).  Every gathered row is read from HBM once: the row's
+// operands, norms and bounds, and the tile's centroid and box partials come from that read; the
+// radius pass reads the tile again while it is still in L2.  With kHalves the statistics of the two
+// 128-row halves of a 256-row tile are written as well (tile t, half h -> entry 2 t + h of H).
+//
+// Arithmetic.  x' = x - c is carried exactly as s + err (s = fl32(x - c), err from TwoSum), so the
+// operands and the bounds need no FP64 conversions per element:
+//   z_hi = round16(s);  r = fl32((s - z_hi) + err) (s - z_hi is exact) with its TwoSum residual rr;
+//   z_lo = round16(r);  x' - z_hi - z_lo = (r - z_lo) + rr, rounded once to FP32.
+// A = ||x'||^2 stays an FP64 sum (its relative error enters the certificate).  Z >= ||z_hi + z_lo||,
+// E >= ||x' - z||, Zl >= ||z_lo|| and the tile radius are FP32 sums of squares made rigorous upper
+// bounds: each term is exact or rounded once (relative 2^-24; additions are exact in the subnormal
+// range, a product that underflows errs by at most 2^-150), a chain of m <= d + 5 roundings errs by at
+// most gamma_m, so  true <= (S + d 2^-140) (1 + (d + 16) 2^-23),  and the square root is taken in FP64
+// and rounded up.  The centroid needs no accuracy (the radius is measured from the value written).
+template <int kScreen, int kSplit, int kL, bool kHalves>
+__global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict__ src, long long n, int d, int tile,
+                                                         const uint32_t* __restrict__ perm,
+                                                         const float* __restrict__ center,
+                                                         const uint32_t* row0_in, const uint32_t* nvalid_in,
+                                                         uint16_t* op, double* nrm2, float* nrm2f, float* zn,
+                                                         float* en, float* yn, float* zl, TileOut T, TileOut H,
+                                                         unsigned long long* status) {
+    constexpr int kFmt = (kScreen == kScreenBF16 || kScreen == kScreenBF16X3) ? 1 : 0;
+    constexpr int kPad = 4 * kL;
+    constexpr int kNG = 256 / kL;              // row groups per block
+    constexpr int kRows = 128 / kNG;           // rows of one group in one 128-row half
+    constexpr int kU = kRows < 4 ? kRows : 4;  // rows whose loads are issued together
+    constexpr int opw = kSplit ? 2 * kPad : kPad;
+    __shared__ float psum[2][1024], pmin[2][1024], pmax[2][1024];   // [half][group * kPad + element]
+    __shared__ float rmx[2][6][kNG];        // [half][bound][group] row-bound maxima
+    __shared__ float cs[3][kPad];           // centroids: tile, half 0, half 1
+    __shared__ float radm[3][kNG];          // per-group maxima of the radius sums
+    const int t = blockIdx.x;
+    const bool tabled = row0_in != nullptr;
+    const long long r0 = tabled ? (long long)row0_in[t] : (long long)t * tile;
+    const int nv = tabled ? (int)nvalid_in[t] : (int)min((long long)tile, n - r0);
+    const int halves = tile == 256 ? 2 : 1;
+    const int grp = threadIdx.x / kL, sub = threadIdx.x % kL;
+    const int k0 = 4 * sub;
+    const bool kin = k0 < d;
+    float cf[4];
+    double cdv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        cf[q] = kin ? center[k0 + q] : 0.f;
+        cdv[q] = (double)cf[q];
+    }
+    const double g64 = (double)(d + 4) * 0x1p-53;
+    const double up64 = (1.0 + 2.0 * g64) * (1.0 + 0x1p-50);
+    const double up32 = 1.0 + (double)(d + 16) * 0x1p-23;
+    const double slack32 = (double)d * 0x1p-140;
+    const double gb = (double)(d + 2) * 0x1p-53;   // beta: |nrm2f - nrm2| + 2 gb nrm2
+    unsigned flags = 0;
+
+    for (int h = 0; h < halves; ++h) {
+        const int hb = h * 128;
+        float ps[4], pl[4], ph[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) { ps[q] = 0.f; pl[q] = INFINITY; ph[q] = -INFINITY; }
+        float my = 0.f, mb = 0.f, mbeta = 0.f, mtask = 0.f;   // task maxima (see below)
+        if (hb < nv) {   // uniform across the block
+            for (int m0 = 0; m0 < kRows; m0 += kU) {
+                float4 xv[kU];
+                int ii[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    ii[u] = hb + grp + (m0 + u) * kNG;
+                    xv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (ii[u] < nv && kin) {
+                        const size_t orig = (size_t)perm[r0 + ii[u]];
+                        xv[u] = __ldg(reinterpret_cast<const float4*>(src + orig * (size_t)d + k0));
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const bool rv = ii[u] < nv;
+                    const float xa[4] = {xv[u].x, xv[u].y, xv[u].z, xv[u].w};
+                    double sx = 0.0;
+                    float sz = 0.f, se = 0.f, sl = 0.f;
+                    uint16_t hbits[4], lbits[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        float x = xa[q];
+                        if (!isfinite(x)) { flags |= 1u; x = 0.f; }
+                        const float sd = x - cf[q];
+                        const float bb = sd - x;
+                        const float err = (x - (sd - bb)) + (-cf[q] - bb);
+                        const double xd = (double)x - cdv[q];
+                        sx = fma(xd, xd, sx);
+                        if (kFmt == 0 && fabsf(sd) > 65504.f) flags |= 2u;
+                        const float zh = round16<kFmt>(sd, hbits[q]);
+                        const float d1 = sd - zh;   // exact
+                        if (kSplit) {
+                            const float r = d1 + err;
+                            const float b2 = r - d1;
+                            const float rr = (d1 - (r - b2)) + (err - b2);
+                            const float zlo = round16<kFmt>(r, lbits[q]);
+                            const float ed = (r - zlo) + rr;
+                            const float z = zh + zlo;
+                            sz = fmaf(z, z, sz);
+                            se = fmaf(ed, ed, se);
+                            sl = fmaf(zlo, zlo, sl);
+                        } else {
+                            lbits[q] = 0;
+                            const float ed = d1 + err;
+                            sz = fmaf(zh, zh, sz);
+                            se = fmaf(ed, ed, se);
+                        }
+                        if (rv && kin) {
+                            ps[q] += x;
+                            pl[q] = fminf(pl[q], x);
+                            ph[q] = fmaxf(ph[q], x);
+                        }
+                    }
+                    const long long r = r0 + ii[u];
+                    if (rv) {
+                        uint2 hv, lv;
+                        hv.x = (uint32_t)hbits[0] | ((uint32_t)hbits[1] << 16);
+                        hv.y = (uint32_t)hbits[2] | ((uint32_t)hbits[3] << 16);
+                        *reinterpret_cast<uint2*>(op + (size_t)r * opw + k0) = hv;
+                        if (kSplit) {
+                            lv.x = (uint32_t)lbits[0] | ((uint32_t)lbits[1] << 16);
+                            lv.y = (uint32_t)lbits[2] | ((uint32_t)lbits[3] << 16);
+                            *reinterpret_cast<uint2*>(op + (size_t)r * opw + kPad + k0) = lv;
+                        }
+                    }
+#pragma unroll
+                    for (int o = kL / 2; o > 0; o >>= 1) {
+                        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+                        sz += __shfl_xor_sync(0xffffffffu, sz, o);
+                        se += __shfl_xor_sync(0xffffffffu, se, o);
+                        if (kSplit) sl += __shfl_xor_sync(0xffffffffu, sl, o);
+                    }
+                    // the four bounds of the row are taken by its first four lanes, one square root each
+                    const unsigned task = sub & 3u;   // 0: |x - c|, 1: |z|, 2: |x - c - z|, 3: |z_lo|
+                    double rt;
+                    if (task == 0) {
+                        rt = sqrt(sx * up64) * (1.0 + 0x1p-50);
+                    } else {
+                        const float v32 = task == 1 ? sz : task == 2 ? se : sl;
+                        rt = (task == 3 && !kSplit) ? 0.0 : sqrt(((double)v32 + slack32) * up32) * (1.0 + 0x1p-50);
+                    }
+                    const double ynorm = __shfl_sync(0xffffffffu, rt, (int)((threadIdx.x & 31u) & ~(unsigned)(kL - 1)));
+                    if (task == 2) rt += 0x1p-50 * ynorm;
+                    const float rv32 = f32_up(rt);
+                    if (rv && sub < 4) {
+                        float* dst = task == 0 ? yn : task == 1 ? zn : task == 2 ? en : zl;
+                        dst[r] = rv32;
+                        mtask = fmaxf(mtask, rv32);
+                    }
+                    if (rv && sub == 0) {
+                        if (sx > 0x1p100) flags |= 1u;
+                        const float sf = __double2float_rn(sx);
+                        nrm2[r] = sx;
+                        nrm2f[r] = sf;
+                        mb = fmaxf(mb, sf);
+                        const double bt = fabs((double)sf - sx) + 2.0 * gb * sx;
+                        mbeta = fmaxf(mbeta, f32_up(bt * (1.0 + 0x1p-40)));
+                    }
+                }
+            }
+        }
+        my = mtask;   // lane 0 of a group: the Y maximum; lanes 1-3: Z, E, Zl
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            psum[h][4 * threadIdx.x + q] = ps[q];
+            pmin[h][4 * threadIdx.x + q] = pl[q];
+            pmax[h][4 * threadIdx.x + q] = ph[q];
+        }
+        if (sub < 4) rmx[h][sub][grp] = my;   // 0: Y, 1: Z, 2: E, 3: Zl
+        if (sub == 0) {
+            rmx[h][4][grp] = mb;
+            rmx[h][5][grp] = mbeta;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) flags |= __shfl_xor_sync(0xffffffffu, flags, o);
+    if ((threadIdx.x & 31) == 0 && flags) {
+        if (flags & 1u) atomicOr(status, (unsigned long long)kStatusBadInput);
+        if (flags & 2u) atomicOr(status, (unsigned long long)kStatusFp16Range);
+    }
+    __syncthreads();
+    // centroids and boxes: groups combined in a fixed order
+    const int nvh[2] = {min(nv, 128), max(0, min(nv - 128, 128))};
+    for (int k = threadIdx.x; k < kPad; k += 256) {
+        float sum[2] = {0.f, 0.f}, lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
+        for (int h = 0; h < halves; ++h)
+            for (int gq = 0; gq < kNG; ++gq) {
+                sum[h] += psum[h][gq * kPad + k];
+                lo[h] = fminf(lo[h], pmin[h][gq * kPad + k]);
+                hi[h] = fmaxf(hi[h], pmax[h][gq * kPad + k]);
+            }
+        const float c = (float)(((double)sum[0] + (double)sum[1]) / (double)max(nv, 1));
+        cs[0][k] = c;
+        if (k < d) {
+            T.ctrT[(size_t)k * T.ntiles + t] = c;
+            T.loT[(size_t)k * T.ntiles + t] = fminf(lo[0], lo[1]);
+            T.hiT[(size_t)k * T.ntiles + t] = fmaxf(hi[0], hi[1]);
+        }
+        if (kHalves) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const float ch = (float)((double)sum[h] / (double)max(nvh[h], 1));
+                cs[1 + h][k] = ch;
+                if (k < d) {
+                    const size_t e = (size_t)k * H.ntiles + 2 * t + h;
+                    H.ctrT[e] = ch;
+                    H.loT[e] = lo[h];
+                    H.hiT[e] = hi[h];
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // radius pass (the tile's rows again, from L2): FP32 sums of squared differences from the
+    // centroids just written, bounded above as described at the top
+    {
+        float ct[4], c0h[4], c1h[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            ct[q] = cs[0][k0 + q];
+            c0h[q] = kHalves ? cs[1][k0 + q] : 0.f;
+            c1h[q] = kHalves ? cs[2][k0 + q] : 0.f;
+        }
+        float mt = 0.f, mh[2] = {0.f, 0.f};
+        for (int h = 0; h < halves; ++h) {
+            const int hb = h * 128;
+            if (hb >= nv) break;   // uniform
+            for (int m0 = 0; m0 < kRows; m0 += kU) {
+                float4 xv[kU];
+                int ii[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    ii[u] = hb + grp + (m0 + u) * kNG;
+                    xv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (ii[u] < nv && kin) {
+                        const size_t orig = (size_t)perm[r0 + ii[u]];
+                        xv[u] = __ldg(reinterpret_cast<const float4*>(src + orig * (size_t)d + k0));
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const float xa[4] = {xv[u].x, xv[u].y, xv[u].z, xv[u].w};
+                    float st_ = 0.f, sh = 0.f;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float x = isfinite(xa[q]) ? xa[q] : 0.f;
+                        const float df = kin ? x - ct[q] : 0.f;
+                        st_ = fmaf(df, df, st_);
+                        if (kHalves) {
+                            const float dh = kin ? x - (h ? c1h[q] : c0h[q]) : 0.f;
+                            sh = fmaf(dh, dh, sh);
+                        }
+                    }
+#pragma unroll
+                    for (int o = kL / 2; o > 0; o >>= 1) {
+                        st_ += __shfl_xor_sync(0xffffffffu, st_, o);
+                        if (kHalves) sh += __shfl_xor_sync(0xffffffffu, sh, o);
+                    }
+                    if (ii[u] < nv) {
+                        mt = fmaxf(mt, st_);
+                        if (kHalves) mh[h] = fmaxf(mh[h], sh);
+                    }
+                }
+            }
+        }
+        if (sub == 0) {
+            radm[0][grp] = mt;
+            radm[1][grp] = mh[0];
+            radm[2][grp] = mh[1];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {   // thread 0: the tile; threads 1, 2: the halves
+        const int w = threadIdx.x;
+        if (w == 0 || kHalves) {
+            float m = 0.f;
+            for (int gq = 0; gq < kNG; ++gq) m = fmaxf(m, radm[w][gq]);
+            const int hv = w == 0 ? nv : nvh[w - 1];
+            const float rb = hv > 0 ? f32_up(sqrt(((double)m + slack32) * up32) * (1.0 + 0x1p-50)) : 0.f;
+            float mx[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            for (int q = 0; q < 6; ++q)
+                for (int h = 0; h < halves; ++h) {
+                    if (w > 0 && h != w - 1) continue;
+                    for (int gq = 0; gq < kNG; ++gq) mx[q] = fmaxf(mx[q], rmx[h][q][gq]);
+                }
+            TileOut& O = w == 0 ? T : H;
+            const int e = w == 0 ? t : 2 * t + (w - 1);
+            O.rad[e] = rb;
+            O.maxY[e] = mx[0];
+            O.maxZ[e] = mx[1];
+            O.maxE[e] = mx[2];
+            O.maxZl[e] = mx[3];
+            O.maxB[e] = mx[4];
+            O.beta[e] = mx[5];
+            if (w > 0) {
+                O.nvalid[e] = (uint32_t)hv;
+                O.row0[e] = (uint32_t)(r0 + 128 * (w - 1));
+            } else if (!tabled) {
+                O.nvalid[e] = (uint32_t)max(nv, 0);
+                O.row0[e] = (uint32_t)r0;
+            }
+        }
+    }
+}
+
 // Candidate test: thread = one S tile J, 16 R tiles per block (from shared memory).
 // Keeps (I, J) unless a rigorous lower bound on every pair distance exceeds sqrt(Tp).
 template <int kCandI>
@@ -1115,8 +1431,102 @@ bool compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d
     return pca;
 }
 
+namespace {
+
+// Device arrays of a tile set (tables uploaded when the host built them).
+void alloc_tiles(TileSet& ts, int tile, int d, int ntiles, cudaStream_t st) {
+    ts.tile = tile;
+    ts.d = d;
+    ts.ntiles = ntiles;
+    const size_t nt = (size_t)std::max(ntiles, 1);
+    ts.ctrT = DBuf<float>(nt * d, st);
+    ts.loT = DBuf<float>(nt * d, st);
+    ts.hiT = DBuf<float>(nt * d, st);
+    ts.rad = DBuf<float>(nt, st);
+    ts.maxZ = DBuf<float>(nt, st);
+    ts.maxE = DBuf<float>(nt, st);
+    ts.maxY = DBuf<float>(nt, st);
+    ts.maxB = DBuf<float>(nt, st);
+    ts.beta = DBuf<float>(nt, st);
+    ts.maxZl = DBuf<float>(nt, st);
+    ts.nvalid = DBuf<uint32_t>(nt, st);
+    ts.row0 = DBuf<uint32_t>(nt, st);
+    if (ntiles > 0 && !ts.h_row0.empty()) {
+        upload(ts.row0.p, ts.h_row0.data(), nt * 4, st);
+        upload(ts.nvalid.p, ts.h_nvalid.data(), nt * 4, st);
+    }
+}
+
+TileOut tile_out(TileSet& ts) {
+    return TileOut{ts.ctrT.p, ts.loT.p, ts.hiT.p, ts.rad.p, ts.maxZ.p, ts.maxE.p, ts.maxY.p, ts.maxB.p,
+                   ts.beta.p, ts.maxZl.p, ts.nvalid.p, ts.row0.p, ts.ntiles};
+}
+
+bool fused_prep_ok(const Side& s) {
+    const bool f16 = s.screen == kScreenBF16 || s.screen == kScreenFP16 || s.screen == kScreenBF16X3 ||
+                     s.screen == kScreenFP16X3;
+    return f16 && s.dtype == kF32 && s.d % 4 == 0 && s.kpad <= 128 && ((uintptr_t)s.src & 15u) == 0;
+}
+
+// The fused pass over one tiling of the side (operands, norms, bounds and tile statistics).
+void prep_tiles(Side& s, const float* center, int tile, TileSet& ts, TileSet* halves, cudaStream_t st,
+                unsigned long long* status) {
+    const bool tabled = !ts.h_row0.empty();
+    const int ntiles = tabled ? (int)ts.h_row0.size() : (int)((s.n + tile - 1) / tile);
+    alloc_tiles(ts, tile, s.d, ntiles, st);
+    TileOut H{};
+    if (halves) {
+        halves->h_row0.clear();
+        halves->h_nvalid.clear();
+        alloc_tiles(*halves, 128, s.d, 2 * ntiles, st);
+        H = tile_out(*halves);
+        halves->built = true;
+    }
+    ts.built = true;
+    // rows past the last tile (the operand padding up to rows_pad) are zero
+    const long long n = s.n, rp = s.rows_pad;
+    if (rp > n) {
+        const size_t opw = (size_t)s.kpad * (s.split ? 2 : 1);
+        TJ_CUDA(cudaMemsetAsync(s.op.p + (size_t)n * opw, 0, (size_t)(rp - n) * opw * sizeof(uint16_t), st));
+        TJ_CUDA(cudaMemsetAsync(s.nrm2.p + n, 0, (size_t)(rp - n) * sizeof(double), st));
+        float* fl[5] = {s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.zl.p};
+        for (float* f : fl) TJ_CUDA(cudaMemsetAsync(f + n, 0, (size_t)(rp - n) * sizeof(float), st));
+    }
+    if (ntiles == 0) return;
+    const uint32_t* r0 = tabled ? (const uint32_t*)ts.row0.p : nullptr;
+    const uint32_t* nvv = tabled ? (const uint32_t*)ts.nvalid.p : nullptr;
+    const TileOut T = tile_out(ts);
+#define TJ_PT(SCR, SPLIT, L, HV)                                                                                   \
+    launch(prep_tiles_kernel<SCR, SPLIT, L, HV>, (unsigned)ntiles, 256, 0, st, (const float*)s.src, n, s.d, tile, \
+           (const uint32_t*)s.perm.p, center, r0, nvv, s.op.p, s.nrm2.p, s.nrm2f.p, s.zn.p, s.en.p, s.yn.p,      \
+           s.zl.p, T, H, status)
+#define TJ_PT_L(SCR, SPLIT, HV)                                  \
+    do {                                                         \
+        if (s.kpad == 16) TJ_PT(SCR, SPLIT, 4, HV);              \
+        else if (s.kpad == 32) TJ_PT(SCR, SPLIT, 8, HV);         \
+        else if (s.kpad == 64) TJ_PT(SCR, SPLIT, 16, HV);        \
+        else TJ_PT(SCR, SPLIT, 32, HV);                          \
+    } while (0)
+#define TJ_PT_H(SCR, SPLIT)                                      \
+    do {                                                         \
+        if (halves) TJ_PT_L(SCR, SPLIT, true);                   \
+        else TJ_PT_L(SCR, SPLIT, false);                         \
+    } while (0)
+    switch (s.screen) {
+        case kScreenBF16: TJ_PT_H(kScreenBF16, 0); break;
+        case kScreenFP16: TJ_PT_H(kScreenFP16, 0); break;
+        case kScreenBF16X3: TJ_PT_H(kScreenBF16X3, 1); break;
+        default: TJ_PT_H(kScreenFP16X3, 1); break;
+    }
+#undef TJ_PT_H
+#undef TJ_PT_L
+#undef TJ_PT
+}
+
+}  // namespace
+
 void prepare_side(Side& s, const FrameParams* fpd, bool pca_frame, const float* center, cudaStream_t st,
-                  unsigned long long* status) {
+                  unsigned long long* status, TileSet* ts, int tile, TileSet* halves) {
     const long long n = s.n;
     const bool i8 = s.screen == kScreenInt8Limb;
     s.split = (s.screen == kScreenBF16X3 || s.screen == kScreenFP16X3) ? 1 : 0;
@@ -1139,7 +1549,12 @@ void prepare_side(Side& s, const FrameParams* fpd, bool pca_frame, const float* 
                    s.perm.p, s.d_rowoff, s.njc);
         int jbits = 0;
         while ((1 << jbits) < s.njc) ++jbits;
-        radix_sort(s.keys.p, s.perm.p, ktmp.p, vtmp.p, (size_t)n, 32 + jbits, ws.p, st);
+        bool in_tmp = false;
+        radix_sort(s.keys.p, s.perm.p, ktmp.p, vtmp.p, (size_t)n, 32 + jbits, ws.p, st, status, &in_tmp);
+        if (in_tmp) {   // odd number of passes: the sorted arrays are the temporaries
+            std::swap(s.keys, ktmp);
+            std::swap(s.perm, vtmp);
+        }
     }
     s.emit = s.perm.p;
     const size_t rp = (size_t)s.rows_pad;
@@ -1156,6 +1571,10 @@ void prepare_side(Side& s, const FrameParams* fpd, bool pca_frame, const float* 
     s.en = DBuf<float>(rp, st);
     s.yn = DBuf<float>(rp, st);
     s.zl = DBuf<float>(rp, st);
+    if (ts && fused_prep_ok(s) && (tile == 128 || tile == 256) && (!halves || tile == 256)) {
+        prep_tiles(s, center, tile, *ts, halves, st, status);
+        return;
+    }
     // lanes per row: 4 for rows of <= 16 elements, 8 for <= 32, else a warp
 #define TJ_PREP_L(SCR, SPLIT, L)                                                                                 \
     launch(prep_rows<SCR, SPLIT, L>, (unsigned)((rp * L + 255) / 256), 256, 0, st, s.src, s.dtype, n, s.d, s.kpad, \
@@ -1180,28 +1599,10 @@ void prepare_side(Side& s, const FrameParams* fpd, bool pca_frame, const float* 
 }
 
 void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st) {
-    ts.tile = tile;
-    ts.d = s.d;
+    if (ts.built) return;   // made by the fused operand pass
     const bool tabled = !ts.h_row0.empty();
-    ts.ntiles = tabled ? (int)ts.h_row0.size() : (int)((s.n + tile - 1) / tile);
-    const size_t nt = (size_t)std::max(ts.ntiles, 1);
-    ts.ctrT = DBuf<float>(nt * s.d, st);
-    ts.loT = DBuf<float>(nt * s.d, st);
-    ts.hiT = DBuf<float>(nt * s.d, st);
-    ts.rad = DBuf<float>(nt, st);
-    ts.maxZ = DBuf<float>(nt, st);
-    ts.maxE = DBuf<float>(nt, st);
-    ts.maxY = DBuf<float>(nt, st);
-    ts.maxB = DBuf<float>(nt, st);
-    ts.beta = DBuf<float>(nt, st);
-    ts.maxZl = DBuf<float>(nt, st);
-    ts.nvalid = DBuf<uint32_t>(nt, st);
-    ts.row0 = DBuf<uint32_t>(nt, st);
+    alloc_tiles(ts, tile, s.d, tabled ? (int)ts.h_row0.size() : (int)((s.n + tile - 1) / tile), st);
     if (ts.ntiles == 0) return;
-    if (tabled) {
-        upload(ts.row0.p, ts.h_row0.data(), nt * 4, st);
-        upload(ts.nvalid.p, ts.h_nvalid.data(), nt * 4, st);
-    }
     // lanes per row as in prep_rows; centroid [d] floats (rounded up to an even count) + per-group
     // partials (256 / kL groups x d x (8 + 4 + 4) bytes)
     const int L = s.d <= 16 ? 4 : s.d <= 32 ? 8 : 32;

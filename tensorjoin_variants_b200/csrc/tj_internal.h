@@ -106,7 +106,7 @@ void exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, uint32_t* t
                         cudaStream_t st);
 size_t radix_workspace_elems(size_t n);
 void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp, size_t n, int bits,
-                uint32_t* ws, cudaStream_t st);
+                uint32_t* ws, cudaStream_t st, unsigned long long* status = nullptr, bool* in_tmp = nullptr);
 int radix_passes(int bits);
 
 // ------------------------------------------------------------------ enums (mirror include/tensorjoin.h)
@@ -156,6 +156,7 @@ struct TileSet {
     DBuf<uint32_t> nvalid;  // [ntiles] rows of the tile that are real points
     DBuf<uint32_t> row0;    // [ntiles] first sorted row of the tile
     std::vector<uint32_t> h_row0, h_nvalid, h_join;   // host tile tables (batched sides; empty: uniform tiles)
+    bool built = false;   // statistics already computed (by the fused operand pass)
 };
 
 // Candidate tile pairs grouped by R tile, cut into chunks scheduled J-window-major.
@@ -191,8 +192,13 @@ constexpr int kFrameAuto = 0, kFrameAxes = 1, kFramePca = 2;
 constexpr long long kPcaMinRows = 1ll << 17;   // below this the frame's fixed cost is not repaid
 bool compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d, int dtype, int frame_mode,
                    FrameParams* fp, float* center, cudaStream_t st);
+// Morton sort and operand preparation of one side.  With a tile set (tile 128 or 256, host tables
+// filled when the tiling is not uniform) the operands and that tiling's statistics come from one
+// fused pass where the side allows it (16-bit screens, FP32 rows, d % 4 == 0, d <= 128), and
+// `halves` (256-row tiles only) receives the statistics of their 128-row halves; the tile sets are
+// then marked built and tile_stats leaves them alone.
 void prepare_side(Side& s, const FrameParams* fp_dev, bool pca_frame, const float* center, cudaStream_t st,
-                  unsigned long long* status);
+                  unsigned long long* status, TileSet* ts = nullptr, int tile = 0, TileSet* halves = nullptr);
 void tile_stats(const Side& s, int tile, TileSet& ts, cudaStream_t st);
 void build_candidates(const TileSet& tr, const TileSet& ts, double T, bool self_join, int chunk_items,
                       Candidates& c, cudaStream_t st);

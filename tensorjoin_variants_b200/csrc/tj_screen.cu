@@ -60,7 +60,7 @@ constexpr int kEpiFirst = 4;                         // warps 0-3: TMA producer,
 constexpr int kScreenThreads = (kEpiFirst + kEpiWarps) * 32;
 constexpr unsigned kABytes = kTileR * 128;          // 16 KB
 constexpr unsigned kBBytes = kTileS * 128;          // 32 KB
-constexpr int kMetaSlots = 3;
+constexpr int kMetaSlots = 8;   // items of column metadata in flight (each epilogue group sees several)
 
 // Stage = one 64-element k-block of A (128 rows) and B (256 rows); with the hi/lo split the
 // stage holds both limbs of both operands: [A_hi | A_lo | B_hi | B_lo].
@@ -72,21 +72,26 @@ template <int kSplit> struct StageCfg {
     static constexpr unsigned kBlo = 2u * kABytes + kBBytes;
 };
 
-// Column metadata of one S tile (256 sorted rows), structure of arrays, one bulk copy per item.
-struct ColMetaF {
+// Column metadata of one S tile (256 sorted rows), structure of arrays.  The screen copies only the
+// leading part (ColMetaHot: what its epilogue reads) into shared memory, one bulk copy per item; the
+// per-column bounds after it are read from global memory by the screen-error diagnostics.
+struct ColMetaHot {
     float nrm2f[kTileS];   // FP32 nearest of ||y - c||^2; +inf for rows beyond the tile's points
-    float zn[kTileS];      // >= ||w||
-    float en[kTileS];      // >= ||y - c - w||
-    float yn[kTileS];      // >= ||y - c||
-    float zl[kTileS];      // >= ||w_lo||
     uint32_t perm[kTileS]; // original row id
-    double nrm2[kTileS];   // ||y - c||^2 (FP64)
     float gminB[kTileS / 8];   // per 8-column group: min of nrm2f (the group-wise fast test)
     float WJ, FJ, YJ, BJ, betaJ, WlJ;   // tile maxima of zn, en, yn, nrm2f, |nrm2f - nrm2| bound, zl
     uint32_t c0, nvJ;      // first sorted row, rows that are real points
 };
-static_assert(sizeof(ColMetaF) % 16 == 0, "bulk copies need 16-byte multiples");
-static_assert(offsetof(ColMetaF, gminB) % 16 == 0, "group minima are read four at a time");
+static_assert(sizeof(ColMetaHot) % 16 == 0, "bulk copies need 16-byte multiples");
+static_assert(offsetof(ColMetaHot, gminB) % 16 == 0, "group minima are read four at a time");
+struct ColMetaF : ColMetaHot {
+    float zn[kTileS];      // >= ||w||
+    float en[kTileS];      // >= ||y - c - w||
+    float yn[kTileS];      // >= ||y - c||
+    float zl[kTileS];      // >= ||w_lo||
+    double nrm2[kTileS];   // ||y - c||^2 (FP64)
+};
+static_assert(sizeof(ColMetaF) % 16 == 0 && sizeof(ColMetaHot) % 16 == 0, "16-byte aligned parts");
 
 template <int kStages>
 struct ScreenCtl {
@@ -121,7 +126,7 @@ template <> struct StageSel<0, true> { using type = StageCfgPair; };
 template <int kSplit, bool kPair>
 constexpr size_t screen_smem() {
     using Cfg = typename StageSel<kSplit, kPair>::type;
-    return 1024 + (size_t)Cfg::kStages * Cfg::kBytes + (size_t)kMetaSlots * sizeof(ColMetaF) +
+    return 1024 + (size_t)Cfg::kStages * Cfg::kBytes + (size_t)kMetaSlots * sizeof(ColMetaHot) +
            sizeof(ScreenCtl<Cfg::kStages>);
 }
 static_assert(screen_smem<0, false>() <= 232448 && screen_smem<1, false>() <= 232448 &&
@@ -272,7 +277,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
     constexpr unsigned kStageBytes = Cfg::kBytes;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    ColMetaF* meta = (ColMetaF*)(smem + (size_t)kStages * kStageBytes);
+    ColMetaHot* meta = (ColMetaHot*)(smem + (size_t)kStages * kStageBytes);
     ScreenCtl<kStages>* ctl = (ScreenCtl<kStages>*)(meta + kMetaSlots);
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long* status = &a.ctr->status;
@@ -359,8 +364,9 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     const int srow = (int)a.stiles[J].x + (int)(rank * kTileR);   // pair: this CTA's half
                     const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
                     if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status, a.wait_ns)) { ok = false; break; }
-                    mbar_arrive_expect_tx(&ctl->meta_full[slot], (unsigned)sizeof(ColMetaF));
-                    bulk_load(&meta[slot], a.s_meta + J, (unsigned)sizeof(ColMetaF), &ctl->meta_full[slot]);
+                    mbar_arrive_expect_tx(&ctl->meta_full[slot], (unsigned)sizeof(ColMetaHot));
+                    bulk_load(&meta[slot], (const ColMetaHot*)(a.s_meta + J), (unsigned)sizeof(ColMetaHot),
+                              &ctl->meta_full[slot]);
                     for (int kb = 0; kb < kblocks; ++kb) {
                         if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status, a.wait_ns)) { ok = false; break; }
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
@@ -568,7 +574,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     ok = false;
                     break;
                 }
-                const ColMetaF& m = meta[slot];
+                const ColMetaHot& m = meta[slot];
                 const unsigned c0 = m.c0;
                 // per-(row, S tile) fast threshold; every error term bounded by tile maxima
                 //   v > tau       =>  D > Tp  (certainly out)
@@ -598,7 +604,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 // lane keeps, per block, the mask of its candidates (v <= tau) and of the certified
                 // accepts among them (v <= tau_in).  No warp-collective step runs here, and the
                 // accumulator is handed back as soon as the last block is in registers.
-                uint32_t cmk[4] = {0u, 0u, 0u, 0u}, imk[4] = {0u, 0u, 0u, 0u};
+                uint32_t cmk0 = 0, cmk1 = 0, cmk2 = 0, cmk3 = 0, imk0 = 0, imk1 = 0, imk2 = 0, imk3 = 0;
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     const int cb = cb_begin + i;
@@ -675,18 +681,19 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         if (lim >= 31) cm = 0;
                         else if (lim >= 0) cm &= ~((2u << lim) - 1u);
                     }
-                    cmk[i] = cm;
-                    imk[i] = im & cm;
+                    im &= cm;
+                    cmk0 = i == 0 ? cm : cmk0; cmk1 = i == 1 ? cm : cmk1;
+                    cmk2 = i == 2 ? cm : cmk2; cmk3 = i == 3 ? cm : cmk3;
+                    imk0 = i == 0 ? im : imk0; imk1 = i == 1 ? im : imk1;
+                    imk2 = i == 2 ? im : imk2; imk3 = i == 3 ? im : imk3;
                 }
                 // phase 2: one warp scan for the part's certified accepts and band pairs together
                 // (accepts in the low 16 bits, band in the high 16: at most 128 of each per lane), one
-                // reservation per list, then each lane writes its pairs' canonical keys
-                unsigned na = 0, nb = 0;
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    na += __popc(imk[i]);
-                    nb += __popc(cmk[i] & ~imk[i]);
-                }
+                // reservation per list, then each lane writes its pairs' canonical keys (these loops stay
+                // rolled: four unrolled copies of each overflow the instruction cache)
+                const unsigned na = __popc(imk0) + __popc(imk1) + __popc(imk2) + __popc(imk3);
+                const unsigned nb = __popc(cmk0 & ~imk0) + __popc(cmk1 & ~imk1) + __popc(cmk2 & ~imk2) +
+                                    __popc(cmk3 & ~imk3);
                 const unsigned packed = na | (nb << 16);
                 if (__any_sync(0xffffffffu, packed != 0)) {
                     unsigned tot;
@@ -697,9 +704,9 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     if (ta) {
                         unsigned long long pos =
                             app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap) + (pre & 0xFFFFu);
-#pragma unroll
+#pragma unroll 1
                         for (int i = 0; i < 4; ++i) {
-                            uint32_t w = imk[i];
+                            uint32_t w = i == 0 ? imk0 : i == 1 ? imk1 : i == 2 ? imk2 : imk3;
                             const int col0 = (int)colbase + (cb_begin + i) * 32;
                             while (w) {
                                 const int k = __ffs(w) - 1;
@@ -712,9 +719,10 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     if (tb) {
                         unsigned long long pos =
                             app_band.reserve(tb, &a.ctr->band_reserved, a.band, a.band_cap) + (pre >> 16);
-#pragma unroll
+#pragma unroll 1
                         for (int i = 0; i < 4; ++i) {
-                            uint32_t w = cmk[i] & ~imk[i];
+                            uint32_t w = i == 0 ? cmk0 & ~imk0 : i == 1 ? cmk1 & ~imk1 : i == 2 ? cmk2 & ~imk2
+                                                                                      : cmk3 & ~imk3;
                             const int col0 = (int)colbase + (cb_begin + i) * 32;
                             while (w) {
                                 const int k = __ffs(w) - 1;

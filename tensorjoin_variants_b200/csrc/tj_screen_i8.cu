@@ -503,6 +503,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
 // lanes 32 (w % 4).., all 128 columns in two passes of 64), so three warps per SM sub-partition
 // overlap their items' latency.
 constexpr int kHHStages = 6;                      // S k-blocks in flight (16 KB each)
+constexpr int kHHMeta = 8;                        // items of column metadata in flight (each group sees several)
 constexpr int kHHMaxKb = 2;                       // resident R k-blocks (kpad <= 256)
 constexpr int kHHAcc = 4;                         // TMEM accumulators of 128 columns
 constexpr int kHHEpi = 12;                        // three groups of four warps, taking alternate items
@@ -518,14 +519,14 @@ struct HHCtl {
     uint64_t empty[kHHStages];
     uint64_t acc_full[kHHAcc];
     uint64_t acc_empty[kHHAcc];
-    uint64_t meta_full[kI8Meta];
-    uint64_t meta_empty[kI8Meta];
+    uint64_t meta_full[kHHMeta];
+    uint64_t meta_empty[kHHMeta];
     uint64_t drain;
     unsigned tmem_base;
     int abort_flag;
 };
 
-constexpr size_t kHHSmem = 1024 + 2 * (size_t)kHHABytes + (size_t)kHHStages * kPart + kI8Meta * sizeof(ColMetaI8) +
+constexpr size_t kHHSmem = 1024 + 2 * (size_t)kHHABytes + (size_t)kHHStages * kPart + kHHMeta * sizeof(ColMetaI8) +
                            sizeof(HHCtl);
 static_assert(kHHSmem <= 232448, "227 KB of shared memory per CTA at most");
 
@@ -544,7 +545,7 @@ __global__ void __launch_bounds__(kHHThreads, 1)
     uint8_t* abuf = smem;                                       // 2 x kHHABytes
     uint8_t* bbuf = smem + 2 * (size_t)kHHABytes;               // kHHStages x kPart
     ColMetaI8* meta = (ColMetaI8*)(bbuf + (size_t)kHHStages * kPart);
-    HHCtl* ctl = (HHCtl*)(meta + kI8Meta);
+    HHCtl* ctl = (HHCtl*)(meta + kHHMeta);
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long* status = &a.ctr->status;
 
@@ -561,7 +562,7 @@ __global__ void __launch_bounds__(kHHThreads, 1)
             mbar_init(&ctl->acc_full[b], 1);
             mbar_init(&ctl->acc_empty[b], 4);   // the four warps of the item's epilogue group
         }
-        for (int m = 0; m < kI8Meta; ++m) {
+        for (int m = 0; m < kHHMeta; ++m) {
             mbar_init(&ctl->meta_full[m], 1);
             mbar_init(&ctl->meta_empty[m], 4);
         }
@@ -596,7 +597,7 @@ __global__ void __launch_bounds__(kHHThreads, 1)
                 for (unsigned e = ch.y; e < ch.z && ok; ++e, ++n) {
                     const unsigned J = a.jlist[e];
                     const int srow = (int)a.s_row0[J];
-                    const unsigned slot = (unsigned)(n % kI8Meta), mph = (unsigned)((n / kI8Meta) & 1);
+                    const unsigned slot = (unsigned)(n % kHHMeta), mph = (unsigned)((n / kHHMeta) & 1);
                     if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status, a.wait_ns)) { ok = false; break; }
                     mbar_arrive_expect_tx(&ctl->meta_full[slot], (unsigned)sizeof(ColMetaI8));
                     bulk_load(&meta[slot], a.s_meta + J, (unsigned)sizeof(ColMetaI8), &ctl->meta_full[slot]);
@@ -620,10 +621,10 @@ __global__ void __launch_bounds__(kHHThreads, 1)
                 const unsigned long long last = ((nc - 1 - ab) / 2) * 2 + ab;
                 mbar_wait(&ctl->a_full[ab], (unsigned)((last >> 1) & 1), status, kDrainLimitNs);
             }
-            for (int s = 0; s < kI8Meta; ++s) {
+            for (int s = 0; s < kHHMeta; ++s) {
                 if (n <= (unsigned long long)s) continue;
-                const unsigned long long last = ((n - 1 - s) / kI8Meta) * kI8Meta + s;
-                mbar_wait(&ctl->meta_full[s], (unsigned)((last / kI8Meta) & 1), status, kDrainLimitNs);
+                const unsigned long long last = ((n - 1 - s) / kHHMeta) * kHHMeta + s;
+                mbar_wait(&ctl->meta_full[s], (unsigned)((last / kHHMeta) & 1), status, kDrainLimitNs);
             }
         }
     } else if (warp == 1) {
@@ -687,7 +688,7 @@ __global__ void __launch_bounds__(kHHThreads, 1)
             for (unsigned e = ch.y; e < ch.z; ++e, ++n) {
                 if ((unsigned)(n % kHHGroups) != group) continue;
                 const unsigned b = (unsigned)(n & (kHHAcc - 1));
-                const unsigned slot = (unsigned)(n % kI8Meta), mph = (unsigned)((n / kI8Meta) & 1);
+                const unsigned slot = (unsigned)(n % kHHMeta), mph = (unsigned)((n / kHHMeta) & 1);
                 if (!__all_sync(0xffffffffu, mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns))) {
                     ok = false;
                     break;

@@ -5,8 +5,8 @@
 // output stage trims it to ceil(log2(max key + 2))).  Each pass is
 //   1. per-block digit histogram (digit-major [256][blocks]),
 //   2. device-wide exclusive scan of that table,
-//   3. stable scatter: every warp ranks its keys round by round with
-//      __match_any_sync, warps are combined in order through shared counters,
+//   3. stable scatter: every warp ranks its keys round by round (the lanes sharing a
+//      digit found by eight ballots), warps are combined in order through shared counters,
 //      the tile is regrouped by digit in shared memory and written out in runs.
 // Stability across passes makes the whole sort correct for any bit width.
 //
@@ -104,6 +104,19 @@ constexpr int kRsTile = kRsThreads * kRsRounds;       // 4096 keys per block
 
 TJ_DEV unsigned digit_of(uint64_t k, int shift) { return (unsigned)(k >> shift) & 0xFFu; }
 
+// Lanes of the warp (among `valid`) whose 8-bit digit equals this lane's, from eight ballots: a
+// peer agrees with the lane on every bit.  Every lane of the warp calls it.  Ballots and logic ops
+// run at full rate, where a match instruction over 32 arbitrary values does not.
+TJ_DEV unsigned digit_peers(unsigned dg, unsigned valid) {
+    unsigned peers = valid;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const unsigned m = __ballot_sync(0xffffffffu, (dg >> b) & 1u);
+        peers &= ((dg >> b) & 1u) ? m : ~m;
+    }
+    return peers;
+}
+
 __global__ void __launch_bounds__(kRsThreads) rs_hist(const uint64_t* keys, size_t n, int shift, uint32_t* hist,
                                                      unsigned nblocks) {
     __shared__ uint32_t h[256];
@@ -144,7 +157,7 @@ TJ_DEV uint32_t block_excl_scan(uint32_t v, uint32_t* warp_tot) {
 }
 
 // Stable scatter of one 4096-key tile.  Keys are ranked per warp (round by round with
-// __match_any_sync), the block's keys are regrouped by digit in shared memory, and then written
+// ballots), the block's keys are regrouped by digit in shared memory, and then written
 // out in that order, so consecutive threads store consecutive addresses of one digit's run
 // (about 16 keys = 128 B per digit and tile for 8-bit digits) instead of scattered 8-byte words.
 template <bool kVals>
@@ -178,15 +191,12 @@ __global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) rs_scatter(const ui
     for (int r = 0; r < kScRounds; ++r) {
         const bool ok = wbase + (size_t)r * 32 + lane < n;
         const unsigned valid = __ballot_sync(0xffffffffu, ok);
-        rank[r] = 0xFFFFFFFFu;
-        if (ok) {
-            const unsigned dg = digit_of(k[r], shift);
-            const unsigned peers = __match_any_sync(valid, dg);
-            const unsigned prev = wcnt[warp][dg];
-            rank[r] = prev + __popc(peers & lt);
-            __syncwarp(valid);
-            if ((peers & lt) == 0) wcnt[warp][dg] = prev + __popc(peers);
-        }
+        const unsigned dg = digit_of(k[r], shift);
+        const unsigned peers = digit_peers(dg, valid);
+        const unsigned prev = ok ? wcnt[warp][dg] : 0u;
+        rank[r] = ok ? prev + __popc(peers & lt) : 0xFFFFFFFFu;
+        __syncwarp();
+        if (ok && (peers & lt) == 0) wcnt[warp][dg] = prev + __popc(peers);
         __syncwarp();
     }
     if (kVals) {   // values load while the block meets at the barrier (fewer live registers above)
@@ -238,7 +248,7 @@ __global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) rs_scatter(const ui
 
 // Whole sort of a small array (n <= kSmallSort) in one CTA: per pass a histogram of all keys and
 // its scan give each digit's start, then the 4096-key chunks are ranked in order exactly as in
-// rs_scatter (16 warps, __match_any_sync) and written to their final positions; the running digit
+// rs_scatter (16 warps, ballot ranking) and written to their final positions; the running digit
 // starts carry stability across chunks.  Keys ping-pong through global memory (L2-resident at this
 // size); __syncthreads orders each pass's writes before the next pass's reads within the block.
 // One launch replaces the four to five launches per pass of the multi-block path.
@@ -279,15 +289,12 @@ __global__ void __launch_bounds__(kScThreads) rs_small(uint64_t* keys, uint32_t*
             for (int r = 0; r < kScRounds; ++r) {
                 const bool ok = wbase + r * 32 + lane < n;
                 const unsigned valid = __ballot_sync(0xffffffffu, ok);
-                rank[r] = 0xFFFFFFFFu;
-                if (ok) {
-                    const unsigned dg = digit_of(k[r], shift);
-                    const unsigned peers = __match_any_sync(valid, dg);
-                    const unsigned prev = wcnt[warp][dg];
-                    rank[r] = prev + __popc(peers & lt);
-                    __syncwarp(valid);
-                    if ((peers & lt) == 0) wcnt[warp][dg] = prev + __popc(peers);
-                }
+                const unsigned dg = digit_of(k[r], shift);
+                const unsigned peers = digit_peers(dg, valid);
+                const unsigned prev = ok ? wcnt[warp][dg] : 0u;
+                rank[r] = ok ? prev + __popc(peers & lt) : 0xFFFFFFFFu;
+                __syncwarp();
+                if (ok && (peers & lt) == 0) wcnt[warp][dg] = prev + __popc(peers);
                 __syncwarp();
             }
             __syncthreads();
@@ -325,20 +332,276 @@ __global__ void __launch_bounds__(kScThreads) rs_small(uint64_t* keys, uint32_t*
     }
 }
 
+// ------------------------------------------------------------------ single-sweep passes
+// For large arrays the digit histograms of all passes come from one read of the keys (os_hist), and
+// each pass is then one kernel (os_scatter): a tile takes the next tile number from a counter,
+// ranks its keys as rs_scatter does, publishes its per-digit counts, and walks back over the tiles
+// before it until it meets one that has published its inclusive prefix (a chained scan across the
+// tiles, each step adding a predecessor's counts).  Tile numbers follow the order in which blocks
+// start, so every tile a block waits on belongs to a block that is already running and publishes its
+// counts without waiting on anything; the walk is bounded all the same and sets the timeout bit if it
+// gives up.  Per pass the keys are read once and written once.
+constexpr uint64_t kOsAgg = 1ull << 62;   // status word: the tile's own count of the digit
+constexpr uint64_t kOsPre = 1ull << 63;   // status word: count of the digit over tiles 0..t
+constexpr uint64_t kOsVal = kOsAgg - 1;
+constexpr int kOsMaxPasses = 8;
+constexpr int kOsHistThreads = 512;
+constexpr int kOsHistKeys = 4;            // keys per thread whose loads are issued together
+
+__global__ void __launch_bounds__(kOsHistThreads) os_hist(const uint64_t* keys, size_t n, int passes,
+                                                          uint32_t* ghist) {
+    __shared__ uint32_t h[kOsMaxPasses][256];
+    for (int i = threadIdx.x; i < kOsMaxPasses * 256; i += kOsHistThreads) (&h[0][0])[i] = 0;
+    __syncthreads();
+    const unsigned lane = threadIdx.x & 31;
+    const size_t step = (size_t)gridDim.x * kOsHistThreads * kOsHistKeys;
+    // whole warps walk the array (indices past n count nothing), kOsHistKeys keys per thread, each
+    // warp's 32 keys of one load contiguous; a digit every lane of the warp shares (the high digits of
+    // nearly sorted keys) is added once instead of 32 times to one counter
+    for (size_t b = (size_t)blockIdx.x * kOsHistThreads * kOsHistKeys; b < n; b += step) {
+        uint64_t k[kOsHistKeys];
+#pragma unroll
+        for (int u = 0; u < kOsHistKeys; ++u) {
+            const size_t i = b + (size_t)u * kOsHistThreads + threadIdx.x;
+            k[u] = i < n ? keys[i] : 0ull;
+        }
+#pragma unroll
+        for (int u = 0; u < kOsHistKeys; ++u) {
+            const size_t i = b + (size_t)u * kOsHistThreads + threadIdx.x;
+            const bool ok = i < n;
+            const unsigned live = __ballot_sync(0xffffffffu, ok);
+            if (!live) continue;
+            for (int p = 0; p < passes; ++p) {
+                const unsigned dg = (unsigned)(k[u] >> (8 * p)) & 0xFFu;
+                const unsigned d0 = __shfl_sync(0xffffffffu, dg, 0);   // lane 0 is live whenever any lane is
+                if (__all_sync(0xffffffffu, !ok || dg == d0)) {
+                    if (lane == 0) atomicAdd(&h[p][d0], (unsigned)__popc(live));
+                } else if (ok) {
+                    atomicAdd(&h[p][dg], 1u);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += kOsHistThreads) {
+        const uint32_t c = (&h[0][0])[i];
+        if (c) atomicAdd(&ghist[i], c);
+    }
+}
+
+// Per pass: the exclusive prefix of the 256 digit counts (one block of 256 threads per pass).
+__global__ void __launch_bounds__(256) os_starts(const uint32_t* ghist, uint32_t* gstart) {
+    __shared__ uint32_t wtot[8];
+    const uint32_t v = ghist[blockIdx.x * 256 + threadIdx.x];
+    gstart[blockIdx.x * 256 + threadIdx.x] = block_excl_scan<8>(v, wtot);
+}
+
+TJ_DEV uint64_t ld_status(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+TJ_DEV void st_status(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
+
+template <bool kVals>
+__global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) os_scatter(const uint64_t* keys_in, const uint32_t* vals_in,
+                                                        uint64_t* keys_out, uint32_t* vals_out, size_t n, int shift,
+                                                        const uint32_t* gstart, uint64_t* tstat, uint32_t* tile_ctr,
+                                                        unsigned long long* status) {
+    extern __shared__ __align__(16) unsigned char rs_dyn[];
+    uint64_t* sk = (uint64_t*)rs_dyn;                      // [kRsTile] keys grouped by digit
+    uint32_t* sv = (uint32_t*)(rs_dyn + kRsTile * 8);      // [kRsTile] values (kVals)
+    __shared__ uint32_t wcnt[kScWarps][256];   // per warp and digit: count, then tile-local start
+    __shared__ uint32_t gdelta[256];   // global start minus tile-local start of each digit's run (mod 2^32)
+    __shared__ uint32_t wtot[kScWarps];
+    __shared__ uint32_t tile_sh;
+    __shared__ int gave_up;   // a look-back ran out of time: this tile writes nothing
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        tile_sh = atomicAdd(tile_ctr, 1u);
+        gave_up = 0;
+    }
+    for (int i = threadIdx.x; i < kScWarps * 256; i += kScThreads) (&wcnt[0][0])[i] = 0;
+    __syncthreads();
+    const unsigned t = tile_sh;
+
+    const size_t tbase = (size_t)t * kRsTile;
+    const size_t wbase = tbase + (size_t)warp * (kScRounds * 32);
+    uint64_t k[kScRounds];
+    uint32_t v[kScRounds];
+    uint32_t rank[kScRounds];
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < kScRounds; ++r) {
+        const size_t i = wbase + (size_t)r * 32 + lane;
+        k[r] = i < n ? keys_in[i] : 0ull;
+    }
+#pragma unroll
+    for (int r = 0; r < kScRounds; ++r) {
+        const bool ok = wbase + (size_t)r * 32 + lane < n;
+        const unsigned valid = __ballot_sync(0xffffffffu, ok);
+        const unsigned dg = digit_of(k[r], shift);
+        const unsigned peers = digit_peers(dg, valid);
+        const unsigned prev = ok ? wcnt[warp][dg] : 0u;
+        rank[r] = ok ? prev + __popc(peers & lt) : 0xFFFFFFFFu;
+        __syncwarp();
+        if (ok && (peers & lt) == 0) wcnt[warp][dg] = prev + __popc(peers);
+        __syncwarp();
+    }
+    if (kVals) {
+#pragma unroll
+        for (int r = 0; r < kScRounds; ++r) {
+            const size_t i = wbase + (size_t)r * 32 + lane;
+            v[r] = i < n ? vals_in[i] : 0u;
+        }
+    }
+    __syncthreads();
+    {   // per digit (threads 0..255): the tile's count, its tile-local start, each warp's start, and
+        // the digit's global start from the chained scan over the tiles before this one
+        const unsigned dg = threadIdx.x;
+        uint32_t run = 0;
+        if (dg < 256) {
+#pragma unroll
+            for (int w = 0; w < kScWarps; ++w) run += wcnt[w][dg];
+        }
+        const uint32_t ls = block_excl_scan<kScWarps>(run, wtot);
+        if (dg < 256) {
+            uint32_t at = ls;
+#pragma unroll
+            for (int w = 0; w < kScWarps; ++w) {
+                const uint32_t c = wcnt[w][dg];
+                wcnt[w][dg] = at;
+                at += c;
+            }
+            uint64_t* mine = tstat + (size_t)t * 256 + dg;
+            uint64_t excl = 0;
+            if (t == 0) {
+                st_status(mine, (uint64_t)run | kOsPre);
+            } else {
+                st_status(mine, (uint64_t)run | kOsAgg);
+                long long j = (long long)t - 1;
+                unsigned spins = 0;
+                unsigned long long t0 = 0;
+                while (true) {
+                    const uint64_t w = ld_status(tstat + (size_t)j * 256 + dg);
+                    if (w & (kOsPre | kOsAgg)) {
+                        excl += w & kOsVal;
+                        if ((w & kOsPre) || j == 0) break;   // tile 0 always publishes a prefix
+                        --j;
+                        continue;
+                    }
+                    if (++spins == 64) t0 = global_ns();
+                    if (spins > 64) {
+                        __nanosleep(32);
+                        if (global_ns() - t0 > kWaitLimitNs) {
+                            atomicOr(status, (unsigned long long)kStatusWaitTimeout);
+                            gave_up = 1;
+                            break;
+                        }
+                    }
+                }
+                st_status(mine, (excl + run) | kOsPre);
+            }
+            gdelta[dg] = gstart[dg] + (uint32_t)excl - ls;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kScRounds; ++r) {
+        if (rank[r] != 0xFFFFFFFFu) {
+            const unsigned p = wcnt[warp][digit_of(k[r], shift)] + rank[r];
+            sk[p] = k[r];
+            if (kVals) sv[p] = v[r];
+        }
+    }
+    __syncthreads();
+    if (gave_up) return;
+    const unsigned cnt = (unsigned)min((size_t)kRsTile, n - tbase);
+    bool outside = false;
+    for (unsigned p = threadIdx.x; p < cnt; p += kScThreads) {
+        const uint64_t key = sk[p];
+        const size_t pos = (size_t)(uint32_t)(gdelta[digit_of(key, shift)] + p);
+        if (pos >= n) {   // cannot happen with consistent counts; checked so that nothing lands outside
+            outside = true;
+            continue;
+        }
+        keys_out[pos] = key;
+        if (kVals) vals_out[pos] = sv[p];
+    }
+    if (outside) atomicOr(status, (unsigned long long)kStatusGuard);
+}
+
 }  // namespace
 
 size_t radix_workspace_elems(size_t n) {
     const size_t nb = (n + kRsTile - 1) / kRsTile;
     const size_t h = 256 * nb;
-    return 2 * h + scan_workspace_elems(h) + 16;
+    // the multi-pass layout (two digit tables and a scan) or the single-sweep one (a 64-bit status
+    // word per tile and digit, the histograms and starts of all passes, the tile counter), whichever
+    // is larger, plus alignment slack
+    return std::max(2 * h + scan_workspace_elems(h), 2 * h + 2 * kOsMaxPasses * 256 + 64) + 16;
 }
 
-// Sorts (keys, vals) ascending by the low `bits` bits of keys.  Result lands in keys/vals
-// (ping-pong through keys_tmp/vals_tmp).  vals may be null.  ws: radix_workspace_elems(n) u32.
+// Sorts (keys, vals) ascending by the low `bits` bits of keys, ping-ponging through
+// keys_tmp/vals_tmp.  vals may be null.  ws: radix_workspace_elems(n) u32.  With a status word
+// (device), arrays of more than kOneSweepMin keys take the single-sweep passes, whose bounded
+// look-back sets kStatusWaitTimeout there if it ever gives up.  With `in_tmp`, a result that ends in
+// the temporaries after an odd number of passes stays there and *in_tmp is set (the caller swaps its
+// buffers); without it the result is copied back into keys/vals.
+constexpr size_t kOneSweepMin = (size_t)1 << 20;
+
 void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp, size_t n, int bits,
-                uint32_t* ws, cudaStream_t st) {
+                uint32_t* ws, cudaStream_t st, unsigned long long* status, bool* in_tmp) {
+    if (in_tmp) *in_tmp = false;
     if (n <= 1 || bits <= 0) return;
     if (n >= (1ull << 32)) fail(-1, "radix_sort: more than 2^32 - 1 keys");
+    if (status && n > kOneSweepMin) {
+        const int passes = (bits + 7) / 8;
+        const size_t dyn_k = (size_t)kRsTile * 8, dyn_kv = (size_t)kRsTile * 12;
+        TJ_CUDA(cudaFuncSetAttribute(os_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_k));
+        TJ_CUDA(cudaFuncSetAttribute(os_scatter<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        if (vals) {
+            TJ_CUDA(cudaFuncSetAttribute(os_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_kv));
+            TJ_CUDA(cudaFuncSetAttribute(os_scatter<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        }
+        const unsigned nb = (unsigned)((n + kRsTile - 1) / kRsTile);
+        uint64_t* tstat = (uint64_t*)(((uintptr_t)ws + 15) & ~(uintptr_t)15);   // [nb][256]
+        uint32_t* ghist = (uint32_t*)(tstat + (size_t)nb * 256);                // [passes][256]
+        uint32_t* gstart = ghist + kOsMaxPasses * 256;                           // [passes][256]
+        uint32_t* ctr = gstart + kOsMaxPasses * 256;                              // [passes]
+        TJ_CUDA(cudaMemsetAsync(ghist, 0, (size_t)passes * 256 * sizeof(uint32_t), st));
+        TJ_CUDA(cudaMemsetAsync(ctr, 0, (size_t)passes * sizeof(uint32_t), st));
+        const unsigned hb = (unsigned)std::min<size_t>((size_t)num_sms() * 4,
+                                                       (n + kOsHistThreads * kOsHistKeys - 1) /
+                                                           (kOsHistThreads * kOsHistKeys));
+        launch(os_hist, hb, kOsHistThreads, 0, st, (const uint64_t*)keys, n, passes, ghist);
+        launch(os_starts, (unsigned)passes, 256, 0, st, (const uint32_t*)ghist, gstart);
+        uint64_t *kin = keys, *kout = keys_tmp;
+        uint32_t *vin = vals, *vout = vals_tmp;
+        for (int p = 0; p < passes; ++p) {
+            TJ_CUDA(cudaMemsetAsync(tstat, 0, (size_t)nb * 256 * sizeof(uint64_t), st));
+            if (vals)
+                launch(os_scatter<true>, nb, kScThreads, dyn_kv, st, (const uint64_t*)kin, (const uint32_t*)vin, kout,
+                       vout, n, 8 * p, (const uint32_t*)(gstart + p * 256), tstat, ctr + p, status);
+            else
+                launch(os_scatter<false>, nb, kScThreads, dyn_k, st, (const uint64_t*)kin, (const uint32_t*)nullptr,
+                       kout, (uint32_t*)nullptr, n, 8 * p, (const uint32_t*)(gstart + p * 256), tstat, ctr + p,
+                       status);
+            std::swap(kin, kout);
+            std::swap(vin, vout);
+        }
+        if (kin != keys) {
+            if (in_tmp) {
+                *in_tmp = true;
+            } else {
+                TJ_CUDA(cudaMemcpyAsync(keys, kin, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+                if (vals) TJ_CUDA(cudaMemcpyAsync(vals, vin, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+            }
+        }
+        return;
+    }
     if (n <= kSmallSort) {
         const int passes = (bits + 7) / 8;
         if (vals)
