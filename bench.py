@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--index-frame", default="auto", choices=["auto", "axes", "pca"],
                     help="cells the rows are sorted by before tiling (default: the library's choice)")
     ap.add_argument("--band-fp32", action="store_true", help="certified FP32 band stage before the FP64 terminal")
+    ap.add_argument("--untuned", action="store_true",
+                    help="library defaults instead of the committed tuning table's knobs for each configuration")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle audit after the timed steps")
@@ -371,6 +373,48 @@ def cpu_baseline_leg(R: np.ndarray, S: np.ndarray, T, rows: int, full_pairs: int
                       f"{secs[0]:.1f} s; full join extrapolated {full_pairs / rate:.0f} s"}
 
 
+# ---------------------------------------------------------------------- tuned knobs
+def tuned_knobs(args, R, S, T, mode: str, screen: str) -> tuple[dict, str | None]:
+    """Knobs the committed B200 tuning table holds for this join and its fixed screen (tile shape,
+    half-tile packing, chunking, cell frame, FP32 band stage); {} on a miss or with --untuned.
+    --index-frame and --band-fp32 given on the command line win over the table."""
+    from tensorjoin_variants_b200 import autotune
+
+    kw: dict = {}
+    key = None
+    if not args.untuned:
+        table = autotune.default_table()
+        key = table.key_for(R, S, T, mode, screen)
+        choice = table.lookup(key)
+        if choice is not None and not choice.screen:
+            kw = choice.kwargs()
+    if args.index_frame != "auto":
+        kw["index_frame"] = args.index_frame
+    if args.band_fp32:
+        kw["band_fp32"] = True
+    return kw, key
+
+
+def tuned_batch_knobs(args, joins, screen: str) -> tuple[dict, str | None]:
+    """The same for a batch of joins (``autotune.Tuner.batch_key``)."""
+    from tensorjoin_variants_b200 import autotune
+
+    kw: dict = {}
+    key = None
+    if not args.untuned:
+        table = autotune.default_table()
+        key = table.batch_key(joins, screen)
+        choice = table.lookup(key)
+        if choice is not None and not choice.screen:
+            kw = choice.kwargs()
+            kw.pop("i8_four_products")
+    if args.index_frame != "auto":
+        kw["index_frame"] = args.index_frame
+    if args.band_fp32:
+        kw["band_fp32"] = True
+    return kw, key
+
+
 # ---------------------------------------------------------------------- one single-join configuration
 def bench_single(name: str, args, steps: int, warmup: int, rank: int, world: int, dist, headline: bool) -> dict:
     import torch
@@ -387,9 +431,10 @@ def bench_single(name: str, args, steps: int, warmup: int, rank: int, world: int
     T = w.T
     d = int(w.R.shape[1])
 
+    knobs, tkey = tuned_knobs(args, R, S, T, mode, screen)
+
     def step():
-        res = tj.join_result(R, S, eps2=T, mode=mode, screen=screen, index_frame=args.index_frame,
-                             band_fp32=args.band_fp32)
+        res = tj.join_result(R, S, eps2=T, mode=mode, screen=screen, **knobs)
         i, j = res.pairs()
         return res, i, j
 
@@ -460,8 +505,7 @@ def bench_single(name: str, args, steps: int, warmup: int, rank: int, world: int
         line["screen_error"] = {"max_abs_err_d2": 0, "note": "exact integer screen (int8 limbs, INT64 recombination)"}
 
     # the GPU result once more, for the plain comparison and the oracle audit
-    res = tj.join_result(R, S, eps2=T, mode=mode, screen=screen, index_frame=args.index_frame,
-                         band_fp32=args.band_fp32)
+    res = tj.join_result(R, S, eps2=T, mode=mode, screen=screen, **knobs)
     keys_t = res.keys()
     del res
 
@@ -489,26 +533,29 @@ def bench_single(name: str, args, steps: int, warmup: int, rank: int, world: int
     if not args.no_e2e:
         Rh = torch.from_numpy(w.R).pin_memory()
         Sh = None if w.S is None else torch.from_numpy(w.S).pin_memory()
-        fn = (lambda: tj.join(Rh, Sh, eps2=T, screen=screen)) if mode == "rs" else \
-            (lambda: tj.self_join(Rh, eps2=T, mode=mode, screen=screen))
+        fn = (lambda: tj.join(Rh, Sh, eps2=T, screen=screen, **knobs)) if mode == "rs" else \
+            (lambda: tj.self_join(Rh, eps2=T, mode=mode, screen=screen, **knobs))
         for _ in range(max(3, warmup)):   # warm-up: the pinned host buffers reach the allocator's cache
             ih, jh = fn()
         torch.cuda.synchronize()
         k_e2e = max(1, min(steps, 3))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(k_e2e):
+        d2h = 0
+        for _ in range(k_e2e):   # each step's host outputs are dropped before the next step allocates its own
             ih, jh = fn()
+            d2h = 16 * len(ih)
+            del ih, jh
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1) / k_e2e
         ems = max_over_ranks(ems, world, dist)
         h2d = Rh.numel() * Rh.element_size() + (0 if Sh is None else Sh.numel() * Sh.element_size())
         line["e2e"] = {"value": world * pairs / (ems / 1000.0), "unit": UNIT, "ms_per_step": ems,
-                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(16 * len(ih)),
+                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                        "api": ("tensorjoin_variants_b200.join" if mode == "rs" else "tensorjoin_variants_b200.self_join")
                               + "(host pinned inputs) -> host (i, j)"}
-        del Rh, Sh, ih, jh
+        del Rh, Sh
 
     keys = _keys_np(keys_t)
     del keys_t, R, S
@@ -522,38 +569,6 @@ def bench_single(name: str, args, steps: int, warmup: int, rank: int, world: int
 
 
 # ---------------------------------------------------------------------- config 5: batched ragged joins
-def ragged_device(joins=4096, lo=256, hi=65536, dims=(8, 32, 128), clusters=8, std=0.05, degree=16, seed=5,
-                  size_scale=1.0):
-    """Config-5 data drawn on the GPU (seeded torch CUDA generator): per dimension class one bulk draw,
-    every join a contiguous slice.  Same shapes and distributions as workloads.ragged4096."""
-    import torch
-    from tensorjoin_variants_b200 import workloads as W
-
-    rng = np.random.default_rng(seed)
-    nr = np.maximum(1, np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), joins)) * size_scale)).astype(np.int64)
-    ns = np.maximum(1, np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), joins)) * size_scale)).astype(np.int64)
-    dj = rng.choice(np.asarray(dims), joins)
-    g = torch.Generator(device="cuda").manual_seed(seed)
-    out = [dict() for _ in range(joins)]
-    classes = []
-    for d in dims:
-        ks = np.flatnonzero(dj == d)
-        if len(ks) == 0:
-            continue
-        centres = torch.from_numpy(rng.random((len(ks), clusters, d)).astype(np.float32)).cuda()
-        for side, counts in (("R", nr[ks]), ("S", ns[ks])):
-            total = int(counts.sum())
-            owner = torch.from_numpy(np.repeat(np.arange(len(ks)), counts)).cuda()
-            label = torch.randint(0, clusters, (total,), generator=g, device="cuda")
-            X = torch.randn((total, d), generator=g, device="cuda") * std + centres[owner, label]
-            classes.append(X)
-            offs = np.concatenate([[0], np.cumsum(counts)])
-            for q, k in enumerate(ks):
-                out[k][side] = X[int(offs[q]):int(offs[q + 1])]
-    eps = [math.sqrt(W.ragged_eps2(int(ns[k]), int(dj[k]), clusters, std, degree)) for k in range(joins)]
-    return [(out[k]["R"], out[k]["S"], eps[k]) for k in range(joins)], classes
-
-
 def ragged_audit(joins, result, count: int, seed: int = 2025) -> dict:
     """`count` seeded joins of the batch, each checked exhaustively by the CPU oracle against the
     batch result's range for that join (local (i, j) keys i * |S| + j)."""
@@ -588,16 +603,19 @@ def bench_ragged(args, steps: int, warmup: int, rank, world, dist, headline: boo
 
     import tensorjoin_variants_b200 as tj
     from tensorjoin_variants_b200 import _lib
+    from tensorjoin_variants_b200 import workloads as W
 
     screen = (args.screen if headline else None) or WORKLOADS["ragged4096"]["screen"]
     scale = (args.n / 11_800 if args.n else 1.0) if headline else 1.0   # --n sets the mean side length
-    joins, classes = ragged_device(size_scale=scale)
+    joins, classes = W.ragged4096_device(size_scale=scale)
     torch.cuda.synchronize()
     nj = len(joins)
     stream = torch.cuda.current_stream()
 
+    knobs, tkey = tuned_batch_knobs(args, joins, screen)
+
     def step(scr):
-        return tj.join_batched_result(joins, screen=scr, band_fp32=args.band_fp32)
+        return tj.join_batched_result(joins, screen=scr, **knobs)
 
     for _ in range(warmup):
         r = step(screen)
@@ -683,7 +701,7 @@ def bench_ragged(args, steps: int, warmup: int, rank, world, dist, headline: boo
                                 "refined_fraction": sd["band"] / max(1, sd["pairs_screened"])}
         del rd
     if screen != "plain":   # per-join spans inside one batched screen launch, and the CTAs' idle tail
-        rt_ = tj.join_batched_result(joins, screen=screen, screen_times=True)
+        rt_ = tj.join_batched_result(joins, screen=screen, screen_times=True, **knobs)
         stt = rt_.stats
         line["batch"].update({"in_batch_join_span_ms_p50": stt["join_span_ms_p50"],
                               "in_batch_join_span_ms_p99": stt["join_span_ms_p99"],
@@ -706,23 +724,34 @@ def bench_ragged(args, steps: int, warmup: int, rank, world, dist, headline: boo
                              "identical_pair_set": bool(torch.equal(rp.keys(), r.keys()))}
         del rp
     if not args.no_e2e:   # host-resident batch: every join's rows from pinned host memory, pairs back to the host
-        hj = [(Rd.cpu().pin_memory(), Sd.cpu().pin_memory(), e) for Rd, Sd, e in joins]
+        # (each join's R and S are views of a few pinned host arrays, one per dimension class and side,
+        # as a caller holding its batch in a few large arrays has them)
+        pins = {X.untyped_storage().data_ptr(): X.cpu().pin_memory() for X in classes}
+
+        def host_view(t):
+            P = pins[t.untyped_storage().data_ptr()].view(-1)
+            return P[t.storage_offset():t.storage_offset() + t.numel()].view(t.shape)
+
+        hj = [(host_view(Rd), host_view(Sd), e) for Rd, Sd, e in joins]
         for _ in range(max(1, min(warmup, 2))):
-            tj.join_batched_result(hj, screen=screen).pairs()
+            tj.join_batched_result(hj, screen=screen, **knobs).pairs()
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         k_e2e = 2
-        for _ in range(k_e2e):
-            ih, jh = tj.join_batched_result(hj, screen=screen).pairs()
+        d2h = 0
+        for _ in range(k_e2e):   # each step's host outputs are dropped before the next step allocates its own
+            ih, jh = tj.join_batched_result(hj, screen=screen, **knobs).pairs()
+            d2h = 16 * len(ih)
+            del ih, jh
         b.record(stream)
         torch.cuda.synchronize()
         ems = a.elapsed_time(b) / k_e2e
-        h2d = sum(x.numel() * 4 + y.numel() * 4 for x, y, _ in hj)
+        h2d = sum(P.numel() * 4 for P in pins.values())
         line["e2e"] = {"value": world * pairs / (ems / 1000.0), "unit": UNIT, "ms_per_step": ems,
-                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(16 * len(ih)),
+                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                        "api": "tensorjoin_variants_b200.join_batched_result(host pinned joins).pairs() -> host (i, j)"}
-        del hj
+        del hj, pins
     if rank == 0 and world == 1 and not args.no_parity:
         line["parity"] = ragged_audit(joins, r, WORKLOADS["ragged4096"]["audit_rows"])
     if rank == 0 and world == 1 and not args.no_cpu:   # the reference's CPU path on one seeded join's rows

@@ -209,7 +209,9 @@ def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "b
                            cta_pair=cta_pair and kw["cta_pair"],
                            index_frame=index_frame if index_frame != "auto" else kw["index_frame"],
                            band_fp32=band_fp32 or kw["band_fp32"], guards=guards, stage_keys=stage_keys,
-                           screen_times=screen_times, k_block=k_block or kw["k_block"], stages=stages or kw["stages"])
+                           screen_times=screen_times, k_block=k_block or kw["k_block"], stages=stages or kw["stages"],
+                           half_pack=half_pack and kw["half_pack"],
+                           i8_four_products=i8_four_products or kw["i8_four_products"])
     flags = (_lib.FLAG_SCREEN_DIAG if screen_diag else 0) | (0 if cta_pair else _lib.FLAG_SCREEN_1SM)
     flags |= FRAME_FLAGS[index_frame] | (_lib.FLAG_BAND_FP32 if band_fp32 else 0)
     flags |= _lib.FLAG_I8_FOUR_PRODUCTS if i8_four_products else 0
@@ -222,12 +224,7 @@ def join_result(R, S, eps=None, *, eps2=None, mode: str = "rs", screen: str = "b
 def join(R, S, eps=None, *, eps2=None, screen: str = "bf16", return_stats: bool = False, **kw):
     """R-S epsilon-join: sorted (i, j) with FP64 direct-difference distance <= eps
     (``screen="auto"``: the tuned choice, see ``join_result``)."""
-    if screen == "auto":
-        res = join_result(R, S, eps, eps2=eps2, mode="rs", screen="auto", capacity=kw.get("capacity", 0),
-                          chunk_items=kw.get("chunk_items", 0))
-        i, j = res.pairs()
-        return (i, j, res.stats) if return_stats else (i, j)
-    res = _run(R, S, eps, eps2, "rs", screen, kw.get("capacity", 0), kw.get("chunk_items", 0))
+    res = join_result(R, S, eps, eps2=eps2, mode="rs", screen=screen, **kw)
     i, j = res.pairs()
     return (i, j, res.stats) if return_stats else (i, j)
 
@@ -237,7 +234,7 @@ def self_join(X, eps=None, *, eps2=None, mode: str = "upper", screen: str = "bf1
     """Self-join: mode 'upper' gives i < j; 'directed' gives all (i, j) incl. the N self pairs."""
     if mode not in ("upper", "directed"):
         raise ValueError("self_join mode must be 'upper' or 'directed'")
-    res = _run(X, None, eps, eps2, mode, screen, kw.get("capacity", 0), kw.get("chunk_items", 0))
+    res = join_result(X, None, eps, eps2=eps2, mode=mode, screen=screen, **kw)
     i, j = res.pairs()
     return (i, j, res.stats) if return_stats else (i, j)
 
@@ -305,6 +302,33 @@ class BatchResult(Result):
         return [(i[o[k]:o[k + 1]], j[o[k]:o[k + 1]]) for k in range(self.njoins)]
 
 
+def _host_views_to_device(xs):
+    """Host tensors that are contiguous 2-D views of one host array (the rows of many joins in a few
+    large arrays) go to the device in one copy per array: the span the views cover is copied once
+    and each view becomes the matching device view, so views that lie back to back on the host stay
+    back to back on the device (the batched join then reads them in place).  Returns, per input,
+    ``(device tensor, True)`` or None for inputs left to ``_as_device``."""
+    out = [None] * len(xs)
+    groups: dict = {}
+    for q, x in enumerate(xs):
+        if (isinstance(x, torch.Tensor) and not x.is_cuda and x.dim() == 2 and x.is_contiguous()
+                and x.dtype == torch.float32):
+            groups.setdefault(x.untyped_storage().data_ptr(), []).append(q)
+    for idx in groups.values():
+        if len(idx) < 2:
+            continue
+        first = xs[idx[0]]
+        lo = min(xs[q].storage_offset() for q in idx)
+        hi = max(xs[q].storage_offset() + xs[q].numel() for q in idx)
+        span = torch.empty(0, dtype=first.dtype).set_(first.untyped_storage(), lo, (hi - lo,), (1,))
+        dev = span.to("cuda", non_blocking=span.is_pinned())
+        for q in idx:
+            x = xs[q]
+            o = x.storage_offset() - lo
+            out[q] = (dev[o:o + x.numel()].view(x.shape), True)
+    return out
+
+
 def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_items: int = 0,
                         index_frame: str = "auto", band_fp32: bool = False,
                         screen_diag: bool = False, screen_times: bool = False, guards: bool = False,
@@ -320,9 +344,10 @@ def join_batched_result(joins, screen: str = "bf16", capacity: int = 0, chunk_it
     descs = (_lib.BatchJoin * len(joins))()
     keep = []
     host = True
+    moved = _host_views_to_device([x for R, S, _ in joins for x in (R, S)])
     for k, (R, S, eps) in enumerate(joins):
-        Rt, hr = _as_device(R, False)
-        St, hs = _as_device(S, False)
+        Rt, hr = moved[2 * k] if moved[2 * k] is not None else _as_device(R, False)
+        St, hs = moved[2 * k + 1] if moved[2 * k + 1] is not None else _as_device(S, False)
         host = host and hr and hs
         keep += [Rt, St]
         descs[k] = _lib.BatchJoin(Rt.data_ptr(), St.data_ptr(), Rt.shape[0], St.shape[0], Rt.shape[1], 0,

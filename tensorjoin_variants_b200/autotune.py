@@ -272,14 +272,25 @@ class Tuner:
         return api.join_result(R, S, eps2=T, mode=mode, screen=choice.screen_for(screen), **choice.kwargs())
 
     # ---------------------------------------------------------------- batched joins
-    def join_batched(self, joins, screen: str = "bf16x3", sample_joins: int = 64, reps: int = 2):
-        """Tuned batched join: the choice is searched on a seeded sample of the batch's joins (the
-        batch's own mix of sizes and dimensions), keyed by the dimensions present, the requested
-        screen, the number of joins and the log2 of the batch's pair space."""
+    @staticmethod
+    def batch_key(joins, screen: str) -> str:
+        """Key of a batch: the dimensions present, the requested screen, the number of joins and the
+        log2 of the batch's pair space."""
         dims = sorted({int(j[0].shape[1]) for j in joins})
         space = sum(int(j[0].shape[0]) * int(j[1].shape[0]) for j in joins)
-        key = (f"batch/d{'-'.join(map(str, dims))}/f32/{screen}/joins2^{int(round(math.log2(max(1, len(joins)))))}"
-               f"/space2^{int(round(math.log2(max(1, space))))}")
+        return (f"batch/d{'-'.join(map(str, dims))}/f32/{screen}/joins2^{int(round(math.log2(max(1, len(joins)))))}"
+                f"/space2^{int(round(math.log2(max(1, space))))}")
+
+    def batch_choice(self, joins, screen: str):
+        """This table's (then the committed table's) choice for the batch, or None; no tuning."""
+        key = self.batch_key(joins, screen)
+        return self.lookup(key) or default_table().lookup(key)
+
+    def join_batched(self, joins, screen: str = "bf16x3", sample_joins: int = 64, reps: int = 2):
+        """Tuned batched join: the choice is searched on a seeded sample of the batch's joins (the
+        batch's own mix of sizes and dimensions), keyed as ``batch_key``."""
+        dims = sorted({int(j[0].shape[1]) for j in joins})
+        key = self.batch_key(joins, screen)
         choice = self.lookup(key) or default_table().lookup(key)
         if choice is None:
             g = torch.Generator().manual_seed(len(joins))
@@ -324,6 +335,10 @@ def _produce(path: str, sample_rows: int) -> None:
         choice, key = t.choose(R, S, float(w.T), mode, screen, sample_rows)
         print(f"{name} {screen}: {key} -> {choice}", flush=True)
         del R, S
+    joins, classes = W.ragged4096_device()
+    _, choice = t.join_batched(joins, "bf16x3")
+    print(f"ragged4096 bf16x3: {t.batch_key(joins, 'bf16x3')} -> {choice}", flush=True)
+    del joins, classes
     print(json.dumps(t.table, indent=1, sort_keys=True))
 
 

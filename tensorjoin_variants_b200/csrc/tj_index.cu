@@ -820,11 +820,13 @@ struct TileOut {
 };
 
 // Operand preparation and tile statistics in one pass, for 16-bit screens over FP32 rows with
-// d % 4 == 0 and kpad = 4 kL <= 128 (one block per tile of 128 or 256 sorted rows; kL lanes per row,
-// each lane four consecutive elements).  Every gathered row is read from HBM once: the row's
-// operands, norms and bounds, and the tile's centroid and box partials come from that read; the
-// radius pass reads the tile again while it is still in L2.  With kHalves the statistics of the two
-// 128-row halves of a 256-row tile are written as well (tile t, half h -> entry 2 t + h of H).
+// d % 4 == 0 and kpad = kE kL <= 128 (one block of 256 threads per tile of 128 or 256 sorted rows;
+// kL lanes per row, each lane kE consecutive elements).  Every gathered row is read from HBM once:
+// the row's operands, norms and bounds, and the tile's centroid and box partials come from that
+// read; the radius pass reads the tile again while it is still in L2.  With kHalves the statistics
+// of the two 128-row halves of a 256-row tile are written as well (tile t, half h -> entry 2 t + h
+// of H).  Partials are combined across the row groups of a warp by shuffles and across the eight
+// warps in shared memory.
 //
 // Arithmetic.  x' = x - c is carried exactly as s + err (s = fl32(x - c), err from TwoSum), so the
 // operands and the bounds need no FP64 conversions per element:
@@ -834,9 +836,11 @@ struct TileOut {
 // E >= ||x' - z||, Zl >= ||z_lo|| and the tile radius are FP32 sums of squares made rigorous upper
 // bounds: each term is exact or rounded once (relative 2^-24; additions are exact in the subnormal
 // range, a product that underflows errs by at most 2^-150), a chain of m <= d + 5 roundings errs by at
-// most gamma_m, so  true <= (S + d 2^-140) (1 + (d + 16) 2^-23),  and the square root is taken in FP64
-// and rounded up.  The centroid needs no accuracy (the radius is measured from the value written).
-template <int kScreen, int kSplit, int kL, bool kHalves>
+// most gamma_m, so  true <= (S + d 2^-140) (1 + (d + 16) 2^-23);  that widening and the square root
+// are taken with upward rounding (FP32 .ru operations), as is Y = sqrt(A (1 + 2 g)).  A non-finite
+// element makes A non-finite, which flags the row.  The centroid needs no accuracy (the radius is
+// measured from the value written).
+template <int kScreen, int kSplit, int kE, int kL, bool kHalves>
 __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict__ src, long long n, int d, int tile,
                                                          const uint32_t* __restrict__ perm,
                                                          const float* __restrict__ center,
@@ -845,92 +849,102 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
                                                          float* en, float* yn, float* zl, TileOut T, TileOut H,
                                                          unsigned long long* status) {
     constexpr int kFmt = (kScreen == kScreenBF16 || kScreen == kScreenBF16X3) ? 1 : 0;
-    constexpr int kPad = 4 * kL;
+    constexpr int kPad = kE * kL;
     constexpr int kNG = 256 / kL;              // row groups per block
     constexpr int kRows = 128 / kNG;           // rows of one group in one 128-row half
-    constexpr int kU = kRows < 4 ? kRows : 4;  // rows whose loads are issued together
+    constexpr int kU = kRows < 2 ? kRows : 2;  // rows whose loads are issued together
+    constexpr int kV = kE / 4;                 // float4 loads per lane and row
     constexpr int opw = kSplit ? 2 * kPad : kPad;
-    __shared__ float psum[2][1024], pmin[2][1024], pmax[2][1024];   // [half][group * kPad + element]
-    __shared__ float rmx[2][6][kNG];        // [half][bound][group] row-bound maxima
-    __shared__ float cs[3][kPad];           // centroids: tile, half 0, half 1
-    __shared__ float radm[3][kNG];          // per-group maxima of the radius sums
+    static_assert(kE % 4 == 0 && kPad <= 128 && kL >= 4 && kL <= 32, "fused preparation shape");
+    __shared__ float wsum[2][8][kPad], wmin[2][8][kPad], wmax[2][8][kPad];   // [half][warp][element]
+    __shared__ float wrow[2][6][8];          // [half][bound][warp] row-bound maxima
+    __shared__ float wrad[3][8];             // [tile, half 0, half 1][warp] radius-sum maxima
+    __shared__ float cs[3][kPad];            // centroids: tile, half 0, half 1
     const int t = blockIdx.x;
     const bool tabled = row0_in != nullptr;
     const long long r0 = tabled ? (long long)row0_in[t] : (long long)t * tile;
     const int nv = tabled ? (int)nvalid_in[t] : (int)min((long long)tile, n - r0);
     const int halves = tile == 256 ? 2 : 1;
     const int grp = threadIdx.x / kL, sub = threadIdx.x % kL;
-    const int k0 = 4 * sub;
-    const bool kin = k0 < d;
-    float cf[4];
-    double cdv[4];
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int k0 = kE * sub;
+    const bool kin = k0 < d;                   // d % 4 == 0: a float4 is wholly inside or outside
+    float cf[kE];
+    double cdv[kE];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        cf[q] = kin ? center[k0 + q] : 0.f;
+    for (int q = 0; q < kE; ++q) {
+        cf[q] = (k0 + q < d) ? center[k0 + q] : 0.f;
         cdv[q] = (double)cf[q];
     }
-    const double g64 = (double)(d + 4) * 0x1p-53;
-    const double up64 = (1.0 + 2.0 * g64) * (1.0 + 0x1p-50);
-    const double up32 = 1.0 + (double)(d + 16) * 0x1p-23;
-    const double slack32 = (double)d * 0x1p-140;
-    const double gb = (double)(d + 2) * 0x1p-53;   // beta: |nrm2f - nrm2| + 2 gb nrm2
+    const double up64 = (1.0 + 2.0 * (double)(d + 4) * 0x1p-53) * (1.0 + 0x1p-50);
+    const float up32 = 1.f + (float)(d + 16) * 0x1p-23f;   // exact in FP32 for d <= 128
+    const float slack32 = (float)d * 0x1p-140f;
+    const double gb = (double)(d + 2) * 0x1p-53;           // beta: |nrm2f - nrm2| + 2 gb nrm2
     unsigned flags = 0;
 
     for (int h = 0; h < halves; ++h) {
         const int hb = h * 128;
-        float ps[4], pl[4], ph[4];
+        float ps[kE], pl[kE], ph[kE];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) { ps[q] = 0.f; pl[q] = INFINITY; ph[q] = -INFINITY; }
-        float my = 0.f, mb = 0.f, mbeta = 0.f, mtask = 0.f;   // task maxima (see below)
+        for (int q = 0; q < kE; ++q) { ps[q] = 0.f; pl[q] = INFINITY; ph[q] = -INFINITY; }
+        float mtask = 0.f, mb = 0.f, mbeta = 0.f;   // lanes 0-3 of a group: max of their bound; lane 0: B, beta
         if (hb < nv) {   // uniform across the block
             for (int m0 = 0; m0 < kRows; m0 += kU) {
-                float4 xv[kU];
+                float4 xv[kU][kV];
                 int ii[kU];
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
                     ii[u] = hb + grp + (m0 + u) * kNG;
-                    xv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (ii[u] < nv && kin) {
-                        const size_t orig = (size_t)perm[r0 + ii[u]];
-                        xv[u] = __ldg(reinterpret_cast<const float4*>(src + orig * (size_t)d + k0));
-                    }
+                    const bool ld = ii[u] < nv && kin;
+                    const float4* rowp = ld ? reinterpret_cast<const float4*>(
+                                                  src + (size_t)perm[r0 + ii[u]] * (size_t)d + k0)
+                                            : nullptr;
+#pragma unroll
+                    for (int v = 0; v < kV; ++v)
+                        xv[u][v] = (ld && k0 + 4 * v < d) ? __ldg(rowp + v) : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
                     const bool rv = ii[u] < nv;
-                    const float xa[4] = {xv[u].x, xv[u].y, xv[u].z, xv[u].w};
                     double sx = 0.0;
                     float sz = 0.f, se = 0.f, sl = 0.f;
-                    uint16_t hbits[4], lbits[4];
+                    uint32_t hw[kE / 2], lw[kE / 2];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        float x = xa[q];
-                        if (!isfinite(x)) { flags |= 1u; x = 0.f; }
+                    for (int q = 0; q < kE; ++q) {
+                        const float4 f4 = xv[u][q / 4];
+                        const float x = (q & 3) == 0 ? f4.x : (q & 3) == 1 ? f4.y : (q & 3) == 2 ? f4.z : f4.w;
                         const float sd = x - cf[q];
                         const float bb = sd - x;
                         const float err = (x - (sd - bb)) + (-cf[q] - bb);
                         const double xd = (double)x - cdv[q];
                         sx = fma(xd, xd, sx);
                         if (kFmt == 0 && fabsf(sd) > 65504.f) flags |= 2u;
-                        const float zh = round16<kFmt>(sd, hbits[q]);
+                        uint16_t hbits, lbits = 0;
+                        const float zh = round16<kFmt>(sd, hbits);
                         const float d1 = sd - zh;   // exact
                         if (kSplit) {
                             const float r = d1 + err;
                             const float b2 = r - d1;
                             const float rr = (d1 - (r - b2)) + (err - b2);
-                            const float zlo = round16<kFmt>(r, lbits[q]);
+                            const float zlo = round16<kFmt>(r, lbits);
                             const float ed = (r - zlo) + rr;
                             const float z = zh + zlo;
                             sz = fmaf(z, z, sz);
                             se = fmaf(ed, ed, se);
                             sl = fmaf(zlo, zlo, sl);
                         } else {
-                            lbits[q] = 0;
                             const float ed = d1 + err;
                             sz = fmaf(zh, zh, sz);
                             se = fmaf(ed, ed, se);
                         }
-                        if (rv && kin) {
+                        if (q & 1) {
+                            hw[q / 2] |= (uint32_t)hbits << 16;
+                            lw[q / 2] |= (uint32_t)lbits << 16;
+                        } else {
+                            hw[q / 2] = hbits;
+                            lw[q / 2] = lbits;
+                        }
+                        if (rv && k0 + q < d) {
                             ps[q] += x;
                             pl[q] = fminf(pl[q], x);
                             ph[q] = fmaxf(ph[q], x);
@@ -938,14 +952,13 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
                     }
                     const long long r = r0 + ii[u];
                     if (rv) {
-                        uint2 hv, lv;
-                        hv.x = (uint32_t)hbits[0] | ((uint32_t)hbits[1] << 16);
-                        hv.y = (uint32_t)hbits[2] | ((uint32_t)hbits[3] << 16);
-                        *reinterpret_cast<uint2*>(op + (size_t)r * opw + k0) = hv;
-                        if (kSplit) {
-                            lv.x = (uint32_t)lbits[0] | ((uint32_t)lbits[1] << 16);
-                            lv.y = (uint32_t)lbits[2] | ((uint32_t)lbits[3] << 16);
-                            *reinterpret_cast<uint2*>(op + (size_t)r * opw + kPad + k0) = lv;
+#pragma unroll
+                        for (int v = 0; v < kE / 4; ++v) {
+                            *reinterpret_cast<uint2*>(op + (size_t)r * opw + k0 + 4 * v) =
+                                make_uint2(hw[2 * v], hw[2 * v + 1]);
+                            if (kSplit)
+                                *reinterpret_cast<uint2*>(op + (size_t)r * opw + kPad + k0 + 4 * v) =
+                                    make_uint2(lw[2 * v], lw[2 * v + 1]);
                         }
                     }
 #pragma unroll
@@ -957,23 +970,22 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
                     }
                     // the four bounds of the row are taken by its first four lanes, one square root each
                     const unsigned task = sub & 3u;   // 0: |x - c|, 1: |z|, 2: |x - c - z|, 3: |z_lo|
-                    double rt;
+                    float rt;
                     if (task == 0) {
-                        rt = sqrt(sx * up64) * (1.0 + 0x1p-50);
+                        rt = __fsqrt_ru(__double2float_ru(sx * up64));
                     } else {
                         const float v32 = task == 1 ? sz : task == 2 ? se : sl;
-                        rt = (task == 3 && !kSplit) ? 0.0 : sqrt(((double)v32 + slack32) * up32) * (1.0 + 0x1p-50);
+                        rt = (task == 3 && !kSplit) ? 0.f : __fsqrt_ru(__fmul_ru(__fadd_ru(v32, slack32), up32));
                     }
-                    const double ynorm = __shfl_sync(0xffffffffu, rt, (int)((threadIdx.x & 31u) & ~(unsigned)(kL - 1)));
-                    if (task == 2) rt += 0x1p-50 * ynorm;
-                    const float rv32 = f32_up(rt);
+                    const float ynorm = __shfl_sync(0xffffffffu, rt, (int)(lane & ~(unsigned)(kL - 1)));
+                    if (task == 2) rt = __fadd_ru(rt, __fmul_ru(0x1p-50f, ynorm));
                     if (rv && sub < 4) {
                         float* dst = task == 0 ? yn : task == 1 ? zn : task == 2 ? en : zl;
-                        dst[r] = rv32;
-                        mtask = fmaxf(mtask, rv32);
+                        dst[r] = rt;
+                        mtask = fmaxf(mtask, rt);
                     }
                     if (rv && sub == 0) {
-                        if (sx > 0x1p100) flags |= 1u;
+                        if (!(sx <= 0x1p100)) flags |= 1u;   // also NaN / Inf anywhere in the row
                         const float sf = __double2float_rn(sx);
                         nrm2[r] = sx;
                         nrm2f[r] = sf;
@@ -984,35 +996,50 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
                 }
             }
         }
-        my = mtask;   // lane 0 of a group: the Y maximum; lanes 1-3: Z, E, Zl
+        // combine over the row groups of this warp (lanes with the same sub), then per warp to shared
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            psum[h][4 * threadIdx.x + q] = ps[q];
-            pmin[h][4 * threadIdx.x + q] = pl[q];
-            pmax[h][4 * threadIdx.x + q] = ph[q];
+        for (int o = kL; o < 32; o <<= 1) {
+#pragma unroll
+            for (int q = 0; q < kE; ++q) {
+                ps[q] += __shfl_xor_sync(0xffffffffu, ps[q], o);
+                pl[q] = fminf(pl[q], __shfl_xor_sync(0xffffffffu, pl[q], o));
+                ph[q] = fmaxf(ph[q], __shfl_xor_sync(0xffffffffu, ph[q], o));
+            }
+            mtask = fmaxf(mtask, __shfl_xor_sync(0xffffffffu, mtask, o));
+            mb = fmaxf(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+            mbeta = fmaxf(mbeta, __shfl_xor_sync(0xffffffffu, mbeta, o));
         }
-        if (sub < 4) rmx[h][sub][grp] = my;   // 0: Y, 1: Z, 2: E, 3: Zl
-        if (sub == 0) {
-            rmx[h][4][grp] = mb;
-            rmx[h][5][grp] = mbeta;
+        if ((int)lane < kL) {   // the warp's first group holds the warp's combined partials
+#pragma unroll
+            for (int q = 0; q < kE; ++q) {
+                wsum[h][warp][k0 + q] = ps[q];
+                wmin[h][warp][k0 + q] = pl[q];
+                wmax[h][warp][k0 + q] = ph[q];
+            }
+            if (sub < 4) wrow[h][sub][warp] = mtask;   // 0: Y, 1: Z, 2: E, 3: Zl
+            if (sub == 0) {
+                wrow[h][4][warp] = mb;
+                wrow[h][5][warp] = mbeta;
+            }
         }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) flags |= __shfl_xor_sync(0xffffffffu, flags, o);
-    if ((threadIdx.x & 31) == 0 && flags) {
+    if (lane == 0 && flags) {
         if (flags & 1u) atomicOr(status, (unsigned long long)kStatusBadInput);
         if (flags & 2u) atomicOr(status, (unsigned long long)kStatusFp16Range);
     }
     __syncthreads();
-    // centroids and boxes: groups combined in a fixed order
-    const int nvh[2] = {min(nv, 128), max(0, min(nv - 128, 128))};
+    // centroids and boxes: the eight warps combined in a fixed order
+    const int nvh0 = min(nv, 128), nvh1 = max(0, min(nv - 128, 128));
     for (int k = threadIdx.x; k < kPad; k += 256) {
         float sum[2] = {0.f, 0.f}, lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
         for (int h = 0; h < halves; ++h)
-            for (int gq = 0; gq < kNG; ++gq) {
-                sum[h] += psum[h][gq * kPad + k];
-                lo[h] = fminf(lo[h], pmin[h][gq * kPad + k]);
-                hi[h] = fmaxf(hi[h], pmax[h][gq * kPad + k]);
+#pragma unroll
+            for (int w = 0; w < 8; ++w) {
+                sum[h] += wsum[h][w][k];
+                lo[h] = fminf(lo[h], wmin[h][w][k]);
+                hi[h] = fmaxf(hi[h], wmax[h][w][k]);
             }
         const float c = (float)(((double)sum[0] + (double)sum[1]) / (double)max(nv, 1));
         cs[0][k] = c;
@@ -1024,7 +1051,7 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
         if (kHalves) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                const float ch = (float)((double)sum[h] / (double)max(nvh[h], 1));
+                const float ch = (float)((double)sum[h] / (double)max(h ? nvh1 : nvh0, 1));
                 cs[1 + h][k] = ch;
                 if (k < d) {
                     const size_t e = (size_t)k * H.ntiles + 2 * t + h;
@@ -1039,40 +1066,43 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
     // radius pass (the tile's rows again, from L2): FP32 sums of squared differences from the
     // centroids just written, bounded above as described at the top
     {
-        float ct[4], c0h[4], c1h[4];
+        float ct[kE], c0h[kE], c1h[kE];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < kE; ++q) {
             ct[q] = cs[0][k0 + q];
             c0h[q] = kHalves ? cs[1][k0 + q] : 0.f;
             c1h[q] = kHalves ? cs[2][k0 + q] : 0.f;
         }
-        float mt = 0.f, mh[2] = {0.f, 0.f};
+        float mt = 0.f, mh0 = 0.f, mh1 = 0.f;
         for (int h = 0; h < halves; ++h) {
             const int hb = h * 128;
             if (hb >= nv) break;   // uniform
             for (int m0 = 0; m0 < kRows; m0 += kU) {
-                float4 xv[kU];
+                float4 xv[kU][kV];
                 int ii[kU];
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
                     ii[u] = hb + grp + (m0 + u) * kNG;
-                    xv[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (ii[u] < nv && kin) {
-                        const size_t orig = (size_t)perm[r0 + ii[u]];
-                        xv[u] = __ldg(reinterpret_cast<const float4*>(src + orig * (size_t)d + k0));
-                    }
+                    const bool ld = ii[u] < nv && kin;
+                    const float4* rowp = ld ? reinterpret_cast<const float4*>(
+                                                  src + (size_t)perm[r0 + ii[u]] * (size_t)d + k0)
+                                            : nullptr;
+#pragma unroll
+                    for (int v = 0; v < kV; ++v)
+                        xv[u][v] = (ld && k0 + 4 * v < d) ? __ldg(rowp + v) : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
-                    const float xa[4] = {xv[u].x, xv[u].y, xv[u].z, xv[u].w};
                     float st_ = 0.f, sh = 0.f;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float x = isfinite(xa[q]) ? xa[q] : 0.f;
-                        const float df = kin ? x - ct[q] : 0.f;
+                    for (int q = 0; q < kE; ++q) {
+                        const float4 f4 = xv[u][q / 4];
+                        const float x = (q & 3) == 0 ? f4.x : (q & 3) == 1 ? f4.y : (q & 3) == 2 ? f4.z : f4.w;
+                        const bool in = k0 + q < d;
+                        const float df = in ? x - ct[q] : 0.f;
                         st_ = fmaf(df, df, st_);
                         if (kHalves) {
-                            const float dh = kin ? x - (h ? c1h[q] : c0h[q]) : 0.f;
+                            const float dh = in ? x - (h ? c1h[q] : c0h[q]) : 0.f;
                             sh = fmaf(dh, dh, sh);
                         }
                     }
@@ -1083,15 +1113,24 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
                     }
                     if (ii[u] < nv) {
                         mt = fmaxf(mt, st_);
-                        if (kHalves) mh[h] = fmaxf(mh[h], sh);
+                        if (kHalves) {
+                            if (h) mh1 = fmaxf(mh1, sh);
+                            else mh0 = fmaxf(mh0, sh);
+                        }
                     }
                 }
             }
         }
-        if (sub == 0) {
-            radm[0][grp] = mt;
-            radm[1][grp] = mh[0];
-            radm[2][grp] = mh[1];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mt = fmaxf(mt, __shfl_xor_sync(0xffffffffu, mt, o));
+            mh0 = fmaxf(mh0, __shfl_xor_sync(0xffffffffu, mh0, o));
+            mh1 = fmaxf(mh1, __shfl_xor_sync(0xffffffffu, mh1, o));
+        }
+        if (lane == 0) {
+            wrad[0][warp] = mt;
+            wrad[1][warp] = mh0;
+            wrad[2][warp] = mh1;
         }
     }
     __syncthreads();
@@ -1099,14 +1138,16 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
         const int w = threadIdx.x;
         if (w == 0 || kHalves) {
             float m = 0.f;
-            for (int gq = 0; gq < kNG; ++gq) m = fmaxf(m, radm[w][gq]);
-            const int hv = w == 0 ? nv : nvh[w - 1];
-            const float rb = hv > 0 ? f32_up(sqrt(((double)m + slack32) * up32) * (1.0 + 0x1p-50)) : 0.f;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) m = fmaxf(m, wrad[w][q]);
+            const int hv = w == 0 ? nv : (w == 1 ? nvh0 : nvh1);
+            const float rb = hv > 0 ? __fsqrt_ru(__fmul_ru(__fadd_ru(m, slack32), up32)) : 0.f;
             float mx[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             for (int q = 0; q < 6; ++q)
                 for (int h = 0; h < halves; ++h) {
                     if (w > 0 && h != w - 1) continue;
-                    for (int gq = 0; gq < kNG; ++gq) mx[q] = fmaxf(mx[q], rmx[h][q][gq]);
+#pragma unroll
+                    for (int x = 0; x < 8; ++x) mx[q] = fmaxf(mx[q], wrow[h][q][x]);
                 }
             TileOut& O = w == 0 ? T : H;
             const int e = w == 0 ? t : 2 * t + (w - 1);
@@ -1496,16 +1537,16 @@ void prep_tiles(Side& s, const float* center, int tile, TileSet& ts, TileSet* ha
     const uint32_t* r0 = tabled ? (const uint32_t*)ts.row0.p : nullptr;
     const uint32_t* nvv = tabled ? (const uint32_t*)ts.nvalid.p : nullptr;
     const TileOut T = tile_out(ts);
-#define TJ_PT(SCR, SPLIT, L, HV)                                                                                   \
-    launch(prep_tiles_kernel<SCR, SPLIT, L, HV>, (unsigned)ntiles, 256, 0, st, (const float*)s.src, n, s.d, tile, \
+#define TJ_PT(SCR, SPLIT, E, L, HV)                                                                                 \
+    launch(prep_tiles_kernel<SCR, SPLIT, E, L, HV>, (unsigned)ntiles, 256, 0, st, (const float*)s.src, n, s.d, tile, \
            (const uint32_t*)s.perm.p, center, r0, nvv, s.op.p, s.nrm2.p, s.nrm2f.p, s.zn.p, s.en.p, s.yn.p,      \
            s.zl.p, T, H, status)
 #define TJ_PT_L(SCR, SPLIT, HV)                                  \
     do {                                                         \
-        if (s.kpad == 16) TJ_PT(SCR, SPLIT, 4, HV);              \
-        else if (s.kpad == 32) TJ_PT(SCR, SPLIT, 8, HV);         \
-        else if (s.kpad == 64) TJ_PT(SCR, SPLIT, 16, HV);        \
-        else TJ_PT(SCR, SPLIT, 32, HV);                          \
+        if (s.kpad == 16) TJ_PT(SCR, SPLIT, 4, 4, HV);           \
+        else if (s.kpad == 32) TJ_PT(SCR, SPLIT, 4, 8, HV);      \
+        else if (s.kpad == 64) TJ_PT(SCR, SPLIT, 8, 8, HV);      \
+        else TJ_PT(SCR, SPLIT, 8, 16, HV);                       \
     } while (0)
 #define TJ_PT_H(SCR, SPLIT)                                      \
     do {                                                         \

@@ -600,6 +600,22 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 }
                 tc_fence_after();
                 const unsigned tbase = tmem + ((q * 32u) << 16) + (kPair ? b * kTileS : b * 128u);
+                if (a.dump && e % a.dump_every == 0 && e / a.dump_every < a.dump_items) {
+                    // diagnostics: the raw accumulators of sampled items, in a rolled pass of its own
+                    // (kept out of the unrolled test below, whose code must stay in the instruction cache)
+                    const size_t slotd = e / a.dump_every;
+#pragma unroll 1
+                    for (int c8 = cb_begin * 4; c8 < cb_end * 4; ++c8) {   // 8 columns per TMEM load
+                        const int col0 = (int)colbase + c8 * 8;
+                        uint32_t raw[8];
+                        tmem_ld8(tbase + c8 * 8, raw);
+                        tmem_ld_wait();
+                        float* out = a.dump + (slotd * kTileR + row) * kTileS + col0;
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) out[k] = __uint_as_float(raw[k]);
+                        if (row == 0 && col0 == 0) a.dump_ids[slotd] = make_uint4(rtile, a.jlist[e] & kJMask, 1u, 0u);
+                    }
+                }
                 // phase 1: every 32-column block of this warp's part is read from TMEM and tested; a
                 // lane keeps, per block, the mask of its candidates (v <= tau) and of the certified
                 // accepts among them (v <= tau_in).  No warp-collective step runs here, and the
@@ -613,13 +629,6 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     uint32_t raw[32];
                     tmem_ld32(tbase + cb * 32, raw);
                     tmem_ld_wait();
-                    if (a.dump && e % a.dump_every == 0 && e / a.dump_every < a.dump_items) {
-                        const size_t slotd = e / a.dump_every;
-                        float* out = a.dump + (slotd * kTileR + row) * kTileS + col0;
-#pragma unroll
-                        for (int k = 0; k < 32; ++k) out[k] = __uint_as_float(raw[k]);
-                        if (row == 0 && col0 == 0) a.dump_ids[slotd] = make_uint4(rtile, a.jlist[e] & kJMask, 1u, 0u);
-                    }
                     if (cb == cb_end - 1) {   // this warp's part read: hand it back
                         tc_fence_before();
                         __syncwarp();

@@ -234,3 +234,35 @@ CONFIGS = {
     "int14x128": int14x128,
     "ragged4096": ragged4096,
 }
+
+
+def ragged4096_device(joins=4096, lo=256, hi=65536, dims=(8, 32, 128), clusters=8, std=0.05, degree=16, seed=5,
+                      size_scale=1.0):
+    """Config 5 drawn on the GPU (seeded torch CUDA generator): the shapes and distributions of
+    ``ragged4096``, one bulk draw per dimension class and side, every join a contiguous slice (views).
+    Returns ``([(R, S, eps), ...], class_arrays)`` with device tensors."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    nr = np.maximum(1, np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), joins)) * size_scale)).astype(np.int64)
+    ns = np.maximum(1, np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), joins)) * size_scale)).astype(np.int64)
+    dj = rng.choice(np.asarray(dims), joins)
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    out = [dict() for _ in range(joins)]
+    classes = []
+    for d in dims:
+        ks = np.flatnonzero(dj == d)
+        if len(ks) == 0:
+            continue
+        centres = torch.from_numpy(rng.random((len(ks), clusters, d)).astype(np.float32)).cuda()
+        for side, counts in (("R", nr[ks]), ("S", ns[ks])):
+            total = int(counts.sum())
+            owner = torch.from_numpy(np.repeat(np.arange(len(ks)), counts)).cuda()
+            label = torch.randint(0, clusters, (total,), generator=g, device="cuda")
+            X = torch.randn((total, d), generator=g, device="cuda") * std + centres[owner, label]
+            classes.append(X)
+            offs = np.concatenate([[0], np.cumsum(counts)])
+            for q, k in enumerate(ks):
+                out[k][side] = X[int(offs[q]):int(offs[q + 1])]
+    eps = [math.sqrt(ragged_eps2(int(ns[k]), int(dj[k]), clusters, std, degree)) for k in range(joins)]
+    return [(out[k]["R"], out[k]["S"], eps[k]) for k in range(joins)], classes

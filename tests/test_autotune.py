@@ -93,6 +93,20 @@ def test_table_persists(tmp_path):
     assert json.load(open(path))["d64/f32/bf16/rs/space2^30/sel2^3"]["ms"] == {"x": 1.5}
 
 
+def test_batch_key_and_lookup(tmp_path):
+    """A batch is keyed by its dimensions, screen, join count and pair space; the lookup returns the
+    recorded choice without tuning."""
+    joins = [(np.zeros((300, 8), np.float32), np.zeros((500, 8), np.float32), 0.1),
+             (np.zeros((1000, 32), np.float32), np.zeros((40, 32), np.float32), 0.2)]
+    key = A.Tuner.batch_key(joins, "bf16x3")
+    assert key == "batch/d8-32/f32/bf16x3/joins2^1/space2^18"   # 190,000 pairs
+    t = A.Tuner(str(tmp_path / "tune.json"))
+    assert t.batch_choice(joins, "bf16x3") is None
+    t.record(key, A.Choice(half_pack=False, stages=3), {})
+    assert t.batch_choice(joins, "bf16x3") == A.Choice(half_pack=False, stages=3)
+    assert t.batch_choice(joins, "fp16") is None
+
+
 @pytest.mark.gpu
 def test_tuned_join_matches_oracle_and_reuses_the_table(tmp_path):
     import torch

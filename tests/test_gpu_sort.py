@@ -72,3 +72,23 @@ def test_index_sort_packed_class(njoins):
         i, j = out[q]
         got = (i.cpu().numpy().astype(np.uint64) * np.uint64(S.shape[0]) + j.cpu().numpy().astype(np.uint64))
         assert np.array_equal(got, want), q
+
+
+def test_batched_host_views_of_one_array():
+    """Joins whose rows are views of two pinned host arrays (one per side) move in one copy per array
+    and come back as host pairs identical to the oracle's."""
+    g = np.random.default_rng(21)
+    nr = g.integers(50, 3000, 40)
+    ns = g.integers(50, 3000, 40)
+    RA = torch.from_numpy(g.standard_normal((int(nr.sum()), 16)).astype(np.float32)).pin_memory()
+    SA = torch.from_numpy(g.standard_normal((int(ns.sum()), 16)).astype(np.float32)).pin_memory()
+    ro, so = np.concatenate([[0], np.cumsum(nr)]), np.concatenate([[0], np.cumsum(ns)])
+    joins = [(RA[ro[k]:ro[k + 1]], SA[so[k]:so[k + 1]], 2.0) for k in range(40)]
+    out = tj.join_batched(joins, screen="bf16x3", guards=True)
+    for k in range(40):
+        R, S, e = joins[k]
+        want = oracle.join_f32(R.numpy(), S.numpy(), e * e, "rs")
+        i, j = out[k]
+        assert not i.is_cuda
+        got = i.numpy().astype(np.uint64) * np.uint64(S.shape[0]) + j.numpy().astype(np.uint64)
+        assert np.array_equal(got, want), k
