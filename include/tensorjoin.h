@@ -147,6 +147,15 @@ typedef struct tj_stats {
      * end inside the screen launch */
     double screen_cta_tail_ms;
     double join_span_ms_p50, join_span_ms_p99, join_span_ms_max;
+    /* TJ_FLAG_SCREEN_TIMES, one-SM and CTA-pair 16-bit screens: where each role of the persistent screen
+     * spent its time, as fractions of that role's running time (SM clock cycles summed over the CTAs;
+     * the epilogue's over its warps).  Producer: waiting for a free operand stage, for a free metadata
+     * slot.  UMMA issuer: waiting for operands, for a free accumulator.  Epilogue: waiting for an
+     * item's metadata, for its accumulator; reading and testing the accumulator; emitting (from the
+     * warp scan to the last key written), and within that the output reservations. */
+    double screen_prod_stage_wait, screen_prod_meta_wait;
+    double screen_mma_operand_wait, screen_mma_acc_wait;
+    double screen_epi_meta_wait, screen_epi_acc_wait, screen_epi_test, screen_epi_emit, screen_epi_reserve;
 } tj_stats;
 
 /* ----------------------------------------------------------------- joins */

@@ -61,7 +61,10 @@ class Stats(C.Structure):
         "screen_max_abs_err", "screen_err_over_bound")] + [("screen_err_pairs", C.c_int64), ("screen_pair", C.c_int64),
                                                    ("index_frame", C.c_int64), ("band_fp64", C.c_int64),
                                                    ("screen_ops_issued", C.c_double)] + [
-        (n, C.c_double) for n in ("screen_cta_tail_ms", "join_span_ms_p50", "join_span_ms_p99", "join_span_ms_max")]
+        (n, C.c_double) for n in ("screen_cta_tail_ms", "join_span_ms_p50", "join_span_ms_p99", "join_span_ms_max",
+                                  "screen_prod_stage_wait", "screen_prod_meta_wait", "screen_mma_operand_wait",
+                                  "screen_mma_acc_wait", "screen_epi_meta_wait", "screen_epi_acc_wait",
+                                  "screen_epi_test", "screen_epi_emit", "screen_epi_reserve")]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

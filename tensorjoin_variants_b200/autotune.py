@@ -116,8 +116,9 @@ def tune_key(d: int, dtype: str, screen: str, mode: str, n_rows: int, n_cols: in
 
 
 def _sample_rows(X: torch.Tensor, k: int) -> torch.Tensor:
+    """An evenly spaced sample of k rows (all rows when k <= 0 or k >= n)."""
     n = X.shape[0]
-    if n <= k:
+    if k <= 0 or n <= k:
         return X
     idx = torch.linspace(0, n - 1, k, device=X.device).round().long()
     return X.index_select(0, idx).contiguous()
@@ -286,12 +287,14 @@ class Tuner:
         key = self.batch_key(joins, screen)
         return self.lookup(key) or default_table().lookup(key)
 
-    def join_batched(self, joins, screen: str = "bf16x3", sample_joins: int = 64, reps: int = 2):
+    def join_batched(self, joins, screen: str = "bf16x3", sample_joins: int = 64, reps: int = 2,
+                     fresh: bool = False):
         """Tuned batched join: the choice is searched on a seeded sample of the batch's joins (the
-        batch's own mix of sizes and dimensions), keyed as ``batch_key``."""
+        batch's own mix of sizes and dimensions), keyed as ``batch_key``; ``fresh`` searches even
+        when a table already holds the key."""
         dims = sorted({int(j[0].shape[1]) for j in joins})
         key = self.batch_key(joins, screen)
-        choice = self.lookup(key) or default_table().lookup(key)
+        choice = None if fresh else (self.lookup(key) or default_table().lookup(key))
         if choice is None:
             g = torch.Generator().manual_seed(len(joins))
             idx = torch.randperm(len(joins), generator=g)[:sample_joins].tolist()
@@ -322,7 +325,9 @@ def _dtype(t: torch.Tensor) -> str:
 
 def _produce(path: str, sample_rows: int) -> None:
     """Tune the five benchmark configurations (seeded synthetic data of their shapes) on this GPU
-    and write the table to `path`."""
+    and write the table to `path`; sample_rows <= 0 times every choice on the full configuration (the
+    batch on all of its joins), which is what the benchmark runs: choices timed on a row sample
+    did not carry over to the full joins, whose tile-pair density and pruning differ."""
     from . import workloads as W
 
     t = Tuner(path)
@@ -332,11 +337,13 @@ def _produce(path: str, sample_rows: int) -> None:
         w = getattr(W, name)()
         R = torch.from_numpy(w.R).cuda()
         S = None if w.S is None else torch.from_numpy(w.S).cuda()
-        choice, key = t.choose(R, S, float(w.T), mode, screen, sample_rows)
+        key = t.key_for(R, S, float(w.T), mode, screen)
+        choice, _, timings = t.tune(R, S, float(w.T), mode, screen, sample_rows)   # always searched afresh
+        t.record(key, choice, timings)
         print(f"{name} {screen}: {key} -> {choice}", flush=True)
         del R, S
     joins, classes = W.ragged4096_device()
-    _, choice = t.join_batched(joins, "bf16x3")
+    _, choice = t.join_batched(joins, "bf16x3", sample_joins=len(joins) if sample_rows <= 0 else 64, fresh=True)
     print(f"ragged4096 bf16x3: {t.batch_key(joins, 'bf16x3')} -> {choice}", flush=True)
     del joins, classes
     print(json.dumps(t.table, indent=1, sort_keys=True))
@@ -347,7 +354,7 @@ if __name__ == "__main__":
 
     ap = argparse.ArgumentParser(description="tune the benchmark configurations and write a table")
     ap.add_argument("--out", default=str(DEFAULT_TABLE))
-    ap.add_argument("--sample-rows", type=int, default=8192)
+    ap.add_argument("--sample-rows", type=int, default=0, help="rows per tuning sample (0: the full configuration)")
     a = ap.parse_args()
     _produce(a.out, a.sample_rows)
 

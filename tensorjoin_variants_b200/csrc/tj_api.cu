@@ -415,7 +415,10 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     const bool allow_pair = !(opt && (opt->flags & TJ_FLAG_SCREEN_1SM));
     const bool likely_pair = allow_pair && ncls == 1 && nj == 1 && !self && !split_screen && cls_d[0] > 192;
     const bool diag_req = opt && (opt->flags & TJ_FLAG_SCREEN_DIAG) && tc16;   // samples whole tile pairs
-    const bool half_packed = tc16 && !likely_pair && !diag_req && !(opt && (opt->flags & TJ_FLAG_WHOLE_TILES));
+    // (the half-tile test keeps eight R tiles' centroid and box in shared memory: rows of at most
+    // 2048 elements)
+    const bool half_packed = tc16 && !likely_pair && !diag_req && !(opt && (opt->flags & TJ_FLAG_WHOLE_TILES)) &&
+                             *std::max_element(cls_d.begin(), cls_d.end()) <= 2048;
     for (int c = 0; c < ncls; ++c) {
         C[c].reset(new Cls());
         Cls& K = *C[c];
@@ -675,12 +678,14 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     const bool stage_keys = opt && (opt->flags & TJ_FLAG_STAGE_KEYS);
     const unsigned long long gs = guards ? kGuardSlots : 0;
     const bool times = opt && (opt->flags & TJ_FLAG_SCREEN_TIMES) && screen != TJ_SCREEN_PLAIN && !i8;
-    DBuf<unsigned long long> join_t, cta_t;
+    DBuf<unsigned long long> join_t, cta_t, role_t;
     if (times) {
         join_t = DBuf<unsigned long long>(2 * (size_t)nj, st);
         cta_t = DBuf<unsigned long long>(2 * (size_t)num_sms(), st);
+        role_t = DBuf<unsigned long long>(16, st);
         g.join_t = join_t.p;
         g.cta_t = cta_t.p;
+        g.role_t = role_t.p;
     }
     DBuf<uint64_t> acc, band;
     Counters h;
@@ -692,6 +697,7 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
             TJ_CUDA(cudaMemsetAsync(join_t.p, 0xFF, (size_t)nj * 8, st));
             TJ_CUDA(cudaMemsetAsync(join_t.p + nj, 0, (size_t)nj * 8, st));
             TJ_CUDA(cudaMemsetAsync(cta_t.p, 0, cta_t.bytes(), st));
+            TJ_CUDA(cudaMemsetAsync(role_t.p, 0, role_t.bytes(), st));
         }
         if (guards) {
             launch(guard_fill, 1, 256, 0, st, acc.p + cap);
@@ -738,9 +744,10 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         S_.screen_err_pairs = (int64_t)dv[2];
     }
     if (times) {
-        std::vector<unsigned long long> jt(2 * (size_t)nj), ct(cta_t.n);
+        std::vector<unsigned long long> jt(2 * (size_t)nj), ct(cta_t.n), rl(16);
         TJ_CUDA(cudaMemcpyAsync(jt.data(), join_t.p, jt.size() * 8, cudaMemcpyDeviceToHost, st));
         TJ_CUDA(cudaMemcpyAsync(ct.data(), cta_t.p, ct.size() * 8, cudaMemcpyDeviceToHost, st));
+        TJ_CUDA(cudaMemcpyAsync(rl.data(), role_t.p, rl.size() * 8, cudaMemcpyDeviceToHost, st));
         TJ_CUDA(cudaStreamSynchronize(st));
         std::vector<double> span;
         for (int k = 0; k < nj; ++k)
@@ -756,6 +763,17 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         for (size_t b = 0; b + 1 < ct.size(); b += 2)
             if (ct[b + 1]) { lo = std::min(lo, ct[b + 1]); hi = std::max(hi, ct[b + 1]); }
         if (hi >= lo && hi) S_.screen_cta_tail_ms = (double)(hi - lo) * 1e-6;
+        // stall accounting: slots as the screen's RoleSlot (producer 0-2, issuer 3-5, epilogue 6-11)
+        auto frac = [&](int part, int whole) { return rl[whole] ? (double)rl[part] / (double)rl[whole] : 0.0; };
+        S_.screen_prod_stage_wait = frac(1, 0);
+        S_.screen_prod_meta_wait = frac(2, 0);
+        S_.screen_mma_operand_wait = frac(4, 3);
+        S_.screen_mma_acc_wait = frac(5, 3);
+        S_.screen_epi_meta_wait = frac(7, 6);
+        S_.screen_epi_acc_wait = frac(8, 6);
+        S_.screen_epi_test = frac(9, 6);
+        S_.screen_epi_emit = frac(10, 6);
+        S_.screen_epi_reserve = frac(11, 6);
     }
     S_.screen_accept = (int64_t)h.screen_accept;
     S_.band = (int64_t)h.band_valid;

@@ -303,6 +303,23 @@ TJ_DEV void tmem_ld8(unsigned taddr, uint32_t (&r)[8]) {
                  : "r"(taddr) : "memory");
 }
 TJ_DEV void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+TJ_DEV void tmem_ld16(unsigned taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr) : "memory");
+}
+// Wait for the outstanding TMEM loads, with the registers of one of them as operands: their uses
+// cannot be scheduled above the wait (a load whose registers are still in flight may be issued
+// before other work, and waited for after it).
+TJ_DEV void tmem_wait16(uint32_t (&r)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15])
+                 :: "memory");
+}
 
 // UMMA shared-memory descriptor: K-major operand in the 128-byte swizzle canonical layout
 // (8-row x 128-byte atoms, atoms stacked every 1024 bytes), as written by a TMA box of

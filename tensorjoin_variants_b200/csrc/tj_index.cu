@@ -1376,46 +1376,62 @@ __global__ void chunk_emit(const uint64_t* keys, size_t cap, const uint32_t* tot
 // skipped.  One block per R tile, threads over its candidate entries.
 __global__ void __launch_bounds__(256) half_mask_kernel(const uint32_t* cnt, const uint32_t* off, uint32_t* jlist,
                                                         const uint4* rtiles, const JoinParams* jps,
-                                                        const HalfView* views, int self_join) {
-    extern __shared__ float hm_sm[];   // [3][d]: R tile centroid, low, high
-    const int I = blockIdx.x;
+                                                        const HalfView* views, int self_join, int ntR, int dmax) {
+    // one warp per R tile (eight per block), its lanes over the tile's candidates; the R tile's
+    // centroid and box sit in the warp's part of shared memory
+    extern __shared__ float hm_sm[];   // [8 warps][3][dmax]: R tile centroid, low, high
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int I = (int)blockIdx.x * 8 + (int)warp;
+    if (I >= ntR) return;   // whole warps leave; no block-wide barrier follows
+    float* rs = hm_sm + (size_t)warp * 3 * dmax;
     const uint4 rt = rtiles[I];
     const HalfView v = views[rt.w];
     const int d = v.d;
     const int il = I - v.rbase;   // class-local R tile
-    for (int k = threadIdx.x; k < d; k += blockDim.x) {
-        hm_sm[k] = v.rctrT[(size_t)k * v.ntR + il];
-        hm_sm[d + k] = v.rloT[(size_t)k * v.ntR + il];
-        hm_sm[2 * d + k] = v.rhiT[(size_t)k * v.ntR + il];
+    for (int k = lane; k < d; k += 32) {
+        rs[k] = v.rctrT[(size_t)k * v.ntR + il];
+        rs[d + k] = v.rloT[(size_t)k * v.ntR + il];
+        rs[2 * d + k] = v.rhiT[(size_t)k * v.ntR + il];
     }
-    __syncthreads();
+    __syncwarp();
     const double Tp = jps[rt.z].Tp;
     const float f = 1.f - (float)(d + 8) * 0x1p-23f;
     const float rtp = (float)(sqrt(Tp) * (1.0 + 0x1p-20));
     const float tpf = (float)(Tp * (1.0 + 0x1p-20));
     const float ri = v.rrad[il];
     const uint32_t e0 = off[I], e1 = e0 + cnt[I];
-    for (uint32_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    for (uint32_t e = e0 + lane; e < e1; e += 32) {
         const uint32_t J = jlist[e] & 0x3FFFFFFFu;
+        const int h0 = 2 * ((int)J - v.sbase);   // class-local half tiles h0, h0 + 1
+        bool live[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            live[h] = h0 + h < v.ntH && v.hnv[h0 + h] != 0;
+            // self-joins: some sorted column of the half must exceed some sorted row of the tile
+            if (self_join && (long long)(h0 + h) * 128 + 127 <= (long long)il * 128) live[h] = false;
+        }
+        const int g0 = live[0] ? h0 : h0 + 1, g1 = live[1] ? h0 + 1 : h0;   // in-range columns for both
+        float ball[2] = {0.f, 0.f}, box[2] = {0.f, 0.f};
+        if (live[0] || live[1]) {
+#pragma unroll 4
+            for (int k = 0; k < d; ++k) {
+                const size_t rk = (size_t)k * v.ntH;
+                const float c = rs[k], lo = rs[d + k], hi = rs[2 * d + k];
+                const float dc0 = c - v.hctrT[rk + g0], dc1 = c - v.hctrT[rk + g1];
+                const float gp0 = fmaxf(fmaxf(v.hloT[rk + g0] - hi, lo - v.hhiT[rk + g0]), 0.f);
+                const float gp1 = fmaxf(fmaxf(v.hloT[rk + g1] - hi, lo - v.hhiT[rk + g1]), 0.f);
+                ball[0] = fmaf(dc0, dc0, ball[0]);
+                ball[1] = fmaf(dc1, dc1, ball[1]);
+                box[0] = fmaf(gp0, gp0, box[0]);
+                box[1] = fmaf(gp1, gp1, box[1]);
+            }
+        }
         unsigned mask = 0;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            const int hl = 2 * ((int)J - v.sbase) + h;   // class-local half tile
-            if (hl >= v.ntH || v.hnv[hl] == 0) continue;
-            if (self_join) {   // some sorted column of the half must exceed some sorted row of the tile
-                const long long maxcol = (long long)hl * 128 + 127;
-                if (maxcol <= (long long)il * 128) continue;
-            }
-            float ball = 0.f, box = 0.f;
-            for (int k = 0; k < d; ++k) {
-                const float dc = hm_sm[k] - v.hctrT[(size_t)k * v.ntH + hl];
-                ball = fmaf(dc, dc, ball);
-                const float gap = fmaxf(fmaxf(v.hloT[(size_t)k * v.ntH + hl] - hm_sm[2 * d + k],
-                                              hm_sm[d + k] - v.hhiT[(size_t)k * v.ntH + hl]), 0.f);
-                box = fmaf(gap, gap, box);
-            }
-            const float lb_box = box * f;
-            const float lb_ball = sqrtf(ball * f) * (1.f - 0x1p-20f) - ri - v.hrad[hl];
+            if (!live[h]) continue;
+            const float lb_box = box[h] * f;
+            const float lb_ball = sqrtf(ball[h] * f) * (1.f - 0x1p-20f) - ri - v.hrad[h0 + h];
             if (!(lb_box > tpf || lb_ball > rtp)) mask |= 1u << h;
         }
         jlist[e] = J | (mask << 30);
@@ -1745,11 +1761,12 @@ void half_masks(const std::vector<HalfView>& views, const Candidates& c, int ntR
     for (const auto& v : views) dmax = std::max(dmax, v.d);
     DBuf<HalfView> dv(views.size(), st);
     upload(dv.p, views.data(), views.size() * sizeof(HalfView), st);
-    const size_t smem = (size_t)3 * dmax * sizeof(float);
+    const size_t smem = (size_t)8 * 3 * dmax * sizeof(float);   // eight R tiles per block
     if (smem > 48 * 1024)
         TJ_CUDA(cudaFuncSetAttribute(half_mask_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    launch(half_mask_kernel, (unsigned)ntR_total, 256, smem, st, (const uint32_t*)c.cnt.p, (const uint32_t*)c.off.p,
-           c.jlist.p, rtiles, jps, (const HalfView*)dv.p, self_join ? 1 : 0);
+    launch(half_mask_kernel, (unsigned)((ntR_total + 7) / 8), 256, smem, st, (const uint32_t*)c.cnt.p,
+           (const uint32_t*)c.off.p, c.jlist.p, rtiles, jps, (const HalfView*)dv.p, self_join ? 1 : 0, ntR_total,
+           dmax);
 }
 
 void build_candidates_batched(const std::vector<CandClassView>& classes, const std::vector<CandBlock>& blocks,

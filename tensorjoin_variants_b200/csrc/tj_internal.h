@@ -281,6 +281,7 @@ struct ScreenInput {
     // %globaltimer stamps, null when off
     unsigned long long* join_t = nullptr;     // [2 njoins]
     unsigned long long* cta_t = nullptr;      // [2 * grid]
+    unsigned long long* role_t = nullptr;     // [16] stall accounting of the 16-bit screens (SM cycles)
 };
 
 void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st);

@@ -192,14 +192,22 @@ WorkspaceScope::~WorkspaceScope() {
         W.cap = 0;
         const size_t gran = (size_t)64 << 20;
         const size_t cap = ((W.need + W.need / 4 + gran - 1) / gran) * gran;
-        // the overflow blocks went back to the pool: hand that memory to the driver first
-        cudaMemPoolTrimTo(pool_for_current(), 0);
         void* p = nullptr;
-        if (cudaMalloc(&p, cap) == cudaSuccess) {
+        if (cudaMalloc(&p, cap) != cudaSuccess) {
+            // the overflow blocks went back to the pool: hand that idle memory to the driver and try
+            // again (only then: a trimmed pool maps its memory anew, which took hundreds of ms)
+            cudaGetLastError();
+            cudaMemPoolTrimTo(pool_for_current(), 0);
+            if (cudaMalloc(&p, cap) != cudaSuccess) p = nullptr;
+        }
+        if (p) {
             W.base = (char*)p;
             W.cap = cap;
         }
         cudaGetLastError();   // a failed growth leaves the next join on the pool
+        if (trace_alloc_ms() >= 0.0)
+            fprintf(stderr, "[tj workspace] re-made at %zu MiB for a need of %zu MiB%s\n", cap >> 20, W.need >> 20,
+                    p ? "" : " (failed: the next join allocates from the pool)");
     } catch (...) {
         cudaGetLastError();
     }

@@ -109,6 +109,13 @@ struct ScreenCtl {
     int abort_flag;
 };
 constexpr int kChunkRing = 4;
+// Stall accounting (TJ_FLAG_SCREEN_TIMES): slots of ScreenArgs::role_t
+enum RoleSlot {
+    kRoleProd = 0, kRoleProdStage, kRoleProdMeta,
+    kRoleMma, kRoleMmaOperand, kRoleMmaAcc,
+    kRoleEpi, kRoleEpiMeta, kRoleEpiAcc, kRoleEpiTest, kRoleEpiEmit, kRoleEpiReserve,
+    kRoleSlots = 16
+};
 constexpr unsigned kNoChunk = 0xFFFFFFFFu;
 
 // CTA pair (cta_group::2, 256 x 256 tile over two SMs): a stage holds this CTA's 128 A rows and its
@@ -181,6 +188,7 @@ struct ScreenArgs {
     // last chunk end (join_t[njoins + j], atomicMax), and each CTA's start and end (cta_t[2 b], [2 b + 1])
     unsigned long long* join_t;
     unsigned long long* cta_t;
+    unsigned long long* role_t;   // [kRoleSlots] SM clock cycles per role and wait, summed over CTAs
     unsigned njoins;
     int nstages;                  // operand stages in the ring (<= the compiled count; a tuning knob)
     int half;                     // one SM: jlist entries carry live-half masks in bits 30-31
@@ -269,7 +277,8 @@ TJ_DEV void chunk_at(const ScreenArgs& a, unsigned c, unsigned rank, unsigned& r
 }
 
 // kFmt: 0 = fp16, 1 = bf16; kSplit: hi/lo operand limbs; kPair: CTA-pair MMA (cta_group::2, no split)
-template <int kFmt, int kSplit, bool kPair>
+// kTimes: stall accounting (ScreenArgs::role_t) compiled in; the production screens are built without it
+template <int kFmt, int kSplit, bool kPair, bool kTimes = false>
 __global__ void __launch_bounds__(kScreenThreads, 1)
     screen_tc_kernel(const __grid_constant__ TMaps tm, const ScreenArgs a) {
     using Cfg = typename StageSel<kSplit, kPair>::type;
@@ -278,6 +287,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     ColMetaHot* meta = (ColMetaHot*)(smem + (size_t)kStages * kStageBytes);
+    __shared__ long long role_acc[kScreenThreads / 32][6];   // stall accounting per warp (TJ_FLAG_SCREEN_TIMES)
     ScreenCtl<kStages>* ctl = (ScreenCtl<kStages>*)(meta + kMetaSlots);
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long* status = &a.ctr->status;
@@ -332,6 +342,8 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             unsigned stage = 0, phase = 0;
             unsigned long long n = 0;   // items issued
             bool ok = true;
+            const long long t_role = kTimes ? clock64() : 0;
+            long long w_stage = 0, w_meta = 0;
             for (unsigned long long qc = 0;; ++qc) {
                 unsigned c;
                 if (kPair) {   // the two CTAs of a pair walk the same static sequence
@@ -363,12 +375,16 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     }
                     const int srow = (int)a.stiles[J].x + (int)(rank * kTileR);   // pair: this CTA's half
                     const unsigned slot = (unsigned)(n % kMetaSlots), mph = (unsigned)((n / kMetaSlots) & 1);
+                    const long long t_m = kTimes ? clock64() : 0;
                     if (!mbar_wait(&ctl->meta_empty[slot], mph ^ 1, status, a.wait_ns)) { ok = false; break; }
+                    if (kTimes) w_meta += clock64() - t_m;
                     mbar_arrive_expect_tx(&ctl->meta_full[slot], (unsigned)sizeof(ColMetaHot));
                     bulk_load(&meta[slot], (const ColMetaHot*)(a.s_meta + J), (unsigned)sizeof(ColMetaHot),
                               &ctl->meta_full[slot]);
                     for (int kb = 0; kb < kblocks; ++kb) {
+                        const long long t_s = kTimes ? clock64() : 0;
                         if (!mbar_wait(&ctl->empty[stage], phase ^ 1, status, a.wait_ns)) { ok = false; break; }
+                        if (kTimes) w_stage += clock64() - t_s;
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         uint8_t* sa = smem + (size_t)stage * kStageBytes;
                         if (kPair) {   // both CTAs' copies complete on the MMA CTA's barrier
@@ -397,6 +413,11 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 }
             }
             if (!ok) ctl->abort_flag = 1;
+            if (kTimes) {
+                atomicAdd(&a.role_t[kRoleProd], (unsigned long long)(clock64() - t_role));
+                atomicAdd(&a.role_t[kRoleProdStage], (unsigned long long)w_stage);
+                atomicAdd(&a.role_t[kRoleProdMeta], (unsigned long long)w_meta);
+            }
             // drain: the last copy issued into every stage / metadata slot must land before exit.  In
             // the pair the stage barriers live in CTA 0 and count both CTAs' copies: CTA 0 waits for
             // the phases it armed, and CTA 1, which cannot see them, waits for its own stages to be
@@ -421,6 +442,8 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             unsigned long long n_mma = 0;   // items issued
             unsigned ns = 0;                // one SM: half-items issued
             bool ok = true;
+            const long long t_role = kTimes ? clock64() : 0;
+            long long w_op = 0, w_acc = 0;
             for (unsigned long long qc = 0;; ++qc) {
                 unsigned c;
                 if (kPair) {
@@ -446,6 +469,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     // one SM: live half h takes the next half-item s = ns, ns + 1, ... (accumulator s mod 4)
                     unsigned bh[2] = {0u, 0u};
                     bool got = true;
+                    const long long t_a = kTimes ? clock64() : 0;
                     if (kPair) {
                         got = mbar_wait_cluster(&ctl->acc_empty[acc], acc_phase ^ 1, status, a.wait_ns);
                     } else {
@@ -459,12 +483,15 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         }
                     }
                     if (!got) { ok = false; break; }
+                    if (kTimes) w_acc += clock64() - t_a;
                     tc_fence_after();
                     const unsigned d_tmem = tmem + acc * kTileS;                 // pair: 256 columns
                     const unsigned d0 = tmem + bh[0] * 128u, d1 = tmem + bh[1] * 128u;   // one SM: 2 x 128
                     const unsigned bhalf = 256u * (unsigned)ca.kbk;              // bytes of 128 B rows
                     for (int kb = 0; kb < kblocks; ++kb) {
+                        const long long t_o = kTimes ? clock64() : 0;
                         if (!mbar_wait(&ctl->full[stage], phase, status, a.wait_ns)) { ok = false; break; }
+                        if (kTimes) w_op += clock64() - t_o;
                         if (*(volatile int*)&ctl->abort_flag) { ok = false; break; }
                         tc_fence_after();
                         const uint8_t* sa = smem + (size_t)stage * kStageBytes;
@@ -507,6 +534,11 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             }
             if (!kPair && n_mma) atomicAdd(&a.ctr->items, n_mma);
             if (!ok) ctl->abort_flag = 1;
+            if (kTimes) {
+                atomicAdd(&a.role_t[kRoleMma], (unsigned long long)(clock64() - t_role));
+                atomicAdd(&a.role_t[kRoleMmaOperand], (unsigned long long)w_op);
+                atomicAdd(&a.role_t[kRoleMmaAcc], (unsigned long long)w_acc);
+            }
             if (kPair) umma_commit_pair_mc(&ctl->drain, 0x1);
             else umma_commit(&ctl->drain);
             mbar_wait(&ctl->drain, 0, status, kDrainLimitNs);
@@ -526,6 +558,12 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
         unsigned long long n_screen_acc = 0, n_rare = 0, n_items = 0;
         unsigned n = 0, ns = 0;   // items, and (one SM) half-items passed: the UMMA issuer's numbering
         bool ok = true;
+        // stall accounting in shared memory (lane 0 of each warp), so that it costs no registers
+        long long* racc = role_acc[warp];
+        if (kTimes && lane == 0) {
+            racc[0] = clock64();
+            for (int k = 1; k < 6; ++k) racc[k] = 0;
+        }
         for (unsigned long long qc = 0;; ++qc) {
             unsigned c;
             if (kPair) {
@@ -570,10 +608,12 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     b = (unsigned)(sub & 3);
                     bph = (unsigned)((sub >> 2) & 1);
                 }
+                if (kTimes && lane == 0) racc[1] -= clock64();
                 if (!__all_sync(0xffffffffu, mbar_wait(&ctl->meta_full[slot], mph, status, a.wait_ns))) {
                     ok = false;
                     break;
                 }
+                if (kTimes && lane == 0) racc[1] += clock64();
                 const ColMetaHot& m = meta[slot];
                 const unsigned c0 = m.c0;
                 // per-(row, S tile) fast threshold; every error term bounded by tile maxima
@@ -594,9 +634,15 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 }
                 // the thresholds above need only the metadata: the accumulator is awaited after them
                 // (warp-uniform: the TMEM loads below are warp-collective)
+                if (kTimes && lane == 0) racc[2] -= clock64();
                 if (!__all_sync(0xffffffffu, mbar_wait(&ctl->acc_full[b], bph, status, a.wait_ns))) {
                     ok = false;
                     break;
+                }
+                if (kTimes && lane == 0) {
+                    const long long now = clock64();
+                    racc[2] += now;
+                    racc[3] -= now;
                 }
                 tc_fence_after();
                 const unsigned tbase = tmem + ((q * 32u) << 16) + (kPair ? b * kTileS : b * 128u);
@@ -619,9 +665,11 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 // phase 1: every 32-column block of this warp's part is read from TMEM and tested; a
                 // lane keeps, per block, the mask of its candidates (v <= tau) and of the certified
                 // accepts among them (v <= tau_in).  No warp-collective step runs here, and the
-                // accumulator is handed back as soon as the last block is in registers.
-                uint32_t cmk0 = 0, cmk1 = 0, cmk2 = 0, cmk3 = 0, imk0 = 0, imk1 = 0, imk2 = 0, imk3 = 0;
-#pragma unroll
+                // accumulator is handed back as soon as the last block is in registers.  The block loop
+                // stays rolled (one copy of the test in the instruction cache); the per-block masks sit
+                // in a small per-thread array indexed by block.
+                uint32_t cmk[4] = {0u, 0u, 0u, 0u}, imk[4] = {0u, 0u, 0u, 0u};
+#pragma unroll 1
                 for (int i = 0; i < 4; ++i) {
                     const int cb = cb_begin + i;
                     if (cb >= cb_end) break;
@@ -637,12 +685,13 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                             else mbar_arrive(&ctl->acc_empty[b]);
                         }
                     }
-                    float vm[4];
+                    uint32_t cm = 0, im = 0;
                     if (kPair) {
                         // dense joins (CTA pair): one test per 8-column group, w = fma(-2, max p, min B~),
                         // a lower bound of every pair's v = fma(-2, p, B~) in the group with the same
                         // magnitude bounds (so the same rounding allowance in tau); four three-input maxes
-                        // and one FMA per 8 pairs
+                        // and one FMA per 8 pairs; only the groups whose value passes tau are examined
+                        // pair by pair
                         const float4 gb = *reinterpret_cast<const float4*>(&m.gminB[col0 >> 3]);
                         const float gbv[4] = {gb.x, gb.y, gb.z, gb.w};
 #pragma unroll
@@ -653,35 +702,37 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                                                          __uint_as_float(r8[3]), __uint_as_float(r8[4])),
                                                    fmaxf(__uint_as_float(r8[5]), __uint_as_float(r8[6])),
                                                    __uint_as_float(r8[7]));
-                            vm[g] = fmaf(-2.f, pm, gbv[g]);
+                            if (fmaf(-2.f, pm, gbv[g]) <= tau) {
+#pragma unroll
+                                for (int k = 8 * g; k < 8 * g + 8; ++k) {
+                                    const float v = fmaf(-2.f, __uint_as_float(raw[k]), m.nrm2f[col0 + k]);
+                                    cm |= (v <= tau ? 1u : 0u) << k;
+                                    im |= (v <= tau_in ? 1u : 0u) << k;
+                                }
+                            }
                         }
                     } else {
-                        // v = fma(-2, p, B~) two pairs per packed FMA, folded by three-input mins (one
-                        // instruction per pair), one min chain per 8-column group: exact per column, which
-                        // matters where the norms vary inside a group (clustered data)
+                        // v = fma(-2, p, B~) two pairs per packed FMA (rounded once, as fmaf), folded by
+                        // three-input mins, one min chain per 8-column group: exact per column, which
+                        // matters where the norms vary inside a group (clustered data); a group that
+                        // passes tau sets its bits from the same eight values
                         const float4* nb4 = reinterpret_cast<const float4*>(&m.nrm2f[col0]);
 #pragma unroll
                         for (int g = 0; g < 4; ++g) {
                             const float4 b0 = nb4[2 * g], b1 = nb4[2 * g + 1];
                             const uint32_t* r8 = raw + 8 * g;
-                            float v0, v1, v2, v3, v4, v5, v6, v7;
-                            fma_m2_x2(__uint_as_float(r8[0]), __uint_as_float(r8[1]), b0.x, b0.y, v0, v1);
-                            fma_m2_x2(__uint_as_float(r8[2]), __uint_as_float(r8[3]), b0.z, b0.w, v2, v3);
-                            fma_m2_x2(__uint_as_float(r8[4]), __uint_as_float(r8[5]), b1.x, b1.y, v4, v5);
-                            fma_m2_x2(__uint_as_float(r8[6]), __uint_as_float(r8[7]), b1.z, b1.w, v6, v7);
-                            vm[g] = fmin3(fmin3(fmin3(v0, v1, v2), v3, v4), fminf(v5, v6), v7);
-                        }
-                    }
-                    // only the groups whose value passes tau in this lane are examined pair by pair
-                    uint32_t cm = 0, im = 0;
+                            float v[8];
+                            fma_m2_x2(__uint_as_float(r8[0]), __uint_as_float(r8[1]), b0.x, b0.y, v[0], v[1]);
+                            fma_m2_x2(__uint_as_float(r8[2]), __uint_as_float(r8[3]), b0.z, b0.w, v[2], v[3]);
+                            fma_m2_x2(__uint_as_float(r8[4]), __uint_as_float(r8[5]), b1.x, b1.y, v[4], v[5]);
+                            fma_m2_x2(__uint_as_float(r8[6]), __uint_as_float(r8[7]), b1.z, b1.w, v[6], v[7]);
+                            const float vm = fmin3(fmin3(fmin3(v[0], v[1], v[2]), v[3], v[4]), fminf(v[5], v[6]), v[7]);
+                            if (vm <= tau) {
 #pragma unroll
-                    for (int g = 0; g < 4; ++g) {
-                        if (vm[g] <= tau) {
-#pragma unroll
-                            for (int k = 8 * g; k < 8 * g + 8; ++k) {
-                                const float v = fmaf(-2.f, __uint_as_float(raw[k]), m.nrm2f[col0 + k]);
-                                cm |= (v <= tau ? 1u : 0u) << k;
-                                im |= (v <= tau_in ? 1u : 0u) << k;
+                                for (int k = 0; k < 8; ++k) {
+                                    cm |= (v[k] <= tau ? 1u : 0u) << (8 * g + k);
+                                    im |= (v[k] <= tau_in ? 1u : 0u) << (8 * g + k);
+                                }
                             }
                         }
                     }
@@ -690,19 +741,21 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         if (lim >= 31) cm = 0;
                         else if (lim >= 0) cm &= ~((2u << lim) - 1u);
                     }
-                    im &= cm;
-                    cmk0 = i == 0 ? cm : cmk0; cmk1 = i == 1 ? cm : cmk1;
-                    cmk2 = i == 2 ? cm : cmk2; cmk3 = i == 3 ? cm : cmk3;
-                    imk0 = i == 0 ? im : imk0; imk1 = i == 1 ? im : imk1;
-                    imk2 = i == 2 ? im : imk2; imk3 = i == 3 ? im : imk3;
+                    cmk[i] = cm;
+                    imk[i] = im & cm;
                 }
                 // phase 2: one warp scan for the part's certified accepts and band pairs together
                 // (accepts in the low 16 bits, band in the high 16: at most 128 of each per lane), one
                 // reservation per list, then each lane writes its pairs' canonical keys (these loops stay
                 // rolled: four unrolled copies of each overflow the instruction cache)
-                const unsigned na = __popc(imk0) + __popc(imk1) + __popc(imk2) + __popc(imk3);
-                const unsigned nb = __popc(cmk0 & ~imk0) + __popc(cmk1 & ~imk1) + __popc(cmk2 & ~imk2) +
-                                    __popc(cmk3 & ~imk3);
+                if (kTimes && lane == 0) {
+                    const long long now = clock64();
+                    racc[3] += now;
+                    racc[4] -= now;
+                }
+                const unsigned na = __popc(imk[0]) + __popc(imk[1]) + __popc(imk[2]) + __popc(imk[3]);
+                const unsigned nb = __popc(cmk[0] & ~imk[0]) + __popc(cmk[1] & ~imk[1]) + __popc(cmk[2] & ~imk[2]) +
+                                    __popc(cmk[3] & ~imk[3]);
                 const unsigned packed = na | (nb << 16);
                 if (__any_sync(0xffffffffu, packed != 0)) {
                     unsigned tot;
@@ -711,11 +764,13 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     n_screen_acc += na;
                     n_rare += nb;
                     if (ta) {
+                        if (kTimes && lane == 0) racc[5] -= clock64();
                         unsigned long long pos =
                             app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap) + (pre & 0xFFFFu);
+                        if (kTimes && lane == 0) racc[5] += clock64();
 #pragma unroll 1
                         for (int i = 0; i < 4; ++i) {
-                            uint32_t w = i == 0 ? imk0 : i == 1 ? imk1 : i == 2 ? imk2 : imk3;
+                            uint32_t w = imk[i];
                             const int col0 = (int)colbase + (cb_begin + i) * 32;
                             while (w) {
                                 const int k = __ffs(w) - 1;
@@ -726,12 +781,13 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         }
                     }
                     if (tb) {
+                        if (kTimes && lane == 0) racc[5] -= clock64();
                         unsigned long long pos =
                             app_band.reserve(tb, &a.ctr->band_reserved, a.band, a.band_cap) + (pre >> 16);
+                        if (kTimes && lane == 0) racc[5] += clock64();
 #pragma unroll 1
                         for (int i = 0; i < 4; ++i) {
-                            uint32_t w = i == 0 ? cmk0 & ~imk0 : i == 1 ? cmk1 & ~imk1 : i == 2 ? cmk2 & ~imk2
-                                                                                      : cmk3 & ~imk3;
+                            uint32_t w = cmk[i] & ~imk[i];
                             const int col0 = (int)colbase + (cb_begin + i) * 32;
                             while (w) {
                                 const int k = __ffs(w) - 1;
@@ -743,6 +799,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     }
                 }
                 __syncwarp();
+                if (kTimes && lane == 0) racc[4] += clock64();
                 if (lane == 0) mbar_arrive_cnt(&ctl->meta_empty[slot], meta_arrivals);   // done with the slot
                 ++n_items;
                 if (kPair && ++acc == 2) { acc = 0; acc_phase ^= 1; }
@@ -769,6 +826,10 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 atomicAdd(&a.ctr->rare_checks, n_rare);
             }
             if (kPair && warp == kEpiFirst && n_items) atomicAdd(&a.ctr->items, n_items);
+            if (kTimes) {
+                atomicAdd(&a.role_t[kRoleEpi], (unsigned long long)(clock64() - racc[0]));
+                for (int k = 1; k < 6; ++k) atomicAdd(&a.role_t[kRoleEpi + k], (unsigned long long)racc[k]);
+            }
         }
     }
     tc_fence_before();
@@ -949,19 +1010,26 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     a.wait_ns = pipeline_wait_ns();
     a.join_t = g.join_t;
     a.cta_t = g.cta_t;
+    a.role_t = g.role_t;
     a.nstages = g.stages;
     a.half = g.half_packed ? 1 : 0;
     a.njoins = (unsigned)g.njoins;
     TJ_CUDA(cudaMemsetAsync(&eb.ctr->chunk_next, 0, sizeof(unsigned long long), st));
     const int grid = num_sms();
-#define TJ_SCREEN(F, SP)                                                                                      \
+#define TJ_SCREEN_T(F, SP, TM)                                                                                \
     do {                                                                                                      \
-        TJ_CUDA(cudaFuncSetAttribute(screen_tc_kernel<F, SP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                     (int)screen_smem<SP, false>()));                                         \
-        launch(screen_tc_kernel<F, SP, false>, grid, kScreenThreads, screen_smem<SP, false>(), st, tm, a);   \
+        TJ_CUDA(cudaFuncSetAttribute(screen_tc_kernel<F, SP, false, TM>,                                      \
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)screen_smem<SP, false>())); \
+        launch(screen_tc_kernel<F, SP, false, TM>, grid, kScreenThreads, screen_smem<SP, false>(), st, tm, a); \
+    } while (0)
+#define TJ_SCREEN(F, SP)                                      \
+    do {                                                      \
+        if (a.role_t) TJ_SCREEN_T(F, SP, true);               \
+        else TJ_SCREEN_T(F, SP, false);                       \
     } while (0)
     if (pair) {
-        auto kern = bf ? screen_tc_kernel<1, 0, true> : screen_tc_kernel<0, 0, true>;
+        auto kern = a.role_t ? (bf ? screen_tc_kernel<1, 0, true, true> : screen_tc_kernel<0, 0, true, true>)
+                             : (bf ? screen_tc_kernel<1, 0, true> : screen_tc_kernel<0, 0, true>);
         const size_t smem = screen_smem<0, true>();
         TJ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         cudaLaunchConfig_t cfg = {};
@@ -987,6 +1055,7 @@ void screen_tc(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
     else if (split) TJ_SCREEN(0, 1);
     else TJ_SCREEN(0, 0);
 #undef TJ_SCREEN
+#undef TJ_SCREEN_T
     if (g.dump && g.dump_items)
         launch(screen_error_kernel, g.dump_items, 256, 0, st, a, (const float*)g.dump, (const uint4*)g.dump_ids,
                g.rsrc, g.ssrc, g.diag_out);

@@ -414,7 +414,6 @@ __global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) os_scatter(const ui
     uint64_t* sk = (uint64_t*)rs_dyn;                      // [kRsTile] keys grouped by digit
     uint32_t* sv = (uint32_t*)(rs_dyn + kRsTile * 8);      // [kRsTile] values (kVals)
     __shared__ uint32_t wcnt[kScWarps][256];   // per warp and digit: count, then tile-local start
-    __shared__ uint32_t hist[256];     // the tile's digit counts (published before the ranking)
     __shared__ uint32_t gdelta[256];   // global start minus tile-local start of each digit's run (mod 2^32)
     __shared__ uint32_t wtot[kScWarps];
     __shared__ uint32_t tile_sh;
@@ -425,10 +424,8 @@ __global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) os_scatter(const ui
         gave_up = 0;
     }
     for (int i = threadIdx.x; i < kScWarps * 256; i += kScThreads) (&wcnt[0][0])[i] = 0;
-    if (threadIdx.x < 256) hist[threadIdx.x] = 0;
     __syncthreads();
     const unsigned t = tile_sh;
-
     const size_t tbase = (size_t)t * kRsTile;
     const size_t wbase = tbase + (size_t)warp * (kScRounds * 32);
     uint64_t k[kScRounds];
@@ -440,23 +437,6 @@ __global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) os_scatter(const ui
         const size_t i = wbase + (size_t)r * 32 + lane;
         k[r] = i < n ? keys_in[i] : 0ull;
     }
-    // the tile's digit counts first, so that the tiles after this one can use them while this one
-    // ranks its keys (a digit the whole warp shares is added once)
-#pragma unroll
-    for (int r = 0; r < kScRounds; ++r) {
-        const bool ok = wbase + (size_t)r * 32 + lane < n;
-        const unsigned valid = __ballot_sync(0xffffffffu, ok);
-        const unsigned dg = digit_of(k[r], shift);
-        const unsigned d0 = __shfl_sync(0xffffffffu, dg, 0);
-        if (__all_sync(0xffffffffu, !ok || dg == d0)) {
-            if (lane == 0 && valid) atomicAdd(&hist[d0], (unsigned)__popc(valid));
-        } else if (ok) {
-            atomicAdd(&hist[dg], 1u);
-        }
-    }
-    __syncthreads();
-    uint64_t* mine = tstat + (size_t)t * 256 + (threadIdx.x & 255);
-    if (threadIdx.x < 256) st_status(mine, (uint64_t)hist[threadIdx.x] | (t == 0 ? kOsPre : kOsAgg));
 #pragma unroll
     for (int r = 0; r < kScRounds; ++r) {
         const bool ok = wbase + (size_t)r * 32 + lane < n;
@@ -477,10 +457,16 @@ __global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) os_scatter(const ui
         }
     }
     __syncthreads();
-    {   // per digit (threads 0..255): its tile-local start, each warp's start, and the digit's global
-        // start from the chained scan over the tiles before this one
+    {   // per digit (threads 0..255): the tile's count, published at once; its tile-local start, each
+        // warp's start, and the digit's global start from the chained scan over the tiles before this one
         const unsigned dg = threadIdx.x;
-        const uint32_t run = dg < 256 ? hist[dg] : 0u;
+        uint64_t* mine = tstat + (size_t)t * 256 + (dg & 255);
+        uint32_t run = 0;
+        if (dg < 256) {
+#pragma unroll
+            for (int w = 0; w < kScWarps; ++w) run += wcnt[w][dg];
+            st_status(mine, (uint64_t)run | (t == 0 ? kOsPre : kOsAgg));
+        }
         const uint32_t ls = block_excl_scan<kScWarps>(run, wtot);
         if (dg < 256) {
             uint32_t at = ls;

@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_structs_match_header_layout():
     assert ctypes.sizeof(_lib.Options) == 24
-    assert ctypes.sizeof(_lib.Stats) == 11 * 8 + 9 * 8 + 8 + 8 + 8 + 8 + 8 + 4 * 8
+    assert ctypes.sizeof(_lib.Stats) == 11 * 8 + 9 * 8 + 8 + 8 + 8 + 8 + 8 + 4 * 8 + 9 * 8
     assert ctypes.sizeof(_lib.BatchJoin) == 48
 
 
