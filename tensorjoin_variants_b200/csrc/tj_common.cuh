@@ -85,6 +85,21 @@ TJ_DEV void fma_m2_x2(float p0, float p1, float c0, float c1, float& v0, float& 
         "mov.b64 {%0, %1}, r;\n\t}"
         : "=f"(v0), "=f"(v1) : "f"(p0), "f"(p1), "f"(c0), "f"(c1), "f"(-2.0f));
 }
+// Position of the j-th (0-based) set bit of w (w has more than j set bits): a binary search on the
+// popcounts of the low halves.
+TJ_DEV int nth_set_bit(uint32_t w, unsigned j) {
+    int pos = 0;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        const unsigned c = __popc(w & ((1u << s) - 1u));
+        if (j >= c) {
+            j -= c;
+            w >>= s;
+            pos += s;
+        }
+    }
+    return pos;
+}
 // min of three floats in one instruction (sm_100); a NaN operand is ignored, as by fminf.
 TJ_DEV float fmin3(float a, float b, float c) {
     float r;

@@ -819,6 +819,112 @@ struct TileOut {
     int ntiles;
 };
 
+// Constants of the fused operand pass for rows of d elements (see prep_tiles_kernel).
+struct PrepBounds {
+    double up64;     // (1 + 2 (d + 4) 2^-53)(1 + 2^-50): A's relative error and its product's rounding
+    float up32;      // 1 + (d + 16) 2^-23: FP32 sums of d squares (exact in FP32 for d <= 128)
+    float slack32;   // d 2^-140: the products that underflow
+    double gb;       // (d + 2) 2^-53: beta = |nrm2f - nrm2| + 2 gb nrm2
+    TJ_DEV explicit PrepBounds(int d)
+        : up64((1.0 + 2.0 * (double)(d + 4) * 0x1p-53) * (1.0 + 0x1p-50)),
+          up32(1.f + (float)(d + 16) * 0x1p-23f),
+          slack32((float)d * 0x1p-140f),
+          gb((double)(d + 2) * 0x1p-53) {}
+};
+
+// One sorted row of the fused operand pass: a group of kL lanes holds the row, kE consecutive elements
+// per lane (k0 = kE sub).  Writes the row's operands (when rv), its norms and bounds (its first four
+// lanes, one bound each), and adds the row to this lane's centroid / box partials and bound maxima.
+// Every lane of the warp calls it (the row reduction is a shuffle tree inside the group).
+template <int kScreen, int kSplit, int kE, int kL>
+TJ_DEV void prep_row(const float (&xa)[kE], const float (&cf)[kE], const double (&cdv)[kE], bool rv, long long r,
+                     int k0, int d, unsigned sub, unsigned lane, const PrepBounds& pb, uint16_t* op, double* nrm2,
+                     float* nrm2f, float* zn, float* en, float* yn, float* zl, float (&ps)[kE], float (&pl)[kE],
+                     float (&ph)[kE], float& mtask, float& mb, float& mbeta, unsigned& flags) {
+    constexpr int kFmt = (kScreen == kScreenBF16 || kScreen == kScreenBF16X3) ? 1 : 0;
+    constexpr int kPad = kE * kL;
+    constexpr int opw = kSplit ? 2 * kPad : kPad;
+    double sx = 0.0;
+    float sz = 0.f, se = 0.f, sl = 0.f;
+    uint32_t hw[kE / 2], lw[kE / 2];
+#pragma unroll
+    for (int q = 0; q < kE; ++q) {
+        const float x = xa[q];
+        const float sd = x - cf[q];   // fl32(x'): |x' - sd| <= 2^-24 |x'| per element
+        const double xd = (double)x - cdv[q];
+        sx = fma(xd, xd, sx);
+        if (kFmt == 0 && fabsf(sd) > 65504.f) flags |= 2u;
+        uint16_t hbits, lbits = 0;
+        const float zh = round16<kFmt>(sd, hbits);
+        const float d1 = sd - zh;   // exact (zh is sd rounded to 8 or 11 bits)
+        if (kSplit) {
+            const float zlo = round16<kFmt>(d1, lbits);
+            const float ed = d1 - zlo;   // exact: sd - z_hi - z_lo
+            const float z = zh + zlo;
+            sz = fmaf(z, z, sz);
+            se = fmaf(ed, ed, se);
+            sl = fmaf(zlo, zlo, sl);
+        } else {
+            sz = fmaf(zh, zh, sz);
+            se = fmaf(d1, d1, se);   // d1 = sd - z_hi exactly
+        }
+        if (q & 1) {
+            hw[q / 2] |= (uint32_t)hbits << 16;
+            lw[q / 2] |= (uint32_t)lbits << 16;
+        } else {
+            hw[q / 2] = hbits;
+            lw[q / 2] = lbits;
+        }
+        if (rv && k0 + q < d) {
+            ps[q] += x;
+            pl[q] = fminf(pl[q], x);
+            ph[q] = fmaxf(ph[q], x);
+        }
+    }
+    if (rv) {
+#pragma unroll
+        for (int v = 0; v < kE / 4; ++v) {
+            *reinterpret_cast<uint2*>(op + (size_t)r * opw + k0 + 4 * v) = make_uint2(hw[2 * v], hw[2 * v + 1]);
+            if (kSplit)
+                *reinterpret_cast<uint2*>(op + (size_t)r * opw + kPad + k0 + 4 * v) =
+                    make_uint2(lw[2 * v], lw[2 * v + 1]);
+        }
+    }
+#pragma unroll
+    for (int o = kL / 2; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sz += __shfl_xor_sync(0xffffffffu, sz, o);
+        se += __shfl_xor_sync(0xffffffffu, se, o);
+        if (kSplit) sl += __shfl_xor_sync(0xffffffffu, sl, o);
+    }
+    // the four bounds of the row are taken by its first four lanes, one square root each
+    const unsigned task = sub & 3u;   // 0: |x - c|, 1: |z|, 2: |x - c - z|, 3: |z_lo|
+    float rt;
+    if (task == 0) {
+        rt = __fsqrt_ru(__double2float_ru(sx * pb.up64));
+    } else {
+        const float v32 = task == 1 ? sz : task == 2 ? se : sl;
+        rt = (task == 3 && !kSplit) ? 0.f : __fsqrt_ru(__fmul_ru(__fadd_ru(v32, pb.slack32), pb.up32));
+    }
+    // E also covers x' - sd (at most 2^-24 |x'| per element, so 2^-24 Y in norm; 2^-23 Y taken)
+    const float ynorm = __shfl_sync(0xffffffffu, rt, (int)(lane & ~(unsigned)(kL - 1)));
+    if (task == 2) rt = __fadd_ru(rt, __fmul_ru(0x1p-23f, ynorm));
+    if (rv && sub < 4) {
+        float* dst = task == 0 ? yn : task == 1 ? zn : task == 2 ? en : zl;
+        dst[r] = rt;
+        mtask = fmaxf(mtask, rt);
+    }
+    if (rv && sub == 0) {
+        if (!(sx <= 0x1p100)) flags |= 1u;   // also NaN / Inf anywhere in the row
+        const float sf = __double2float_rn(sx);
+        nrm2[r] = sx;
+        nrm2f[r] = sf;
+        mb = fmaxf(mb, sf);
+        const double bt = fabs((double)sf - sx) + 2.0 * pb.gb * sx;
+        mbeta = fmaxf(mbeta, f32_up(bt * (1.0 + 0x1p-40)));
+    }
+}
+
 // Operand preparation and tile statistics in one pass, for 16-bit screens over FP32 rows with
 // d % 4 == 0 and kpad = kE kL <= 128 (one block of 256 threads per tile of 128 or 256 sorted rows;
 // kL lanes per row, each lane kE consecutive elements).  Every gathered row is read from HBM once:
@@ -828,18 +934,18 @@ struct TileOut {
 // of H).  Partials are combined across the row groups of a warp by shuffles and across the eight
 // warps in shared memory.
 //
-// Arithmetic.  x' = x - c is carried exactly as s + err (s = fl32(x - c), err from TwoSum), so the
-// operands and the bounds need no FP64 conversions per element:
-//   z_hi = round16(s);  r = fl32((s - z_hi) + err) (s - z_hi is exact) with its TwoSum residual rr;
-//   z_lo = round16(r);  x' - z_hi - z_lo = (r - z_lo) + rr, rounded once to FP32.
-// A = ||x'||^2 stays an FP64 sum (its relative error enters the certificate).  Z >= ||z_hi + z_lo||,
-// E >= ||x' - z||, Zl >= ||z_lo|| and the tile radius are FP32 sums of squares made rigorous upper
-// bounds: each term is exact or rounded once (relative 2^-24; additions are exact in the subnormal
-// range, a product that underflows errs by at most 2^-150), a chain of m <= d + 5 roundings errs by at
-// most gamma_m, so  true <= (S + d 2^-140) (1 + (d + 16) 2^-23);  that widening and the square root
-// are taken with upward rounding (FP32 .ru operations), as is Y = sqrt(A (1 + 2 g)).  A non-finite
-// element makes A non-finite, which flags the row.  The centroid needs no accuracy (the radius is
-// measured from the value written).
+// Arithmetic.  The operands split s = fl32(x - c), which differs from x' = x - c by at most
+// 2^-24 |x'| per element (a difference that is subnormal is exact): z_hi = round16(s), and with the
+// split z_lo = round16(s - z_hi); s - z_hi and s - z_hi - z_lo are exact in FP32.  So
+// ||x' - z|| <= ||s - z|| + 2^-24 ||x'||, and E adds 2^-23 Y to the bound of ||s - z||.
+// A = ||x'||^2 stays an FP64 sum of the exact x' (its relative error enters the certificate).
+// Z >= ||z_hi + z_lo||, ||s - z||, Zl >= ||z_lo|| and the tile radius are FP32 sums of squares made
+// rigorous upper bounds: each term is exact or rounded once (relative 2^-24; additions are exact in
+// the subnormal range, a product that underflows errs by at most 2^-150), a chain of m <= d + 5
+// roundings errs by at most gamma_m, so  true <= (S + d 2^-140) (1 + (d + 16) 2^-23);  that widening
+// and the square root are taken with upward rounding (FP32 .ru operations), as is
+// Y = sqrt(A (1 + 2 g)).  A non-finite element makes A non-finite, which flags the row.  The
+// centroid needs no accuracy (the radius is measured from the value written).
 template <int kScreen, int kSplit, int kE, int kL, bool kHalves>
 __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict__ src, long long n, int d, int tile,
                                                          const uint32_t* __restrict__ perm,
@@ -848,13 +954,11 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
                                                          uint16_t* op, double* nrm2, float* nrm2f, float* zn,
                                                          float* en, float* yn, float* zl, TileOut T, TileOut H,
                                                          unsigned long long* status) {
-    constexpr int kFmt = (kScreen == kScreenBF16 || kScreen == kScreenBF16X3) ? 1 : 0;
     constexpr int kPad = kE * kL;
     constexpr int kNG = 256 / kL;              // row groups per block
     constexpr int kRows = 128 / kNG;           // rows of one group in one 128-row half
     constexpr int kU = kRows < 2 ? kRows : 2;  // rows whose loads are issued together
     constexpr int kV = kE / 4;                 // float4 loads per lane and row
-    constexpr int opw = kSplit ? 2 * kPad : kPad;
     static_assert(kE % 4 == 0 && kPad <= 128 && kL >= 4 && kL <= 32, "fused preparation shape");
     __shared__ float wsum[2][8][kPad], wmin[2][8][kPad], wmax[2][8][kPad];   // [half][warp][element]
     __shared__ float wrow[2][6][8];          // [half][bound][warp] row-bound maxima
@@ -876,10 +980,8 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
         cf[q] = (k0 + q < d) ? center[k0 + q] : 0.f;
         cdv[q] = (double)cf[q];
     }
-    const double up64 = (1.0 + 2.0 * (double)(d + 4) * 0x1p-53) * (1.0 + 0x1p-50);
-    const float up32 = 1.f + (float)(d + 16) * 0x1p-23f;   // exact in FP32 for d <= 128
-    const float slack32 = (float)d * 0x1p-140f;
-    const double gb = (double)(d + 2) * 0x1p-53;           // beta: |nrm2f - nrm2| + 2 gb nrm2
+    const PrepBounds pb(d);
+    const float up32 = pb.up32, slack32 = pb.slack32;
     unsigned flags = 0;
 
     for (int h = 0; h < halves; ++h) {
@@ -905,94 +1007,15 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
                 }
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
-                    const bool rv = ii[u] < nv;
-                    double sx = 0.0;
-                    float sz = 0.f, se = 0.f, sl = 0.f;
-                    uint32_t hw[kE / 2], lw[kE / 2];
+                    float xa[kE];
 #pragma unroll
                     for (int q = 0; q < kE; ++q) {
                         const float4 f4 = xv[u][q / 4];
-                        const float x = (q & 3) == 0 ? f4.x : (q & 3) == 1 ? f4.y : (q & 3) == 2 ? f4.z : f4.w;
-                        const float sd = x - cf[q];
-                        const float bb = sd - x;
-                        const float err = (x - (sd - bb)) + (-cf[q] - bb);
-                        const double xd = (double)x - cdv[q];
-                        sx = fma(xd, xd, sx);
-                        if (kFmt == 0 && fabsf(sd) > 65504.f) flags |= 2u;
-                        uint16_t hbits, lbits = 0;
-                        const float zh = round16<kFmt>(sd, hbits);
-                        const float d1 = sd - zh;   // exact
-                        if (kSplit) {
-                            const float r = d1 + err;
-                            const float b2 = r - d1;
-                            const float rr = (d1 - (r - b2)) + (err - b2);
-                            const float zlo = round16<kFmt>(r, lbits);
-                            const float ed = (r - zlo) + rr;
-                            const float z = zh + zlo;
-                            sz = fmaf(z, z, sz);
-                            se = fmaf(ed, ed, se);
-                            sl = fmaf(zlo, zlo, sl);
-                        } else {
-                            const float ed = d1 + err;
-                            sz = fmaf(zh, zh, sz);
-                            se = fmaf(ed, ed, se);
-                        }
-                        if (q & 1) {
-                            hw[q / 2] |= (uint32_t)hbits << 16;
-                            lw[q / 2] |= (uint32_t)lbits << 16;
-                        } else {
-                            hw[q / 2] = hbits;
-                            lw[q / 2] = lbits;
-                        }
-                        if (rv && k0 + q < d) {
-                            ps[q] += x;
-                            pl[q] = fminf(pl[q], x);
-                            ph[q] = fmaxf(ph[q], x);
-                        }
+                        xa[q] = (q & 3) == 0 ? f4.x : (q & 3) == 1 ? f4.y : (q & 3) == 2 ? f4.z : f4.w;
                     }
-                    const long long r = r0 + ii[u];
-                    if (rv) {
-#pragma unroll
-                        for (int v = 0; v < kE / 4; ++v) {
-                            *reinterpret_cast<uint2*>(op + (size_t)r * opw + k0 + 4 * v) =
-                                make_uint2(hw[2 * v], hw[2 * v + 1]);
-                            if (kSplit)
-                                *reinterpret_cast<uint2*>(op + (size_t)r * opw + kPad + k0 + 4 * v) =
-                                    make_uint2(lw[2 * v], lw[2 * v + 1]);
-                        }
-                    }
-#pragma unroll
-                    for (int o = kL / 2; o > 0; o >>= 1) {
-                        sx += __shfl_xor_sync(0xffffffffu, sx, o);
-                        sz += __shfl_xor_sync(0xffffffffu, sz, o);
-                        se += __shfl_xor_sync(0xffffffffu, se, o);
-                        if (kSplit) sl += __shfl_xor_sync(0xffffffffu, sl, o);
-                    }
-                    // the four bounds of the row are taken by its first four lanes, one square root each
-                    const unsigned task = sub & 3u;   // 0: |x - c|, 1: |z|, 2: |x - c - z|, 3: |z_lo|
-                    float rt;
-                    if (task == 0) {
-                        rt = __fsqrt_ru(__double2float_ru(sx * up64));
-                    } else {
-                        const float v32 = task == 1 ? sz : task == 2 ? se : sl;
-                        rt = (task == 3 && !kSplit) ? 0.f : __fsqrt_ru(__fmul_ru(__fadd_ru(v32, slack32), up32));
-                    }
-                    const float ynorm = __shfl_sync(0xffffffffu, rt, (int)(lane & ~(unsigned)(kL - 1)));
-                    if (task == 2) rt = __fadd_ru(rt, __fmul_ru(0x1p-50f, ynorm));
-                    if (rv && sub < 4) {
-                        float* dst = task == 0 ? yn : task == 1 ? zn : task == 2 ? en : zl;
-                        dst[r] = rt;
-                        mtask = fmaxf(mtask, rt);
-                    }
-                    if (rv && sub == 0) {
-                        if (!(sx <= 0x1p100)) flags |= 1u;   // also NaN / Inf anywhere in the row
-                        const float sf = __double2float_rn(sx);
-                        nrm2[r] = sx;
-                        nrm2f[r] = sf;
-                        mb = fmaxf(mb, sf);
-                        const double bt = fabs((double)sf - sx) + 2.0 * gb * sx;
-                        mbeta = fmaxf(mbeta, f32_up(bt * (1.0 + 0x1p-40)));
-                    }
+                    prep_row<kScreen, kSplit, kE, kL>(xa, cf, cdv, ii[u] < nv, r0 + ii[u], k0, d, (unsigned)sub, lane,
+                                                      pb, op, nrm2, nrm2f, zn, en, yn, zl, ps, pl, ph, mtask, mb,
+                                                      mbeta, flags);
                 }
             }
         }
@@ -1165,6 +1188,196 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
                 O.nvalid[e] = (uint32_t)max(nv, 0);
                 O.row0[e] = (uint32_t)r0;
             }
+        }
+    }
+}
+
+// The fused operand pass for rows of at most 32 elements (kpad 16 or 32): one warp per tile, eight
+// tiles per block, 4 elements per lane and 32 / kL rows per warp step; every combine is a shuffle, so
+// the tile needs no shared memory and no block barrier (a 128-row tile of 8-element rows is 4 KB of
+// input: a block per tile spent its time in barriers and serial combines).  The arithmetic is
+// prep_row's, the statistics those of prep_tiles_kernel.
+template <int kScreen, int kSplit, int kL, bool kHalves>
+__global__ void __launch_bounds__(256) prep_tiles_warp_kernel(const float* __restrict__ src, long long n, int d,
+                                                              int tile, int ntiles, const uint32_t* __restrict__ perm,
+                                                              const float* __restrict__ center,
+                                                              const uint32_t* row0_in, const uint32_t* nvalid_in,
+                                                              uint16_t* op, double* nrm2, float* nrm2f, float* zn,
+                                                              float* en, float* yn, float* zl, TileOut T, TileOut H,
+                                                              unsigned long long* status) {
+    constexpr int kE = 4;
+    constexpr int kRW = 32 / kL;               // rows per warp step
+    constexpr int kSteps = 128 / kRW;          // steps per 128-row half
+    constexpr int kU = 4;                      // steps whose loads are issued together
+    static_assert(kL == 4 || kL == 8, "rows of 16 or 32 padded elements");
+    const unsigned lane = threadIdx.x & 31;
+    const int t = (int)blockIdx.x * 8 + (int)(threadIdx.x >> 5);
+    if (t >= ntiles) return;   // whole warps; no block barrier in this kernel
+    const bool tabled = row0_in != nullptr;
+    const long long r0 = tabled ? (long long)row0_in[t] : (long long)t * tile;
+    const int nv = tabled ? (int)nvalid_in[t] : (int)min((long long)tile, n - r0);
+    const int halves = tile == 256 ? 2 : 1;
+    const unsigned grp = lane / kL, sub = lane % kL;
+    const int k0 = kE * (int)sub;
+    const bool kin = k0 < d;
+    float cf[kE];
+    double cdv[kE];
+#pragma unroll
+    for (int q = 0; q < kE; ++q) {
+        cf[q] = (k0 + q < d) ? center[k0 + q] : 0.f;
+        cdv[q] = (double)cf[q];
+    }
+    const PrepBounds pb(d);
+    unsigned flags = 0;
+    // per half: the lane's centroid / box partials (combined over the warp's row groups below) and the
+    // bound maxima (lanes 0-3 of a group: Y, Z, E, Zl; lane 0 also B and beta)
+    float hs[2][kE], hl[2][kE], hh[2][kE], hm[2][6];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        float ps[kE], pl[kE], ph[kE];
+#pragma unroll
+        for (int q = 0; q < kE; ++q) { ps[q] = 0.f; pl[q] = INFINITY; ph[q] = -INFINITY; }
+        float mtask = 0.f, mb = 0.f, mbeta = 0.f;
+        if (h < halves && h * 128 < nv) {   // uniform across the warp
+            for (int s0 = 0; s0 < kSteps; s0 += kU) {
+                float4 xv[kU];
+                int ii[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    ii[u] = h * 128 + (s0 + u) * kRW + (int)grp;
+                    xv[u] = (ii[u] < nv && kin)
+                                ? __ldg(reinterpret_cast<const float4*>(src + (size_t)perm[r0 + ii[u]] * (size_t)d + k0))
+                                : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const float xa[kE] = {xv[u].x, xv[u].y, xv[u].z, xv[u].w};
+                    prep_row<kScreen, kSplit, kE, kL>(xa, cf, cdv, ii[u] < nv, r0 + ii[u], k0, d, sub, lane, pb, op,
+                                                      nrm2, nrm2f, zn, en, yn, zl, ps, pl, ph, mtask, mb, mbeta, flags);
+                }
+            }
+        }
+#pragma unroll
+        for (int o = kL; o < 32; o <<= 1) {
+#pragma unroll
+            for (int q = 0; q < kE; ++q) {
+                ps[q] += __shfl_xor_sync(0xffffffffu, ps[q], o);
+                pl[q] = fminf(pl[q], __shfl_xor_sync(0xffffffffu, pl[q], o));
+                ph[q] = fmaxf(ph[q], __shfl_xor_sync(0xffffffffu, ph[q], o));
+            }
+            mtask = fmaxf(mtask, __shfl_xor_sync(0xffffffffu, mtask, o));
+            mb = fmaxf(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+            mbeta = fmaxf(mbeta, __shfl_xor_sync(0xffffffffu, mbeta, o));
+        }
+#pragma unroll
+        for (int q = 0; q < kE; ++q) { hs[h][q] = ps[q]; hl[h][q] = pl[q]; hh[h][q] = ph[q]; }
+        // bound maxima to every lane: Y, Z, E, Zl from lanes 0-3, B and beta from lane 0
+#pragma unroll
+        for (int b = 0; b < 4; ++b) hm[h][b] = __shfl_sync(0xffffffffu, mtask, b);
+        hm[h][4] = __shfl_sync(0xffffffffu, mb, 0);
+        hm[h][5] = __shfl_sync(0xffffffffu, mbeta, 0);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) flags |= __shfl_xor_sync(0xffffffffu, flags, o);
+    if (lane == 0 && flags) {
+        if (flags & 1u) atomicOr(status, (unsigned long long)kStatusBadInput);
+        if (flags & 2u) atomicOr(status, (unsigned long long)kStatusFp16Range);
+    }
+    const int nvh0 = min(nv, 128), nvh1 = max(0, min(nv - 128, 128));
+    float ct[kE], c0h[kE], c1h[kE];
+#pragma unroll
+    for (int q = 0; q < kE; ++q) {
+        const int k = k0 + q;
+        ct[q] = (float)(((double)hs[0][q] + (double)hs[1][q]) / (double)max(nv, 1));
+        c0h[q] = (float)((double)hs[0][q] / (double)max(nvh0, 1));
+        c1h[q] = (float)((double)hs[1][q] / (double)max(nvh1, 1));
+        if (grp == 0 && k < d) {
+            T.ctrT[(size_t)k * T.ntiles + t] = ct[q];
+            T.loT[(size_t)k * T.ntiles + t] = fminf(hl[0][q], hl[1][q]);
+            T.hiT[(size_t)k * T.ntiles + t] = fmaxf(hh[0][q], hh[1][q]);
+            if (kHalves) {
+                const size_t e0 = (size_t)k * H.ntiles + 2 * t;
+                H.ctrT[e0] = c0h[q];
+                H.loT[e0] = hl[0][q];
+                H.hiT[e0] = hh[0][q];
+                H.ctrT[e0 + 1] = c1h[q];
+                H.loT[e0 + 1] = hl[1][q];
+                H.hiT[e0 + 1] = hh[1][q];
+            }
+        }
+    }
+    // radius pass (the tile's rows again, from L2), bounded as in prep_tiles_kernel
+    float mt = 0.f, mh0 = 0.f, mh1 = 0.f;
+    for (int h = 0; h < halves; ++h) {
+        if (h * 128 >= nv) break;   // uniform
+        for (int s0 = 0; s0 < kSteps; s0 += kU) {
+            float4 xv[kU];
+            int ii[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                ii[u] = h * 128 + (s0 + u) * kRW + (int)grp;
+                xv[u] = (ii[u] < nv && kin)
+                            ? __ldg(reinterpret_cast<const float4*>(src + (size_t)perm[r0 + ii[u]] * (size_t)d + k0))
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const float xa[kE] = {xv[u].x, xv[u].y, xv[u].z, xv[u].w};
+                float st_ = 0.f, sh = 0.f;
+#pragma unroll
+                for (int q = 0; q < kE; ++q) {
+                    const bool in = k0 + q < d;
+                    const float df = in ? xa[q] - ct[q] : 0.f;
+                    st_ = fmaf(df, df, st_);
+                    if (kHalves) {
+                        const float dh = in ? xa[q] - (h ? c1h[q] : c0h[q]) : 0.f;
+                        sh = fmaf(dh, dh, sh);
+                    }
+                }
+#pragma unroll
+                for (int o = kL / 2; o > 0; o >>= 1) {
+                    st_ += __shfl_xor_sync(0xffffffffu, st_, o);
+                    if (kHalves) sh += __shfl_xor_sync(0xffffffffu, sh, o);
+                }
+                if (ii[u] < nv) {
+                    mt = fmaxf(mt, st_);
+                    if (kHalves) {
+                        if (h) mh1 = fmaxf(mh1, sh);
+                        else mh0 = fmaxf(mh0, sh);
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mt = fmaxf(mt, __shfl_xor_sync(0xffffffffu, mt, o));
+        mh0 = fmaxf(mh0, __shfl_xor_sync(0xffffffffu, mh0, o));
+        mh1 = fmaxf(mh1, __shfl_xor_sync(0xffffffffu, mh1, o));
+    }
+    if (lane < 3 && (lane == 0 || kHalves)) {   // lane 0: the tile; lanes 1, 2: the halves
+        const int w = (int)lane;
+        const float m = w == 0 ? mt : (w == 1 ? mh0 : mh1);
+        const int hv = w == 0 ? nv : (w == 1 ? nvh0 : nvh1);
+        TileOut& O = w == 0 ? T : H;
+        const int e = w == 0 ? t : 2 * t + (w - 1);
+        O.rad[e] = hv > 0 ? __fsqrt_ru(__fmul_ru(__fadd_ru(m, pb.slack32), pb.up32)) : 0.f;
+        float mx[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+            mx[q] = w == 0 ? fmaxf(hm[0][q], hm[1][q]) : (w == 1 ? hm[0][q] : hm[1][q]);
+        O.maxY[e] = mx[0];
+        O.maxZ[e] = mx[1];
+        O.maxE[e] = mx[2];
+        O.maxZl[e] = mx[3];
+        O.maxB[e] = mx[4];
+        O.beta[e] = mx[5];
+        if (w > 0) {
+            O.nvalid[e] = (uint32_t)hv;
+            O.row0[e] = (uint32_t)(r0 + 128 * (w - 1));
+        } else if (!tabled) {
+            O.nvalid[e] = (uint32_t)max(nv, 0);
+            O.row0[e] = (uint32_t)r0;
         }
     }
 }
@@ -1557,10 +1770,14 @@ void prep_tiles(Side& s, const float* center, int tile, TileSet& ts, TileSet* ha
     launch(prep_tiles_kernel<SCR, SPLIT, E, L, HV>, (unsigned)ntiles, 256, 0, st, (const float*)s.src, n, s.d, tile, \
            (const uint32_t*)s.perm.p, center, r0, nvv, s.op.p, s.nrm2.p, s.nrm2f.p, s.zn.p, s.en.p, s.yn.p,      \
            s.zl.p, T, H, status)
+#define TJ_PTW(SCR, SPLIT, L, HV)                                                                            \
+    launch(prep_tiles_warp_kernel<SCR, SPLIT, L, HV>, (unsigned)((ntiles + 7) / 8), 256, 0, st, (const float*)s.src, \
+           n, s.d, tile, ntiles, (const uint32_t*)s.perm.p, center, r0, nvv, s.op.p, s.nrm2.p, s.nrm2f.p, s.zn.p,    \
+           s.en.p, s.yn.p, s.zl.p, T, H, status)
 #define TJ_PT_L(SCR, SPLIT, HV)                                  \
     do {                                                         \
-        if (s.kpad == 16) TJ_PT(SCR, SPLIT, 4, 4, HV);           \
-        else if (s.kpad == 32) TJ_PT(SCR, SPLIT, 4, 8, HV);      \
+        if (s.kpad == 16) TJ_PTW(SCR, SPLIT, 4, HV);             \
+        else if (s.kpad == 32) TJ_PTW(SCR, SPLIT, 8, HV);        \
         else if (s.kpad == 64) TJ_PT(SCR, SPLIT, 8, 8, HV);      \
         else TJ_PT(SCR, SPLIT, 8, 16, HV);                       \
     } while (0)
@@ -1577,6 +1794,7 @@ void prep_tiles(Side& s, const float* center, int tile, TileSet& ts, TileSet* ha
     }
 #undef TJ_PT_H
 #undef TJ_PT_L
+#undef TJ_PTW
 #undef TJ_PT
 }
 

@@ -276,7 +276,9 @@ __global__ void refine_kernel(const RefineArgs a) {
                 const JoinParams& jp = a.jps[lo];
                 const uint64_t local = key - jp.key_off;
                 const uint64_t i = local / (uint64_t)jp.n_cols, j = local - i * (uint64_t)jp.n_cols;
-                if (a.is_int) {   // int14 rows: the exact integer predicate decides every pair
+                if (i >= (uint64_t)jp.n_rows) {   // not a key the screen wrote: flagged, no row is read
+                    atomicOr(&a.ctr->status, (unsigned long long)kStatusGuard);
+                } else if (a.is_int) {   // int14 rows: the exact integer predicate decides every pair
                     const int16_t* xi = (const int16_t*)a.rsrc[lo] + (size_t)i * jp.d;
                     const int16_t* yi = (const int16_t*)a.ssrc[lo] + (size_t)j * jp.d;
                     ok = exact_d2_i16(xi, yi, jp.d) <= a.T_int;

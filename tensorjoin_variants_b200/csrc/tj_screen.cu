@@ -763,37 +763,56 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     const unsigned ta = tot & 0xFFFFu, tb = tot >> 16;
                     n_screen_acc += na;
                     n_rare += nb;
-                    if (ta) {
-                        if (kTimes && lane == 0) racc[5] -= clock64();
-                        unsigned long long pos =
-                            app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap) + (pre & 0xFFFFu);
-                        if (kTimes && lane == 0) racc[5] += clock64();
+                    // one reservation per list (warp-collective); then the warp writes each list's keys
+                    // 32 at a time in the warp's order (lane by lane, block by block, column by column):
+                    // slot s finds its lane by a shuffle search over the lanes' prefixes and its column
+                    // as the right set bit of that lane's masks, so each store of the warp covers 32
+                    // consecutive slots and the loop runs once per 32 keys, however unevenly the lanes'
+                    // keys fall
+                    if (kTimes && lane == 0) racc[5] -= clock64();
+                    unsigned long long pa = 0, pb = 0;
+                    if (ta) pa = app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap);
+                    if (tb) pb = app_band.reserve(tb, &a.ctr->band_reserved, a.band, a.band_cap);
+                    if (kTimes && lane == 0) racc[5] += clock64();
 #pragma unroll 1
-                        for (int i = 0; i < 4; ++i) {
-                            uint32_t w = imk[i];
-                            const int col0 = (int)colbase + (cb_begin + i) * 32;
-                            while (w) {
-                                const int k = __ffs(w) - 1;
-                                w &= w - 1;
-                                if (pos < a.acc_cap) a.acc[pos] = pair_key(jp, oi, m.perm[col0 + k]);
-                                ++pos;
+                    for (int list = 0; list < 2; ++list) {   // 0: certified accepts, 1: band
+                        const unsigned tl = list ? tb : ta;
+                        if (!tl) continue;   // warp-uniform
+                        const unsigned mypre = list ? (pre >> 16) : (pre & 0xFFFFu);
+                        uint32_t mk[4];
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) mk[i] = list ? (cmk[i] & ~imk[i]) : imk[i];
+                        uint64_t* buf = list ? a.band : a.acc;
+                        const unsigned long long cap = list ? a.band_cap : a.acc_cap;
+                        const unsigned long long first = list ? pb : pa;
+                        for (unsigned s0 = 0; s0 < tl; s0 += 32) {
+                            const unsigned sidx = s0 + lane;
+                            unsigned owner = 0;   // the last lane whose prefix is <= sidx
+#pragma unroll
+                            for (unsigned step = 16; step > 0; step >>= 1) {
+                                const unsigned cand = owner + step;   // <= 31
+                                if (__shfl_sync(0xffffffffu, mypre, cand) <= sidx) owner = cand;
                             }
-                        }
-                    }
-                    if (tb) {
-                        if (kTimes && lane == 0) racc[5] -= clock64();
-                        unsigned long long pos =
-                            app_band.reserve(tb, &a.ctr->band_reserved, a.band, a.band_cap) + (pre >> 16);
-                        if (kTimes && lane == 0) racc[5] += clock64();
-#pragma unroll 1
-                        for (int i = 0; i < 4; ++i) {
-                            uint32_t w = cmk[i] & ~imk[i];
-                            const int col0 = (int)colbase + (cb_begin + i) * 32;
-                            while (w) {
-                                const int k = __ffs(w) - 1;
-                                w &= w - 1;
-                                if (pos < a.band_cap) a.band[pos] = pair_key(jp, oi, m.perm[col0 + k]);
-                                ++pos;
+                            unsigned j = sidx - __shfl_sync(0xffffffffu, mypre, owner);
+                            const uint32_t w0 = __shfl_sync(0xffffffffu, mk[0], owner);
+                            const uint32_t w1 = __shfl_sync(0xffffffffu, mk[1], owner);
+                            const uint32_t w2 = __shfl_sync(0xffffffffu, mk[2], owner);
+                            const uint32_t w3 = __shfl_sync(0xffffffffu, mk[3], owner);
+                            const uint32_t ooi = __shfl_sync(0xffffffffu, oi, owner);
+                            if (sidx < tl) {
+                                const unsigned c0n = __popc(w0), c1n = __popc(w1), c2n = __popc(w2);
+                                int blk;
+                                uint32_t wsel;
+                                if (j < c0n) { blk = 0; wsel = w0; }
+                                else if ((j -= c0n) < c1n) { blk = 1; wsel = w1; }
+                                else if ((j -= c1n) < c2n) { blk = 2; wsel = w2; }
+                                else { j -= c2n; blk = 3; wsel = w3; }
+                                const int col = (int)colbase + (cb_begin + blk) * 32 + nth_set_bit(wsel, j);
+                                const uint32_t oj = m.perm[col];
+                                const uint64_t key = jp.self_join ? pair_key(jp, ooi, oj)
+                                                                  : jp.key_off + (uint64_t)ooi * (uint64_t)jp.n_cols + oj;
+                                const unsigned long long pos = first + sidx;
+                                if (pos < cap) buf[pos] = key;
                             }
                         }
                     }
