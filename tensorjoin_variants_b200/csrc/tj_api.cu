@@ -634,7 +634,8 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
                     }
                 tile_stats(*g.S[c], 128, H, st);
             }
-            hv[c] = HalfView{K.tR.ctrT.p, K.tR.loT.p, K.tR.hiT.p, K.tR.rad.p, H.ctrT.p, H.loT.p, H.hiT.p, H.rad.p,
+            tile_stats_rowmajor(H, st);
+            hv[c] = HalfView{K.tR.ctrT.p, K.tR.loT.p, K.tR.hiT.p, K.tR.rad.p, H.ctrR.p, H.loR.p, H.hiR.p, H.rad.p,
                              H.nvalid.p, K.tR.ntiles, H.ntiles, g.rbase[c], g.sbase[c], cls_d[c], 0};
         }
         half_masks(hv, cand, g.ntR_total, d_rt.p, d_jps.p, self, st);
@@ -818,11 +819,16 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
     const int bits = bits_for(kspace);   // sentinel low bits (all ones) exceed every valid key
     if (guards) launch(guard_fill, 1, 256, 0, st, keys.p + slots);   // keys holds >= slots + gs words
     if (slots > 1) {
-        DBuf<uint64_t> ktmp(slots + gs, st);
+        // an odd number of single-sweep passes ends in the temporaries: they are then a result buffer
+        // and the two buffers change places instead of copying the keys back
+        const bool swap = radix_result_in_tmp(slots, bits);
+        DBuf<uint64_t> ktmp = swap ? DBuf<uint64_t>::result(slots + gs, st) : DBuf<uint64_t>(slots + gs, st);
         DBuf<uint32_t> ws(radix_workspace_elems(slots), st);
         if (guards) launch(guard_fill, 1, 256, 0, st, ktmp.p + slots);
-        radix_sort(keys.p, nullptr, ktmp.p, nullptr, slots, bits, ws.p, st, &ctr.p->status);
+        bool in_tmp = false;
+        radix_sort(keys.p, nullptr, ktmp.p, nullptr, slots, bits, ws.p, st, &ctr.p->status, swap ? &in_tmp : nullptr);
         if (guards) launch(guard_check, 1, 256, 0, st, (const uint64_t*)(ktmp.p + slots), ctr.p);
+        if (in_tmp) std::swap(keys, ktmp);
     }
     if (guards) launch(guard_check, 1, 256, 0, st, (const uint64_t*)(keys.p + slots), ctr.p);
     if (nj > 1) {

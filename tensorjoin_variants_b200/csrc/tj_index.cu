@@ -35,8 +35,10 @@ TJ_DEV float load_x(const void* src, int dtype, size_t idx) {
 
 // Per-block partial statistics for every dimension.  Threads are laid out as
 // (row group g, dimension k); groups are combined in shared memory in a fixed order.
-__global__ void __launch_bounds__(256) dim_stats_partial(const void* src, int dtype, long long n, int d, float* pmin,
-                                                         float* pmax, double* psum, double* psq, int blk_base) {
+// Rows rstride * r for r < n (a strided sample of the source when rstride > 1).
+__global__ void __launch_bounds__(256) dim_stats_partial(const void* src, int dtype, long long n, long long rstride,
+                                                         int d, float* pmin, float* pmax, double* psum, double* psq,
+                                                         int blk_base) {
     __shared__ float smn[256], smx[256];
     __shared__ double ss[256], sq[256];
     const int G = d >= 256 ? 1 : 256 / d;
@@ -54,7 +56,7 @@ __global__ void __launch_bounds__(256) dim_stats_partial(const void* src, int dt
             for (; r + 3 * G < r1; r += 4 * G) {   // four independent loads in flight per thread
                 float v[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) v[u] = load_x(src, dtype, (size_t)(r + u * G) * d + k);
+                for (int u = 0; u < 4; ++u) v[u] = load_x(src, dtype, (size_t)((r + u * G) * rstride) * d + k);
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     mn = fminf(mn, v[u]);
@@ -64,7 +66,7 @@ __global__ void __launch_bounds__(256) dim_stats_partial(const void* src, int dt
                 }
             }
             for (; r < r1; r += G) {
-                const float v = load_x(src, dtype, (size_t)r * d + k);
+                const float v = load_x(src, dtype, (size_t)(r * rstride) * d + k);
                 mn = fminf(mn, v);
                 mx = fmaxf(mx, v);
                 s += v;
@@ -1586,69 +1588,96 @@ __global__ void chunk_emit(const uint64_t* keys, size_t cap, const uint32_t* tot
 // tile I with cand_test's rigorous ball and box bounds (on the halves' own statistics) and stores the
 // live halves in bits 30-31 of the jlist entry.  The screen then issues and tests only live halves,
 // packing them densely into its MMA and epilogue pipeline; an entry whose halves are both dead is
-// skipped.  One block per R tile, threads over its candidate entries.
-__global__ void __launch_bounds__(256) half_mask_kernel(const uint32_t* cnt, const uint32_t* off, uint32_t* jlist,
+// skipped.  Warps stride over the scheduling chunks (at most chunk_items candidates of one R tile),
+// the chunk's R tile statistics in the warp's shared memory, and take its candidates one at a time
+// with the lanes over the dimensions; the halves' statistics are read row-major, so each load of
+// the warp is one contiguous run of a candidate's row.
+__global__ void __launch_bounds__(256) half_mask_kernel(const uint4* chunks, const uint32_t* nchunks, uint32_t* jlist,
                                                         const uint4* rtiles, const JoinParams* jps,
-                                                        const HalfView* views, int self_join, int ntR, int dmax) {
-    // one warp per R tile (eight per block), its lanes over the tile's candidates; the R tile's
-    // centroid and box sit in the warp's part of shared memory
+                                                        const HalfView* views, int self_join, int dmax) {
     extern __shared__ float hm_sm[];   // [8 warps][3][dmax]: R tile centroid, low, high
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int I = (int)blockIdx.x * 8 + (int)warp;
-    if (I >= ntR) return;   // whole warps leave; no block-wide barrier follows
     float* rs = hm_sm + (size_t)warp * 3 * dmax;
-    const uint4 rt = rtiles[I];
-    const HalfView v = views[rt.w];
-    const int d = v.d;
-    const int il = I - v.rbase;   // class-local R tile
-    for (int k = lane; k < d; k += 32) {
-        rs[k] = v.rctrT[(size_t)k * v.ntR + il];
-        rs[d + k] = v.rloT[(size_t)k * v.ntR + il];
-        rs[2 * d + k] = v.rhiT[(size_t)k * v.ntR + il];
-    }
-    __syncwarp();
-    const double Tp = jps[rt.z].Tp;
-    const float f = 1.f - (float)(d + 8) * 0x1p-23f;
-    const float rtp = (float)(sqrt(Tp) * (1.0 + 0x1p-20));
-    const float tpf = (float)(Tp * (1.0 + 0x1p-20));
-    const float ri = v.rrad[il];
-    const uint32_t e0 = off[I], e1 = e0 + cnt[I];
-    for (uint32_t e = e0 + lane; e < e1; e += 32) {
-        const uint32_t J = jlist[e] & 0x3FFFFFFFu;
-        const int h0 = 2 * ((int)J - v.sbase);   // class-local half tiles h0, h0 + 1
-        bool live[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            live[h] = h0 + h < v.ntH && v.hnv[h0 + h] != 0;
-            // self-joins: some sorted column of the half must exceed some sorted row of the tile
-            if (self_join && (long long)(h0 + h) * 128 + 127 <= (long long)il * 128) live[h] = false;
+    const unsigned nch = *nchunks;
+    for (unsigned ci = blockIdx.x * 8 + warp; ci < nch; ci += gridDim.x * 8) {   // warp-uniform
+        const uint4 ch = chunks[ci];
+        const int I = (int)ch.x;
+        const uint4 rt = rtiles[I];
+        const HalfView v = views[rt.w];
+        const int d = v.d;
+        const int il = I - v.rbase;   // class-local R tile
+        __syncwarp();                  // the previous chunk's reads of rs are done
+        for (int k = lane; k < d; k += 32) {
+            rs[k] = v.rctrT[(size_t)k * v.ntR + il];
+            rs[d + k] = v.rloT[(size_t)k * v.ntR + il];
+            rs[2 * d + k] = v.rhiT[(size_t)k * v.ntR + il];
         }
-        const int g0 = live[0] ? h0 : h0 + 1, g1 = live[1] ? h0 + 1 : h0;   // in-range columns for both
-        float ball[2] = {0.f, 0.f}, box[2] = {0.f, 0.f};
-        if (live[0] || live[1]) {
-#pragma unroll 4
-            for (int k = 0; k < d; ++k) {
-                const size_t rk = (size_t)k * v.ntH;
-                const float c = rs[k], lo = rs[d + k], hi = rs[2 * d + k];
-                const float dc0 = c - v.hctrT[rk + g0], dc1 = c - v.hctrT[rk + g1];
-                const float gp0 = fmaxf(fmaxf(v.hloT[rk + g0] - hi, lo - v.hhiT[rk + g0]), 0.f);
-                const float gp1 = fmaxf(fmaxf(v.hloT[rk + g1] - hi, lo - v.hhiT[rk + g1]), 0.f);
-                ball[0] = fmaf(dc0, dc0, ball[0]);
-                ball[1] = fmaf(dc1, dc1, ball[1]);
-                box[0] = fmaf(gp0, gp0, box[0]);
-                box[1] = fmaf(gp1, gp1, box[1]);
+        __syncwarp();
+        const double Tp = jps[rt.z].Tp;
+        const float f = 1.f - (float)(d + 8) * 0x1p-23f;
+        const float rtp = (float)(sqrt(Tp) * (1.0 + 0x1p-20));
+        const float tpf = (float)(Tp * (1.0 + 0x1p-20));
+        const float ri = v.rrad[il];
+        // one candidate at a time, the warp's lanes over its dimensions (coalesced reads of the
+        // halves' row-major statistics whatever tiles the candidates are), sums by a shuffle tree
+        for (uint32_t e = ch.y; e < ch.z; ++e) {   // warp-uniform
+            const uint32_t J = jlist[e] & 0x3FFFFFFFu;
+            const int h0 = 2 * ((int)J - v.sbase);   // class-local half tiles h0, h0 + 1
+            bool live[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                live[h] = h0 + h < v.ntH && v.hnv[h0 + h] != 0;
+                // self-joins: some sorted column of the half must exceed some sorted row of the tile
+                if (self_join && (long long)(h0 + h) * 128 + 127 <= (long long)il * 128) live[h] = false;
             }
-        }
-        unsigned mask = 0;
+            const int g0 = live[0] ? h0 : h0 + 1, g1 = live[1] ? h0 + 1 : h0;   // in-range rows for both
+            float ball[2] = {0.f, 0.f}, box[2] = {0.f, 0.f};
+            if (live[0] || live[1]) {
+                const float *c0 = v.hctrR + (size_t)g0 * d, *c1 = v.hctrR + (size_t)g1 * d;
+                const float *l0 = v.hloR + (size_t)g0 * d, *l1 = v.hloR + (size_t)g1 * d;
+                const float *u0 = v.hhiR + (size_t)g0 * d, *u1 = v.hhiR + (size_t)g1 * d;
+                for (int k = lane; k < d; k += 32) {
+                    const float c = rs[k], lo = rs[d + k], hi = rs[2 * d + k];
+                    const float dc0 = c - c0[k], dc1 = c - c1[k];
+                    const float gp0 = fmaxf(fmaxf(l0[k] - hi, lo - u0[k]), 0.f);
+                    const float gp1 = fmaxf(fmaxf(l1[k] - hi, lo - u1[k]), 0.f);
+                    ball[0] = fmaf(dc0, dc0, ball[0]);
+                    ball[1] = fmaf(dc1, dc1, ball[1]);
+                    box[0] = fmaf(gp0, gp0, box[0]);
+                    box[1] = fmaf(gp1, gp1, box[1]);
+                }
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            if (!live[h]) continue;
-            const float lb_box = box[h] * f;
-            const float lb_ball = sqrtf(ball[h] * f) * (1.f - 0x1p-20f) - ri - v.hrad[h0 + h];
-            if (!(lb_box > tpf || lb_ball > rtp)) mask |= 1u << h;
+                for (int o = 16; o > 0; o >>= 1) {
+                    ball[0] += __shfl_xor_sync(0xffffffffu, ball[0], o);
+                    ball[1] += __shfl_xor_sync(0xffffffffu, ball[1], o);
+                    box[0] += __shfl_xor_sync(0xffffffffu, box[0], o);
+                    box[1] += __shfl_xor_sync(0xffffffffu, box[1], o);
+                }
+            }
+            // each partial sum is a sum of non-negative FP32 terms, one more rounding per shuffle
+            // level: the deflation by f = 1 - (d + 8) 2^-23 covers d + 5 roundings
+            unsigned mask = 0;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (!live[h]) continue;
+                const float lb_box = box[h] * f;
+                const float lb_ball = sqrtf(ball[h] * f) * (1.f - 0x1p-20f) - ri - v.hrad[h0 + h];
+                if (!(lb_box > tpf || lb_ball > rtp)) mask |= 1u << h;
+            }
+            if (lane == 0) jlist[e] = J | (mask << 30);
         }
-        jlist[e] = J | (mask << 30);
     }
+}
+
+// [d][nt] -> [nt][d] for the three per-dimension statistics of a tile set.
+__global__ void stats_rowmajor_kernel(const float* ctrT, const float* loT, const float* hiT, int nt, int d, float* ctrR,
+                                      float* loR, float* hiR) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;   // row-major index t * d + k
+    if (i >= (size_t)nt * d) return;
+    const size_t t = i / (size_t)d, k = i - t * (size_t)d;
+    ctrR[i] = ctrT[k * nt + t];
+    loR[i] = loT[k * nt + t];
+    hiR[i] = hiT[k * nt + t];
 }
 
 }  // namespace
@@ -1657,18 +1686,29 @@ __global__ void __launch_bounds__(256) half_mask_kernel(const uint32_t* cnt, con
 
 bool compute_frame(const void* const* srcs, const long long* ns, int nsrc, int d, int dtype, int frame_mode,
                    FrameParams* fp, float* center, cudaStream_t st) {
-    long long ntot = 0;
-    for (int s = 0; s < nsrc; ++s) ntot += ns[s];
+    // The per-dimension statistics choose the Morton frame and the centre c; any centre and any frame
+    // leave the pairs unchanged (the certificate is computed from the operands actually formed, and
+    // cell coordinates outside the measured range are clamped), so they come from an evenly strided
+    // sample of at most kStatSampleRows rows per side.
+    constexpr long long kStatSampleRows = 1ll << 16;
+    long long ntot = 0, nstat = 0;
+    std::vector<long long> rstride(nsrc), nsampled(nsrc);
+    for (int s = 0; s < nsrc; ++s) {
+        ntot += ns[s];
+        rstride[s] = std::max(1ll, ns[s] / kStatSampleRows);
+        nsampled[s] = (ns[s] + rstride[s] - 1) / rstride[s];   // (nsampled - 1) * rstride < ns
+        nstat += nsampled[s];
+    }
     const int parts = nsrc * kStatBlocks;
     DBuf<float> pmin((size_t)parts * d, st), pmax((size_t)parts * d, st);
     DBuf<double> psum((size_t)parts * d, st), psq((size_t)parts * d, st);
     DBuf<float> ws((size_t)3 * d, st);
     for (int s = 0; s < nsrc; ++s) {
         const int nb = kStatBlocks;
-        launch(dim_stats_partial, nb, 256, 0, st, srcs[s], dtype, ns[s], d, pmin.p, pmax.p, psum.p, psq.p,
-                                              s * kStatBlocks);
+        launch(dim_stats_partial, nb, 256, 0, st, srcs[s], dtype, nsampled[s], rstride[s], d, pmin.p, pmax.p, psum.p,
+               psq.p, s * kStatBlocks);
     }
-    launch(dim_reduce, (unsigned)d, 256, 0, st, pmin.p, pmax.p, psum.p, psq.p, parts, ntot, d, ws.p,
+    launch(dim_reduce, (unsigned)d, 256, 0, st, pmin.p, pmax.p, psum.p, psq.p, parts, nstat, d, ws.p,
            ws.p + d, ws.p + 2 * d, center);
     const bool pca = frame_mode != kFrameAxes && d >= 9 && d <= kPcaMaxD && ntot > 0 &&
                      (frame_mode == kFramePca || ntot >= kPcaMinRows);
@@ -1979,12 +2019,25 @@ void half_masks(const std::vector<HalfView>& views, const Candidates& c, int ntR
     for (const auto& v : views) dmax = std::max(dmax, v.d);
     DBuf<HalfView> dv(views.size(), st);
     upload(dv.p, views.data(), views.size() * sizeof(HalfView), st);
-    const size_t smem = (size_t)8 * 3 * dmax * sizeof(float);   // eight R tiles per block
+    const size_t smem = (size_t)8 * 3 * dmax * sizeof(float);   // one R tile per warp
     if (smem > 48 * 1024)
         TJ_CUDA(cudaFuncSetAttribute(half_mask_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    launch(half_mask_kernel, (unsigned)((ntR_total + 7) / 8), 256, smem, st, (const uint32_t*)c.cnt.p,
-           (const uint32_t*)c.off.p, c.jlist.p, rtiles, jps, (const HalfView*)dv.p, self_join ? 1 : 0, ntR_total,
+    // warps stride over the chunks (their count is on the device); at most the chunk capacity
+    const unsigned blocks = (unsigned)std::min<size_t>((size_t)num_sms() * 8, (c.chunks_cap + 7) / 8);
+    launch(half_mask_kernel, std::max(1u, blocks), 256, smem, st, (const uint4*)c.chunks.p,
+           (const uint32_t*)(c.dev_counts.p + 1), c.jlist.p, rtiles, jps, (const HalfView*)dv.p, self_join ? 1 : 0,
            dmax);
+}
+
+void tile_stats_rowmajor(TileSet& ts, cudaStream_t st) {
+    const size_t n = (size_t)std::max(ts.ntiles, 1) * ts.d;
+    ts.ctrR = DBuf<float>(n, st);
+    ts.loR = DBuf<float>(n, st);
+    ts.hiR = DBuf<float>(n, st);
+    if (ts.ntiles == 0) return;
+    const size_t m = (size_t)ts.ntiles * ts.d;
+    launch(stats_rowmajor_kernel, (unsigned)((m + 255) / 256), 256, 0, st, (const float*)ts.ctrT.p,
+           (const float*)ts.loT.p, (const float*)ts.hiT.p, ts.ntiles, ts.d, ts.ctrR.p, ts.loR.p, ts.hiR.p);
 }
 
 void build_candidates_batched(const std::vector<CandClassView>& classes, const std::vector<CandBlock>& blocks,

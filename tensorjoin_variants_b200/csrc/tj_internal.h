@@ -108,6 +108,8 @@ size_t radix_workspace_elems(size_t n);
 void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* vals_tmp, size_t n, int bits,
                 uint32_t* ws, cudaStream_t st, unsigned long long* status = nullptr, bool* in_tmp = nullptr);
 int radix_passes(int bits);
+// True when radix_sort with a status word and in_tmp leaves the sorted keys in the temporaries.
+bool radix_result_in_tmp(size_t n, int bits);
 
 // ------------------------------------------------------------------ enums (mirror include/tensorjoin.h)
 enum DType { kF32 = 0, kI16 = 1 };
@@ -157,6 +159,7 @@ struct TileSet {
     DBuf<uint32_t> row0;    // [ntiles] first sorted row of the tile
     std::vector<uint32_t> h_row0, h_nvalid, h_join;   // host tile tables (batched sides; empty: uniform tiles)
     bool built = false;   // statistics already computed (by the fused operand pass)
+    DBuf<float> ctrR, loR, hiR;   // [ntiles][d] row-major copies (half tiles: the half-mask test)
 };
 
 // Candidate tile pairs grouped by R tile, cut into chunks scheduled J-window-major.
@@ -223,14 +226,16 @@ void build_candidates_batched(const std::vector<CandClassView>& classes, const s
 // Half-tile masks (one-SM tensor-core screen): R tile statistics and 128-row S half-tile statistics
 // of one class, class-local indices; ntH = 2 x the class's 256-row S tiles.
 struct HalfView {
-    const float *rctrT, *rloT, *rhiT, *rrad;
-    const float *hctrT, *hloT, *hhiT, *hrad;
+    const float *rctrT, *rloT, *rhiT, *rrad;   // R tiles: [d][ntR]
+    const float *hctrR, *hloR, *hhiR, *hrad;   // halves: [ntH][d] (row-major)
     const uint32_t* hnv;   // [ntH] rows of each half that are real points
     int ntR, ntH, rbase, sbase, d, pad;
 };
 // Marks the live 128-row halves of every candidate's S tile in bits 30-31 of its jlist entry.
 void half_masks(const std::vector<HalfView>& views, const Candidates& c, int ntR_total, const uint4* rtiles,
                 const JoinParams* jps, bool self_join, cudaStream_t st);
+// Row-major copies (ctrR, loR, hiR) of a tile set's centroids and boxes.
+void tile_stats_rowmajor(TileSet& ts, cudaStream_t st);
 constexpr uint32_t kJMask = 0x3FFFFFFFu;   // jlist entry: S tile id in the low 30 bits
 
 // ------------------------------------------------------------------ screen / refine / emit

@@ -642,4 +642,6 @@ void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* va
 
 int radix_passes(int bits) { return (bits + 7) / 8; }
 
+bool radix_result_in_tmp(size_t n, int bits) { return n > kOneSweepMin && radix_passes(bits) % 2 == 1; }
+
 }  // namespace tj
