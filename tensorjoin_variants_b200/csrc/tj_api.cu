@@ -484,6 +484,18 @@ void run_batch_body(const std::vector<JoinIn>& joins, int dtype, int mode, int s
         // tile tables: tiles never span two joins; sorted rows of join q are [ro[q], ro[q+1])
         g.rbase[c] = (int)rtiles.size();
         g.sbase[c] = (int)stiles.size();
+        {
+            size_t ntr = 0, nts = 0;
+            for (int q = 0; q < njc; ++q) {
+                const int k = J[q];
+                ntr += (size_t)((joins[k].nR + kTileR - 1) / kTileR);
+                nts += (size_t)(((self ? joins[k].nR : joins[k].nS) + stile - 1) / stile);
+            }
+            for (auto* v : {&K.tR.h_row0, &K.tR.h_nvalid, &K.tR.h_join}) v->reserve(ntr);
+            for (auto* v : {&K.tS.h_row0, &K.tS.h_nvalid, &K.tS.h_join}) v->reserve(nts);
+            rtiles.reserve(rtiles.size() + ntr);
+            stiles.reserve(stiles.size() + nts);
+        }
         for (int q = 0; q < njc; ++q) {
             const int k = J[q];
             for (long long t = 0; t * kTileR < joins[k].nR; ++t) {

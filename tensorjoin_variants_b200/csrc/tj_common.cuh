@@ -191,6 +191,14 @@ TJ_DEV void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar)
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
         :: "r"(smem_u32(dst)), "l"((uint64_t)src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
+// 16-byte global -> shared copy issued by one thread (both addresses 16-byte aligned), bypassing L1;
+// copies are grouped by commit and waited for by group count.
+TJ_DEV void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(smem_u32(dst)), "l"((uint64_t)src) : "memory");
+}
+TJ_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int kPending>
+TJ_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(kPending) : "memory"); }
 TJ_DEV void prefetch_tmap(const CUtensorMap* map) {
     asm volatile("prefetch.tensormap [%0];" :: "l"((uint64_t)map) : "memory");
 }

@@ -536,6 +536,26 @@ TJ_DEV float round16(float v, uint16_t& bits) {
     return __half2float(h);
 }
 
+// Two values rounded to the 16-bit format at once (one packed conversion): returns the packed word
+// (a in the low half, b in the high half, the operand layout) and the two rounded values.  The
+// same round-to-nearest-even as round16 per value.
+template <int kFmt>
+TJ_DEV uint32_t round16x2(float a, float b, float& ra, float& rb) {
+    uint32_t w;
+    if (kFmt == 1) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        w = *reinterpret_cast<const uint32_t*>(&h);
+        ra = __uint_as_float(w << 16);
+        rb = __uint_as_float(w & 0xFFFF0000u);
+    } else {
+        const __half2 h = __floats2half2_rn(a, b);
+        w = *reinterpret_cast<const uint32_t*>(&h);
+        ra = __low2float(h);
+        rb = __high2float(h);
+    }
+    return w;
+}
+
 // One group of kL lanes per sorted row (a warp for wide rows, 4 or 8 lanes for rows of at most
 // 16 or 32 elements): operand conversion and certificate metadata.
 //   plain:      FP32 copy in sorted order, ||x||^2.
@@ -849,38 +869,47 @@ TJ_DEV void prep_row(const float (&xa)[kE], const float (&cf)[kE], const double 
     double sx = 0.0;
     float sz = 0.f, se = 0.f, sl = 0.f;
     uint32_t hw[kE / 2], lw[kE / 2];
+    // element pairs (one packed 16-bit conversion per pair and part); every sum still runs over the
+    // elements in order
 #pragma unroll
-    for (int q = 0; q < kE; ++q) {
-        const float x = xa[q];
-        const float sd = x - cf[q];   // fl32(x'): |x' - sd| <= 2^-24 |x'| per element
-        const double xd = (double)x - cdv[q];
-        sx = fma(xd, xd, sx);
-        if (kFmt == 0 && fabsf(sd) > 65504.f) flags |= 2u;
-        uint16_t hbits, lbits = 0;
-        const float zh = round16<kFmt>(sd, hbits);
-        const float d1 = sd - zh;   // exact (zh is sd rounded to 8 or 11 bits)
+    for (int q = 0; q < kE; q += 2) {
+        float sd[2], zh[2], d1[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            sd[e] = xa[q + e] - cf[q + e];   // fl32(x'): |x' - sd| <= 2^-24 |x'| per element
+            const double xd = (double)xa[q + e] - cdv[q + e];
+            sx = fma(xd, xd, sx);
+            if (kFmt == 0 && fabsf(sd[e]) > 65504.f) flags |= 2u;
+        }
+        hw[q / 2] = round16x2<kFmt>(sd[0], sd[1], zh[0], zh[1]);
+        d1[0] = sd[0] - zh[0];   // exact (zh is sd rounded to 8 or 11 bits)
+        d1[1] = sd[1] - zh[1];
         if (kSplit) {
-            const float zlo = round16<kFmt>(d1, lbits);
-            const float ed = d1 - zlo;   // exact: sd - z_hi - z_lo
-            const float z = zh + zlo;
-            sz = fmaf(z, z, sz);
-            se = fmaf(ed, ed, se);
-            sl = fmaf(zlo, zlo, sl);
+            float zlo[2];
+            lw[q / 2] = round16x2<kFmt>(d1[0], d1[1], zlo[0], zlo[1]);
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const float ed = d1[e] - zlo[e];   // exact: sd - z_hi - z_lo
+                const float z = zh[e] + zlo[e];
+                sz = fmaf(z, z, sz);
+                se = fmaf(ed, ed, se);
+                sl = fmaf(zlo[e], zlo[e], sl);
+            }
         } else {
-            sz = fmaf(zh, zh, sz);
-            se = fmaf(d1, d1, se);   // d1 = sd - z_hi exactly
+            lw[q / 2] = 0u;
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                sz = fmaf(zh[e], zh[e], sz);
+                se = fmaf(d1[e], d1[e], se);   // d1 = sd - z_hi exactly
+            }
         }
-        if (q & 1) {
-            hw[q / 2] |= (uint32_t)hbits << 16;
-            lw[q / 2] |= (uint32_t)lbits << 16;
-        } else {
-            hw[q / 2] = hbits;
-            lw[q / 2] = lbits;
-        }
-        if (rv && k0 + q < d) {
-            ps[q] += x;
-            pl[q] = fminf(pl[q], x);
-            ph[q] = fmaxf(ph[q], x);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            if (rv && k0 + q + e < d) {
+                ps[q + e] += xa[q + e];
+                pl[q + e] = fminf(pl[q + e], xa[q + e]);
+                ph[q + e] = fmaxf(ph[q + e], xa[q + e]);
+            }
         }
     }
     if (rv) {
@@ -1200,7 +1229,7 @@ __global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict
 // input: a block per tile spent its time in barriers and serial combines).  The arithmetic is
 // prep_row's, the statistics those of prep_tiles_kernel.
 template <int kScreen, int kSplit, int kL, bool kHalves>
-__global__ void __launch_bounds__(256) prep_tiles_warp_kernel(const float* __restrict__ src, long long n, int d,
+__global__ void __launch_bounds__(256, 3) prep_tiles_warp_kernel(const float* __restrict__ src, long long n, int d,
                                                               int tile, int ntiles, const uint32_t* __restrict__ perm,
                                                               const float* __restrict__ center,
                                                               const uint32_t* row0_in, const uint32_t* nvalid_in,
@@ -1210,8 +1239,10 @@ __global__ void __launch_bounds__(256) prep_tiles_warp_kernel(const float* __res
     constexpr int kE = 4;
     constexpr int kRW = 32 / kL;               // rows per warp step
     constexpr int kSteps = 128 / kRW;          // steps per 128-row half
-    constexpr int kU = 4;                      // steps whose loads are issued together
+    constexpr int kRing = 16;                  // steps in flight
     static_assert(kL == 4 || kL == 8, "rows of 16 or 32 padded elements");
+    extern __shared__ __align__(16) float4 pw_ring[];   // [8 warps][kRing][32 lanes]
+    __shared__ uint32_t pw_perm[8][256];                 // the warp's tile rows' original ids
     const unsigned lane = threadIdx.x & 31;
     const int t = (int)blockIdx.x * 8 + (int)(threadIdx.x >> 5);
     if (t >= ntiles) return;   // whole warps; no block barrier in this kernel
@@ -1231,6 +1262,27 @@ __global__ void __launch_bounds__(256) prep_tiles_warp_kernel(const float* __res
     }
     const PrepBounds pb(d);
     unsigned flags = 0;
+    // loads: the warp's rows stream through a per-lane ring of kRing 16-byte slots in shared memory
+    // (cp.async, one commit group per step, kRing steps in flight), first for the statistics pass and
+    // then again for the radius pass; the tile's permutation entries are staged first
+    const int warp = (int)(threadIdx.x >> 5);
+    float4* ring = pw_ring + (size_t)warp * kRing * 32 + lane;   // slot q at ring[32 q]
+    uint32_t* wperm = pw_perm[warp];
+    for (int k = (int)lane; k < nv; k += 32) wperm[k] = perm[r0 + k];
+    __syncwarp();
+    const int nh = nv > 128 && halves == 2 ? 2 : 1;
+    const int pass_steps = nh * kSteps, total_steps = 2 * pass_steps;
+    auto issue = [&](int q) {
+        if (q < total_steps) {
+            const int rem = q < pass_steps ? q : q - pass_steps;
+            const int ii = (rem / kSteps) * 128 + (rem % kSteps) * kRW + (int)grp;
+            if (ii < nv && kin) cp_async16(&ring[32 * (q % kRing)], src + (size_t)wperm[ii] * (size_t)d + k0);
+        }
+        cp_async_commit();
+    };
+#pragma unroll 1
+    for (int q = 0; q < kRing; ++q) issue(q);
+    int qc = 0;   // next step to consume
     // per half: the lane's centroid / box partials (combined over the warp's row groups below) and the
     // bound maxima (lanes 0-3 of a group: Y, Z, E, Zl; lane 0 also B and beta)
     float hs[2][kE], hl[2][kE], hh[2][kE], hm[2][6];
@@ -1240,23 +1292,17 @@ __global__ void __launch_bounds__(256) prep_tiles_warp_kernel(const float* __res
 #pragma unroll
         for (int q = 0; q < kE; ++q) { ps[q] = 0.f; pl[q] = INFINITY; ph[q] = -INFINITY; }
         float mtask = 0.f, mb = 0.f, mbeta = 0.f;
-        if (h < halves && h * 128 < nv) {   // uniform across the warp
-            for (int s0 = 0; s0 < kSteps; s0 += kU) {
-                float4 xv[kU];
-                int ii[kU];
-#pragma unroll
-                for (int u = 0; u < kU; ++u) {
-                    ii[u] = h * 128 + (s0 + u) * kRW + (int)grp;
-                    xv[u] = (ii[u] < nv && kin)
-                                ? __ldg(reinterpret_cast<const float4*>(src + (size_t)perm[r0 + ii[u]] * (size_t)d + k0))
-                                : make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-#pragma unroll
-                for (int u = 0; u < kU; ++u) {
-                    const float xa[kE] = {xv[u].x, xv[u].y, xv[u].z, xv[u].w};
-                    prep_row<kScreen, kSplit, kE, kL>(xa, cf, cdv, ii[u] < nv, r0 + ii[u], k0, d, sub, lane, pb, op,
-                                                      nrm2, nrm2f, zn, en, yn, zl, ps, pl, ph, mtask, mb, mbeta, flags);
-                }
+        if (h < nh) {   // uniform across the warp
+#pragma unroll 1
+            for (int s = 0; s < kSteps; ++s) {
+                const int ii = h * 128 + s * kRW + (int)grp;
+                cp_async_wait<kRing - 1>();
+                const float4 xv = (ii < nv && kin) ? ring[32 * (qc % kRing)] : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float xa[kE] = {xv.x, xv.y, xv.z, xv.w};
+                prep_row<kScreen, kSplit, kE, kL>(xa, cf, cdv, ii < nv, r0 + ii, k0, d, sub, lane, pb, op, nrm2,
+                                                  nrm2f, zn, en, yn, zl, ps, pl, ph, mtask, mb, mbeta, flags);
+                issue(qc + kRing);
+                ++qc;
             }
         }
 #pragma unroll
@@ -1308,23 +1354,16 @@ __global__ void __launch_bounds__(256) prep_tiles_warp_kernel(const float* __res
             }
         }
     }
-    // radius pass (the tile's rows again, from L2), bounded as in prep_tiles_kernel
+    // radius pass (the tile's rows again, from L2 through the ring), bounded as in prep_tiles_kernel
     float mt = 0.f, mh0 = 0.f, mh1 = 0.f;
-    for (int h = 0; h < halves; ++h) {
-        if (h * 128 >= nv) break;   // uniform
-        for (int s0 = 0; s0 < kSteps; s0 += kU) {
-            float4 xv[kU];
-            int ii[kU];
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                ii[u] = h * 128 + (s0 + u) * kRW + (int)grp;
-                xv[u] = (ii[u] < nv && kin)
-                            ? __ldg(reinterpret_cast<const float4*>(src + (size_t)perm[r0 + ii[u]] * (size_t)d + k0))
-                            : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                const float xa[kE] = {xv[u].x, xv[u].y, xv[u].z, xv[u].w};
+    for (int h = 0; h < nh; ++h) {
+#pragma unroll 1
+        for (int s = 0; s < kSteps; ++s) {
+            const int ii = h * 128 + s * kRW + (int)grp;
+            cp_async_wait<kRing - 1>();
+            const float4 xv = (ii < nv && kin) ? ring[32 * (qc % kRing)] : make_float4(0.f, 0.f, 0.f, 0.f);
+            {
+                const float xa[kE] = {xv.x, xv.y, xv.z, xv.w};
                 float st_ = 0.f, sh = 0.f;
 #pragma unroll
                 for (int q = 0; q < kE; ++q) {
@@ -1341,7 +1380,7 @@ __global__ void __launch_bounds__(256) prep_tiles_warp_kernel(const float* __res
                     st_ += __shfl_xor_sync(0xffffffffu, st_, o);
                     if (kHalves) sh += __shfl_xor_sync(0xffffffffu, sh, o);
                 }
-                if (ii[u] < nv) {
+                if (ii < nv) {
                     mt = fmaxf(mt, st_);
                     if (kHalves) {
                         if (h) mh1 = fmaxf(mh1, sh);
@@ -1349,8 +1388,11 @@ __global__ void __launch_bounds__(256) prep_tiles_warp_kernel(const float* __res
                     }
                 }
             }
+            issue(qc + kRing);
+            ++qc;
         }
     }
+    cp_async_wait<0>();   // the ring's trailing (empty) groups
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         mt = fmaxf(mt, __shfl_xor_sync(0xffffffffu, mt, o));
@@ -1810,10 +1852,17 @@ void prep_tiles(Side& s, const float* center, int tile, TileSet& ts, TileSet* ha
     launch(prep_tiles_kernel<SCR, SPLIT, E, L, HV>, (unsigned)ntiles, 256, 0, st, (const float*)s.src, n, s.d, tile, \
            (const uint32_t*)s.perm.p, center, r0, nvv, s.op.p, s.nrm2.p, s.nrm2f.p, s.zn.p, s.en.p, s.yn.p,      \
            s.zl.p, T, H, status)
-#define TJ_PTW(SCR, SPLIT, L, HV)                                                                            \
-    launch(prep_tiles_warp_kernel<SCR, SPLIT, L, HV>, (unsigned)((ntiles + 7) / 8), 256, 0, st, (const float*)s.src, \
-           n, s.d, tile, ntiles, (const uint32_t*)s.perm.p, center, r0, nvv, s.op.p, s.nrm2.p, s.nrm2f.p, s.zn.p,    \
-           s.en.p, s.yn.p, s.zl.p, T, H, status)
+#define TJ_PTW(SCR, SPLIT, L, HV)                                                                                 \
+    do {                                                                                                          \
+        const int ring_bytes = 8 * 16 * 32 * 16;                                                                  \
+        TJ_CUDA(cudaFuncSetAttribute(prep_tiles_warp_kernel<SCR, SPLIT, L, HV>,                                   \
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, ring_bytes));                   \
+        TJ_CUDA(cudaFuncSetAttribute(prep_tiles_warp_kernel<SCR, SPLIT, L, HV>,                                   \
+                                     cudaFuncAttributePreferredSharedMemoryCarveout, 100));                       \
+        launch(prep_tiles_warp_kernel<SCR, SPLIT, L, HV>, (unsigned)((ntiles + 7) / 8), 256, ring_bytes, st,      \
+               (const float*)s.src, n, s.d, tile, ntiles, (const uint32_t*)s.perm.p, center, r0, nvv, s.op.p,     \
+               s.nrm2.p, s.nrm2f.p, s.zn.p, s.en.p, s.yn.p, s.zl.p, T, H, status);                               \
+    } while (0)
 #define TJ_PT_L(SCR, SPLIT, HV)                                  \
     do {                                                         \
         if (s.kpad == 16) TJ_PTW(SCR, SPLIT, 4, HV);             \

@@ -61,6 +61,7 @@ constexpr int kScreenThreads = (kEpiFirst + kEpiWarps) * 32;
 constexpr unsigned kABytes = kTileR * 128;          // 16 KB
 constexpr unsigned kBBytes = kTileS * 128;          // 32 KB
 constexpr int kMetaSlots = 8;   // items of column metadata in flight (each epilogue group sees several)
+constexpr unsigned kDirectMax = 2;   // emission: parts whose lanes hold at most this many pairs each write per lane
 
 // Stage = one 64-element k-block of A (128 rows) and B (256 rows); with the hi/lo split the
 // stage holds both limbs of both operands: [A_hi | A_lo | B_hi | B_lo].
@@ -588,6 +589,13 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
             const float Ei = rvalid ? ca.r_en[rs] : 0.f;
             const float Zli = rvalid ? ca.r_zl[rs] : 0.f;
             const uint32_t oi = rvalid ? ca.r_emit[rs] : 0u;
+            // the row's parts of the per-item thresholds below (FP64; every sum keeps the margins
+            // that cover its rounding)
+            const double Zd = Zi, Ed = Ei, Zld = Zli;
+            const double cabs = jp.cabs;
+            const double zg = jp.gmma * Zd, pz = Zd * (1.0 + jp.gmma), gA = jp.gn * Ai;
+            const double tp_base = jp.Tp - Ai + 0x1p-50 * (jp.Tp + Ai) + 0x1p-1000;
+            const double tm_base = jp.Tm - Ai - 0x1p-50 * (jp.Tm + Ai) - 0x1p-1000;
             for (unsigned e = e0; e < e1 && ok; ++e) {
               unsigned hm = 3u;   // one SM: live 128-row halves of the item's S tile
               if (!kPair && a.half) {
@@ -622,15 +630,12 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                 float tau = -INFINITY, tau_in = -INFINITY;
                 if (rvalid) {
                     const double WJ = m.WJ, FJ = m.FJ, YJ = m.YJ, BJ = m.BJ, betaJ = m.betaJ, WlJ = m.WlJ;
-                    const double Zd = Zi, Ed = Ei, Zld = Zli;
-                    const double RiJ = jp.gmma * Zd * WJ + jp.cabs + Ed * YJ + Zd * FJ + Zld * WlJ;
-                    const double PiJ = Zd * WJ * (1.0 + jp.gmma) + jp.cabs;
-                    const double slack = jp.gn * Ai + 0x1p-23 * (BJ + 2.0 * PiJ) + betaJ + 2.0 * RiJ;
+                    const double RiJ = zg * WJ + cabs + Ed * YJ + Zd * FJ + Zld * WlJ;
+                    const double PiJ = pz * WJ + cabs;
+                    const double slack = gA + 0x1p-23 * (BJ + 2.0 * PiJ) + betaJ + 2.0 * RiJ;
                     // the 2^-40 / 2^-50 terms exceed the FP64 rounding of these sums even under cancellation
-                    const double t = jp.Tp - Ai + slack * (1.0 + 0x1p-40) + 0x1p-50 * (jp.Tp + Ai) + 0x1p-1000;
-                    tau = f32_up(t);
-                    const double ti = jp.Tm - Ai - slack * (1.0 + 0x1p-40) - 0x1p-50 * (jp.Tm + Ai) - 0x1p-1000;
-                    tau_in = f32_dn(ti);
+                    tau = f32_up(tp_base + slack * (1.0 + 0x1p-40));
+                    tau_in = f32_dn(tm_base - slack * (1.0 + 0x1p-40));
                 }
                 // the thresholds above need only the metadata: the accumulator is awaited after them
                 // (warp-uniform: the TMEM loads below are warp-collective)
@@ -774,8 +779,42 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                     if (ta) pa = app_acc.reserve(ta, &a.ctr->acc_reserved, a.acc, a.acc_cap);
                     if (tb) pb = app_band.reserve(tb, &a.ctr->band_reserved, a.band, a.band_cap);
                     if (kTimes && lane == 0) racc[5] += clock64();
+                    // sparse parts (no lane with more than kDirectMax pairs): every lane writes its own
+                    // pairs, accepts and band in one pass in column order, into the same slots the
+                    // cooperative loop below would give them (lane by lane, block by block, column by
+                    // column), in at most kDirectMax steps of the warp
+                    const unsigned most = __reduce_max_sync(0xffffffffu, na + nb);
+                    if (most <= kDirectMax) {
+                        uint32_t w0 = cmk[0], w1 = cmk[1], w2 = cmk[2], w3 = cmk[3];
+                        unsigned long long sa = pa + (pre & 0xFFFFu), sb = pb + (pre >> 16);
+#pragma unroll
+                        for (unsigned it = 0; it < kDirectMax; ++it) {
+                            if (it >= most) break;   // warp-uniform
+                            if (w0 | w1 | w2 | w3) {
+                                const int blk = w0 ? 0 : w1 ? 1 : w2 ? 2 : 3;
+                                const uint32_t w = w0 ? w0 : w1 ? w1 : w2 ? w2 : w3;
+                                const uint32_t bit = w & (0u - w);   // lowest set bit
+                                const uint32_t acc_w = blk == 0 ? imk[0] : blk == 1 ? imk[1] : blk == 2 ? imk[2] : imk[3];
+                                if (blk == 0) w0 ^= bit;
+                                else if (blk == 1) w1 ^= bit;
+                                else if (blk == 2) w2 ^= bit;
+                                else w3 ^= bit;
+                                const int col = (int)colbase + (cb_begin + blk) * 32 + (__ffs(bit) - 1);
+                                const uint32_t oj = m.perm[col];
+                                const uint64_t key = jp.self_join ? pair_key(jp, oi, oj)
+                                                                  : jp.key_off + (uint64_t)oi * (uint64_t)jp.n_cols + oj;
+                                if (acc_w & bit) {
+                                    if (sa < a.acc_cap) a.acc[sa] = key;
+                                    ++sa;
+                                } else {
+                                    if (sb < a.band_cap) a.band[sb] = key;
+                                    ++sb;
+                                }
+                            }
+                        }
+                    }
 #pragma unroll 1
-                    for (int list = 0; list < 2; ++list) {   // 0: certified accepts, 1: band
+                    for (int list = 0; list < (most <= kDirectMax ? 0 : 2); ++list) {   // 0: certified accepts, 1: band
                         const unsigned tl = list ? tb : ta;
                         if (!tl) continue;   // warp-uniform
                         const unsigned mypre = list ? (pre >> 16) : (pre & 0xFFFFu);

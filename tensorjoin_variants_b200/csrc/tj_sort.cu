@@ -348,16 +348,18 @@ constexpr int kOsMaxPasses = 8;
 constexpr int kOsHistThreads = 512;
 constexpr int kOsHistKeys = 4;            // keys per thread whose loads are issued together
 
-__global__ void __launch_bounds__(kOsHistThreads) os_hist(const uint64_t* keys, size_t n, int passes,
-                                                          uint32_t* ghist) {
-    __shared__ uint32_t h[kOsMaxPasses][256];
-    for (int i = threadIdx.x; i < kOsMaxPasses * 256; i += kOsHistThreads) (&h[0][0])[i] = 0;
+// All digit histograms from one read.  Per pass, each run of lanes that share a digit (keys arrive
+// in array order, so the high digits of nearly sorted keys form long runs) adds its length once, from
+// the run's first lane: a shuffle finds the run starts, a ballot of the starts gives each run's end.
+template <int kPasses>
+__global__ void __launch_bounds__(kOsHistThreads) os_hist(const uint64_t* keys, size_t n, uint32_t* ghist) {
+    __shared__ uint32_t h[kPasses][256];
+    for (int i = threadIdx.x; i < kPasses * 256; i += kOsHistThreads) (&h[0][0])[i] = 0;
     __syncthreads();
     const unsigned lane = threadIdx.x & 31;
     const size_t step = (size_t)gridDim.x * kOsHistThreads * kOsHistKeys;
     // whole warps walk the array (indices past n count nothing), kOsHistKeys keys per thread, each
-    // warp's 32 keys of one load contiguous; a digit every lane of the warp shares (the high digits of
-    // nearly sorted keys) is added once instead of 32 times to one counter
+    // warp's 32 keys of one load contiguous
     for (size_t b = (size_t)blockIdx.x * kOsHistThreads * kOsHistKeys; b < n; b += step) {
         uint64_t k[kOsHistKeys];
 #pragma unroll
@@ -368,22 +370,23 @@ __global__ void __launch_bounds__(kOsHistThreads) os_hist(const uint64_t* keys, 
 #pragma unroll
         for (int u = 0; u < kOsHistKeys; ++u) {
             const size_t i = b + (size_t)u * kOsHistThreads + threadIdx.x;
-            const bool ok = i < n;
-            const unsigned live = __ballot_sync(0xffffffffu, ok);
-            if (!live) continue;
-            for (int p = 0; p < passes; ++p) {
+            const unsigned live = __ballot_sync(0xffffffffu, i < n);   // a prefix of the warp's lanes
+            const uint64_t prev = __shfl_up_sync(0xffffffffu, k[u], 1);
+#pragma unroll
+            for (int p = 0; p < kPasses; ++p) {
                 const unsigned dg = (unsigned)(k[u] >> (8 * p)) & 0xFFu;
-                const unsigned d0 = __shfl_sync(0xffffffffu, dg, 0);   // lane 0 is live whenever any lane is
-                if (__all_sync(0xffffffffu, !ok || dg == d0)) {
-                    if (lane == 0) atomicAdd(&h[p][d0], (unsigned)__popc(live));
-                } else if (ok) {
-                    atomicAdd(&h[p][dg], 1u);
+                const bool start = (lane == 0 || dg != ((unsigned)(prev >> (8 * p)) & 0xFFu)) && ((live >> lane) & 1u);
+                const unsigned starts = __ballot_sync(0xffffffffu, start) | ~live;   // the dead tail ends a run
+                if (start) {
+                    const unsigned after = starts & ~((2u << lane) - 1u);   // run starts above this lane
+                    const unsigned end = after ? (unsigned)__ffs(after) - 1u : 32u;
+                    atomicAdd(&h[p][dg], end - lane);
                 }
             }
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < passes * 256; i += kOsHistThreads) {
+    for (int i = threadIdx.x; i < kPasses * 256; i += kOsHistThreads) {
         const uint32_t c = (&h[0][0])[i];
         if (c) atomicAdd(&ghist[i], c);
     }
@@ -405,14 +408,18 @@ TJ_DEV void st_status(uint64_t* p, uint64_t v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
 }
 
-template <bool kVals>
-__global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) os_scatter(const uint64_t* keys_in, const uint32_t* vals_in,
-                                                        uint64_t* keys_out, uint32_t* vals_out, size_t n, int shift,
-                                                        const uint32_t* gstart, uint64_t* tstat, uint32_t* tile_ctr,
-                                                        unsigned long long* status) {
+// kRounds keys per thread: 8 (4096-key tiles) with values, 16 (8192-key tiles, two blocks per SM)
+// for keys alone, which halves the tiles and with them the fixed per-tile cost (the barriers, the
+// digit scan and the look-back round trip) against the same traffic.
+template <bool kVals, int kRounds>
+__global__ void __launch_bounds__(kScThreads, 2) os_scatter(const uint64_t* keys_in, const uint32_t* vals_in,
+                                                            uint64_t* keys_out, uint32_t* vals_out, size_t n, int shift,
+                                                            const uint32_t* gstart, uint64_t* tstat, uint32_t* tile_ctr,
+                                                            unsigned long long* status) {
+    constexpr int kTile = kRounds * kScThreads;
     extern __shared__ __align__(16) unsigned char rs_dyn[];
-    uint64_t* sk = (uint64_t*)rs_dyn;                      // [kRsTile] keys grouped by digit
-    uint32_t* sv = (uint32_t*)(rs_dyn + kRsTile * 8);      // [kRsTile] values (kVals)
+    uint64_t* sk = (uint64_t*)rs_dyn;                      // [kTile] keys grouped by digit
+    uint32_t* sv = (uint32_t*)(rs_dyn + kTile * 8);        // [kTile] values (kVals)
     __shared__ uint32_t wcnt[kScWarps][256];   // per warp and digit: count, then tile-local start
     __shared__ uint32_t gdelta[256];   // global start minus tile-local start of each digit's run (mod 2^32)
     __shared__ uint32_t wtot[kScWarps];
@@ -426,19 +433,19 @@ __global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) os_scatter(const ui
     for (int i = threadIdx.x; i < kScWarps * 256; i += kScThreads) (&wcnt[0][0])[i] = 0;
     __syncthreads();
     const unsigned t = tile_sh;
-    const size_t tbase = (size_t)t * kRsTile;
-    const size_t wbase = tbase + (size_t)warp * (kScRounds * 32);
-    uint64_t k[kScRounds];
-    uint32_t v[kScRounds];
-    uint32_t rank[kScRounds];
+    const size_t tbase = (size_t)t * kTile;
+    const size_t wbase = tbase + (size_t)warp * (kRounds * 32);
+    uint64_t k[kRounds];
+    uint32_t v[kRounds];
+    uint32_t rank[kRounds];
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
-    for (int r = 0; r < kScRounds; ++r) {
+    for (int r = 0; r < kRounds; ++r) {
         const size_t i = wbase + (size_t)r * 32 + lane;
         k[r] = i < n ? keys_in[i] : 0ull;
     }
 #pragma unroll
-    for (int r = 0; r < kScRounds; ++r) {
+    for (int r = 0; r < kRounds; ++r) {
         const bool ok = wbase + (size_t)r * 32 + lane < n;
         const unsigned valid = __ballot_sync(0xffffffffu, ok);
         const unsigned dg = digit_of(k[r], shift);
@@ -451,7 +458,7 @@ __global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) os_scatter(const ui
     }
     if (kVals) {
 #pragma unroll
-        for (int r = 0; r < kScRounds; ++r) {
+        for (int r = 0; r < kRounds; ++r) {
             const size_t i = wbase + (size_t)r * 32 + lane;
             v[r] = i < n ? vals_in[i] : 0u;
         }
@@ -506,7 +513,7 @@ __global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) os_scatter(const ui
     }
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < kScRounds; ++r) {
+    for (int r = 0; r < kRounds; ++r) {
         if (rank[r] != 0xFFFFFFFFu) {
             const unsigned p = wcnt[warp][digit_of(k[r], shift)] + rank[r];
             sk[p] = k[r];
@@ -515,7 +522,7 @@ __global__ void __launch_bounds__(kScThreads, kVals ? 2 : 3) os_scatter(const ui
     }
     __syncthreads();
     if (gave_up) return;
-    const unsigned cnt = (unsigned)min((size_t)kRsTile, n - tbase);
+    const unsigned cnt = (unsigned)min((size_t)kTile, n - tbase);
     bool outside = false;
     for (unsigned p = threadIdx.x; p < cnt; p += kScThreads) {
         const uint64_t key = sk[p];
@@ -556,14 +563,22 @@ void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* va
     if (n >= (1ull << 32)) fail(-1, "radix_sort: more than 2^32 - 1 keys");
     if (status && n > kOneSweepMin) {
         const int passes = (bits + 7) / 8;
-        const size_t dyn_k = (size_t)kRsTile * 8, dyn_kv = (size_t)kRsTile * 12;
-        TJ_CUDA(cudaFuncSetAttribute(os_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_k));
-        TJ_CUDA(cudaFuncSetAttribute(os_scatter<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        // keys alone: 8192-key tiles; with values: 4096-key tiles
+        constexpr int kRoundsK = 16, kRoundsV = 8;
+        const size_t tile = (size_t)kScThreads * (vals ? kRoundsV : kRoundsK);
+        const size_t dyn_k = tile * 8, dyn_kv = tile * 12;
         if (vals) {
-            TJ_CUDA(cudaFuncSetAttribute(os_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_kv));
-            TJ_CUDA(cudaFuncSetAttribute(os_scatter<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+            TJ_CUDA(cudaFuncSetAttribute(os_scatter<true, kRoundsV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)dyn_kv));
+            TJ_CUDA(cudaFuncSetAttribute(os_scatter<true, kRoundsV>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         100));
+        } else {
+            TJ_CUDA(cudaFuncSetAttribute(os_scatter<false, kRoundsK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)dyn_k));
+            TJ_CUDA(cudaFuncSetAttribute(os_scatter<false, kRoundsK>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         100));
         }
-        const unsigned nb = (unsigned)((n + kRsTile - 1) / kRsTile);
+        const unsigned nb = (unsigned)((n + tile - 1) / tile);
         uint64_t* tstat = (uint64_t*)(((uintptr_t)ws + 15) & ~(uintptr_t)15);   // [nb][256]
         uint32_t* ghist = (uint32_t*)(tstat + (size_t)nb * 256);                // [passes][256]
         uint32_t* gstart = ghist + kOsMaxPasses * 256;                           // [passes][256]
@@ -573,19 +588,26 @@ void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* va
         const unsigned hb = (unsigned)std::min<size_t>((size_t)num_sms() * 4,
                                                        (n + kOsHistThreads * kOsHistKeys - 1) /
                                                            (kOsHistThreads * kOsHistKeys));
-        launch(os_hist, hb, kOsHistThreads, 0, st, (const uint64_t*)keys, n, passes, ghist);
+        switch (passes) {
+#define TJ_OSH(P) \
+    case P: launch(os_hist<P>, hb, kOsHistThreads, 0, st, (const uint64_t*)keys, n, ghist); break;
+            TJ_OSH(1) TJ_OSH(2) TJ_OSH(3) TJ_OSH(4) TJ_OSH(5) TJ_OSH(6) TJ_OSH(7) TJ_OSH(8)
+#undef TJ_OSH
+            default: fail(-1, "radix_sort: more than 64 key bits");
+        }
         launch(os_starts, (unsigned)passes, 256, 0, st, (const uint32_t*)ghist, gstart);
         uint64_t *kin = keys, *kout = keys_tmp;
         uint32_t *vin = vals, *vout = vals_tmp;
         for (int p = 0; p < passes; ++p) {
             TJ_CUDA(cudaMemsetAsync(tstat, 0, (size_t)nb * 256 * sizeof(uint64_t), st));
             if (vals)
-                launch(os_scatter<true>, nb, kScThreads, dyn_kv, st, (const uint64_t*)kin, (const uint32_t*)vin, kout,
-                       vout, n, 8 * p, (const uint32_t*)(gstart + p * 256), tstat, ctr + p, status);
-            else
-                launch(os_scatter<false>, nb, kScThreads, dyn_k, st, (const uint64_t*)kin, (const uint32_t*)nullptr,
-                       kout, (uint32_t*)nullptr, n, 8 * p, (const uint32_t*)(gstart + p * 256), tstat, ctr + p,
+                launch(os_scatter<true, kRoundsV>, nb, kScThreads, dyn_kv, st, (const uint64_t*)kin,
+                       (const uint32_t*)vin, kout, vout, n, 8 * p, (const uint32_t*)(gstart + p * 256), tstat, ctr + p,
                        status);
+            else
+                launch(os_scatter<false, kRoundsK>, nb, kScThreads, dyn_k, st, (const uint64_t*)kin,
+                       (const uint32_t*)nullptr, kout, (uint32_t*)nullptr, n, 8 * p, (const uint32_t*)(gstart + p * 256),
+                       tstat, ctr + p, status);
             std::swap(kin, kout);
             std::swap(vin, vout);
         }
