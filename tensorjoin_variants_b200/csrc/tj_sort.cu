@@ -116,6 +116,26 @@ TJ_DEV unsigned digit_peers(unsigned dg, unsigned valid) {
     }
     return peers;
 }
+// The same with each step as one three-input logic op (the single-sweep scatter).
+TJ_DEV unsigned digit_peers_lop3(unsigned dg, unsigned valid) {
+    unsigned peers = valid;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const unsigned bit = (dg >> b) & 1u;
+        const unsigned m = __ballot_sync(0xffffffffu, bit);
+        const unsigned ext = 0u - bit;   // all ones where the lane's bit is set
+        // peers &= ~(m ^ ext): the lanes whose bit b equals this lane's, in one three-input logic op
+        asm("lop3.b32 %0, %1, %2, %3, 0x90;" : "=r"(peers) : "r"(peers), "r"(m), "r"(ext));
+    }
+    return peers;
+}
+
+// Byte kByte of a key (a compile-time digit position: a constant shift and mask).
+template <int kByte>
+TJ_DEV unsigned key_byte(uint64_t k) {
+    const uint32_t w = kByte < 4 ? (uint32_t)k : (uint32_t)(k >> 32);
+    return (w >> (8 * (kByte & 3))) & 0xFFu;
+}
 
 __global__ void __launch_bounds__(kRsThreads) rs_hist(const uint64_t* keys, size_t n, int shift, uint32_t* hist,
                                                      unsigned nblocks) {
@@ -411,9 +431,9 @@ TJ_DEV void st_status(uint64_t* p, uint64_t v) {
 // kRounds keys per thread: 8 (4096-key tiles) with values, 16 (8192-key tiles, two blocks per SM)
 // for keys alone, which halves the tiles and with them the fixed per-tile cost (the barriers, the
 // digit scan and the look-back round trip) against the same traffic.
-template <bool kVals, int kRounds>
+template <bool kVals, int kRounds, int kByte>
 __global__ void __launch_bounds__(kScThreads, 2) os_scatter(const uint64_t* keys_in, const uint32_t* vals_in,
-                                                            uint64_t* keys_out, uint32_t* vals_out, size_t n, int shift,
+                                                            uint64_t* keys_out, uint32_t* vals_out, size_t n,
                                                             const uint32_t* gstart, uint64_t* tstat, uint32_t* tile_ctr,
                                                             unsigned long long* status) {
     constexpr int kTile = kRounds * kScThreads;
@@ -439,17 +459,16 @@ __global__ void __launch_bounds__(kScThreads, 2) os_scatter(const uint64_t* keys
     uint32_t v[kRounds];
     uint32_t rank[kRounds];
     const unsigned lt = (1u << lane) - 1u;
+    // keys of this warp's run that exist (n < 2^32, so 32-bit offsets)
+    const unsigned rem = wbase >= n ? 0u : (unsigned)min(n - wbase, (size_t)(kRounds * 32));
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) k[r] = (unsigned)(r * 32) + lane < rem ? keys_in[wbase + r * 32 + lane] : 0ull;
 #pragma unroll
     for (int r = 0; r < kRounds; ++r) {
-        const size_t i = wbase + (size_t)r * 32 + lane;
-        k[r] = i < n ? keys_in[i] : 0ull;
-    }
-#pragma unroll
-    for (int r = 0; r < kRounds; ++r) {
-        const bool ok = wbase + (size_t)r * 32 + lane < n;
+        const bool ok = (unsigned)(r * 32) + lane < rem;
         const unsigned valid = __ballot_sync(0xffffffffu, ok);
-        const unsigned dg = digit_of(k[r], shift);
-        const unsigned peers = digit_peers(dg, valid);
+        const unsigned dg = key_byte<kByte>(k[r]);
+        const unsigned peers = digit_peers_lop3(dg, valid);
         const unsigned prev = ok ? wcnt[warp][dg] : 0u;
         rank[r] = ok ? prev + __popc(peers & lt) : 0xFFFFFFFFu;
         __syncwarp();
@@ -458,10 +477,7 @@ __global__ void __launch_bounds__(kScThreads, 2) os_scatter(const uint64_t* keys
     }
     if (kVals) {
 #pragma unroll
-        for (int r = 0; r < kRounds; ++r) {
-            const size_t i = wbase + (size_t)r * 32 + lane;
-            v[r] = i < n ? vals_in[i] : 0u;
-        }
+        for (int r = 0; r < kRounds; ++r) v[r] = (unsigned)(r * 32) + lane < rem ? vals_in[wbase + r * 32 + lane] : 0u;
     }
     __syncthreads();
     {   // per digit (threads 0..255): the tile's count, published at once; its tile-local start, each
@@ -515,7 +531,7 @@ __global__ void __launch_bounds__(kScThreads, 2) os_scatter(const uint64_t* keys
 #pragma unroll
     for (int r = 0; r < kRounds; ++r) {
         if (rank[r] != 0xFFFFFFFFu) {
-            const unsigned p = wcnt[warp][digit_of(k[r], shift)] + rank[r];
+            const unsigned p = wcnt[warp][key_byte<kByte>(k[r])] + rank[r];
             sk[p] = k[r];
             if (kVals) sv[p] = v[r];
         }
@@ -526,8 +542,8 @@ __global__ void __launch_bounds__(kScThreads, 2) os_scatter(const uint64_t* keys
     bool outside = false;
     for (unsigned p = threadIdx.x; p < cnt; p += kScThreads) {
         const uint64_t key = sk[p];
-        const size_t pos = (size_t)(uint32_t)(gdelta[digit_of(key, shift)] + p);
-        if (pos >= n) {   // cannot happen with consistent counts; checked so that nothing lands outside
+        const uint32_t pos = gdelta[key_byte<kByte>(key)] + p;
+        if (pos >= (uint32_t)n) {   // cannot happen with consistent counts; checked so that nothing lands outside
             outside = true;
             continue;
         }
@@ -535,6 +551,29 @@ __global__ void __launch_bounds__(kScThreads, 2) os_scatter(const uint64_t* keys
         if (kVals) vals_out[pos] = sv[p];
     }
     if (outside) atomicOr(status, (unsigned long long)kStatusGuard);
+}
+
+// One single-sweep pass over digit `byte` (the kernel is compiled per digit position).
+template <bool kVals, int kRounds, int kByte>
+void os_scatter_launch(unsigned nb, size_t dyn, cudaStream_t st, const uint64_t* kin, const uint32_t* vin,
+                       uint64_t* kout, uint32_t* vout, size_t n, const uint32_t* gstart, uint64_t* tstat,
+                       uint32_t* ctr, unsigned long long* status) {
+    auto* f = os_scatter<kVals, kRounds, kByte>;
+    TJ_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    TJ_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    launch(f, nb, kScThreads, dyn, st, kin, vin, kout, vout, n, gstart, tstat, ctr, status);
+}
+template <bool kVals, int kRounds>
+void os_scatter_pass(int byte, unsigned nb, size_t dyn, cudaStream_t st, const uint64_t* kin, const uint32_t* vin,
+                     uint64_t* kout, uint32_t* vout, size_t n, const uint32_t* gstart, uint64_t* tstat, uint32_t* ctr,
+                     unsigned long long* status) {
+    switch (byte) {
+#define TJ_OSS(B) \
+    case B: os_scatter_launch<kVals, kRounds, B>(nb, dyn, st, kin, vin, kout, vout, n, gstart, tstat, ctr, status); break;
+        TJ_OSS(0) TJ_OSS(1) TJ_OSS(2) TJ_OSS(3) TJ_OSS(4) TJ_OSS(5) TJ_OSS(6) TJ_OSS(7)
+#undef TJ_OSS
+        default: fail(-1, "radix_sort: digit position out of range");
+    }
 }
 
 }  // namespace
@@ -567,17 +606,6 @@ void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* va
         constexpr int kRoundsK = 16, kRoundsV = 8;
         const size_t tile = (size_t)kScThreads * (vals ? kRoundsV : kRoundsK);
         const size_t dyn_k = tile * 8, dyn_kv = tile * 12;
-        if (vals) {
-            TJ_CUDA(cudaFuncSetAttribute(os_scatter<true, kRoundsV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)dyn_kv));
-            TJ_CUDA(cudaFuncSetAttribute(os_scatter<true, kRoundsV>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                         100));
-        } else {
-            TJ_CUDA(cudaFuncSetAttribute(os_scatter<false, kRoundsK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)dyn_k));
-            TJ_CUDA(cudaFuncSetAttribute(os_scatter<false, kRoundsK>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                         100));
-        }
         const unsigned nb = (unsigned)((n + tile - 1) / tile);
         uint64_t* tstat = (uint64_t*)(((uintptr_t)ws + 15) & ~(uintptr_t)15);   // [nb][256]
         uint32_t* ghist = (uint32_t*)(tstat + (size_t)nb * 256);                // [passes][256]
@@ -601,13 +629,11 @@ void radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_tmp, uint32_t* va
         for (int p = 0; p < passes; ++p) {
             TJ_CUDA(cudaMemsetAsync(tstat, 0, (size_t)nb * 256 * sizeof(uint64_t), st));
             if (vals)
-                launch(os_scatter<true, kRoundsV>, nb, kScThreads, dyn_kv, st, (const uint64_t*)kin,
-                       (const uint32_t*)vin, kout, vout, n, 8 * p, (const uint32_t*)(gstart + p * 256), tstat, ctr + p,
-                       status);
+                os_scatter_pass<true, kRoundsV>(p, nb, dyn_kv, st, kin, vin, kout, vout, n, gstart + p * 256, tstat,
+                                                ctr + p, status);
             else
-                launch(os_scatter<false, kRoundsK>, nb, kScThreads, dyn_k, st, (const uint64_t*)kin,
-                       (const uint32_t*)nullptr, kout, (uint32_t*)nullptr, n, 8 * p, (const uint32_t*)(gstart + p * 256),
-                       tstat, ctr + p, status);
+                os_scatter_pass<false, kRoundsK>(p, nb, dyn_k, st, kin, nullptr, kout, nullptr, n, gstart + p * 256,
+                                                 tstat, ctr + p, status);
             std::swap(kin, kout);
             std::swap(vin, vout);
         }
