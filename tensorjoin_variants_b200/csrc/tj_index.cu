@@ -978,7 +978,7 @@ TJ_DEV void prep_row(const float (&xa)[kE], const float (&cf)[kE], const double 
 // Y = sqrt(A (1 + 2 g)).  A non-finite element makes A non-finite, which flags the row.  The
 // centroid needs no accuracy (the radius is measured from the value written).
 template <int kScreen, int kSplit, int kE, int kL, bool kHalves>
-__global__ void __launch_bounds__(256) prep_tiles_kernel(const float* __restrict__ src, long long n, int d, int tile,
+__global__ void __launch_bounds__(256, 3) prep_tiles_kernel(const float* __restrict__ src, long long n, int d, int tile,
                                                          const uint32_t* __restrict__ perm,
                                                          const float* __restrict__ center,
                                                          const uint32_t* row0_in, const uint32_t* nvalid_in,
