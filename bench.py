@@ -79,6 +79,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle audit after the timed steps")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the other 16-bit operand format's run on the headline join")
     ap.add_argument("--configs", default="auto", choices=["auto", "none"],
                     help="auto: a default single-GPU run also measures the other configurations")
     ap.add_argument("--sub-steps", type=int, default=5, help="timed steps of each other configuration")
@@ -528,6 +530,43 @@ def bench_single(name: str, args, steps: int, warmup: int, rank: int, world: int
                              "note": "one run; the same index, candidates, refinement and sort as the "
                                      "tensor-core path, only the screen differs"}
         del resp, kp, Rp, Sp
+
+    # the other unsplit 16-bit operand format on the same join (FP16 against BF16): time, band, screen
+    # error against sequential FP64 and whether the pair set is the same
+    other = {"fp16": "bf16", "bf16": "fp16"}.get(screen)
+    if headline and other and not args.no_compare:
+        kwo = {k: v for k, v in knobs.items()}
+        for _ in range(2):
+            r_ = tj.join_result(R, S, eps2=T, mode=mode, screen=other, **kwo)
+            del r_
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k_cmp = 3
+        ost = []
+        e0.record(stream)
+        for _ in range(k_cmp):
+            r_ = tj.join_result(R, S, eps2=T, mode=mode, screen=other, **kwo)
+            ost.append(r_.stats)
+            del r_
+        e1.record(stream)
+        torch.cuda.synchronize()
+        oms = e0.elapsed_time(e1) / k_cmp
+        ro = tj.join_result(R, S, eps2=T, mode=mode, screen=other, **kwo)
+        same = bool(torch.equal(ro.keys(), keys_t))
+        del ro
+        rd = tj.join_result(R, S, eps2=T, mode=mode, screen=other, screen_diag=True)
+        sd = rd.stats
+        del rd
+        line["screens_compared"] = {
+            screen: {"ms_per_step": ms, "ms_screen": screen_ms, "band": st["band"],
+                     "refined_fraction": st["band"] / max(1, st["pairs_screened"]),
+                     "max_abs_err_d2": line.get("screen_error", {}).get("max_abs_err_d2")},
+            other: {"ms_per_step": oms, "ms_screen": statistics.mean(s["ms_screen"] for s in ost),
+                    "band": ost[-1]["band"], "refined_fraction": ost[-1]["band"] / max(1, ost[-1]["pairs_screened"]),
+                    "max_abs_err_d2": sd["screen_max_abs_err"],
+                    "max_err_over_certified_radius": sd["screen_err_over_bound"],
+                    "identical_pair_set": same, "steps": k_cmp},
+        }
 
     # end to end through the public API with host buffers (pinned inputs, host outputs)
     if not args.no_e2e:

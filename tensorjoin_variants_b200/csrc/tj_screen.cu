@@ -697,16 +697,26 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                         // magnitude bounds (so the same rounding allowance in tau); four three-input maxes
                         // and one FMA per 8 pairs; only the groups whose value passes tau are examined
                         // pair by pair
+                        // (the same test over the whole 32-column block first: one compare and branch
+                        // per block while no pair of the block is near the threshold)
                         const float4 gb = *reinterpret_cast<const float4*>(&m.gminB[col0 >> 3]);
                         const float gbv[4] = {gb.x, gb.y, gb.z, gb.w};
+                        float pmv[4];
 #pragma unroll
                         for (int g = 0; g < 4; ++g) {
                             const uint32_t* r8 = raw + 8 * g;
-                            const float pm = fmax3(fmax3(fmax3(__uint_as_float(r8[0]), __uint_as_float(r8[1]),
-                                                               __uint_as_float(r8[2])),
-                                                         __uint_as_float(r8[3]), __uint_as_float(r8[4])),
-                                                   fmaxf(__uint_as_float(r8[5]), __uint_as_float(r8[6])),
-                                                   __uint_as_float(r8[7]));
+                            pmv[g] = fmax3(fmax3(fmax3(__uint_as_float(r8[0]), __uint_as_float(r8[1]),
+                                                       __uint_as_float(r8[2])),
+                                                 __uint_as_float(r8[3]), __uint_as_float(r8[4])),
+                                           fmaxf(__uint_as_float(r8[5]), __uint_as_float(r8[6])),
+                                           __uint_as_float(r8[7]));
+                        }
+                        const float pblk = fmaxf(fmax3(pmv[0], pmv[1], pmv[2]), pmv[3]);
+                        const float bblk = fminf(fmin3(gbv[0], gbv[1], gbv[2]), gbv[3]);
+                        if (fmaf(-2.f, pblk, bblk) <= tau) {
+#pragma unroll
+                        for (int g = 0; g < 4; ++g) {
+                            const float pm = pmv[g];
                             if (fmaf(-2.f, pm, gbv[g]) <= tau) {
 #pragma unroll
                                 for (int k = 8 * g; k < 8 * g + 8; ++k) {
@@ -715,6 +725,7 @@ __global__ void __launch_bounds__(kScreenThreads, 1)
                                     im |= (v <= tau_in ? 1u : 0u) << k;
                                 }
                             }
+                        }
                         }
                     } else {
                         // v = fma(-2, p, B~) two pairs per packed FMA (rounded once, as fmaf), folded by
