@@ -506,6 +506,45 @@ __global__ void perm_local_kernel(const uint64_t* keys, const uint32_t* perm, co
     if (r < n) out[r] = (uint32_t)((long long)perm[r] - rowoff[keys[r] >> 32]);
 }
 
+// int14 sides: the rows of every 128-row tile put in order of their exact squared norm (ties by
+// position).  The int8-limb screens test 8 columns of an S tile at a time against the smallest norm of
+// the 8; with norms rising along the tile that bound stays close to every column's own.  A tile keeps
+// its rows (only their order inside it changes), so candidate tile pairs and results are unchanged.
+// Block per tile, a warp per row for the norms, rank by counting in shared memory.
+__global__ void __launch_bounds__(128) order_tile_rows_by_norm(const void* src, int dtype, long long n, int d,
+                                                              uint32_t* perm) {
+    __shared__ long long key[128];
+    __shared__ uint32_t pv[128];
+    const long long r0 = (long long)blockIdx.x * 128;
+    const int nv = (int)min(128ll, n - r0);
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = (int)warp; i < nv; i += 4) {
+        const uint32_t o = perm[r0 + i];
+        long long s = 0;
+        for (int k = (int)lane; k < d; k += 32) {
+            const long long q = (long long)load_x(src, dtype, (size_t)o * d + k);
+            s += q * q;
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (lane == 0) {
+            key[i] = s;
+            pv[i] = o;
+        }
+    }
+    __syncthreads();
+    const int t = (int)threadIdx.x;
+    if (t < nv) {
+        const long long kt = key[t];
+        int rank = 0;
+        for (int u = 0; u < nv; ++u) {
+            const long long ku = key[u];
+            rank += (ku < kt || (ku == kt && u < t)) ? 1 : 0;
+        }
+        perm[r0 + rank] = pv[t];
+    }
+}
+
 // Concatenate many row-major matrices (one per join) into one: row r of the output comes from the
 // source whose row range contains r.
 __global__ void gather_rows_kernel(const void* const* srcs, const long long* rowoff, int nsrc, long long nrows,
@@ -1919,6 +1958,11 @@ void prepare_side(Side& s, const FrameParams* fpd, bool pca_frame, const float* 
             std::swap(s.keys, ktmp);
             std::swap(s.perm, vtmp);
         }
+        // joins on int14 rows (one join, 128-row tiles): rows inside each tile by norm (the sorted
+        // keys are not read again on this path)
+        if (i8 && ts && tile == 128 && s.njc <= 1)
+            launch(order_tile_rows_by_norm, (unsigned)((n + 127) / 128), 128, 0, st, s.src, s.dtype, n, s.d,
+                   s.perm.p);
     }
     s.emit = s.perm.p;
     const size_t rp = (size_t)s.rows_pad;

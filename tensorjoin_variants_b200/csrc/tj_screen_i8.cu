@@ -733,29 +733,33 @@ __global__ void __launch_bounds__(kHHThreads, 1)
                 for (int h = 0; h < 2; ++h) {
                     const unsigned cc = pass * 64 + h * 32;
                     const uint32_t (&hv)[32] = hv2[h];
-                    // per-pair fast test folded over the 32-column block: hh_j - b_j < a_iJ for every
-                    // column proves the block out (one subtract per pair, b_j four at a time from the
-                    // metadata, three-input maxima on two chains).  A group-wise max hh - min b test
-                    // let most warps into the per-pair loop: on uniform int14 rows some lane's group
-                    // passed in nearly every block.
-                    const int4* b4 = reinterpret_cast<const int4*>(&m.bq[cc]);
-                    int mx0 = INT_MIN, mx1 = INT_MIN;
+                    // group fast test: hh_j - b_j <= max hh - min b over 8 columns, so
+                    // max hh - min b < a_iJ proves the whole group out.  The rows of every S tile are in
+                    // order of their norms (index build), so the group's min b is close to each b_j: on
+                    // uniform int14 rows about 4 % of the warp's 32-column blocks have a lane whose group
+                    // passes (22 % in Morton order, where a per-pair subtract was the cheaper test).
+                    const int4 gb = *reinterpret_cast<const int4*>(&m.gminb[cc >> 3]);
+                    const int gbv[4] = {gb.x, gb.y, gb.z, gb.w};
+                    unsigned gmask = 0;
 #pragma unroll
-                    for (int g = 0; g < 8; ++g) {
-                        const int4 bb = b4[g];
-                        const int t0 = (int)hv[4 * g] - bb.x, t1 = (int)hv[4 * g + 1] - bb.y;
-                        const int t2 = (int)hv[4 * g + 2] - bb.z, t3 = (int)hv[4 * g + 3] - bb.w;
-                        mx0 = __vimax3_s32(mx0, t0, t1);
-                        mx1 = __vimax3_s32(mx1, t2, t3);
+                    for (int g = 0; g < 4; ++g) {
+                        const uint32_t* h8 = hv + 8 * g;
+                        const int a3 = __vimax3_s32((int)h8[0], (int)h8[1], (int)h8[2]);
+                        const int b3 = __vimax3_s32((int)h8[3], (int)h8[4], (int)h8[5]);
+                        const int gm = __vimax3_s32(a3, b3, max((int)h8[6], (int)h8[7]));
+                        gmask |= (gm - gbv[g] >= ai ? 1u : 0u) << g;
                     }
-                    const bool hit = max(mx0, mx1) >= ai;
-                    if (!__any_sync(0xffffffffu, hit)) continue;
+                    if (!__any_sync(0xffffffffu, gmask != 0)) continue;
                     uint32_t cmask = 0;
-                    if (hit) {   // b_j read again (volatile): keeping the differences live would spill
+                    if (gmask) {   // b_j read again (volatile): nothing of the group test stays live
                         const volatile int* bqv = &m.bq[cc];
 #pragma unroll
-                        for (int k = 0; k < 32; ++k)
-                            cmask |= ((int)hv[k] - bqv[k] >= ai ? 1u : 0u) << k;
+                        for (int g = 0; g < 4; ++g) {
+                            if (!(gmask & (1u << g))) continue;
+#pragma unroll
+                            for (int k = 8 * g; k < 8 * g + 8; ++k)
+                                cmask |= ((int)hv[k] - bqv[k] >= ai ? 1u : 0u) << k;
+                        }
                     }
                     cmask &= valid_cols(m.nvJ, cc);
                     if (jp.self_join && cmask) {   // keep sorted column > sorted row only
