@@ -502,33 +502,43 @@ __global__ void __launch_bounds__(kI8Threads, 1)
 // idle, warps 4..15 epilogue in three groups of four that take alternate items (warp w reads TMEM
 // lanes 32 (w % 4).., all 128 columns in two passes of 64), so three warps per SM sub-partition
 // overlap their items' latency.
-constexpr int kHHStages = 6;                      // S k-blocks in flight (16 KB each)
-constexpr int kHHMeta = 8;                        // items of column metadata in flight (each group sees several)
-constexpr int kHHMaxKb = 2;                       // resident R k-blocks (kpad <= 256)
+constexpr int kHHMaxKb = 2;                       // resident R k-blocks at most (kpad <= 256)
 constexpr int kHHAcc = 4;                         // TMEM accumulators of 128 columns
 constexpr int kHHEpi = 12;                        // three groups of four warps, taking alternate items
 constexpr int kHHGroups = kHHEpi / 4;
 constexpr int kHHEpiFirst = 4;
 constexpr int kHHThreads = (kHHEpiFirst + kHHEpi) * 32;
-constexpr unsigned kHHABytes = kHHMaxKb * kPart;  // one resident R tile
 
-struct HHCtl {
+// Shared-memory plan per resident R k-block count: the double-buffered R tile, then as many 16 KB
+// S k-block stages as fit (the MMA waits on S tiles that come from HBM: 6 -> 8 stages took the
+// 2M-row int14 screen from 561 to 540 ms), and per-item column metadata for every staged item plus
+// the four held in TMEM accumulators.
+template <int kMaxKb> struct HHCfg {
+    static constexpr int kStages = kMaxKb == 1 ? 10 : 8;
+    static constexpr int kMeta = kStages + kHHAcc;
+    static constexpr unsigned kABytes = kMaxKb * kPart;   // one resident R tile
+};
+
+template <int kStages, int kMeta> struct HHCtl {
     uint64_t a_full[2];
     uint64_t a_empty[2];
-    uint64_t full[kHHStages];
-    uint64_t empty[kHHStages];
+    uint64_t full[kStages];
+    uint64_t empty[kStages];
     uint64_t acc_full[kHHAcc];
     uint64_t acc_empty[kHHAcc];
-    uint64_t meta_full[kHHMeta];
-    uint64_t meta_empty[kHHMeta];
+    uint64_t meta_full[kMeta];
+    uint64_t meta_empty[kMeta];
     uint64_t drain;
     unsigned tmem_base;
     int abort_flag;
 };
 
-constexpr size_t kHHSmem = 1024 + 2 * (size_t)kHHABytes + (size_t)kHHStages * kPart + kHHMeta * sizeof(ColMetaI8) +
-                           sizeof(HHCtl);
-static_assert(kHHSmem <= 232448, "227 KB of shared memory per CTA at most");
+template <int kMaxKb> constexpr size_t hh_smem() {
+    using C = HHCfg<kMaxKb>;
+    return 1024 + 2 * (size_t)C::kABytes + (size_t)C::kStages * kPart + C::kMeta * sizeof(ColMetaI8) +
+           sizeof(HHCtl<C::kStages, C::kMeta>);
+}
+static_assert(hh_smem<1>() <= 232448 && hh_smem<2>() <= 232448, "227 KB of shared memory per CTA at most");
 
 struct HHArgs {
     I8Args b;                  // tile tables, row data, threshold, output (as the four-product screen)
@@ -536,9 +546,14 @@ struct HHArgs {
     unsigned long long band_cap;
 };
 
+template <int kMaxKb>
 __global__ void __launch_bounds__(kHHThreads, 1)
     screen_i8_hh_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                         const HHArgs ha) {
+    constexpr int kHHStages = HHCfg<kMaxKb>::kStages;
+    constexpr int kHHMeta = HHCfg<kMaxKb>::kMeta;
+    constexpr unsigned kHHABytes = HHCfg<kMaxKb>::kABytes;
+    using HHCtl = tj::HHCtl<kHHStages, kHHMeta>;
     const I8Args& a = ha.b;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -873,8 +888,15 @@ void screen_i8(const ScreenInput& g, const EmitBuffers& eb, cudaStream_t st) {
         ha.b = a;
         ha.band = eb.band;
         ha.band_cap = eb.band_cap;
-        TJ_CUDA(cudaFuncSetAttribute(screen_i8_hh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHHSmem));
-        launch(screen_i8_hh_kernel, num_sms(), kHHThreads, kHHSmem, st, tmA, tmB, ha);
+        if (a.kblocks == 1) {
+            TJ_CUDA(cudaFuncSetAttribute(screen_i8_hh_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)hh_smem<1>()));
+            launch(screen_i8_hh_kernel<1>, num_sms(), kHHThreads, hh_smem<1>(), st, tmA, tmB, ha);
+        } else {
+            TJ_CUDA(cudaFuncSetAttribute(screen_i8_hh_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)hh_smem<2>()));
+            launch(screen_i8_hh_kernel<2>, num_sms(), kHHThreads, hh_smem<2>(), st, tmA, tmB, ha);
+        }
         return;
     }
     TJ_CUDA(cudaFuncSetAttribute(screen_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kI8Smem));
