@@ -53,6 +53,19 @@ struct PlainArgs {
     Counters* ctr;
 };
 
+// a0 += (r - s0)^2, a1 += (r - s1)^2 as one packed FP32x2 subtract and one packed FP32x2 FMA (sm_100);
+// each lane is rounded exactly as the scalar subtract and fmaf
+TJ_DEV void sqdiff_acc_x2(float r, float s0, float s1, float& a0, float& a1) {
+    asm("{\n\t.reg .b64 x, y, t, c;\n\t"
+        "mov.b64 x, {%2, %2};\n\t"
+        "mov.b64 y, {%3, %4};\n\t"
+        "mov.b64 c, {%0, %1};\n\t"
+        "sub.rn.f32x2 t, x, y;\n\t"
+        "fma.rn.f32x2 c, t, t, c;\n\t"
+        "mov.b64 {%0, %1}, c;\n\t}"
+        : "+f"(a0), "+f"(a1) : "f"(r), "f"(s0), "f"(s1));
+}
+
 __global__ void __launch_bounds__(kPT, 1) plain_kernel(const PlainArgs a) {
     __shared__ float sR[kPK][kTileR + 1];   // +1: conflict-free transposed stores
     __shared__ float sS[kPK][kTileS + 1];
@@ -98,10 +111,8 @@ __global__ void __launch_bounds__(kPT, 1) plain_kernel(const PlainArgs a) {
 #pragma unroll
                     for (int i = 0; i < kPR; ++i)
 #pragma unroll
-                        for (int j = 0; j < kPC; ++j) {
-                            const float t = rv[i] - sv[j];
-                            acc[i][j] = fmaf(t, t, acc[i][j]);
-                        }
+                        for (int j = 0; j < kPC; j += 2)
+                            sqdiff_acc_x2(rv[i], sv[j], sv[j + 1], acc[i][j], acc[i][j + 1]);
                 }
             }
             // classify: groups of 32 pairs (2 rows x 16 cols) so that emission stays warp-uniform
